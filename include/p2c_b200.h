@@ -1,0 +1,210 @@
+/*
+ * p2c_b200.h — C ABI of the B200 (sm_100a) certification hot path of P2C-CCD.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns an
+ * int status (P2C_OK = 0) and leaves a message for p2c_last_error() on failure.
+ * Pointers named `*_dev` are device pointers; `*_host` are host pointers.  All
+ * device work is issued on the caller's `stream` (a cudaStream_t passed as
+ * void*, NULL = legacy default stream) and is asynchronous unless the entry
+ * point says otherwise.
+ *
+ * Record layouts are byte-identical to the reference's host structs so that a
+ * std::vector of reference primitives can be handed over without repacking:
+ *   p2c_point_triangle == p2cccd::PointTriangleIntervalPrimitive (240 B)
+ *   p2c_edge_edge      == p2cccd::EdgeEdgeIntervalPrimitive      (240 B)
+ *   p2c_interval_result== p2cccd::PrimitiveIntervalResult        (72 B)
+ * (reference: src/cpp/certificate/certificate_engine.h:32-81).
+ */
+#ifndef P2C_B200_H_
+#define P2C_B200_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define P2C_OK 0
+#define P2C_ERR_INVALID 1  /* invalid argument; the reference raises ValueError */
+#define P2C_ERR_CUDA 2     /* a CUDA runtime call failed */
+#define P2C_ERR_CAPACITY 3 /* an output buffer was too small; required size reported */
+#define P2C_ERR_TIMEOUT 4  /* a bounded device wait gave up (error word set) */
+
+/* CertificateStatus (reference: src/cpp/common/runtime_contracts.h:20-24) */
+#define P2C_STATUS_COLLISION 0
+#define P2C_STATUS_SEPARATION 1
+#define P2C_STATUS_UNDECIDED 2
+
+/* ExactFeatureFamilyMask (reference: certificate_engine.h:12-15) */
+#define P2C_FAMILY_POINT_TRIANGLE 1u
+#define P2C_FAMILY_EDGE_EDGE 2u
+
+/* CertificateReasonCode (reference: certificate_engine.h:17-22) */
+#define P2C_REASON_NONE 0
+#define P2C_REASON_MISSING_GEOMETRY 1
+#define P2C_REASON_MAX_SUBDIVISION_DEPTH 2
+#define P2C_REASON_INVALID_INPUT 3
+
+/* CertificateRefinementMode (reference: runtime_contracts.h:26-31) */
+#define P2C_REFINE_NONE 0
+#define P2C_REFINE_BISECT_INTERVAL 1
+#define P2C_REFINE_REQUEST_GEOMETRY 2
+#define P2C_REFINE_ESCALATE_PRECISION 3
+
+/* ---- records ------------------------------------------------------------ */
+typedef struct p2c_trajectory {            /* LinearVertexTrajectory, 56 B */
+  int64_t feature_id;
+  double position_t0[3];
+  double position_t1[3];
+} p2c_trajectory;
+
+typedef struct p2c_point_triangle {        /* PointTriangleIntervalPrimitive, 240 B */
+  int64_t point_id;
+  int64_t triangle_id;
+  p2c_trajectory point;
+  p2c_trajectory triangle_v0;
+  p2c_trajectory triangle_v1;
+  p2c_trajectory triangle_v2;
+} p2c_point_triangle;
+
+typedef struct p2c_edge_edge {             /* EdgeEdgeIntervalPrimitive, 240 B */
+  int64_t edge_a_id;
+  int64_t edge_b_id;
+  p2c_trajectory edge_a0;
+  p2c_trajectory edge_a1;
+  p2c_trajectory edge_b0;
+  p2c_trajectory edge_b1;
+} p2c_edge_edge;
+
+typedef struct p2c_interval_result {       /* PrimitiveIntervalResult, 72 B */
+  uint8_t status;                          /* P2C_STATUS_* */
+  uint8_t pad0[3];
+  uint32_t covered_feature_mask;
+  double interval_t0;
+  double interval_t1;
+  double toi_upper;
+  double safe_margin_lb;
+  uint8_t witness_family;
+  uint8_t pad1[7];
+  int64_t witness_id_a;
+  int64_t witness_id_b;
+  uint16_t reason_code;
+  uint8_t next_refinement_mode;
+  uint8_t pad2[5];
+} p2c_interval_result;
+
+typedef struct p2c_cert_config {           /* CertificateEngineConfig */
+  double eps_time;
+  double eps_space;
+  uint16_t max_subdivision_depth;
+  uint16_t pad[3];
+} p2c_cert_config;
+
+/* Aggregated work-item certificate, the reduction CertificateEngine::Evaluate
+ * performs over its VF then EE primitive lists (certificate_engine.cpp:729-824). */
+typedef struct p2c_query_certificate {
+  uint8_t status;
+  uint8_t witness_family;
+  uint16_t reason_code;
+  uint32_t covered_feature_mask;
+  double toi_upper;
+  double safe_margin_lb;
+  int64_t witness_id_a;
+  int64_t witness_id_b;
+  int64_t witness_index;                   /* position of the witness primitive in its list, -1 if none */
+  uint8_t next_refinement_mode;
+  uint8_t pad[7];
+} p2c_query_certificate;
+
+/* Device-side counters of one certification launch. */
+typedef struct p2c_certify_stats {
+  uint64_t nodes_evaluated;                /* interval nodes whose mid sample was evaluated */
+  uint64_t distance_evals;                 /* distance evaluations (3 per root + 1 per child) */
+  uint64_t fp64_ops;                       /* counted FP64 add/sub/mul/div/sqrt (census launches only) */
+  uint64_t donations;                      /* subtrees handed between lanes of a warp */
+  uint64_t queries;                        /* queries certified */
+  uint64_t error_word;                     /* nonzero if a bounded wait or a capacity check failed */
+} p2c_certify_stats;
+
+/* ---- library ------------------------------------------------------------ */
+const char* p2c_last_error(void);
+int p2c_abi_version(void);
+/* Replaces IsCudaExactBuilt (src/cpp/certificate/certificate_cuda.h:10). */
+int p2c_is_cuda_exact_built(void);
+/* Device properties the kernels are sized from (SM count, smem per block). */
+int p2c_device_info(int* sm_count, int* max_smem_per_block, int* cc_major, int* cc_minor);
+
+/* ---- narrow phase: batch interval certificates ------------------------- */
+/* Scratch bytes the device entry points below need for a batch of n primitives. */
+size_t p2c_certify_workspace_bytes(int64_t n);
+
+/* Replaces EvaluatePointTriangleBatchCuda (certificate_cuda.h:11-15), with
+ * device pointers, a caller stream and caller-owned scratch.  Results are
+ * bit-identical to EvaluatePointTriangleInterval (certificate_engine.cpp:481-515)
+ * applied to each primitive.  stats_dev may be NULL. */
+int p2c_certify_pt_batch(const p2c_point_triangle* prims_dev, int64_t n,
+                         double interval_t0, double interval_t1,
+                         const p2c_cert_config* config,
+                         p2c_interval_result* results_dev,
+                         void* workspace_dev, size_t workspace_bytes,
+                         p2c_certify_stats* stats_dev, void* stream);
+
+/* Replaces EvaluateEdgeEdgeBatchCuda (certificate_cuda.h:16-20). */
+int p2c_certify_ee_batch(const p2c_edge_edge* prims_dev, int64_t n,
+                         double interval_t0, double interval_t1,
+                         const p2c_cert_config* config,
+                         p2c_interval_result* results_dev,
+                         void* workspace_dev, size_t workspace_bytes,
+                         p2c_certify_stats* stats_dev, void* stream);
+
+/* Both families in one persistent launch (point-triangle list, then
+ * edge-edge list, as CrossCheckCpuCudaExact takes them, certificate_cuda.h:21-26);
+ * each result equals the single-family entry points'.  Either list may be empty. */
+int p2c_certify_batch2(const p2c_point_triangle* pt_dev, int64_t n_pt,
+                       const p2c_edge_edge* ee_dev, int64_t n_ee,
+                       double interval_t0, double interval_t1,
+                       const p2c_cert_config* config,
+                       p2c_interval_result* pt_results_dev,
+                       p2c_interval_result* ee_results_dev,
+                       void* workspace_dev, size_t workspace_bytes,
+                       p2c_certify_stats* stats_dev, void* stream);
+
+/* Host-buffer forms with the reference's ownership model (host-owned arrays,
+ * synchronous, library-managed device memory): the drop-in for the pybind
+ * `evaluate_point_triangle_batch_cuda` / `evaluate_edge_edge_batch_cuda`
+ * (src/cpp/bindings/py_module.cpp:1972-1983).  n == 0 returns P2C_OK. */
+int p2c_certify_pt_batch_host(const p2c_point_triangle* prims_host, int64_t n,
+                              double interval_t0, double interval_t1,
+                              const p2c_cert_config* config,
+                              p2c_interval_result* results_host);
+int p2c_certify_ee_batch_host(const p2c_edge_edge* prims_host, int64_t n,
+                              double interval_t0, double interval_t1,
+                              const p2c_cert_config* config,
+                              p2c_interval_result* results_host);
+
+/* Census launch: the same certifier with lane-local depth-first order (the
+ * reference's node set exactly) and FP64 operation counting.  Used to state the
+ * algorithmic FP64 work of a batch; not a production path. */
+int p2c_certify_census(const p2c_point_triangle* pt_dev, int64_t n_pt,
+                       const p2c_edge_edge* ee_dev, int64_t n_ee,
+                       double interval_t0, double interval_t1,
+                       const p2c_cert_config* config,
+                       p2c_interval_result* pt_results_dev,
+                       p2c_interval_result* ee_results_dev,
+                       void* workspace_dev, size_t workspace_bytes,
+                       p2c_certify_stats* stats_dev, void* stream);
+
+/* ---- diagnostics ------------------------------------------------------- */
+/* FP64 throughput probe: launches independent separately rounded multiply/add
+ * chains over a full-occupancy grid and reports the FP64 operations it issues;
+ * the caller times it (CUDA events) to obtain the measured FP64 rate that the
+ * certifier's roofline is quoted against.  No reference counterpart. */
+int p2c_probe_fp64(void* out_dev, int iters, long long* fp64_ops_out, void* stream);
+
+#ifdef __cplusplus
+}  /* extern "C" */
+#endif
+
+#endif  /* P2C_B200_H_ */

@@ -1,0 +1,279 @@
+"""Python access to the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+Two checkers, both loaded with ctypes:
+  * ``_build/libccd_oracle.so``: ccd_oracle.c, a plain-C restatement of the
+    reference algorithms (certifier, aggregation, swept boxes, sort-and-sweep
+    pairs, group any-hit with fallback replay, refinement children);
+  * ``_ref/libp2c_ref.so``: the reference's own sources compiled unchanged with
+    ref_abi.cpp (present when the reference checkout was available at build
+    time; the built file travels with the tree).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this package.  The product library never does.
+"""
+from __future__ import annotations
+
+import ctypes
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ORACLE_SO = HERE / "_build" / "libccd_oracle.so"
+REF_SO = HERE / "_ref" / "libp2c_ref.so"
+
+TRAJ = np.dtype([("feature_id", "<i8"), ("position_t0", "<f8", (3,)), ("position_t1", "<f8", (3,))])
+PT = np.dtype([("point_id", "<i8"), ("triangle_id", "<i8"), ("point", TRAJ), ("triangle_v0", TRAJ),
+               ("triangle_v1", TRAJ), ("triangle_v2", TRAJ)])
+EE = np.dtype([("edge_a_id", "<i8"), ("edge_b_id", "<i8"), ("edge_a0", TRAJ), ("edge_a1", TRAJ),
+               ("edge_b0", TRAJ), ("edge_b1", TRAJ)])
+RESULT = np.dtype({
+    "names": ["status", "covered_feature_mask", "interval_t0", "interval_t1", "toi_upper", "safe_margin_lb",
+              "witness_family", "witness_id_a", "witness_id_b", "reason_code", "next_refinement_mode"],
+    "formats": ["u1", "<u4", "<f8", "<f8", "<f8", "<f8", "u1", "<i8", "<i8", "<u2", "u1"],
+    "offsets": [0, 4, 8, 16, 24, 32, 40, 48, 56, 64, 66],
+    "itemsize": 72,
+})
+QUERY_CERT = np.dtype({
+    "names": ["status", "witness_family", "reason_code", "covered_feature_mask", "toi_upper", "safe_margin_lb",
+              "witness_id_a", "witness_id_b", "witness_index", "next_refinement_mode"],
+    "formats": ["u1", "u1", "<u2", "<u4", "<f8", "<f8", "<i8", "<i8", "<i8", "u1"],
+    "offsets": [0, 1, 2, 4, 8, 16, 24, 32, 40, 48],
+    "itemsize": 56,
+})
+
+
+class _Cfg(ctypes.Structure):
+    _fields_ = [("eps_time", ctypes.c_double), ("eps_space", ctypes.c_double),
+                ("max_subdivision_depth", ctypes.c_uint16), ("pad", ctypes.c_uint16 * 3)]
+
+
+def build() -> None:
+    """Compile the oracle (always) and the reference library (when its sources exist)."""
+    subprocess.run(["make", "-s", "-C", str(HERE), "all"], check=True)
+
+
+_oracle = None
+_ref = None
+
+
+def _p(a):
+    return None if a is None else ctypes.c_void_p(a.ctypes.data)
+
+
+def lib() -> ctypes.CDLL:
+    global _oracle
+    if _oracle is None:
+        if not ORACLE_SO.exists():
+            build()
+        _oracle = ctypes.CDLL(str(ORACLE_SO))
+        L = _oracle
+        vp, i64, f64 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double
+        L.oracle_eval_pt_batch.argtypes = [vp, i64, f64, f64, ctypes.POINTER(_Cfg), vp, vp, vp]
+        L.oracle_eval_ee_batch.argtypes = [vp, i64, f64, f64, ctypes.POINTER(_Cfg), vp, vp, vp]
+        L.oracle_eval_pt_batch.restype = i64
+        L.oracle_eval_ee_batch.restype = i64
+        L.oracle_aggregate.argtypes = [ctypes.c_uint32, f64, vp, i64, vp, i64, vp]
+        L.oracle_swept_boxes.argtypes = [vp, vp, vp, ctypes.c_int, i64, f64, vp]
+        for name in ("oracle_vf_pairs_brute", "oracle_vf_pairs_sweep"):
+            getattr(L, name).argtypes = [vp, vp, vp, i64, vp, vp, vp, i64, vp, ctypes.c_int32, vp, i64]
+            getattr(L, name).restype = i64
+        for name in ("oracle_ee_pairs_brute", "oracle_ee_pairs_sweep"):
+            getattr(L, name).argtypes = [vp, vp, vp, i64, vp, ctypes.c_int32, vp, i64]
+            getattr(L, name).restype = i64
+        L.oracle_object_allowed.argtypes = [vp, vp, vp, i64, ctypes.c_int32, f64, ctypes.c_int, vp]
+        L.oracle_group_anyhit.argtypes = [i64, vp, vp, ctypes.c_int32, vp, vp, vp, vp, vp, vp]
+        L.oracle_refinement_children.argtypes = [f64, f64, ctypes.c_uint16, ctypes.c_uint8, ctypes.c_uint8, f64,
+                                                 ctypes.c_uint16, f64, vp, vp]
+        L.oracle_refinement_children.restype = ctypes.c_int
+    return _oracle
+
+
+def ref_available() -> bool:
+    return REF_SO.exists()
+
+
+def ref() -> ctypes.CDLL:
+    global _ref
+    if _ref is None:
+        if not REF_SO.exists():
+            raise FileNotFoundError(f"{REF_SO} is not built (the reference sources were not available)")
+        _ref = ctypes.CDLL(str(REF_SO))
+        R = _ref
+        vp, i64, f64, ci = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int
+        R.ref_last_error.restype = ctypes.c_char_p
+        for name in ("ref_eval_pt_batch", "ref_eval_ee_batch"):
+            getattr(R, name).argtypes = [vp, i64, f64, f64, f64, f64, ci, vp, vp, ci]
+            getattr(R, name).restype = i64
+        for name in ("ref_eval_pt_one", "ref_eval_ee_one"):
+            getattr(R, name).argtypes = [vp, f64, f64, f64, f64, ci, vp]
+            getattr(R, name).restype = ci
+        R.ref_evaluate_query.argtypes = [ctypes.c_uint32, f64, f64, f64, f64, ci, vp, i64, vp, i64, vp]
+        R.ref_build_mesh_query.argtypes = [vp, i64, vp, i64, vp, vp, vp, i64, vp, i64, vp, vp, ctypes.c_uint32,
+                                           ci, ctypes.c_uint64, ctypes.c_uint64, vp, vp, vp, vp]
+        R.ref_refinement_children.argtypes = [f64, f64, ctypes.c_uint16, ctypes.c_uint8, ctypes.c_uint8, f64,
+                                              ctypes.c_uint16, f64, vp, vp]
+        R.ref_refinement_children.restype = ci
+    return _ref
+
+
+def _family(records: np.ndarray) -> int:
+    if records.dtype.itemsize != 240:
+        raise ValueError("records must be 240-byte primitives")
+    return 1 if records.dtype.names[0] == "point_id" else 2
+
+
+def eval_batch(records: np.ndarray, t0: float = 0.0, t1: float = 1.0, eps_time: float = 1e-4,
+               eps_space: float = 1e-6, max_depth: int = 32):
+    """Oracle certificates: returns (results RESULT array, status uint8 (0 ok / 1 invalid), nodes uint64)."""
+    rec = np.ascontiguousarray(records)
+    n = len(rec)
+    out = np.zeros(n, dtype=RESULT)
+    status = np.zeros(n, dtype=np.uint8)
+    nodes = np.zeros(n, dtype=np.uint64)
+    cfg = _Cfg(eps_time, eps_space, max_depth)
+    fn = lib().oracle_eval_pt_batch if _family(rec) == 1 else lib().oracle_eval_ee_batch
+    fn(_p(rec), n, t0, t1, ctypes.byref(cfg), _p(out), _p(status), _p(nodes))
+    return out, status, nodes
+
+
+def ref_eval_batch(records: np.ndarray, t0: float = 0.0, t1: float = 1.0, eps_time: float = 1e-4,
+                   eps_space: float = 1e-6, max_depth: int = 32, threads: int = 1):
+    """Reference certificates (unchanged reference code): (results, status)."""
+    rec = np.ascontiguousarray(records)
+    n = len(rec)
+    out = np.zeros(n, dtype=RESULT)
+    status = np.zeros(n, dtype=np.uint8)
+    fn = ref().ref_eval_pt_batch if _family(rec) == 1 else ref().ref_eval_ee_batch
+    fn(_p(rec), n, t0, t1, eps_time, eps_space, max_depth, _p(out), _p(status), threads)
+    return out, status
+
+
+def ref_eval_error(record: np.ndarray, t0: float, t1: float, eps_time: float, eps_space: float,
+                   max_depth: int) -> str | None:
+    """Error message the reference raises for one primitive (None if it succeeds)."""
+    rec = np.ascontiguousarray(record.reshape(1))
+    out = np.zeros(1, dtype=RESULT)
+    fn = ref().ref_eval_pt_one if _family(rec) == 1 else ref().ref_eval_ee_one
+    rc = fn(_p(rec), t0, t1, eps_time, eps_space, max_depth, _p(out))
+    return ref().ref_last_error().decode() if rc else None
+
+
+def aggregate(family_mask: int, pt_results: np.ndarray, ee_results: np.ndarray,
+              interval_t1: float = 1.0) -> np.ndarray:
+    out = np.zeros(1, dtype=QUERY_CERT)
+    pt_r = np.ascontiguousarray(pt_results)
+    ee_r = np.ascontiguousarray(ee_results)
+    lib().oracle_aggregate(family_mask, interval_t1, _p(pt_r), len(pt_r), _p(ee_r), len(ee_r), _p(out))
+    return out[0]
+
+
+def ref_evaluate_query(family_mask: int, pts: np.ndarray, ees: np.ndarray, t0: float = 0.0, t1: float = 1.0,
+                       eps_time: float = 1e-4, eps_space: float = 1e-6, max_depth: int = 32):
+    out = np.zeros(1, dtype=QUERY_CERT)
+    a = np.ascontiguousarray(pts)
+    b = np.ascontiguousarray(ees)
+    rc = ref().ref_evaluate_query(family_mask, t0, t1, eps_time, eps_space, max_depth, _p(a), len(a), _p(b),
+                                  len(b), _p(out))
+    if rc:
+        raise ValueError(ref().ref_last_error().decode())
+    return out[0]
+
+
+def swept_boxes(v_t0: np.ndarray, v_t1: np.ndarray, prim_vertices: np.ndarray | None, k: int,
+                thickness: float = 0.0) -> np.ndarray:
+    v_t0 = np.ascontiguousarray(v_t0, dtype=np.float64)
+    v_t1 = np.ascontiguousarray(v_t1, dtype=np.float64)
+    if prim_vertices is None:
+        n = len(v_t0)
+        pv = None
+    else:
+        pv = np.ascontiguousarray(prim_vertices, dtype=np.int32)
+        n = pv.shape[0]
+    out = np.zeros((n, 6), dtype=np.float64)
+    lib().oracle_swept_boxes(_p(v_t0), _p(v_t1), _p(pv), k, n, thickness, _p(out))
+    return out
+
+
+def _pairs(fn, *args, cap: int | None = None) -> np.ndarray:
+    n = fn(*args, None, 0)
+    out = np.zeros(max(n, 1), dtype=np.uint64)
+    fn(*args, _p(out), n)
+    return out[:n]
+
+
+def vf_pairs(vbox, v_obj, v_valid, fbox, f_obj, faces, allowed, method: str = "sweep") -> np.ndarray:
+    vbox = np.ascontiguousarray(vbox, dtype=np.float64)
+    fbox = np.ascontiguousarray(fbox, dtype=np.float64)
+    v_obj = np.ascontiguousarray(v_obj, dtype=np.int32)
+    f_obj = np.ascontiguousarray(f_obj, dtype=np.int32)
+    faces = np.ascontiguousarray(faces, dtype=np.int32)
+    allowed = np.ascontiguousarray(allowed, dtype=np.uint8)
+    v_valid = None if v_valid is None else np.ascontiguousarray(v_valid, dtype=np.uint8)
+    fn = lib().oracle_vf_pairs_sweep if method == "sweep" else lib().oracle_vf_pairs_brute
+    return _pairs(fn, _p(vbox), _p(v_obj), _p(v_valid), len(vbox), _p(fbox), _p(f_obj), _p(faces), len(fbox),
+                  _p(allowed), allowed.shape[0])
+
+
+def ee_pairs(ebox, e_obj, edges, allowed, method: str = "sweep") -> np.ndarray:
+    ebox = np.ascontiguousarray(ebox, dtype=np.float64)
+    e_obj = np.ascontiguousarray(e_obj, dtype=np.int32)
+    edges = np.ascontiguousarray(edges, dtype=np.int32)
+    allowed = np.ascontiguousarray(allowed, dtype=np.uint8)
+    fn = lib().oracle_ee_pairs_sweep if method == "sweep" else lib().oracle_ee_pairs_brute
+    return _pairs(fn, _p(ebox), _p(e_obj), _p(edges), len(ebox), _p(allowed), allowed.shape[0])
+
+
+def object_allowed(v_t0, v_t1, v_obj, n_obj: int, thickness: float = 0.0, exclude_self: bool = False):
+    v_t0 = np.ascontiguousarray(v_t0, dtype=np.float64)
+    v_t1 = np.ascontiguousarray(v_t1, dtype=np.float64)
+    v_obj = np.ascontiguousarray(v_obj, dtype=np.int32)
+    out = np.zeros((n_obj, n_obj), dtype=np.uint8)
+    lib().oracle_object_allowed(_p(v_t0), _p(v_t1), _p(v_obj), len(v_obj), n_obj, thickness, int(exclude_self),
+                                _p(out))
+    return out
+
+
+def group_anyhit(cand_group, cand_hit, n_groups: int, top_offsets, top_index):
+    cand_group = np.ascontiguousarray(cand_group, dtype=np.int32)
+    cand_hit = np.ascontiguousarray(cand_hit, dtype=np.uint8)
+    top_offsets = np.ascontiguousarray(top_offsets, dtype=np.int64)
+    top_index = np.ascontiguousarray(top_index, dtype=np.int64)
+    det = np.zeros(n_groups, dtype=np.uint8)
+    pc = np.zeros(n_groups, dtype=np.int64)
+    fc = np.zeros(n_groups, dtype=np.int64)
+    ev = np.zeros(len(cand_group), dtype=np.uint8)
+    lib().oracle_group_anyhit(len(cand_group), _p(cand_group), _p(cand_hit), n_groups, _p(top_offsets),
+                              _p(top_index), _p(det), _p(pc), _p(fc), _p(ev))
+    return det, pc, fc, ev
+
+
+def refinement_children(t0, t1, depth, status, mode, toi, max_child_depth=64, min_width=1e-4, use_ref=False):
+    c0 = np.zeros(2)
+    c1 = np.zeros(2)
+    L = ref() if use_ref else lib()
+    fn = L.ref_refinement_children if use_ref else L.oracle_refinement_children
+    n = fn(t0, t1, depth, status, mode, toi, max_child_depth, min_width, _p(c0), _p(c1))
+    return [(float(c0[i]), float(c1[i])) for i in range(max(n, 0))]
+
+
+def ref_build_mesh_query(va, fa, ta0, ta1, vb, fb, tb0, tb1, family_mask=3, prune=True, max_pt=0, max_ee=0):
+    """BuildMeshExactCertificateQuery via the reference: (pt records, ee records)."""
+    va = np.ascontiguousarray(va, dtype=np.float64)
+    vb = np.ascontiguousarray(vb, dtype=np.float64)
+    fa = np.ascontiguousarray(fa, dtype=np.uint32)
+    fb = np.ascontiguousarray(fb, dtype=np.uint32)
+    t = [np.ascontiguousarray(x, dtype=np.float64) for x in (ta0, ta1, tb0, tb1)]
+    npt = ctypes.c_int64(0)
+    nee = ctypes.c_int64(0)
+    R = ref()
+    args = [_p(va), len(va), _p(fa), len(fa), _p(t[0]), _p(t[1]), _p(vb), len(vb), _p(fb), len(fb), _p(t[2]),
+            _p(t[3]), family_mask, int(prune), max_pt, max_ee]
+    rc = R.ref_build_mesh_query(*args, None, ctypes.byref(npt), None, ctypes.byref(nee))
+    if rc:
+        raise ValueError(R.ref_last_error().decode())
+    pts = np.zeros(npt.value, dtype=PT)
+    ees = np.zeros(nee.value, dtype=EE)
+    R.ref_build_mesh_query(*args, _p(pts), ctypes.byref(npt), _p(ees), ctypes.byref(nee))
+    return pts, ees

@@ -1,0 +1,234 @@
+// certify.cu — batch interval certificates over the reference's 240-byte
+// primitive records: the sm_100a replacement of PointTriangleKernel /
+// EdgeEdgeKernel + RunCudaBatch (cpp/certificate/certificate_cuda.cu:348-552),
+// with the CPU certifier's semantics (certificate_engine.cpp:300-386, 481-551).
+#include "certify_core.cuh"
+#include "certify_launch.cuh"
+#include "p2c_internal.cuh"
+
+namespace p2c {
+
+namespace {
+
+// Word layout of a 240-byte record: [id_a, id_b, 4 x (feature_id, p0[3], p1[3])].
+__device__ __forceinline__ void load_record(const unsigned long long* __restrict__ rec, Geo& g, int& bad) {
+  const long long ida = (long long)__ldg(rec + 0);
+  const long long idb = (long long)__ldg(rec + 1);
+  bool finite = true;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      const double a = __longlong_as_double((long long)__ldg(rec + 3 + 7 * i + k));
+      const double b = __longlong_as_double((long long)__ldg(rec + 6 + 7 * i + k));
+      g.p0[3 * i + k] = a;
+      g.p1[3 * i + k] = b;
+      finite = finite && isfinite(a) && isfinite(b);
+    }
+  }
+  bad = (ida < 0 || idb < 0) ? 1 : (finite ? 0 : 2);
+}
+
+struct RecordSrc {
+  const unsigned long long* recs;  // 30 words per record
+  double T0, T1;
+  __device__ __forceinline__ void load(long long q, Geo& g, double& t0, double& t1, int& bad) const {
+    load_record(recs + 30 * q, g, bad);
+    t0 = T0;
+    t1 = T1;
+  }
+};
+
+struct RecordSink {
+  const unsigned long long* recs;
+  p2c_interval_result* out;
+  unsigned long long* invalid_key;  // min over (index << 2 | reason)
+  __device__ __forceinline__ void finish(long long q, int family, const Outcome& o) const {
+    store_interval_result(out + q, family, o, (long long)recs[30 * q], (long long)recs[30 * q + 1]);
+  }
+  __device__ __forceinline__ void invalid(long long q, int family, int bad, double T0, double T1) const {
+    Outcome o{3, T0, T1, T1, 0.0};
+    store_interval_result(out + q, family, o, -1, -1);
+    atomicMin(invalid_key, ((unsigned long long)q << 2) | (unsigned long long)bad);
+  }
+};
+
+template <bool kDonate, bool kCount>
+__global__ void __launch_bounds__(kCertifyThreads, 1)
+    certify_records_kernel(const unsigned long long* __restrict__ pt, long long n_pt,
+                           const unsigned long long* __restrict__ ee, long long n_ee, double T0, double T1,
+                           CertParams prm_pt, CertParams prm_ee, p2c_interval_result* out_pt,
+                           p2c_interval_result* out_ee, CertifyScratch* scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
+  WarpStats st;
+  const unsigned long long t_start = global_ns();
+  bool ok = true;
+  if (n_pt > 0) {
+    RecordSrc src{pt, T0, T1};
+    RecordSink sink{pt, out_pt, &scratch->invalid_key[0]};
+    ok = run_warp<1, kDonate, kCount>(src, sink, n_pt, &scratch->queue_head[0], prm_pt, ws, st, t_start);
+  }
+  if (ok && n_ee > 0) {
+    RecordSrc src{ee, T0, T1};
+    RecordSink sink{ee, out_ee, &scratch->invalid_key[1]};
+    ok = run_warp<2, kDonate, kCount>(src, sink, n_ee, &scratch->queue_head[1], prm_ee, ws, st, t_start);
+  }
+  flush_stats(st, ok, scratch);
+}
+
+}  // namespace
+
+// Launch both families in one persistent launch.  Scratch must hold a
+// CertifyScratch and is reset here.
+int launch_certify_records(const void* pt, long long n_pt, const void* ee, long long n_ee, double T0,
+                           double T1, const p2c_cert_config& cfg, p2c_interval_result* out_pt,
+                           p2c_interval_result* out_ee, void* scratch, size_t scratch_bytes, bool census,
+                           cudaStream_t stream) {
+  if (scratch_bytes < sizeof(CertifyScratch))
+    return fail(P2C_ERR_INVALID, "certification workspace too small: %zu < %zu bytes", scratch_bytes,
+                sizeof(CertifyScratch));
+  CertifyScratch* sc = reinterpret_cast<CertifyScratch*>(scratch);
+  P2C_CUDA(reset_scratch(sc, stream));
+  if (n_pt + n_ee == 0) return P2C_OK;
+  LaunchShape shape;
+  int rc = census ? certify_shape(certify_records_kernel<false, true>, &shape)
+                  : certify_shape(certify_records_kernel<true, false>, &shape);
+  if (rc != P2C_OK) return rc;
+  const CertParams ppt = make_params(cfg, shape, n_pt);
+  const CertParams pee = make_params(cfg, shape, n_ee);
+  const auto* a = reinterpret_cast<const unsigned long long*>(pt);
+  const auto* b = reinterpret_cast<const unsigned long long*>(ee);
+  if (census) {
+    certify_records_kernel<false, true><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
+        a, n_pt, b, n_ee, T0, T1, ppt, pee, out_pt, out_ee, sc);
+  } else {
+    certify_records_kernel<true, false><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
+        a, n_pt, b, n_ee, T0, T1, ppt, pee, out_pt, out_ee, sc);
+  }
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+}  // namespace p2c
+
+using namespace p2c;
+
+namespace {
+
+int validate_batch_args(int64_t n, double t0, double t1, const p2c_cert_config* cfg, const void* prims,
+                        const void* out) {
+  if (cfg == nullptr) return fail(P2C_ERR_INVALID, "CertificateEngineConfig pointer is null");
+  if (n < 0) return fail(P2C_ERR_INVALID, "primitive count must be non-negative");
+  if (n > 0 && (prims == nullptr || out == nullptr))
+    return fail(P2C_ERR_INVALID, "CUDA exact result output pointer is null");
+  return validate_cert_config(*cfg, t0, t1);
+}
+
+HostApiBuffers g_host_buffers;
+
+int certify_host(const void* prims, int64_t n, int family, double t0, double t1, const p2c_cert_config* cfg,
+                 p2c_interval_result* results) {
+  int rc = validate_batch_args(n, t0, t1, cfg, prims, results);
+  if (rc != P2C_OK) return rc;
+  if (n == 0) return P2C_OK;  // RunCudaBatch returns Ok on empty input (certificate_cuda.cu:465-468)
+  std::lock_guard<std::mutex> lock(g_host_buffers.mu);
+  const size_t in_bytes = (size_t)n * 240u, out_bytes = (size_t)n * sizeof(p2c_interval_result);
+  const size_t ws_off = (in_bytes + out_bytes + 255u) & ~size_t(255);
+  rc = ensure_buffer(g_host_buffers, ws_off + sizeof(CertifyScratch));
+  if (rc != P2C_OK) return rc;
+  char* base = static_cast<char*>(g_host_buffers.dev);
+  void* d_in = base;
+  auto* d_out = reinterpret_cast<p2c_interval_result*>(base + in_bytes);
+  void* d_ws = base + ws_off;
+  cudaStream_t s = nullptr;
+  P2C_CUDA(cudaMemcpyAsync(d_in, prims, in_bytes, cudaMemcpyHostToDevice, s));
+  rc = family == 1 ? launch_certify_records(d_in, n, nullptr, 0, t0, t1, *cfg, d_out, nullptr, d_ws,
+                                            sizeof(CertifyScratch), false, s)
+                   : launch_certify_records(nullptr, 0, d_in, n, t0, t1, *cfg, nullptr, d_out, d_ws,
+                                            sizeof(CertifyScratch), false, s);
+  if (rc != P2C_OK) return rc;
+  P2C_CUDA(cudaMemcpyAsync(results, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
+  CertifyScratch host_sc;
+  P2C_CUDA(cudaMemcpyAsync(&host_sc, d_ws, sizeof(CertifyScratch), cudaMemcpyDeviceToHost, s));
+  P2C_CUDA(cudaStreamSynchronize(s));
+  return check_scratch_outcome(host_sc, family);
+}
+
+}  // namespace
+
+extern "C" {
+
+size_t p2c_certify_workspace_bytes(int64_t n) {
+  (void)n;
+  return sizeof(CertifyScratch);
+}
+
+int p2c_certify_pt_batch(const p2c_point_triangle* prims_dev, int64_t n, double interval_t0, double interval_t1,
+                         const p2c_cert_config* config, p2c_interval_result* results_dev, void* workspace_dev,
+                         size_t workspace_bytes, p2c_certify_stats* stats_dev, void* stream) {
+  int rc = validate_batch_args(n, interval_t0, interval_t1, config, prims_dev, results_dev);
+  if (rc != P2C_OK) return rc;
+  if (workspace_dev == nullptr) return fail(P2C_ERR_INVALID, "workspace pointer is null");
+  rc = launch_certify_records(prims_dev, n, nullptr, 0, interval_t0, interval_t1, *config, results_dev, nullptr,
+                              workspace_dev, workspace_bytes, false, as_stream(stream));
+  if (rc != P2C_OK) return rc;
+  return export_stats(reinterpret_cast<CertifyScratch*>(workspace_dev), stats_dev, as_stream(stream));
+}
+
+int p2c_certify_ee_batch(const p2c_edge_edge* prims_dev, int64_t n, double interval_t0, double interval_t1,
+                         const p2c_cert_config* config, p2c_interval_result* results_dev, void* workspace_dev,
+                         size_t workspace_bytes, p2c_certify_stats* stats_dev, void* stream) {
+  int rc = validate_batch_args(n, interval_t0, interval_t1, config, prims_dev, results_dev);
+  if (rc != P2C_OK) return rc;
+  if (workspace_dev == nullptr) return fail(P2C_ERR_INVALID, "workspace pointer is null");
+  rc = launch_certify_records(nullptr, 0, prims_dev, n, interval_t0, interval_t1, *config, nullptr, results_dev,
+                              workspace_dev, workspace_bytes, false, as_stream(stream));
+  if (rc != P2C_OK) return rc;
+  return export_stats(reinterpret_cast<CertifyScratch*>(workspace_dev), stats_dev, as_stream(stream));
+}
+
+int p2c_certify_batch2(const p2c_point_triangle* pt_dev, int64_t n_pt, const p2c_edge_edge* ee_dev, int64_t n_ee,
+                       double interval_t0, double interval_t1, const p2c_cert_config* config,
+                       p2c_interval_result* pt_results_dev, p2c_interval_result* ee_results_dev,
+                       void* workspace_dev, size_t workspace_bytes, p2c_certify_stats* stats_dev, void* stream) {
+  int rc = validate_batch_args(n_pt, interval_t0, interval_t1, config, pt_dev, pt_results_dev);
+  if (rc != P2C_OK) return rc;
+  rc = validate_batch_args(n_ee, interval_t0, interval_t1, config, ee_dev, ee_results_dev);
+  if (rc != P2C_OK) return rc;
+  if (workspace_dev == nullptr) return fail(P2C_ERR_INVALID, "workspace pointer is null");
+  rc = launch_certify_records(pt_dev, n_pt, ee_dev, n_ee, interval_t0, interval_t1, *config, pt_results_dev,
+                              ee_results_dev, workspace_dev, workspace_bytes, false, as_stream(stream));
+  if (rc != P2C_OK) return rc;
+  return export_stats(reinterpret_cast<CertifyScratch*>(workspace_dev), stats_dev, as_stream(stream));
+}
+
+int p2c_certify_pt_batch_host(const p2c_point_triangle* prims_host, int64_t n, double interval_t0,
+                              double interval_t1, const p2c_cert_config* config,
+                              p2c_interval_result* results_host) {
+  return certify_host(prims_host, n, 1, interval_t0, interval_t1, config, results_host);
+}
+
+int p2c_certify_ee_batch_host(const p2c_edge_edge* prims_host, int64_t n, double interval_t0,
+                              double interval_t1, const p2c_cert_config* config,
+                              p2c_interval_result* results_host) {
+  return certify_host(prims_host, n, 2, interval_t0, interval_t1, config, results_host);
+}
+
+int p2c_certify_census(const p2c_point_triangle* pt_dev, int64_t n_pt, const p2c_edge_edge* ee_dev, int64_t n_ee,
+                       double interval_t0, double interval_t1, const p2c_cert_config* config,
+                       p2c_interval_result* pt_results_dev, p2c_interval_result* ee_results_dev,
+                       void* workspace_dev, size_t workspace_bytes, p2c_certify_stats* stats_dev,
+                       void* stream) {
+  int rc = validate_batch_args(n_pt, interval_t0, interval_t1, config, pt_dev, pt_results_dev);
+  if (rc != P2C_OK) return rc;
+  rc = validate_batch_args(n_ee, interval_t0, interval_t1, config, ee_dev, ee_results_dev);
+  if (rc != P2C_OK) return rc;
+  if (workspace_dev == nullptr) return fail(P2C_ERR_INVALID, "workspace pointer is null");
+  rc = launch_certify_records(pt_dev, n_pt, ee_dev, n_ee, interval_t0, interval_t1, *config, pt_results_dev,
+                              ee_results_dev, workspace_dev, workspace_bytes, true, as_stream(stream));
+  if (rc != P2C_OK) return rc;
+  return export_stats(reinterpret_cast<CertifyScratch*>(workspace_dev), stats_dev, as_stream(stream));
+}
+
+}  // extern "C"

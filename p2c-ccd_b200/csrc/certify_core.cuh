@@ -1,0 +1,619 @@
+// certify_core.cuh — FP64 interval certifier for sm_100a.
+//
+// Restates the reference certifier (cpp/certificate/certificate_engine.cpp) so
+// that every decision, time of impact and margin is bit-identical:
+//  * all arithmetic goes through explicitly rounded intrinsics (__dmul_rn,
+//    __dadd_rn, __dsub_rn, __ddiv_rn, __dsqrt_rn), so no FMA contraction can
+//    occur whatever the compiler flags; the association order is the one the
+//    reference source writes;
+//  * std::clamp/min/max are restated with the same comparisons (NaN and signed
+//    zero behave as in libstdc++).
+//
+// Engine: one persistent loop per warp.  A lane owns one interval node at a
+// time and walks its subtree depth-first, left child first, with no stack: the
+// node is (path bits, depth) and its endpoints are recomputed from the root by
+// replaying the bisections (the same 0.5*(a+b) roundings the reference
+// recursion performs).  Every non-root node needs only its midpoint sample:
+// its endpoints are midpoints or endpoints of ancestors, already known to be
+// farther than eps_space (otherwise the ancestor would be a collision leaf).
+// When the query queue is empty, idle lanes take the shallowest pending right
+// subtree of a busy lane ("donation"), so one grazing query is bisected by up
+// to 32 lanes.  Per-query reduction in shared memory reproduces the recursion's
+// result exactly: the leftmost collision leaf in depth-first order (smallest
+// left-aligned path key) wins; else any undecided leaf makes the query
+// undecided; else separation with the minimum leaf margin.  Nodes right of a
+// known collision are pruned (the serial recursion never visits them).
+#pragma once
+
+#include <cstdint>
+#include <type_traits>
+
+#include "p2c_b200.h"
+
+namespace p2c {
+
+constexpr double kNumEps = 1.0e-14;  // kNumericalEpsilon, certificate_engine.cpp:20
+
+// ---- optional FP64 operation census ---------------------------------------
+struct NoCount {
+  static constexpr unsigned long long n = 0;
+  __device__ __forceinline__ void add(int) {}
+};
+struct OpCount {
+  unsigned long long n = 0;
+  __device__ __forceinline__ void add(int k) { n += (unsigned long long)k; }
+};
+
+struct V3 {
+  double x, y, z;
+};
+
+__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+
+__device__ __forceinline__ V3 vadd(V3 a, V3 b) { return {add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)}; }
+__device__ __forceinline__ V3 vsub(V3 a, V3 b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
+__device__ __forceinline__ V3 vscale(V3 a, double s) { return {mul(a.x, s), mul(a.y, s), mul(a.z, s)}; }
+// a.x*b.x + a.y*b.y + a.z*b.z, left to right
+__device__ __forceinline__ double vdot(V3 a, V3 b) {
+  return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z));
+}
+__device__ __forceinline__ V3 vcross(V3 a, V3 b) {
+  return {sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
+          sub(mul(a.x, b.y), mul(a.y, b.x))};
+}
+// std::clamp(v, lo, hi) as libstdc++ evaluates it
+__device__ __forceinline__ double clamp_std(double v, double lo, double hi) {
+  return (v < lo) ? lo : ((hi < v) ? hi : v);
+}
+__device__ __forceinline__ double max_std(double a, double b) { return (a < b) ? b : a; }
+__device__ __forceinline__ double min_std(double a, double b) { return (b < a) ? b : a; }
+
+template <class C>
+__device__ __forceinline__ double dist_pp(V3 a, V3 b, C& c) {  // :78-80
+  c.add(9);
+  const V3 d = vsub(a, b);
+  return __dsqrt_rn(vdot(d, d));
+}
+
+template <class C>
+__device__ __forceinline__ double dist_point_segment(V3 p, V3 a, V3 b, C& c) {  // :82-90
+  const V3 ab = vsub(b, a);
+  const double ab2 = vdot(ab, ab);
+  c.add(8);
+  if (ab2 <= kNumEps) return dist_pp(p, a, c);
+  const double t = clamp_std(dvd(vdot(vsub(p, a), ab), ab2), 0.0, 1.0);
+  c.add(15);
+  return dist_pp(p, vadd(a, vscale(ab, t)), c);
+}
+
+// DistancePointTriangle, certificate_engine.cpp:133-184
+template <class C>
+__device__ __forceinline__ double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C& c) {
+  const V3 ab = vsub(b, a);
+  const V3 ac = vsub(cc, a);
+  const V3 n = vcross(ab, ac);
+  c.add(20);
+  if (vdot(n, n) <= kNumEps) {
+    double m = dist_point_segment(p, a, b, c);
+    const double m1 = dist_point_segment(p, b, cc, c);
+    const double m2 = dist_point_segment(p, cc, a, c);
+    if (m1 < m) m = m1;  // std::min({...}) keeps the first smallest
+    if (m2 < m) m = m2;
+    return m;
+  }
+  const V3 ap = vsub(p, a);
+  const double d1 = vdot(ab, ap);
+  const double d2 = vdot(ac, ap);
+  c.add(13);
+  if (d1 <= 0.0 && d2 <= 0.0) return dist_pp(p, a, c);
+  const V3 bp = vsub(p, b);
+  const double d3 = vdot(ab, bp);
+  const double d4 = vdot(ac, bp);
+  c.add(13);
+  if (d3 >= 0.0 && d4 <= d3) return dist_pp(p, b, c);
+  const double vc = sub(mul(d1, d4), mul(d3, d2));
+  c.add(3);
+  if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+    const double v = dvd(d1, sub(d1, d3));
+    c.add(8);
+    return dist_pp(p, vadd(a, vscale(ab, v)), c);
+  }
+  const V3 cp = vsub(p, cc);
+  const double d5 = vdot(ab, cp);
+  const double d6 = vdot(ac, cp);
+  c.add(13);
+  if (d6 >= 0.0 && d5 <= d6) return dist_pp(p, cc, c);
+  const double vb = sub(mul(d5, d2), mul(d1, d6));
+  c.add(3);
+  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+    const double w = dvd(d2, sub(d2, d6));
+    c.add(8);
+    return dist_pp(p, vadd(a, vscale(ac, w)), c);
+  }
+  const double va = sub(mul(d3, d6), mul(d5, d4));
+  const double d43 = sub(d4, d3);
+  const double d56 = sub(d5, d6);
+  c.add(5);
+  if (va <= 0.0 && d43 >= 0.0 && d56 >= 0.0) {
+    const double w = dvd(d43, add(d43, d56));
+    c.add(11);
+    return dist_pp(p, vadd(b, vscale(vsub(cc, b), w)), c);
+  }
+  const double nn = __dsqrt_rn(vdot(n, n));
+  const double sd = dvd(vdot(ap, n), nn);
+  c.add(12);
+  return fabs(sd);
+}
+
+// DistanceSegmentSegment, certificate_engine.cpp:92-131
+template <class C>
+__device__ __forceinline__ double dist_segment_segment(V3 p1, V3 q1, V3 p2, V3 q2, C& c) {
+  const V3 d1 = vsub(q1, p1);
+  const V3 d2 = vsub(q2, p2);
+  const V3 r = vsub(p1, p2);
+  const double a = vdot(d1, d1);
+  const double e = vdot(d2, d2);
+  const double f = vdot(d2, r);
+  c.add(24);
+  double s = 0.0, t = 0.0;
+  if (a <= kNumEps && e <= kNumEps) return dist_pp(p1, p2, c);
+  if (a <= kNumEps) {
+    t = clamp_std(dvd(f, e), 0.0, 1.0);
+    c.add(1);
+  } else {
+    const double cd = vdot(d1, r);
+    c.add(5);
+    if (e <= kNumEps) {
+      s = clamp_std(dvd(-cd, a), 0.0, 1.0);
+      c.add(1);
+    } else {
+      const double b = vdot(d1, d2);
+      const double denom = sub(mul(a, e), mul(b, b));
+      c.add(8);
+      if (denom != 0.0) {
+        s = clamp_std(dvd(sub(mul(b, f), mul(cd, e)), denom), 0.0, 1.0);
+        c.add(4);
+      }
+      t = dvd(add(mul(b, s), f), e);
+      c.add(3);
+      if (t < 0.0) {
+        t = 0.0;
+        s = clamp_std(dvd(-cd, a), 0.0, 1.0);
+        c.add(1);
+      } else if (t > 1.0) {
+        t = 1.0;
+        s = clamp_std(dvd(sub(b, cd), a), 0.0, 1.0);
+        c.add(2);
+      }
+    }
+  }
+  c.add(12);
+  return dist_pp(vadd(p1, vscale(d1, s)), vadd(p2, vscale(d2, t)), c);
+}
+
+// Query geometry: 4 trajectories (VF: point, v0, v1, v2; EE: a0, a1, b0, b1).
+struct Geo {
+  double p0[12];
+  double p1[12];
+};
+
+// PositionAt (:67-69) for the 4 vertices, then the family's distance.
+template <int kFamily, class C>
+__device__ __forceinline__ double distance_at(const Geo& g, double t, C& c) {
+  V3 x[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const double u = sub(1.0, t);
+    x[i] = vadd(vscale(V3{g.p0[3 * i], g.p0[3 * i + 1], g.p0[3 * i + 2]}, u),
+                vscale(V3{g.p1[3 * i], g.p1[3 * i + 1], g.p1[3 * i + 2]}, t));
+  }
+  c.add(40);
+  if (kFamily == 1) return dist_point_triangle(x[0], x[1], x[2], x[3], c);
+  return dist_segment_segment(x[0], x[1], x[2], x[3], c);
+}
+
+// Norm(Sub(p1, p0)) of each trajectory: constant per query, hoisted out of
+// MaxDisplacementFromMidpoint (:71-76); the same rounded value either way.
+template <class C>
+__device__ __forceinline__ void motion_norms(const Geo& g, double nrm[4], C& c) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const V3 d = vsub(V3{g.p1[3 * i], g.p1[3 * i + 1], g.p1[3 * i + 2]},
+                      V3{g.p0[3 * i], g.p0[3 * i + 1], g.p0[3 * i + 2]});
+    nrm[i] = __dsqrt_rn(vdot(d, d));
+  }
+  c.add(36);
+}
+
+// PointTriangleMotionRadius / EdgeEdgeMotionRadius (:200-222); each
+// MaxDisplacementFromMidpoint is (0.5 * max(0, t1 - t0)) * norm.
+template <int kFamily, class C>
+__device__ __forceinline__ double motion_radius(const double nrm[4], double t0, double t1, C& c) {
+  const double h = mul(0.5, max_std(0.0, sub(t1, t0)));
+  const double m0 = mul(h, nrm[0]), m1 = mul(h, nrm[1]), m2 = mul(h, nrm[2]), m3 = mul(h, nrm[3]);
+  c.add(7);
+  if (kFamily == 1) {
+    double m = m1;  // std::max({...}) keeps the first largest
+    if (m < m2) m = m2;
+    if (m < m3) m = m3;
+    return add(m0, m);
+  }
+  return add(max_std(m0, m1), max_std(m2, m3));
+}
+
+// ---- path arithmetic -------------------------------------------------------
+// Level l (1-based) of a node's path is bit (64 - l); bit 1 = went right.
+__device__ __forceinline__ unsigned long long top_bits(int k) {  // levels 1..k
+  return k <= 0 ? 0ull : (k >= 64 ? ~0ull : (~0ull << (64 - k)));
+}
+__device__ __forceinline__ unsigned long long level_bit(int l) { return 1ull << (64 - l); }
+
+// Pending right siblings of the current node inside the lane's subtree:
+// levels in (sub_depth, depth] where the path went left and that were not
+// handed to another lane.
+__device__ __forceinline__ unsigned long long pending_levels(unsigned long long path,
+                                                             unsigned long long donated, int depth,
+                                                             int sub_depth) {
+  return top_bits(depth) & ~top_bits(sub_depth) & ~path & ~donated;
+}
+
+// Endpoints of the node (path, depth) under root [T0, T1], recomputed with the
+// recursion's own roundings.
+__device__ __forceinline__ void replay(double T0, double T1, unsigned long long path, int depth,
+                                       double& a, double& b) {
+  a = T0;
+  b = T1;
+  for (int l = 1; l <= depth; ++l) {
+    const double m = mul(0.5, add(a, b));
+    if ((path >> (64 - l)) & 1ull) a = m;
+    else b = m;
+  }
+}
+
+// ---- result packing (p2c_interval_result, 72 B = 9 words) ---------------
+struct Outcome {
+  int status;
+  double t0, t1, toi, margin;
+};
+
+__device__ __forceinline__ void store_interval_result(p2c_interval_result* dst, int family, const Outcome& o,
+                                                      long long id_a, long long id_b) {
+  unsigned long long* w = reinterpret_cast<unsigned long long*>(dst);
+  unsigned long long w0, w5, w8;
+  long long ia = -1, ib = -1;
+  if (o.status == P2C_STATUS_COLLISION) {
+    w0 = 0ull;
+    w5 = (unsigned long long)family;
+    ia = id_a;
+    ib = id_b;
+    w8 = 0ull;
+  } else if (o.status == P2C_STATUS_SEPARATION) {
+    w0 = 1ull | ((unsigned long long)family << 32);
+    w5 = 0ull;
+    w8 = 0ull;
+  } else if (o.status == P2C_STATUS_UNDECIDED) {
+    w0 = 2ull;
+    w5 = 0ull;
+    w8 = (unsigned long long)P2C_REASON_MAX_SUBDIVISION_DEPTH |
+         ((unsigned long long)P2C_REFINE_BISECT_INTERVAL << 16);
+  } else {  // invalid primitive: undecided with InvalidInput (never produced by a valid query)
+    w0 = 2ull;
+    w5 = 0ull;
+    w8 = (unsigned long long)P2C_REASON_INVALID_INPUT |
+         ((unsigned long long)P2C_REFINE_REQUEST_GEOMETRY << 16);
+  }
+  w[0] = w0;
+  w[1] = __double_as_longlong(o.t0);
+  w[2] = __double_as_longlong(o.t1);
+  w[3] = __double_as_longlong(o.toi);
+  w[4] = __double_as_longlong(o.margin);
+  w[5] = w5;
+  w[6] = (unsigned long long)ia;
+  w[7] = (unsigned long long)ib;
+  w[8] = w8;
+}
+
+struct CertParams {
+  double eps_time;
+  double eps_space;
+  int max_depth;
+  int fetch_limit;               // queries a warp keeps in flight (1..32)
+  unsigned long long budget_ns;  // device time budget of one launch (0 = none)
+};
+
+// Per-warp shared state: 32 query slots, struct-of-arrays so that lanes
+// reading their own slot hit distinct banks.
+struct WarpSlots {
+  double p0[12][32];
+  double p1[12][32];
+  double T0[32], T1[32];
+  double coll_t0[32], coll_t1[32], coll_toi[32];
+  unsigned long long coll_key[32];
+  unsigned long long margin_bits[32];
+  long long qidx[32];
+  int outstanding[32];
+  int undecided[32];
+};
+
+struct WarpStats {
+  unsigned long long nodes = 0, evals = 0, donations = 0, queries = 0, ops = 0;
+};
+
+// Position of the (r+1)-th set bit of m (r counts from 0); m has > r set bits.
+__device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
+  for (int i = 0; i < r; ++i) m &= m - 1u;
+  return __ffs((int)m) - 1;
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// The warp engine.  Src provides load(q, Geo&, T0&, T1&, bad&) (bad: 0 valid,
+// 1 negative id, 2 non-finite coordinate); Sink provides finish(q, family,
+// Outcome) and invalid(q, family, bad, T0, T1).  Returns false if the time budget
+// ran out (the caller raises the error word).
+template <int kFamily, bool kDonate, bool kCount, class Src, class Sink>
+__device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned long long* counter,
+                         const CertParams& prm, WarpSlots& ws, WarpStats& st,
+                         unsigned long long t_start) {
+  using Counter = typename std::conditional<kCount, OpCount, NoCount>::type;
+  const unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned lt_mask = (1u << lane) - 1u;
+
+  int slot = -1;
+  int phase = 0;
+  unsigned long long path = 0, donated = 0;
+  int depth = 0, sub_depth = 0;
+  double t0 = 0.0, t1 = 0.0, T0 = 0.0, T1 = 0.0, d1root = 0.0;
+  Geo g;
+  double nrm[4];
+  Counter ops;
+  unsigned free_mask = FULL;
+  bool exhausted = false;
+  bool ok = true;
+
+  for (unsigned iter = 0;; ++iter) {
+    if ((iter & 63u) == 0u && prm.budget_ns != 0ull) {
+      int over = 0;
+      if (lane == 0) over = (global_ns() - t_start) > prm.budget_ns;
+      if (__shfl_sync(FULL, over, 0)) {
+        ok = false;
+        break;
+      }
+    }
+    // (A) idle lanes fetch new queries from the global queue; a warp keeps at
+    // most fetch_limit queries in flight so that, on small batches, the other
+    // lanes bisect those queries instead of idling.
+    unsigned idle = __ballot_sync(FULL, slot < 0);
+    const int room = prm.fetch_limit - (32 - __popc(free_mask));
+    if (idle != 0u && !exhausted && room > 0) {
+      const int k = min(__popc(idle), room);
+      unsigned long long base = 0;
+      if (lane == 0) base = atomicAdd(counter, (unsigned long long)k);
+      base = __shfl_sync(FULL, base, 0);
+      if ((long long)base + k >= n) exhausted = true;
+      bool fresh = false;
+      const int r = __popc(idle & lt_mask);
+      if (slot < 0 && r < k) {
+        const long long q = (long long)base + r;
+        if (q < n) {
+          const int s = nth_set_bit(free_mask, r);
+          int bad = 0;
+          src.load(q, g, T0, T1, bad);
+          if (bad != 0) {
+            sink.invalid(q, kFamily, bad, T0, T1);
+          } else {
+            slot = s;
+            fresh = true;
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+              ws.p0[i][s] = g.p0[i];
+              ws.p1[i][s] = g.p1[i];
+            }
+            ws.T0[s] = T0;
+            ws.T1[s] = T1;
+            ws.coll_key[s] = ~0ull;
+            ws.margin_bits[s] = 0x7ff0000000000000ull;  // +inf
+            ws.qidx[s] = q;
+            ws.outstanding[s] = 1;
+            ws.undecided[s] = 0;
+            motion_norms(g, nrm, ops);
+            phase = 0;
+            path = 0ull;
+            donated = 0ull;
+            depth = 0;
+            sub_depth = 0;
+            t0 = T0;
+            t1 = T1;
+            st.queries += 1;
+          }
+        }
+      }
+      free_mask &= ~__reduce_or_sync(FULL, fresh ? (1u << slot) : 0u);
+      __syncwarp();
+    }
+    // (B) donation: idle lanes take the shallowest pending subtree of a busy lane
+    if (kDonate) {
+      idle = __ballot_sync(FULL, slot < 0);
+      if (idle != 0u) {
+        const unsigned long long pend =
+            (slot >= 0 && phase == 2) ? pending_levels(path, donated, depth, sub_depth) : 0ull;
+        const unsigned donors = __ballot_sync(FULL, pend != 0ull);
+        const int npair = min(__popc(idle), __popc(donors));
+        if (npair > 0) {
+          unsigned long long gpath = 0ull;
+          int gdepth = 0, gslot = -1;
+          if (((donors >> lane) & 1u) && __popc(donors & lt_mask) < npair) {
+            const int b = 63 - __clzll((long long)pend);
+            const int l = 64 - b;
+            donated |= (1ull << b);
+            gpath = (path & top_bits(l - 1)) | (1ull << b);
+            gdepth = l;
+            gslot = slot;
+            atomicAdd(&ws.outstanding[slot], 1);
+            st.donations += 1;
+          }
+          const bool receiver = ((idle >> lane) & 1u) && __popc(idle & lt_mask) < npair;
+          const int src_lane = receiver ? nth_set_bit(donors, __popc(idle & lt_mask)) : lane;
+          const unsigned long long rpath = __shfl_sync(FULL, gpath, src_lane);
+          const int rdepth = __shfl_sync(FULL, gdepth, src_lane);
+          const int rslot = __shfl_sync(FULL, gslot, src_lane);
+          __syncwarp();
+          if (receiver) {
+            slot = rslot;
+#pragma unroll
+            for (int i = 0; i < 12; ++i) {
+              g.p0[i] = ws.p0[i][slot];
+              g.p1[i] = ws.p1[i][slot];
+            }
+            T0 = ws.T0[slot];
+            T1 = ws.T1[slot];
+            NoCount nc;
+            motion_norms(g, nrm, nc);  // same rounded values as the owner's
+            path = rpath;
+            depth = rdepth;
+            sub_depth = rdepth;
+            donated = 0ull;
+            phase = 2;
+            double a, b;
+            replay(T0, T1, path, depth - 1, a, b);
+            t0 = mul(0.5, add(a, b));
+            t1 = b;
+          }
+        }
+      }
+    }
+    const unsigned busy = __ballot_sync(FULL, slot >= 0);
+    if (busy == 0u) {
+      if (exhausted) break;
+      continue;
+    }
+    // (C) prune: a node right of a known collision leaf of its query is not
+    // needed (depth-first order would return before reaching it), and neither
+    // is anything after it in this lane's subtree.
+    bool done_lane = false;
+    if (slot >= 0 && phase == 2 && depth > 0 && ws.coll_key[slot] < path) done_lane = true;
+    const bool active = slot >= 0 && !done_lane;
+
+    // (D) one distance sample per active lane
+    double d = 0.0;
+    double mid = 0.0;
+    if (active) {
+      mid = mul(0.5, add(t0, t1));
+      const double t = phase == 0 ? t0 : (phase == 1 ? t1 : mid);
+      d = distance_at<kFamily>(g, t, ops);
+      st.evals += 1;
+      if (phase == 2) st.nodes += 1;
+      if (kCount) ops.add(phase == 2 ? 2 : 0);
+    }
+    // (E) classify.  leaf: 0 none, 1 collision, 2 separation, 3 undecided
+    int leaf = 0;
+    double toi = 0.0, margin = 0.0;
+    if (active) {
+      if (phase == 0) {
+        if (d <= prm.eps_space) {
+          leaf = 1;
+          toi = t0;
+        } else {
+          phase = 1;
+        }
+      } else if (phase == 1) {
+        d1root = d;
+        phase = 2;
+      } else {
+        if (d <= prm.eps_space) {
+          leaf = 1;
+          toi = mid;
+        } else if (depth == 0 && d1root <= prm.eps_space) {
+          leaf = 1;
+          toi = t1;
+        } else {
+          const double lb = sub(d, motion_radius<kFamily>(nrm, t0, t1, ops));
+          if (kCount) ops.add(1);
+          if (lb > prm.eps_space) {
+            leaf = 2;
+            margin = max_std(0.0, sub(lb, prm.eps_space));
+            if (kCount) ops.add(1);
+          } else if (depth >= prm.max_depth || sub(t1, t0) <= prm.eps_time) {
+            leaf = 3;
+          } else {
+            depth += 1;  // descend into the left child (its path bit stays 0)
+            t1 = mid;
+          }
+        }
+      }
+    }
+    // (F) reduce leaves into the query's slot
+    if (leaf == 1) atomicMin(&ws.coll_key[slot], path);
+    if (leaf == 2) atomicMin(&ws.margin_bits[slot], (unsigned long long)__double_as_longlong(margin));
+    if (leaf == 3) ws.undecided[slot] = 1;
+    __syncwarp();
+    if (leaf == 1 && ws.coll_key[slot] == path) {
+      ws.coll_t0[slot] = t0;
+      ws.coll_t1[slot] = t1;
+      ws.coll_toi[slot] = toi;
+    }
+    __syncwarp();
+    // (G) after a leaf, move to the deepest pending right sibling
+    if (leaf != 0) {
+      const unsigned long long pend = pending_levels(path, donated, depth, sub_depth);
+      if (pend == 0ull) {
+        done_lane = true;
+      } else {
+        const int b = __ffsll((long long)pend) - 1;
+        const int l = 64 - b;
+        path = (path & top_bits(l - 1)) | (1ull << b);
+        donated &= top_bits(l - 1);
+        double a, bb;
+        replay(T0, T1, path, l - 1, a, bb);
+        t0 = mul(0.5, add(a, bb));
+        t1 = bb;
+        depth = l;
+        phase = 2;
+      }
+    }
+    unsigned freed = 0u;
+    if (done_lane) {
+      const int old = atomicSub(&ws.outstanding[slot], 1);
+      if (old == 1) {
+        Outcome o;
+        const double RT0 = ws.T0[slot], RT1 = ws.T1[slot];
+        if (ws.coll_key[slot] != ~0ull) {
+          o.status = P2C_STATUS_COLLISION;
+          o.t0 = ws.coll_t0[slot];
+          o.t1 = ws.coll_t1[slot];
+          o.toi = ws.coll_toi[slot];
+          o.margin = 0.0;
+        } else if (ws.undecided[slot]) {
+          o.status = P2C_STATUS_UNDECIDED;
+          o.t0 = RT0;
+          o.t1 = RT1;
+          o.toi = RT1;
+          o.margin = 0.0;
+        } else {
+          o.status = P2C_STATUS_SEPARATION;
+          o.t0 = RT0;
+          o.t1 = RT1;
+          o.toi = RT1;
+          o.margin = __longlong_as_double((long long)ws.margin_bits[slot]);
+        }
+        sink.finish(ws.qidx[slot], kFamily, o);
+        freed = 1u << slot;
+      }
+      slot = -1;
+    }
+    free_mask |= __reduce_or_sync(FULL, freed);
+    __syncwarp();
+  }
+  if (kCount) st.ops += ops.n;
+  return ok;
+}
+
+}  // namespace p2c

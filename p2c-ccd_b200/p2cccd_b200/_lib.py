@@ -1,0 +1,99 @@
+"""ctypes binding of libp2c_b200.so (the C ABI in include/p2c_b200.h).
+
+The library is the only compute path: if it is missing or fails to load, every
+entry point raises.  There is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "libp2c_b200.so"
+
+P2C_OK = 0
+P2C_ERR_INVALID = 1
+P2C_ERR_CUDA = 2
+P2C_ERR_CAPACITY = 3
+P2C_ERR_TIMEOUT = 4
+
+_c_void_p = ctypes.c_void_p
+_i64 = ctypes.c_int64
+_f64 = ctypes.c_double
+_int = ctypes.c_int
+_size = ctypes.c_size_t
+
+
+class CertConfig(ctypes.Structure):
+    _fields_ = [("eps_time", ctypes.c_double), ("eps_space", ctypes.c_double),
+                ("max_subdivision_depth", ctypes.c_uint16), ("pad", ctypes.c_uint16 * 3)]
+
+
+class P2CError(RuntimeError):
+    """Raised when the library reports a failure that is not a ValueError."""
+
+
+# Signatures of every exported entry point: name -> (restype, argtypes).
+SIGNATURES: dict[str, tuple] = {
+    "p2c_last_error": (ctypes.c_char_p, []),
+    "p2c_abi_version": (_int, []),
+    "p2c_is_cuda_exact_built": (_int, []),
+    "p2c_device_info": (_int, [_c_void_p, _c_void_p, _c_void_p, _c_void_p]),
+    "p2c_certify_workspace_bytes": (_size, [_i64]),
+    "p2c_certify_pt_batch": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p,
+                                    _c_void_p, _size, _c_void_p, _c_void_p]),
+    "p2c_certify_ee_batch": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p,
+                                    _c_void_p, _size, _c_void_p, _c_void_p]),
+    "p2c_certify_pt_batch_host": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
+    "p2c_certify_ee_batch_host": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
+    "p2c_certify_batch2": (_int, [_c_void_p, _i64, _c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig),
+                                  _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
+    "p2c_probe_fp64": (_int, [_c_void_p, _int, ctypes.POINTER(ctypes.c_longlong), _c_void_p]),
+    "p2c_certify_census": (_int, [_c_void_p, _i64, _c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig),
+                                  _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
+}
+
+_lock = threading.Lock()
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise if it is absent (no fallback path exists)."""
+    global _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        path = Path(os.environ.get("P2C_B200_LIB", LIB_PATH))
+        if not path.exists():
+            raise P2CError(f"libp2c_b200.so not found at {path}; build it with p2cccd_b200.build.build()")
+        lib = ctypes.CDLL(str(path))
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+        return lib
+
+
+def last_error() -> str:
+    msg = load().p2c_last_error()
+    return msg.decode("utf-8", "replace") if msg else ""
+
+
+def check(rc: int) -> None:
+    """Map a status code to the reference's error convention (ValueError)."""
+    if rc == P2C_OK:
+        return
+    msg = last_error()
+    if rc == P2C_ERR_INVALID:
+        raise ValueError(msg)
+    raise P2CError(f"p2c error {rc}: {msg}")
+
+
+def make_config(eps_time: float, eps_space: float, max_subdivision_depth: int) -> CertConfig:
+    cfg = CertConfig()
+    cfg.eps_time = float(eps_time)
+    cfg.eps_space = float(eps_space)
+    cfg.max_subdivision_depth = int(max_subdivision_depth) & 0xFFFF
+    return cfg

@@ -1,0 +1,109 @@
+"""numpy record dtypes of the C ABI (include/p2c_b200.h).
+
+They are byte-identical to the reference's host structs
+(``cpp/certificate/certificate_engine.h:32-81``): a packed array of these
+records is what ``std::vector<PointTriangleIntervalPrimitive>`` holds.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+TRAJECTORY_DTYPE = np.dtype([
+    ("feature_id", "<i8"),
+    ("position_t0", "<f8", (3,)),
+    ("position_t1", "<f8", (3,)),
+])
+
+POINT_TRIANGLE_DTYPE = np.dtype([
+    ("point_id", "<i8"),
+    ("triangle_id", "<i8"),
+    ("point", TRAJECTORY_DTYPE),
+    ("triangle_v0", TRAJECTORY_DTYPE),
+    ("triangle_v1", TRAJECTORY_DTYPE),
+    ("triangle_v2", TRAJECTORY_DTYPE),
+])
+
+EDGE_EDGE_DTYPE = np.dtype([
+    ("edge_a_id", "<i8"),
+    ("edge_b_id", "<i8"),
+    ("edge_a0", TRAJECTORY_DTYPE),
+    ("edge_a1", TRAJECTORY_DTYPE),
+    ("edge_b0", TRAJECTORY_DTYPE),
+    ("edge_b1", TRAJECTORY_DTYPE),
+])
+
+INTERVAL_RESULT_DTYPE = np.dtype({
+    "names": ["status", "covered_feature_mask", "interval_t0", "interval_t1", "toi_upper",
+              "safe_margin_lb", "witness_family", "witness_id_a", "witness_id_b", "reason_code",
+              "next_refinement_mode"],
+    "formats": ["u1", "<u4", "<f8", "<f8", "<f8", "<f8", "u1", "<i8", "<i8", "<u2", "u1"],
+    "offsets": [0, 4, 8, 16, 24, 32, 40, 48, 56, 64, 66],
+    "itemsize": 72,
+})
+
+QUERY_CERTIFICATE_DTYPE = np.dtype({
+    "names": ["status", "witness_family", "reason_code", "covered_feature_mask", "toi_upper",
+              "safe_margin_lb", "witness_id_a", "witness_id_b", "witness_index", "next_refinement_mode"],
+    "formats": ["u1", "u1", "<u2", "<u4", "<f8", "<f8", "<i8", "<i8", "<i8", "u1"],
+    "offsets": [0, 1, 2, 4, 8, 16, 24, 32, 40, 48],
+    "itemsize": 56,
+})
+
+CERTIFY_STATS_DTYPE = np.dtype([
+    ("nodes_evaluated", "<u8"),
+    ("distance_evals", "<u8"),
+    ("fp64_ops", "<u8"),
+    ("donations", "<u8"),
+    ("queries", "<u8"),
+    ("error_word", "<u8"),
+])
+
+assert POINT_TRIANGLE_DTYPE.itemsize == 240
+assert EDGE_EDGE_DTYPE.itemsize == 240
+assert INTERVAL_RESULT_DTYPE.itemsize == 72
+
+# CertificateStatus / reason / refinement constants (runtime_contracts.h:20-31,
+# certificate_engine.h:12-22)
+STATUS_COLLISION = 0
+STATUS_SEPARATION = 1
+STATUS_UNDECIDED = 2
+FAMILY_POINT_TRIANGLE = 1
+FAMILY_EDGE_EDGE = 2
+REASON_NONE = 0
+REASON_MISSING_GEOMETRY = 1
+REASON_MAX_SUBDIVISION_DEPTH = 2
+REASON_INVALID_INPUT = 3
+REFINE_NONE = 0
+REFINE_BISECT_INTERVAL = 1
+REFINE_REQUEST_GEOMETRY = 2
+REFINE_ESCALATE_PRECISION = 3
+
+RESULT_FIELDS = INTERVAL_RESULT_DTYPE.names
+
+
+def pack_primitives(p0: np.ndarray, p1: np.ndarray, ids_a: np.ndarray, ids_b: np.ndarray,
+                    feature_ids: np.ndarray | None = None, family: int = FAMILY_POINT_TRIANGLE) -> np.ndarray:
+    """Pack (n, 4, 3) t0/t1 positions plus ids into 240-byte records.
+
+    Vertex order is (point, v0, v1, v2) for point-triangle and (a0, a1, b0, b1)
+    for edge-edge.
+    """
+    n = p0.shape[0]
+    dt = POINT_TRIANGLE_DTYPE if family == FAMILY_POINT_TRIANGLE else EDGE_EDGE_DTYPE
+    rec = np.zeros(n, dtype=dt)
+    names = dt.names
+    rec[names[0]] = ids_a
+    rec[names[1]] = ids_b
+    for k in range(4):
+        rec[names[2 + k]]["position_t0"] = p0[:, k, :]
+        rec[names[2 + k]]["position_t1"] = p1[:, k, :]
+        rec[names[2 + k]]["feature_id"] = -1 if feature_ids is None else feature_ids[:, k]
+    return rec
+
+
+def unpack_positions(rec: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """Inverse of pack_primitives for the geometry: (n, 4, 3) t0 and t1 arrays."""
+    names = rec.dtype.names
+    p0 = np.stack([rec[names[2 + k]]["position_t0"] for k in range(4)], axis=1)
+    p1 = np.stack([rec[names[2 + k]]["position_t1"] for k in range(4)], axis=1)
+    return p0, p1
