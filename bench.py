@@ -172,7 +172,156 @@ class PlainWorkload:
                 "sample": f"the full {self.queries}-query batch repeated {done // self.queries}x"}
 
 
-WORKLOADS = {"plain": PlainWorkload}
+class SceneWorkload:
+    """Two 40,960-triangle UV spheres (FP64), B translating toward A with
+    per-vertex N(0, 1e-3) jitter: swept-AABB candidates (mesh-pair semantics:
+    A x B pairs only) then certificates of every candidate."""
+
+    name = "scene"
+
+    def __init__(self, device, rank: int):
+        import torch
+
+        from p2cccd_b200 import certify, scenes
+        from p2cccd_b200.scene import ScenePipeline
+
+        self.torch = torch
+        self.scene = scenes.two_spheres(seed=20261203 + rank)
+        self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
+        self.pipe = ScenePipeline(self.scene, device, exclude_self=True, config=self.cfg)
+        summ = self.pipe.step_checked()
+        self.n_vf, self.n_ee = summ["vf_certified"], summ["ee_certified"]
+        self.queries = self.n_vf + self.n_ee
+        self.first_summary = summ
+        self.h_t0 = torch.from_numpy(self.scene["v_t0"].copy()).pin_memory()
+        self.h_t1 = torch.from_numpy(self.scene["v_t1"].copy()).pin_memory()
+        self.h_vf = torch.empty_like(self.pipe.vf_results, device="cpu").pin_memory()
+        self.h_ee = torch.empty_like(self.pipe.ee_results, device="cpu").pin_memory()
+        self.h_summary = torch.empty_like(self.pipe.summary, device="cpu").pin_memory()
+        self.phase_events = []
+        self.launches_per_step = None
+
+    def config(self) -> dict:
+        sp = self.scene["spec"]
+        return {"workload": "single-scene broad+narrow: two UV spheres of 40,960 triangles each (160 x 128 rings; "
+                            "40,960 is not an icosphere level), FP64, B translating toward A "
+                            f"(gap {sp['gap']}, approach {sp['approach']} per step) + per-vertex N(0,{sp['jitter']}) "
+                            "jitter, swept-AABB candidates (A x B) then exact VF/EE certificates of every candidate",
+                "vertices": int(len(self.scene["v_t0"])), "triangles": int(len(self.scene["faces"])),
+                "edges": int(len(self.scene["edges"])), "vf_candidates": self.n_vf, "ee_candidates": self.n_ee,
+                "queries_per_step": self.queries, "eps_time": self.cfg.eps_time, "eps_space": self.cfg.eps_space,
+                "max_subdivision_depth": self.cfg.max_subdivision_depth, "seed": sp["seed"]}
+
+    def step(self):
+        self.pipe.step()
+
+    def step_phased(self):
+        """The same step with events between the broad and the narrow phase."""
+        torch = self.torch
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        self.pipe.candidates()
+        e1.record()
+        self.pipe.certify()
+        e2.record()
+        self.phase_events.append((e0, e1, e2))
+
+    def step_e2e(self):
+        self.pipe.v_t0.copy_(self.h_t0, non_blocking=True)
+        self.pipe.v_t1.copy_(self.h_t1, non_blocking=True)
+        self.pipe.step()
+        self.h_vf.copy_(self.pipe.vf_results, non_blocking=True)
+        self.h_ee.copy_(self.pipe.ee_results, non_blocking=True)
+        self.h_summary.copy_(self.pipe.summary, non_blocking=True)
+
+    def io_bytes(self) -> tuple[int, int]:
+        return (self.h_t0.numel() * 8 + self.h_t1.numel() * 8,
+                self.h_vf.numel() + self.h_ee.numel() + self.h_summary.numel())
+
+    def census(self) -> dict:
+        from p2cccd_b200 import certify
+
+        vf_rec, ee_rec = self.pipe.materialize()
+        return certify.census(certify.records_to_device(vf_rec, self.pipe.device),
+                              certify.records_to_device(ee_rec, self.pipe.device), 0.0, 1.0, self.cfg)["stats"]
+
+    def broad_phase_bytes(self) -> int:
+        """Algorithmic bytes of candidate generation: read every vertex
+        trajectory (48 B), face (12 B) and edge (8 B) once, write every pair (8 B)."""
+        s = self.scene
+        return 48 * len(s["v_t0"]) + 12 * len(s["faces"]) + 8 * len(s["edges"]) + 8 * self.queries
+
+    def cpu_reference(self, threads: int, budget_s: float) -> dict:
+        return _scene_reference_sample(self.scene, self.cfg, budget_s, threads)
+
+
+def _scene_reference_sample(scene, cfg, budget_s: float, threads: int) -> dict:
+    """The reference CPU path on the scene workload, bounded.
+
+    The reference mesh builder (BuildMeshExactCertificateQuery) is
+    translation-only, so it runs on the translation-only form of the same
+    scene: the two unjittered spheres, A at rest, B translating as in the
+    step.  Its pair loops cost one identical swept-box test per pair, O(V*F +
+    E^2) (~5.4e9 tests at full size), so the build runs on a sample: sphere A
+    restricted to the primitives whose x extent reaches B's swept bounding box
+    (every candidate of the full query lies in it), and the build time is
+    scaled by the exact ratio of pair tests full/sample.  The certificates of
+    every primitive it returns are then timed in full on `threads` threads.
+    """
+    import numpy as np
+
+    import oracle
+    from p2cccd_b200 import scenes
+
+    sp = scene["spec"]
+    base, faces = scenes.uv_sphere(sp["n_lon"], sp["n_rings"])
+    ang = 0.37
+    rot = np.array([[np.cos(ang), 0.0, np.sin(ang)], [0.0, 1.0, 0.0], [-np.sin(ang), 0.0, np.cos(ang)]])
+    vb = base @ rot.T
+    tb0 = np.array([2.0 + sp["gap"], 0.0, 0.0])
+    tb1 = tb0 - np.array([sp["approach"], 0.0, 0.0])
+    b_min_x = min((vb + tb0)[:, 0].min(), (vb + tb1)[:, 0].min())
+    keep_f = (base[faces][:, :, 0].max(axis=1) >= b_min_x)
+    fa_s = faces[keep_f]
+    used = np.unique(fa_s)
+    remap = -np.ones(len(base), np.int64)
+    remap[used] = np.arange(len(used))
+    va_s = base[used]
+    fa_s = remap[fa_s].astype(np.uint32)
+    ea_full = len(scenes.unique_edges(faces))
+    ea_s = len(scenes.unique_edges(fa_s.astype(np.int32)))
+    nvb, nfb = len(vb), len(faces)
+    tests_full = len(base) * nfb + nvb * len(faces) + ea_full * ea_full
+    tests_sample = len(va_s) * nfb + nvb * len(fa_s) + ea_s * ea_full
+    z = np.zeros(3)
+    t_start = time.perf_counter()
+    build_s, cert_s, rounds, n_q = 0.0, 0.0, 0, 0
+    while True:
+        t0 = time.perf_counter()
+        pts, ees = oracle.ref_build_mesh_query(va_s, fa_s, z, z, vb, faces.astype(np.uint32), tb0, tb1)
+        t1 = time.perf_counter()
+        for rec in (pts, ees):
+            if len(rec):
+                oracle.ref_eval_batch(rec, 0.0, 1.0, cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth,
+                                      threads=threads)
+        t2 = time.perf_counter()
+        build_s += t1 - t0
+        cert_s += t2 - t1
+        n_q += len(pts) + len(ees)
+        rounds += 1
+        if time.perf_counter() - t_start >= budget_s:
+            break
+    scale = tests_full / tests_sample
+    step_s = (build_s * scale + cert_s) / rounds
+    return {"queries": n_q / rounds, "seconds": step_s,
+            "sample": f"translation-only form of the scene through the reference BuildMeshExactCertificateQuery "
+                      f"on sphere A's {len(fa_s)} triangles that reach B (all {n_q // rounds} candidates) vs the "
+                      f"full sphere B; build time x{scale:.1f} (= full/sample pair tests), plus reference "
+                      f"certificates of every candidate; {rounds} round(s)",
+            "build_s_full_extrapolated": build_s * scale / rounds, "certify_s": cert_s / rounds}
+
+
+WORKLOADS = {"plain": PlainWorkload, "scene": SceneWorkload}
 
 
 # --------------------------------------------------------------------------
@@ -228,6 +377,27 @@ def time_steps(torch, fn, steps, flush, stream):
     return times
 
 
+def count_kernels(torch, fn) -> tuple[int, dict]:
+    """Kernels one call of fn launches (torch profiler / CUPTI), by name."""
+    try:
+        from torch.profiler import ProfilerActivity, profile
+
+        torch.cuda.synchronize()
+        with profile(activities=[ProfilerActivity.CUDA]) as prof:
+            fn()
+            torch.cuda.synchronize()
+        names: dict[str, int] = {}
+        for ev in prof.events():
+            if getattr(ev, "device_type", None) is not None and "CUDA" in str(ev.device_type):
+                nm = ev.name
+                if "memcpy" in nm.lower() or "memset" in nm.lower():
+                    continue
+                names[nm] = names.get(nm, 0) + 1
+        return sum(names.values()), names
+    except Exception as exc:  # profiler unavailable: report unknown
+        return -1, {"error": str(exc)}
+
+
 def run_b200(args) -> dict | None:
     import torch
 
@@ -243,7 +413,8 @@ def run_b200(args) -> dict | None:
     torch.cuda.synchronize()
     _barrier(world)
     torch.cuda.synchronize()
-    sampler = ClockSampler(dev.index if world > 1 else int(os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0] or 0))
+    gpu_index = dev.index if world > 1 else int((os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]) or 0)
+    sampler = ClockSampler(gpu_index)
     sampler.start()
     times = time_steps(torch, wl.step, args.steps, flush, stream)
     torch.cuda.synchronize()
@@ -261,38 +432,67 @@ def run_b200(args) -> dict | None:
     total_q = wl.queries * world
     value = total_q / (ms_max * 1e-3)
     e2e_value = total_q / (e2e_ms * 1e-3)
+    n_kernels, kernel_names = count_kernels(torch, wl.step)
     census = wl.census()
     fp64_rate = certify.probe_fp64_rate(dev)
-    kernel_ms = ms  # the step is one certification launch (plus a 112-byte scratch reset)
-    achieved = census["fp64_ops"] / (kernel_ms * 1e-3)
+    peaks = _load_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "of fallback (6.65 TB/s)"
+    fp64_roof = {"bound": "fp64", "peak": fp64_rate / 1e12, "unit": "TFLOP/s", "traffic": None,
+                 "peak_source": "measured in-run: p2c_probe_fp64 (separately rounded DMUL+DADD chains)",
+                 "algorithmic_fp64_ops_per_launch": census["fp64_ops"],
+                 "nodes_per_launch": census["nodes_evaluated"]}
+    phases = None
+    if hasattr(wl, "step_phased"):
+        wl.phase_events.clear()
+        for _ in range(args.steps):
+            flush.fill_(1)
+            wl.step_phased()
+        torch.cuda.synchronize()
+        bp = statistics.mean(e0.elapsed_time(e1) for e0, e1, _ in wl.phase_events)
+        npm = statistics.mean(e1.elapsed_time(e2) for _, e1, e2 in wl.phase_events)
+        phases = {"broad_ms": bp, "narrow_ms": npm}
+        bp_bytes = wl.broad_phase_bytes()
+        broad_roof = {"bound": "hbm", "achieved": bp_bytes / (bp * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
+                      "frac": bp_bytes / (bp * 1e-3) / 1e9 / hbm_peak, "traffic": None,
+                      "peak_source": hbm_src, "kernel": "candidate generation (boxes, sort, sweep)",
+                      "algorithmic_bytes_per_step": bp_bytes}
+        narrow = dict(fp64_roof, kernel="certify_scene_kernel",
+                      achieved=census["fp64_ops"] / (npm * 1e-3) / 1e12,
+                      frac=census["fp64_ops"] / (npm * 1e-3) / fp64_rate)
+        roofline, secondary = (narrow, broad_roof) if npm >= bp else (broad_roof, narrow)
+    else:
+        roofline = dict(fp64_roof, kernel="certify_records_kernel", achieved=census["fp64_ops"] / (ms * 1e-3) / 1e12,
+                        frac=census["fp64_ops"] / (ms * 1e-3) / fp64_rate)
+        secondary = None
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
         r = wl.cpu_reference(threads, args.cpu_budget)
         cpu = {"value": r["queries"] / r["seconds"], "unit": "queries/s", "cores": threads, "kind": "reference",
-               "sample": r["sample"] + f" ({r['seconds']:.1f} s, {threads} threads over the reference's "
-                                       "EvaluatePointTriangleInterval/EvaluateEdgeEdgeInterval)"}
+               "sample": r["sample"]}
     if rank != 0:
         return None
     h2d, d2h = wl.io_bytes()
-    return {
+    line = {
         "metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
         "p50_ms": statistics.median(times), "p99_ms": sorted(times)[max(0, int(0.99 * len(times)) - 1)],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {**wl.config(), "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write)",
                    "parallelism": f"replicas x{world}"},
-        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-        "gpu_launches": wl.launches_per_step * args.steps,
-        "roofline": {"bound": "fp64", "achieved": achieved / 1e12, "peak": fp64_rate / 1e12, "unit": "TFLOP/s",
-                     "frac": achieved / fp64_rate, "traffic": None,
-                     "peak_source": "measured in-run: p2c_probe_fp64 (DMUL+DADD chains, no FMA)",
-                     "kernel": "certify_records_kernel",
-                     "algorithmic_fp64_ops_per_launch": census["fp64_ops"],
-                     "nodes_per_launch": census["nodes_evaluated"]},
+        "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "ms_per_step": e2e_ms},
+        "gpu_launches": n_kernels * args.steps if n_kernels >= 0 else None,
+        "kernels_per_step": kernel_names,
+        "roofline": roofline,
         "cpu_baseline": cpu,
         "clocks": clocks,
     }
+    if phases is not None:
+        line["phases"] = phases
+        line["roofline_secondary"] = secondary
+    return line
 
 
 def run_reference(args) -> dict | None:
@@ -300,38 +500,48 @@ def run_reference(args) -> dict | None:
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
-    import numpy as np  # noqa: F401
-
     import oracle
-    from p2cccd_b200 import certify, workloads
+    from p2cccd_b200 import certify, scenes, workloads
 
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libp2c_ref.so was not built"}
     threads = os.cpu_count() or 1
+    cfg = certify.CertConfig(1e-6, 1e-6, 32)
     if args.workload == "plain":
         spec = workloads.PlainSpec()
         w = workloads.plain_queries(spec)
-        cfg = certify.CertConfig(1e-6, 1e-6, 32)
         nq = len(w["vf"]) + len(w["ee"])
 
         def step():
+            t0 = time.perf_counter()
             for fam in ("vf", "ee"):
                 oracle.ref_eval_batch(w[fam], 0.0, 1.0, cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth,
                                       threads=threads)
-            return nq
+            return nq, time.perf_counter() - t0
         conf = {"workload": "plain exact CCD: 10,000 VF + 10,000 EE seeded FP64 queries", "queries_per_step": nq}
-        sample = f"the full {nq}-query batch per step"
+        sample = f"the full {nq}-query batch per step, {threads} threads over the reference certifier"
     else:
-        raise SystemExit(f"unknown workload {args.workload}")
+        scene = scenes.two_spheres()
+        holder = {}
+
+        def step():
+            r = _scene_reference_sample(scene, cfg, 0.0, threads)
+            holder["sample"] = r["sample"]
+            return r["queries"], r["seconds"]
+        conf = {"workload": "single-scene broad+narrow: two 40,960-triangle UV spheres, translation-only form "
+                            "(the reference mesh builder takes rigid translations only)"}
+        sample = None
     for _ in range(args.warmup):
         step()
-    times = []
+    times, q = [], 0
     for _ in range(args.steps):
-        t0 = time.perf_counter()
-        q = step()
-        times.append(time.perf_counter() - t0)
+        q, sec = step()
+        times.append(sec)
     ms = statistics.mean(times) * 1e3
     value = q / (ms * 1e-3)
+    if sample is None:
+        sample = holder["sample"]
+    conf["queries_per_step"] = q
     return {"metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": conf,
@@ -346,7 +556,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--workload", default="plain", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")

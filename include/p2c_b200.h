@@ -196,6 +196,79 @@ int p2c_certify_census(const p2c_point_triangle* pt_dev, int64_t n_pt,
                        void* workspace_dev, size_t workspace_bytes,
                        p2c_certify_stats* stats_dev, void* stream);
 
+/* ---- scenes: swept-AABB candidates and their certificates ----------------- */
+/* A scene: vertex trajectories over one step plus topology, all device arrays.
+ * Objects are connected components (the scene tool's DSU objects,
+ * scene_object_envelope_native_ti_walltime.cpp:497-520) or whole meshes. */
+typedef struct p2c_scene {
+  const double* v_t0;        /* nv x 3 positions at t = 0 */
+  const double* v_t1;        /* nv x 3 positions at t = 1 */
+  const int32_t* faces;      /* nf x 3 vertex indices */
+  const int32_t* edges;      /* ne x 2 vertex indices (unique edges) */
+  const int32_t* v_obj;      /* nv object ids; < 0 = vertex in no face (never a candidate) */
+  const int32_t* f_obj;      /* nf object ids */
+  const int32_t* e_obj;      /* ne object ids */
+  int64_t nv, nf, ne;
+  double thickness;          /* >= 0, added to every swept box (Expand, :263-270) */
+  int32_t exclude_self;      /* 1: no candidate inside one object (mesh-pair queries) */
+  int32_t pad;
+} p2c_scene;
+
+/* Workspace of p2c_scene_candidates for the given sizes and pair capacities. */
+size_t p2c_scene_candidates_workspace_bytes(int64_t nv, int64_t nf, int64_t ne, int64_t vf_cap, int64_t ee_cap);
+
+/* Swept-AABB candidate pairs of a scene by sweep-and-prune.  Replaces the
+ * pair loops of BuildMeshExactCertificateQuery (cpp/certificate/
+ * mesh_exact_query.cpp:211-317) and the scene tool's SweepPairs /
+ * BuildVFCandidates / BuildEECandidates (tools/scene_object_envelope_native_
+ * ti_walltime.cpp:603-699) with the same pair set.  Pairs are written as
+ * (vertex << 32 | face) and (edge_lo << 32 | edge_hi); counts_dev[0..3] =
+ * {vf pairs, ee pairs, error word (1: non-finite coordinate), sweep axis}.
+ * When a count exceeds its capacity only capacity pairs are kept and the
+ * caller retries with a larger buffer (counts are the full totals).
+ * sort_pairs = 1 sorts each list ascending, padding with ~0 up to its
+ * capacity: the order BuildMeshExactCertificateQuery emits its primitives. */
+int p2c_scene_candidates(const p2c_scene* scene, uint64_t* vf_pairs_dev, int64_t vf_cap,
+                         uint64_t* ee_pairs_dev, int64_t ee_cap, uint64_t* counts_dev,
+                         int sort_pairs, void* workspace_dev, size_t workspace_bytes, void* stream);
+
+/* Aggregate of a scene certification: the CertificateEngine::Evaluate
+ * reduction (certificate_engine.cpp:729-824) over the VF list then the EE list
+ * in pair order, plus per-status counts and the undecided (fallback-replay)
+ * queue length. */
+typedef struct p2c_scene_summary {
+  p2c_query_certificate query;
+  uint64_t collisions, separations, undecided;
+  uint64_t vf_certified, ee_certified;
+  uint64_t undecided_queued;                /* entries written to the undecided queue */
+  uint64_t error_word;                      /* 1: time budget, 2: pair overflow, 4: invalid geometry */
+} p2c_scene_summary;
+
+size_t p2c_scene_certify_workspace_bytes(void);
+
+/* Certificates of every candidate pair (the scene tool's every-candidate
+ * rows, RunAllExactRows :1239-1281, with the reference certifier instead of
+ * the external exact kernel).  n per family = min(counts_dev[k], cap) read on
+ * the device, so this can follow p2c_scene_candidates without a host sync.
+ * Results are positional with the pair lists.  Undecided candidates are
+ * appended to undecided_queue_dev as (family << 63 | pair position) when it is
+ * non-NULL (capacity undecided_cap).  summary_dev may be NULL. */
+int p2c_scene_certify(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t vf_cap,
+                      const uint64_t* ee_pairs_dev, int64_t ee_cap, const uint64_t* counts_dev,
+                      double interval_t0, double interval_t1, const p2c_cert_config* config,
+                      uint32_t family_mask,
+                      p2c_interval_result* vf_results_dev, p2c_interval_result* ee_results_dev,
+                      uint64_t* undecided_queue_dev, int64_t undecided_cap,
+                      p2c_scene_summary* summary_dev,
+                      void* workspace_dev, size_t workspace_bytes, void* stream);
+
+/* Materialise candidate pairs as reference primitive records (the output
+ * list of BuildMeshExactCertificateQuery): ids are scene indices, trajectory
+ * feature ids are vertex indices. */
+int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t n_vf,
+                          const uint64_t* ee_pairs_dev, int64_t n_ee,
+                          p2c_point_triangle* vf_records_dev, p2c_edge_edge* ee_records_dev, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* FP64 throughput probe: launches independent separately rounded multiply/add
  * chains over a full-occupancy grid and reports the FP64 operations it issues;

@@ -510,7 +510,8 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
       const double t = phase == 0 ? t0 : (phase == 1 ? t1 : mid);
       d = distance_at<kFamily>(g, t, ops);
       st.evals += 1;
-      if (phase == 2) st.nodes += 1;
+      // a node is counted once: the root at its first sample, others at their midpoint
+      if (phase == 0 || (phase == 2 && depth > 0)) st.nodes += 1;
       if (kCount) ops.add(phase == 2 ? 2 : 0);
     }
     // (E) classify.  leaf: 0 none, 1 collision, 2 separation, 3 undecided

@@ -1,0 +1,337 @@
+// scene.cu — certificates of scene candidate pairs, gathered straight from the
+// vertex/face/edge arrays (no 240-byte records are built), with the
+// CertificateEngine::Evaluate reduction and the on-device undecided queue.
+#include "broadphase.cuh"
+#include "certify_core.cuh"
+#include "certify_launch.cuh"
+
+namespace p2c {
+namespace {
+
+struct SceneAgg {
+  unsigned long long coll_key;     // min over collisions of (family - 1) << 63 | pair key
+  unsigned long long margin_bits;  // min separation margin (bit pattern of a non-negative double)
+  unsigned int any_sep[2];
+  unsigned int any_undecided[2];
+  unsigned long long collisions, separations, undecided, queued;
+  unsigned long long n_certified[2];
+};
+
+struct SceneScratch {
+  CertifyScratch cert;
+  SceneAgg agg;
+};
+
+struct ScenePairs {
+  const double* v_t0;
+  const double* v_t1;
+  const int32_t* faces;
+  const int32_t* edges;
+  const unsigned long long* pairs;
+  double T0, T1;
+};
+
+__device__ __forceinline__ void load_vertex(const ScenePairs& s, long long v, Geo& g, int slot, bool& finite) {
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double x0 = __ldg(s.v_t0 + 3 * v + a), x1 = __ldg(s.v_t1 + 3 * v + a);
+    g.p0[3 * slot + a] = x0;
+    g.p1[3 * slot + a] = x1;
+    finite = finite && isfinite(x0) && isfinite(x1);
+  }
+}
+
+template <int kFamily>
+struct PairSrc {
+  ScenePairs s;
+  __device__ __forceinline__ void load(long long q, Geo& g, double& t0, double& t1, int& bad) const {
+    const unsigned long long key = __ldg(s.pairs + q);
+    const long long a = (long long)(key >> 32), b = (long long)(key & 0xffffffffull);
+    bool finite = true;
+    if (kFamily == 1) {  // point = vertex a, triangle = face b
+      load_vertex(s, a, g, 0, finite);
+      const int32_t* f = s.faces + 3 * b;
+      load_vertex(s, __ldg(f), g, 1, finite);
+      load_vertex(s, __ldg(f + 1), g, 2, finite);
+      load_vertex(s, __ldg(f + 2), g, 3, finite);
+    } else {  // edge a then edge b
+      const int32_t* ea = s.edges + 2 * a;
+      const int32_t* eb = s.edges + 2 * b;
+      load_vertex(s, __ldg(ea), g, 0, finite);
+      load_vertex(s, __ldg(ea + 1), g, 1, finite);
+      load_vertex(s, __ldg(eb), g, 2, finite);
+      load_vertex(s, __ldg(eb + 1), g, 3, finite);
+    }
+    bad = finite ? 0 : 2;
+    t0 = s.T0;
+    t1 = s.T1;
+  }
+};
+
+template <int kFamily>
+struct PairSink {
+  const unsigned long long* pairs;
+  p2c_interval_result* out;
+  SceneAgg* agg;
+  unsigned long long* undecided_queue;
+  unsigned long long undecided_cap;
+  __device__ __forceinline__ void finish(long long q, int family, const Outcome& o) const {
+    const unsigned long long key = pairs[q];
+    store_interval_result(out + q, family, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
+    const int f = kFamily - 1;
+    if (o.status == P2C_STATUS_COLLISION) {
+      atomicMin(&agg->coll_key, ((unsigned long long)f << 63) | key);
+      atomicAdd(&agg->collisions, 1ull);
+    } else if (o.status == P2C_STATUS_SEPARATION) {
+      atomicMin(&agg->margin_bits, (unsigned long long)__double_as_longlong(o.margin));
+      if (agg->any_sep[f] == 0u) atomicExch(&agg->any_sep[f], 1u);
+      atomicAdd(&agg->separations, 1ull);
+    } else {
+      if (agg->any_undecided[f] == 0u) atomicExch(&agg->any_undecided[f], 1u);
+      atomicAdd(&agg->undecided, 1ull);
+      if (undecided_queue != nullptr) {
+        const unsigned long long slot = atomicAdd(&agg->queued, 1ull);
+        if (slot < undecided_cap) undecided_queue[slot] = ((unsigned long long)f << 63) | (unsigned long long)q;
+      }
+    }
+  }
+  __device__ __forceinline__ void invalid(long long q, int family, int bad, double T0, double T1) const {
+    Outcome o{3, T0, T1, T1, 0.0};
+    store_interval_result(out + q, family, o, -1, -1);
+    atomicOr((unsigned long long*)&reinterpret_cast<SceneScratch*>(agg)->cert.stats.error_word, 4ull);
+  }
+};
+
+__global__ void __launch_bounds__(kCertifyThreads, 1)
+    certify_scene_kernel(ScenePairs vf, long long vf_cap, ScenePairs ee, long long ee_cap,
+                         const unsigned long long* counts, unsigned family_mask, CertParams prm,
+                         p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
+                         unsigned long long uq_cap, SceneScratch* scratch) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
+  WarpStats st;
+  const unsigned long long t_start = global_ns();
+  const long long cvf = (long long)counts[0], cee = (long long)counts[1];
+  const long long n_vf = (family_mask & 1u) ? (cvf < vf_cap ? cvf : vf_cap) : 0;
+  const long long n_ee = (family_mask & 2u) ? (cee < ee_cap ? cee : ee_cap) : 0;
+  // fetch width from the device-side sizes (the host did not see them)
+  const long long warps = (long long)gridDim.x * kCertifyWarps;
+  CertParams p1 = prm, p2 = prm;
+  p1.fetch_limit = (int)min(32ll, max(1ll, (n_vf + warps - 1) / warps));
+  p2.fetch_limit = (int)min(32ll, max(1ll, (n_ee + warps - 1) / warps));
+  bool ok = true;
+  if (n_vf > 0)
+    ok = run_warp<1, true, false>(PairSrc<1>{vf}, PairSink<1>{vf.pairs, out_vf, &scratch->agg, uq, uq_cap}, n_vf,
+                                  &scratch->cert.queue_head[0], p1, ws, st, t_start);
+  if (ok && n_ee > 0)
+    ok = run_warp<2, true, false>(PairSrc<2>{ee}, PairSink<2>{ee.pairs, out_ee, &scratch->agg, uq, uq_cap}, n_ee,
+                                  &scratch->cert.queue_head[1], p2, ws, st, t_start);
+  flush_stats(st, ok, &scratch->cert);
+  if (threadIdx.x == 0 && blockIdx.x == 0) {
+    scratch->agg.n_certified[0] = (unsigned long long)n_vf;
+    scratch->agg.n_certified[1] = (unsigned long long)n_ee;
+    if (cvf > vf_cap || cee > ee_cap) atomicOr((unsigned long long*)&scratch->cert.stats.error_word, 2ull);
+  }
+}
+
+__device__ __forceinline__ uint8_t refinement_for_reason(uint16_t r) {  // certificate_engine.cpp:279-291
+  return r == P2C_REASON_MISSING_GEOMETRY ? P2C_REFINE_REQUEST_GEOMETRY
+         : r == P2C_REASON_MAX_SUBDIVISION_DEPTH ? P2C_REFINE_BISECT_INTERVAL
+         : r == P2C_REASON_INVALID_INPUT ? P2C_REFINE_REQUEST_GEOMETRY
+                                         : P2C_REFINE_ESCALATE_PRECISION;
+}
+
+// CertificateEngine::Evaluate over (VF list, EE list) from the reduced flags;
+// the collision witness is the candidate whose key won the atomicMin.
+__global__ void scene_summary_kernel(const SceneScratch* sc, const unsigned long long* vf_pairs,
+                                     const unsigned long long* ee_pairs, const p2c_interval_result* out_vf,
+                                     const p2c_interval_result* out_ee, unsigned family_mask, double T1,
+                                     p2c_scene_summary* summary) {
+  const SceneAgg& a = sc->agg;
+  const long long n_vf = (long long)a.n_certified[0], n_ee = (long long)a.n_certified[1];
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (a.coll_key != ~0ull) {
+    const int f = (int)(a.coll_key >> 63);
+    const unsigned long long key = a.coll_key & ~(1ull << 63);
+    const long long n = f == 0 ? n_vf : n_ee;
+    const unsigned long long* pairs = f == 0 ? vf_pairs : ee_pairs;
+    if (t < n && pairs[t] == key) {  // unique winner writes the certificate
+      const p2c_interval_result& r = (f == 0 ? out_vf : out_ee)[t];
+      p2c_query_certificate q{};
+      q.status = P2C_STATUS_COLLISION;
+      q.witness_family = r.witness_family;
+      q.toi_upper = r.toi_upper;
+      q.witness_id_a = r.witness_id_a;
+      q.witness_id_b = r.witness_id_b;
+      q.witness_index = t;
+      summary->query = q;
+    }
+  }
+  if (t != 0) return;
+  summary->collisions = a.collisions;
+  summary->separations = a.separations;
+  summary->undecided = a.undecided;
+  summary->vf_certified = (unsigned long long)n_vf;
+  summary->ee_certified = (unsigned long long)n_ee;
+  summary->undecided_queued = a.queued;
+  summary->error_word = sc->cert.stats.error_word;
+  if (a.coll_key != ~0ull) return;
+  // no collision: undecided (with the reference's reason order) or separation
+  p2c_query_certificate q{};
+  q.witness_id_a = -1;
+  q.witness_id_b = -1;
+  q.witness_index = -1;
+  q.toi_upper = T1;
+  bool evaluated_any = false, has_undecided = false;
+  uint16_t reason = P2C_REASON_NONE;
+  for (int f = 0; f < 2; ++f) {
+    if ((family_mask & (1u << f)) == 0u) continue;
+    const long long n = f == 0 ? n_vf : n_ee;
+    if (n == 0) {
+      has_undecided = true;
+      reason = P2C_REASON_MISSING_GEOMETRY;
+    } else {
+      evaluated_any = true;
+      if (a.any_undecided[f]) {
+        has_undecided = true;
+        reason = P2C_REASON_MAX_SUBDIVISION_DEPTH;
+      }
+    }
+  }
+  if (!evaluated_any || has_undecided) {
+    const uint16_t r = !evaluated_any ? (uint16_t)P2C_REASON_MISSING_GEOMETRY
+                                      : (reason == P2C_REASON_NONE ? (uint16_t)P2C_REASON_MAX_SUBDIVISION_DEPTH
+                                                                   : reason);
+    q.status = P2C_STATUS_UNDECIDED;
+    q.reason_code = r;
+    q.next_refinement_mode = refinement_for_reason(r);
+  } else {
+    q.status = P2C_STATUS_SEPARATION;
+    const double m = __longlong_as_double((long long)a.margin_bits);
+    q.safe_margin_lb = isfinite(m) ? m : 0.0;
+    q.covered_feature_mask = (a.any_sep[0] ? 1u : 0u) | (a.any_sep[1] ? 2u : 0u);
+  }
+  summary->query = q;
+}
+
+__global__ void materialize_kernel(ScenePairs s, long long n, int family, unsigned long long* recs) {
+  const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= n) return;
+  const unsigned long long key = s.pairs[q];
+  const long long a = (long long)(key >> 32), b = (long long)(key & 0xffffffffull);
+  long long v[4];
+  if (family == 1) {
+    v[0] = a;
+    v[1] = s.faces[3 * b];
+    v[2] = s.faces[3 * b + 1];
+    v[3] = s.faces[3 * b + 2];
+  } else {
+    v[0] = s.edges[2 * a];
+    v[1] = s.edges[2 * a + 1];
+    v[2] = s.edges[2 * b];
+    v[3] = s.edges[2 * b + 1];
+  }
+  unsigned long long* r = recs + 30 * q;
+  r[0] = (unsigned long long)a;
+  r[1] = (unsigned long long)b;
+  for (int i = 0; i < 4; ++i) {
+    unsigned long long* t = r + 2 + 7 * i;
+    t[0] = (unsigned long long)v[i];
+    for (int k = 0; k < 3; ++k) {
+      t[1 + k] = (unsigned long long)__double_as_longlong(s.v_t0[3 * v[i] + k]);
+      t[4 + k] = (unsigned long long)__double_as_longlong(s.v_t1[3 * v[i] + k]);
+    }
+  }
+}
+
+}  // namespace
+
+int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pairs, long long vf_cap,
+                         const unsigned long long* ee_pairs, long long ee_cap, const unsigned long long* counts,
+                         double T0, double T1, const p2c_cert_config& cfg, unsigned family_mask,
+                         p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
+                         long long uq_cap, p2c_scene_summary* summary, void* ws, size_t ws_bytes,
+                         cudaStream_t s) {
+  if (ws == nullptr || ws_bytes < sizeof(SceneScratch))
+    return fail(P2C_ERR_INVALID, "scene certification workspace too small");
+  SceneScratch* sc = reinterpret_cast<SceneScratch*>(ws);
+  P2C_CUDA(reset_scratch(&sc->cert, s));
+  P2C_CUDA(cudaMemsetAsync(&sc->agg, 0, sizeof(SceneAgg), s));
+  P2C_CUDA(cudaMemsetAsync(&sc->agg.coll_key, 0xff, sizeof(unsigned long long), s));
+  const unsigned long long inf_bits = 0x7ff0000000000000ull;
+  P2C_CUDA(cudaMemcpyAsync(&sc->agg.margin_bits, &inf_bits, sizeof(inf_bits), cudaMemcpyHostToDevice, s));
+  LaunchShape shape;
+  int rc = certify_shape(certify_scene_kernel, &shape);
+  if (rc != P2C_OK) return rc;
+  const CertParams prm = make_params(cfg, shape, 32ll * shape.grid * kCertifyWarps);
+  ScenePairs a{scene.v_t0, scene.v_t1, scene.faces, scene.edges, vf_pairs, T0, T1};
+  ScenePairs b{scene.v_t0, scene.v_t1, scene.faces, scene.edges, ee_pairs, T0, T1};
+  certify_scene_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
+      a, vf_cap, b, ee_cap, counts, family_mask, prm, out_vf, out_ee, uq, (unsigned long long)(uq_cap > 0 ? uq_cap : 0),
+      sc);
+  P2C_CUDA(cudaGetLastError());
+  if (summary != nullptr) {
+    const long long nmax = (vf_cap > ee_cap ? vf_cap : ee_cap);
+    const unsigned grid = (unsigned)((nmax + 255) / 256 > 0 ? (nmax + 255) / 256 : 1);
+    scene_summary_kernel<<<grid, 256, 0, s>>>(sc, vf_pairs, ee_pairs, out_vf, out_ee, family_mask, T1, summary);
+    P2C_CUDA(cudaGetLastError());
+  }
+  return P2C_OK;
+}
+
+int validate_scene(const p2c_scene* sc);
+
+}  // namespace p2c
+
+extern "C" {
+
+size_t p2c_scene_certify_workspace_bytes(void) { return sizeof(p2c::SceneScratch); }
+
+int p2c_scene_certify(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t vf_cap,
+                      const uint64_t* ee_pairs_dev, int64_t ee_cap, const uint64_t* counts_dev, double interval_t0,
+                      double interval_t1, const p2c_cert_config* config, uint32_t family_mask,
+                      p2c_interval_result* vf_results_dev, p2c_interval_result* ee_results_dev,
+                      uint64_t* undecided_queue_dev, int64_t undecided_cap, p2c_scene_summary* summary_dev,
+                      void* workspace_dev, size_t workspace_bytes, void* stream) {
+  int rc = p2c::validate_scene(scene);
+  if (rc != P2C_OK) return rc;
+  if (config == nullptr) return p2c::fail(P2C_ERR_INVALID, "CertificateEngineConfig pointer is null");
+  rc = p2c::validate_cert_config(*config, interval_t0, interval_t1);
+  if (rc != P2C_OK) return rc;
+  if (counts_dev == nullptr) return p2c::fail(P2C_ERR_INVALID, "counts pointer is null");
+  if (family_mask == 0u || family_mask > 3u)
+    return p2c::fail(P2C_ERR_INVALID, "ExactWorkItem.feature_family_mask is required");
+  if ((vf_cap > 0 && (vf_pairs_dev == nullptr || vf_results_dev == nullptr)) ||
+      (ee_cap > 0 && (ee_pairs_dev == nullptr || ee_results_dev == nullptr)))
+    return p2c::fail(P2C_ERR_INVALID, "pair or result pointer is null");
+  return p2c::launch_scene_certify(*scene, reinterpret_cast<const unsigned long long*>(vf_pairs_dev), vf_cap,
+                                   reinterpret_cast<const unsigned long long*>(ee_pairs_dev), ee_cap,
+                                   reinterpret_cast<const unsigned long long*>(counts_dev), interval_t0, interval_t1,
+                                   *config, family_mask, vf_results_dev, ee_results_dev,
+                                   reinterpret_cast<unsigned long long*>(undecided_queue_dev), undecided_cap,
+                                   summary_dev, workspace_dev, workspace_bytes, p2c::as_stream(stream));
+}
+
+int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t n_vf,
+                          const uint64_t* ee_pairs_dev, int64_t n_ee, p2c_point_triangle* vf_records_dev,
+                          p2c_edge_edge* ee_records_dev, void* stream) {
+  int rc = p2c::validate_scene(scene);
+  if (rc != P2C_OK) return rc;
+  cudaStream_t s = p2c::as_stream(stream);
+  if (n_vf > 0) {
+    p2c::ScenePairs a{scene->v_t0, scene->v_t1, scene->faces, scene->edges,
+                      reinterpret_cast<const unsigned long long*>(vf_pairs_dev), 0.0, 1.0};
+    p2c::materialize_kernel<<<(unsigned)((n_vf + 255) / 256), 256, 0, s>>>(
+        a, n_vf, 1, reinterpret_cast<unsigned long long*>(vf_records_dev));
+  }
+  if (n_ee > 0) {
+    p2c::ScenePairs b{scene->v_t0, scene->v_t1, scene->faces, scene->edges,
+                      reinterpret_cast<const unsigned long long*>(ee_pairs_dev), 0.0, 1.0};
+    p2c::materialize_kernel<<<(unsigned)((n_ee + 255) / 256), 256, 0, s>>>(
+        b, n_ee, 2, reinterpret_cast<unsigned long long*>(ee_records_dev));
+  }
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+}  // extern "C"
