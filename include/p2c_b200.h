@@ -196,6 +196,30 @@ int p2c_certify_census(const p2c_point_triangle* pt_dev, int64_t n_pt,
                        void* workspace_dev, size_t workspace_bytes,
                        p2c_certify_stats* stats_dev, void* stream);
 
+/* ---- work queues: many work items in one launch --------------------------- */
+size_t p2c_certify_queries_workspace_bytes(int64_t n_queries);
+
+/* CertificateEngine::Evaluate (certificate_engine.cpp:729-824) for every work
+ * item of a queue (ProcessExactWorkQueueCpu, :593-661) in one launch.  The
+ * queue's primitives are two flat record lists; pt_query/ee_query give each
+ * primitive's work-item index (non-decreasing; a work item's primitives are
+ * contiguous and in its list order) and pt_offsets/ee_offsets (n_queries + 1)
+ * the same as CSR offsets.  Each work item has its interval (q_t0, q_t1,
+ * already validated) and feature_family_mask; only primitives of requested
+ * families may be listed.  certs_dev[q] is the work item's certificate; a
+ * primitive failing validation before the first collision makes it undecided
+ * with reason InvalidInput, as the work queue reports an Evaluate error
+ * (:629-632).  One CertificateEngineConfig for the whole call. */
+int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const int64_t* pt_query_dev,
+                        const p2c_edge_edge* ee_dev, int64_t n_ee, const int64_t* ee_query_dev,
+                        int64_t n_queries, const int64_t* pt_offsets_dev, const int64_t* ee_offsets_dev,
+                        const double* q_t0_dev, const double* q_t1_dev, const uint32_t* q_mask_dev,
+                        const p2c_cert_config* config,
+                        p2c_interval_result* pt_results_dev, p2c_interval_result* ee_results_dev,
+                        p2c_query_certificate* certs_dev,
+                        void* workspace_dev, size_t workspace_bytes,
+                        p2c_certify_stats* stats_dev, void* stream);
+
 /* ---- scenes: swept-AABB candidates and their certificates ----------------- */
 /* A scene: vertex trajectories over one step plus topology, all device arrays.
  * Objects are connected components (the scene tool's DSU objects,

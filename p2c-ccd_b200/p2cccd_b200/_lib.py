@@ -49,6 +49,10 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_certify_ee_batch_host": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
     "p2c_certify_batch2": (_int, [_c_void_p, _i64, _c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig),
                                   _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
+    "p2c_certify_queries_workspace_bytes": (_size, [_i64]),
+    "p2c_certify_queries": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _i64, _c_void_p, _i64, _c_void_p,
+                                   _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.POINTER(CertConfig),
+                                   _c_void_p, _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
     "p2c_scene_candidates_workspace_bytes": (_size, [_i64, _i64, _i64, _i64, _i64]),
     "p2c_scene_candidates": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _i64, _c_void_p, _int, _c_void_p,
                                     _size, _c_void_p]),

@@ -1,0 +1,808 @@
+"""``p2cccd_cpp`` — the reference's compiled module surface for the
+certification hot path, backed by the B200 library.
+
+The reference builds ``p2cccd_cpp`` with pybind11
+(cpp/bindings/py_module.cpp:1803-2015); its Python host API
+(``p2cccd.cuda_bindings``, ``p2cccd.bench.rt_exact``) imports it by that name.
+This module keeps the names, argument meanings, return types and error
+convention (``ValueError`` for every reference ``Status`` error,
+py_module.cpp:38-42) of the entry points on this path, so those callers switch
+by putting this directory first on ``sys.path``.  Every certificate is computed
+by ``libp2c_b200.so`` on the GPU; there is no CPU certifier here (names ending
+in ``_cpu`` keep the reference's name; they run on the GPU too).
+
+Beyond the reference surface, ``*_tensor`` entry points take and return CUDA
+tensors of 240-byte / 72-byte records (``device_pointer_abi`` is True).
+"""
+from __future__ import annotations
+
+import enum
+import math
+from typing import Any, Sequence
+
+import numpy as np
+
+from p2cccd_b200 import _lib, records as _rec
+from p2cccd_b200.certify import CertConfig as _CertConfig
+
+# ---------------------------------------------------------------------------
+# enums (py_module.cpp:1326-1357)
+
+
+class ProxyType(enum.IntEnum):
+    UNKNOWN = 0
+    SWEPT_AABB = 1
+    CAPSULE = 2
+
+
+class ProposalSource(enum.IntEnum):
+    RAW = 0
+    REFINED = 1
+    FALLBACK = 2
+
+
+class CertificateStatus(enum.IntEnum):
+    COLLISION = 0
+    SEPARATION = 1
+    UNDECIDED = 2
+    Collision = 0
+    Separation = 1
+    Undecided = 2
+
+
+class CertificateRefinementMode(enum.IntEnum):
+    NONE = 0
+    BISECT_INTERVAL = 1
+    REQUEST_GEOMETRY = 2
+    ESCALATE_PRECISION = 3
+
+
+class AuditStage(enum.IntEnum):
+    RT = 0
+    PROPOSAL = 1
+    EXACT = 2
+    REFINE = 3
+    CERTIFY = 4
+
+
+FEATURE_FAMILY_POINT_TRIANGLE = 1
+FEATURE_FAMILY_EDGE_EDGE = 2
+CERTIFICATE_REASON_NONE = 0
+CERTIFICATE_REASON_MISSING_GEOMETRY = 1
+CERTIFICATE_REASON_MAX_SUBDIVISION_DEPTH = 2
+CERTIFICATE_REASON_INVALID_INPUT = 3
+EXACT_AUDIT_DEQUEUED = 1
+EXACT_AUDIT_COLLISION = 2
+EXACT_AUDIT_SEPARATION = 3
+EXACT_AUDIT_UNDECIDED = 4
+EXACT_AUDIT_INVALID_INPUT = 5
+CUDA_DEVICE_POINTER_ABI_ENABLED = True
+
+
+# ---------------------------------------------------------------------------
+# plain structs with the reference's fields and defaults
+
+
+class _Struct:
+    _fields: tuple = ()
+
+    def __init__(self):
+        for name, default in self._fields:
+            object.__setattr__(self, name, default() if callable(default) else default)
+
+    def __repr__(self):
+        inner = ", ".join(f"{n}={getattr(self, n)!r}" for n, _ in self._fields)
+        return f"{type(self).__name__}({inner})"
+
+    def __eq__(self, other):
+        return type(self) is type(other) and all(getattr(self, n) == getattr(other, n) for n, _ in self._fields)
+
+
+def _vec3(v) -> list:
+    out = [float(x) for x in v]
+    if len(out) != 3:
+        raise TypeError("expected a sequence of 3 floats")
+    return out
+
+
+class LinearVertexTrajectory(_Struct):
+    _fields = (("feature_id", -1), ("position_t0", lambda: [0.0, 0.0, 0.0]),
+               ("position_t1", lambda: [0.0, 0.0, 0.0]))
+
+    def __setattr__(self, name, value):
+        if name in ("position_t0", "position_t1"):
+            value = _vec3(value)
+        elif name == "feature_id":
+            value = int(value)
+        object.__setattr__(self, name, value)
+
+
+class PointTriangleIntervalPrimitive(_Struct):
+    _fields = (("point_id", -1), ("triangle_id", -1), ("point", LinearVertexTrajectory),
+               ("triangle_v0", LinearVertexTrajectory), ("triangle_v1", LinearVertexTrajectory),
+               ("triangle_v2", LinearVertexTrajectory))
+
+
+class EdgeEdgeIntervalPrimitive(_Struct):
+    _fields = (("edge_a_id", -1), ("edge_b_id", -1), ("edge_a0", LinearVertexTrajectory),
+               ("edge_a1", LinearVertexTrajectory), ("edge_b0", LinearVertexTrajectory),
+               ("edge_b1", LinearVertexTrajectory))
+
+
+class CertificateEngineConfig(_Struct):
+    _fields = (("eps_time", 1.0e-4), ("eps_space", 1.0e-6), ("max_subdivision_depth", 32))
+
+    def __setattr__(self, name, value):
+        if name == "max_subdivision_depth":
+            value = int(value)
+            if not 0 <= value <= 0xFFFF:
+                raise TypeError("max_subdivision_depth must fit in uint16")
+        else:
+            value = float(value)
+        object.__setattr__(self, name, value)
+
+
+class PrimitiveIntervalResult(_Struct):
+    _fields = (("status", CertificateStatus.UNDECIDED), ("covered_feature_mask", 0), ("interval_t0", 0.0),
+               ("interval_t1", 1.0), ("toi_upper", 1.0), ("safe_margin_lb", 0.0), ("witness_family", 0),
+               ("witness_id_a", -1), ("witness_id_b", -1), ("reason_code", 0),
+               ("next_refinement_mode", CertificateRefinementMode.NONE))
+
+
+class ExactWorkItem(_Struct):
+    _fields = (("work_item_id", 0), ("parent_candidate_id", 0), ("query_id", 0), ("slab_id", 0), ("patch_a_id", 0),
+               ("patch_b_id", 0), ("interval_t0", 0.0), ("interval_t1", 1.0), ("feature_family_mask", 0),
+               ("topk_feature_ids_offset", 0), ("depth", 0), ("priority_score", 0.0),
+               ("source", ProposalSource.RAW))
+
+
+class CertificateResult(_Struct):
+    _fields = (("work_item_id", 0), ("query_id", 0), ("status", CertificateStatus.UNDECIDED), ("interval_t0", 0.0),
+               ("interval_t1", 1.0), ("toi_upper", 1.0), ("safe_margin_lb", 0.0), ("witness_family", 0),
+               ("witness_id_a", -1), ("witness_id_b", -1), ("covered_feature_mask", 0), ("eps_time", 1.0e-4),
+               ("eps_space", 1.0e-6), ("reason_code", 0), ("next_refinement_mode", CertificateRefinementMode.NONE))
+
+
+class AuditLogRow(_Struct):
+    _fields = (("event_id", 0), ("query_id", 0), ("candidate_id", 0), ("work_item_id", 0), ("stage", AuditStage.RT),
+               ("action", 0), ("depth", 0), ("interval_t0", 0.0), ("interval_t1", 1.0), ("timestamp_us", 0),
+               ("aux_value0", 0.0), ("aux_value1", 0.0))
+
+
+class ExactCertificateQuery(_Struct):
+    _fields = (("work_item", ExactWorkItem), ("config", CertificateEngineConfig),
+               ("point_triangle_primitives", list), ("edge_edge_primitives", list))
+
+
+class ExactWorkQueueConfig(_Struct):
+    _fields = (("first_event_id", 1), ("first_timestamp_us", 1), ("emit_dequeue_events", True))
+
+
+class ExactWorkQueueResult(_Struct):
+    _fields = (("certificates", list), ("audit_log", list), ("processed_count", 0))
+
+
+class ExactRefinementConfig(_Struct):
+    _fields = (("first_child_work_item_id", 1), ("max_child_depth", 64), ("min_interval_width", 1.0e-4))
+
+
+class Mesh(_Struct):
+    _fields = (("vertices_ref", list), ("triangles", list), ("patch_ids", list))
+
+
+class MeshExactBuildConfig(_Struct):
+    _fields = (("prune_by_swept_aabb", True), ("max_point_triangle_primitives", 0), ("max_edge_edge_primitives", 0))
+
+
+class MeshExactBuildStats(_Struct):
+    _fields = tuple((n, 0) for n in (
+        "vertex_count_a", "vertex_count_b", "triangle_count_a", "triangle_count_b", "edge_count_a", "edge_count_b",
+        "point_triangle_total_pairs", "point_triangle_kept_pairs", "point_triangle_pruned_pairs",
+        "edge_edge_total_pairs", "edge_edge_kept_pairs", "edge_edge_pruned_pairs"))
+
+
+class MeshExactBuildResult(_Struct):
+    _fields = (("query", ExactCertificateQuery), ("stats", MeshExactBuildStats))
+
+
+# ---------------------------------------------------------------------------
+# conversions between these structs and the ABI records
+
+_PT_NAMES = ("point", "triangle_v0", "triangle_v1", "triangle_v2")
+_EE_NAMES = ("edge_a0", "edge_a1", "edge_b0", "edge_b1")
+
+
+def _to_records(prims: Sequence[Any], family: int) -> np.ndarray:
+    dt = _rec.POINT_TRIANGLE_DTYPE if family == 1 else _rec.EDGE_EDGE_DTYPE
+    names = _PT_NAMES if family == 1 else _EE_NAMES
+    ids = ("point_id", "triangle_id") if family == 1 else ("edge_a_id", "edge_b_id")
+    n = len(prims)
+    flat = np.zeros((n, 30), dtype=np.float64)
+    iv = flat.view(np.int64)
+    for i, p in enumerate(prims):
+        iv[i, 0] = int(getattr(p, ids[0]))
+        iv[i, 1] = int(getattr(p, ids[1]))
+        for k, nm in enumerate(names):
+            t = getattr(p, nm)
+            iv[i, 2 + 7 * k] = int(t.feature_id)
+            flat[i, 3 + 7 * k:6 + 7 * k] = t.position_t0
+            flat[i, 6 + 7 * k:9 + 7 * k] = t.position_t1
+    return flat.view(np.uint8).reshape(n, 240).view(dt).reshape(-1) if n else np.zeros(0, dtype=dt)
+
+
+def _from_records(rec: np.ndarray, family: int) -> list:
+    names = _PT_NAMES if family == 1 else _EE_NAMES
+    cls = PointTriangleIntervalPrimitive if family == 1 else EdgeEdgeIntervalPrimitive
+    ids = ("point_id", "triangle_id") if family == 1 else ("edge_a_id", "edge_b_id")
+    out = []
+    for r in rec:
+        p = cls()
+        setattr(p, ids[0], int(r[ids[0]]))
+        setattr(p, ids[1], int(r[ids[1]]))
+        for nm in names:
+            t = LinearVertexTrajectory()
+            t.feature_id = int(r[nm]["feature_id"])
+            t.position_t0 = r[nm]["position_t0"].tolist()
+            t.position_t1 = r[nm]["position_t1"].tolist()
+            setattr(p, nm, t)
+        out.append(p)
+    return out
+
+
+def _result_objects(res: np.ndarray) -> list:
+    out = []
+    for r in res:
+        o = PrimitiveIntervalResult()
+        o.status = CertificateStatus(int(r["status"]))
+        o.covered_feature_mask = int(r["covered_feature_mask"])
+        o.interval_t0 = float(r["interval_t0"])
+        o.interval_t1 = float(r["interval_t1"])
+        o.toi_upper = float(r["toi_upper"])
+        o.safe_margin_lb = float(r["safe_margin_lb"])
+        o.witness_family = int(r["witness_family"])
+        o.witness_id_a = int(r["witness_id_a"])
+        o.witness_id_b = int(r["witness_id_b"])
+        o.reason_code = int(r["reason_code"])
+        o.next_refinement_mode = CertificateRefinementMode(int(r["next_refinement_mode"]))
+        out.append(o)
+    return out
+
+
+def _config(c: CertificateEngineConfig) -> _CertConfig:
+    return _CertConfig(float(c.eps_time), float(c.eps_space), int(c.max_subdivision_depth))
+
+
+# ---------------------------------------------------------------------------
+# restated validators (cpp/common/validators.cpp)
+
+
+def _require_nonzero(v, name):
+    if int(v) == 0:
+        raise ValueError(f"{name} is required")
+
+
+def _require_finite(v, name):
+    if not math.isfinite(float(v)):
+        raise ValueError(f"{name} must be finite")
+
+
+def _validate_unit_interval(t0, t1):  # :60-72
+    _require_finite(t0, "interval_t0")
+    _require_finite(t1, "interval_t1")
+    if t0 < 0.0 or t1 > 1.0 or t0 > t1:
+        raise ValueError("interval must satisfy 0 <= interval_t0 <= interval_t1 <= 1")
+
+
+def validate_exact_work_item(item: ExactWorkItem) -> bool:  # validators.cpp:207-230
+    _require_nonzero(item.work_item_id, "ExactWorkItem.work_item_id")
+    _require_nonzero(item.parent_candidate_id, "ExactWorkItem.parent_candidate_id")
+    _require_nonzero(item.query_id, "ExactWorkItem.query_id")
+    _validate_unit_interval(item.interval_t0, item.interval_t1)
+    if int(item.feature_family_mask) == 0:
+        raise ValueError("ExactWorkItem.feature_family_mask is required")
+    _require_finite(item.priority_score, "ExactWorkItem.priority_score")
+    if int(item.source) not in (0, 1, 2):
+        raise ValueError("ExactWorkItem.source is invalid")
+    return True
+
+
+def validate_certificate_result(result: CertificateResult) -> bool:  # validators.cpp:232-293
+    _require_nonzero(result.work_item_id, "CertificateResult.work_item_id")
+    _require_nonzero(result.query_id, "CertificateResult.query_id")
+    if int(result.status) not in (0, 1, 2):
+        raise ValueError("CertificateResult.status is invalid")
+    _validate_unit_interval(result.interval_t0, result.interval_t1)
+    _require_finite(result.toi_upper, "CertificateResult.toi_upper")
+    _require_finite(result.safe_margin_lb, "CertificateResult.safe_margin_lb")
+    for v, n in ((result.eps_time, "CertificateResult.eps_time"), (result.eps_space, "CertificateResult.eps_space")):
+        _require_finite(v, n)
+        if not v > 0.0:
+            raise ValueError(f"{n} must be positive")
+    if int(result.next_refinement_mode) not in (0, 1, 2, 3):
+        raise ValueError("CertificateResult.next_refinement_mode is invalid")
+    st, mode = int(result.status), int(result.next_refinement_mode)
+    if st == 0:
+        if result.toi_upper < result.interval_t0 or result.toi_upper > result.interval_t1:
+            raise ValueError("CertificateResult.toi_upper must lie inside the certified interval")
+        if result.witness_id_a < 0 or result.witness_id_b < 0:
+            raise ValueError("CertificateResult collision witnesses are required")
+        if mode != 0:
+            raise ValueError("CertificateResult collision cannot request refinement")
+    if st == 1:
+        if result.safe_margin_lb < 0.0:
+            raise ValueError("CertificateResult.safe_margin_lb must be non-negative")
+        if result.covered_feature_mask == 0:
+            raise ValueError("CertificateResult.covered_feature_mask is required for separation")
+        if mode != 0:
+            raise ValueError("CertificateResult separation cannot request refinement")
+    if st == 2 and int(result.reason_code) == 0:
+        raise ValueError("CertificateResult.reason_code is required for undecided results")
+    if st == 2 and mode == 0:
+        raise ValueError("CertificateResult.next_refinement_mode is required for undecided results")
+    return True
+
+
+def validate_audit_log_row(row: AuditLogRow) -> bool:  # validators.cpp ValidateAuditLogRow
+    _require_nonzero(row.event_id, "AuditLogRow.event_id")
+    _require_nonzero(row.query_id, "AuditLogRow.query_id")
+    if int(row.stage) not in (0, 1, 2, 3, 4):
+        raise ValueError("AuditLogRow.stage is invalid")
+    _validate_unit_interval(row.interval_t0, row.interval_t1)
+    if int(row.timestamp_us) == 0:
+        raise ValueError("AuditLogRow.timestamp_us is required")
+    _require_finite(row.aux_value0, "AuditLogRow.aux_value0")
+    _require_finite(row.aux_value1, "AuditLogRow.aux_value1")
+    return True
+
+
+def validate_audit_log_rows(rows: Sequence[AuditLogRow]) -> bool:  # py_module.cpp:470-475
+    for r in rows:
+        validate_audit_log_row(r)
+    return True
+
+
+def audit_log_rows_for_query(rows: Sequence[AuditLogRow], query_id: int) -> list:  # py_module.cpp:477-487
+    return [r for r in rows if r.query_id == query_id]
+
+
+def _validate_config(c: CertificateEngineConfig) -> None:  # certificate_engine.cpp:224-232
+    if not math.isfinite(c.eps_time) or c.eps_time <= 0.0:
+        raise ValueError("CertificateEngineConfig.eps_time must be finite and positive")
+    if not math.isfinite(c.eps_space) or c.eps_space <= 0.0:
+        raise ValueError("CertificateEngineConfig.eps_space must be finite and positive")
+
+
+# ---------------------------------------------------------------------------
+# CUDA batch entry points (cuda_bindings.py:8-14; py_module.cpp:1966-1991)
+
+
+def is_cuda_exact_built() -> bool:
+    return bool(_lib.load().p2c_is_cuda_exact_built())
+
+
+def cuda_binding_status() -> dict:
+    built = is_cuda_exact_built()
+    return {
+        "cuda_exact_built": built,
+        "host_batch_exact_api": True,
+        "device_pointer_abi": True,
+        "backend_name": "b200_sm100a" if built else "unavailable",
+        "safety_policy": ("host-owned batch entry points copy in and out on the library's stream; "
+                          "*_tensor entry points take caller-owned CUDA tensors and never free them."),
+    }
+
+
+def _batch(primitives, family, interval_t0, interval_t1, config):
+    from p2cccd_b200 import certify
+
+    rec = _to_records(list(primitives), family)
+    res = certify.certify_batch_host(rec, float(interval_t0), float(interval_t1), _config(config))
+    return _result_objects(res)
+
+
+def evaluate_point_triangle_batch_cuda(primitives, interval_t0, interval_t1, config) -> list:
+    return _batch(primitives, 1, interval_t0, interval_t1, config)
+
+
+def evaluate_edge_edge_batch_cuda(primitives, interval_t0, interval_t1, config) -> list:
+    return _batch(primitives, 2, interval_t0, interval_t1, config)
+
+
+def evaluate_point_triangle_interval(primitive, interval_t0, interval_t1, config) -> PrimitiveIntervalResult:
+    return _batch([primitive], 1, interval_t0, interval_t1, config)[0]
+
+
+def evaluate_edge_edge_interval(primitive, interval_t0, interval_t1, config) -> PrimitiveIntervalResult:
+    return _batch([primitive], 2, interval_t0, interval_t1, config)[0]
+
+
+def evaluate_point_triangle_batch_cuda_tensor(records, interval_t0, interval_t1, config):
+    """CUDA uint8 (n, 240) records -> CUDA uint8 (n, 72) results (caller's stream, asynchronous)."""
+    from p2cccd_b200 import certify
+
+    return certify.certify_batch(records, 1, interval_t0, interval_t1, _config(config))
+
+
+def evaluate_edge_edge_batch_cuda_tensor(records, interval_t0, interval_t1, config):
+    from p2cccd_b200 import certify
+
+    return certify.certify_batch(records, 2, interval_t0, interval_t1, _config(config))
+
+
+def _compare(a: np.ndarray, b: np.ndarray, eps_cert: float, label: str) -> None:
+    """ComparePrimitiveResults (certificate_cuda.cu:554-583)."""
+    for x, y in zip(a, b):
+        if x["status"] != y["status"]:
+            raise ValueError(f"{label} status mismatch")
+        if x["covered_feature_mask"] != y["covered_feature_mask"]:
+            raise ValueError(f"{label} covered feature mask mismatch")
+        if x["status"] == 0:
+            if abs(x["toi_upper"] - y["toi_upper"]) > eps_cert:
+                raise ValueError(f"{label} TOI mismatch")
+            if (x["witness_family"], x["witness_id_a"], x["witness_id_b"]) != (
+                    y["witness_family"], y["witness_id_a"], y["witness_id_b"]):
+                raise ValueError(f"{label} witness mismatch")
+        if x["status"] == 1 and abs(x["safe_margin_lb"] - y["safe_margin_lb"]) > eps_cert:
+            raise ValueError(f"{label} safe margin mismatch")
+        if x["status"] == 2 and (x["reason_code"], x["next_refinement_mode"]) != (
+                y["reason_code"], y["next_refinement_mode"]):
+            raise ValueError(f"{label} undecided refinement mismatch")
+
+
+def cross_check_cpu_cuda_exact(point_triangles, edge_edges, interval_t0, interval_t1, config, eps_cert) -> bool:
+    """The reference cross-checks its CUDA kernel against its CPU recursion
+    (certificate_cuda.cu:616-679).  Here both sides run on the GPU: the
+    production warp-cooperative launch against the census launch, whose lanes
+    walk each interval tree depth-first exactly as the CPU recursion does; the
+    comparison rules are the reference's."""
+    import torch
+
+    from p2cccd_b200 import certify
+
+    if not math.isfinite(float(eps_cert)) or float(eps_cert) < 0.0:
+        raise ValueError("eps_cert must be finite and non-negative")
+    cfg = _config(config)
+    pt = _to_records(list(point_triangles), 1)
+    ee = _to_records(list(edge_edges), 2)
+    fast_pt = certify.certify_batch_host(pt, interval_t0, interval_t1, cfg)
+    fast_ee = certify.certify_batch_host(ee, interval_t0, interval_t1, cfg)
+    if len(pt) + len(ee) == 0:
+        return True
+    dev = torch.device("cuda", torch.cuda.current_device())
+    cen = certify.census(certify.records_to_device(pt, dev) if len(pt) else None,
+                         certify.records_to_device(ee, dev) if len(ee) else None, interval_t0, interval_t1, cfg)
+    _compare(certify.results_to_numpy(cen["pt"]), fast_pt, float(eps_cert), "point-triangle CPU/CUDA cross-check")
+    _compare(certify.results_to_numpy(cen["ee"]), fast_ee, float(eps_cert), "edge-edge CPU/CUDA cross-check")
+    return True
+
+
+# ---------------------------------------------------------------------------
+# certificate engine and work queue (certificate_engine.cpp:593-824)
+
+
+def _base_certificate(item: ExactWorkItem, cfg: CertificateEngineConfig) -> CertificateResult:  # :388-402
+    r = CertificateResult()
+    r.work_item_id = item.work_item_id
+    r.query_id = item.query_id
+    r.interval_t0 = item.interval_t0
+    r.interval_t1 = item.interval_t1
+    r.toi_upper = item.interval_t1
+    r.eps_time = cfg.eps_time
+    r.eps_space = cfg.eps_space
+    r.status = CertificateStatus.UNDECIDED
+    r.reason_code = CERTIFICATE_REASON_MISSING_GEOMETRY
+    r.next_refinement_mode = CertificateRefinementMode.REQUEST_GEOMETRY
+    return r
+
+
+def _certify_queries(queries: Sequence[ExactCertificateQuery]) -> list:
+    """One GPU launch per distinct config; returns per query a CertificateResult
+    or a ValueError (the Status Evaluate would return)."""
+    from p2cccd_b200 import queue
+
+    out: list = [None] * len(queries)
+    groups: dict = {}
+    for i, q in enumerate(queries):
+        try:
+            _validate_config(q.config)
+        except ValueError as exc:
+            out[i] = exc
+            continue
+        key = (float(q.config.eps_time), float(q.config.eps_space), int(q.config.max_subdivision_depth))
+        groups.setdefault(key, []).append(i)
+    for key, idx in groups.items():
+        pts, ees, pto, eeo, t0, t1, mask = [], [], [0], [0], [], [], []
+        for i in idx:
+            q = queries[i]
+            m = int(q.work_item.feature_family_mask)
+            p = list(q.point_triangle_primitives) if m & 1 else []
+            e = list(q.edge_edge_primitives) if m & 2 else []
+            pts += p
+            ees += e
+            pto.append(pto[-1] + len(p))
+            eeo.append(eeo[-1] + len(e))
+            t0.append(float(q.work_item.interval_t0))
+            t1.append(float(q.work_item.interval_t1))
+            mask.append(m)
+        res = queue.certify_work_items(_to_records(pts, 1), np.array(pto), _to_records(ees, 2), np.array(eeo),
+                                       np.array(t0), np.array(t1), np.array(mask, np.uint32), _CertConfig(*key))
+        invalid_msg = _first_invalid_messages(pts, ees, pto, eeo, res)
+        for j, i in enumerate(idx):
+            c = res["certs"][j]
+            if c["status"] == 2 and c["reason_code"] == CERTIFICATE_REASON_INVALID_INPUT:
+                out[i] = ValueError(invalid_msg.get(j, "primitive failed validation"))
+                continue
+            q = queries[i]
+            r = _base_certificate(q.work_item, q.config)
+            r.status = CertificateStatus(int(c["status"]))
+            r.toi_upper = float(c["toi_upper"])
+            r.safe_margin_lb = float(c["safe_margin_lb"])
+            r.witness_family = int(c["witness_family"])
+            r.witness_id_a = int(c["witness_id_a"])
+            r.witness_id_b = int(c["witness_id_b"])
+            r.covered_feature_mask = int(c["covered_feature_mask"])
+            r.reason_code = int(c["reason_code"])
+            r.next_refinement_mode = CertificateRefinementMode(int(c["next_refinement_mode"]))
+            out[i] = r
+    return out
+
+
+def _first_invalid_messages(pts, ees, pto, eeo, res) -> dict:
+    """Reference message of the first invalid primitive of each failed query."""
+    msgs = {}
+    for j in range(len(pto) - 1):
+        for fam, lst, off, results in ((1, pts, pto, res["pt_results"]), (2, ees, eeo, res["ee_results"])):
+            if j in msgs:
+                break
+            for k in range(off[j], off[j + 1]):
+                if results[k]["reason_code"] == CERTIFICATE_REASON_INVALID_INPUT:
+                    p = lst[k]
+                    a, b = (p.point_id, p.triangle_id) if fam == 1 else (p.edge_a_id, p.edge_b_id)
+                    kind = "point-triangle" if fam == 1 else "edge-edge"
+                    msgs[j] = (f"{kind} primitive ids are required" if a < 0 or b < 0
+                               else f"{kind} primitive trajectories must be finite")
+                    break
+    return msgs
+
+
+def evaluate_certificate_query_cpu(query: ExactCertificateQuery) -> CertificateResult:
+    _validate_config(query.config)
+    validate_exact_work_item(query.work_item)
+    r = _certify_queries([query])[0]
+    if isinstance(r, Exception):
+        raise r
+    return r
+
+
+class CertificateEngine:
+    def evaluate_work_item(self, work_item: ExactWorkItem) -> CertificateResult:  # :722-727
+        return _base_certificate(work_item, CertificateEngineConfig())
+
+    def evaluate_query(self, query: ExactCertificateQuery) -> CertificateResult:
+        return evaluate_certificate_query_cpu(query)
+
+
+def _audit_action(c: CertificateResult) -> int:  # :443-454
+    if c.status == CertificateStatus.COLLISION:
+        return EXACT_AUDIT_COLLISION
+    if c.status == CertificateStatus.SEPARATION:
+        return EXACT_AUDIT_SEPARATION
+    return EXACT_AUDIT_INVALID_INPUT if c.reason_code == CERTIFICATE_REASON_INVALID_INPUT else EXACT_AUDIT_UNDECIDED
+
+
+def _audit_row(event_id, ts, item, stage, action, aux0, aux1) -> AuditLogRow:  # :456-477
+    r = AuditLogRow()
+    r.event_id, r.query_id, r.candidate_id, r.work_item_id = event_id, item.query_id, item.parent_candidate_id, \
+        item.work_item_id
+    r.stage, r.action, r.depth = stage, action, item.depth
+    r.interval_t0, r.interval_t1, r.timestamp_us = item.interval_t0, item.interval_t1, ts
+    r.aux_value0, r.aux_value1 = float(aux0), float(aux1)
+    return r
+
+
+def process_exact_work_queue_cpu(work_queue: Sequence[ExactCertificateQuery],
+                                 config: ExactWorkQueueConfig) -> ExactWorkQueueResult:
+    """ProcessExactWorkQueueCpu (:593-661): every work item certified in one
+    GPU launch per config; audit rows and the coverage guard on the host."""
+    if int(config.first_event_id) == 0:
+        raise ValueError("ExactWorkQueueConfig.first_event_id must be non-zero")
+    if int(config.first_timestamp_us) == 0:
+        raise ValueError("ExactWorkQueueConfig.first_timestamp_us must be non-zero")
+    queue_list = list(work_queue)
+    for q in queue_list:
+        validate_exact_work_item(q.work_item)
+    certs = _certify_queries(queue_list)
+    result = ExactWorkQueueResult()
+    ev, ts = int(config.first_event_id), int(config.first_timestamp_us)
+    for q, c in zip(queue_list, certs):
+        if config.emit_dequeue_events:
+            row = _audit_row(ev, ts, q.work_item, AuditStage.EXACT, EXACT_AUDIT_DEQUEUED,
+                             float(np.float32(q.work_item.priority_score)), float(q.work_item.feature_family_mask))
+            validate_audit_log_row(row)
+            result.audit_log.append(row)
+            ev, ts = ev + 1, ts + 1
+        if isinstance(c, Exception):  # MakeInvalidInputCertificate, :426-431
+            c = _base_certificate(q.work_item, q.config)
+            c.reason_code = CERTIFICATE_REASON_INVALID_INPUT
+            c.next_refinement_mode = CertificateRefinementMode.REQUEST_GEOMETRY
+            c.safe_margin_lb = 0.0
+            c.covered_feature_mask = 0
+        validate_certificate_result(c)
+        aux0 = c.safe_margin_lb if c.status == CertificateStatus.SEPARATION else c.toi_upper
+        row = _audit_row(ev, ts, q.work_item, AuditStage.CERTIFY, _audit_action(c), aux0,
+                         float(int(c.next_refinement_mode)))
+        validate_audit_log_row(row)
+        ev, ts = ev + 1, ts + 1
+        result.certificates.append(c)
+        result.audit_log.append(row)
+        result.processed_count += 1
+    validate_exact_work_queue_coverage(queue_list, result)
+    return result
+
+
+def validate_exact_work_queue_coverage(work_queue, result) -> bool:  # :553-591
+    if result.processed_count != len(work_queue):
+        raise ValueError("exact work queue processed_count must match input size")
+    if len(result.certificates) != len(work_queue):
+        raise ValueError("each exact work item must produce exactly one certificate")
+    expected = set()
+    for q in work_queue:
+        validate_exact_work_item(q.work_item)
+        key = (q.work_item.query_id, q.work_item.work_item_id)
+        if key in expected:
+            raise ValueError("exact work queue contains duplicate work_item_id for a query")
+        expected.add(key)
+    covered = set()
+    for c in result.certificates:
+        validate_certificate_result(c)
+        key = (c.query_id, c.work_item_id)
+        if key not in expected:
+            raise ValueError("certificate references a work item that was not queued")
+        if key in covered:
+            raise ValueError("exact work item produced more than one certificate")
+        covered.add(key)
+    if len(covered) != len(expected):
+        raise ValueError("at least one exact work item disappeared without certificate coverage")
+    return True
+
+
+def generate_conservative_refinement_work_items(parent: ExactWorkItem, certificate: CertificateResult,
+                                                config: ExactRefinementConfig) -> list:  # :663-720
+    validate_exact_work_item(parent)
+    validate_certificate_result(certificate)
+    if certificate.work_item_id != parent.work_item_id or certificate.query_id != parent.query_id:
+        raise ValueError("certificate must correspond to the parent exact work item")
+    if int(config.first_child_work_item_id) == 0:
+        raise ValueError("ExactRefinementConfig.first_child_work_item_id must be non-zero")
+    if not math.isfinite(config.min_interval_width) or config.min_interval_width <= 0.0:
+        raise ValueError("ExactRefinementConfig.min_interval_width must be finite and positive")
+    if parent.depth >= config.max_child_depth:
+        return []
+
+    def child(wid, t0, t1):
+        c = ExactWorkItem()
+        for n, _ in ExactWorkItem._fields:
+            setattr(c, n, getattr(parent, n))
+        c.work_item_id, c.interval_t0, c.interval_t1 = wid, t0, t1
+        c.depth = (parent.depth + 1) & 0xFFFF
+        c.source = ProposalSource.REFINED
+        return c
+
+    if certificate.status == CertificateStatus.COLLISION:
+        t0 = parent.interval_t0
+        toi = certificate.toi_upper
+        t1 = parent.interval_t0 if toi < parent.interval_t0 else (parent.interval_t1 if parent.interval_t1 < toi
+                                                                  else toi)
+        return [child(config.first_child_work_item_id, t0, t1)] if t1 - t0 > config.min_interval_width else []
+    if (certificate.status == CertificateStatus.UNDECIDED
+            and certificate.next_refinement_mode == CertificateRefinementMode.BISECT_INTERVAL):
+        if parent.interval_t1 - parent.interval_t0 > config.min_interval_width:
+            mid = 0.5 * (parent.interval_t0 + parent.interval_t1)
+            return [child(config.first_child_work_item_id, parent.interval_t0, mid),
+                    child(config.first_child_work_item_id + 1, mid, parent.interval_t1)]
+    return []
+
+
+# ---------------------------------------------------------------------------
+# mesh-pair query (cpp/certificate/mesh_exact_query.cpp:143-327)
+
+
+def _mesh_arrays(mesh: Mesh):
+    v = np.asarray(mesh.vertices_ref, dtype=np.float64).reshape(-1, 3)
+    f = np.asarray(mesh.triangles, dtype=np.int64).reshape(-1, 3)
+    if not np.isfinite(v).all():
+        raise ValueError("mesh vertices must be finite")
+    if len(f) and (f.min() < 0 or f.max() >= len(v)):
+        raise ValueError("mesh triangle index out of range")
+    return v, f
+
+
+def build_mesh_exact_certificate_query(mesh_a, translation_a_t0, translation_a_t1, mesh_b, translation_b_t0,
+                                       translation_b_t1, work_item, config, build_config) -> MeshExactBuildResult:
+    """Candidate primitives of a translating mesh pair, found by the GPU
+    sweep-and-prune instead of the reference's O(V*F + E^2) loops; the list,
+    ids, order and statistics equal BuildMeshExactCertificateQuery's."""
+    import torch
+
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.scene import ScenePipeline
+
+    va, fa = _mesh_arrays(mesh_a)
+    vb, fb = _mesh_arrays(mesh_b)
+    validate_exact_work_item(work_item)
+    if int(build_config.max_point_triangle_primitives) >= 2 ** 64 - 1:
+        raise ValueError("max_point_triangle_primitives must be smaller than uint64 max")
+    if int(build_config.max_edge_edge_primitives) >= 2 ** 64 - 1:
+        raise ValueError("max_edge_edge_primitives must be smaller than uint64 max")
+    ta0, ta1, tb0, tb1 = (np.asarray(_vec3(t)) for t in (translation_a_t0, translation_a_t1, translation_b_t0,
+                                                         translation_b_t1))
+    ea, eb = scenes.unique_edges(fa.astype(np.int32)), scenes.unique_edges(fb.astype(np.int32))
+    scene = scenes.combine([(va + ta0, va + ta1, fa.astype(np.int32), ea), (vb + tb0, vb + tb1,
+                                                                            fb.astype(np.int32), eb)])
+    mask = int(work_item.feature_family_mask)
+    st = MeshExactBuildStats()
+    st.vertex_count_a, st.vertex_count_b = len(va), len(vb)
+    st.triangle_count_a, st.triangle_count_b = len(fa), len(fb)
+    st.edge_count_a, st.edge_count_b = len(ea), len(eb)
+    if build_config.prune_by_swept_aabb:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        pipe = ScenePipeline(scene, dev, exclude_self=True, config=_config(config), family_mask=3)
+        pipe.step_checked()
+        vf_rec, ee_rec = pipe.materialize()
+    else:  # every pair, no box test
+        nva, nfa, nea = len(va), len(fa), len(ea)
+        ab = np.stack(np.meshgrid(np.arange(nva), np.arange(len(fb)) + nfa, indexing="ij"), -1).reshape(-1, 2)
+        ba = np.stack(np.meshgrid(np.arange(len(vb)) + nva, np.arange(nfa), indexing="ij"), -1).reshape(-1, 2)
+        vf_pairs = np.concatenate([ab, ba])
+        ee_pairs = np.stack(np.meshgrid(np.arange(nea), np.arange(len(eb)) + nea, indexing="ij"), -1).reshape(-1, 2)
+        vf_rec = _materialize_host(scene, vf_pairs, 1)
+        ee_rec = _materialize_host(scene, ee_pairs, 2)
+    # the reference's trajectory feature ids (mesh_exact_query.cpp:244-258,
+    # 282-289, 302-313): B-triangle vertices carry triangle_offset_b + the B
+    # vertex index, A-side ids are plain A indices, B points and B edge
+    # vertices carry vertex_offset_b + index
+    nva, nfa = len(va), len(fa)
+    if len(vf_rec):
+        a_side = vf_rec["point_id"] < nva
+        for k in ("triangle_v0", "triangle_v1", "triangle_v2"):
+            fid = vf_rec[k]["feature_id"]
+            vf_rec[k]["feature_id"] = np.where(a_side, fid - nva + nfa, fid)
+    result = MeshExactBuildResult()
+    result.query.work_item = work_item
+    result.query.config = config
+    if mask & 1:
+        st.point_triangle_total_pairs = len(va) * len(fb) + len(vb) * len(fa)
+        st.point_triangle_kept_pairs = len(vf_rec)
+        st.point_triangle_pruned_pairs = st.point_triangle_total_pairs - len(vf_rec)
+        if build_config.max_point_triangle_primitives > 0 and len(vf_rec) > build_config.max_point_triangle_primitives:
+            raise ValueError("point-triangle primitive budget exceeded")
+        result.query.point_triangle_primitives = _from_records(vf_rec, 1)
+    if mask & 2:
+        st.edge_edge_total_pairs = len(ea) * len(eb)
+        st.edge_edge_kept_pairs = len(ee_rec)
+        st.edge_edge_pruned_pairs = st.edge_edge_total_pairs - len(ee_rec)
+        if build_config.max_edge_edge_primitives > 0 and len(ee_rec) > build_config.max_edge_edge_primitives:
+            raise ValueError("edge-edge primitive budget exceeded")
+        result.query.edge_edge_primitives = _from_records(ee_rec, 2)
+    result.stats = st
+    return result
+
+
+def _materialize_host(scene: dict, pairs: np.ndarray, family: int) -> np.ndarray:
+    n = len(pairs)
+    dt = _rec.POINT_TRIANGLE_DTYPE if family == 1 else _rec.EDGE_EDGE_DTYPE
+    rec = np.zeros(n, dtype=dt)
+    if n == 0:
+        return rec
+    a, b = pairs[:, 0], pairs[:, 1]
+    if family == 1:
+        verts = np.stack([a, *scene["faces"][b].T], 1)
+    else:
+        verts = np.concatenate([scene["edges"][a], scene["edges"][b]], 1)
+    names = dt.names
+    rec[names[0]], rec[names[1]] = a, b
+    for k in range(4):
+        rec[names[2 + k]]["feature_id"] = verts[:, k]
+        rec[names[2 + k]]["position_t0"] = scene["v_t0"][verts[:, k]]
+        rec[names[2 + k]]["position_t1"] = scene["v_t1"][verts[:, k]]
+    return rec

@@ -171,8 +171,8 @@ def test_undecided_queue_and_invalid_geometry(cuda_device, oracle_mod):
     pipe = ScenePipeline(s, cuda_device, exclude_self=True, config=cfg)
     summ = pipe.step_checked()
     vf_res, ee_res = pipe.results()
-    expect = sorted([(0 << 63) | i for i in np.nonzero(vf_res["status"] == 2)[0]] +
-                    [(1 << 63) | i for i in np.nonzero(ee_res["status"] == 2)[0]])
+    expect = sorted([int(i) for i in np.nonzero(vf_res["status"] == 2)[0]] +
+                    [(1 << 63) | int(i) for i in np.nonzero(ee_res["status"] == 2)[0]])
     assert summ["undecided"] == len(expect) > 0
     np.testing.assert_array_equal(np.sort(pipe.undecided_entries), np.array(expect, dtype=np.uint64))
     bad = dict(s)
