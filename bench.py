@@ -50,7 +50,7 @@ def _load_peaks() -> dict:
 class ClockSampler:
     """nvidia-smi clock/throttle sampling during the timed region."""
 
-    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    QUERY = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -63,7 +63,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.gpu_index}", f"--query-gpu={self.QUERY}", "--format=csv,noheader",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                 "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self._t = threading.Thread(target=self._read, daemon=True)
             self._t.start()
         except Exception:
@@ -73,30 +73,38 @@ class ClockSampler:
         for line in self.proc.stdout:
             self.lines.append(line.strip())
 
-    def stop(self) -> dict:
+    def stop(self, window: tuple[float, float] | None = None) -> dict:
+        """Median SM clock and active throttle reasons of the samples taken
+        inside ``window`` (epoch seconds); all samples if none fall in it."""
+        import datetime
+
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.12)
         self.proc.terminate()
         try:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm, mx, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        parsed = []
         for ln in self.lines:
             parts = [x.strip() for x in ln.split(",")]
-            if len(parts) < 9:
+            if len(parts) < 10:
                 continue
             try:
-                sm.append(float(parts[1].split()[0]))
-                mx = float(parts[2].split()[0])
+                ts = datetime.datetime.strptime(parts[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                sm = float(parts[2].split()[0])
+                mx = float(parts[3].split()[0])
             except ValueError:
                 continue
-            for name, val in zip(names, parts[5:9]):
-                if val.lower() == "active":
-                    reasons.add(name)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+            parsed.append((ts, sm, mx, [n for n, v in zip(names, parts[6:10]) if v.lower() == "active"]))
+        inside = [p for p in parsed if window and window[0] - 0.06 <= p[0] <= window[1] + 0.06]
+        use = inside or parsed
+        return {"sm_mhz": statistics.median(p[1] for p in use) if use else None,
+                "sm_max_mhz": use[-1][2] if use else None,
+                "reasons": sorted({r for p in use for r in p[3]}), "samples": len(use),
+                "samples_in_timed_region": len(inside)}
 
 
 # --------------------------------------------------------------------------
@@ -190,6 +198,7 @@ class SceneWorkload:
         self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
         self.pipe = ScenePipeline(self.scene, device, exclude_self=True, config=self.cfg)
         summ = self.pipe.step_checked()
+        self.pipe.capture()
         self.n_vf, self.n_ee = summ["vf_certified"], summ["ee_certified"]
         self.queries = self.n_vf + self.n_ee
         self.first_summary = summ
@@ -213,6 +222,9 @@ class SceneWorkload:
                 "max_subdivision_depth": self.cfg.max_subdivision_depth, "seed": sp["seed"]}
 
     def step(self):
+        self.pipe.replay()  # the captured step: one graph launch
+
+    def step_uncaptured(self):
         self.pipe.step()
 
     def step_phased(self):
@@ -229,7 +241,7 @@ class SceneWorkload:
     def step_e2e(self):
         self.pipe.v_t0.copy_(self.h_t0, non_blocking=True)
         self.pipe.v_t1.copy_(self.h_t1, non_blocking=True)
-        self.pipe.step()
+        self.pipe.replay()
         self.h_vf.copy_(self.pipe.vf_results, non_blocking=True)
         self.h_ee.copy_(self.pipe.ee_results, non_blocking=True)
         self.h_summary.copy_(self.pipe.summary, non_blocking=True)
@@ -408,18 +420,20 @@ def run_b200(args) -> dict | None:
     wl = WORKLOADS[args.workload](dev, rank)
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    gpu_index = dev.index if world > 1 else int((os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]) or 0)
+    sampler = ClockSampler(gpu_index)
+    sampler.start()
     for _ in range(args.warmup):
         wl.step()
     torch.cuda.synchronize()
     _barrier(world)
     torch.cuda.synchronize()
-    gpu_index = dev.index if world > 1 else int((os.environ.get("CUDA_VISIBLE_DEVICES", "0").split(",")[0]) or 0)
-    sampler = ClockSampler(gpu_index)
-    sampler.start()
+    t_begin = time.time()
     times = time_steps(torch, wl.step, args.steps, flush, stream)
     torch.cuda.synchronize()
+    t_end = time.time()
     _barrier(world)
-    clocks = sampler.stop()
+    clocks = sampler.stop((t_begin, t_end))
     # e2e through the public API with pinned host buffers
     for _ in range(max(1, args.warmup)):
         wl.step_e2e()
@@ -432,7 +446,7 @@ def run_b200(args) -> dict | None:
     total_q = wl.queries * world
     value = total_q / (ms_max * 1e-3)
     e2e_value = total_q / (e2e_ms * 1e-3)
-    n_kernels, kernel_names = count_kernels(torch, wl.step)
+    n_kernels, kernel_names = count_kernels(torch, getattr(wl, "step_uncaptured", wl.step))
     census = wl.census()
     fp64_rate = certify.probe_fp64_rate(dev)
     peaks = _load_peaks()
@@ -554,8 +568,8 @@ def run_reference(args) -> dict | None:
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
-    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")

@@ -235,7 +235,10 @@ typedef struct p2c_scene {
   int64_t nv, nf, ne;
   double thickness;          /* >= 0, added to every swept box (Expand, :263-270) */
   int32_t exclude_self;      /* 1: no candidate inside one object (mesh-pair queries) */
-  int32_t pad;
+  int32_t n_obj;             /* object ids lie in [0, n_obj); with exclude_self and
+                                1 <= n_obj <= 64, primitives outside every other object's
+                                swept box are culled first (the scene tool's object
+                                envelopes, :521-545); 0 = no culling */
 } p2c_scene;
 
 /* Workspace of p2c_scene_candidates for the given sizes and pair capacities. */

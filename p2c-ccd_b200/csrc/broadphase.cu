@@ -1,4 +1,5 @@
-// broadphase.cu — swept-AABB candidate generation by sweep-and-prune.
+// broadphase.cu — swept-AABB candidate generation by a column-subdivided
+// sweep-and-prune.
 //
 // Replaces the reference's CPU candidate builders: the brute-force
 // BuildMeshExactCertificateQuery pair loops (cpp/certificate/
@@ -9,45 +10,71 @@
 // against a face that contains it and no edges sharing a vertex inside one
 // object, optionally no pairs inside one object at all.
 //
-// Steps (all on the caller's stream, no host synchronisation):
-//   1. swept boxes of vertices, edges, faces (t0 and t1 positions, +thickness)
-//      with per-axis statistics;
-//   2. the sweep axis is chosen on the device: smallest mean box extent
-//      relative to the spread of box centres;
-//   3. CUB radix sort of the box minima along that axis (64-bit
-//      order-preserving keys), gather into struct-of-arrays in sorted order;
-//   4. sweeps: vertex-face as two bipartite passes (each pair found once:
-//      from the vertex when the face minimum is >= the vertex minimum, else
-//      from the face), edge-edge as one forward scan over the sorted list;
-//      overlapping pairs are compacted per warp with a ballot and appended with
-//      one atomic per warp.
-// The object-pair permission of the scene tool (PrepareScene, :521-545) needs
-// no separate pass: a primitive box lies inside its object's box (same
-// vertices, same thickness), so two overlapping primitive boxes of different
-// objects imply overlapping object boxes; only the same-object rule remains.
+// A one-axis sweep over a surface mesh scans windows of ~sqrt(n) boxes (a
+// whole slice of surface projects onto the axis).  Here the two non-sweep
+// axes are cut into columns at least as wide as the largest box, each box is
+// filed under the column of its min corner, and a box scans only the
+// columns its partners' min corners can lie in (at most 3 x 3).  Steps, all
+// on the caller's stream without host synchronisation:
+//   1. swept boxes (t0 and t1 positions, +thickness), per-axis statistics and
+//      object envelopes;
+//   2. culling: with self pairs excluded, a primitive outside every other
+//      object's envelope cannot have a candidate (the scene tool's object-pair
+//      permission, PrepareScene :521-545, used as a filter);
+//   3. device-side choice of the sweep axis (smallest mean extent relative to
+//      the spread of centres) and of the column grid;
+//   4. CUB radix sort on a 48-bit key (column << 32 | float(min) rounded
+//      down) and gather into struct-of-arrays;
+//   5. sweeps over float windows rounded outward, exact double tests, and an
+//      ownership rule so that every pair is emitted once; pairs are compacted
+//      per warp with a ballot and appended with one atomic per warp.
+// Overlapping boxes of different objects imply overlapping object envelopes
+// (each box lies inside its object's envelope), so beyond culling only the
+// same-object rule remains.
 #include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+#include <cmath>
 
 #include "broadphase.cuh"
 
 namespace p2c {
 namespace {
 
-constexpr int kBoxThreads = 256;
-constexpr int kSweepThreads = 256;
+constexpr int kThreads = 256;
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
 
-// Swept box of primitive i made of K vertices (K = 1 vertex, 2 edge, 3 face).
+inline unsigned grid_for(long long n, int threads) {
+  const long long g = (n + threads - 1) / threads;
+  return (unsigned)(g > 0 ? g : 1);
+}
+
+__global__ void init_scratch_kernel(BroadScratch* sc) {
+  const int t = threadIdx.x;
+  for (int i = t; i < kMaxCullObjects * 3; i += blockDim.x) {
+    (&sc->obj_lo[0][0])[i] = ~0ull;
+    (&sc->obj_hi[0][0])[i] = 0ull;
+  }
+  if (t < 9) {
+    sc->list[t / 3].lo_min[t % 3] = ~0ull;
+    sc->list[t / 3].hi_max[t % 3] = 0ull;
+  }
+}
+
+// Swept box of primitive i made of K vertices (K = 1 vertex, 2 edge, 3 face):
+// Extend/Expand/Swept*Box, scene_object_envelope_native_ti_walltime.cpp:256-301.
 template <int K>
-__global__ void __launch_bounds__(kBoxThreads) boxes_kernel(const double* __restrict__ v_t0,
-                                                            const double* __restrict__ v_t1,
-                                                            const int32_t* __restrict__ prim, long long n,
-                                                            double thickness, double* __restrict__ box,
-                                                            BroadScratch* sc) {
-  __shared__ double red[9][kBoxThreads / 32];
+__global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restrict__ v_t0,
+                                                         const double* __restrict__ v_t1,
+                                                         const int32_t* __restrict__ prim, long long n,
+                                                         double thickness, const int32_t* __restrict__ v_obj,
+                                                         int cull_objects, double* __restrict__ box,
+                                                         BroadScratch* sc) {
+  __shared__ double red[9][kThreads / 32];
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double ext[3] = {0, 0, 0}, cen[3] = {0, 0, 0}, cen2[3] = {0, 0, 0};
+  double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   unsigned long long cnt = 0;
   if (i < n) {
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -72,15 +99,25 @@ __global__ void __launch_bounds__(kBoxThreads) boxes_kernel(const double* __rest
     for (int a = 0; a < 3; ++a) {
       b[a] = __dsub_rn(mn[a], thickness);
       b[3 + a] = __dadd_rn(mx[a], thickness);
-      ext[a] = b[3 + a] - b[a];
-      cen[a] = 0.5 * (b[3 + a] + b[a]);
-      cen2[a] = cen[a] * cen[a];
+      const double c = 0.5 * (b[3 + a] + b[a]);
+      vals[a] = b[3 + a] - b[a];
+      vals[3 + a] = c;
+      vals[6 + a] = c * c;
     }
     cnt = 1;
     if (!finite) atomicOr(&sc->error_word, 1ull);
+    // object envelopes: the union of the object's vertex boxes
+    if (K == 1 && cull_objects > 0) {
+      const int o = v_obj[i];
+      if (o >= 0 && o < cull_objects) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          atomicMin(&sc->obj_lo[o][a], order_key(b[a]));
+          atomicMax(&sc->obj_hi[o][a], order_key(b[3 + a]));
+        }
+      }
+    }
   }
-  // block reduction of the axis statistics
-  double vals[9] = {ext[0], ext[1], ext[2], cen[0], cen[1], cen[2], cen2[0], cen2[1], cen2[2]};
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     double v = vals[k];
@@ -94,80 +131,170 @@ __global__ void __launch_bounds__(kBoxThreads) boxes_kernel(const double* __rest
   __syncthreads();
   if (threadIdx.x < 9) {
     double s = 0.0;
-    for (int w = 0; w < kBoxThreads / 32; ++w) s += red[threadIdx.x][w];
-    double* dst = threadIdx.x < 3 ? &sc->stats.extent_sum[threadIdx.x]
-                  : threadIdx.x < 6 ? &sc->stats.center_sum[threadIdx.x - 3]
-                                    : &sc->stats.center_sq_sum[threadIdx.x - 6];
+    for (int w = 0; w < kThreads / 32; ++w) s += red[threadIdx.x][w];
+    double* dst = threadIdx.x < 3 ? &sc->extent_sum[threadIdx.x]
+                  : threadIdx.x < 6 ? &sc->center_sum[threadIdx.x - 3]
+                                    : &sc->center_sq_sum[threadIdx.x - 6];
     atomicAdd(dst, s);
   }
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sc->stats.count, c);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sc->count, c);
 }
 
-// Sweep axis: the one whose mean box extent is smallest relative to the
-// standard deviation of box centres (fewest boxes overlap along it).
-__device__ __forceinline__ int choose_axis(const AxisStats& st) {
-  const double n = st.count > 0 ? (double)st.count : 1.0;
-  int best = 0;
-  double best_score = INFINITY;
+// Keep a box unless it is a vertex in no face or (self pairs excluded) it
+// lies outside every other object's envelope.  Per-list extents of the kept
+// boxes size the column grid.
+__global__ void __launch_bounds__(kThreads) classify_kernel(int list, const double* __restrict__ box, long long n,
+                                                            const int32_t* __restrict__ obj, int vertex_list,
+                                                            int cull_objects, unsigned char* __restrict__ active,
+                                                            BroadScratch* sc) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  bool keep = false;
+  double b[6] = {0, 0, 0, 0, 0, 0};
+  if (i < n) {
+    const int o = obj[i];
+    keep = !(vertex_list && o < 0);
+#pragma unroll
+    for (int k = 0; k < 6; ++k) b[k] = box[6 * i + k];
+    if (keep && cull_objects > 0) {
+      bool near_other = false;
+      for (int q = 0; q < cull_objects && !near_other; ++q) {
+        if (q == o || sc->obj_hi[q][0] == 0ull) continue;
+        bool ov = true;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+          const double olo = unorder_key(sc->obj_lo[q][a]), ohi = unorder_key(sc->obj_hi[q][a]);
+          ov = ov && b[a] <= ohi && olo <= b[3 + a];
+        }
+        near_other = ov;
+      }
+      keep = near_other;
+    }
+    active[i] = keep ? 1 : 0;
+  }
+  ListStats& L = sc->list[list];
+  const unsigned mask = __ballot_sync(0xffffffffu, keep);
+  if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&L.active, (unsigned long long)__popc(mask));
+#pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const double mean = st.center_sum[a] / n;
-    const double var = fmax(st.center_sq_sum[a] / n - mean * mean, 0.0);
-    const double score = (st.extent_sum[a] / n) / (sqrt(var) + 1e-300);
-    if (score < best_score) {
-      best_score = score;
-      best = a;
+    unsigned long long ext = keep ? (unsigned long long)__double_as_longlong(b[3 + a] - b[a]) : 0ull;
+    unsigned long long lo = keep ? order_key(b[a]) : ~0ull;
+    unsigned long long hi = keep ? order_key(b[3 + a]) : 0ull;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+      ext = max(ext, __shfl_down_sync(0xffffffffu, ext, s));
+      lo = min(lo, __shfl_down_sync(0xffffffffu, lo, s));
+      hi = max(hi, __shfl_down_sync(0xffffffffu, hi, s));
+    }
+    if ((threadIdx.x & 31) == 0 && mask) {
+      atomicMax(&L.ext_max[a], ext);
+      atomicMin(&L.lo_min[a], lo);
+      atomicMax(&L.hi_max[a], hi);
     }
   }
-  return best;
 }
 
-// Keys for one list; valid == nullptr keeps every primitive, otherwise
-// primitives with valid[i] < 0 sort to the end with key ~0 and are skipped.
-__global__ void __launch_bounds__(kBoxThreads) keys_kernel(const double* __restrict__ box, long long n,
-                                                           const int32_t* __restrict__ skip_if_negative,
-                                                           unsigned long long* __restrict__ keys,
-                                                           unsigned int* __restrict__ vals, BroadScratch* sc) {
+// Sweep axis and column grid (one thread).
+__global__ void grid_kernel(BroadScratch* sc) {
+  const double n = sc->count > 0 ? (double)sc->count : 1.0;
+  int axis = 0;
+  double best = INFINITY;
+  for (int a = 0; a < 3; ++a) {
+    const double mean = sc->center_sum[a] / n;
+    const double var = fmax(sc->center_sq_sum[a] / n - mean * mean, 0.0);
+    const double score = (sc->extent_sum[a] / n) / (sqrt(var) + 1e-300);
+    if (score < best) {
+      best = score;
+      axis = a;
+    }
+  }
+  Grid g;
+  g.axis = axis;
+  g.a1 = axis == 0 ? 1 : 0;
+  g.a2 = axis == 2 ? 1 : 2;
+  g.pad = 0;
+  const int ax[2] = {g.a1, g.a2};
+  double base[2], inv[2];
+  int cols[2];
+  for (int k = 0; k < 2; ++k) {
+    double lo = INFINITY, hi = -INFINITY, reach = 0.0;
+    for (int l = 0; l < 3; ++l) {
+      const ListStats& L = sc->list[l];
+      if (L.active == 0) {
+        (k == 0 ? g.reach1 : g.reach2)[l] = 0.0;
+        continue;
+      }
+      lo = fmin(lo, unorder_key(L.lo_min[ax[k]]));
+      hi = fmax(hi, unorder_key(L.hi_max[ax[k]]));
+      const double r = __longlong_as_double((long long)L.ext_max[ax[k]]);
+      (k == 0 ? g.reach1 : g.reach2)[l] = r;
+      reach = fmax(reach, r);
+    }
+    const double range = (hi > lo) ? hi - lo : 0.0;
+    double width = fmax(reach, range / kMaxColumns);
+    if (!(width > 0.0) || !isfinite(width)) width = 1.0;
+    int c = (int)fmin((double)kMaxColumns, floor(range / width) + 1.0);
+    if (c < 1) c = 1;
+    base[k] = isfinite(lo) ? lo : 0.0;
+    inv[k] = 1.0 / width;
+    cols[k] = c;
+  }
+  g.base1 = base[0];
+  g.base2 = base[1];
+  g.inv1 = inv[0];
+  g.inv2 = inv[1];
+  g.g1 = cols[0];
+  g.g2 = cols[1];
+  sc->grid = g;
+}
+
+__device__ __forceinline__ int column(double x, double base, double inv, int g) {
+  const double c = floor((x - base) * inv);
+  return c < 0.0 ? 0 : (c >= (double)g ? g - 1 : (int)c);
+}
+
+__global__ void __launch_bounds__(kThreads) keys_kernel(const double* __restrict__ box, long long n,
+                                                        const unsigned char* __restrict__ active,
+                                                        unsigned long long* __restrict__ keys,
+                                                        unsigned int* __restrict__ vals, const BroadScratch* sc) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int axis = choose_axis(sc->stats);
-  if (i == 0 && blockIdx.x == 0) sc->stats.axis = axis;
-  const bool skip = skip_if_negative != nullptr && skip_if_negative[i] < 0;
-  keys[i] = skip ? ~0ull : order_key(box[6 * i + axis]);
+  const Grid& g = sc->grid;
+  unsigned long long key = ~0ull;
+  if (active[i]) {
+    const double* b = box + 6 * i;
+    const int c = column(b[g.a1], g.base1, g.inv1, g.g1) * g.g2 + column(b[g.a2], g.base2, g.inv2, g.g2);
+    key = ((unsigned long long)(unsigned)c << 32) | fkey_down(b[g.axis]);
+  }
+  keys[i] = key;
   vals[i] = (unsigned int)i;
 }
 
-__global__ void __launch_bounds__(kBoxThreads) gather_kernel(const double* __restrict__ box, long long n,
-                                                             const int32_t* __restrict__ skip_if_negative,
-                                                             const unsigned int* __restrict__ order,
-                                                             const int32_t* __restrict__ obj, SortedBoxes s,
-                                                             const BroadScratch* sc) {
+// Sorted entries to struct-of-arrays plus the column ranges.
+__global__ void __launch_bounds__(kThreads) gather_kernel(const double* __restrict__ box,
+                                                          const unsigned long long* __restrict__ keys,
+                                                          const unsigned int* __restrict__ order, int list,
+                                                          const int32_t* __restrict__ obj, SortedBoxes s,
+                                                          const BroadScratch* sc) {
+  const long long n = (long long)sc->list[list].active;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int axis = choose_axis(sc->stats);
-  const int a1 = axis == 0 ? 1 : 0;
-  const int a2 = axis == 2 ? 1 : 2;
-  const unsigned int j = order[i];
-  if (skip_if_negative != nullptr && skip_if_negative[j] < 0) {
-    // skipped entries (vertices in no face) sorted last: keep lo monotonic
-    s.lo[i] = INFINITY;
-    s.hi[i] = -INFINITY;
-    s.alo[i] = INFINITY;
-    s.ahi[i] = -INFINITY;
-    s.blo[i] = INFINITY;
-    s.bhi[i] = -INFINITY;
-    s.id[i] = (int32_t)j;
-    s.obj[i] = -1;
-    return;
-  }
+  const Grid& g = sc->grid;
+  const unsigned long long key = keys[i];
+  const unsigned j = order[i];
   const double* b = box + 6 * (long long)j;
-  s.lo[i] = b[axis];
-  s.hi[i] = b[3 + axis];
-  s.alo[i] = b[a1];
-  s.ahi[i] = b[3 + a1];
-  s.blo[i] = b[a2];
-  s.bhi[i] = b[3 + a2];
+  s.lo[i] = b[g.axis];
+  s.hi[i] = b[3 + g.axis];
+  s.alo[i] = b[g.a1];
+  s.ahi[i] = b[3 + g.a1];
+  s.blo[i] = b[g.a2];
+  s.bhi[i] = b[3 + g.a2];
+  s.fkey[i] = (unsigned)(key & 0xffffffffull);
   s.id[i] = (int32_t)j;
   s.obj[i] = obj[j];
+  const int cell = (int)(key >> 32);
+  s.cell[i] = cell;
+  if (i == 0 || (int)(keys[i - 1] >> 32) != cell) s.cell_begin[cell] = (unsigned)i;
+  if (i == n - 1 || (int)(keys[i + 1] >> 32) != cell) s.cell_end[cell] = (unsigned)(i + 1);
 }
 
 // Warp-aggregated append of the pairs found by this iteration.
@@ -186,60 +313,93 @@ __device__ __forceinline__ void append_pair(bool found, unsigned long long key, 
   }
 }
 
-__device__ __forceinline__ long long lower_bound_ge(const double* a, long long n, double x) {
-  long long lo = 0, hi = n;
-  while (lo < hi) {
-    const long long m = (lo + hi) >> 1;
-    if (a[m] < x) lo = m + 1;
-    else hi = m;
+// Walk over the candidate entries of one scanning box: the columns its
+// partners' min corners can lie in, and in each the float window
+// [fkey_down(lo), fkey_up(hi)] of the partner list.
+struct Walker {
+  int c1, c1_end, c2_begin, c2, c2_end;
+  unsigned j, j_end, fk_hi;
+
+  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g, unsigned fk_lo) {
+    for (;;) {
+      if (++c2 > c2_end) {
+        c2 = c2_begin;
+        if (++c1 > c1_end) return false;
+      }
+      const int cell = c1 * g.g2 + c2;
+      unsigned b = Q.cell_begin[cell], e = Q.cell_end[cell];
+      // lower bound of fk_lo in [b, e)
+      while (b < e) {
+        const unsigned m = (b + e) >> 1;
+        if (Q.fkey[m] < fk_lo) b = m + 1;
+        else e = m;
+      }
+      j = b;
+      j_end = Q.cell_end[cell];
+      if (j < j_end && Q.fkey[j] <= fk_hi) return true;
+    }
   }
-  return lo;
-}
-__device__ __forceinline__ long long upper_bound_gt(const double* a, long long n, double x) {
-  long long lo = 0, hi = n;
-  while (lo < hi) {
-    const long long m = (lo + hi) >> 1;
-    if (a[m] <= x) lo = m + 1;
-    else hi = m;
-  }
-  return lo;
+};
+
+__device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double alo, double ahi, double blo,
+                                            double bhi, double reach1, double reach2, double hi) {
+  // widen the lower columns by a relative 2^-40 so that the rounding of
+  // alo - reach can never skip the column of a partner's min corner
+  const double l1 = alo - reach1 - (fabs(alo) + reach1) * 0x1p-40;
+  const double l2 = blo - reach2 - (fabs(blo) + reach2) * 0x1p-40;
+  w.c1 = column(l1, g.base1, g.inv1, g.g1);
+  w.c1_end = column(ahi, g.base1, g.inv1, g.g1);
+  w.c2_begin = column(l2, g.base2, g.inv2, g.g2);
+  w.c2_end = column(bhi, g.base2, g.inv2, g.g2);
+  w.c2 = w.c2_begin - 1;
+  w.j = w.j_end = 0;
+  w.fk_hi = fkey_up(hi);
 }
 
-__device__ __forceinline__ bool overlap_other_axes(const SortedBoxes& p, long long i, const SortedBoxes& q,
-                                                   long long j) {
-  return p.alo[i] <= q.ahi[j] && q.alo[j] <= p.ahi[i] && p.blo[i] <= q.bhi[j] && q.blo[j] <= p.bhi[i];
+__device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, const SortedBoxes& Q, long long j) {
+  return P.lo[i] <= Q.hi[j] && Q.lo[j] <= P.hi[i] && P.alo[i] <= Q.ahi[j] && Q.alo[j] <= P.ahi[i] &&
+         P.blo[i] <= Q.bhi[j] && Q.blo[j] <= P.bhi[i];
 }
 
-// Vertex-face: threads [0, nv) scan faces from each vertex, threads
-// [nv, nv + nf) scan vertices from each face.  Keys are (vertex << 32 | face).
-__global__ void __launch_bounds__(kSweepThreads) sweep_vf_kernel(SortedBoxes V, long long nv, SortedBoxes F,
-                                                                 long long nf, const int32_t* __restrict__ faces,
-                                                                 int exclude_self, unsigned long long* out,
-                                                                 unsigned long long cap, BroadScratch* sc) {
+// Vertex-face pairs: threads [0, nv) scan faces from a vertex and own the
+// pairs whose face minimum is >= the vertex minimum; threads [nv, nv + nf)
+// scan vertices from a face and own the others.  Keys (vertex << 32 | face).
+__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
+                                                            const int32_t* __restrict__ faces, int exclude_self,
+                                                            unsigned long long* out, unsigned long long cap,
+                                                            BroadScratch* sc) {
+  const long long nv = (long long)sc->list[0].active, nf = (long long)sc->list[1].active;
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if ((long long)blockIdx.x * blockDim.x >= nv + nf) return;  // whole warp beyond the work
   const bool from_vertex = t < nv;
   const long long i = from_vertex ? t : t - nv;
-  bool live = from_vertex ? (t < nv) : (i < nf);
-  // the caller sorted skipped vertices (object < 0) to the end
-  if (live && from_vertex && V.obj[i] < 0) live = false;
-  const SortedBoxes P = from_vertex ? V : F;  // this thread's box
-  const SortedBoxes Q = from_vertex ? F : V;  // the list it scans
-  const long long nq = from_vertex ? nf : nv;
-  long long j = 0;
-  double hi = 0.0;
+  bool live = from_vertex ? true : (i < nf);
+  const SortedBoxes P = from_vertex ? V : F;
+  const SortedBoxes Q = from_vertex ? F : V;
+  const Grid& g = sc->grid;
+  Walker w;
+  double lo = 0.0;
+  int32_t pid = 0, pobj = 0;
+  unsigned fk_lo = 0;
   if (live) {
-    hi = P.hi[i];
-    j = from_vertex ? lower_bound_ge(Q.lo, nq, P.lo[i]) : upper_bound_gt(Q.lo, nq, P.lo[i]);
+    lo = P.lo[i];
+    pid = P.id[i];
+    pobj = P.obj[i];
+    fk_lo = P.fkey[i];
+    walker_init(w, g, P.alo[i], P.ahi[i], P.blo[i], P.bhi[i], from_vertex ? g.reach1[1] : g.reach1[0],
+                from_vertex ? g.reach2[1] : g.reach2[0], P.hi[i]);
+    live = w.next_cell(Q, g, fk_lo);
   }
-  const int32_t pid = live ? P.id[i] : 0, pobj = live ? P.obj[i] : 0;
   for (;;) {
-    const bool active = live && j < nq && Q.lo[j] <= hi;
-    if (!__any_sync(0xffffffffu, active)) break;
+    if (!__any_sync(0xffffffffu, live)) break;
     bool found = false;
     unsigned long long key = 0;
-    if (active) {
-      const int32_t qobj = Q.obj[j];
-      if (qobj >= 0 && P.lo[i] <= Q.hi[j] && overlap_other_axes(P, i, Q, j)) {
+    if (live) {
+      const unsigned j = w.j;
+      const double qlo = Q.lo[j];
+      const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
+      if (own && overlap3(P, i, Q, j)) {
+        const int32_t qobj = Q.obj[j];
         const int32_t vtx = from_vertex ? pid : Q.id[j];
         const int32_t fc = from_vertex ? Q.id[j] : pid;
         bool ok = true;
@@ -255,38 +415,48 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_vf_kernel(SortedBoxes V, 
           key = ((unsigned long long)(unsigned)vtx << 32) | (unsigned)fc;
         }
       }
-      ++j;
+      ++w.j;
+      if (w.j >= w.j_end || Q.fkey[w.j] > w.fk_hi) live = w.next_cell(Q, g, fk_lo);
     }
     append_pair(found, key, out, cap, &sc->vf_count);
   }
 }
 
-// Edge-edge: each edge scans forward over the sorted list; keys are
-// (min edge << 32 | max edge).
-__global__ void __launch_bounds__(kSweepThreads) sweep_ee_kernel(SortedBoxes E, long long ne,
-                                                                 const int32_t* __restrict__ edges, int exclude_self,
-                                                                 unsigned long long* out, unsigned long long cap,
-                                                                 BroadScratch* sc) {
+// Edge-edge pairs: each edge scans its own list and owns the pairs whose
+// partner minimum is larger (ties: larger edge index).
+// Keys (min edge << 32 | max edge).
+__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
+                                                            int exclude_self, unsigned long long* out,
+                                                            unsigned long long cap, BroadScratch* sc) {
+  const long long ne = (long long)sc->list[2].active;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool live = i < ne;
-  double hi = 0.0;
+  if ((long long)blockIdx.x * blockDim.x >= ne) return;
+  bool live = i < ne;
+  const Grid& g = sc->grid;
+  Walker w;
+  double lo = 0.0;
   int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
+  unsigned fk_lo = 0;
   if (live) {
-    hi = E.hi[i];
+    lo = E.lo[i];
     eid = E.id[i];
     eobj = E.obj[i];
+    fk_lo = E.fkey[i];
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
+    walker_init(w, g, E.alo[i], E.ahi[i], E.blo[i], E.bhi[i], g.reach1[2], g.reach2[2], E.hi[i]);
+    live = w.next_cell(E, g, fk_lo);
   }
-  long long j = i + 1;
   for (;;) {
-    const bool active = live && j < ne && E.lo[j] <= hi;
-    if (!__any_sync(0xffffffffu, active)) break;
+    if (!__any_sync(0xffffffffu, live)) break;
     bool found = false;
     unsigned long long key = 0;
-    if (active) {
-      if (overlap_other_axes(E, i, E, j)) {
-        const int32_t oid = E.id[j];
+    if (live) {
+      const unsigned j = w.j;
+      const double qlo = E.lo[j];
+      const int32_t oid = E.id[j];
+      const bool own = qlo > lo || (qlo == lo && oid > eid);
+      if (own && overlap3(E, i, E, j)) {
         bool ok = true;
         if (E.obj[j] == eobj) {
           if (exclude_self) ok = false;
@@ -297,11 +467,12 @@ __global__ void __launch_bounds__(kSweepThreads) sweep_ee_kernel(SortedBoxes E, 
         }
         if (ok) {
           found = true;
-          const unsigned lo = (unsigned)min(eid, oid), hi2 = (unsigned)max(eid, oid);
-          key = ((unsigned long long)lo << 32) | hi2;
+          const unsigned l = (unsigned)min(eid, oid), h = (unsigned)max(eid, oid);
+          key = ((unsigned long long)l << 32) | h;
         }
       }
-      ++j;
+      ++w.j;
+      if (w.j >= w.j_end || E.fkey[w.j] > w.fk_hi) live = w.next_cell(E, g, fk_lo);
     }
     append_pair(found, key, out, cap, &sc->ee_count);
   }
@@ -316,10 +487,10 @@ __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long*
   counts[0] = sc->vf_count;
   counts[1] = sc->ee_count;
   counts[2] = sc->error_word;
-  counts[3] = (unsigned long long)sc->stats.axis;
+  counts[3] = (unsigned long long)sc->grid.axis | ((unsigned long long)sc->grid.g1 << 8) |
+              ((unsigned long long)sc->grid.g2 << 24) | (sc->list[0].active + sc->list[1].active + sc->list[2].active)
+                                                            << 40;
 }
-
-inline unsigned grid_for(long long n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 // ---- workspace carving -----------------------------------------------------
 struct Carver {
@@ -335,7 +506,7 @@ struct Carver {
   }
 };
 
-size_t sort_temp_bytes(long long n) {
+size_t sort_pairs_temp_bytes(long long n) {
   size_t bytes = 0;
   cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
   cub::DoubleBuffer<unsigned int> v(nullptr, nullptr);
@@ -352,16 +523,20 @@ size_t sort_keys_temp_bytes(long long n) {
 
 struct Layout {
   BroadScratch* sc;
-  BoxList V, F, E;
+  BoxList L[3];  // vertices, faces, edges
+  unsigned* cells;  // 3 lists x (begin, end) x kMaxColumns^2
   void* sort_tmp;
   size_t sort_tmp_bytes;
-  unsigned long long* pair_alt;  // double buffer for sorting pairs
+  unsigned long long* pair_alt;
   size_t total;
 };
+
+constexpr long long kCells = (long long)kMaxColumns * kMaxColumns;
 
 void carve_list(Carver& c, BoxList& L, long long n) {
   L.n = n;
   L.box = c.take<double>(6 * n);
+  L.active = c.take<unsigned char>(n);
   L.keys[0] = c.take<unsigned long long>(n);
   L.keys[1] = c.take<unsigned long long>(n);
   L.vals[0] = c.take<unsigned int>(n);
@@ -372,27 +547,39 @@ void carve_list(Carver& c, BoxList& L, long long n) {
   L.s.ahi = c.take<double>(n);
   L.s.blo = c.take<double>(n);
   L.s.bhi = c.take<double>(n);
+  L.s.fkey = c.take<unsigned>(n);
   L.s.id = c.take<int32_t>(n);
   L.s.obj = c.take<int32_t>(n);
+  L.s.cell = c.take<int32_t>(n);
 }
 
 Layout carve(void* base, long long nv, long long nf, long long ne, long long pair_cap, bool dry) {
   Carver c{static_cast<char*>(base), 0, dry};
   Layout L;
   L.sc = c.take<BroadScratch>(1);
-  carve_list(c, L.V, nv);
-  carve_list(c, L.F, nf);
-  carve_list(c, L.E, ne);
-  long long nmax = nv > nf ? nv : nf;
-  nmax = nmax > ne ? nmax : ne;
-  size_t tb = sort_temp_bytes(nmax);
-  const size_t tk = sort_keys_temp_bytes(pair_cap);
-  if (tk > tb) tb = tk;
-  L.sort_tmp_bytes = tb;
-  L.sort_tmp = c.take<char>((long long)tb);
+  carve_list(c, L.L[0], nv);
+  carve_list(c, L.L[1], nf);
+  carve_list(c, L.L[2], ne);
+  L.cells = c.take<unsigned>(6 * kCells);
+  for (int l = 0; l < 3; ++l) {
+    L.L[l].s.cell_begin = dry ? nullptr : L.cells + (2 * l) * kCells;
+    L.L[l].s.cell_end = dry ? nullptr : L.cells + (2 * l + 1) * kCells;
+  }
+  const long long nmax = std::max(nv, std::max(nf, ne));
+  L.sort_tmp_bytes = std::max(sort_pairs_temp_bytes(nmax), sort_keys_temp_bytes(pair_cap));
+  L.sort_tmp = c.take<char>((long long)L.sort_tmp_bytes);
   L.pair_alt = c.take<unsigned long long>(pair_cap);
   L.total = c.off + 256;
   return L;
+}
+
+int bit_length(long long x) {
+  int b = 0;
+  while (x > 0) {
+    ++b;
+    x >>= 1;
+  }
+  return b;
 }
 
 int sort_list(BoxList& L, const Layout& lay, cudaStream_t s) {
@@ -400,7 +587,8 @@ int sort_list(BoxList& L, const Layout& lay, cudaStream_t s) {
   cub::DoubleBuffer<unsigned long long> k(L.keys[0], L.keys[1]);
   cub::DoubleBuffer<unsigned int> v(L.vals[0], L.vals[1]);
   size_t tb = lay.sort_tmp_bytes;
-  P2C_CUDA(cub::DeviceRadixSort::SortPairs(lay.sort_tmp, tb, k, v, (int)L.n, 0, 64, s));
+  // key = column (16 bits) << 32 | float key; inactive entries are ~0 and sort last
+  P2C_CUDA(cub::DeviceRadixSort::SortPairs(lay.sort_tmp, tb, k, v, (int)L.n, 0, 32 + kCellBits, s));
   if (k.Current() != L.keys[0]) {
     std::swap(L.keys[0], L.keys[1]);
     std::swap(L.vals[0], L.vals[1]);
@@ -408,11 +596,13 @@ int sort_list(BoxList& L, const Layout& lay, cudaStream_t s) {
   return P2C_OK;
 }
 
-int sort_pairs(unsigned long long* pairs, long long cap, const Layout& lay, cudaStream_t s) {
+int sort_pairs(unsigned long long* pairs, long long cap, long long first_count, const Layout& lay, cudaStream_t s) {
   if (cap <= 1) return P2C_OK;
   cub::DoubleBuffer<unsigned long long> k(pairs, lay.pair_alt);
   size_t tb = lay.sort_tmp_bytes;
-  P2C_CUDA(cub::DeviceRadixSort::SortKeys(lay.sort_tmp, tb, k, (int)cap, 0, 64, s));
+  // keys are (first << 32 | second) with first < first_count; padding is ~0
+  const int end_bit = std::min(64, 32 + bit_length(first_count) + 1);
+  P2C_CUDA(cub::DeviceRadixSort::SortKeys(lay.sort_tmp, tb, k, (int)cap, 0, end_bit, s));
   if (k.Current() != pairs)
     P2C_CUDA(cudaMemcpyAsync(pairs, k.Current(), sizeof(unsigned long long) * cap, cudaMemcpyDeviceToDevice, s));
   return P2C_OK;
@@ -427,6 +617,7 @@ int validate_scene(const p2c_scene* sc) {
     return fail(P2C_ERR_INVALID, "scene counts must stay below 2^31");
   if (!(sc->thickness >= 0.0) || !std::isfinite(sc->thickness))
     return fail(P2C_ERR_INVALID, "scene thickness must be finite and non-negative");
+  if (sc->n_obj < 0) return fail(P2C_ERR_INVALID, "scene n_obj must be non-negative");
   if (sc->nv > 0 && (sc->v_t0 == nullptr || sc->v_t1 == nullptr || sc->v_obj == nullptr))
     return fail(P2C_ERR_INVALID, "scene vertex arrays are null");
   if (sc->nf > 0 && (sc->faces == nullptr || sc->f_obj == nullptr))
@@ -440,55 +631,61 @@ size_t broadphase_workspace_bytes(long long nv, long long nf, long long ne, long
   return carve(nullptr, nv, nf, ne, pair_cap, true).total;
 }
 
-// Candidate generation; counts_dev receives {vf_count, ee_count, error_word, axis}.
+// Candidate generation; counts_dev receives {vf_count, ee_count, error_word,
+// axis | g1 << 8 | g2 << 24 | kept boxes << 40}.
 int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long long vf_cap,
                       unsigned long long* ee_out, long long ee_cap, unsigned long long* counts_dev, bool sort_out,
                       void* ws, size_t ws_bytes, cudaStream_t s) {
-  const long long pair_cap = vf_cap > ee_cap ? vf_cap : ee_cap;
+  const long long pair_cap = std::max(vf_cap, ee_cap);
   const size_t need = broadphase_workspace_bytes(scene.nv, scene.nf, scene.ne, pair_cap);
   if (ws == nullptr || ws_bytes < need)
     return fail(P2C_ERR_INVALID, "candidate workspace too small: %zu < %zu bytes", ws_bytes, need);
   Layout L = carve(ws, scene.nv, scene.nf, scene.ne, pair_cap, false);
+  const int cull = (scene.exclude_self && scene.n_obj >= 1 && scene.n_obj <= kMaxCullObjects) ? scene.n_obj : 0;
   P2C_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(BroadScratch), s));
+  P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
+  init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
   if (scene.nv > 0)
-    boxes_kernel<1><<<grid_for(scene.nv, kBoxThreads), kBoxThreads, 0, s>>>(scene.v_t0, scene.v_t1, nullptr,
-                                                                             scene.nv, scene.thickness, L.V.box, L.sc);
-  if (scene.ne > 0)
-    boxes_kernel<2><<<grid_for(scene.ne, kBoxThreads), kBoxThreads, 0, s>>>(
-        scene.v_t0, scene.v_t1, scene.edges, scene.ne, scene.thickness, L.E.box, L.sc);
+    boxes_kernel<1><<<grid_for(scene.nv, kThreads), kThreads, 0, s>>>(
+        scene.v_t0, scene.v_t1, nullptr, scene.nv, scene.thickness, scene.v_obj, cull, L.L[0].box, L.sc);
   if (scene.nf > 0)
-    boxes_kernel<3><<<grid_for(scene.nf, kBoxThreads), kBoxThreads, 0, s>>>(
-        scene.v_t0, scene.v_t1, scene.faces, scene.nf, scene.thickness, L.F.box, L.sc);
+    boxes_kernel<3><<<grid_for(scene.nf, kThreads), kThreads, 0, s>>>(
+        scene.v_t0, scene.v_t1, scene.faces, scene.nf, scene.thickness, nullptr, 0, L.L[1].box, L.sc);
+  if (scene.ne > 0)
+    boxes_kernel<2><<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(
+        scene.v_t0, scene.v_t1, scene.edges, scene.ne, scene.thickness, nullptr, 0, L.L[2].box, L.sc);
   P2C_CUDA(cudaGetLastError());
   const int32_t* objs[3] = {scene.v_obj, scene.f_obj, scene.e_obj};
-  BoxList* lists[3] = {&L.V, &L.F, &L.E};
-  for (int k = 0; k < 3; ++k) {
-    BoxList& B = *lists[k];
+  for (int l = 0; l < 3; ++l) {
+    if (L.L[l].n == 0) continue;
+    classify_kernel<<<grid_for(L.L[l].n, kThreads), kThreads, 0, s>>>(l, L.L[l].box, L.L[l].n, objs[l], l == 0,
+                                                                      cull, L.L[l].active, L.sc);
+  }
+  grid_kernel<<<1, 1, 0, s>>>(L.sc);
+  P2C_CUDA(cudaGetLastError());
+  for (int l = 0; l < 3; ++l) {
+    BoxList& B = L.L[l];
     if (B.n == 0) continue;
-    keys_kernel<<<grid_for(B.n, kBoxThreads), kBoxThreads, 0, s>>>(B.box, B.n, k == 0 ? scene.v_obj : nullptr,
-                                                                   B.keys[0], B.vals[0], L.sc);
+    keys_kernel<<<grid_for(B.n, kThreads), kThreads, 0, s>>>(B.box, B.n, B.active, B.keys[0], B.vals[0], L.sc);
     P2C_CUDA(cudaGetLastError());
     int rc = sort_list(B, L, s);
     if (rc != P2C_OK) return rc;
-    gather_kernel<<<grid_for(B.n, kBoxThreads), kBoxThreads, 0, s>>>(B.box, B.n, k == 0 ? scene.v_obj : nullptr,
-                                                                     B.vals[0], objs[k], B.s, L.sc);
+    gather_kernel<<<grid_for(B.n, kThreads), kThreads, 0, s>>>(B.box, B.keys[0], B.vals[0], l, objs[l], B.s, L.sc);
     P2C_CUDA(cudaGetLastError());
   }
-  if (sort_out && vf_cap > 0)
-    fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
-  if (sort_out && ee_cap > 0)
-    fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
+  if (sort_out && vf_cap > 0) fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
+  if (sort_out && ee_cap > 0) fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
   if (scene.nv + scene.nf > 0 && vf_out != nullptr)
-    sweep_vf_kernel<<<grid_for(scene.nv + scene.nf, kSweepThreads), kSweepThreads, 0, s>>>(
-        L.V.s, scene.nv, L.F.s, scene.nf, scene.faces, scene.exclude_self, vf_out, (unsigned long long)vf_cap, L.sc);
+    sweep_vf_kernel<<<grid_for(scene.nv + scene.nf, kThreads), kThreads, 0, s>>>(
+        L.L[0].s, L.L[1].s, scene.faces, scene.exclude_self, vf_out, (unsigned long long)vf_cap, L.sc);
   if (scene.ne > 0 && ee_out != nullptr)
-    sweep_ee_kernel<<<grid_for(scene.ne, kSweepThreads), kSweepThreads, 0, s>>>(
-        L.E.s, scene.ne, scene.edges, scene.exclude_self, ee_out, (unsigned long long)ee_cap, L.sc);
+    sweep_ee_kernel<<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(L.L[2].s, scene.edges, scene.exclude_self,
+                                                                      ee_out, (unsigned long long)ee_cap, L.sc);
   P2C_CUDA(cudaGetLastError());
   if (sort_out) {
-    int rc = sort_pairs(vf_out, vf_cap, L, s);
+    int rc = sort_pairs(vf_out, vf_cap, scene.nv, L, s);
     if (rc != P2C_OK) return rc;
-    rc = sort_pairs(ee_out, ee_cap, L, s);
+    rc = sort_pairs(ee_out, ee_cap, scene.ne, L, s);
     if (rc != P2C_OK) return rc;
   }
   export_counts_kernel<<<1, 1, 0, s>>>(L.sc, counts_dev);

@@ -1,5 +1,5 @@
-// broadphase.cuh — scene description and scratch layout of the swept-AABB
-// sweep-and-prune (device side of p2c_scene_candidates).
+// broadphase.cuh — scratch layout of the column-subdivided sweep-and-prune
+// (device side of p2c_scene_candidates).
 #pragma once
 
 #include <cstdint>
@@ -9,49 +9,75 @@
 
 namespace p2c {
 
-// Order-preserving map of a finite double to uint64 (radix-sortable key).
+constexpr int kMaxCullObjects = 64;  // object-envelope culling up to this many objects
+constexpr int kMaxColumns = 256;     // columns per non-sweep axis (cell id < 2^16)
+constexpr int kCellBits = 16;
+
+// Order-preserving maps to unsigned integers (radix-sortable keys).
 __device__ __forceinline__ unsigned long long order_key(double x) {
   const unsigned long long b = (unsigned long long)__double_as_longlong(x);
   return (b & 0x8000000000000000ull) ? ~b : (b | 0x8000000000000000ull);
 }
+__device__ __forceinline__ double unorder_key(unsigned long long k) {
+  const unsigned long long b = (k & 0x8000000000000000ull) ? (k & ~0x8000000000000000ull) : ~k;
+  return __longlong_as_double((long long)b);
+}
+__device__ __forceinline__ unsigned fkey_bits(float f) {
+  const unsigned b = __float_as_uint(f);
+  return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
+}
+// Float keys that bracket a double: down(x) <= x <= up(x) in key order.
+__device__ __forceinline__ unsigned fkey_down(double x) { return fkey_bits(__double2float_rd(x)); }
+__device__ __forceinline__ unsigned fkey_up(double x) { return fkey_bits(__double2float_ru(x)); }
 
-// One primitive list sorted along the sweep axis, struct-of-arrays so that a
-// warp scanning consecutive sorted entries issues coalesced loads.
+// One primitive list in (column, min) order, struct-of-arrays for coalesced scans.
 struct SortedBoxes {
-  double* lo;   // min along the sweep axis
-  double* hi;   // max along the sweep axis
-  double* alo;  // min / max along the other two axes
+  double* lo;     // min along the sweep axis
+  double* hi;     // max along the sweep axis
+  double* alo;    // min / max along the first non-sweep axis
   double* ahi;
-  double* blo;
+  double* blo;    // min / max along the second non-sweep axis
   double* bhi;
-  int32_t* id;  // primitive index in the scene
-  int32_t* obj; // object id
+  unsigned* fkey; // fkey_down(lo)
+  int32_t* id;    // primitive index in the scene
+  int32_t* obj;   // object id
+  int32_t* cell;  // column of the box's min corner
+  unsigned* cell_begin;  // [kMaxColumns^2] first entry of each column
+  unsigned* cell_end;    // [kMaxColumns^2] one past its last entry
 };
 
 struct BoxList {
   long long n = 0;
-  double* box = nullptr;                // n x 6 (unsorted, primitive order)
+  double* box = nullptr;  // n x 6 (primitive order)
+  unsigned char* active = nullptr;
   unsigned long long* keys[2] = {nullptr, nullptr};
   unsigned int* vals[2] = {nullptr, nullptr};
   SortedBoxes s{};
 };
 
-// Per-axis statistics for the device-side choice of the sweep axis.
-struct AxisStats {
-  double extent_sum[3];
-  double center_sum[3];
-  double center_sq_sum[3];
-  unsigned long long count;
-  int axis;
-  int pad;
+struct ListStats {
+  unsigned long long active;     // boxes kept
+  unsigned long long ext_max[3]; // bit pattern of the largest extent per axis (non-negative)
+  unsigned long long lo_min[3];  // order_key of the smallest min per axis
+  unsigned long long hi_max[3];  // order_key of the largest max per axis
+};
+
+struct Grid {
+  int axis, a1, a2, g1, g2, pad;
+  double base1, base2, inv1, inv2;  // column = floor((x - base) * inv)
+  double reach1[3], reach2[3];      // per list: the largest extent along a1 / a2
 };
 
 struct BroadScratch {
-  AxisStats stats;
+  double extent_sum[3], center_sum[3], center_sq_sum[3];
+  unsigned long long count;
+  unsigned long long obj_lo[kMaxCullObjects][3];  // order keys of object swept boxes
+  unsigned long long obj_hi[kMaxCullObjects][3];
+  ListStats list[3];  // 0 vertices, 1 faces, 2 edges
+  Grid grid;
   unsigned long long vf_count;
   unsigned long long ee_count;
   unsigned long long error_word;  // bit 0: non-finite coordinate
-  unsigned long long pad[5];
 };
 
 }  // namespace p2c

@@ -54,7 +54,7 @@ struct RecordSink {
 };
 
 template <bool kDonate, bool kCount>
-__global__ void __launch_bounds__(kCertifyThreads, 1)
+__global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
     certify_records_kernel(const unsigned long long* __restrict__ pt, long long n_pt,
                            const unsigned long long* __restrict__ ee, long long n_ee, double T0, double T1,
                            CertParams prm_pt, CertParams prm_ee, p2c_interval_result* out_pt,
@@ -63,16 +63,22 @@ __global__ void __launch_bounds__(kCertifyThreads, 1)
   WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
+  // odd warps take the edge-edge queue first, so that the tail of one
+  // family overlaps the bulk of the other
+  const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
   bool ok = true;
-  if (n_pt > 0) {
-    RecordSrc src{pt, T0, T1};
-    RecordSink sink{pt, out_pt, &scratch->invalid_key[0]};
-    ok = run_warp<1, kDonate, kCount>(src, sink, n_pt, &scratch->queue_head[0], prm_pt, ws, st, t_start);
-  }
-  if (ok && n_ee > 0) {
-    RecordSrc src{ee, T0, T1};
-    RecordSink sink{ee, out_ee, &scratch->invalid_key[1]};
-    ok = run_warp<2, kDonate, kCount>(src, sink, n_ee, &scratch->queue_head[1], prm_ee, ws, st, t_start);
+  for (int pass = 0; pass < 2 && ok; ++pass) {
+    if ((pass == 0) != ee_first) {
+      if (n_pt > 0) {
+        RecordSrc src{pt, T0, T1};
+        RecordSink sink{pt, out_pt, &scratch->invalid_key[0]};
+        ok = run_warp<1, kDonate, kCount>(src, sink, n_pt, &scratch->queue_head[0], prm_pt, ws, st, t_start);
+      }
+    } else if (n_ee > 0) {
+      RecordSrc src{ee, T0, T1};
+      RecordSink sink{ee, out_ee, &scratch->invalid_key[1]};
+      ok = run_warp<2, kDonate, kCount>(src, sink, n_ee, &scratch->queue_head[1], prm_ee, ws, st, t_start);
+    }
   }
   flush_stats(st, ok, scratch);
 }

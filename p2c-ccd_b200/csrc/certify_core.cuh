@@ -200,15 +200,26 @@ struct Geo {
   double p1[12];
 };
 
+// Query geometry held in a warp's shared slot (struct-of-arrays [k][slot]):
+// lanes read their own slot's 24 coordinates per sample instead of keeping
+// them in registers, which halves the engine's register footprint.
+template <class Slots>
+struct SlotGeo {
+  const Slots& ws;
+  int slot;
+  __device__ __forceinline__ double p0(int k) const { return ws.p0[k][slot]; }
+  __device__ __forceinline__ double p1(int k) const { return ws.p1[k][slot]; }
+};
+
 // PositionAt (:67-69) for the 4 vertices, then the family's distance.
-template <int kFamily, class C>
-__device__ __forceinline__ double distance_at(const Geo& g, double t, C& c) {
+template <int kFamily, class G, class C>
+__device__ __forceinline__ double distance_at(const G& g, double t, C& c) {
   V3 x[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const double u = sub(1.0, t);
-    x[i] = vadd(vscale(V3{g.p0[3 * i], g.p0[3 * i + 1], g.p0[3 * i + 2]}, u),
-                vscale(V3{g.p1[3 * i], g.p1[3 * i + 1], g.p1[3 * i + 2]}, t));
+    x[i] = vadd(vscale(V3{g.p0(3 * i), g.p0(3 * i + 1), g.p0(3 * i + 2)}, u),
+                vscale(V3{g.p1(3 * i), g.p1(3 * i + 1), g.p1(3 * i + 2)}, t));
   }
   c.add(40);
   if (kFamily == 1) return dist_point_triangle(x[0], x[1], x[2], x[3], c);
@@ -217,12 +228,12 @@ __device__ __forceinline__ double distance_at(const Geo& g, double t, C& c) {
 
 // Norm(Sub(p1, p0)) of each trajectory: constant per query, hoisted out of
 // MaxDisplacementFromMidpoint (:71-76); the same rounded value either way.
-template <class C>
-__device__ __forceinline__ void motion_norms(const Geo& g, double nrm[4], C& c) {
+template <class G, class C>
+__device__ __forceinline__ void motion_norms(const G& g, double nrm[4], C& c) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
-    const V3 d = vsub(V3{g.p1[3 * i], g.p1[3 * i + 1], g.p1[3 * i + 2]},
-                      V3{g.p0[3 * i], g.p0[3 * i + 1], g.p0[3 * i + 2]});
+    const V3 d = vsub(V3{g.p1(3 * i), g.p1(3 * i + 1), g.p1(3 * i + 2)},
+                      V3{g.p0(3 * i), g.p0(3 * i + 1), g.p0(3 * i + 2)});
     nrm[i] = __dsqrt_rn(vdot(d, d));
   }
   c.add(36);
@@ -372,7 +383,6 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
   unsigned long long path = 0, donated = 0;
   int depth = 0, sub_depth = 0;
   double t0 = 0.0, t1 = 0.0, T0 = 0.0, T1 = 0.0, d1root = 0.0;
-  Geo g;
   double nrm[4];
   Counter ops;
   unsigned free_mask = FULL;
@@ -406,6 +416,7 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
         if (q < n) {
           const int s = nth_set_bit(free_mask, r);
           int bad = 0;
+          Geo g;
           src.load(q, g, T0, T1, bad);
           if (bad != 0) {
             sink.invalid(q, kFamily, bad, T0, T1);
@@ -424,7 +435,7 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
             ws.qidx[s] = q;
             ws.outstanding[s] = 1;
             ws.undecided[s] = 0;
-            motion_norms(g, nrm, ops);
+            motion_norms(SlotGeo<WarpSlots>{ws, s}, nrm, ops);
             phase = 0;
             path = 0ull;
             donated = 0ull;
@@ -468,15 +479,10 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
           __syncwarp();
           if (receiver) {
             slot = rslot;
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-              g.p0[i] = ws.p0[i][slot];
-              g.p1[i] = ws.p1[i][slot];
-            }
             T0 = ws.T0[slot];
             T1 = ws.T1[slot];
             NoCount nc;
-            motion_norms(g, nrm, nc);  // same rounded values as the owner's
+            motion_norms(SlotGeo<WarpSlots>{ws, slot}, nrm, nc);  // same rounded values as the owner's
             path = rpath;
             depth = rdepth;
             sub_depth = rdepth;
@@ -508,7 +514,7 @@ __device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned
     if (active) {
       mid = mul(0.5, add(t0, t1));
       const double t = phase == 0 ? t0 : (phase == 1 ? t1 : mid);
-      d = distance_at<kFamily>(g, t, ops);
+      d = distance_at<kFamily>(SlotGeo<WarpSlots>{ws, slot}, t, ops);
       st.evals += 1;
       // a node is counted once: the root at its first sample, others at their midpoint
       if (phase == 0 || (phase == 2 && depth > 0)) st.nodes += 1;

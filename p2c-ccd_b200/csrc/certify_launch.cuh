@@ -12,6 +12,7 @@ namespace p2c {
 
 constexpr int kCertifyThreads = 128;  // 4 warps per block, one WarpSlots each
 constexpr int kCertifyWarps = kCertifyThreads / 32;
+constexpr int kCertifyMinBlocks = 4;  // 16 warps per SM: caps registers at 128 per thread
 
 // Device scratch of one certification launch (reset by the launcher).
 struct CertifyScratch {

@@ -88,7 +88,7 @@ struct QuerySink {
   }
 };
 
-__global__ void __launch_bounds__(kCertifyThreads, 1)
+__global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
     certify_queries_kernel(const unsigned long long* pt, long long n_pt, const long long* pt_query,
                            const unsigned long long* ee, long long n_ee, const long long* ee_query,
                            const double* q_t0, const double* q_t1, CertParams prm_pt, CertParams prm_ee,
@@ -98,13 +98,18 @@ __global__ void __launch_bounds__(kCertifyThreads, 1)
   WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
+  const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
   bool ok = true;
-  if (n_pt > 0)
-    ok = run_warp<1, true, false>(QuerySrc{pt, pt_query, q_t0, q_t1}, QuerySink<1>{pt, pt_query, out_pt, agg},
-                                  n_pt, &sc->queue_head[0], prm_pt, ws, st, t_start);
-  if (ok && n_ee > 0)
-    ok = run_warp<2, true, false>(QuerySrc{ee, ee_query, q_t0, q_t1}, QuerySink<2>{ee, ee_query, out_ee, agg},
-                                  n_ee, &sc->queue_head[1], prm_ee, ws, st, t_start);
+  for (int pass = 0; pass < 2 && ok; ++pass) {
+    if ((pass == 0) != ee_first) {
+      if (n_pt > 0)
+        ok = run_warp<1, true, false>(QuerySrc{pt, pt_query, q_t0, q_t1}, QuerySink<1>{pt, pt_query, out_pt, agg},
+                                      n_pt, &sc->queue_head[0], prm_pt, ws, st, t_start);
+    } else if (n_ee > 0) {
+      ok = run_warp<2, true, false>(QuerySrc{ee, ee_query, q_t0, q_t1}, QuerySink<2>{ee, ee_query, out_ee, agg},
+                                    n_ee, &sc->queue_head[1], prm_ee, ws, st, t_start);
+    }
+  }
   flush_stats(st, ok, sc);
 }
 

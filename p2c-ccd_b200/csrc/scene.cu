@@ -102,7 +102,7 @@ struct PairSink {
   }
 };
 
-__global__ void __launch_bounds__(kCertifyThreads, 1)
+__global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
     certify_scene_kernel(ScenePairs vf, long long vf_cap, ScenePairs ee, long long ee_cap,
                          const unsigned long long* counts, unsigned family_mask, CertParams prm,
                          p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
@@ -119,19 +119,31 @@ __global__ void __launch_bounds__(kCertifyThreads, 1)
   CertParams p1 = prm, p2 = prm;
   p1.fetch_limit = (int)min(32ll, max(1ll, (n_vf + warps - 1) / warps));
   p2.fetch_limit = (int)min(32ll, max(1ll, (n_ee + warps - 1) / warps));
+  const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
   bool ok = true;
-  if (n_vf > 0)
-    ok = run_warp<1, true, false>(PairSrc<1>{vf}, PairSink<1>{vf.pairs, out_vf, &scratch->agg, uq, uq_cap}, n_vf,
-                                  &scratch->cert.queue_head[0], p1, ws, st, t_start);
-  if (ok && n_ee > 0)
-    ok = run_warp<2, true, false>(PairSrc<2>{ee}, PairSink<2>{ee.pairs, out_ee, &scratch->agg, uq, uq_cap}, n_ee,
-                                  &scratch->cert.queue_head[1], p2, ws, st, t_start);
+  for (int pass = 0; pass < 2 && ok; ++pass) {
+    if ((pass == 0) != ee_first) {
+      if (n_vf > 0)
+        ok = run_warp<1, true, false>(PairSrc<1>{vf}, PairSink<1>{vf.pairs, out_vf, &scratch->agg, uq, uq_cap},
+                                      n_vf, &scratch->cert.queue_head[0], p1, ws, st, t_start);
+    } else if (n_ee > 0) {
+      ok = run_warp<2, true, false>(PairSrc<2>{ee}, PairSink<2>{ee.pairs, out_ee, &scratch->agg, uq, uq_cap}, n_ee,
+                                    &scratch->cert.queue_head[1], p2, ws, st, t_start);
+    }
+  }
   flush_stats(st, ok, &scratch->cert);
   if (threadIdx.x == 0 && blockIdx.x == 0) {
     scratch->agg.n_certified[0] = (unsigned long long)n_vf;
     scratch->agg.n_certified[1] = (unsigned long long)n_ee;
     if (cvf > vf_cap || cee > ee_cap) atomicOr((unsigned long long*)&scratch->cert.stats.error_word, 2ull);
   }
+}
+
+__global__ void init_scene_agg_kernel(SceneAgg* a) {
+  SceneAgg z{};
+  z.coll_key = ~0ull;
+  z.margin_bits = 0x7ff0000000000000ull;  // +inf
+  *a = z;
 }
 
 __device__ __forceinline__ uint8_t refinement_for_reason(uint16_t r) {  // certificate_engine.cpp:279-291
@@ -256,10 +268,7 @@ int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pa
     return fail(P2C_ERR_INVALID, "scene certification workspace too small");
   SceneScratch* sc = reinterpret_cast<SceneScratch*>(ws);
   P2C_CUDA(reset_scratch(&sc->cert, s));
-  P2C_CUDA(cudaMemsetAsync(&sc->agg, 0, sizeof(SceneAgg), s));
-  P2C_CUDA(cudaMemsetAsync(&sc->agg.coll_key, 0xff, sizeof(unsigned long long), s));
-  const unsigned long long inf_bits = 0x7ff0000000000000ull;
-  P2C_CUDA(cudaMemcpyAsync(&sc->agg.margin_bits, &inf_bits, sizeof(inf_bits), cudaMemcpyHostToDevice, s));
+  init_scene_agg_kernel<<<1, 1, 0, s>>>(&sc->agg);
   LaunchShape shape;
   int rc = certify_shape(certify_scene_kernel, &shape);
   if (rc != P2C_OK) return rc;

@@ -24,7 +24,7 @@ class SceneStruct(ctypes.Structure):
     _fields_ = [("v_t0", ctypes.c_void_p), ("v_t1", ctypes.c_void_p), ("faces", ctypes.c_void_p),
                 ("edges", ctypes.c_void_p), ("v_obj", ctypes.c_void_p), ("f_obj", ctypes.c_void_p),
                 ("e_obj", ctypes.c_void_p), ("nv", ctypes.c_int64), ("nf", ctypes.c_int64), ("ne", ctypes.c_int64),
-                ("thickness", ctypes.c_double), ("exclude_self", ctypes.c_int32), ("pad", ctypes.c_int32)]
+                ("thickness", ctypes.c_double), ("exclude_self", ctypes.c_int32), ("n_obj", ctypes.c_int32)]
 
 
 SUMMARY_DTYPE = np.dtype({
@@ -75,6 +75,8 @@ class ScenePipeline:
         self.f_obj = torch.as_tensor(np.ascontiguousarray(scene.f_obj, dtype=np.int32)).to(d)
         self.e_obj = torch.as_tensor(np.ascontiguousarray(scene.e_obj, dtype=np.int32)).to(d)
         self.thickness = float(thickness)
+        self.n_obj = int(max(scene.v_obj.max(initial=-1), scene.f_obj.max(initial=-1),
+                             scene.e_obj.max(initial=-1)) + 1)
         self.exclude_self = bool(exclude_self)
         self.config = config
         self.interval = (float(interval[0]), float(interval[1]))
@@ -98,6 +100,7 @@ class ScenePipeline:
         s.nv, s.nf, s.ne = self.v_t0.shape[0], self.faces.shape[0], self.edges.shape[0]
         s.thickness = self.thickness
         s.exclude_self = 1 if self.exclude_self else 0
+        s.n_obj = self.n_obj
 
     def _alloc(self, vf_cap: int, ee_cap: int):
         d = self.device
@@ -136,6 +139,25 @@ class ScenePipeline:
         """Candidates then certificates, asynchronous on the current stream."""
         self.candidates()
         self.certify()
+
+    def capture(self) -> None:
+        """Capture one step (candidates + certificates, ~60 launches) into a
+        CUDA graph; ``replay`` then costs one graph launch.  Buffers and
+        capacities are fixed at capture time: re-capture after growth."""
+        self.graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self.step()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        with torch.cuda.graph(self.graph):
+            self.step()
+        self._graph_caps = (self.vf_cap, self.ee_cap)
+
+    def replay(self) -> None:
+        if getattr(self, "graph", None) is None or self._graph_caps != (self.vf_cap, self.ee_cap):
+            self.capture()
+        self.graph.replay()
 
     def read_counts(self) -> tuple[int, int, int]:
         c = self.counts.cpu().numpy()
