@@ -13,19 +13,22 @@
 // A one-axis sweep over a surface mesh scans windows of ~sqrt(n) boxes (a
 // whole slice of surface projects onto the axis).  Here the two non-sweep
 // axes are cut into columns at least as wide as the largest box, each box is
-// filed under the column of its min corner, and a box scans only the
-// columns its partners' min corners can lie in (at most 3 x 3).  Steps, all
-// on the caller's stream without host synchronisation:
-//   1. swept boxes (t0 and t1 positions, +thickness), per-axis statistics and
-//      object envelopes;
+// filed under the column of its min corner, and a box scans only the columns
+// its partners' min corners can lie in (at most 3 x 3).  Steps, all on the
+// caller's stream without host synchronisation:
+//   1. swept boxes of every vertex, face and edge (t0 and t1 positions,
+//      +thickness) in one launch, with per-axis statistics and object
+//      envelopes (reduced per warp before the atomics);
 //   2. culling: with self pairs excluded, a primitive outside every other
 //      object's envelope cannot have a candidate (the scene tool's object-pair
 //      permission, PrepareScene :521-545, used as a filter);
 //   3. device-side choice of the sweep axis (smallest mean extent relative to
-//      the spread of centres) and of the column grid;
-//   4. CUB radix sort on a 48-bit key (column << 32 | float(min) rounded
-//      down) and gather into struct-of-arrays;
-//   5. sweeps over float windows rounded outward, exact double tests, and an
+//      the spread of centres), the column grid and a 16-bit quantiser of the
+//      sweep-axis minimum;
+//   4. ONE CUB radix sort of all three lists on a 32-bit key
+//      (list << 30 | column << 16 | quantised minimum; 4 onesweep passes) and
+//      a gather into per-list struct-of-arrays;
+//   5. sweeps over monotone quantised windows with exact double tests and an
 //      ownership rule so that every pair is emitted once; pairs are compacted
 //      per warp with a ballot and appended with one atomic per warp.
 // Overlapping boxes of different objects imply overlapping object envelopes
@@ -42,6 +45,7 @@ namespace p2c {
 namespace {
 
 constexpr int kThreads = 256;
+constexpr unsigned kFull = 0xffffffffu;
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
@@ -50,6 +54,14 @@ inline unsigned grid_for(long long n, int threads) {
   const long long g = (n + threads - 1) / threads;
   return (unsigned)(g > 0 ? g : 1);
 }
+
+struct Lists {
+  long long off[4];  // global index g: list l holds [off[l], off[l + 1])
+  const int32_t* prim[3];
+  const int32_t* obj[3];
+  double* box[3];
+  __device__ __forceinline__ int list_of(long long g) const { return g < off[1] ? 0 : (g < off[2] ? 1 : 2); }
+};
 
 __global__ void init_scratch_kernel(BroadScratch* sc) {
   const int t = threadIdx.x;
@@ -63,71 +75,103 @@ __global__ void init_scratch_kernel(BroadScratch* sc) {
   }
 }
 
-// Swept box of primitive i made of K vertices (K = 1 vertex, 2 edge, 3 face):
-// Extend/Expand/Swept*Box, scene_object_envelope_native_ti_walltime.cpp:256-301.
 template <int K>
+__device__ __forceinline__ bool swept_box(const double* __restrict__ v_t0, const double* __restrict__ v_t1,
+                                          const int32_t* __restrict__ prim, long long i, double thickness,
+                                          double b[6]) {
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const long long v = K == 1 ? i : (long long)__ldg(prim + K * i + k);
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      const double* p = (f == 0 ? v_t0 : v_t1) + 3 * v;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double x = __ldg(p + a);
+        finite = finite && isfinite(x);
+        mn[a] = dmin(mn[a], x);
+        mx[a] = dmax(mx[a], x);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {  // Expand(box, thickness), :263-270
+    b[a] = __dsub_rn(mn[a], thickness);
+    b[3 + a] = __dadd_rn(mx[a], thickness);
+  }
+  return finite;
+}
+
+// Swept boxes of all primitives (Extend/Expand/Swept*Box,
+// scene_object_envelope_native_ti_walltime.cpp:256-301) in one launch.
 __global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restrict__ v_t0,
-                                                         const double* __restrict__ v_t1,
-                                                         const int32_t* __restrict__ prim, long long n,
-                                                         double thickness, const int32_t* __restrict__ v_obj,
-                                                         int cull_objects, double* __restrict__ box,
-                                                         BroadScratch* sc) {
+                                                         const double* __restrict__ v_t1, Lists L,
+                                                         double thickness, int cull_objects, BroadScratch* sc) {
   __shared__ double red[9][kThreads / 32];
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  unsigned long long cnt = 0;
-  if (i < n) {
-    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-    bool finite = true;
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int lane = threadIdx.x & 31;
+  double b[6] = {0, 0, 0, 0, 0, 0};
+  bool live = g < L.off[3];
+  int l = 0, o = -1;
+  if (live) {
+    l = L.list_of(g);
+    const long long i = g - L.off[l];
+    const bool finite = l == 0 ? swept_box<1>(v_t0, v_t1, nullptr, i, thickness, b)
+                        : l == 1 ? swept_box<3>(v_t0, v_t1, L.prim[1], i, thickness, b)
+                                 : swept_box<2>(v_t0, v_t1, L.prim[2], i, thickness, b);
+    double* dst = L.box[l] + 6 * i;
 #pragma unroll
-    for (int k = 0; k < K; ++k) {
-      const long long v = K == 1 ? i : (long long)__ldg(prim + K * i + k);
+    for (int k = 0; k < 6; ++k) dst[k] = b[k];
+    if (!finite) atomicOr(&sc->error_word, 1ull);
+    if (l == 0) o = L.obj[0][i];
+  }
+  // object envelopes = union of each object's vertex boxes; one atomic per
+  // object per warp
+  if (cull_objects > 0) {
+    const bool mine0 = live && l == 0 && o >= 0 && o < cull_objects;
+    unsigned remaining = __ballot_sync(kFull, mine0);
+    while (remaining) {
+      const int leader = __ffs((int)remaining) - 1;
+      const int lo_obj = __shfl_sync(kFull, o, leader);
+      const bool mine = mine0 && o == lo_obj;
+      remaining &= ~__ballot_sync(kFull, mine);
 #pragma unroll
-      for (int f = 0; f < 2; ++f) {
-        const double* p = (f == 0 ? v_t0 : v_t1) + 3 * v;
+      for (int a = 0; a < 3; ++a) {
+        unsigned long long kmin = mine ? order_key(b[a]) : ~0ull;
+        unsigned long long kmax = mine ? order_key(b[3 + a]) : 0ull;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          const double x = __ldg(p + a);
-          finite = finite && isfinite(x);
-          mn[a] = dmin(mn[a], x);
-          mx[a] = dmax(mx[a], x);
+        for (int s = 16; s > 0; s >>= 1) {
+          kmin = min(kmin, __shfl_xor_sync(kFull, kmin, s));
+          kmax = max(kmax, __shfl_xor_sync(kFull, kmax, s));
+        }
+        if (lane == leader) {
+          atomicMin(&sc->obj_lo[lo_obj][a], kmin);
+          atomicMax(&sc->obj_hi[lo_obj][a], kmax);
         }
       }
     }
-    double* b = box + 6 * i;
+  }
+  // axis statistics (sums of extents, centres, squared centres)
+  double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (live) {
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      b[a] = __dsub_rn(mn[a], thickness);
-      b[3 + a] = __dadd_rn(mx[a], thickness);
       const double c = 0.5 * (b[3 + a] + b[a]);
       vals[a] = b[3 + a] - b[a];
       vals[3 + a] = c;
       vals[6 + a] = c * c;
-    }
-    cnt = 1;
-    if (!finite) atomicOr(&sc->error_word, 1ull);
-    // object envelopes: the union of the object's vertex boxes
-    if (K == 1 && cull_objects > 0) {
-      const int o = v_obj[i];
-      if (o >= 0 && o < cull_objects) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-          atomicMin(&sc->obj_lo[o][a], order_key(b[a]));
-          atomicMax(&sc->obj_hi[o][a], order_key(b[3 + a]));
-        }
-      }
     }
   }
 #pragma unroll
   for (int k = 0; k < 9; ++k) {
     double v = vals[k];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_down_sync(kFull, v, s);
+    if (lane == 0) red[k][threadIdx.x >> 5] = v;
   }
-  unsigned long long c = cnt;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) c += __shfl_down_sync(0xffffffffu, c, o);
+  const unsigned cnt = __popc(__ballot_sync(kFull, live));
   __syncthreads();
   if (threadIdx.x < 9) {
     double s = 0.0;
@@ -137,24 +181,25 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restric
                                     : &sc->center_sq_sum[threadIdx.x - 6];
     atomicAdd(dst, s);
   }
-  if ((threadIdx.x & 31) == 0 && c) atomicAdd(&sc->count, c);
+  if (lane == 0 && cnt) atomicAdd(&sc->count, (unsigned long long)cnt);
 }
 
 // Keep a box unless it is a vertex in no face or (self pairs excluded) it
-// lies outside every other object's envelope.  Per-list extents of the kept
-// boxes size the column grid.
-__global__ void __launch_bounds__(kThreads) classify_kernel(int list, const double* __restrict__ box, long long n,
-                                                            const int32_t* __restrict__ obj, int vertex_list,
-                                                            int cull_objects, unsigned char* __restrict__ active,
-                                                            BroadScratch* sc) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+// lies outside every other object's envelope.  The kept boxes' extents per
+// list size the column grid.
+__global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_objects,
+                                                            unsigned char* __restrict__ active, BroadScratch* sc) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool keep = false;
+  int l = 3;
   double b[6] = {0, 0, 0, 0, 0, 0};
-  if (i < n) {
-    const int o = obj[i];
-    keep = !(vertex_list && o < 0);
+  if (g < L.off[3]) {
+    l = L.list_of(g);
+    const long long i = g - L.off[l];
+    const int o = L.obj[l][i];
+    keep = !(l == 0 && o < 0);
 #pragma unroll
-    for (int k = 0; k < 6; ++k) b[k] = box[6 * i + k];
+    for (int k = 0; k < 6; ++k) b[k] = L.box[l][6 * i + k];
     if (keep && cull_objects > 0) {
       bool near_other = false;
       for (int q = 0; q < cull_objects && !near_other; ++q) {
@@ -169,31 +214,39 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(int list, const doub
       }
       keep = near_other;
     }
-    active[i] = keep ? 1 : 0;
+    active[g] = keep ? 1 : 0;
   }
-  ListStats& L = sc->list[list];
-  const unsigned mask = __ballot_sync(0xffffffffu, keep);
-  if ((threadIdx.x & 31) == 0 && mask) atomicAdd(&L.active, (unsigned long long)__popc(mask));
+  // per-list reductions; most warps hold one list only
+  const int l0 = __shfl_sync(kFull, l, 0);
+  const bool uniform = __all_sync(kFull, l == l0);
+  for (int ll = 0; ll < 3; ++ll) {
+    if (uniform && ll != l0) continue;
+    const bool mine = keep && l == ll;
+    const unsigned mask = __ballot_sync(kFull, mine);
+    if (mask == 0u) continue;
+    ListStats& S = sc->list[ll];
+    if ((threadIdx.x & 31) == 0) atomicAdd(&S.active, (unsigned long long)__popc(mask));
 #pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    unsigned long long ext = keep ? (unsigned long long)__double_as_longlong(b[3 + a] - b[a]) : 0ull;
-    unsigned long long lo = keep ? order_key(b[a]) : ~0ull;
-    unsigned long long hi = keep ? order_key(b[3 + a]) : 0ull;
+    for (int a = 0; a < 3; ++a) {
+      unsigned long long ext = mine ? (unsigned long long)__double_as_longlong(b[3 + a] - b[a]) : 0ull;
+      unsigned long long lo = mine ? order_key(b[a]) : ~0ull;
+      unsigned long long hi = mine ? order_key(b[3 + a]) : 0ull;
 #pragma unroll
-    for (int s = 16; s > 0; s >>= 1) {
-      ext = max(ext, __shfl_down_sync(0xffffffffu, ext, s));
-      lo = min(lo, __shfl_down_sync(0xffffffffu, lo, s));
-      hi = max(hi, __shfl_down_sync(0xffffffffu, hi, s));
-    }
-    if ((threadIdx.x & 31) == 0 && mask) {
-      atomicMax(&L.ext_max[a], ext);
-      atomicMin(&L.lo_min[a], lo);
-      atomicMax(&L.hi_max[a], hi);
+      for (int s = 16; s > 0; s >>= 1) {
+        ext = max(ext, __shfl_xor_sync(kFull, ext, s));
+        lo = min(lo, __shfl_xor_sync(kFull, lo, s));
+        hi = max(hi, __shfl_xor_sync(kFull, hi, s));
+      }
+      if ((threadIdx.x & 31) == 0) {
+        atomicMax(&S.ext_max[a], ext);
+        atomicMin(&S.lo_min[a], lo);
+        atomicMax(&S.hi_max[a], hi);
+      }
     }
   }
 }
 
-// Sweep axis and column grid (one thread).
+// Sweep axis, column grid, sweep-axis quantiser and list segments (one thread).
 __global__ void grid_kernel(BroadScratch* sc) {
   const double n = sc->count > 0 ? (double)sc->count : 1.0;
   int axis = 0;
@@ -212,31 +265,31 @@ __global__ void grid_kernel(BroadScratch* sc) {
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
   g.pad = 0;
-  const int ax[2] = {g.a1, g.a2};
-  double base[2], inv[2];
-  int cols[2];
-  for (int k = 0; k < 2; ++k) {
+  const int ax[3] = {g.a1, g.a2, axis};
+  double base[3], inv[3];
+  int cols[2] = {1, 1};
+  for (int k = 0; k < 3; ++k) {
     double lo = INFINITY, hi = -INFINITY, reach = 0.0;
     for (int l = 0; l < 3; ++l) {
       const ListStats& L = sc->list[l];
-      if (L.active == 0) {
-        (k == 0 ? g.reach1 : g.reach2)[l] = 0.0;
-        continue;
-      }
+      const double r = L.active ? __longlong_as_double((long long)L.ext_max[ax[k]]) : 0.0;
+      if (k < 2) (k == 0 ? g.reach1 : g.reach2)[l] = r;
+      if (L.active == 0) continue;
       lo = fmin(lo, unorder_key(L.lo_min[ax[k]]));
       hi = fmax(hi, unorder_key(L.hi_max[ax[k]]));
-      const double r = __longlong_as_double((long long)L.ext_max[ax[k]]);
-      (k == 0 ? g.reach1 : g.reach2)[l] = r;
       reach = fmax(reach, r);
     }
     const double range = (hi > lo) ? hi - lo : 0.0;
-    double width = fmax(reach, range / kMaxColumns);
-    if (!(width > 0.0) || !isfinite(width)) width = 1.0;
-    int c = (int)fmin((double)kMaxColumns, floor(range / width) + 1.0);
-    if (c < 1) c = 1;
     base[k] = isfinite(lo) ? lo : 0.0;
-    inv[k] = 1.0 / width;
-    cols[k] = c;
+    if (k < 2) {
+      double width = fmax(reach, range / kMaxColumns);
+      if (!(width > 0.0) || !isfinite(width)) width = 1.0;
+      int c = (int)fmin((double)kMaxColumns, floor(range / width) + 1.0);
+      cols[k] = c < 1 ? 1 : c;
+      inv[k] = 1.0 / width;
+    } else {
+      inv[k] = (range > 0.0 && isfinite(range)) ? (double)kQMax / range : 0.0;
+    }
   }
   g.base1 = base[0];
   g.base2 = base[1];
@@ -244,6 +297,12 @@ __global__ void grid_kernel(BroadScratch* sc) {
   g.inv2 = inv[1];
   g.g1 = cols[0];
   g.g2 = cols[1];
+  g.base0 = base[2];
+  g.scale0 = inv[2];
+  g.seg[0] = 0;
+  g.seg[1] = sc->list[0].active;
+  g.seg[2] = g.seg[1] + sc->list[1].active;
+  g.seg[3] = g.seg[2] + sc->list[2].active;
   sc->grid = g;
 }
 
@@ -252,61 +311,68 @@ __device__ __forceinline__ int column(double x, double base, double inv, int g) 
   return c < 0.0 ? 0 : (c >= (double)g ? g - 1 : (int)c);
 }
 
-__global__ void __launch_bounds__(kThreads) keys_kernel(const double* __restrict__ box, long long n,
-                                                        const unsigned char* __restrict__ active,
-                                                        unsigned long long* __restrict__ keys,
-                                                        unsigned int* __restrict__ vals, const BroadScratch* sc) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Grid& g = sc->grid;
-  unsigned long long key = ~0ull;
-  if (active[i]) {
-    const double* b = box + 6 * i;
-    const int c = column(b[g.a1], g.base1, g.inv1, g.g1) * g.g2 + column(b[g.a2], g.base2, g.inv2, g.g2);
-    key = ((unsigned long long)(unsigned)c << 32) | fkey_down(b[g.axis]);
-  }
-  keys[i] = key;
-  vals[i] = (unsigned int)i;
+// Monotone (non-decreasing) in x: the sweep windows rely on it.
+__device__ __forceinline__ unsigned quantise(double x, const Grid& g) {
+  const double c = floor((x - g.base0) * g.scale0);
+  return c < 0.0 ? 0u : (c >= (double)kQMax ? kQMax : (unsigned)c);
 }
 
-// Sorted entries to struct-of-arrays plus the column ranges.
-__global__ void __launch_bounds__(kThreads) gather_kernel(const double* __restrict__ box,
-                                                          const unsigned long long* __restrict__ keys,
-                                                          const unsigned int* __restrict__ order, int list,
-                                                          const int32_t* __restrict__ obj, SortedBoxes s,
-                                                          const BroadScratch* sc) {
-  const long long n = (long long)sc->list[list].active;
+__global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned char* __restrict__ active,
+                                                        unsigned* __restrict__ keys, unsigned* __restrict__ vals,
+                                                        const BroadScratch* sc) {
+  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= L.off[3]) return;
+  const Grid& G = sc->grid;
+  unsigned key = ~0u;
+  if (active[g]) {
+    const int l = L.list_of(g);
+    const double* b = L.box[l] + 6 * (g - L.off[l]);
+    const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
+                                  column(b[G.a2], G.base2, G.inv2, G.g2));
+    key = ((unsigned)l << 30) | (c << kQBits) | quantise(b[G.axis], G);
+  }
+  keys[g] = key;
+  vals[g] = (unsigned)g;
+}
+
+// Sorted entries into per-list struct-of-arrays plus the column ranges.
+__global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigned* __restrict__ keys,
+                                                          const unsigned* __restrict__ order, SortedBoxes s0,
+                                                          SortedBoxes s1, SortedBoxes s2, const BroadScratch* sc) {
+  const Grid& G = sc->grid;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
-  const Grid& g = sc->grid;
-  const unsigned long long key = keys[i];
-  const unsigned j = order[i];
-  const double* b = box + 6 * (long long)j;
-  s.lo[i] = b[g.axis];
-  s.hi[i] = b[3 + g.axis];
-  s.alo[i] = b[g.a1];
-  s.ahi[i] = b[3 + g.a1];
-  s.blo[i] = b[g.a2];
-  s.bhi[i] = b[3 + g.a2];
-  s.fkey[i] = (unsigned)(key & 0xffffffffull);
-  s.id[i] = (int32_t)j;
-  s.obj[i] = obj[j];
-  const int cell = (int)(key >> 32);
-  s.cell[i] = cell;
-  if (i == 0 || (int)(keys[i - 1] >> 32) != cell) s.cell_begin[cell] = (unsigned)i;
-  if (i == n - 1 || (int)(keys[i + 1] >> 32) != cell) s.cell_end[cell] = (unsigned)(i + 1);
+  if (i >= (long long)G.seg[3]) return;
+  const unsigned key = keys[i];
+  const int l = (int)(key >> 30);
+  const SortedBoxes s = l == 0 ? s0 : (l == 1 ? s1 : s2);
+  const long long k = i - (long long)G.seg[l];
+  const long long j = (long long)order[i] - L.off[l];
+  const double* b = L.box[l] + 6 * j;
+  s.lo[k] = b[G.axis];
+  s.hi[k] = b[3 + G.axis];
+  s.alo[k] = b[G.a1];
+  s.ahi[k] = b[3 + G.a1];
+  s.blo[k] = b[G.a2];
+  s.bhi[k] = b[3 + G.a2];
+  s.q[k] = key & kQMax;
+  s.id[k] = (int32_t)j;
+  s.obj[k] = L.obj[l][j];
+  const unsigned head = key >> kQBits;  // list and column
+  const unsigned cell = head & ((1u << kCellBits) - 1u);
+  if (i == (long long)G.seg[l] || (keys[i - 1] >> kQBits) != head) s.cell_begin[cell] = (unsigned)k;
+  if (i + 1 == (long long)G.seg[l + 1] || (keys[i + 1] >> kQBits) != head) s.cell_end[cell] = (unsigned)(k + 1);
 }
 
 // Warp-aggregated append of the pairs found by this iteration.
 __device__ __forceinline__ void append_pair(bool found, unsigned long long key, unsigned long long* out,
                                             unsigned long long cap, unsigned long long* count) {
-  const unsigned mask = __ballot_sync(0xffffffffu, found);
+  const unsigned mask = __ballot_sync(kFull, found);
   if (mask == 0u) return;
   const int lane = threadIdx.x & 31;
   const int leader = __ffs((int)mask) - 1;
   unsigned long long base = 0;
   if (lane == leader) base = atomicAdd(count, (unsigned long long)__popc(mask));
-  base = __shfl_sync(0xffffffffu, base, leader);
+  base = __shfl_sync(kFull, base, leader);
   if (found) {
     const unsigned long long slot = base + (unsigned long long)__popc(mask & ((1u << lane) - 1u));
     if (slot < cap) out[slot] = key;
@@ -314,13 +380,13 @@ __device__ __forceinline__ void append_pair(bool found, unsigned long long key, 
 }
 
 // Walk over the candidate entries of one scanning box: the columns its
-// partners' min corners can lie in, and in each the float window
-// [fkey_down(lo), fkey_up(hi)] of the partner list.
+// partners' min corners can lie in, and in each the quantised window
+// [q(lo), q(hi)] of the partner list.
 struct Walker {
   int c1, c1_end, c2_begin, c2, c2_end;
-  unsigned j, j_end, fk_hi;
+  unsigned j, j_end, q_lo, q_hi;
 
-  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g, unsigned fk_lo) {
+  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g) {
     for (;;) {
       if (++c2 > c2_end) {
         c2 = c2_begin;
@@ -328,21 +394,21 @@ struct Walker {
       }
       const int cell = c1 * g.g2 + c2;
       unsigned b = Q.cell_begin[cell], e = Q.cell_end[cell];
-      // lower bound of fk_lo in [b, e)
-      while (b < e) {
+      const unsigned end = e;
+      while (b < e) {  // first entry with q >= q_lo
         const unsigned m = (b + e) >> 1;
-        if (Q.fkey[m] < fk_lo) b = m + 1;
+        if (Q.q[m] < q_lo) b = m + 1;
         else e = m;
       }
       j = b;
-      j_end = Q.cell_end[cell];
-      if (j < j_end && Q.fkey[j] <= fk_hi) return true;
+      j_end = end;
+      if (j < j_end && Q.q[j] <= q_hi) return true;
     }
   }
 };
 
-__device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double alo, double ahi, double blo,
-                                            double bhi, double reach1, double reach2, double hi) {
+__device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double lo, double hi, double alo, double ahi,
+                                            double blo, double bhi, double reach1, double reach2) {
   // widen the lower columns by a relative 2^-40 so that the rounding of
   // alo - reach can never skip the column of a partner's min corner
   const double l1 = alo - reach1 - (fabs(alo) + reach1) * 0x1p-40;
@@ -353,7 +419,8 @@ __device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double alo
   w.c2_end = column(bhi, g.base2, g.inv2, g.g2);
   w.c2 = w.c2_begin - 1;
   w.j = w.j_end = 0;
-  w.fk_hi = fkey_up(hi);
+  w.q_lo = quantise(lo, g);
+  w.q_hi = quantise(hi, g);
 }
 
 __device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, const SortedBoxes& Q, long long j) {
@@ -361,37 +428,39 @@ __device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, cons
          P.blo[i] <= Q.bhi[j] && Q.blo[j] <= P.bhi[i];
 }
 
+__device__ __forceinline__ unsigned long long pair_key(unsigned a, unsigned b, int pack_shift) {
+  return pack_shift > 0 ? (((unsigned long long)a << pack_shift) | b) : (((unsigned long long)a << 32) | b);
+}
+
 // Vertex-face pairs: threads [0, nv) scan faces from a vertex and own the
 // pairs whose face minimum is >= the vertex minimum; threads [nv, nv + nf)
-// scan vertices from a face and own the others.  Keys (vertex << 32 | face).
+// scan vertices from a face and own the others.  Keys (vertex, face).
 __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
                                                             const int32_t* __restrict__ faces, int exclude_self,
-                                                            unsigned long long* out, unsigned long long cap,
-                                                            BroadScratch* sc) {
-  const long long nv = (long long)sc->list[0].active, nf = (long long)sc->list[1].active;
+                                                            int pack_shift, unsigned long long* out,
+                                                            unsigned long long cap, BroadScratch* sc) {
+  const Grid& g = sc->grid;
+  const long long nv = (long long)(g.seg[1] - g.seg[0]), nf = (long long)(g.seg[2] - g.seg[1]);
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((long long)blockIdx.x * blockDim.x >= nv + nf) return;  // whole warp beyond the work
+  if ((long long)blockIdx.x * blockDim.x >= nv + nf) return;  // whole block beyond the work
   const bool from_vertex = t < nv;
   const long long i = from_vertex ? t : t - nv;
-  bool live = from_vertex ? true : (i < nf);
+  bool live = from_vertex || i < nf;
   const SortedBoxes P = from_vertex ? V : F;
   const SortedBoxes Q = from_vertex ? F : V;
-  const Grid& g = sc->grid;
   Walker w;
   double lo = 0.0;
   int32_t pid = 0, pobj = 0;
-  unsigned fk_lo = 0;
   if (live) {
     lo = P.lo[i];
     pid = P.id[i];
     pobj = P.obj[i];
-    fk_lo = P.fkey[i];
-    walker_init(w, g, P.alo[i], P.ahi[i], P.blo[i], P.bhi[i], from_vertex ? g.reach1[1] : g.reach1[0],
-                from_vertex ? g.reach2[1] : g.reach2[0], P.hi[i]);
-    live = w.next_cell(Q, g, fk_lo);
+    walker_init(w, g, lo, P.hi[i], P.alo[i], P.ahi[i], P.blo[i], P.bhi[i], from_vertex ? g.reach1[1] : g.reach1[0],
+                from_vertex ? g.reach2[1] : g.reach2[0]);
+    live = w.next_cell(Q, g);
   }
   for (;;) {
-    if (!__any_sync(0xffffffffu, live)) break;
+    if (!__any_sync(kFull, live)) break;
     bool found = false;
     unsigned long long key = 0;
     if (live) {
@@ -412,43 +481,40 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
         }
         if (ok) {
           found = true;
-          key = ((unsigned long long)(unsigned)vtx << 32) | (unsigned)fc;
+          key = pair_key((unsigned)vtx, (unsigned)fc, pack_shift);
         }
       }
       ++w.j;
-      if (w.j >= w.j_end || Q.fkey[w.j] > w.fk_hi) live = w.next_cell(Q, g, fk_lo);
+      if (w.j >= w.j_end || Q.q[w.j] > w.q_hi) live = w.next_cell(Q, g);
     }
     append_pair(found, key, out, cap, &sc->vf_count);
   }
 }
 
 // Edge-edge pairs: each edge scans its own list and owns the pairs whose
-// partner minimum is larger (ties: larger edge index).
-// Keys (min edge << 32 | max edge).
+// partner minimum is larger (ties: larger edge index).  Keys (lower, higher).
 __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
-                                                            int exclude_self, unsigned long long* out,
+                                                            int exclude_self, int pack_shift, unsigned long long* out,
                                                             unsigned long long cap, BroadScratch* sc) {
-  const long long ne = (long long)sc->list[2].active;
+  const Grid& g = sc->grid;
+  const long long ne = (long long)(g.seg[3] - g.seg[2]);
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if ((long long)blockIdx.x * blockDim.x >= ne) return;
   bool live = i < ne;
-  const Grid& g = sc->grid;
   Walker w;
   double lo = 0.0;
   int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
-  unsigned fk_lo = 0;
   if (live) {
     lo = E.lo[i];
     eid = E.id[i];
     eobj = E.obj[i];
-    fk_lo = E.fkey[i];
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
-    walker_init(w, g, E.alo[i], E.ahi[i], E.blo[i], E.bhi[i], g.reach1[2], g.reach2[2], E.hi[i]);
-    live = w.next_cell(E, g, fk_lo);
+    walker_init(w, g, lo, E.hi[i], E.alo[i], E.ahi[i], E.blo[i], E.bhi[i], g.reach1[2], g.reach2[2]);
+    live = w.next_cell(E, g);
   }
   for (;;) {
-    if (!__any_sync(0xffffffffu, live)) break;
+    if (!__any_sync(kFull, live)) break;
     bool found = false;
     unsigned long long key = 0;
     if (live) {
@@ -467,12 +533,11 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
         }
         if (ok) {
           found = true;
-          const unsigned l = (unsigned)min(eid, oid), h = (unsigned)max(eid, oid);
-          key = ((unsigned long long)l << 32) | h;
+          key = pair_key((unsigned)min(eid, oid), (unsigned)max(eid, oid), pack_shift);
         }
       }
       ++w.j;
-      if (w.j >= w.j_end || E.fkey[w.j] > w.fk_hi) live = w.next_cell(E, g, fk_lo);
+      if (w.j >= w.j_end || E.q[w.j] > w.q_hi) live = w.next_cell(E, g);
     }
     append_pair(found, key, out, cap, &sc->ee_count);
   }
@@ -483,13 +548,21 @@ __global__ void fill_u64_kernel(unsigned long long* p, long long n, unsigned lon
   if (i < n) p[i] = v;
 }
 
+// Packed (a << shift | b) keys back to (a << 32 | b); padding stays ~0.
+__global__ void unpack_pairs_kernel(unsigned long long* p, long long n, int shift) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const unsigned long long k = p[i];
+  if (k == ~0ull) return;
+  p[i] = ((k >> shift) << 32) | (k & ((1ull << shift) - 1ull));
+}
+
 __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long* counts) {
   counts[0] = sc->vf_count;
   counts[1] = sc->ee_count;
   counts[2] = sc->error_word;
   counts[3] = (unsigned long long)sc->grid.axis | ((unsigned long long)sc->grid.g1 << 8) |
-              ((unsigned long long)sc->grid.g2 << 24) | (sc->list[0].active + sc->list[1].active + sc->list[2].active)
-                                                            << 40;
+              ((unsigned long long)sc->grid.g2 << 24) | (sc->grid.seg[3] << 40);
 }
 
 // ---- workspace carving -----------------------------------------------------
@@ -506,10 +579,10 @@ struct Carver {
   }
 };
 
-size_t sort_pairs_temp_bytes(long long n) {
+size_t sort_entries_temp_bytes(long long n) {
   size_t bytes = 0;
-  cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
-  cub::DoubleBuffer<unsigned int> v(nullptr, nullptr);
+  cub::DoubleBuffer<unsigned> k(nullptr, nullptr);
+  cub::DoubleBuffer<unsigned> v(nullptr, nullptr);
   cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)(n > 0 ? n : 1));
   return bytes;
 }
@@ -521,52 +594,54 @@ size_t sort_keys_temp_bytes(long long n) {
   return bytes;
 }
 
+constexpr long long kCells = (long long)kMaxColumns * kMaxColumns;
+
 struct Layout {
   BroadScratch* sc;
-  BoxList L[3];  // vertices, faces, edges
-  unsigned* cells;  // 3 lists x (begin, end) x kMaxColumns^2
+  BoxList B[3];  // vertices, faces, edges
+  unsigned char* active;
+  unsigned* keys[2];
+  unsigned* vals[2];
+  unsigned* cells;  // 3 lists x (begin, end) x kCells
   void* sort_tmp;
   size_t sort_tmp_bytes;
   unsigned long long* pair_alt;
   size_t total;
 };
 
-constexpr long long kCells = (long long)kMaxColumns * kMaxColumns;
-
 void carve_list(Carver& c, BoxList& L, long long n) {
   L.n = n;
   L.box = c.take<double>(6 * n);
-  L.active = c.take<unsigned char>(n);
-  L.keys[0] = c.take<unsigned long long>(n);
-  L.keys[1] = c.take<unsigned long long>(n);
-  L.vals[0] = c.take<unsigned int>(n);
-  L.vals[1] = c.take<unsigned int>(n);
   L.s.lo = c.take<double>(n);
   L.s.hi = c.take<double>(n);
   L.s.alo = c.take<double>(n);
   L.s.ahi = c.take<double>(n);
   L.s.blo = c.take<double>(n);
   L.s.bhi = c.take<double>(n);
-  L.s.fkey = c.take<unsigned>(n);
+  L.s.q = c.take<unsigned>(n);
   L.s.id = c.take<int32_t>(n);
   L.s.obj = c.take<int32_t>(n);
-  L.s.cell = c.take<int32_t>(n);
 }
 
 Layout carve(void* base, long long nv, long long nf, long long ne, long long pair_cap, bool dry) {
   Carver c{static_cast<char*>(base), 0, dry};
   Layout L;
+  const long long n = nv + nf + ne;
   L.sc = c.take<BroadScratch>(1);
-  carve_list(c, L.L[0], nv);
-  carve_list(c, L.L[1], nf);
-  carve_list(c, L.L[2], ne);
+  carve_list(c, L.B[0], nv);
+  carve_list(c, L.B[1], nf);
+  carve_list(c, L.B[2], ne);
+  L.active = c.take<unsigned char>(n);
+  L.keys[0] = c.take<unsigned>(n);
+  L.keys[1] = c.take<unsigned>(n);
+  L.vals[0] = c.take<unsigned>(n);
+  L.vals[1] = c.take<unsigned>(n);
   L.cells = c.take<unsigned>(6 * kCells);
   for (int l = 0; l < 3; ++l) {
-    L.L[l].s.cell_begin = dry ? nullptr : L.cells + (2 * l) * kCells;
-    L.L[l].s.cell_end = dry ? nullptr : L.cells + (2 * l + 1) * kCells;
+    L.B[l].s.cell_begin = dry ? nullptr : L.cells + (2 * l) * kCells;
+    L.B[l].s.cell_end = dry ? nullptr : L.cells + (2 * l + 1) * kCells;
   }
-  const long long nmax = std::max(nv, std::max(nf, ne));
-  L.sort_tmp_bytes = std::max(sort_pairs_temp_bytes(nmax), sort_keys_temp_bytes(pair_cap));
+  L.sort_tmp_bytes = std::max(sort_entries_temp_bytes(n), sort_keys_temp_bytes(pair_cap));
   L.sort_tmp = c.take<char>((long long)L.sort_tmp_bytes);
   L.pair_alt = c.take<unsigned long long>(pair_cap);
   L.total = c.off + 256;
@@ -582,27 +657,11 @@ int bit_length(long long x) {
   return b;
 }
 
-int sort_list(BoxList& L, const Layout& lay, cudaStream_t s) {
-  if (L.n == 0) return P2C_OK;
-  cub::DoubleBuffer<unsigned long long> k(L.keys[0], L.keys[1]);
-  cub::DoubleBuffer<unsigned int> v(L.vals[0], L.vals[1]);
-  size_t tb = lay.sort_tmp_bytes;
-  // key = column (16 bits) << 32 | float key; inactive entries are ~0 and sort last
-  P2C_CUDA(cub::DeviceRadixSort::SortPairs(lay.sort_tmp, tb, k, v, (int)L.n, 0, 32 + kCellBits, s));
-  if (k.Current() != L.keys[0]) {
-    std::swap(L.keys[0], L.keys[1]);
-    std::swap(L.vals[0], L.vals[1]);
-  }
-  return P2C_OK;
-}
-
-int sort_pairs(unsigned long long* pairs, long long cap, long long first_count, const Layout& lay, cudaStream_t s) {
+int sort_pairs(unsigned long long* pairs, long long cap, int key_bits, const Layout& lay, cudaStream_t s) {
   if (cap <= 1) return P2C_OK;
   cub::DoubleBuffer<unsigned long long> k(pairs, lay.pair_alt);
   size_t tb = lay.sort_tmp_bytes;
-  // keys are (first << 32 | second) with first < first_count; padding is ~0
-  const int end_bit = std::min(64, 32 + bit_length(first_count) + 1);
-  P2C_CUDA(cub::DeviceRadixSort::SortKeys(lay.sort_tmp, tb, k, (int)cap, 0, end_bit, s));
+  P2C_CUDA(cub::DeviceRadixSort::SortKeys(lay.sort_tmp, tb, k, (int)cap, 0, key_bits, s));
   if (k.Current() != pairs)
     P2C_CUDA(cudaMemcpyAsync(pairs, k.Current(), sizeof(unsigned long long) * cap, cudaMemcpyDeviceToDevice, s));
   return P2C_OK;
@@ -613,8 +672,7 @@ int sort_pairs(unsigned long long* pairs, long long cap, long long first_count, 
 int validate_scene(const p2c_scene* sc) {
   if (sc == nullptr) return fail(P2C_ERR_INVALID, "scene pointer is null");
   if (sc->nv < 0 || sc->nf < 0 || sc->ne < 0) return fail(P2C_ERR_INVALID, "scene counts must be non-negative");
-  if (sc->nv >= (1ll << 31) || sc->nf >= (1ll << 31) || sc->ne >= (1ll << 31))
-    return fail(P2C_ERR_INVALID, "scene counts must stay below 2^31");
+  if (sc->nv + sc->nf + sc->ne >= (1ll << 31)) return fail(P2C_ERR_INVALID, "scene primitive count must stay below 2^31");
   if (!(sc->thickness >= 0.0) || !std::isfinite(sc->thickness))
     return fail(P2C_ERR_INVALID, "scene thickness must be finite and non-negative");
   if (sc->n_obj < 0) return fail(P2C_ERR_INVALID, "scene n_obj must be non-negative");
@@ -641,52 +699,61 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   if (ws == nullptr || ws_bytes < need)
     return fail(P2C_ERR_INVALID, "candidate workspace too small: %zu < %zu bytes", ws_bytes, need);
   Layout L = carve(ws, scene.nv, scene.nf, scene.ne, pair_cap, false);
+  const long long n = scene.nv + scene.nf + scene.ne;
   const int cull = (scene.exclude_self && scene.n_obj >= 1 && scene.n_obj <= kMaxCullObjects) ? scene.n_obj : 0;
+  Lists lists;
+  lists.off[0] = 0;
+  lists.off[1] = scene.nv;
+  lists.off[2] = scene.nv + scene.nf;
+  lists.off[3] = n;
+  lists.prim[0] = nullptr;
+  lists.prim[1] = scene.faces;
+  lists.prim[2] = scene.edges;
+  lists.obj[0] = scene.v_obj;
+  lists.obj[1] = scene.f_obj;
+  lists.obj[2] = scene.e_obj;
+  for (int l = 0; l < 3; ++l) lists.box[l] = L.B[l].box;
   P2C_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(BroadScratch), s));
   P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
   init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
-  if (scene.nv > 0)
-    boxes_kernel<1><<<grid_for(scene.nv, kThreads), kThreads, 0, s>>>(
-        scene.v_t0, scene.v_t1, nullptr, scene.nv, scene.thickness, scene.v_obj, cull, L.L[0].box, L.sc);
-  if (scene.nf > 0)
-    boxes_kernel<3><<<grid_for(scene.nf, kThreads), kThreads, 0, s>>>(
-        scene.v_t0, scene.v_t1, scene.faces, scene.nf, scene.thickness, nullptr, 0, L.L[1].box, L.sc);
-  if (scene.ne > 0)
-    boxes_kernel<2><<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(
-        scene.v_t0, scene.v_t1, scene.edges, scene.ne, scene.thickness, nullptr, 0, L.L[2].box, L.sc);
-  P2C_CUDA(cudaGetLastError());
-  const int32_t* objs[3] = {scene.v_obj, scene.f_obj, scene.e_obj};
-  for (int l = 0; l < 3; ++l) {
-    if (L.L[l].n == 0) continue;
-    classify_kernel<<<grid_for(L.L[l].n, kThreads), kThreads, 0, s>>>(l, L.L[l].box, L.L[l].n, objs[l], l == 0,
-                                                                      cull, L.L[l].active, L.sc);
+  if (n > 0) {
+    boxes_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(scene.v_t0, scene.v_t1, lists, scene.thickness, cull,
+                                                            L.sc);
+    classify_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, cull, L.active, L.sc);
   }
   grid_kernel<<<1, 1, 0, s>>>(L.sc);
   P2C_CUDA(cudaGetLastError());
-  for (int l = 0; l < 3; ++l) {
-    BoxList& B = L.L[l];
-    if (B.n == 0) continue;
-    keys_kernel<<<grid_for(B.n, kThreads), kThreads, 0, s>>>(B.box, B.n, B.active, B.keys[0], B.vals[0], L.sc);
+  if (n > 0) {
+    keys_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, L.active, L.keys[0], L.vals[0], L.sc);
     P2C_CUDA(cudaGetLastError());
-    int rc = sort_list(B, L, s);
-    if (rc != P2C_OK) return rc;
-    gather_kernel<<<grid_for(B.n, kThreads), kThreads, 0, s>>>(B.box, B.keys[0], B.vals[0], l, objs[l], B.s, L.sc);
+    cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
+    cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
+    size_t tb = L.sort_tmp_bytes;
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, 32, s));
+    gather_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, k.Current(), v.Current(), L.B[0].s, L.B[1].s,
+                                                             L.B[2].s, L.sc);
     P2C_CUDA(cudaGetLastError());
   }
+  // with sorting, pairs are emitted packed so that the sort touches fewer bits
+  const int vf_shift = sort_out ? std::max(1, bit_length(scene.nf)) : 0;
+  const int ee_shift = sort_out ? std::max(1, bit_length(scene.ne)) : 0;
   if (sort_out && vf_cap > 0) fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
   if (sort_out && ee_cap > 0) fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
   if (scene.nv + scene.nf > 0 && vf_out != nullptr)
     sweep_vf_kernel<<<grid_for(scene.nv + scene.nf, kThreads), kThreads, 0, s>>>(
-        L.L[0].s, L.L[1].s, scene.faces, scene.exclude_self, vf_out, (unsigned long long)vf_cap, L.sc);
+        L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out, (unsigned long long)vf_cap, L.sc);
   if (scene.ne > 0 && ee_out != nullptr)
-    sweep_ee_kernel<<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(L.L[2].s, scene.edges, scene.exclude_self,
-                                                                      ee_out, (unsigned long long)ee_cap, L.sc);
+    sweep_ee_kernel<<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(L.B[2].s, scene.edges, scene.exclude_self,
+                                                                      ee_shift, ee_out, (unsigned long long)ee_cap,
+                                                                      L.sc);
   P2C_CUDA(cudaGetLastError());
   if (sort_out) {
-    int rc = sort_pairs(vf_out, vf_cap, scene.nv, L, s);
+    int rc = sort_pairs(vf_out, vf_cap, bit_length(scene.nv) + vf_shift, L, s);
     if (rc != P2C_OK) return rc;
-    rc = sort_pairs(ee_out, ee_cap, scene.ne, L, s);
+    rc = sort_pairs(ee_out, ee_cap, bit_length(scene.ne) + ee_shift, L, s);
     if (rc != P2C_OK) return rc;
+    if (vf_cap > 0) unpack_pairs_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, vf_shift);
+    if (ee_cap > 0) unpack_pairs_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ee_shift);
   }
   export_counts_kernel<<<1, 1, 0, s>>>(L.sc, counts_dev);
   P2C_CUDA(cudaGetLastError());

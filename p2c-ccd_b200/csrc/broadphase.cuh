@@ -10,8 +10,10 @@
 namespace p2c {
 
 constexpr int kMaxCullObjects = 64;  // object-envelope culling up to this many objects
-constexpr int kMaxColumns = 256;     // columns per non-sweep axis (cell id < 2^16)
-constexpr int kCellBits = 16;
+constexpr int kMaxColumns = 128;     // columns per non-sweep axis (cell id < 2^14)
+constexpr int kCellBits = 14;
+constexpr int kQBits = 16;           // quantised sweep-axis minimum
+constexpr unsigned kQMax = (1u << kQBits) - 1u;
 
 // Order-preserving maps to unsigned integers (radix-sortable keys).
 __device__ __forceinline__ unsigned long long order_key(double x) {
@@ -38,10 +40,9 @@ struct SortedBoxes {
   double* ahi;
   double* blo;    // min / max along the second non-sweep axis
   double* bhi;
-  unsigned* fkey; // fkey_down(lo)
+  unsigned* q;    // quantised min along the sweep axis (the sort key's low bits)
   int32_t* id;    // primitive index in the scene
   int32_t* obj;   // object id
-  int32_t* cell;  // column of the box's min corner
   unsigned* cell_begin;  // [kMaxColumns^2] first entry of each column
   unsigned* cell_end;    // [kMaxColumns^2] one past its last entry
 };
@@ -49,9 +50,6 @@ struct SortedBoxes {
 struct BoxList {
   long long n = 0;
   double* box = nullptr;  // n x 6 (primitive order)
-  unsigned char* active = nullptr;
-  unsigned long long* keys[2] = {nullptr, nullptr};
-  unsigned int* vals[2] = {nullptr, nullptr};
   SortedBoxes s{};
 };
 
@@ -65,7 +63,9 @@ struct ListStats {
 struct Grid {
   int axis, a1, a2, g1, g2, pad;
   double base1, base2, inv1, inv2;  // column = floor((x - base) * inv)
+  double base0, scale0;             // quantiser of the sweep axis: floor((x - base0) * scale0)
   double reach1[3], reach2[3];      // per list: the largest extent along a1 / a2
+  unsigned long long seg[4];        // list l's sorted entries are [seg[l], seg[l + 1])
 };
 
 struct BroadScratch {
