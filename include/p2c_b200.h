@@ -220,6 +220,28 @@ int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const in
                         void* workspace_dev, size_t workspace_bytes,
                         p2c_certify_stats* stats_dev, void* stream);
 
+/* Work queues for callers that cannot allocate device memory — code running
+ * while a CUDA graph is captured, frame loops that forbid allocation, hosts that
+ * own all device memory under a fixed budget.  No counterpart in the reference.
+ * Same arguments and results as p2c_certify_queries without the workspace: the
+ * scratch is a 1 MiB file-scope device array that every GPU loading this library
+ * holds until exit, so at most P2C_STATIC_QUEUE_MAX_QUERIES work items per call
+ * (larger queues return P2C_ERR_INVALID).  The first call on a device resolves
+ * the array's device address (cudaGetSymbolAddress); make that first call before
+ * any stream capture.  Each call clears the scratch it uses before reading it,
+ * but all calls on a device share the one array: calls that overlap on the GPU
+ * (different streams, or host threads without ordering) race and must not be
+ * issued.  It calls no cudaMalloc, cudaFree or allocating library routine. */
+#define P2C_STATIC_QUEUE_MAX_QUERIES 26000
+int p2c_certify_queries_static(const p2c_point_triangle* pt_dev, int64_t n_pt, const int64_t* pt_query_dev,
+                               const p2c_edge_edge* ee_dev, int64_t n_ee, const int64_t* ee_query_dev,
+                               int64_t n_queries, const int64_t* pt_offsets_dev, const int64_t* ee_offsets_dev,
+                               const double* q_t0_dev, const double* q_t1_dev, const uint32_t* q_mask_dev,
+                               const p2c_cert_config* config,
+                               p2c_interval_result* pt_results_dev, p2c_interval_result* ee_results_dev,
+                               p2c_query_certificate* certs_dev,
+                               p2c_certify_stats* stats_dev, void* stream);
+
 /* ---- scenes: swept-AABB candidates and their certificates ----------------- */
 /* A scene: vertex trajectories over one step plus topology, all device arrays.
  * Objects are connected components (the scene tool's DSU objects,

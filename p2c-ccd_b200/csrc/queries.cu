@@ -13,6 +13,8 @@
 // makes the query an InvalidInput error (Evaluate returns the status, and the
 // work queue turns it into an undecided InvalidInput certificate, :629-632);
 // otherwise any undecided makes it undecided, else separation.
+#include <mutex>
+
 #include "certify_core.cuh"
 #include "certify_launch.cuh"
 
@@ -258,3 +260,66 @@ int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const in
 }
 
 }  // extern "C"
+
+// ---- work queues without allocation ----------------------------------------
+// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
+// being captured, physics or rendering loops that forbid allocation inside a
+// frame, and host frameworks that own all device memory under a fixed budget.
+// For them p2c_certify_queries_static keeps its scratch (the launch counters
+// and one reduction record per work item) in the file-scope array below
+// instead of a caller-provided workspace.
+namespace p2c {
+namespace {
+
+constexpr size_t kStaticQueueScratchBytes = 1u << 20;  // 1 MiB per device, held until exit
+static __device__ __align__(256) unsigned char g_static_queue_scratch[kStaticQueueScratchBytes];
+static_assert(P2C_STATIC_QUEUE_MAX_QUERIES > 0, "capacity must be positive");
+
+std::mutex g_static_mu;
+void* g_static_ptr[64] = {};
+
+// Device address of the array on the current device, resolved once per
+// device (the array's host-side name is only a stand-in for it).
+int static_queue_scratch(void** out) {
+  int dev = 0;
+  P2C_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) return fail(P2C_ERR_CUDA, "device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(g_static_mu);
+  if (g_static_ptr[dev] == nullptr) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_static_queue_scratch);
+    if (e != cudaSuccess) return fail(P2C_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    g_static_ptr[dev] = p;
+  }
+  *out = g_static_ptr[dev];
+  return P2C_OK;
+}
+
+}  // namespace
+}  // namespace p2c
+
+extern "C" int p2c_certify_queries_static(const p2c_point_triangle* pt_dev, int64_t n_pt, const int64_t* pt_query_dev,
+                                          const p2c_edge_edge* ee_dev, int64_t n_ee, const int64_t* ee_query_dev,
+                                          int64_t n_queries, const int64_t* pt_offsets_dev,
+                                          const int64_t* ee_offsets_dev, const double* q_t0_dev,
+                                          const double* q_t1_dev, const uint32_t* q_mask_dev,
+                                          const p2c_cert_config* config, p2c_interval_result* pt_results_dev,
+                                          p2c_interval_result* ee_results_dev, p2c_query_certificate* certs_dev,
+                                          p2c_certify_stats* stats_dev, void* stream) {
+  if (n_queries > P2C_STATIC_QUEUE_MAX_QUERIES)
+    return p2c::fail(P2C_ERR_INVALID,
+                     "p2c_certify_queries_static takes at most %d work items per call (got %lld); split the queue "
+                     "or use p2c_certify_queries with a workspace",
+                     P2C_STATIC_QUEUE_MAX_QUERIES, (long long)n_queries);
+  if (p2c::queries_workspace_bytes(n_queries) > p2c::kStaticQueueScratchBytes)
+    return p2c::fail(P2C_ERR_INVALID, "static scratch too small for %lld work items", (long long)n_queries);
+  void* scratch = nullptr;
+  const int rc = p2c::static_queue_scratch(&scratch);
+  if (rc != P2C_OK) return rc;
+  // the existing entry point clears the counters and the per-item records
+  // it needs at the start of every call
+  return p2c_certify_queries(pt_dev, n_pt, pt_query_dev, ee_dev, n_ee, ee_query_dev, n_queries, pt_offsets_dev,
+                             ee_offsets_dev, q_t0_dev, q_t1_dev, q_mask_dev, config, pt_results_dev, ee_results_dev,
+                             certs_dev, scratch, p2c::kStaticQueueScratchBytes, stats_dev, stream);
+}
+

@@ -53,6 +53,10 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_certify_queries": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _i64, _c_void_p, _i64, _c_void_p,
                                    _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.POINTER(CertConfig),
                                    _c_void_p, _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
+    "p2c_certify_queries_static": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p, _i64, _c_void_p, _i64,
+                                          _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                          ctypes.POINTER(CertConfig), _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                          _c_void_p]),
     "p2c_scene_candidates_workspace_bytes": (_size, [_i64, _i64, _i64, _i64, _i64]),
     "p2c_scene_candidates": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _i64, _c_void_p, _int, _c_void_p,
                                     _size, _c_void_p]),
