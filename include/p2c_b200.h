@@ -126,6 +126,8 @@ typedef struct p2c_certify_stats {
   uint64_t donations;                      /* subtrees handed between lanes of a warp */
   uint64_t queries;                        /* queries certified */
   uint64_t error_word;                     /* nonzero if a bounded wait or a capacity check failed */
+  uint64_t max_warp_iterations;            /* longest warp loop (one distance sample per lane per iteration) */
+  uint64_t busy_lane_iterations;           /* sum over iterations of lanes holding work */
 } p2c_certify_stats;
 
 /* ---- library ------------------------------------------------------------ */

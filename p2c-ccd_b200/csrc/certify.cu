@@ -29,57 +29,42 @@ __device__ __forceinline__ void load_record(const unsigned long long* __restrict
   bad = (ida < 0 || idb < 0) ? 1 : (finite ? 0 : 2);
 }
 
-struct RecordSrc {
-  const unsigned long long* recs;  // 30 words per record
+// Both families of a batch of 240-byte records over one interval.
+struct RecordProblem {
+  const unsigned long long* recs[2];  // 30 words per record
+  long long count[2];
+  p2c_interval_result* out[2];
+  unsigned long long* invalid_key;    // [2]: min over (index << 2 | reason)
   double T0, T1;
-  __device__ __forceinline__ void load(long long q, Geo& g, double& t0, double& t1, int& bad) const {
-    load_record(recs + 30 * q, g, bad);
+  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
+    load_record(recs[f - 1] + 30 * q, g, bad);
     t0 = T0;
     t1 = T1;
   }
-};
-
-struct RecordSink {
-  const unsigned long long* recs;
-  p2c_interval_result* out;
-  unsigned long long* invalid_key;  // min over (index << 2 | reason)
-  __device__ __forceinline__ void finish(long long q, int family, const Outcome& o) const {
-    store_interval_result(out + q, family, o, (long long)recs[30 * q], (long long)recs[30 * q + 1]);
+  __device__ __forceinline__ void finish(int f, long long q, const Outcome& o) const {
+    const unsigned long long* r = recs[f - 1] + 30 * q;
+    store_interval_result(out[f - 1] + q, f, o, (long long)r[0], (long long)r[1]);
   }
-  __device__ __forceinline__ void invalid(long long q, int family, int bad, double T0, double T1) const {
-    Outcome o{3, T0, T1, T1, 0.0};
-    store_interval_result(out + q, family, o, -1, -1);
-    atomicMin(invalid_key, ((unsigned long long)q << 2) | (unsigned long long)bad);
+  __device__ __forceinline__ void invalid(int f, long long q, int bad, double t0, double t1) const {
+    Outcome o{3, t0, t1, t1, 0.0};
+    store_interval_result(out[f - 1] + q, f, o, -1, -1);
+    atomicMin(&invalid_key[f - 1], ((unsigned long long)q << 2) | (unsigned long long)bad);
   }
 };
 
-template <bool kDonate, bool kCount>
+template <bool kShare, bool kCount>
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    certify_records_kernel(const unsigned long long* __restrict__ pt, long long n_pt,
-                           const unsigned long long* __restrict__ ee, long long n_ee, double T0, double T1,
-                           CertParams prm_pt, CertParams prm_ee, p2c_interval_result* out_pt,
-                           p2c_interval_result* out_ee, CertifyScratch* scratch) {
+    certify_records_kernel(RecordProblem prob, CertParams prm_pt, CertParams prm_ee, CertifyScratch* scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
+  EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
-  // odd warps take the edge-edge queue first, so that the tail of one
-  // family overlaps the bulk of the other
+  // odd warps take the edge-edge queue first, so that the tail of one family
+  // overlaps the bulk of the other
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  bool ok = true;
-  for (int pass = 0; pass < 2 && ok; ++pass) {
-    if ((pass == 0) != ee_first) {
-      if (n_pt > 0) {
-        RecordSrc src{pt, T0, T1};
-        RecordSink sink{pt, out_pt, &scratch->invalid_key[0]};
-        ok = run_warp<1, kDonate, kCount>(src, sink, n_pt, &scratch->queue_head[0], prm_pt, ws, st, t_start);
-      }
-    } else if (n_ee > 0) {
-      RecordSrc src{ee, T0, T1};
-      RecordSink sink{ee, out_ee, &scratch->invalid_key[1]};
-      ok = run_warp<2, kDonate, kCount>(src, sink, n_ee, &scratch->queue_head[1], prm_ee, ws, st, t_start);
-    }
-  }
+  const bool ok = run_engine<kShare, kShare, kCount>(prob, prm_pt, prm_ee, ee_first, sh, st, &scratch->engine,
+                                                     pools_at(scratch), t_start);
   flush_stats(st, ok, scratch);
 }
 
@@ -91,11 +76,11 @@ int launch_certify_records(const void* pt, long long n_pt, const void* ee, long 
                            double T1, const p2c_cert_config& cfg, p2c_interval_result* out_pt,
                            p2c_interval_result* out_ee, void* scratch, size_t scratch_bytes, bool census,
                            cudaStream_t stream) {
-  if (scratch_bytes < sizeof(CertifyScratch))
+  if (scratch_bytes < kScratchHeaderBytes + kPoolBytes)
     return fail(P2C_ERR_INVALID, "certification workspace too small: %zu < %zu bytes", scratch_bytes,
-                sizeof(CertifyScratch));
+                kScratchHeaderBytes + kPoolBytes);
   CertifyScratch* sc = reinterpret_cast<CertifyScratch*>(scratch);
-  P2C_CUDA(reset_scratch(sc, stream));
+  P2C_CUDA(reset_scratch(sc, stream, !census));
   if (n_pt + n_ee == 0) return P2C_OK;
   LaunchShape shape;
   int rc = census ? certify_shape(certify_records_kernel<false, true>, &shape)
@@ -103,14 +88,20 @@ int launch_certify_records(const void* pt, long long n_pt, const void* ee, long 
   if (rc != P2C_OK) return rc;
   const CertParams ppt = make_params(cfg, shape, n_pt);
   const CertParams pee = make_params(cfg, shape, n_ee);
-  const auto* a = reinterpret_cast<const unsigned long long*>(pt);
-  const auto* b = reinterpret_cast<const unsigned long long*>(ee);
+  RecordProblem prob;
+  prob.recs[0] = reinterpret_cast<const unsigned long long*>(pt);
+  prob.recs[1] = reinterpret_cast<const unsigned long long*>(ee);
+  prob.count[0] = n_pt;
+  prob.count[1] = n_ee;
+  prob.out[0] = out_pt;
+  prob.out[1] = out_ee;
+  prob.invalid_key = sc->invalid_key;
+  prob.T0 = T0;
+  prob.T1 = T1;
   if (census) {
-    certify_records_kernel<false, true><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
-        a, n_pt, b, n_ee, T0, T1, ppt, pee, out_pt, out_ee, sc);
+    certify_records_kernel<false, true><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(prob, ppt, pee, sc);
   } else {
-    certify_records_kernel<true, false><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
-        a, n_pt, b, n_ee, T0, T1, ppt, pee, out_pt, out_ee, sc);
+    certify_records_kernel<true, false><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(prob, ppt, pee, sc);
   }
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;
@@ -141,7 +132,8 @@ int certify_host(const void* prims, int64_t n, int family, double t0, double t1,
   std::lock_guard<std::mutex> lock(g_host_buffers.mu);
   const size_t in_bytes = (size_t)n * 240u, out_bytes = (size_t)n * sizeof(p2c_interval_result);
   const size_t ws_off = (in_bytes + out_bytes + 255u) & ~size_t(255);
-  rc = ensure_buffer(g_host_buffers, ws_off + sizeof(CertifyScratch));
+  const size_t ws_bytes = kScratchHeaderBytes + kPoolBytes;
+  rc = ensure_buffer(g_host_buffers, ws_off + ws_bytes);
   if (rc != P2C_OK) return rc;
   char* base = static_cast<char*>(g_host_buffers.dev);
   void* d_in = base;
@@ -149,10 +141,10 @@ int certify_host(const void* prims, int64_t n, int family, double t0, double t1,
   void* d_ws = base + ws_off;
   cudaStream_t s = nullptr;
   P2C_CUDA(cudaMemcpyAsync(d_in, prims, in_bytes, cudaMemcpyHostToDevice, s));
-  rc = family == 1 ? launch_certify_records(d_in, n, nullptr, 0, t0, t1, *cfg, d_out, nullptr, d_ws,
-                                            sizeof(CertifyScratch), false, s)
-                   : launch_certify_records(nullptr, 0, d_in, n, t0, t1, *cfg, nullptr, d_out, d_ws,
-                                            sizeof(CertifyScratch), false, s);
+  rc = family == 1 ? launch_certify_records(d_in, n, nullptr, 0, t0, t1, *cfg, d_out, nullptr, d_ws, ws_bytes,
+                                            false, s)
+                   : launch_certify_records(nullptr, 0, d_in, n, t0, t1, *cfg, nullptr, d_out, d_ws, ws_bytes,
+                                            false, s);
   if (rc != P2C_OK) return rc;
   P2C_CUDA(cudaMemcpyAsync(results, d_out, out_bytes, cudaMemcpyDeviceToHost, s));
   CertifyScratch host_sc;
@@ -166,8 +158,8 @@ int certify_host(const void* prims, int64_t n, int family, double t0, double t1,
 extern "C" {
 
 size_t p2c_certify_workspace_bytes(int64_t n) {
-  (void)n;
-  return sizeof(CertifyScratch);
+  (void)n;  // the scratch does not grow with the batch
+  return kScratchHeaderBytes + kPoolBytes;
 }
 
 int p2c_certify_pt_batch(const p2c_point_triangle* prims_dev, int64_t n, double interval_t0, double interval_t1,

@@ -336,21 +336,20 @@ struct CertParams {
 };
 
 // Per-warp shared state: 32 query slots, struct-of-arrays so that lanes
-// reading their own slot hit distinct banks.
+// reading their own slot hit distinct banks.  A slot caches one query's
+// geometry for the lanes of this warp that work on it; the query's reduction
+// lives in global memory (QueryAgg) so that other warps can share its tree.
 struct WarpSlots {
   double p0[12][32];
   double p1[12][32];
   double T0[32], T1[32];
-  double coll_t0[32], coll_t1[32], coll_toi[32];
-  unsigned long long coll_key[32];
-  unsigned long long margin_bits[32];
+  unsigned long long coll_key[32];  // this warp's view of the leftmost collision (pruning)
   long long qidx[32];
-  int outstanding[32];
-  int undecided[32];
+  int family[32];
 };
 
 struct WarpStats {
-  unsigned long long nodes = 0, evals = 0, donations = 0, queries = 0, ops = 0;
+  unsigned long long nodes = 0, evals = 0, donations = 0, queries = 0, ops = 0, iters = 0, busy = 0;
 };
 
 // Position of the (r+1)-th set bit of m (r counts from 0); m has > r set bits.
@@ -363,264 +362,6 @@ __device__ __forceinline__ unsigned long long global_ns() {
   unsigned long long t;
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
-}
-
-// The warp engine.  Src provides load(q, Geo&, T0&, T1&, bad&) (bad: 0 valid,
-// 1 negative id, 2 non-finite coordinate); Sink provides finish(q, family,
-// Outcome) and invalid(q, family, bad, T0, T1).  Returns false if the time budget
-// ran out (the caller raises the error word).
-template <int kFamily, bool kDonate, bool kCount, class Src, class Sink>
-__device__ bool run_warp(const Src& src, const Sink& sink, long long n, unsigned long long* counter,
-                         const CertParams& prm, WarpSlots& ws, WarpStats& st,
-                         unsigned long long t_start) {
-  using Counter = typename std::conditional<kCount, OpCount, NoCount>::type;
-  const unsigned FULL = 0xffffffffu;
-  const int lane = threadIdx.x & 31;
-  const unsigned lt_mask = (1u << lane) - 1u;
-
-  int slot = -1;
-  int phase = 0;
-  unsigned long long path = 0, donated = 0;
-  int depth = 0, sub_depth = 0;
-  double t0 = 0.0, t1 = 0.0, T0 = 0.0, T1 = 0.0, d1root = 0.0;
-  double nrm[4];
-  Counter ops;
-  unsigned free_mask = FULL;
-  bool exhausted = false;
-  bool ok = true;
-
-  for (unsigned iter = 0;; ++iter) {
-    if ((iter & 63u) == 0u && prm.budget_ns != 0ull) {
-      int over = 0;
-      if (lane == 0) over = (global_ns() - t_start) > prm.budget_ns;
-      if (__shfl_sync(FULL, over, 0)) {
-        ok = false;
-        break;
-      }
-    }
-    // (A) idle lanes fetch new queries from the global queue; a warp keeps at
-    // most fetch_limit queries in flight so that, on small batches, the other
-    // lanes bisect those queries instead of idling.
-    unsigned idle = __ballot_sync(FULL, slot < 0);
-    const int room = prm.fetch_limit - (32 - __popc(free_mask));
-    if (idle != 0u && !exhausted && room > 0) {
-      const int k = min(__popc(idle), room);
-      unsigned long long base = 0;
-      if (lane == 0) base = atomicAdd(counter, (unsigned long long)k);
-      base = __shfl_sync(FULL, base, 0);
-      if ((long long)base + k >= n) exhausted = true;
-      bool fresh = false;
-      const int r = __popc(idle & lt_mask);
-      if (slot < 0 && r < k) {
-        const long long q = (long long)base + r;
-        if (q < n) {
-          const int s = nth_set_bit(free_mask, r);
-          int bad = 0;
-          Geo g;
-          src.load(q, g, T0, T1, bad);
-          if (bad != 0) {
-            sink.invalid(q, kFamily, bad, T0, T1);
-          } else {
-            slot = s;
-            fresh = true;
-#pragma unroll
-            for (int i = 0; i < 12; ++i) {
-              ws.p0[i][s] = g.p0[i];
-              ws.p1[i][s] = g.p1[i];
-            }
-            ws.T0[s] = T0;
-            ws.T1[s] = T1;
-            ws.coll_key[s] = ~0ull;
-            ws.margin_bits[s] = 0x7ff0000000000000ull;  // +inf
-            ws.qidx[s] = q;
-            ws.outstanding[s] = 1;
-            ws.undecided[s] = 0;
-            motion_norms(SlotGeo<WarpSlots>{ws, s}, nrm, ops);
-            phase = 0;
-            path = 0ull;
-            donated = 0ull;
-            depth = 0;
-            sub_depth = 0;
-            t0 = T0;
-            t1 = T1;
-            st.queries += 1;
-          }
-        }
-      }
-      free_mask &= ~__reduce_or_sync(FULL, fresh ? (1u << slot) : 0u);
-      __syncwarp();
-    }
-    // (B) donation: idle lanes take the shallowest pending subtree of a busy lane
-    if (kDonate) {
-      idle = __ballot_sync(FULL, slot < 0);
-      if (idle != 0u) {
-        const unsigned long long pend =
-            (slot >= 0 && phase == 2) ? pending_levels(path, donated, depth, sub_depth) : 0ull;
-        const unsigned donors = __ballot_sync(FULL, pend != 0ull);
-        const int npair = min(__popc(idle), __popc(donors));
-        if (npair > 0) {
-          unsigned long long gpath = 0ull;
-          int gdepth = 0, gslot = -1;
-          if (((donors >> lane) & 1u) && __popc(donors & lt_mask) < npair) {
-            const int b = 63 - __clzll((long long)pend);
-            const int l = 64 - b;
-            donated |= (1ull << b);
-            gpath = (path & top_bits(l - 1)) | (1ull << b);
-            gdepth = l;
-            gslot = slot;
-            atomicAdd(&ws.outstanding[slot], 1);
-            st.donations += 1;
-          }
-          const bool receiver = ((idle >> lane) & 1u) && __popc(idle & lt_mask) < npair;
-          const int src_lane = receiver ? nth_set_bit(donors, __popc(idle & lt_mask)) : lane;
-          const unsigned long long rpath = __shfl_sync(FULL, gpath, src_lane);
-          const int rdepth = __shfl_sync(FULL, gdepth, src_lane);
-          const int rslot = __shfl_sync(FULL, gslot, src_lane);
-          __syncwarp();
-          if (receiver) {
-            slot = rslot;
-            T0 = ws.T0[slot];
-            T1 = ws.T1[slot];
-            NoCount nc;
-            motion_norms(SlotGeo<WarpSlots>{ws, slot}, nrm, nc);  // same rounded values as the owner's
-            path = rpath;
-            depth = rdepth;
-            sub_depth = rdepth;
-            donated = 0ull;
-            phase = 2;
-            double a, b;
-            replay(T0, T1, path, depth - 1, a, b);
-            t0 = mul(0.5, add(a, b));
-            t1 = b;
-          }
-        }
-      }
-    }
-    const unsigned busy = __ballot_sync(FULL, slot >= 0);
-    if (busy == 0u) {
-      if (exhausted) break;
-      continue;
-    }
-    // (C) prune: a node right of a known collision leaf of its query is not
-    // needed (depth-first order would return before reaching it), and neither
-    // is anything after it in this lane's subtree.
-    bool done_lane = false;
-    if (slot >= 0 && phase == 2 && depth > 0 && ws.coll_key[slot] < path) done_lane = true;
-    const bool active = slot >= 0 && !done_lane;
-
-    // (D) one distance sample per active lane
-    double d = 0.0;
-    double mid = 0.0;
-    if (active) {
-      mid = mul(0.5, add(t0, t1));
-      const double t = phase == 0 ? t0 : (phase == 1 ? t1 : mid);
-      d = distance_at<kFamily>(SlotGeo<WarpSlots>{ws, slot}, t, ops);
-      st.evals += 1;
-      // a node is counted once: the root at its first sample, others at their midpoint
-      if (phase == 0 || (phase == 2 && depth > 0)) st.nodes += 1;
-      if (kCount) ops.add(phase == 2 ? 2 : 0);
-    }
-    // (E) classify.  leaf: 0 none, 1 collision, 2 separation, 3 undecided
-    int leaf = 0;
-    double toi = 0.0, margin = 0.0;
-    if (active) {
-      if (phase == 0) {
-        if (d <= prm.eps_space) {
-          leaf = 1;
-          toi = t0;
-        } else {
-          phase = 1;
-        }
-      } else if (phase == 1) {
-        d1root = d;
-        phase = 2;
-      } else {
-        if (d <= prm.eps_space) {
-          leaf = 1;
-          toi = mid;
-        } else if (depth == 0 && d1root <= prm.eps_space) {
-          leaf = 1;
-          toi = t1;
-        } else {
-          const double lb = sub(d, motion_radius<kFamily>(nrm, t0, t1, ops));
-          if (kCount) ops.add(1);
-          if (lb > prm.eps_space) {
-            leaf = 2;
-            margin = max_std(0.0, sub(lb, prm.eps_space));
-            if (kCount) ops.add(1);
-          } else if (depth >= prm.max_depth || sub(t1, t0) <= prm.eps_time) {
-            leaf = 3;
-          } else {
-            depth += 1;  // descend into the left child (its path bit stays 0)
-            t1 = mid;
-          }
-        }
-      }
-    }
-    // (F) reduce leaves into the query's slot
-    if (leaf == 1) atomicMin(&ws.coll_key[slot], path);
-    if (leaf == 2) atomicMin(&ws.margin_bits[slot], (unsigned long long)__double_as_longlong(margin));
-    if (leaf == 3) ws.undecided[slot] = 1;
-    __syncwarp();
-    if (leaf == 1 && ws.coll_key[slot] == path) {
-      ws.coll_t0[slot] = t0;
-      ws.coll_t1[slot] = t1;
-      ws.coll_toi[slot] = toi;
-    }
-    __syncwarp();
-    // (G) after a leaf, move to the deepest pending right sibling
-    if (leaf != 0) {
-      const unsigned long long pend = pending_levels(path, donated, depth, sub_depth);
-      if (pend == 0ull) {
-        done_lane = true;
-      } else {
-        const int b = __ffsll((long long)pend) - 1;
-        const int l = 64 - b;
-        path = (path & top_bits(l - 1)) | (1ull << b);
-        donated &= top_bits(l - 1);
-        double a, bb;
-        replay(T0, T1, path, l - 1, a, bb);
-        t0 = mul(0.5, add(a, bb));
-        t1 = bb;
-        depth = l;
-        phase = 2;
-      }
-    }
-    unsigned freed = 0u;
-    if (done_lane) {
-      const int old = atomicSub(&ws.outstanding[slot], 1);
-      if (old == 1) {
-        Outcome o;
-        const double RT0 = ws.T0[slot], RT1 = ws.T1[slot];
-        if (ws.coll_key[slot] != ~0ull) {
-          o.status = P2C_STATUS_COLLISION;
-          o.t0 = ws.coll_t0[slot];
-          o.t1 = ws.coll_t1[slot];
-          o.toi = ws.coll_toi[slot];
-          o.margin = 0.0;
-        } else if (ws.undecided[slot]) {
-          o.status = P2C_STATUS_UNDECIDED;
-          o.t0 = RT0;
-          o.t1 = RT1;
-          o.toi = RT1;
-          o.margin = 0.0;
-        } else {
-          o.status = P2C_STATUS_SEPARATION;
-          o.t0 = RT0;
-          o.t1 = RT1;
-          o.toi = RT1;
-          o.margin = __longlong_as_double((long long)ws.margin_bits[slot]);
-        }
-        sink.finish(ws.qidx[slot], kFamily, o);
-        freed = 1u << slot;
-      }
-      slot = -1;
-    }
-    free_mask |= __reduce_or_sync(FULL, freed);
-    __syncwarp();
-  }
-  if (kCount) st.ops += ops.n;
-  return ok;
 }
 
 }  // namespace p2c

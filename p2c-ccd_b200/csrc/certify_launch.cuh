@@ -6,6 +6,7 @@
 #include <cstring>
 
 #include "certify_core.cuh"
+#include "certify_engine.cuh"
 #include "p2c_internal.cuh"
 
 namespace p2c {
@@ -17,20 +18,41 @@ constexpr int kCertifyMinBlocks = 4;  // 16 warps per SM: caps registers at 128 
 // Device scratch of one certification launch (reset by the launcher).
 struct CertifyScratch {
   p2c_certify_stats stats;             // exported verbatim to the caller
-  unsigned long long queue_head[4];    // per-family query queue heads
   unsigned long long invalid_key[2];   // min over (index << 2 | reason), ~0 if none
-  unsigned long long pad[2];
+  EngineState engine;                  // queues, pool cursors, hungry warps
 };
+
+// Fixed-size pools of the cross-warp sharing (independent of the batch size):
+// reduction records of trees whose subtrees left their warp, and published
+// subtree tasks.  Task tags must read zero before each launch.
+constexpr unsigned long long kTreeAggCap = 8192;
+constexpr unsigned long long kTaskCap = 16384;
+constexpr unsigned long long kHelperWarps = 296;  // idle warps that stay for subtrees (2 per SM)
+constexpr size_t kScratchHeaderBytes = (sizeof(CertifyScratch) + 255) & ~size_t(255);
+constexpr size_t kPoolBytes = kTreeAggCap * sizeof(TreeAgg) + kTaskCap * sizeof(SubtreeTask);
+
+__host__ __device__ inline EnginePools pools_at(void* scratch) {
+  EnginePools p;
+  char* base = static_cast<char*>(scratch) + kScratchHeaderBytes;
+  p.tasks = reinterpret_cast<SubtreeTask*>(base);
+  p.aggs = reinterpret_cast<TreeAgg*>(base + kTaskCap * sizeof(SubtreeTask));
+  p.task_cap = kTaskCap;
+  p.agg_cap = kTreeAggCap;
+  p.helper_cap = kHelperWarps;
+  return p;
+}
 
 struct LaunchShape {
   int grid = 0;
   size_t smem = 0;
 };
 
-inline cudaError_t reset_scratch(CertifyScratch* sc, cudaStream_t s) {
+inline cudaError_t reset_scratch(CertifyScratch* sc, cudaStream_t s, bool with_pools = false) {
   cudaError_t e = cudaMemsetAsync(sc, 0, sizeof(CertifyScratch), s);
   if (e != cudaSuccess) return e;
-  return cudaMemsetAsync(sc->invalid_key, 0xff, sizeof(sc->invalid_key), s);
+  e = cudaMemsetAsync(sc->invalid_key, 0xff, sizeof(sc->invalid_key), s);
+  if (e != cudaSuccess || !with_pools) return e;
+  return cudaMemsetAsync(pools_at(sc).tasks, 0, kTaskCap * sizeof(SubtreeTask), s);
 }
 
 template <class K>
@@ -38,7 +60,7 @@ int certify_shape(K kernel, LaunchShape* shape) {
   DeviceInfo dev;
   int rc = current_device_info(&dev);
   if (rc != P2C_OK) return rc;
-  const size_t smem = sizeof(WarpSlots) * kCertifyWarps;
+  const size_t smem = sizeof(EngineShared) * kCertifyWarps;
   if (smem > 48 * 1024) {
     P2C_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
@@ -66,9 +88,10 @@ inline CertParams make_params(const p2c_cert_config& cfg, const LaunchShape& sha
 
 // Validation of CertificateEngineConfig and the interval
 // (certificate_engine.cpp:224-242) plus the GPU engine's depth range: node
-// paths are 64-bit, so a tree deeper than 64 levels must be impossible, which
-// holds when max_subdivision_depth <= 64 or eps_time >= 2^-50 (bisection of a
-// sub-interval of [0, 1] reaches width <= 2^-50 within 51 levels).
+// keys are 64-bit with a sentinel bit, so a tree deeper than 63 levels must be
+// impossible, which holds when max_subdivision_depth <= 63 or eps_time >=
+// 2^-50 (bisection of a sub-interval of [0, 1] reaches width <= 2^-50 within
+// 51 levels).
 inline int validate_cert_config(const p2c_cert_config& cfg, double t0, double t1) {
   if (!std::isfinite(cfg.eps_time) || cfg.eps_time <= 0.0)
     return fail(P2C_ERR_INVALID, "CertificateEngineConfig.eps_time must be finite and positive");
@@ -78,10 +101,10 @@ inline int validate_cert_config(const p2c_cert_config& cfg, double t0, double t1
     return fail(P2C_ERR_INVALID, "certificate interval endpoints must be finite");
   if (t0 < 0.0 || t1 > 1.0 || t0 > t1)
     return fail(P2C_ERR_INVALID, "certificate interval must satisfy 0 <= t0 <= t1 <= 1");
-  if (cfg.max_subdivision_depth > 64 && cfg.eps_time < std::ldexp(1.0, -50))
+  if (cfg.max_subdivision_depth > kMaxTreeDepth && cfg.eps_time < std::ldexp(1.0, -50))
     return fail(P2C_ERR_INVALID,
-                "CertificateEngineConfig.max_subdivision_depth > 64 needs eps_time >= 2^-50 on the GPU "
-                "certifier (interval trees deeper than 64 levels are not supported)");
+                "CertificateEngineConfig.max_subdivision_depth > 63 needs eps_time >= 2^-50 on the GPU "
+                "certifier (interval trees deeper than 63 levels are not supported)");
   return P2C_OK;
 }
 
@@ -95,6 +118,9 @@ __device__ __forceinline__ void flush_stats(const WarpStats& st, bool ok, Certif
   const unsigned long long nodes = warp_sum(st.nodes), evals = warp_sum(st.evals),
                            don = warp_sum(st.donations), q = warp_sum(st.queries), ops = warp_sum(st.ops);
   if ((threadIdx.x & 31) == 0) {
+    // iteration counters are warp-uniform: lane 0's copy is the warp's
+    if (st.iters) atomicMax((unsigned long long*)&sc->stats.max_warp_iterations, st.iters);
+    if (st.busy) atomicAdd((unsigned long long*)&sc->stats.busy_lane_iterations, st.busy);
     if (nodes) atomicAdd((unsigned long long*)&sc->stats.nodes_evaluated, nodes);
     if (evals) atomicAdd((unsigned long long*)&sc->stats.distance_evals, evals);
     if (don) atomicAdd((unsigned long long*)&sc->stats.donations, don);

@@ -70,6 +70,7 @@ unsigned long long device_budget_ns() {
     const char* e = std::getenv("P2C_DEVICE_BUDGET_MS");
     unsigned long long ms = 30000ull;
     if (e != nullptr && *e != '\0') ms = std::strtoull(e, nullptr, 10);
+    if (ms == 0ull || ms > 600000ull) ms = 30000ull;  // never unbounded, never above 10 minutes
     return ms * 1000000ull;
   }();
   return v;

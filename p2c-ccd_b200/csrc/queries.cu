@@ -29,14 +29,6 @@ struct QueryAgg {
   unsigned int any_undecided[2];
 };
 
-struct QuerySrc {
-  const unsigned long long* recs;
-  const long long* prim_query;
-  const double* q_t0;
-  const double* q_t1;
-  __device__ __forceinline__ void load(long long q, Geo& g, double& t0, double& t1, int& bad) const;
-};
-
 __device__ __forceinline__ void load_rec(const unsigned long long* __restrict__ rec, Geo& g, int& bad) {
   const long long ida = (long long)__ldg(rec + 0);
   const long long idb = (long long)__ldg(rec + 1);
@@ -55,63 +47,54 @@ __device__ __forceinline__ void load_rec(const unsigned long long* __restrict__ 
   bad = (ida < 0 || idb < 0) ? 1 : (finite ? 0 : 2);
 }
 
-__device__ __forceinline__ void QuerySrc::load(long long q, Geo& g, double& t0, double& t1, int& bad) const {
-  load_rec(recs + 30 * q, g, bad);
-  const long long qi = prim_query[q];
-  t0 = q_t0[qi];
-  t1 = q_t1[qi];
-}
-
-template <int kFamily>
-struct QuerySink {
-  const unsigned long long* recs;
-  const long long* prim_query;
-  p2c_interval_result* out;
+// Both families of a work queue: each primitive over its work item's interval.
+struct QueryProblem {
+  const unsigned long long* recs[2];
+  const long long* prim_query[2];
+  long long count[2];
+  const double* q_t0;
+  const double* q_t1;
+  p2c_interval_result* out[2];
   QueryAgg* agg;
-  __device__ __forceinline__ unsigned long long key(long long q) const {
-    return ((unsigned long long)(kFamily - 1) << 62) | (unsigned long long)q;
+  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ unsigned long long key(int f, long long q) const {
+    return ((unsigned long long)(f - 1) << 62) | (unsigned long long)q;
   }
-  __device__ __forceinline__ void finish(long long q, int family, const Outcome& o) const {
-    store_interval_result(out + q, family, o, (long long)recs[30 * q], (long long)recs[30 * q + 1]);
-    QueryAgg& a = agg[prim_query[q]];
-    const int f = kFamily - 1;
-    if (o.status == P2C_STATUS_COLLISION) atomicMin(&a.first_key, key(q));
+  __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
+    load_rec(recs[f - 1] + 30 * q, g, bad);
+    const long long qi = prim_query[f - 1][q];
+    t0 = q_t0[qi];
+    t1 = q_t1[qi];
+  }
+  __device__ __forceinline__ void finish(int f, long long q, const Outcome& o) const {
+    const unsigned long long* r = recs[f - 1] + 30 * q;
+    store_interval_result(out[f - 1] + q, f, o, (long long)r[0], (long long)r[1]);
+    QueryAgg& a = agg[prim_query[f - 1][q]];
+    if (o.status == P2C_STATUS_COLLISION) atomicMin(&a.first_key, key(f, q));
     else if (o.status == P2C_STATUS_SEPARATION) {
       atomicMin(&a.margin_bits, (unsigned long long)__double_as_longlong(o.margin));
-      if (a.any_sep[f] == 0u) atomicExch(&a.any_sep[f], 1u);
-    } else if (a.any_undecided[f] == 0u) {
-      atomicExch(&a.any_undecided[f], 1u);
+      if (a.any_sep[f - 1] == 0u) atomicExch(&a.any_sep[f - 1], 1u);
+    } else if (a.any_undecided[f - 1] == 0u) {
+      atomicExch(&a.any_undecided[f - 1], 1u);
     }
   }
-  __device__ __forceinline__ void invalid(long long q, int family, int bad, double T0, double T1) const {
-    Outcome o{3, T0, T1, T1, 0.0};
-    store_interval_result(out + q, family, o, -1, -1);
-    atomicMin(&agg[prim_query[q]].invalid_key, key(q));
+  __device__ __forceinline__ void invalid(int f, long long q, int bad, double t0, double t1) const {
+    Outcome o{3, t0, t1, t1, 0.0};
+    store_interval_result(out[f - 1] + q, f, o, -1, -1);
+    atomicMin(&agg[prim_query[f - 1][q]].invalid_key, key(f, q));
   }
 };
 
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    certify_queries_kernel(const unsigned long long* pt, long long n_pt, const long long* pt_query,
-                           const unsigned long long* ee, long long n_ee, const long long* ee_query,
-                           const double* q_t0, const double* q_t1, CertParams prm_pt, CertParams prm_ee,
-                           p2c_interval_result* out_pt, p2c_interval_result* out_ee, QueryAgg* agg,
-                           CertifyScratch* sc) {
+    certify_queries_kernel(QueryProblem prob, CertParams prm_pt, CertParams prm_ee, CertifyScratch* sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
+  EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  bool ok = true;
-  for (int pass = 0; pass < 2 && ok; ++pass) {
-    if ((pass == 0) != ee_first) {
-      if (n_pt > 0)
-        ok = run_warp<1, true, false>(QuerySrc{pt, pt_query, q_t0, q_t1}, QuerySink<1>{pt, pt_query, out_pt, agg},
-                                      n_pt, &sc->queue_head[0], prm_pt, ws, st, t_start);
-    } else if (n_ee > 0) {
-      ok = run_warp<2, true, false>(QuerySrc{ee, ee_query, q_t0, q_t1}, QuerySink<2>{ee, ee_query, out_ee, agg},
-                                    n_ee, &sc->queue_head[1], prm_ee, ws, st, t_start);
-    }
-  }
+  // no cross-warp pools here: the scratch stays one record per work item
+  const bool ok = run_engine<true, false, false>(prob, prm_pt, prm_ee, ee_first, sh, st, &sc->engine,
+                                                 EnginePools{}, t_start);
   flush_stats(st, ok, sc);
 }
 
@@ -245,10 +228,19 @@ int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const in
     rc = certify_shape(certify_queries_kernel, &shape);
     if (rc != P2C_OK) return rc;
     const CertParams ppt = make_params(*config, shape, n_pt), pee = make_params(*config, shape, n_ee);
-    certify_queries_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
-        reinterpret_cast<const unsigned long long*>(pt_dev), n_pt, reinterpret_cast<const long long*>(pt_query_dev),
-        reinterpret_cast<const unsigned long long*>(ee_dev), n_ee, reinterpret_cast<const long long*>(ee_query_dev),
-        q_t0_dev, q_t1_dev, ppt, pee, pt_results_dev, ee_results_dev, agg, sc);
+    QueryProblem prob;
+    prob.recs[0] = reinterpret_cast<const unsigned long long*>(pt_dev);
+    prob.recs[1] = reinterpret_cast<const unsigned long long*>(ee_dev);
+    prob.prim_query[0] = reinterpret_cast<const long long*>(pt_query_dev);
+    prob.prim_query[1] = reinterpret_cast<const long long*>(ee_query_dev);
+    prob.count[0] = n_pt;
+    prob.count[1] = n_ee;
+    prob.q_t0 = q_t0_dev;
+    prob.q_t1 = q_t1_dev;
+    prob.out[0] = pt_results_dev;
+    prob.out[1] = ee_results_dev;
+    prob.agg = agg;
+    certify_queries_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, ppt, pee, sc);
     P2C_CUDA(cudaGetLastError());
   }
   finalize_queries_kernel<<<(unsigned)((n_queries + 127) / 128), 128, 0, s>>>(

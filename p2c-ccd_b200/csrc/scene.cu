@@ -17,10 +17,14 @@ struct SceneAgg {
   unsigned long long n_certified[2];
 };
 
-struct SceneScratch {
-  CertifyScratch cert;
-  SceneAgg agg;
-};
+// Scratch of a scene certification: the engine header and pools, then the
+// scene reduction.
+constexpr size_t kSceneAggOffset = kScratchHeaderBytes + kPoolBytes;
+constexpr size_t kSceneScratchBytes = kSceneAggOffset + ((sizeof(SceneAgg) + 255) & ~size_t(255));
+
+__host__ __device__ inline SceneAgg* scene_agg(void* ws) {
+  return reinterpret_cast<SceneAgg*>(static_cast<char*>(ws) + kSceneAggOffset);
+}
 
 struct ScenePairs {
   const double* v_t0;
@@ -41,19 +45,28 @@ __device__ __forceinline__ void load_vertex(const ScenePairs& s, long long v, Ge
   }
 }
 
-template <int kFamily>
-struct PairSrc {
-  ScenePairs s;
-  __device__ __forceinline__ void load(long long q, Geo& g, double& t0, double& t1, int& bad) const {
+// Both families of a scene's candidate pairs over one interval; each result
+// also feeds the scene reduction and, when undecided, the fallback queue.
+struct PairProblem {
+  ScenePairs sp[2];
+  long long count[2];
+  p2c_interval_result* out[2];
+  SceneAgg* agg;
+  unsigned long long* undecided_queue;
+  unsigned long long undecided_cap;
+  unsigned long long* error_word;
+  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
+    const ScenePairs& s = sp[f - 1];
     const unsigned long long key = __ldg(s.pairs + q);
     const long long a = (long long)(key >> 32), b = (long long)(key & 0xffffffffull);
     bool finite = true;
-    if (kFamily == 1) {  // point = vertex a, triangle = face b
+    if (f == 1) {  // point = vertex a, triangle = face b
       load_vertex(s, a, g, 0, finite);
-      const int32_t* f = s.faces + 3 * b;
-      load_vertex(s, __ldg(f), g, 1, finite);
-      load_vertex(s, __ldg(f + 1), g, 2, finite);
-      load_vertex(s, __ldg(f + 2), g, 3, finite);
+      const int32_t* fc = s.faces + 3 * b;
+      load_vertex(s, __ldg(fc), g, 1, finite);
+      load_vertex(s, __ldg(fc + 1), g, 2, finite);
+      load_vertex(s, __ldg(fc + 2), g, 3, finite);
     } else {  // edge a then edge b
       const int32_t* ea = s.edges + 2 * a;
       const int32_t* eb = s.edges + 2 * b;
@@ -66,19 +79,10 @@ struct PairSrc {
     t0 = s.T0;
     t1 = s.T1;
   }
-};
-
-template <int kFamily>
-struct PairSink {
-  const unsigned long long* pairs;
-  p2c_interval_result* out;
-  SceneAgg* agg;
-  unsigned long long* undecided_queue;
-  unsigned long long undecided_cap;
-  __device__ __forceinline__ void finish(long long q, int family, const Outcome& o) const {
-    const unsigned long long key = pairs[q];
-    store_interval_result(out + q, family, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
-    const int f = kFamily - 1;
+  __device__ __forceinline__ void finish(int fam, long long q, const Outcome& o) const {
+    const unsigned long long key = sp[fam - 1].pairs[q];
+    store_interval_result(out[fam - 1] + q, fam, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
+    const int f = fam - 1;
     if (o.status == P2C_STATUS_COLLISION) {
       atomicMin(&agg->coll_key, ((unsigned long long)f << 63) | key);
       atomicAdd(&agg->collisions, 1ull);
@@ -95,10 +99,10 @@ struct PairSink {
       }
     }
   }
-  __device__ __forceinline__ void invalid(long long q, int family, int bad, double T0, double T1) const {
-    Outcome o{3, T0, T1, T1, 0.0};
-    store_interval_result(out + q, family, o, -1, -1);
-    atomicOr((unsigned long long*)&reinterpret_cast<SceneScratch*>(agg)->cert.stats.error_word, 4ull);
+  __device__ __forceinline__ void invalid(int fam, long long q, int bad, double t0, double t1) const {
+    Outcome o{3, t0, t1, t1, 0.0};
+    store_interval_result(out[fam - 1] + q, fam, o, -1, -1);
+    atomicOr(error_word, 4ull);
   }
 };
 
@@ -106,9 +110,9 @@ __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
     certify_scene_kernel(ScenePairs vf, long long vf_cap, ScenePairs ee, long long ee_cap,
                          const unsigned long long* counts, unsigned family_mask, CertParams prm,
                          p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
-                         unsigned long long uq_cap, SceneScratch* scratch) {
+                         unsigned long long uq_cap, CertifyScratch* scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  WarpSlots& ws = reinterpret_cast<WarpSlots*>(smem_raw)[threadIdx.x >> 5];
+  EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
   const long long cvf = (long long)counts[0], cee = (long long)counts[1];
@@ -119,23 +123,26 @@ __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
   CertParams p1 = prm, p2 = prm;
   p1.fetch_limit = (int)min(32ll, max(1ll, (n_vf + warps - 1) / warps));
   p2.fetch_limit = (int)min(32ll, max(1ll, (n_ee + warps - 1) / warps));
+  SceneAgg* agg = scene_agg(scratch);
+  PairProblem prob;
+  prob.sp[0] = vf;
+  prob.sp[1] = ee;
+  prob.count[0] = n_vf;
+  prob.count[1] = n_ee;
+  prob.out[0] = out_vf;
+  prob.out[1] = out_ee;
+  prob.agg = agg;
+  prob.undecided_queue = uq;
+  prob.undecided_cap = uq_cap;
+  prob.error_word = (unsigned long long*)&scratch->stats.error_word;
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  bool ok = true;
-  for (int pass = 0; pass < 2 && ok; ++pass) {
-    if ((pass == 0) != ee_first) {
-      if (n_vf > 0)
-        ok = run_warp<1, true, false>(PairSrc<1>{vf}, PairSink<1>{vf.pairs, out_vf, &scratch->agg, uq, uq_cap},
-                                      n_vf, &scratch->cert.queue_head[0], p1, ws, st, t_start);
-    } else if (n_ee > 0) {
-      ok = run_warp<2, true, false>(PairSrc<2>{ee}, PairSink<2>{ee.pairs, out_ee, &scratch->agg, uq, uq_cap}, n_ee,
-                                    &scratch->cert.queue_head[1], p2, ws, st, t_start);
-    }
-  }
-  flush_stats(st, ok, &scratch->cert);
+  const bool ok = run_engine<true, true, false>(prob, p1, p2, ee_first, sh, st, &scratch->engine, pools_at(scratch),
+                                                t_start);
+  flush_stats(st, ok, scratch);
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    scratch->agg.n_certified[0] = (unsigned long long)n_vf;
-    scratch->agg.n_certified[1] = (unsigned long long)n_ee;
-    if (cvf > vf_cap || cee > ee_cap) atomicOr((unsigned long long*)&scratch->cert.stats.error_word, 2ull);
+    agg->n_certified[0] = (unsigned long long)n_vf;
+    agg->n_certified[1] = (unsigned long long)n_ee;
+    if (cvf > vf_cap || cee > ee_cap) atomicOr((unsigned long long*)&scratch->stats.error_word, 2ull);
   }
 }
 
@@ -155,11 +162,11 @@ __device__ __forceinline__ uint8_t refinement_for_reason(uint16_t r) {  // certi
 
 // CertificateEngine::Evaluate over (VF list, EE list) from the reduced flags;
 // the collision witness is the candidate whose key won the atomicMin.
-__global__ void scene_summary_kernel(const SceneScratch* sc, const unsigned long long* vf_pairs,
+__global__ void scene_summary_kernel(const CertifyScratch* sc, const SceneAgg* agg, const unsigned long long* vf_pairs,
                                      const unsigned long long* ee_pairs, const p2c_interval_result* out_vf,
                                      const p2c_interval_result* out_ee, unsigned family_mask, double T1,
                                      p2c_scene_summary* summary) {
-  const SceneAgg& a = sc->agg;
+  const SceneAgg& a = *agg;
   const long long n_vf = (long long)a.n_certified[0], n_ee = (long long)a.n_certified[1];
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (a.coll_key != ~0ull) {
@@ -186,7 +193,7 @@ __global__ void scene_summary_kernel(const SceneScratch* sc, const unsigned long
   summary->vf_certified = (unsigned long long)n_vf;
   summary->ee_certified = (unsigned long long)n_ee;
   summary->undecided_queued = a.queued;
-  summary->error_word = sc->cert.stats.error_word;
+  summary->error_word = sc->stats.error_word;
   if (a.coll_key != ~0ull) return;
   // no collision: undecided (with the reference's reason order) or separation
   p2c_query_certificate q{};
@@ -264,11 +271,12 @@ int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pa
                          p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
                          long long uq_cap, p2c_scene_summary* summary, void* ws, size_t ws_bytes,
                          cudaStream_t s) {
-  if (ws == nullptr || ws_bytes < sizeof(SceneScratch))
-    return fail(P2C_ERR_INVALID, "scene certification workspace too small");
-  SceneScratch* sc = reinterpret_cast<SceneScratch*>(ws);
-  P2C_CUDA(reset_scratch(&sc->cert, s));
-  init_scene_agg_kernel<<<1, 1, 0, s>>>(&sc->agg);
+  if (ws == nullptr || ws_bytes < kSceneScratchBytes)
+    return fail(P2C_ERR_INVALID, "scene certification workspace too small: %zu < %zu bytes", ws_bytes,
+                kSceneScratchBytes);
+  CertifyScratch* sc = reinterpret_cast<CertifyScratch*>(ws);
+  P2C_CUDA(reset_scratch(sc, s, true));
+  init_scene_agg_kernel<<<1, 1, 0, s>>>(scene_agg(ws));
   LaunchShape shape;
   int rc = certify_shape(certify_scene_kernel, &shape);
   if (rc != P2C_OK) return rc;
@@ -282,7 +290,8 @@ int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pa
   if (summary != nullptr) {
     const long long nmax = (vf_cap > ee_cap ? vf_cap : ee_cap);
     const unsigned grid = (unsigned)((nmax + 255) / 256 > 0 ? (nmax + 255) / 256 : 1);
-    scene_summary_kernel<<<grid, 256, 0, s>>>(sc, vf_pairs, ee_pairs, out_vf, out_ee, family_mask, T1, summary);
+    scene_summary_kernel<<<grid, 256, 0, s>>>(sc, scene_agg(ws), vf_pairs, ee_pairs, out_vf, out_ee, family_mask,
+                                              T1, summary);
     P2C_CUDA(cudaGetLastError());
   }
   return P2C_OK;
@@ -294,7 +303,7 @@ int validate_scene(const p2c_scene* sc);
 
 extern "C" {
 
-size_t p2c_scene_certify_workspace_bytes(void) { return sizeof(p2c::SceneScratch); }
+size_t p2c_scene_certify_workspace_bytes(void) { return p2c::kSceneScratchBytes; }
 
 int p2c_scene_certify(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t vf_cap,
                       const uint64_t* ee_pairs_dev, int64_t ee_cap, const uint64_t* counts_dev, double interval_t0,

@@ -56,6 +56,8 @@ CERTIFY_STATS_DTYPE = np.dtype([
     ("donations", "<u8"),
     ("queries", "<u8"),
     ("error_word", "<u8"),
+    ("max_warp_iterations", "<u8"),
+    ("busy_lane_iterations", "<u8"),
 ])
 
 assert POINT_TRIANGLE_DTYPE.itemsize == 240
