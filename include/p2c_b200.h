@@ -320,6 +320,54 @@ int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, 
                           const uint64_t* ee_pairs_dev, int64_t n_ee,
                           p2c_point_triangle* vf_records_dev, p2c_edge_edge* ee_records_dev, void* stream);
 
+/* ---- candidate groups: scheduled any-hit with fallback replay ------------ */
+/* Per-call totals of p2c_group_anyhit. */
+typedef struct p2c_anyhit_summary {
+  uint64_t candidates;          /* candidates considered: min(*count_dev, cap) */
+  uint64_t groups;              /* groups with at least one candidate */
+  uint64_t detected_groups;     /* groups with a hit (each group stops at its first hit) */
+  uint64_t proposal_calls;      /* certificates the proposal phase counts */
+  uint64_t fallback_calls;      /* certificates the fallback replay counts */
+  uint64_t fallback_groups;     /* groups with no hit among their proposals */
+  uint64_t first_hit_rank_sum;  /* over detected groups: calls up to and including the hit */
+  uint64_t speculative;         /* certificates computed on the device and discarded
+                                   (started before an earlier candidate of their group hit) */
+  uint64_t error_word;          /* 1: time budget, 4: non-finite geometry (counted as a hit),
+                                   8: object id outside [0, n_obj) or pair index outside the
+                                   scene (the candidate is left out), 16: NaN score (ranked last) */
+} p2c_anyhit_summary;
+
+/* Workspace of p2c_group_anyhit for cap candidates and n_obj objects. */
+size_t p2c_group_anyhit_workspace_bytes(int64_t cap, int32_t n_obj);
+
+/* Scheduled any-hit over one family's candidate pairs of a scene, with
+ * conservative fallback replay: the scene tool's RunScheduledAnyHitRows
+ * (tools/scene_object_envelope_native_ti_walltime.cpp:1283-1410) with the
+ * reference certifier as the exact judge (hit = collision or undecided).
+ *   - group of a candidate = unordered object pair (GroupKey :756-770),
+ *     index lo * n_obj + hi with the scene's v_obj/f_obj (family 1) or e_obj
+ *     (family 2);
+ *   - proposals: per group the top_k candidates by score, higher first,
+ *     certified in that order until the first hit;
+ *   - fallback replay: every other candidate of a group without a proposal
+ *     hit, in candidate order, until the first hit.
+ * Ties in score rank the lower candidate index first (the reference's heap
+ * order is unspecified for ties; with distinct scores both orders agree).
+ * The device certifies candidates speculatively in parallel and cancels those
+ * behind a known hit; the reported calls, hits and groups are exactly the
+ * sequential procedure's.  n = min(*count_dev, cap) is read on the device, so
+ * this can follow p2c_scene_candidates without a host sync.  Outputs (each
+ * optional): evaluated_dev[n] (0: not called, 1: proposal call, 2: fallback
+ * call), hit_dev[n] (1: called and hit), per group (n_obj * n_obj) detected,
+ * proposal calls and fallback calls, and the summary. */
+int p2c_group_anyhit(const p2c_scene* scene, int family, const uint64_t* pairs_dev, int64_t cap,
+                     const uint64_t* count_dev, const double* scores_dev, int64_t top_k,
+                     double interval_t0, double interval_t1, const p2c_cert_config* config,
+                     uint8_t* evaluated_dev, uint8_t* hit_dev, uint8_t* group_detected_dev,
+                     int64_t* group_proposal_calls_dev, int64_t* group_fallback_calls_dev,
+                     p2c_anyhit_summary* summary_dev, void* workspace_dev, size_t workspace_bytes,
+                     void* stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* FP64 throughput probe: launches independent separately rounded multiply/add
  * chains over a full-occupancy grid and reports the FP64 operations it issues;

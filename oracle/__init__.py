@@ -7,6 +7,9 @@ Two checkers, both loaded with ctypes:
   * ``_ref/libp2c_ref.so``: the reference's own sources compiled unchanged with
     ref_abi.cpp (present when the reference checkout was available at build
     time; the built file travels with the tree).
+  * ``_ref/libp2c_ref_tool.so``: the reference's scene any-hit tool compiled
+    unchanged (ref_tool.cpp), its Tight-Inclusion calls answered by the
+    reference certifier through shim/tight_inclusion/ccd.hpp.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
 this package.  The product library never does.
@@ -22,6 +25,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libccd_oracle.so"
 REF_SO = HERE / "_ref" / "libp2c_ref.so"
+REF_TOOL_SO = HERE / "_ref" / "libp2c_ref_tool.so"
 
 TRAJ = np.dtype([("feature_id", "<i8"), ("position_t0", "<f8", (3,)), ("position_t1", "<f8", (3,))])
 PT = np.dtype([("point_id", "<i8"), ("triangle_id", "<i8"), ("point", TRAJ), ("triangle_v0", TRAJ),
@@ -277,3 +281,77 @@ def ref_build_mesh_query(va, fa, ta0, ta1, vb, fb, tb0, tb1, family_mask=3, prun
     ees = np.zeros(nee.value, dtype=EE)
     R.ref_build_mesh_query(*args, _p(pts), ctypes.byref(npt), _p(ees), ctypes.byref(nee))
     return pts, ees
+
+
+# ---- the reference scene tool (tools/scene_object_envelope_native_ti_walltime.cpp) ----
+
+_ref_tool = None
+
+TOOL_ROW_FIELDS = ("all_exact_calls", "all_hit_count", "all_group_count", "all_positive_groups",
+                   "exact_calls", "proposal_exact_calls", "fallback_exact_calls", "hit_count", "group_count",
+                   "positive_groups", "fallback_groups", "tp", "fp", "fn", "tn", "positive_first_hit_rank_sum")
+
+
+def ref_tool() -> ctypes.CDLL:
+    global _ref_tool
+    if _ref_tool is None:
+        if not REF_TOOL_SO.exists():
+            raise FileNotFoundError(f"{REF_TOOL_SO} is not built (the reference sources were not available)")
+        T = ctypes.CDLL(str(REF_TOOL_SO))
+        vp, i64, f64, ci, u64 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int, ctypes.c_uint64
+        T.ref_tool_last_error.restype = ctypes.c_char_p
+        T.ref_tool_prepare.argtypes = [vp, vp, i64, vp, i64, f64, ci]
+        T.ref_tool_objects.argtypes = [vp, vp]
+        T.ref_tool_edges.argtypes = [vp, vp]
+        T.ref_tool_edges.restype = i64
+        T.ref_tool_candidates.argtypes = [ci, u64, vp, vp, i64, vp]
+        T.ref_tool_candidates.restype = i64
+        T.ref_tool_random_scores.argtypes = [ci, vp]
+        T.ref_tool_anyhit.argtypes = [ci, u64, f64, f64, ci, vp]
+        _ref_tool = T
+    return _ref_tool
+
+
+class RefToolScene:
+    """The reference tool's PrepareScene over one step of a triangle soup,
+    then its candidate lists, random-policy scores and any-hit rows."""
+
+    def __init__(self, v_t0, v_t1, faces, thickness: float = 0.0, exclude_self: bool = False):
+        T = ref_tool()
+        self.v_t0 = np.ascontiguousarray(v_t0, dtype=np.float64)
+        self.v_t1 = np.ascontiguousarray(v_t1, dtype=np.float64)
+        self.faces = np.ascontiguousarray(faces, dtype=np.int32)
+        if T.ref_tool_prepare(_p(self.v_t0), _p(self.v_t1), len(self.v_t0), _p(self.faces), len(self.faces),
+                              float(thickness), int(exclude_self)):
+            raise ValueError(T.ref_tool_last_error().decode())
+        self.v_obj = np.zeros(len(self.v_t0), dtype=np.int32)
+        self.f_obj = np.zeros(len(self.faces), dtype=np.int32)
+        self.n_obj = T.ref_tool_objects(_p(self.v_obj), _p(self.f_obj))
+        ne = T.ref_tool_edges(None, None)
+        self.edges = np.zeros((ne, 2), dtype=np.int32)
+        self.e_obj = np.zeros(ne, dtype=np.int32)
+        T.ref_tool_edges(_p(self.edges), _p(self.e_obj))
+
+    def candidates(self, kind: str, max_candidates: int = 0) -> np.ndarray:
+        """(n, 2) int32 pairs in the tool's emission order: (vertex, face) or (edge, edge)."""
+        T = ref_tool()
+        k = 0 if kind == "vf" else 1
+        capped = ctypes.c_int(0)
+        n = T.ref_tool_candidates(k, max_candidates, None, None, 0, ctypes.byref(capped))
+        a = np.zeros(max(n, 1), dtype=np.int32)
+        b = np.zeros(max(n, 1), dtype=np.int32)
+        T.ref_tool_candidates(k, max_candidates, _p(a), _p(b), n, ctypes.byref(capped))
+        self.capped = bool(capped.value)
+        return np.stack([a[:n], b[:n]], axis=1)
+
+    def random_scores(self, kind: str, n: int) -> np.ndarray:
+        out = np.zeros(max(n, 1), dtype=np.float64)
+        ref_tool().ref_tool_random_scores(0 if kind == "vf" else 1, _p(out))
+        return out[:n]
+
+    def anyhit(self, kind: str, top_k: int, eps_time: float, eps_space: float, max_depth: int) -> dict:
+        out = np.zeros(16, dtype=np.uint64)
+        T = ref_tool()
+        if T.ref_tool_anyhit(0 if kind == "vf" else 1, top_k, eps_time, eps_space, max_depth, _p(out)):
+            raise ValueError(T.ref_tool_last_error().decode())
+        return {k: int(v) for k, v in zip(TOOL_ROW_FIELDS, out)}

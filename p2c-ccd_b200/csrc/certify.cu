@@ -37,6 +37,7 @@ struct RecordProblem {
   unsigned long long* invalid_key;    // [2]: min over (index << 2 | reason)
   double T0, T1;
   __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
     load_record(recs[f - 1] + 30 * q, g, bad);
     t0 = T0;

@@ -101,6 +101,7 @@ struct EngineShared {
 
 // The problem a launch certifies: both families' queries.  P provides
 //   long long n(int family) const;
+//   bool skip(int family, long long q) const;   // drop q unevaluated (a cancelled candidate)
 //   void load(int family, long long q, Geo&, double& T0, double& T1, int& bad) const;
 //   void finish(int family, long long q, const Outcome&) const;
 //   void invalid(int family, long long q, int bad, double T0, double T1) const;
@@ -200,8 +201,11 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
             int bad = 0;
             Geo g;
             double RT0, RT1;
-            prob.load(cur, q, g, RT0, RT1, bad);
-            if (bad != 0) {
+            const bool dropped = prob.skip(cur, q);
+            if (!dropped) prob.load(cur, q, g, RT0, RT1, bad);
+            if (dropped) {
+              atomicAdd(&es->finalized.v, 1ull);
+            } else if (bad != 0) {
               prob.invalid(cur, q, bad, RT0, RT1);
               atomicAdd(&es->finalized.v, 1ull);
             } else {

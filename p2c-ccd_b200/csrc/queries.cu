@@ -60,6 +60,7 @@ struct QueryProblem {
   __device__ __forceinline__ unsigned long long key(int f, long long q) const {
     return ((unsigned long long)(f - 1) << 62) | (unsigned long long)q;
   }
+  __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
     load_rec(recs[f - 1] + 30 * q, g, bad);
     const long long qi = prim_query[f - 1][q];

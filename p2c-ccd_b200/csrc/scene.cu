@@ -4,6 +4,7 @@
 #include "broadphase.cuh"
 #include "certify_core.cuh"
 #include "certify_launch.cuh"
+#include "scene_pairs.cuh"
 
 namespace p2c {
 namespace {
@@ -26,25 +27,6 @@ __host__ __device__ inline SceneAgg* scene_agg(void* ws) {
   return reinterpret_cast<SceneAgg*>(static_cast<char*>(ws) + kSceneAggOffset);
 }
 
-struct ScenePairs {
-  const double* v_t0;
-  const double* v_t1;
-  const int32_t* faces;
-  const int32_t* edges;
-  const unsigned long long* pairs;
-  double T0, T1;
-};
-
-__device__ __forceinline__ void load_vertex(const ScenePairs& s, long long v, Geo& g, int slot, bool& finite) {
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const double x0 = __ldg(s.v_t0 + 3 * v + a), x1 = __ldg(s.v_t1 + 3 * v + a);
-    g.p0[3 * slot + a] = x0;
-    g.p1[3 * slot + a] = x1;
-    finite = finite && isfinite(x0) && isfinite(x1);
-  }
-}
-
 // Both families of a scene's candidate pairs over one interval; each result
 // also feeds the scene reduction and, when undecided, the fallback queue.
 struct PairProblem {
@@ -56,26 +38,10 @@ struct PairProblem {
   unsigned long long undecided_cap;
   unsigned long long* error_word;
   __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
     const ScenePairs& s = sp[f - 1];
-    const unsigned long long key = __ldg(s.pairs + q);
-    const long long a = (long long)(key >> 32), b = (long long)(key & 0xffffffffull);
-    bool finite = true;
-    if (f == 1) {  // point = vertex a, triangle = face b
-      load_vertex(s, a, g, 0, finite);
-      const int32_t* fc = s.faces + 3 * b;
-      load_vertex(s, __ldg(fc), g, 1, finite);
-      load_vertex(s, __ldg(fc + 1), g, 2, finite);
-      load_vertex(s, __ldg(fc + 2), g, 3, finite);
-    } else {  // edge a then edge b
-      const int32_t* ea = s.edges + 2 * a;
-      const int32_t* eb = s.edges + 2 * b;
-      load_vertex(s, __ldg(ea), g, 0, finite);
-      load_vertex(s, __ldg(ea + 1), g, 1, finite);
-      load_vertex(s, __ldg(eb), g, 2, finite);
-      load_vertex(s, __ldg(eb + 1), g, 3, finite);
-    }
-    bad = finite ? 0 : 2;
+    bad = load_pair(s, f, __ldg(s.pairs + q), g) ? 0 : 2;
     t0 = s.T0;
     t1 = s.T1;
   }
