@@ -308,6 +308,7 @@ def ref_tool() -> ctypes.CDLL:
         T.ref_tool_candidates.restype = i64
         T.ref_tool_random_scores.argtypes = [ci, vp]
         T.ref_tool_anyhit.argtypes = [ci, u64, f64, f64, ci, vp]
+        T.ref_tool_time_step.argtypes = [u64, f64, f64, ci, vp, vp, vp]
         _ref_tool = T
     return _ref_tool
 
@@ -355,3 +356,14 @@ class RefToolScene:
         if T.ref_tool_anyhit(0 if kind == "vf" else 1, top_k, eps_time, eps_space, max_depth, _p(out)):
             raise ValueError(T.ref_tool_last_error().decode())
         return {k: int(v) for k, v in zip(TOOL_ROW_FIELDS, out)}
+
+    def time_step(self, top_k: int, eps_time: float, eps_space: float, max_depth: int) -> dict:
+        """The tool's candidates + scheduled any-hit of both families, timed inside the library."""
+        secs = np.zeros(3)
+        calls = np.zeros(2, dtype=np.uint64)
+        cands = np.zeros(2, dtype=np.uint64)
+        T = ref_tool()
+        if T.ref_tool_time_step(top_k, eps_time, eps_space, max_depth, _p(secs), _p(calls), _p(cands)):
+            raise ValueError(T.ref_tool_last_error().decode())
+        return {"candidates_s": float(secs[0]), "anyhit_vf_s": float(secs[1]), "anyhit_ee_s": float(secs[2]),
+                "calls": int(calls.sum()), "candidates": int(cands.sum())}

@@ -226,4 +226,46 @@ int ref_tool_anyhit(int kind, std::uint64_t top_k, double eps_time, double eps_s
   return 0;
 }
 
+// One timed step of the tool on the prepared scene, single-threaded as the
+// tool runs: candidate generation of both families, then the scheduled
+// any-hit of each family ("random" scores).  The group set handed to
+// RunScheduledAnyHitRows is built from the candidates without certifying
+// them (the every-candidate truth rows are not part of the step).
+// seconds[0..2] = {candidates, any-hit vf, any-hit ee}; calls[0..1] = exact
+// calls of the vf and ee rows; cands[0..1] = candidate counts.
+int ref_tool_time_step(std::uint64_t top_k, double eps_time, double eps_space, int max_depth, double* seconds,
+                       std::uint64_t* calls, std::uint64_t* cands) {
+  if (!g_scene_ready) return 1;
+  g_tool_config.eps_time = eps_time;
+  g_tool_config.eps_space = eps_space;
+  g_tool_config.max_subdivision_depth = static_cast<std::uint16_t>(max_depth);
+  Args args;
+  args.proposal_top_k = static_cast<std::size_t>(top_k);
+  try {
+    const auto t0 = std::chrono::steady_clock::now();
+    bool c0 = false, c1 = false;
+    g_candidates[0] = BuildVFCandidates(g_scene, 0, &c0);
+    g_candidates[1] = BuildEECandidates(g_scene, 0, &c1);
+    const auto t1 = std::chrono::steady_clock::now();
+    seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+    const TinyStpfWeights weights;
+    for (int kind = 0; kind < 2; ++kind) {
+      const std::string k = kind == 0 ? "vf" : "ee";
+      std::unordered_map<std::uint64_t, GroupTruth> groups;
+      for (const Candidate& c : g_candidates[kind]) groups[GroupKey(g_scene, k, c)];
+      const auto a = std::chrono::steady_clock::now();
+      const MethodRow row = RunScheduledAnyHitRows(g_scene, args, k, g_candidates[kind], false, 0.0,
+                                                   "ScheduledAnyHit", "random", weights, groups);
+      const auto b = std::chrono::steady_clock::now();
+      seconds[1 + kind] = std::chrono::duration<double>(b - a).count();
+      calls[kind] = row.exact_calls;
+      cands[kind] = g_candidates[kind].size();
+    }
+  } catch (const std::exception& e) {
+    g_tool_error = e.what();
+    return 1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -61,7 +61,13 @@ class ScenePipeline:
     def __init__(self, scene: SceneArrays | dict, device: str | torch.device = "cuda", *,
                  thickness: float = 0.0, exclude_self: bool = True, config: CertConfig = CertConfig(),
                  interval: tuple[float, float] = (0.0, 1.0), family_mask: int = 3, sort_pairs: bool = True,
-                 vf_capacity: int = 1 << 16, ee_capacity: int = 1 << 16, undecided_capacity: int = 1 << 14):
+                 vf_capacity: int = 1 << 16, ee_capacity: int = 1 << 16, undecided_capacity: int = 1 << 14,
+                 narrow: str = "certify", top_k: int = 4096, scheduler_seed: int = 0):
+        """narrow = "certify": every candidate is certified (p2c_scene_certify);
+        narrow = "anyhit": candidates are grouped by object pair and run
+        through the scheduled any-hit with fallback replay
+        (p2c_group_anyhit) with proposal size top_k and priority scores from
+        a seeded scheduler stub (uniform random, positional per candidate)."""
         if isinstance(scene, dict):
             scene = SceneArrays.from_dict(scene)
         self.lib = _lib.load()
@@ -87,6 +93,11 @@ class ScenePipeline:
         self.cert_ws = torch.empty(int(self.lib.p2c_scene_certify_workspace_bytes()), dtype=torch.uint8, device=d)
         self.undecided_capacity = int(undecided_capacity)
         self.undecided_queue = torch.empty(max(1, self.undecided_capacity), dtype=torch.int64, device=d)
+        if narrow not in ("certify", "anyhit"):
+            raise ValueError("narrow must be 'certify' or 'anyhit'")
+        self.narrow = narrow
+        self.top_k = int(top_k)
+        self.scheduler_seed = int(scheduler_seed)
         self._struct = SceneStruct()
         self._refresh_struct()
         self._alloc(vf_capacity, ee_capacity)
@@ -112,6 +123,14 @@ class ScenePipeline:
         nbytes = self.lib.p2c_scene_candidates_workspace_bytes(self._struct.nv, self._struct.nf, self._struct.ne,
                                                                self.vf_cap, self.ee_cap)
         self.bp_ws = torch.empty(int(nbytes), dtype=torch.uint8, device=d)
+        if self.narrow == "anyhit":
+            from .anyhit import GroupAnyHit
+
+            gen = torch.Generator(device=d).manual_seed(self.scheduler_seed)
+            self.vf_scores = torch.rand(self.vf_cap, dtype=torch.float64, device=d, generator=gen)
+            self.ee_scores = torch.rand(self.ee_cap, dtype=torch.float64, device=d, generator=gen)
+            self.anyhit_vf = GroupAnyHit(self._struct, self.n_obj, "vf", self.vf_cap, d)
+            self.anyhit_ee = GroupAnyHit(self._struct, self.n_obj, "ee", self.ee_cap, d)
 
     def update_positions(self, v_t0: torch.Tensor, v_t1: torch.Tensor) -> None:
         """Copy a new step's trajectories into the resident buffers (async)."""
@@ -135,10 +154,25 @@ class ScenePipeline:
             self.vf_results.data_ptr(), self.ee_results.data_ptr(), self.undecided_queue.data_ptr(),
             self.undecided_capacity, self.summary.data_ptr(), self.cert_ws.data_ptr(), self.cert_ws.numel(), stream))
 
+    def anyhit(self) -> None:
+        """Scheduled any-hit with fallback replay of both families (async)."""
+        if self.family_mask & 1:
+            self.anyhit_vf.run(self.vf_pairs, self.counts[0:1], self.vf_scores, self.top_k, self.config,
+                               self.interval)
+        if self.family_mask & 2:
+            self.anyhit_ee.run(self.ee_pairs, self.counts[1:2], self.ee_scores, self.top_k, self.config,
+                               self.interval)
+
+    def narrow_phase(self) -> None:
+        if self.narrow == "anyhit":
+            self.anyhit()
+        else:
+            self.certify()
+
     def step(self) -> None:
-        """Candidates then certificates, asynchronous on the current stream."""
+        """Candidates then the narrow phase, asynchronous on the current stream."""
         self.candidates()
-        self.certify()
+        self.narrow_phase()
 
     def capture(self) -> None:
         """Capture one step (candidates + certificates, ~60 launches) into a
@@ -172,12 +206,25 @@ class ScenePipeline:
             if err & 1:
                 raise ValueError("scene trajectories must be finite")
             if n_vf <= self.vf_cap and n_ee <= self.ee_cap:
-                summ = self.read_summary()
+                summ = self.read_summary() if self.narrow == "certify" else self.read_anyhit_summary()
                 if summ["error_word"] & ERR_BUDGET:
                     raise _lib.P2CError("certification exceeded the device time budget (P2C_DEVICE_BUDGET_MS)")
                 return summ
             self._alloc(max(self.vf_cap, int(n_vf * 1.25) + 1024), max(self.ee_cap, int(n_ee * 1.25) + 1024))
         raise _lib.P2CError("pair buffers kept overflowing")
+
+    def read_anyhit_summary(self) -> dict:
+        """Both families' any-hit summaries plus their sums."""
+        out = {"vf": self.anyhit_vf.read_summary() if self.family_mask & 1 else None,
+               "ee": self.anyhit_ee.read_summary() if self.family_mask & 2 else None}
+        parts = [v for v in out.values() if v is not None]
+        for k in ("candidates", "groups", "detected_groups", "proposal_calls", "fallback_calls", "speculative"):
+            out[k] = sum(p[k] for p in parts)
+        out["calls"] = out["proposal_calls"] + out["fallback_calls"]
+        out["error_word"] = 0
+        for p in parts:
+            out["error_word"] |= p["error_word"]
+        return out
 
     def read_summary(self) -> dict:
         raw = self.summary.cpu().numpy().view(SUMMARY_DTYPE)[0]
