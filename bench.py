@@ -267,6 +267,128 @@ class SceneWorkload:
         return _scene_reference_sample(self.scene, self.cfg, budget_s, threads)
 
 
+class BatchWorkload:
+    """Batched uneven scenes: 256 independent two-sphere scenes, triangle
+    counts log-uniform over 1k-200k (9.57M triangles), random rigid motion +
+    jitter, every scene's swept-AABB candidates then the certificates of all
+    their candidates in ONE persistent launch, the whole step one CUDA graph
+    with an autotuned launch shape."""
+
+    name = "batch"
+    narrow_kernel = "batch_certify_kernel"
+
+    def __init__(self, device, rank: int):
+        import numpy as np
+        import torch
+
+        from p2cccd_b200 import certify, scenes
+        from p2cccd_b200.batch import BatchPipeline
+
+        self.torch = torch
+        self.seed = 20261203 + rank
+        self.scenes = scenes.uneven_batch(256, seed=self.seed)
+        self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
+        self.bp = BatchPipeline(self.scenes, device, exclude_self=True, config=self.cfg, streams=8)
+        summ = self.bp.step_checked()
+        self.tuning = self.bp.autotune(reps=3)
+        self.bp.capture()
+        self.summaries = summ
+        self.queries = sum(x["vf_certified"] + x["ee_certified"] for x in summ)
+        hits = np.array([x["collisions"] + x["undecided"] for x in summ], dtype=np.float64)
+        cands = np.array([max(1, x["vf_certified"] + x["ee_certified"]) for x in summ], dtype=np.float64)
+        self.hit_frac = hits / cands
+        self.h_t0 = torch.empty_like(self.bp.v_t0, device="cpu").pin_memory()
+        self.h_t1 = torch.empty_like(self.bp.v_t1, device="cpu").pin_memory()
+        self.h_t0.copy_(self.bp.v_t0)
+        self.h_t1.copy_(self.bp.v_t1)
+        self.d2h = [(self.bp.vf_results, torch.empty_like(self.bp.vf_results, device="cpu").pin_memory()),
+                    (self.bp.ee_results, torch.empty_like(self.bp.ee_results, device="cpu").pin_memory()),
+                    (self.bp.summaries, torch.empty_like(self.bp.summaries, device="cpu").pin_memory())]
+        self.phase_events = []
+
+    def config(self) -> dict:
+        tris = [s["spec"]["triangles"] for s in self.scenes]
+        return {"workload": "batched uneven scenes: 256 independent two-UV-sphere scenes, triangle counts "
+                            "log-uniform 1k-200k, random rigid motion (rotation + translation into contact, "
+                            "penetration 0.25 f, f ~ U[5%, 40%]) + N(0,1e-3) jitter, FP64; per-scene swept-AABB "
+                            "candidates then every candidate certified in one persistent launch, one CUDA graph",
+                "scenes": len(self.scenes), "triangles": int(sum(tris)), "triangles_min": int(min(tris)),
+                "triangles_max": int(max(tris)), "queries_per_step": self.queries,
+                "contact_fraction_measured": {"min": float(self.hit_frac.min()), "mean": float(self.hit_frac.mean()),
+                                              "max": float(self.hit_frac.max()),
+                                              "definition": "(collisions + undecided) / candidates per scene"},
+                "autotuned": {k: self.tuning[k] for k in ("blocks_per_sm", "fetch_limit", "helper_warps", "streams")},
+                "eps_time": self.cfg.eps_time, "eps_space": self.cfg.eps_space,
+                "max_subdivision_depth": self.cfg.max_subdivision_depth, "seed": self.seed}
+
+    def step(self):
+        self.bp.replay()
+
+    def step_uncaptured(self):
+        self.bp.step()
+
+    def step_phased(self):
+        torch = self.torch
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
+        self.bp.candidates()
+        e1.record()
+        self.bp.certify()
+        e2.record()
+        self.phase_events.append((e0, e1, e2))
+
+    def step_e2e(self):
+        self.bp.v_t0.copy_(self.h_t0, non_blocking=True)
+        self.bp.v_t1.copy_(self.h_t1, non_blocking=True)
+        self.bp.replay()
+        for d, h in self.d2h:
+            h.copy_(d, non_blocking=True)
+
+    def io_bytes(self) -> tuple[int, int]:
+        return self.h_t0.numel() * 8 + self.h_t1.numel() * 8, sum(h.numel() for _, h in self.d2h)
+
+    def census(self) -> dict:
+        import numpy as np
+
+        from p2cccd_b200 import certify
+
+        vf, ee = zip(*(self.bp.materialize(i) for i in range(self.bp.n)))
+        vf, ee = np.concatenate(vf), np.concatenate(ee)
+        return certify.census(certify.records_to_device(vf, self.bp.device),
+                              certify.records_to_device(ee, self.bp.device), 0.0, 1.0, self.cfg)["stats"]
+
+    def broad_phase_bytes(self) -> int:
+        return sum(48 * len(s["v_t0"]) + 12 * len(s["faces"]) + 8 * len(s["edges"]) for s in self.scenes) + \
+            8 * self.queries
+
+    def cpu_reference(self, threads: int, budget_s: float) -> dict:
+        return _batch_reference_sample(self.scenes, self.cfg, budget_s)
+
+
+def _batch_reference_sample(scenes_list, cfg, budget_s: float, order=None) -> dict:
+    """The reference scene tool (compiled unchanged, 1 thread as written) on
+    whole scenes of the batch, in batch order (or `order`), until budget_s:
+    its sweep-and-prune candidates (self pairs excluded) then its
+    every-candidate certificate rows (RunAllExactRows) of both families."""
+    import oracle
+
+    t_start = time.perf_counter()
+    secs, calls, done, tris = 0.0, 0, 0, 0
+    for i in (order if order is not None else range(len(scenes_list))):
+        s = scenes_list[i]
+        tool = oracle.RefToolScene(s["v_t0"], s["v_t1"], s["faces"], 0.0, True)
+        r = tool.time_all_exact(cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth)
+        secs += r["candidates_s"] + r["certify_s"]
+        calls += r["calls"]
+        done += 1
+        tris += len(s["faces"])
+        if time.perf_counter() - t_start >= budget_s:
+            break
+    return {"queries": calls, "seconds": secs, "threads": 1, "scenes": done,
+            "sample": f"reference scene tool (SweepPairs candidates + RunAllExactRows, 1 thread as written) on "
+                      f"{done} whole scene(s) of the batch ({tris} triangles, {calls} candidates)"}
+
+
 class ClothWorkload:
     """Dense-contact stress: a 513 x 513 cloth grid (524,288 triangles)
     draped onto a 100,000-triangle UV sphere (250 x 200 rings) with a 1e-4
@@ -276,6 +398,7 @@ class ClothWorkload:
     of the procedure (proposal or fallback replay)."""
 
     name = "cloth"
+    narrow_kernel = "anyhit_certify_kernel"
 
     def __init__(self, device, rank: int):
         import torch
@@ -485,7 +608,7 @@ def _scene_reference_sample(scene, cfg, budget_s: float, threads: int) -> dict:
     return {"queries": q_sum / rounds, "seconds": s_sum / rounds, "sample": ref.describe() + f"; {rounds} round(s)"}
 
 
-WORKLOADS = {"plain": PlainWorkload, "scene": SceneWorkload, "cloth": ClothWorkload}
+WORKLOADS = {"plain": PlainWorkload, "scene": SceneWorkload, "cloth": ClothWorkload, "batch": BatchWorkload}
 
 
 # --------------------------------------------------------------------------
@@ -623,7 +746,7 @@ def run_b200(args) -> dict | None:
                       "frac": bp_bytes / (bp * 1e-3) / 1e9 / hbm_peak, "traffic": None,
                       "peak_source": hbm_src, "kernel": "candidate generation (boxes, sort, sweep)",
                       "algorithmic_bytes_per_step": bp_bytes}
-        narrow = dict(fp64_roof, kernel="certify_scene_kernel",
+        narrow = dict(fp64_roof, kernel=getattr(wl, "narrow_kernel", "certify_scene_kernel"),
                       achieved=census["fp64_ops"] / (npm * 1e-3) / 1e12,
                       frac=census["fp64_ops"] / (npm * 1e-3) / fp64_rate)
         roofline, secondary = (narrow, broad_roof) if npm >= bp else (broad_roof, narrow)
@@ -707,6 +830,26 @@ def run_reference(args) -> dict | None:
         conf = {"workload": "single-scene broad+narrow: two 40,960-triangle UV spheres, translation-only form "
                             "(the reference mesh builder takes rigid translations only)"}
         sample = ref.describe() + "; one slice per step"
+    elif args.workload == "batch":
+        batch = scenes.uneven_batch(256)
+        by_size = sorted(range(len(batch)), key=lambda i: len(batch[i]["faces"]))
+        chosen, spent = [], 0.0
+        for i in by_size:  # smallest scenes first while their mean tool time fits the per-step budget
+            r = _batch_reference_sample(batch, cfg, 0.0, order=[i])
+            if chosen and (spent + r["seconds"]) / (len(chosen) + 1) > per_step_s:
+                break
+            chosen.append(i)
+            spent += r["seconds"]
+
+        def step(i):
+            r = _batch_reference_sample(batch, cfg, 0.0, order=[chosen[i % len(chosen)]])
+            return r["queries"], r["seconds"]
+        conf = {"workload": "batched uneven scenes: 256 two-UV-sphere scenes, 1k-200k triangles (the reference "
+                            "scene tool, one scene per step)"}
+        sample = (f"reference scene tool (SweepPairs candidates + RunAllExactRows, 1 thread as written), one whole "
+                  f"scene per step cycling over the {len(chosen)} smallest scenes of the batch (up to "
+                  f"{len(batch[chosen[-1]]['faces'])} triangles) whose mean step fits {per_step_s * 1e3:.0f} ms")
+        threads = 1
     else:
         tool, n = None, None
         for cand in (17, 33, 65, 129, 257):  # largest instance whose step fits the per-step wall budget

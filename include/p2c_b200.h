@@ -320,6 +320,46 @@ int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, 
                           const uint64_t* ee_pairs_dev, int64_t n_ee,
                           p2c_point_triangle* vf_records_dev, p2c_edge_edge* ee_records_dev, void* stream);
 
+/* ---- batches: many scenes certified in one launch ------------------------ */
+/* One scene of a batch: its geometry (scene-local indices), the candidate
+ * pairs p2c_scene_candidates wrote for it, and where its certificates go.
+ * An array of these lives in device memory. */
+typedef struct p2c_batch_scene {
+  const double* v_t0;              /* nv x 3 */
+  const double* v_t1;              /* nv x 3 */
+  const int32_t* faces;            /* nf x 3 */
+  const int32_t* edges;            /* ne x 2 */
+  const uint64_t* vf_pairs;        /* vf_cap entries */
+  const uint64_t* ee_pairs;        /* ee_cap entries */
+  int64_t vf_cap, ee_cap;
+  const uint64_t* counts;          /* candidate counts: n = min(counts[k], cap) */
+  p2c_interval_result* vf_results; /* vf_cap entries */
+  p2c_interval_result* ee_results; /* ee_cap entries */
+} p2c_batch_scene;
+
+/* Launch shape of the batch certifier (the autotuned parameters). */
+typedef struct p2c_batch_tuning {
+  int32_t blocks_per_sm;  /* resident blocks of 4 warps per SM; 0: the occupancy maximum */
+  int32_t fetch_limit;    /* queries a warp holds at once (1..32); 0: from the batch size */
+  int32_t helper_warps;   /* idle warps that stay for exported subtrees; 0: 2 per SM */
+  int32_t reserved;
+} p2c_batch_tuning;
+
+size_t p2c_batch_certify_workspace_bytes(int32_t n_scenes);
+
+/* Certificates of every candidate pair of every scene of a batch in ONE
+ * persistent launch: the scenes' VF lists then EE lists form two global
+ * queues that all warps drain together, so small and large scenes share the
+ * GPU.  Per scene, summaries_dev[s] (may be NULL) receives the
+ * CertificateEngine::Evaluate reduction exactly as p2c_scene_certify writes
+ * it; undecided candidates are appended to undecided_queue_dev (may be NULL)
+ * as (scene << 40 | (family - 1) << 39 | pair position).  No host sync; the
+ * sizes are read on the device.  tuning may be NULL (defaults). */
+int p2c_batch_certify(const p2c_batch_scene* scenes_dev, int32_t n_scenes, double interval_t0, double interval_t1,
+                      const p2c_cert_config* config, uint32_t family_mask, p2c_scene_summary* summaries_dev,
+                      uint64_t* undecided_queue_dev, int64_t undecided_cap, const p2c_batch_tuning* tuning,
+                      void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- candidate groups: scheduled any-hit with fallback replay ------------ */
 /* Per-call totals of p2c_group_anyhit. */
 typedef struct p2c_anyhit_summary {

@@ -309,6 +309,7 @@ def ref_tool() -> ctypes.CDLL:
         T.ref_tool_random_scores.argtypes = [ci, vp]
         T.ref_tool_anyhit.argtypes = [ci, u64, f64, f64, ci, vp]
         T.ref_tool_time_step.argtypes = [u64, f64, f64, ci, vp, vp, vp]
+        T.ref_tool_time_all_exact.argtypes = [f64, f64, ci, vp, vp]
         _ref_tool = T
     return _ref_tool
 
@@ -367,3 +368,12 @@ class RefToolScene:
             raise ValueError(T.ref_tool_last_error().decode())
         return {"candidates_s": float(secs[0]), "anyhit_vf_s": float(secs[1]), "anyhit_ee_s": float(secs[2]),
                 "calls": int(calls.sum()), "candidates": int(cands.sum())}
+
+    def time_all_exact(self, eps_time: float, eps_space: float, max_depth: int) -> dict:
+        """The tool's candidates + every-candidate certificates of both families, timed inside the library."""
+        secs = np.zeros(2)
+        calls = np.zeros(1, dtype=np.uint64)
+        T = ref_tool()
+        if T.ref_tool_time_all_exact(eps_time, eps_space, max_depth, _p(secs), _p(calls)):
+            raise ValueError(T.ref_tool_last_error().decode())
+        return {"candidates_s": float(secs[0]), "certify_s": float(secs[1]), "calls": int(calls[0])}

@@ -268,4 +268,39 @@ int ref_tool_time_step(std::uint64_t top_k, double eps_time, double eps_space, i
   return 0;
 }
 
+// One timed every-candidate step of the tool on the prepared scene (its
+// RunAllExactRows, :1239-1281, for both families after the candidate sweep),
+// single-threaded.  seconds[0..1] = {candidates, certificates}; returns the
+// number of certified candidates through *calls.
+int ref_tool_time_all_exact(double eps_time, double eps_space, int max_depth, double* seconds,
+                            std::uint64_t* calls) {
+  if (!g_scene_ready) return 1;
+  g_tool_config.eps_time = eps_time;
+  g_tool_config.eps_space = eps_space;
+  g_tool_config.max_subdivision_depth = static_cast<std::uint16_t>(max_depth);
+  Args args;
+  try {
+    const auto t0 = std::chrono::steady_clock::now();
+    bool c0 = false, c1 = false;
+    g_candidates[0] = BuildVFCandidates(g_scene, 0, &c0);
+    g_candidates[1] = BuildEECandidates(g_scene, 0, &c1);
+    const auto t1 = std::chrono::steady_clock::now();
+    std::uint64_t n = 0;
+    for (int kind = 0; kind < 2; ++kind) {
+      std::unordered_map<std::uint64_t, GroupTruth> truth;
+      const MethodRow row =
+          RunAllExactRows(g_scene, args, kind == 0 ? "vf" : "ee", g_candidates[kind], false, 0.0, &truth);
+      n += row.exact_calls;
+    }
+    const auto t2 = std::chrono::steady_clock::now();
+    seconds[0] = std::chrono::duration<double>(t1 - t0).count();
+    seconds[1] = std::chrono::duration<double>(t2 - t1).count();
+    *calls = n;
+  } catch (const std::exception& e) {
+    g_tool_error = e.what();
+    return 1;
+  }
+  return 0;
+}
+
 }  // extern "C"

@@ -122,3 +122,47 @@ def cloth_on_sphere(n: int = 513, sphere_lon: int = 250, sphere_rings: int = 200
     s["spec"] = {"kind": "cloth_on_sphere", "cloth_n": n, "cloth_triangles": int(len(cf)),
                  "sphere_triangles": int(len(sf)), "seed": seed, "gap": gap, "drop": drop}
     return s
+
+
+def _rotation(axis: np.ndarray, angle: float) -> np.ndarray:
+    a = axis / np.linalg.norm(axis)
+    k = np.array([[0.0, -a[2], a[1]], [a[2], 0.0, -a[0]], [-a[1], a[0], 0.0]])
+    return np.eye(3) + np.sin(angle) * k + (1.0 - np.cos(angle)) * (k @ k)
+
+
+def uneven_batch(n_scenes: int = 256, tri_min: float = 1.0e3, tri_max: float = 2.0e5, seed: int = 20261203,
+                 jitter: float = 1.0e-3) -> list[dict]:
+    """Independent two-sphere scenes of uneven size: total triangle counts
+    log-uniform over [tri_min, tri_max]; each scene is two UV spheres of half
+    that count, sphere A turning slightly (up to 0.02 rad) about a random
+    axis, sphere B starting gap ~ U[0.01, 0.03] away along a random direction
+    and moving rigidly (rotation up to 0.05 rad) toward A to a penetration
+    depth of 0.25 f at t1, f ~ U[5%, 40%] the scene's contact parameter (the
+    share of candidates that then hit is measured, not imposed);
+    per-vertex N(0, jitter) at t0 and t1."""
+    g = rng(seed)
+    out = []
+    for i in range(n_scenes):
+        tris = float(np.exp(g.uniform(np.log(tri_min), np.log(tri_max))))
+        rings = max(3, int(round(np.sqrt(tris / 5.0))))
+        lon = max(4, int(round(tris / 2.0 / (2.0 * rings))))
+        v, f = uv_sphere(lon, rings)
+        e = unique_edges(f)
+        frac = float(g.uniform(0.05, 0.40))
+        gap = float(g.uniform(0.01, 0.03))
+        u = g.normal(size=3)
+        u /= np.linalg.norm(u)
+        ra1 = _rotation(g.normal(size=3), float(g.uniform(0.0, 0.02)))
+        rb0 = _rotation(g.normal(size=3), float(g.uniform(0.0, np.pi)))
+        rb1 = _rotation(g.normal(size=3), float(g.uniform(0.0, 0.05))) @ rb0
+        cb0 = (2.0 + gap) * u
+        cb1 = (2.0 - 0.25 * frac) * u
+        a0 = v + g.normal(0.0, jitter, v.shape)
+        a1 = v @ ra1.T + g.normal(0.0, jitter, v.shape)
+        b0 = v @ rb0.T + cb0 + g.normal(0.0, jitter, v.shape)
+        b1 = v @ rb1.T + cb1 + g.normal(0.0, jitter, v.shape)
+        s = combine([(a0, a1, f, e), (b0, b1, f, e)])
+        s["spec"] = {"kind": "uneven_batch_scene", "index": i, "n_lon": lon, "n_rings": rings,
+                     "triangles": int(2 * len(f)), "contact_parameter": frac, "gap": gap, "seed": seed}
+        out.append(s)
+    return out

@@ -1,0 +1,105 @@
+"""GPU parity of batched scenes (p2c_batch_certify): every scene of an
+uneven batch certified in one launch gets exactly the candidates, the
+certificates and the Evaluate summary that the single-scene path gives, and
+every certificate equals the oracle's byte for byte."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+import torch
+
+import anyhit_case as A
+
+pytestmark = pytest.mark.gpu
+
+
+def _small_batch(n=9, seed=7):
+    from p2cccd_b200 import scenes
+
+    return scenes.uneven_batch(n, tri_min=200, tri_max=6000, seed=seed)
+
+
+def _cands(pairs):
+    return np.stack([(pairs >> np.uint64(32)).astype(np.int64), (pairs & np.uint64(0xffffffff)).astype(np.int64)], 1)
+
+
+def _bytes(a):
+    return np.ascontiguousarray(a).view(np.uint8).reshape(-1, 72)
+
+
+@pytest.mark.parametrize("depth", [32, 4])
+def test_batch_matches_single_scene_and_oracle(cuda_device, oracle_mod, depth):
+    from p2cccd_b200.batch import BatchPipeline
+    from p2cccd_b200.certify import CertConfig
+    from p2cccd_b200.scene import ScenePipeline
+
+    cfg = CertConfig(1e-6, 1e-6, depth)
+    batch = _small_batch()
+    bp = BatchPipeline(batch, cuda_device, config=cfg, streams=3)
+    summ = bp.step_checked()
+    bp.capture()
+    bp.replay()
+    bp.replay()
+    torch.cuda.synchronize(cuda_device)
+    summ_graph = bp.read_summaries()
+    assert summ_graph == summ
+    total_undecided = 0
+    for i, s in enumerate(batch):
+        sp = ScenePipeline(s, cuda_device, config=cfg)
+        single = sp.step_checked()
+        assert summ[i] == single, i
+        vf, ee = bp.pairs(i)
+        svf, see = sp.pairs()
+        assert np.array_equal(vf, svf) and np.array_equal(ee, see)
+        rvf, ree = bp.results(i)
+        srvf, sree = sp.results()
+        assert np.array_equal(_bytes(rvf), _bytes(srvf)) and np.array_equal(_bytes(ree), _bytes(sree))
+        for kind, pairs, res in (("vf", vf, rvf), ("ee", ee, ree)):
+            if len(pairs) == 0:
+                continue
+            rec = A.primitives(s, s["edges"], _cands(pairs), kind)
+            cpu, st, _ = oracle_mod.eval_batch(rec, 0.0, 1.0, cfg.eps_time, cfg.eps_space, depth)
+            assert st.sum() == 0
+            assert np.array_equal(_bytes(cpu), _bytes(res)), (i, kind)
+        total_undecided += summ[i]["undecided"]
+    # undecided queue: (scene << 40 | family << 39 | position), one entry per undecided certificate
+    n_q = min(sum(x["undecided_queued"] for x in summ), bp.undecided_capacity)
+    assert n_q == total_undecided
+    entries = bp.undecided_queue[:n_q].cpu().numpy().view(np.uint64)
+    for e in entries[:200]:
+        sc, fam, pos = int(e >> np.uint64(40)), int((e >> np.uint64(39)) & np.uint64(1)), int(e & np.uint64((1 << 39) - 1))
+        res = bp.results(sc)[fam]
+        assert res[pos]["status"] == 2
+    if depth == 4:
+        assert total_undecided > 0
+
+
+def test_batch_autotune_keeps_results(cuda_device, tmp_path):
+    from p2cccd_b200.batch import BatchPipeline
+    from p2cccd_b200.certify import CertConfig
+
+    cfg = CertConfig(1e-6, 1e-6, 32)
+    bp = BatchPipeline(_small_batch(12, seed=3), cuda_device, config=cfg)
+    summ = bp.step_checked()
+    before = [tuple(map(_bytes, bp.results(i))) for i in range(bp.n)]
+    best = bp.autotune(reps=2, cache=tmp_path / "tune.json")
+    assert best["ms"] > 0 and best["streams"] in (1, 4, 8, 16)
+    cached = bp.autotune(reps=2, cache=tmp_path / "tune.json")
+    assert cached.get("cached") is True
+    bp.replay()
+    torch.cuda.synchronize(cuda_device)
+    assert bp.read_summaries() == summ
+    for i in range(bp.n):
+        after = tuple(map(_bytes, bp.results(i)))
+        assert all(np.array_equal(a, b) for a, b in zip(before[i], after))
+
+
+def test_batch_rejects_bad_arguments(cuda_device):
+    from p2cccd_b200.batch import BatchPipeline, BatchTuning
+
+    bp = BatchPipeline(_small_batch(2, seed=1), cuda_device)
+    bp.tuning = BatchTuning(0, 33, 0, 0)
+    with pytest.raises(ValueError):
+        bp.certify()
+    with pytest.raises(ValueError):
+        BatchPipeline([], cuda_device)
