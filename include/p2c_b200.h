@@ -321,21 +321,46 @@ int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, 
                           p2c_point_triangle* vf_records_dev, p2c_edge_edge* ee_records_dev, void* stream);
 
 /* ---- batches: many scenes certified in one launch ------------------------ */
-/* One scene of a batch: its geometry (scene-local indices), the candidate
- * pairs p2c_scene_candidates wrote for it, and where its certificates go.
- * An array of these lives in device memory. */
+/* One scene of a batch: its geometry (scene-local indices) and object ids,
+ * its candidate pair buffers and counts (written by p2c_batch_candidates or
+ * p2c_scene_candidates) and where its certificates go.  An array of these
+ * lives in device memory (and, for p2c_batch_candidates, a host copy). */
 typedef struct p2c_batch_scene {
   const double* v_t0;              /* nv x 3 */
   const double* v_t1;              /* nv x 3 */
   const int32_t* faces;            /* nf x 3 */
   const int32_t* edges;            /* ne x 2 */
-  const uint64_t* vf_pairs;        /* vf_cap entries */
-  const uint64_t* ee_pairs;        /* ee_cap entries */
+  uint64_t* vf_pairs;              /* vf_cap entries */
+  uint64_t* ee_pairs;              /* ee_cap entries */
   int64_t vf_cap, ee_cap;
-  const uint64_t* counts;          /* candidate counts: n = min(counts[k], cap) */
+  uint64_t* counts;                /* 4 entries, as p2c_scene_candidates writes them */
   p2c_interval_result* vf_results; /* vf_cap entries */
   p2c_interval_result* ee_results; /* ee_cap entries */
+  const int32_t* v_obj;            /* nv object ids (< 0: vertex in no face) */
+  const int32_t* f_obj;            /* nf */
+  const int32_t* e_obj;            /* ne */
+  int64_t nv, nf, ne;
+  double thickness;
+  int32_t exclude_self;
+  int32_t n_obj;
 } p2c_batch_scene;
+
+/* Workspace of p2c_batch_candidates for the scenes of a host table. */
+size_t p2c_batch_candidates_workspace_bytes(const p2c_batch_scene* scenes_host, int32_t n_scenes);
+
+/* Swept-AABB candidates of every scene of a batch in one launch sequence
+ * (about 35 launches whatever the number of scenes): the algorithm of
+ * p2c_scene_candidates with scene-segmented reductions, one radix sort of
+ * (scene, list, column, quantised minimum) keys over all primitives, per
+ * scene column grids and sweeps that stay inside their scene, then one sort
+ * of all scenes' pairs.  Each scene's pairs are written sorted and padded
+ * with ~0 up to its capacity (the order p2c_scene_candidates with
+ * sort_pairs = 1 writes) and its counts as p2c_scene_candidates writes them.
+ * scenes_host is read on the host for the sizes (nv, nf, ne, caps); the
+ * kernels read scenes_dev (the same table in device memory).  Every scene
+ * needs nv, nf, ne < 2^22. */
+int p2c_batch_candidates(const p2c_batch_scene* scenes_host, const p2c_batch_scene* scenes_dev, int32_t n_scenes,
+                         void* workspace_dev, size_t workspace_bytes, void* stream);
 
 /* Launch shape of the batch certifier (the autotuned parameters). */
 typedef struct p2c_batch_tuning {

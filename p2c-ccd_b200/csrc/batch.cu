@@ -20,7 +20,7 @@
 namespace p2c {
 namespace {
 
-static_assert(sizeof(p2c_batch_scene) == 88, "p2c_batch_scene layout");
+static_assert(sizeof(p2c_batch_scene) == 152, "p2c_batch_scene layout");
 static_assert(sizeof(p2c_batch_tuning) == 16, "p2c_batch_tuning layout");
 
 constexpr int kPrepThreads = 1024;

@@ -47,9 +47,6 @@ namespace {
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
-__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
-
 inline unsigned grid_for(long long n, int threads) {
   const long long g = (n + threads - 1) / threads;
   return (unsigned)(g > 0 ? g : 1);
@@ -73,35 +70,6 @@ __global__ void init_scratch_kernel(BroadScratch* sc) {
     sc->list[t / 3].lo_min[t % 3] = ~0ull;
     sc->list[t / 3].hi_max[t % 3] = 0ull;
   }
-}
-
-template <int K>
-__device__ __forceinline__ bool swept_box(const double* __restrict__ v_t0, const double* __restrict__ v_t1,
-                                          const int32_t* __restrict__ prim, long long i, double thickness,
-                                          double b[6]) {
-  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
-  bool finite = true;
-#pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const long long v = K == 1 ? i : (long long)__ldg(prim + K * i + k);
-#pragma unroll
-    for (int f = 0; f < 2; ++f) {
-      const double* p = (f == 0 ? v_t0 : v_t1) + 3 * v;
-#pragma unroll
-      for (int a = 0; a < 3; ++a) {
-        const double x = __ldg(p + a);
-        finite = finite && isfinite(x);
-        mn[a] = dmin(mn[a], x);
-        mx[a] = dmax(mx[a], x);
-      }
-    }
-  }
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {  // Expand(box, thickness), :263-270
-    b[a] = __dsub_rn(mn[a], thickness);
-    b[3 + a] = __dadd_rn(mx[a], thickness);
-  }
-  return finite;
 }
 
 // Swept boxes of all primitives (Extend/Expand/Swept*Box,
@@ -306,17 +274,6 @@ __global__ void grid_kernel(BroadScratch* sc) {
   sc->grid = g;
 }
 
-__device__ __forceinline__ int column(double x, double base, double inv, int g) {
-  const double c = floor((x - base) * inv);
-  return c < 0.0 ? 0 : (c >= (double)g ? g - 1 : (int)c);
-}
-
-// Monotone (non-decreasing) in x: the sweep windows rely on it.
-__device__ __forceinline__ unsigned quantise(double x, const Grid& g) {
-  const double c = floor((x - g.base0) * g.scale0);
-  return c < 0.0 ? 0u : (c >= (double)kQMax ? kQMax : (unsigned)c);
-}
-
 __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned char* __restrict__ active,
                                                         unsigned* __restrict__ keys, unsigned* __restrict__ vals,
                                                         const BroadScratch* sc) {
@@ -377,59 +334,6 @@ __device__ __forceinline__ void append_pair(bool found, unsigned long long key, 
     const unsigned long long slot = base + (unsigned long long)__popc(mask & ((1u << lane) - 1u));
     if (slot < cap) out[slot] = key;
   }
-}
-
-// Walk over the candidate entries of one scanning box: the columns its
-// partners' min corners can lie in, and in each the quantised window
-// [q(lo), q(hi)] of the partner list.
-struct Walker {
-  int c1, c1_end, c2_begin, c2, c2_end;
-  unsigned j, j_end, q_lo, q_hi;
-
-  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g) {
-    for (;;) {
-      if (++c2 > c2_end) {
-        c2 = c2_begin;
-        if (++c1 > c1_end) return false;
-      }
-      const int cell = c1 * g.g2 + c2;
-      unsigned b = Q.cell_begin[cell], e = Q.cell_end[cell];
-      const unsigned end = e;
-      while (b < e) {  // first entry with q >= q_lo
-        const unsigned m = (b + e) >> 1;
-        if (Q.q[m] < q_lo) b = m + 1;
-        else e = m;
-      }
-      j = b;
-      j_end = end;
-      if (j < j_end && Q.q[j] <= q_hi) return true;
-    }
-  }
-};
-
-__device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double lo, double hi, double alo, double ahi,
-                                            double blo, double bhi, double reach1, double reach2) {
-  // widen the lower columns by a relative 2^-40 so that the rounding of
-  // alo - reach can never skip the column of a partner's min corner
-  const double l1 = alo - reach1 - (fabs(alo) + reach1) * 0x1p-40;
-  const double l2 = blo - reach2 - (fabs(blo) + reach2) * 0x1p-40;
-  w.c1 = column(l1, g.base1, g.inv1, g.g1);
-  w.c1_end = column(ahi, g.base1, g.inv1, g.g1);
-  w.c2_begin = column(l2, g.base2, g.inv2, g.g2);
-  w.c2_end = column(bhi, g.base2, g.inv2, g.g2);
-  w.c2 = w.c2_begin - 1;
-  w.j = w.j_end = 0;
-  w.q_lo = quantise(lo, g);
-  w.q_hi = quantise(hi, g);
-}
-
-__device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, const SortedBoxes& Q, long long j) {
-  return P.lo[i] <= Q.hi[j] && Q.lo[j] <= P.hi[i] && P.alo[i] <= Q.ahi[j] && Q.alo[j] <= P.ahi[i] &&
-         P.blo[i] <= Q.bhi[j] && Q.blo[j] <= P.bhi[i];
-}
-
-__device__ __forceinline__ unsigned long long pair_key(unsigned a, unsigned b, int pack_shift) {
-  return pack_shift > 0 ? (((unsigned long long)a << pack_shift) | b) : (((unsigned long long)a << 32) | b);
 }
 
 // Vertex-face pairs: threads [0, nv) scan faces from a vertex and own the

@@ -80,4 +80,106 @@ struct BroadScratch {
   unsigned long long error_word;  // bit 0: non-finite coordinate
 };
 
+
+// ---- device helpers shared by the single-scene and batched sweeps ---------
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; }  // std::min
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; }  // std::max
+
+// Swept box of a primitive with K vertices (Extend/Expand/Swept*Box,
+// scene_object_envelope_native_ti_walltime.cpp:256-301): min/max over the
+// t0 and t1 positions, then +-thickness.  Returns false on a non-finite
+// coordinate.
+template <int K>
+__device__ __forceinline__ bool swept_box(const double* __restrict__ v_t0, const double* __restrict__ v_t1,
+                                          const int32_t* __restrict__ prim, long long i, double thickness,
+                                          double b[6]) {
+  double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+  bool finite = true;
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const long long v = K == 1 ? i : (long long)__ldg(prim + K * i + k);
+#pragma unroll
+    for (int f = 0; f < 2; ++f) {
+      const double* p = (f == 0 ? v_t0 : v_t1) + 3 * v;
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        const double x = __ldg(p + a);
+        finite = finite && isfinite(x);
+        mn[a] = dmin(mn[a], x);
+        mx[a] = dmax(mx[a], x);
+      }
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {  // Expand(box, thickness), :263-270
+    b[a] = __dsub_rn(mn[a], thickness);
+    b[3 + a] = __dadd_rn(mx[a], thickness);
+  }
+  return finite;
+}
+
+__device__ __forceinline__ int column(double x, double base, double inv, int g) {
+  const double c = floor((x - base) * inv);
+  return c < 0.0 ? 0 : (c >= (double)g ? g - 1 : (int)c);
+}
+
+// Monotone (non-decreasing) in x: the sweep windows rely on it.
+__device__ __forceinline__ unsigned quantise(double x, const Grid& g) {
+  const double c = floor((x - g.base0) * g.scale0);
+  return c < 0.0 ? 0u : (c >= (double)kQMax ? kQMax : (unsigned)c);
+}
+
+// Walk over the candidate entries of one scanning box: the columns its
+// partners' min corners can lie in, and in each the quantised window
+// [q(lo), q(hi)] of the partner list.
+struct Walker {
+  int c1, c1_end, c2_begin, c2, c2_end;
+  unsigned j, j_end, q_lo, q_hi;
+
+  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g) {
+    for (;;) {
+      if (++c2 > c2_end) {
+        c2 = c2_begin;
+        if (++c1 > c1_end) return false;
+      }
+      const int cell = c1 * g.g2 + c2;
+      unsigned b = Q.cell_begin[cell], e = Q.cell_end[cell];
+      const unsigned end = e;
+      while (b < e) {  // first entry with q >= q_lo
+        const unsigned m = (b + e) >> 1;
+        if (Q.q[m] < q_lo) b = m + 1;
+        else e = m;
+      }
+      j = b;
+      j_end = end;
+      if (j < j_end && Q.q[j] <= q_hi) return true;
+    }
+  }
+};
+
+__device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double lo, double hi, double alo, double ahi,
+                                            double blo, double bhi, double reach1, double reach2) {
+  // widen the lower columns by a relative 2^-40 so that the rounding of
+  // alo - reach can never skip the column of a partner's min corner
+  const double l1 = alo - reach1 - (fabs(alo) + reach1) * 0x1p-40;
+  const double l2 = blo - reach2 - (fabs(blo) + reach2) * 0x1p-40;
+  w.c1 = column(l1, g.base1, g.inv1, g.g1);
+  w.c1_end = column(ahi, g.base1, g.inv1, g.g1);
+  w.c2_begin = column(l2, g.base2, g.inv2, g.g2);
+  w.c2_end = column(bhi, g.base2, g.inv2, g.g2);
+  w.c2 = w.c2_begin - 1;
+  w.j = w.j_end = 0;
+  w.q_lo = quantise(lo, g);
+  w.q_hi = quantise(hi, g);
+}
+
+__device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, const SortedBoxes& Q, long long j) {
+  return P.lo[i] <= Q.hi[j] && Q.lo[j] <= P.hi[i] && P.alo[i] <= Q.ahi[j] && Q.alo[j] <= P.ahi[i] &&
+         P.blo[i] <= Q.bhi[j] && Q.blo[j] <= P.bhi[i];
+}
+
+__device__ __forceinline__ unsigned long long pair_key(unsigned a, unsigned b, int pack_shift) {
+  return pack_shift > 0 ? (((unsigned long long)a << pack_shift) | b) : (((unsigned long long)a << 32) | b);
+}
+
 }  // namespace p2c

@@ -67,6 +67,8 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_scene_materialize": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _i64, _c_void_p, _c_void_p,
                                      _c_void_p]),
     "p2c_batch_certify_workspace_bytes": (_size, [ctypes.c_int32]),
+    "p2c_batch_candidates_workspace_bytes": (_size, [_c_void_p, ctypes.c_int32]),
+    "p2c_batch_candidates": (_int, [_c_void_p, _c_void_p, ctypes.c_int32, _c_void_p, _size, _c_void_p]),
     "p2c_batch_certify": (_int, [_c_void_p, ctypes.c_int32, _f64, _f64, ctypes.POINTER(CertConfig), ctypes.c_uint32,
                                  _c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p, _size, _c_void_p]),
     "p2c_group_anyhit_workspace_bytes": (_size, [_i64, ctypes.c_int32]),

@@ -32,9 +32,17 @@ from .scene import SUMMARY_DTYPE, SceneStruct
 BATCH_SCENE_DTYPE = np.dtype([
     ("v_t0", "<u8"), ("v_t1", "<u8"), ("faces", "<u8"), ("edges", "<u8"), ("vf_pairs", "<u8"),
     ("ee_pairs", "<u8"), ("vf_cap", "<i8"), ("ee_cap", "<i8"), ("counts", "<u8"), ("vf_results", "<u8"),
-    ("ee_results", "<u8"),
+    ("ee_results", "<u8"), ("v_obj", "<u8"), ("f_obj", "<u8"), ("e_obj", "<u8"), ("nv", "<i8"), ("nf", "<i8"),
+    ("ne", "<i8"), ("thickness", "<f8"), ("exclude_self", "<i4"), ("n_obj", "<i4"),
 ])
-assert BATCH_SCENE_DTYPE.itemsize == 88
+assert BATCH_SCENE_DTYPE.itemsize == 152
+
+
+def scene_row(st, vf_pairs: int, ee_pairs: int, vf_cap: int, ee_cap: int, counts: int, vf_results: int,
+              ee_results: int) -> tuple:
+    """One p2c_batch_scene row from a SceneStruct and the scene's buffers."""
+    return (st.v_t0, st.v_t1, st.faces, st.edges, vf_pairs, ee_pairs, vf_cap, ee_cap, counts, vf_results,
+            ee_results, st.v_obj, st.f_obj, st.e_obj, st.nv, st.nf, st.ne, st.thickness, st.exclude_self, st.n_obj)
 
 
 class BatchTuning(ctypes.Structure):
@@ -56,7 +64,7 @@ class BatchPipeline:
     def __init__(self, scenes: list[dict], device: str | torch.device = "cuda", *, thickness: float = 0.0,
                  exclude_self: bool = True, config: CertConfig = CertConfig(),
                  interval: tuple[float, float] = (0.0, 1.0), family_mask: int = 3, streams: int = 8,
-                 undecided_capacity: int = 1 << 16):
+                 undecided_capacity: int = 1 << 16, broad: str = "batched"):
         if not scenes:
             raise ValueError("a batch needs at least one scene")
         self.lib = _lib.load()
@@ -68,6 +76,9 @@ class BatchPipeline:
         self.thickness = float(thickness)
         self.exclude_self = bool(exclude_self)
         self.n_streams = max(1, int(streams))
+        if broad not in ("batched", "per_scene"):
+            raise ValueError("broad must be 'batched' or 'per_scene'")
+        self.broad = broad
         self.tuning = BatchTuning(0, 0, 0, 0)
         # concatenated geometry; each scene's slice starts on a 256-byte boundary
         nv = [len(s["v_t0"]) for s in scenes]
@@ -146,14 +157,15 @@ class BatchPipeline:
         self.bp_ws = torch.empty(int(self.bp_ws_off[-1]), dtype=torch.uint8, device=d)
         table = np.zeros(self.n, dtype=BATCH_SCENE_DTYPE)
         for i, st in enumerate(self.structs):
-            table[i] = (st.v_t0, st.v_t1, st.faces, st.edges,
-                        self.vf_pairs.data_ptr() + 8 * int(self.vf_pair_off[i]),
-                        self.ee_pairs.data_ptr() + 8 * int(self.ee_pair_off[i]), self.vf_caps[i], self.ee_caps[i],
-                        self.counts.data_ptr() + 32 * i,
-                        self.vf_results.data_ptr() + 72 * int(self.vf_pair_off[i]),
-                        self.ee_results.data_ptr() + 72 * int(self.ee_pair_off[i]))
+            table[i] = scene_row(st, self.vf_pairs.data_ptr() + 8 * int(self.vf_pair_off[i]),
+                                 self.ee_pairs.data_ptr() + 8 * int(self.ee_pair_off[i]), self.vf_caps[i],
+                                 self.ee_caps[i], self.counts.data_ptr() + 32 * i,
+                                 self.vf_results.data_ptr() + 72 * int(self.vf_pair_off[i]),
+                                 self.ee_results.data_ptr() + 72 * int(self.ee_pair_off[i]))
         self.table_host = table
         self.table = torch.from_numpy(table.view(np.uint8).copy()).to(d)
+        self.bb_ws = torch.empty(int(self.lib.p2c_batch_candidates_workspace_bytes(table.ctypes.data, self.n)),
+                                 dtype=torch.uint8, device=d)
         self.graph = None
 
     def update_positions(self, v_t0: torch.Tensor, v_t1: torch.Tensor) -> None:
@@ -163,8 +175,17 @@ class BatchPipeline:
 
     # -- hot path ---------------------------------------------------------
     def candidates(self) -> None:
-        """Candidate generation of every scene, round-robin over the side
-        streams (they join the current stream before returning)."""
+        """Candidate generation of every scene: one batched launch sequence
+        (``broad="batched"``, the default) or one p2c_scene_candidates per
+        scene round-robin over side streams (``broad="per_scene"``)."""
+        if self.broad == "batched":
+            _lib.check(self.lib.p2c_batch_candidates(self.table_host.ctypes.data, self.table.data_ptr(), self.n,
+                                                     self.bb_ws.data_ptr(), self.bb_ws.numel(),
+                                                     _stream_ptr(self.device)))
+            return
+        self._candidates_per_scene()
+
+    def _candidates_per_scene(self) -> None:
         main = torch.cuda.current_stream(self.device)
         if not hasattr(self, "_side") or len(self._side) != self.n_streams:
             self._side = [torch.cuda.Stream(self.device) for _ in range(self.n_streams)]
@@ -312,16 +333,18 @@ class BatchPipeline:
         trials.sort()
         _, bps, fetch, helpers = trials[0]
         self.tuning = BatchTuning(bps, fetch, helpers, 0)
-        stream_trials = []
-        for ns in (1, 4, 8, 16):
-            self.n_streams = ns
-            self.graph = None
-            stream_trials.append((self._time_replays(reps), ns))
-        stream_trials.sort()
+        stream_trials = [(trials[0][0], self.n_streams)]
+        if self.broad == "per_scene":  # the per-scene broad phase fans out over side streams
+            stream_trials = []
+            for ns in (1, 4, 8, 16):
+                self.n_streams = ns
+                self.graph = None
+                stream_trials.append((self._time_replays(reps), ns))
+            stream_trials.sort()
         self.n_streams = stream_trials[0][1]
         self.graph = None
         best = {"blocks_per_sm": bps, "fetch_limit": fetch, "helper_warps": helpers, "streams": self.n_streams,
-                "ms": stream_trials[0][0], "trials": len(trials) + len(stream_trials)}
+                "broad": self.broad, "ms": stream_trials[0][0], "trials": len(trials) + len(stream_trials)}
         if key is not None:
             path = Path(cache)
             known = json.loads(path.read_text()) if path.exists() else {}

@@ -9,7 +9,8 @@ and the device memory the in-flight requests hold stays under the budget;
 the requests admitted together form one group on the slot's own CUDA stream:
 
     host -> device copies of the trajectories,
-    swept-AABB candidates of every request (p2c_scene_candidates),
+    swept-AABB candidates of every request in one batched launch sequence
+    (p2c_batch_candidates),
     ONE certification launch over the whole group (p2c_batch_certify), its
     undecided certificates appended to the group's fallback-replay queue,
     device -> host copies of the per-request summaries (and certificates),
@@ -35,7 +36,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .batch import BATCH_SCENE_DTYPE, BatchTuning
+from .batch import BATCH_SCENE_DTYPE, BatchTuning, scene_row
 from .certify import CertConfig
 from .records import INTERVAL_RESULT_DTYPE, QUERY_CERTIFICATE_DTYPE
 from .scene import SUMMARY_DTYPE, SceneStruct
@@ -87,11 +88,11 @@ class _Group:
 
 
 def _request_bytes(m: Mesh) -> int:
-    """Device bytes one in-flight request holds (trajectories, pairs,
-    certificates, candidate workspace)."""
-    lib = _lib.load()
-    ws = int(lib.p2c_scene_candidates_workspace_bytes(m.nv, m.nf, m.ne, m.vf_cap, m.ee_cap))
-    return 48 * m.nv + (8 + 72) * (m.vf_cap + m.ee_cap) + ws + 4096
+    """Device bytes one in-flight request holds: trajectories, pairs,
+    certificates, and its share of the batched candidate workspace (about
+    150 bytes per primitive plus 16 per pair slot)."""
+    prims = m.nv + m.nf + m.ne
+    return 48 * m.nv + (8 + 72) * (m.vf_cap + m.ee_cap) + 150 * prims + 16 * (m.vf_cap + m.ee_cap) + 4096
 
 
 class ServeEngine:
@@ -190,9 +191,6 @@ class ServeEngine:
                 ee = torch.empty(m.ee_cap, dtype=torch.int64, device=d)
                 rvf = torch.empty((m.vf_cap, 72), dtype=torch.uint8, device=d)
                 ree = torch.empty((m.ee_cap, 72), dtype=torch.uint8, device=d)
-                ws = torch.empty(int(self.lib.p2c_scene_candidates_workspace_bytes(m.nv, m.nf, m.ne, m.vf_cap,
-                                                                                    m.ee_cap)),
-                                 dtype=torch.uint8, device=d)
                 st = SceneStruct()
                 st.v_t0, st.v_t1 = v0.data_ptr(), v1.data_ptr()
                 st.faces, st.edges = m.faces.data_ptr(), m.edges.data_ptr()
@@ -201,16 +199,17 @@ class ServeEngine:
                 st.thickness = m.thickness
                 st.exclude_self = 1 if m.exclude_self else 0
                 st.n_obj = m.n_obj
-                _lib.check(self.lib.p2c_scene_candidates(ctypes.byref(st), vf.data_ptr(), m.vf_cap, ee.data_ptr(),
-                                                         m.ee_cap, counts.data_ptr() + 32 * i, 1, ws.data_ptr(),
-                                                         ws.numel(), stream.cuda_stream))
-                table[i] = (v0.data_ptr(), v1.data_ptr(), m.faces.data_ptr(), m.edges.data_ptr(), vf.data_ptr(),
-                            ee.data_ptr(), m.vf_cap, m.ee_cap, counts.data_ptr() + 32 * i, rvf.data_ptr(),
-                            ree.data_ptr())
-                keep.append((v0, v1, vf, ee, rvf, ree, ws, (m.vf_cap, m.ee_cap)))
+                table[i] = scene_row(st, vf.data_ptr(), ee.data_ptr(), m.vf_cap, m.ee_cap, counts.data_ptr() + 32 * i,
+                                     rvf.data_ptr(), ree.data_ptr())
+                keep.append((v0, v1, vf, ee, rvf, ree, None, (m.vf_cap, m.ee_cap)))
             h_table = torch.from_numpy(table.view(np.uint8).copy()).pin_memory()
             d_table = torch.empty_like(h_table, device=d)
             d_table.copy_(h_table, non_blocking=True)
+            # every request's candidates in one batched launch sequence
+            ws_bb = torch.empty(int(self.lib.p2c_batch_candidates_workspace_bytes(table.ctypes.data, n)),
+                                dtype=torch.uint8, device=d)
+            _lib.check(self.lib.p2c_batch_candidates(table.ctypes.data, d_table.data_ptr(), n, ws_bb.data_ptr(),
+                                                     ws_bb.numel(), stream.cuda_stream))
             summaries = torch.empty((n, SUMMARY_DTYPE.itemsize), dtype=torch.uint8, device=d)
             ws_cert = torch.empty(int(self.lib.p2c_batch_certify_workspace_bytes(n)), dtype=torch.uint8, device=d)
             uq = torch.empty(self.undecided_capacity, dtype=torch.int64, device=d)
@@ -236,6 +235,7 @@ class ServeEngine:
                     h_res.append(None)
             g.event.record(stream)
         g.tensors = {"keep": keep, "h_table": h_table, "d_table": d_table, "summaries": summaries, "ws": ws_cert,
+                     "ws_bb": ws_bb,
                      "counts": counts, "h_sum": h_sum, "h_cnt": h_cnt, "h_res": h_res, "uq": uq, "h_uq": h_uq}
         self.busy[slot] = g
         self.in_flight_bytes += nbytes

@@ -103,3 +103,49 @@ def test_batch_rejects_bad_arguments(cuda_device):
         bp.certify()
     with pytest.raises(ValueError):
         BatchPipeline([], cuda_device)
+
+
+@pytest.mark.parametrize("exclude_self,thickness", [(True, 0.0), (False, 0.0), (False, 2e-3)])
+def test_batched_candidates_equal_per_scene(cuda_device, oracle_mod, exclude_self, thickness):
+    """p2c_batch_candidates writes every scene's pair buffer (pairs sorted,
+    ~0 padding) and counts exactly as p2c_scene_candidates does per scene,
+    with self pairs, thickness, far-apart scenes with no candidates and
+    scenes of many objects."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.batch import BatchPipeline
+    from p2cccd_b200.certify import CertConfig
+
+    batch = _small_batch(7, seed=21)
+    batch += [A.sphere_cluster(6, 3), A.cloth_small()]
+    far = scenes.two_spheres(n_lon=12, n_rings=8, gap=5.0, approach=0.1)  # no candidates at all
+    batch.append(far)
+    cfg = CertConfig(1e-6, 1e-6, 32)
+    a = BatchPipeline(batch, cuda_device, config=cfg, exclude_self=exclude_self, thickness=thickness)
+    b = BatchPipeline(batch, cuda_device, config=cfg, exclude_self=exclude_self, thickness=thickness,
+                      broad="per_scene")
+    sa, sb = a.step_checked(), b.step_checked()
+    ca, cb = a.read_counts(), b.read_counts()
+    assert np.array_equal(ca[:, :3], cb[:, :3])
+    if exclude_self:  # the far-apart pair of spheres has no candidate between them
+        assert ca[-1, 0] == 0 and ca[-1, 1] == 0
+    for i in range(len(batch)):
+        pa, pb = a.pairs(i), b.pairs(i)
+        assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1]), i
+        # padding after the pairs
+        off, cap = int(a.vf_pair_off[i]), a.vf_caps[i]
+        tail = a.vf_pairs[off + int(ca[i, 0]):off + cap].cpu().numpy().view(np.uint64)
+        assert (tail == np.uint64(0xFFFFFFFFFFFFFFFF)).all()
+    assert sa == sb
+    # the oracle's pair sets for two of the scenes
+    for i in (0, len(batch) - 3):
+        s = batch[i]
+        n_obj = int(s["n_obj"])
+        allowed = oracle_mod.object_allowed(s["v_t0"], s["v_t1"], s["v_obj"], n_obj, thickness, exclude_self)
+        vbox = oracle_mod.swept_boxes(s["v_t0"], s["v_t1"], None, 1, thickness)
+        fbox = oracle_mod.swept_boxes(s["v_t0"], s["v_t1"], s["faces"], 3, thickness)
+        ebox = oracle_mod.swept_boxes(s["v_t0"], s["v_t1"], s["edges"], 2, thickness)
+        valid = (s["v_obj"] >= 0).astype(np.uint8)
+        vf = oracle_mod.vf_pairs(vbox, s["v_obj"], valid, fbox, s["f_obj"], s["faces"], allowed, "sweep")
+        ee = oracle_mod.ee_pairs(ebox, s["e_obj"], s["edges"], allowed, "sweep")
+        pa = a.pairs(i)
+        assert np.array_equal(np.sort(vf), pa[0]) and np.array_equal(np.sort(ee), pa[1]), i
