@@ -365,7 +365,7 @@ class BatchWorkload:
         return _batch_reference_sample(self.scenes, self.cfg, budget_s)
 
 
-def _batch_reference_sample(scenes_list, cfg, budget_s: float, order=None) -> dict:
+def _batch_reference_sample(scenes_list, cfg, budget_s: float, order=None, exclude_self: bool = True) -> dict:
     """The reference scene tool (compiled unchanged, 1 thread as written) on
     whole scenes of the batch, in batch order (or `order`), until budget_s:
     its sweep-and-prune candidates (self pairs excluded) then its
@@ -376,7 +376,7 @@ def _batch_reference_sample(scenes_list, cfg, budget_s: float, order=None) -> di
     secs, calls, done, tris = 0.0, 0, 0, 0
     for i in (order if order is not None else range(len(scenes_list))):
         s = scenes_list[i]
-        tool = oracle.RefToolScene(s["v_t0"], s["v_t1"], s["faces"], 0.0, True)
+        tool = oracle.RefToolScene(s["v_t0"], s["v_t1"], s["faces"], 0.0, exclude_self)
         r = tool.time_all_exact(cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth)
         secs += r["candidates_s"] + r["certify_s"]
         calls += r["calls"]
@@ -784,6 +784,159 @@ def run_b200(args) -> dict | None:
     return line
 
 
+# --------------------------------------------------------------------------
+# serving: a Poisson stream of mixed CCD steps through the continuous-batching engine
+
+
+def _serve_pool(seed: int) -> list[tuple[str, dict, bool]]:
+    """Meshes of the serving stream: the three scene kinds (two spheres,
+    uneven-batch scene, cloth on sphere) at 10k-600k triangles."""
+    from p2cccd_b200 import scenes
+
+    pool = []
+    for k, tris in enumerate((10_000, 25_000, 60_000, 150_000, 300_000, 600_000)):
+        kind = ("spheres", "rigid", "cloth")[k % 3]
+        if kind == "spheres":
+            r = max(3, int(round((tris / 4 / 1.25) ** 0.5)))
+            s = scenes.two_spheres(n_lon=max(4, int(round(tris / 4 / r))), n_rings=r, seed=seed + k)
+            pool.append((f"{kind}{tris}", s, True))
+        elif kind == "rigid":
+            s = scenes.uneven_batch(1, tri_min=tris, tri_max=tris, seed=seed + k)[0]
+            pool.append((f"{kind}{tris}", s, True))
+        else:
+            sphere = tris // 6
+            r = max(6, int(round((sphere / 2 / 1.25) ** 0.5)))
+            lon = max(8, int(round(sphere / 2 / r)))
+            n = int(round(((tris - 2 * lon * r) / 2) ** 0.5)) + 1
+            s = scenes.cloth_on_sphere(n=n, sphere_lon=lon, sphere_rings=r, seed=seed + k)
+            pool.append((f"{kind}{tris}", s, False))
+    for kind, tris in (("cloth", 300_000), ("spheres", 600_000), ("rigid", 10_000)):
+        if kind == "cloth":
+            s = scenes.cloth_on_sphere(n=353, sphere_lon=130, sphere_rings=100, seed=seed + 17)
+        elif kind == "spheres":
+            s = scenes.two_spheres(n_lon=432, n_rings=347, seed=seed + 18)
+        else:
+            s = scenes.uneven_batch(1, tri_min=tris, tri_max=tris, seed=seed + 19)[0]
+        pool.append((f"{kind}{tris}b", s, kind != "cloth"))
+    return pool
+
+
+def run_serve(args) -> dict:
+    import numpy as np
+    import torch
+
+    from p2cccd_b200 import certify
+    from p2cccd_b200.scene import ScenePipeline
+    from p2cccd_b200.serve import Request, ServeEngine, latency_stats
+
+    world, rank, local = _dist_setup(args)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    seed = 20261203 + rank
+    cfg = certify.CertConfig(1e-6, 1e-6, 32)
+    pool = _serve_pool(seed)
+    eng = ServeEngine(dev, config=cfg, slots=4, max_group=16)
+    host = {}
+    for key, s, excl in pool:
+        eng.register_mesh(key, s, exclude_self=excl)
+        host[key] = (torch.from_numpy(np.ascontiguousarray(s["v_t0"])).pin_memory(),
+                     torch.from_numpy(np.ascontiguousarray(s["v_t1"])).pin_memory(), len(s["faces"]), excl, s)
+    rng = np.random.default_rng(seed)
+    n_req = args.serve_requests
+    keys = [k for k, _, _ in pool]
+
+    def stream(rate: float):
+        t, out = 0.0, []
+        for i in range(n_req):
+            t += float(rng.exponential(1.0 / rate))
+            k = keys[int(rng.integers(len(keys)))]
+            out.append(Request(rid=i, mesh=k, v_t0=host[k][0], v_t1=host[k][1], arrival_s=t))
+        return out
+
+    # warm-up: every mesh once (sizes the candidate state), then a short stream
+    eng.run([Request(rid=-1 - i, mesh=k, v_t0=host[k][0], v_t1=host[k][1], arrival_s=0.0) for i, k in enumerate(keys)])
+    for _ in range(max(0, args.warmup)):
+        eng.start()
+        eng.run(stream(args.serve_rate)[: max(8, n_req // 8)])
+    sampler = ClockSampler(dev.index if world > 1 else 0)
+    sampler.start()
+    torch.cuda.synchronize()
+    results = []
+    t_begin = time.time()
+    for _ in range(args.steps):
+        reqs = stream(args.serve_rate)
+        eng.start()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        done = eng.run(reqs)
+        e1.record()
+        torch.cuda.synchronize()
+        results.append((done, e0.elapsed_time(e1)))
+    t_end = time.time()
+    clocks = sampler.stop((t_begin, t_end))
+    done_all = [r for d, _ in results for r in d]
+    q_total = sum(r.queries for r in done_all)
+    ms_total = sum(ms for _, ms in results)
+    stats = latency_stats(done_all)
+    tris = np.array([host[r.mesh][2] for r in done_all], dtype=np.float64)
+    lat = np.array([r.latency_ms for r in done_all])
+    per100k = lat / np.maximum(tris / 1e5, 1e-9)
+    # the plain per-step path: each request alone, synchronously, through ScenePipeline
+    plain_ms, plain_q = 0.0, 0
+    pipes = {}
+    for r in results[-1][0]:
+        v0, v1, _, excl, s = host[r.mesh]
+        if r.mesh not in pipes:
+            pipes[r.mesh] = ScenePipeline(s, dev, exclude_self=excl, config=cfg,
+                                          vf_capacity=eng.meshes[r.mesh].vf_cap,
+                                          ee_capacity=eng.meshes[r.mesh].ee_cap)
+            pipes[r.mesh].step_checked()
+        p = pipes[r.mesh]
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        p.v_t0.copy_(v0, non_blocking=True)
+        p.v_t1.copy_(v1, non_blocking=True)
+        summ = p.step_checked()
+        plain_ms += (time.perf_counter() - t0) * 1e3
+        plain_q += summ["vf_certified"] + summ["ee_certified"]
+    value = q_total / (ms_total * 1e-3)
+    plain_value = plain_q / (plain_ms * 1e-3)
+    h2d = int(sum(2 * host[r.mesh][0].numel() * 8 for r in done_all) / max(1, args.steps))
+    d2h = int(sum(112 + 32 for _ in done_all) / max(1, args.steps))
+    census_q = {}
+    return {
+        "metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
+        "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "serving stream: Poisson arrivals of CCD steps drawn from the two-sphere, rigid "
+                               "uneven-scene and cloth-on-sphere kinds at 10k-600k triangles, admitted by slots and "
+                               "device memory into continuous batches (one candidate launch sequence + one "
+                               "certification launch per batch), every candidate certified; a step of this line "
+                               f"is one stream of {n_req} requests",
+                   "arrival_rate_per_s": args.serve_rate, "requests_per_step": n_req,
+                   "meshes": {k: int(host[k][2]) for k in keys},
+                   "latency_ms": stats, "latency_ms_per_100k_triangles": {
+                       "p50": float(np.percentile(per100k, 50)), "p99": float(np.percentile(per100k, 99))},
+                   "served_requests_per_s": len(done_all) / (ms_total * 1e-3),
+                   "groups_run": eng.groups_run, "reruns": int(sum(r.reruns for r in done_all)),
+                   "plain_path": {"value": plain_value, "unit": "queries/s",
+                                  "what": "the same requests one at a time through ScenePipeline.step_checked "
+                                          "(host sync per step)"},
+                   "served_over_plain": value / plain_value,
+                   "eps_time": cfg.eps_time, "eps_space": cfg.eps_space,
+                   "max_subdivision_depth": cfg.max_subdivision_depth, "seed": seed,
+                   "l2": "requests stream fresh trajectories from host memory", "parallelism": f"replicas x{world}"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "what": "the serving loop is end to end: trajectories copied from pinned host memory, summaries "
+                        "and counts copied back, per request"},
+        "gpu_launches": None,
+        "roofline": None,
+        "cpu_baseline": None,
+        "clocks": clocks,
+    }
+
+
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
 
 
@@ -830,24 +983,33 @@ def run_reference(args) -> dict | None:
         conf = {"workload": "single-scene broad+narrow: two 40,960-triangle UV spheres, translation-only form "
                             "(the reference mesh builder takes rigid translations only)"}
         sample = ref.describe() + "; one slice per step"
-    elif args.workload == "batch":
-        batch = scenes.uneven_batch(256)
+    elif args.workload in ("batch", "serve"):
+        if args.workload == "batch":
+            batch = scenes.uneven_batch(256)
+            excl = [True] * len(batch)
+        else:
+            pool = _serve_pool(20261203)
+            batch = [s for _, s, _ in pool]
+            excl = [e for _, _, e in pool]
         by_size = sorted(range(len(batch)), key=lambda i: len(batch[i]["faces"]))
         chosen, spent = [], 0.0
         for i in by_size:  # smallest scenes first while their mean tool time fits the per-step budget
-            r = _batch_reference_sample(batch, cfg, 0.0, order=[i])
+            r = _batch_reference_sample(batch, cfg, 0.0, order=[i], exclude_self=excl[i])
             if chosen and (spent + r["seconds"]) / (len(chosen) + 1) > per_step_s:
                 break
             chosen.append(i)
             spent += r["seconds"]
 
         def step(i):
-            r = _batch_reference_sample(batch, cfg, 0.0, order=[chosen[i % len(chosen)]])
+            j = chosen[i % len(chosen)]
+            r = _batch_reference_sample(batch, cfg, 0.0, order=[j], exclude_self=excl[j])
             return r["queries"], r["seconds"]
-        conf = {"workload": "batched uneven scenes: 256 two-UV-sphere scenes, 1k-200k triangles (the reference "
-                            "scene tool, one scene per step)"}
+        conf = {"workload": ("batched uneven scenes: 256 two-UV-sphere scenes, 1k-200k triangles"
+                             if args.workload == "batch" else
+                             "serving stream of mixed CCD steps (two spheres, rigid scenes, cloth), 10k-600k "
+                             "triangles") + " (the reference scene tool, one scene per step)"}
         sample = (f"reference scene tool (SweepPairs candidates + RunAllExactRows, 1 thread as written), one whole "
-                  f"scene per step cycling over the {len(chosen)} smallest scenes of the batch (up to "
+                  f"scene per step cycling over the {len(chosen)} smallest scenes of the {args.workload} (up to "
                   f"{len(batch[chosen[-1]]['faces'])} triangles) whose mean step fits {per_step_s * 1e3:.0f} ms")
         threads = 1
     else:
@@ -894,12 +1056,19 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS) + ["serve"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
+    ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     args = ap.parse_args()
-    line = run_reference(args) if args.impl == "reference" else run_b200(args)
+    if args.impl == "reference":
+        line = run_reference(args)
+    elif args.workload == "serve":
+        line = run_serve(args)
+    else:
+        line = run_b200(args)
     if line is not None:
         print(json.dumps(line), flush=True)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.impl == "b200":
