@@ -111,11 +111,11 @@ struct BatchProblem {
   unsigned long long uq_cap;
   unsigned long long* error_word;
   double T0, T1;
-  __device__ __forceinline__ long long n(int f) const { return total[f - 1]; }
+  __device__ __forceinline__ long long n(int f) const { return pick(total, f); }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void locate(int f, long long q, int& s, long long& local) const {
-    s = find_scene(off[f - 1], n_scenes, (unsigned long long)q);
-    local = q - (long long)__ldg(off[f - 1] + s);
+    s = find_scene(pick(off, f), n_scenes, (unsigned long long)q);
+    local = q - (long long)__ldg(pick(off, f) + s);
   }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
     int s;

@@ -36,20 +36,20 @@ struct RecordProblem {
   p2c_interval_result* out[2];
   unsigned long long* invalid_key;    // [2]: min over (index << 2 | reason)
   double T0, T1;
-  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ long long n(int f) const { return pick(count, f); }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
-    load_record(recs[f - 1] + 30 * q, g, bad);
+    load_record(pick(recs, f) + 30 * q, g, bad);
     t0 = T0;
     t1 = T1;
   }
   __device__ __forceinline__ void finish(int f, long long q, const Outcome& o) const {
-    const unsigned long long* r = recs[f - 1] + 30 * q;
-    store_interval_result(out[f - 1] + q, f, o, (long long)r[0], (long long)r[1]);
+    const unsigned long long* r = pick(recs, f) + 30 * q;
+    store_interval_result(pick(out, f) + q, f, o, (long long)r[0], (long long)r[1]);
   }
   __device__ __forceinline__ void invalid(int f, long long q, int bad, double t0, double t1) const {
     Outcome o{3, t0, t1, t1, 0.0};
-    store_interval_result(out[f - 1] + q, f, o, -1, -1);
+    store_interval_result(pick(out, f) + q, f, o, -1, -1);
     atomicMin(&invalid_key[f - 1], ((unsigned long long)q << 2) | (unsigned long long)bad);
   }
 };

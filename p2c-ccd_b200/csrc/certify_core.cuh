@@ -353,6 +353,13 @@ struct WarpStats {
 };
 
 // Position of the (r+1)-th set bit of m (r counts from 0); m has > r set bits.
+// Entry f-1 of a two-entry member array, chosen by value: a run-time index
+// into such an array would move the whole object to local memory.
+template <class T>
+__device__ __forceinline__ T pick(const T (&a)[2], int f) {
+  return f == 1 ? a[0] : a[1];
+}
+
 __device__ __forceinline__ int nth_set_bit(unsigned m, int r) {
   for (int i = 0; i < r; ++i) m &= m - 1u;
   return __ffs((int)m) - 1;

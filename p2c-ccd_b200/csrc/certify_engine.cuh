@@ -127,14 +127,14 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
   Counter ops;
   unsigned free_mask = FULL;
   int cur = ee_first ? 2 : 1;              // family whose queue this warp drains
-  bool exhausted[2] = {n1 == 0, n2 == 0};
+  unsigned exhausted = (n1 == 0 ? 1u : 0u) | (n2 == 0 ? 2u : 0u);  // bit f-1: family f's queue is empty
   bool hungry = false;                     // this warp is counted in es->hungry
   bool helper = false;                     // this warp is counted in es->helpers
   unsigned backoff = 256;                  // ns slept per idle poll (doubles up to 4 us)
   unsigned long long pool_hungry = 0, pool_size = 0;
   bool ok = true;
 
-  auto queues_done = [&]() { return exhausted[0] && exhausted[1]; };
+  auto queues_done = [&]() { return exhausted == 3u; };
 
   // Finish a tree: one result for query (f, q).
   auto finalize = [&](int f, long long q, const Outcome& o) {
@@ -182,16 +182,16 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
     // ---- (A) new queries from the per-family queues -------------------------
     unsigned idle = __ballot_sync(FULL, slot < 0);
     if (idle != 0u && !queues_done()) {
-      if (exhausted[cur - 1]) cur = 3 - cur;
-      const CertParams& prm = cur == 1 ? prm1 : prm2;
-      const int room = prm.fetch_limit - (32 - __popc(free_mask));
+      if (exhausted & (1u << (cur - 1))) cur = 3 - cur;
+      const int fetch_limit = cur == 1 ? prm1.fetch_limit : prm2.fetch_limit;
+      const int room = fetch_limit - (32 - __popc(free_mask));
       if (room > 0) {
         const long long nc = cur == 1 ? n1 : n2;
         const int k = min(__popc(idle), room);
         unsigned long long base = 0;
         if (lane == 0) base = atomicAdd(&es->queue_head[cur - 1].v, (unsigned long long)k);
         base = __shfl_sync(FULL, base, 0);
-        if ((long long)base + k >= nc) exhausted[cur - 1] = true;
+        if ((long long)base + k >= nc) exhausted |= 1u << (cur - 1);
         bool fresh = false;
         const int r = __popc(idle & lt_mask);
         if (slot < 0 && r < k) {

@@ -56,21 +56,21 @@ struct QueryProblem {
   const double* q_t1;
   p2c_interval_result* out[2];
   QueryAgg* agg;
-  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ long long n(int f) const { return pick(count, f); }
   __device__ __forceinline__ unsigned long long key(int f, long long q) const {
     return ((unsigned long long)(f - 1) << 62) | (unsigned long long)q;
   }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
-    load_rec(recs[f - 1] + 30 * q, g, bad);
-    const long long qi = prim_query[f - 1][q];
+    load_rec(pick(recs, f) + 30 * q, g, bad);
+    const long long qi = pick(prim_query, f)[q];
     t0 = q_t0[qi];
     t1 = q_t1[qi];
   }
   __device__ __forceinline__ void finish(int f, long long q, const Outcome& o) const {
-    const unsigned long long* r = recs[f - 1] + 30 * q;
-    store_interval_result(out[f - 1] + q, f, o, (long long)r[0], (long long)r[1]);
-    QueryAgg& a = agg[prim_query[f - 1][q]];
+    const unsigned long long* r = pick(recs, f) + 30 * q;
+    store_interval_result(pick(out, f) + q, f, o, (long long)r[0], (long long)r[1]);
+    QueryAgg& a = agg[pick(prim_query, f)[q]];
     if (o.status == P2C_STATUS_COLLISION) atomicMin(&a.first_key, key(f, q));
     else if (o.status == P2C_STATUS_SEPARATION) {
       atomicMin(&a.margin_bits, (unsigned long long)__double_as_longlong(o.margin));
@@ -81,8 +81,8 @@ struct QueryProblem {
   }
   __device__ __forceinline__ void invalid(int f, long long q, int bad, double t0, double t1) const {
     Outcome o{3, t0, t1, t1, 0.0};
-    store_interval_result(out[f - 1] + q, f, o, -1, -1);
-    atomicMin(&agg[prim_query[f - 1][q]].invalid_key, key(f, q));
+    store_interval_result(pick(out, f) + q, f, o, -1, -1);
+    atomicMin(&agg[pick(prim_query, f)[q]].invalid_key, key(f, q));
   }
 };
 

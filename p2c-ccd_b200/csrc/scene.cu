@@ -29,23 +29,23 @@ struct PairProblem {
   unsigned long long* undecided_queue;
   unsigned long long undecided_cap;
   unsigned long long* error_word;
-  __device__ __forceinline__ long long n(int f) const { return count[f - 1]; }
+  __device__ __forceinline__ long long n(int f) const { return pick(count, f); }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
-    const ScenePairs& s = sp[f - 1];
+    const ScenePairs& s = pick(sp, f);
     bad = load_pair(s, f, __ldg(s.pairs + q), g) ? 0 : 2;
     t0 = s.T0;
     t1 = s.T1;
   }
   __device__ __forceinline__ void finish(int fam, long long q, const Outcome& o) const {
-    const unsigned long long key = sp[fam - 1].pairs[q];
-    store_interval_result(out[fam - 1] + q, fam, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
+    const unsigned long long key = pick(sp, fam).pairs[q];
+    store_interval_result(pick(out, fam) + q, fam, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
     scene_agg_record(agg, fam, key, o, undecided_queue, undecided_cap,
                      ((unsigned long long)(fam - 1) << 63) | (unsigned long long)q);
   }
   __device__ __forceinline__ void invalid(int fam, long long q, int bad, double t0, double t1) const {
     Outcome o{3, t0, t1, t1, 0.0};
-    store_interval_result(out[fam - 1] + q, fam, o, -1, -1);
+    store_interval_result(pick(out, fam) + q, fam, o, -1, -1);
     atomicOr(error_word, 4ull);
   }
 };

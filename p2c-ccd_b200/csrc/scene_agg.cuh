@@ -26,20 +26,28 @@ __device__ __forceinline__ void scene_agg_init(SceneAgg& a) {
 // One finished certificate of family fam (1: VF, 2: EE) with pair key `key`;
 // an undecided one is appended to the undecided (fallback-replay) queue as
 // `entry` when the queue exists.
+// Lanes that finish together add their counts with one atomic per (scene,
+// status); a minimum is only written when it can still decrease.
 __device__ __forceinline__ void scene_agg_record(SceneAgg* agg, int fam, unsigned long long key, const Outcome& o,
                                                  unsigned long long* uq, unsigned long long uq_cap,
                                                  unsigned long long entry) {
   const int f = fam - 1;
+  const unsigned act = __activemask();
+  const unsigned m = __match_any_sync(act, (reinterpret_cast<unsigned long long>(agg) << 2) | o.status);
+  const bool leader = (int)(threadIdx.x & 31) == __ffs((int)m) - 1;
+  const unsigned long long n = (unsigned long long)__popc(m);
   if (o.status == P2C_STATUS_COLLISION) {
-    atomicMin(&agg->coll_key, ((unsigned long long)f << 63) | key);
-    atomicAdd(&agg->collisions, 1ull);
+    const unsigned long long k = ((unsigned long long)f << 63) | key;
+    if (k < *reinterpret_cast<volatile unsigned long long*>(&agg->coll_key)) atomicMin(&agg->coll_key, k);
+    if (leader) atomicAdd(&agg->collisions, n);
   } else if (o.status == P2C_STATUS_SEPARATION) {
-    atomicMin(&agg->margin_bits, (unsigned long long)__double_as_longlong(o.margin));
+    const unsigned long long mb = (unsigned long long)__double_as_longlong(o.margin);
+    if (mb < *reinterpret_cast<volatile unsigned long long*>(&agg->margin_bits)) atomicMin(&agg->margin_bits, mb);
     if (agg->any_sep[f] == 0u) atomicExch(&agg->any_sep[f], 1u);
-    atomicAdd(&agg->separations, 1ull);
+    if (leader) atomicAdd(&agg->separations, n);
   } else {
     if (agg->any_undecided[f] == 0u) atomicExch(&agg->any_undecided[f], 1u);
-    atomicAdd(&agg->undecided, 1ull);
+    if (leader) atomicAdd(&agg->undecided, n);
     if (uq != nullptr) {
       const unsigned long long slot = atomicAdd(&agg->queued, 1ull);
       if (slot < uq_cap) uq[slot] = entry;
