@@ -197,6 +197,8 @@ class SceneWorkload:
         self.scene = scenes.two_spheres(seed=20261203 + rank)
         self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
         self.pipe = ScenePipeline(self.scene, device, exclude_self=True, config=self.cfg)
+        self.pipe.step_checked()
+        self.pipe.fit_capacities()
         summ = self.pipe.step_checked()
         self.pipe.capture()
         self.n_vf, self.n_ee = summ["vf_certified"], summ["ee_certified"]
@@ -286,11 +288,16 @@ class BatchWorkload:
 
         self.torch = torch
         self.seed = 20261203 + rank
-        self.scenes = scenes.uneven_batch(256, seed=self.seed)
+        self.scenes = scenes.uneven_batch(BATCH_SCENES, seed=self.seed)
         self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
         self.bp = BatchPipeline(self.scenes, device, exclude_self=True, config=self.cfg, streams=8)
+        self.bp.step_checked()
+        self.bp.fit_capacities()
         summ = self.bp.step_checked()
-        self.tuning = self.bp.autotune(reps=3)
+        if AUTOTUNE_REPS > 0:
+            self.tuning = self.bp.autotune(reps=AUTOTUNE_REPS)
+        else:  # the library's default launch shape
+            self.tuning = dict(self.bp.tuning.as_dict(), streams=self.bp.n_streams)
         self.bp.capture()
         self.summaries = summ
         self.queries = sum(x["vf_certified"] + x["ee_certified"] for x in summ)
@@ -308,7 +315,7 @@ class BatchWorkload:
 
     def config(self) -> dict:
         tris = [s["spec"]["triangles"] for s in self.scenes]
-        return {"workload": "batched uneven scenes: 256 independent two-UV-sphere scenes, triangle counts "
+        return {"workload": f"batched uneven scenes: {len(self.scenes)} independent two-UV-sphere scenes, triangle counts "
                             "log-uniform 1k-200k, random rigid motion (rotation + translation into contact, "
                             "penetration 0.25 f, f ~ U[5%, 40%]) + N(0,1e-3) jitter, FP64; per-scene swept-AABB "
                             "candidates then every candidate certified in one persistent launch, one CUDA graph",
@@ -414,6 +421,8 @@ class ClothWorkload:
         self.pipe = ScenePipeline(self.scene, device, exclude_self=False, config=self.cfg, narrow="anyhit",
                                   top_k=self.top_k, scheduler_seed=self.seed, vf_capacity=1 << 20,
                                   ee_capacity=3 << 20)
+        self.pipe.step_checked()
+        self.pipe.fit_capacities()
         summ = self.pipe.step_checked()
         self.pipe.capture()
         self.first_summary = summ
@@ -937,6 +946,8 @@ def run_serve(args) -> dict:
     }
 
 
+BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
+AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
 
 
@@ -985,7 +996,7 @@ def run_reference(args) -> dict | None:
         sample = ref.describe() + "; one slice per step"
     elif args.workload in ("batch", "serve"):
         if args.workload == "batch":
-            batch = scenes.uneven_batch(256)
+            batch = scenes.uneven_batch(BATCH_SCENES)
             excl = [True] * len(batch)
         else:
             pool = _serve_pool(20261203)
@@ -1060,9 +1071,14 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--scenes", type=int, default=256, help="batch: number of scenes")
+    ap.add_argument("--autotune-reps", type=int, default=3,
+                    help="batch: graph replays per autotuner trial (0: the library's default launch shape)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     args = ap.parse_args()
+    global BATCH_SCENES, AUTOTUNE_REPS
+    BATCH_SCENES, AUTOTUNE_REPS = max(1, args.scenes), max(0, args.autotune_reps)
     if args.impl == "reference":
         line = run_reference(args)
     elif args.workload == "serve":

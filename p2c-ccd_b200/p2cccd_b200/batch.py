@@ -253,6 +253,14 @@ class BatchPipeline:
                          for cap, n, o in zip(self.ee_caps, c[:, 1], over_ee)])
         raise _lib.P2CError("pair buffers kept overflowing")
 
+    def fit_capacities(self, margin: float = 1.25, slack: int = 256) -> None:
+        """Resize every scene's pair buffers to its last candidate count x
+        margin + slack.  The pair sort and the result buffers scale with the
+        capacities, not the counts, so a step after this costs less; a later
+        step whose counts grow past the capacities needs ``step_checked``."""
+        c = self.read_counts()
+        self._alloc([int(n * margin) + slack for n in c[:, 0]], [int(n * margin) + slack for n in c[:, 1]])
+
     def read_summaries(self) -> list[dict]:
         raw = self.summaries.cpu().numpy().reshape(-1).view(SUMMARY_DTYPE)
         out = []

@@ -226,6 +226,15 @@ class ScenePipeline:
             out["error_word"] |= p["error_word"]
         return out
 
+    def fit_capacities(self, margin: float = 1.25, slack: int = 256) -> None:
+        """Resize the pair buffers to the last candidate counts x margin +
+        slack: the pair sorts, the any-hit sorts and the result buffers scale
+        with the capacities, not the counts.  A later step whose counts grow
+        past them needs ``step_checked``; a captured graph is re-captured."""
+        n_vf, n_ee, _ = self.read_counts()
+        self._alloc(int(n_vf * margin) + slack, int(n_ee * margin) + slack)
+        self.graph = None
+
     def read_summary(self) -> dict:
         raw = self.summary.cpu().numpy().view(SUMMARY_DTYPE)[0]
         out = {k: int(raw[k]) for k in SUMMARY_DTYPE.names if k != "query"}

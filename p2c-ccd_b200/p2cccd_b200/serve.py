@@ -264,6 +264,10 @@ class ServeEngine:
                 r.reruns += 1
                 rerun.append(r)
                 continue
+            # candidate state: the mesh's next requests get buffers fitted to
+            # this step's counts (pair sorts and copies scale with capacity)
+            m.vf_cap = min(m.vf_cap, int(n_vf * 1.25) + 1024)
+            m.ee_cap = min(m.ee_cap, int(n_ee * 1.25) + 1024)
             s = summ[i]
             d = {k: int(s[k]) for k in SUMMARY_DTYPE.names if k != "query"}
             d["query"] = {k: s["query"][k].item() for k in QUERY_CERTIFICATE_DTYPE.names}

@@ -82,6 +82,9 @@ def test_batch_autotune_keeps_results(cuda_device, tmp_path):
     bp = BatchPipeline(_small_batch(12, seed=3), cuda_device, config=cfg)
     summ = bp.step_checked()
     before = [tuple(map(_bytes, bp.results(i))) for i in range(bp.n)]
+    bp.fit_capacities(margin=1.0, slack=0)  # exact-size buffers: same candidates and certificates
+    assert bp.step_checked() == summ
+    assert all(cap == int(n) for cap, n in zip(bp.vf_caps, bp.read_counts()[:, 0]) if n > 0)
     best = bp.autotune(reps=2, cache=tmp_path / "tune.json")
     assert best["ms"] > 0 and best["streams"] in (1, 4, 8, 16)
     cached = bp.autotune(reps=2, cache=tmp_path / "tune.json")
