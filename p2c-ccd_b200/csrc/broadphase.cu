@@ -232,7 +232,7 @@ __global__ void grid_kernel(BroadScratch* sc) {
   g.axis = axis;
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
-  g.pad = 0;
+  g.qmax = kQMax;
   const int ax[3] = {g.a1, g.a2, axis};
   double base[3], inv[3];
   int cols[2] = {1, 1};

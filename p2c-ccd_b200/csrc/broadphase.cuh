@@ -61,7 +61,8 @@ struct ListStats {
 };
 
 struct Grid {
-  int axis, a1, a2, g1, g2, pad;
+  int axis, a1, a2, g1, g2;
+  unsigned qmax;                    // largest quantised value (the key's quantiser field is full)
   double base1, base2, inv1, inv2;  // column = floor((x - base) * inv)
   double base0, scale0;             // quantiser of the sweep axis: floor((x - base0) * scale0)
   double reach1[3], reach2[3];      // per list: the largest extent along a1 / a2
@@ -126,7 +127,7 @@ __device__ __forceinline__ int column(double x, double base, double inv, int g) 
 // Monotone (non-decreasing) in x: the sweep windows rely on it.
 __device__ __forceinline__ unsigned quantise(double x, const Grid& g) {
   const double c = floor((x - g.base0) * g.scale0);
-  return c < 0.0 ? 0u : (c >= (double)kQMax ? kQMax : (unsigned)c);
+  return c < 0.0 ? 0u : (c >= (double)g.qmax ? g.qmax : (unsigned)c);
 }
 
 // Walk over the candidate entries of one scanning box: the columns its

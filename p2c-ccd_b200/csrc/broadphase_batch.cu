@@ -15,11 +15,11 @@
 //   4. one thread per scene: sweep axis, column grid (at most
 //      max(64, n/4) cells for a scene of n primitives, 128 x 128 at most),
 //      quantiser;
-//   5. ONE radix sort of 64-bit keys (scene, list, column, quantised min)
-//      over all primitives, a gather into one struct-of-arrays in sorted
+//   5. ONE radix sort of 64-bit keys (scene, list, column, 14-bit quantised
+//      min: 30 + scene bits, 5 passes for up to 256 scenes) over all primitives, a gather into one struct-of-arrays in sorted
 //      order and per-scene column tables holding sorted positions;
 //   6. sweeps that walk only their own scene's columns, appending pairs as
-//      (scene << 44 | packed pair) into a buffer of the scenes' summed
+//      (scene << w | packed pair), w the widest scene's packed pair, into a buffer of the scenes' summed
 //      capacities (scene s owns its capacity's slice, pre-filled with its
 //      padding key);
 //   7. ONE sort of all pairs and a scatter into each scene's own buffer,
@@ -43,9 +43,9 @@ namespace {
 constexpr int kThreads = 256;
 constexpr int kPrepThreads = 1024;
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kPairBits = 44;  // packed pair key bits (a < 2^22, b < 2^22)
-constexpr unsigned long long kPairMask = (1ull << kPairBits) - 1ull;
-constexpr long long kMaxScenePrims = 1ll << 22;
+constexpr long long kMaxScenePrims = 1ll << 22;  // packed pairs of one scene stay below 2^44
+constexpr int kBatchQBits = 14;                 // quantiser of the batched key (5 radix passes)
+constexpr unsigned kBatchQMax = (1u << kBatchQBits) - 1u;
 
 inline unsigned grid_for(long long n, int threads) {
   const long long g = (n + threads - 1) / threads;
@@ -92,7 +92,17 @@ struct BatchBroad {
   unsigned* cell_begin;      // 3 x total cells
   unsigned* cell_end;
   unsigned long long* pack[2][2];  // vf / ee pair buffers and their sort alternates
+  int pair_bits[2];                // packed pair bits of the widest scene, per family
 };
+
+__device__ __forceinline__ unsigned long long pair_mask(int bits) { return (1ull << bits) - 1ull; }
+
+// Scene of global primitive g, starting from the block's first scene.
+__device__ __forceinline__ int scene_from(const BatchBroad& B, int s_lo, unsigned long long g) {
+  int s = s_lo;
+  while (s + 1 < B.n && __ldg(B.off.prim + s + 1) <= g) ++s;
+  return s;
+}
 
 __device__ __forceinline__ int find_segment(const unsigned long long* off, int n, unsigned long long x) {
   int lo = 0, hi = n - 1;
@@ -159,8 +169,11 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(BatchBroad B, unsigned 
   const bool live = g < P;
   int s = -1, l = 0, o = -1;
   double b[6] = {0, 0, 0, 0, 0, 0};
+  __shared__ int block_scene;
+  if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
+  __syncthreads();
   if (live) {
-    s = find_segment(B.off.prim, B.n, g);
+    s = scene_from(B, block_scene, g);
     const p2c_batch_scene& d = B.scenes[s];
     const long long loc = (long long)(g - B.off.prim[s]);
     l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
@@ -274,8 +287,11 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsign
   bool keep = false;
   int s = -1, l = 3;
   double b[6] = {0, 0, 0, 0, 0, 0};
+  __shared__ int block_scene;
+  if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
+  __syncthreads();
   if (g < P) {
-    s = find_segment(B.off.prim, B.n, g);
+    s = scene_from(B, block_scene, g);
     const p2c_batch_scene& d = B.scenes[s];
     const long long loc = (long long)(g - B.off.prim[s]);
     l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
@@ -357,7 +373,7 @@ __global__ void grid_kernel(BatchBroad B) {
   g.axis = axis;
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
-  g.pad = 0;
+  g.qmax = kBatchQMax;
   const int ax[3] = {g.a1, g.a2, axis};
   double base[3], inv[3];
   int cols[2] = {1, 1};
@@ -381,7 +397,7 @@ __global__ void grid_kernel(BatchBroad B) {
       cols[k] = c < 1 ? 1 : c;
       inv[k] = 1.0 / width;
     } else {
-      inv[k] = (range > 0.0 && isfinite(range)) ? (double)kQMax / range : 0.0;
+      inv[k] = (range > 0.0 && isfinite(range)) ? (double)kBatchQMax / range : 0.0;
     }
   }
   g.base1 = base[0];
@@ -402,10 +418,13 @@ __global__ void grid_kernel(BatchBroad B) {
 // ---- 5. keys, sort, gather ---------------------------------------------------------
 __global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned long long P) {
   const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  __shared__ int block_scene;
+  if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
+  __syncthreads();
   if (g >= P) return;
   unsigned long long key = ~0ull;
   if (B.active[g]) {
-    const int s = find_segment(B.off.prim, B.n, g);
+    const int s = scene_from(B, block_scene, g);
     const p2c_batch_scene& d = B.scenes[s];
     const long long loc = (long long)(g - B.off.prim[s]);
     const int l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
@@ -413,7 +432,7 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned l
     const double* b = B.box + 6 * g;
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
-    key = ((unsigned long long)s << 32) | ((unsigned long long)l << 30) | ((unsigned long long)c << kQBits) |
+    key = ((unsigned long long)s << 30) | ((unsigned long long)l << 28) | ((unsigned long long)c << kBatchQBits) |
           quantise(b[G.axis], G);
   }
   B.keys[0][g] = key;
@@ -431,8 +450,8 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const un
   if (i >= P) return;
   const unsigned long long key = keys[i];
   if (key == ~0ull) return;  // culled entries sort last
-  const int s = (int)(key >> 32);
-  const int l = (int)((key >> 30) & 3ull);
+  const int s = (int)(key >> 30);
+  const int l = (int)((key >> 28) & 3ull);
   const p2c_batch_scene& d = B.scenes[s];
   const Grid& G = B.sc[s].grid;
   const unsigned long long g = order[i];
@@ -445,28 +464,29 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const un
   B.S.ahi[i] = b[3 + G.a1];
   B.S.blo[i] = b[G.a2];
   B.S.bhi[i] = b[3 + G.a2];
-  B.S.q[i] = (unsigned)(key & kQMax);
+  B.S.q[i] = (unsigned)(key & kBatchQMax);
   B.S.id[i] = (int32_t)j;
   B.S.obj[i] = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[j];
-  const unsigned long long head = key >> kQBits;  // scene, list and column
+  const unsigned long long head = key >> kBatchQBits;  // scene, list and column
   const unsigned cell = (unsigned)(head & ((1ull << kCellBits) - 1ull));
-  if (i == 0 || (keys[i - 1] >> kQBits) != head) cell_table(B, B.cell_begin, s, l)[cell] = (unsigned)i;
-  if (i + 1 == P || (keys[i + 1] >> kQBits) != head) cell_table(B, B.cell_end, s, l)[cell] = (unsigned)(i + 1);
+  if (i == 0 || (keys[i - 1] >> kBatchQBits) != head) cell_table(B, B.cell_begin, s, l)[cell] = (unsigned)i;
+  if (i + 1 == P || (keys[i + 1] >> kBatchQBits) != head) cell_table(B, B.cell_end, s, l)[cell] = (unsigned)(i + 1);
 }
 
 // ---- 6. sweeps -------------------------------------------------------------------
 // Scene s's padding key: sorts after all of its pairs, before scene s + 1's.
 __global__ void fill_pack_kernel(unsigned long long* pack, const unsigned long long* cap_off, int n,
-                                 unsigned long long total) {
+                                 unsigned long long total, int bits) {
   const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
   const int s = find_segment(cap_off, n, i);
-  pack[i] = ((unsigned long long)s << kPairBits) | kPairMask;
+  pack[i] = ((unsigned long long)s << bits) | pair_mask(bits);
 }
 
 // Warp append of found pairs, one atomic per scene present in the warp.
 __device__ __forceinline__ void append_scene_pair(bool found, int s, unsigned long long key, unsigned long long* pack,
-                                                  const unsigned long long* cap_off, BroadScratch* sc, bool vf) {
+                                                  const unsigned long long* cap_off, BroadScratch* sc, bool vf,
+                                                  int bits) {
   unsigned todo = __ballot_sync(kFull, found);
   const int lane = threadIdx.x & 31;
   while (todo) {
@@ -481,7 +501,7 @@ __device__ __forceinline__ void append_scene_pair(bool found, int s, unsigned lo
     if (mine) {
       const unsigned long long slot = base + (unsigned long long)__popc(mask & ((1u << lane) - 1u));
       const unsigned long long cap = cap_off[s + 1] - cap_off[s];
-      if (slot < cap) pack[cap_off[s] + slot] = ((unsigned long long)s << kPairBits) | key;
+      if (slot < cap) pack[cap_off[s] + slot] = ((unsigned long long)s << bits) | key;
     }
   }
 }
@@ -503,9 +523,9 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
   bool from_vertex = false;
   if (i < P) {
     const unsigned long long key = keys[i];
-    const int l = key == ~0ull ? 3 : (int)((key >> 30) & 3ull);
+    const int l = key == ~0ull ? 3 : (int)((key >> 28) & 3ull);
     live = l <= 1;
-    s = (int)(key >> 32);
+    s = (int)(key >> 30);
     from_vertex = l == 0;
   }
   if (!__any_sync(kFull, live)) return;
@@ -558,7 +578,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
       ++w.j;
       if (w.j >= w.j_end || Q.q[w.j] > w.q_hi) live = w.next_cell(Q, g);
     }
-    append_scene_pair(found, s, key, B.pack[0][0], B.off.vf_cap, B.sc, true);
+    append_scene_pair(found, s, key, B.pack[0][0], B.off.vf_cap, B.sc, true, B.pair_bits[0]);
   }
 }
 
@@ -571,8 +591,8 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
   int s = 0;
   if (i < P) {
     const unsigned long long key = keys[i];
-    live = key != ~0ull && ((key >> 30) & 3ull) == 2ull;
-    s = (int)(key >> 32);
+    live = key != ~0ull && ((key >> 28) & 3ull) == 2ull;
+    s = (int)(key >> 30);
   }
   if (!__any_sync(kFull, live)) return;
   Walker w;
@@ -623,7 +643,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
       ++w.j;
       if (w.j >= w.j_end || E.q[w.j] > w.q_hi) live = w.next_cell(E, g);
     }
-    append_scene_pair(found, s, key, B.pack[1][0], B.off.ee_cap, B.sc, false);
+    append_scene_pair(found, s, key, B.pack[1][0], B.off.ee_cap, B.sc, false, B.pair_bits[1]);
   }
 }
 
@@ -633,13 +653,14 @@ __global__ void scatter_pairs_kernel(BatchBroad B, const unsigned long long* __r
   const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= total) return;
   const unsigned long long k = sorted[i];
-  const int s = (int)(k >> kPairBits);
+  const int bits = B.pair_bits[family];
+  const int s = (int)(k >> bits);
   const unsigned long long* cap_off = family == 0 ? B.off.vf_cap : B.off.ee_cap;
   const unsigned long long local = i - cap_off[s];
   const p2c_batch_scene& d = B.scenes[s];
   unsigned long long* out = reinterpret_cast<unsigned long long*>(family == 0 ? d.vf_pairs : d.ee_pairs);
-  const unsigned long long p = k & kPairMask;
-  if (p == kPairMask) {
+  const unsigned long long p = k & pair_mask(bits);
+  if (p == pair_mask(bits)) {
     out[local] = ~0ull;
   } else {
     const int shift = max(1, bit_length_dev(family == 0 ? d.nf : d.ne));
@@ -662,6 +683,7 @@ __global__ void export_counts_kernel(BatchBroad B) {
 // ---- workspace ---------------------------------------------------------------------
 struct Totals {
   unsigned long long P = 0, vf = 0, ee = 0, cells = 0;
+  int pair_bits[2] = {2, 2};  // widest packed pair of any scene: vf, ee
 };
 
 Totals totals_of(const p2c_batch_scene* h, int n) {
@@ -672,6 +694,8 @@ Totals totals_of(const p2c_batch_scene* h, int n) {
     t.vf += (unsigned long long)h[s].vf_cap;
     t.ee += (unsigned long long)h[s].ee_cap;
     t.cells += (unsigned long long)cell_budget(np);
+    t.pair_bits[0] = std::max(t.pair_bits[0], bit_length(h[s].nv) + std::max(1, bit_length(h[s].nf)));
+    t.pair_bits[1] = std::max(t.pair_bits[1], bit_length(h[s].ne) + std::max(1, bit_length(h[s].ne)));
   }
   return t;
 }
@@ -770,7 +794,9 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
     return fail(P2C_ERR_INVALID, "batch candidate workspace too small: %zu < %zu bytes", ws_bytes, need.total);
   Carve C = carve(ws, dev, n, t);
   BatchBroad& B = C.B;
-  const int scene_bits = std::max(1, bit_length(n));
+  const int scene_bits = std::max(1, bit_length(n - 1));
+  B.pair_bits[0] = t.pair_bits[0];
+  B.pair_bits[1] = t.pair_bits[1];
   P2C_CUDA(cudaMemsetAsync(B.sc, 0, sizeof(BroadScratch) * (size_t)n, s));
   P2C_CUDA(cudaMemsetAsync(B.cell_begin, 0, 4 * 3 * (size_t)t.cells, s));
   P2C_CUDA(cudaMemsetAsync(B.cell_end, 0, 4 * 3 * (size_t)t.cells, s));
@@ -788,7 +814,7 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
     P2C_CUDA(cudaGetLastError());
     size_t tb = C.tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(C.tmp, tb, B.keys[0], B.keys[1], B.vals[0], B.vals[1], (int)P, 0,
-                                             32 + scene_bits, s));
+                                             30 + scene_bits, s));
     gather_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, B.keys[1], B.vals[1], P);
     P2C_CUDA(cudaGetLastError());
   }
@@ -796,7 +822,7 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
     const unsigned long long tot = f == 0 ? t.vf : t.ee;
     if (tot > 0)
       fill_pack_kernel<<<grid_for((long long)tot, 256), 256, 0, s>>>(B.pack[f][0], f == 0 ? B.off.vf_cap : B.off.ee_cap,
-                                                                       n, tot);
+                                                                       n, tot, B.pair_bits[f]);
   }
   P2C_CUDA(cudaGetLastError());
   if (P > 0) {
@@ -809,7 +835,7 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
     if (tot == 0) continue;
     size_t tb = C.tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortKeys(C.tmp, tb, B.pack[f][0], B.pack[f][1], (int)tot, 0,
-                                            kPairBits + scene_bits, s));
+                                            B.pair_bits[f] + scene_bits, s));
     scatter_pairs_kernel<<<grid_for((long long)tot, 256), 256, 0, s>>>(B, B.pack[f][1], f, tot);
     P2C_CUDA(cudaGetLastError());
   }
