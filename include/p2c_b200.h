@@ -433,6 +433,30 @@ int p2c_group_anyhit(const p2c_scene* scene, int family, const uint64_t* pairs_d
                      p2c_anyhit_summary* summary_dev, void* workspace_dev, size_t workspace_bytes,
                      void* stream);
 
+/* ---- refinement children ------------------------------------------------- */
+size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
+
+/* GenerateConservativeRefinementWorkItems (cpp/certificate/
+ * certificate_engine.cpp:663-720) for n_parents work items at once: parent i
+ * (interval [parent_t0, parent_t1], depth parent_depth, certificate certs[i])
+ * gets at depth < max_child_depth one child [t0, clamp(toi_upper, t0, t1)]
+ * for a collision, two halves around 0.5 * (t0 + t1) for an undecided
+ * certificate asking for bisection, each only when wider than
+ * min_interval_width.  Children are written compacted in parent order
+ * (capacity 2 * n_parents): the parent index, interval, depth + 1 and
+ * work_item_id first_child_work_item_id + position (the ids of calling the
+ * reference once per parent in order with the next free id); the caller
+ * copies the parent's other ExactWorkItem fields and sets source = refined.
+ * *child_count_dev receives the number written.  A parent whose interval is
+ * not 0 <= t0 <= t1 <= 1 gets no child and sets bit 1 of *error_word_dev
+ * (may be NULL).  No host sync. */
+int p2c_refinement_children(int64_t n_parents, const double* parent_t0_dev, const double* parent_t1_dev,
+                            const uint16_t* parent_depth_dev, const p2c_query_certificate* certs_dev,
+                            uint16_t max_child_depth, double min_interval_width, uint64_t first_child_work_item_id,
+                            int64_t* child_parent_dev, double* child_t0_dev, double* child_t1_dev,
+                            uint16_t* child_depth_dev, uint64_t* child_work_item_id_dev, uint64_t* child_count_dev,
+                            uint64_t* error_word_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- diagnostics ------------------------------------------------------- */
 /* FP64 throughput probe: launches independent separately rounded multiply/add
  * chains over a full-occupancy grid and reports the FP64 operations it issues;
