@@ -104,14 +104,13 @@ __device__ __forceinline__ int find_scene(const unsigned long long* off, int n_s
 struct BatchProblem {
   const p2c_batch_scene* scenes;
   int n_scenes;
-  const unsigned long long* off[2];
-  long long total[2];
+  const unsigned long long* off[2];  // prefix offsets written by the prep kernel
   SceneAgg* aggs;
   unsigned long long* uq;
   unsigned long long uq_cap;
   unsigned long long* error_word;
   double T0, T1;
-  __device__ __forceinline__ long long n(int f) const { return pick(total, f); }
+  __device__ __forceinline__ long long n(int f) const { return (long long)pick(off, f)[n_scenes]; }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void locate(int f, long long q, int& s, long long& local) const {
     s = find_scene(pick(off, f), n_scenes, (unsigned long long)q);
@@ -151,37 +150,21 @@ struct BatchProblem {
 };
 
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    batch_certify_kernel(const p2c_batch_scene* scenes, int n_scenes, BatchLayout L, double T0, double T1,
-                         CertParams prm, int fixed_fetch, unsigned long long* uq, unsigned long long uq_cap,
-                         EnginePools pools) {
+    batch_certify_kernel(const __grid_constant__ BatchProblem prob, const __grid_constant__ CertParams prm,
+                         int fixed_fetch, const __grid_constant__ EnginePools pools, CertifyScratch* sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
-  BatchProblem prob;
-  prob.scenes = scenes;
-  prob.n_scenes = n_scenes;
-  prob.off[0] = L.off[0];
-  prob.off[1] = L.off[1];
-  prob.total[0] = (long long)L.off[0][n_scenes];
-  prob.total[1] = (long long)L.off[1][n_scenes];
-  prob.aggs = L.aggs;
-  prob.uq = uq;
-  prob.uq_cap = uq_cap;
-  prob.error_word = (unsigned long long*)&L.sc->stats.error_word;
-  prob.T0 = T0;
-  prob.T1 = T1;
   const long long warps = (long long)gridDim.x * kCertifyWarps;
-  CertParams p1 = prm, p2 = prm;
-  if (fixed_fetch > 0) {
-    p1.fetch_limit = p2.fetch_limit = fixed_fetch;
-  } else {
-    p1.fetch_limit = (int)min(32ll, max(1ll, (prob.total[0] + warps - 1) / warps));
-    p2.fetch_limit = (int)min(32ll, max(1ll, (prob.total[1] + warps - 1) / warps));
+  int f1 = fixed_fetch, f2 = fixed_fetch;
+  if (fixed_fetch <= 0) {
+    f1 = (int)min(32ll, max(1ll, (prob.n(1) + warps - 1) / warps));
+    f2 = (int)min(32ll, max(1ll, (prob.n(2) + warps - 1) / warps));
   }
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  const bool ok = run_engine<true, true, false>(prob, p1, p2, ee_first, sh, st, &L.sc->engine, pools, t_start);
-  flush_stats(st, ok, L.sc);
+  const bool ok = run_engine<true, true, false>(prob, prm, f1, f2, ee_first, sh, st, &sc->engine, pools, t_start);
+  flush_stats(st, ok, sc);
 }
 
 // Collision witnesses (grid-stride over both queues) and per-scene fields.
@@ -233,8 +216,18 @@ int launch_batch_certify(const p2c_batch_scene* scenes, int n_scenes, double T0,
   const CertParams prm = make_params(cfg, shape, 32ll * shape.grid * kCertifyWarps);
   EnginePools pools = pools_at(L.sc);
   if (tune.helper_warps > 0) pools.helper_cap = (unsigned long long)tune.helper_warps;
-  batch_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
-      scenes, n_scenes, L, T0, T1, prm, tune.fetch_limit, uq, (unsigned long long)(uq_cap > 0 ? uq_cap : 0), pools);
+  BatchProblem prob;
+  prob.scenes = scenes;
+  prob.n_scenes = n_scenes;
+  prob.off[0] = L.off[0];
+  prob.off[1] = L.off[1];
+  prob.aggs = L.aggs;
+  prob.uq = uq;
+  prob.uq_cap = (unsigned long long)(uq_cap > 0 ? uq_cap : 0);
+  prob.error_word = (unsigned long long*)&L.sc->stats.error_word;
+  prob.T0 = T0;
+  prob.T1 = T1;
+  batch_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, prm, tune.fetch_limit, pools, L.sc);
   P2C_CUDA(cudaGetLastError());
   if (summaries != nullptr) {
     batch_witness_kernel<<<shape.grid, 256, 0, s>>>(scenes, n_scenes, L, summaries);

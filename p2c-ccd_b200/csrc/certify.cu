@@ -56,7 +56,9 @@ struct RecordProblem {
 
 template <bool kShare, bool kCount>
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    certify_records_kernel(RecordProblem prob, CertParams prm_pt, CertParams prm_ee, CertifyScratch* scratch) {
+    certify_records_kernel(const __grid_constant__ RecordProblem prob, const __grid_constant__ CertParams prm,
+                           int fetch_pt, int fetch_ee, const __grid_constant__ EnginePools pools,
+                           CertifyScratch* scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
@@ -64,8 +66,8 @@ __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
   // odd warps take the edge-edge queue first, so that the tail of one family
   // overlaps the bulk of the other
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  const bool ok = run_engine<kShare, kShare, kCount>(prob, prm_pt, prm_ee, ee_first, sh, st, &scratch->engine,
-                                                     pools_at(scratch), t_start);
+  const bool ok = run_engine<kShare, kShare, kCount>(prob, prm, fetch_pt, fetch_ee, ee_first, sh, st,
+                                                     &scratch->engine, pools, t_start);
   flush_stats(st, ok, scratch);
 }
 
@@ -99,10 +101,13 @@ int launch_certify_records(const void* pt, long long n_pt, const void* ee, long 
   prob.invalid_key = sc->invalid_key;
   prob.T0 = T0;
   prob.T1 = T1;
+  const EnginePools pools = pools_at(sc);
   if (census) {
-    certify_records_kernel<false, true><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(prob, ppt, pee, sc);
+    certify_records_kernel<false, true><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
+        prob, ppt, ppt.fetch_limit, pee.fetch_limit, pools, sc);
   } else {
-    certify_records_kernel<true, false><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(prob, ppt, pee, sc);
+    certify_records_kernel<true, false><<<shape.grid, kCertifyThreads, shape.smem, stream>>>(
+        prob, ppt, ppt.fetch_limit, pee.fetch_limit, pools, sc);
   }
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;

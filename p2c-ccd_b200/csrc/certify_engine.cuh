@@ -106,8 +106,8 @@ struct EngineShared {
 //   void finish(int family, long long q, const Outcome&) const;
 //   void invalid(int family, long long q, int bad, double T0, double T1) const;
 template <bool kDonate, bool kExport, bool kCount, class P>
-__device__ bool run_engine(const P& prob, const CertParams& prm1, const CertParams& prm2, bool ee_first,
-                           EngineShared& sh, WarpStats& st, EngineState* es, const EnginePools pools,
+__device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int fetch2, bool ee_first,
+                           EngineShared& sh, WarpStats& st, EngineState* es, const EnginePools& pools,
                            unsigned long long t_start) {
   using Counter = typename std::conditional<kCount, OpCount, NoCount>::type;
   const unsigned FULL = 0xffffffffu;
@@ -117,8 +117,8 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
   SlotAgg& sa = sh.sa;
   const long long n1 = prob.n(1), n2 = prob.n(2);
   const unsigned long long n_total = (unsigned long long)(n1 + n2);
-  const double eps_space = prm1.eps_space, eps_time = prm1.eps_time;
-  const int max_depth = prm1.max_depth;
+  const double eps_space = prm.eps_space, eps_time = prm.eps_time;
+  const int max_depth = prm.max_depth;
 
   int slot = -1, fam = 1, phase = 0, depth = 0, sub_depth = 0;
   unsigned long long path = 0, donated = 0;
@@ -171,9 +171,9 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
   };
 
   for (unsigned iter = 0;; ++iter) {
-    if ((iter & 63u) == 0u && prm1.budget_ns != 0ull) {
+    if ((iter & 63u) == 0u && prm.budget_ns != 0ull) {
       int over = 0;
-      if (lane == 0) over = (global_ns() - t_start) > prm1.budget_ns;
+      if (lane == 0) over = (global_ns() - t_start) > prm.budget_ns;
       if (__shfl_sync(FULL, over, 0)) {
         ok = false;
         break;
@@ -183,7 +183,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
     unsigned idle = __ballot_sync(FULL, slot < 0);
     if (idle != 0u && !queues_done()) {
       if (exhausted & (1u << (cur - 1))) cur = 3 - cur;
-      const int fetch_limit = cur == 1 ? prm1.fetch_limit : prm2.fetch_limit;
+      const int fetch_limit = cur == 1 ? fetch1 : fetch2;
       const int room = fetch_limit - (32 - __popc(free_mask));
       if (room > 0) {
         const long long nc = cur == 1 ? n1 : n2;
@@ -319,7 +319,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm1, const CertPara
           for (unsigned spin = 0; tag == 0ull; ++spin) {
             __nanosleep(64);
             tag = volatile_load(&tk->tag);
-            if ((spin & 255u) == 255u && prm1.budget_ns != 0ull && (global_ns() - t_start) > prm1.budget_ns) break;
+            if ((spin & 255u) == 255u && prm.budget_ns != 0ull && (global_ns() - t_start) > prm.budget_ns) break;
           }
           if (tag != 0ull) {
             __threadfence();

@@ -249,13 +249,17 @@ struct AnyhitProblem {
   ScenePairs sp;
   int family;
   const unsigned* list;
-  long long count;
+  const unsigned long long* n_top;  // proposal phase: list length (else null)
+  const int* n_fallback;            // fallback phase: list length (else null)
   const unsigned* grp;
   const unsigned* rank;  // null in the fallback phase: the key is the index
   unsigned* min_hit;
   unsigned char* state;
   unsigned long long* error_word;
-  __device__ __forceinline__ long long n(int f) const { return f == family ? count : 0; }
+  __device__ __forceinline__ long long count() const {
+    return n_top != nullptr ? (long long)*n_top : (long long)*n_fallback;
+  }
+  __device__ __forceinline__ long long n(int f) const { return f == family ? count() : 0; }
   __device__ __forceinline__ unsigned order_key(unsigned c) const { return rank != nullptr ? __ldg(rank + c) : c; }
   __device__ __forceinline__ bool skip(int, long long q) const {
     const unsigned c = __ldg(list + q);
@@ -282,19 +286,15 @@ struct AnyhitProblem {
 };
 
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    anyhit_certify_kernel(ScenePairs sp, int family, const unsigned* list, const unsigned long long* n_top,
-                          const int* n_fallback, const unsigned* grp, const unsigned* rank, unsigned* min_hit,
-                          unsigned char* state, unsigned long long* error_word, CertParams prm,
-                          CertifyScratch* scratch) {
+    anyhit_certify_kernel(const __grid_constant__ AnyhitProblem prob, const __grid_constant__ CertParams prm,
+                          const __grid_constant__ EnginePools pools, CertifyScratch* scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
-  const long long count = n_top != nullptr ? (long long)*n_top : (long long)*n_fallback;
   const long long warps = (long long)gridDim.x * kCertifyWarps;
-  prm.fetch_limit = (int)min(32ll, max(1ll, (count + warps - 1) / warps));
-  AnyhitProblem prob{sp, family, list, count, grp, rank, min_hit, state, error_word};
-  const bool ok = run_engine<true, true, false>(prob, prm, prm, false, sh, st, &scratch->engine, pools_at(scratch),
+  const int fetch = (int)min(32ll, max(1ll, (prob.count() + warps - 1) / warps));
+  const bool ok = run_engine<true, true, false>(prob, prm, fetch, fetch, false, sh, st, &scratch->engine, pools,
                                                 t_start);
   flush_stats(st, ok, scratch);
 }
@@ -422,9 +422,9 @@ int launch_group_anyhit(const p2c_scene& scene, int family, const unsigned long 
     size_t tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key32[0], L.key32[1], L.val[0], L.val[1], (int)cap, 0,
                                              bit_width(K), s));
-    anyhit_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
-        sp, family, L.val[1], &L.ctr->n_top, nullptr, L.grp, L.rank, L.g_min_hit, L.state, &L.ctr->error_word, prm,
-        L.sc);
+    const AnyhitProblem prop{sp, family, L.val[1], &L.ctr->n_top, nullptr, L.grp, L.rank, L.g_min_hit, L.state,
+                             &L.ctr->error_word};
+    anyhit_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prop, prm, pools_at(L.sc), L.sc);
     P2C_CUDA(cudaGetLastError());
   }
   if (cap > 0) {
@@ -433,9 +433,9 @@ int launch_group_anyhit(const p2c_scene& scene, int family, const unsigned long 
     size_t tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceSelect::Flagged(L.tmp, tb, L.key32[0], L.flags, L.fb_list, &L.ctr->fb_count, (int)cap, s));
     P2C_CUDA(reset_engine(L.sc, s));
-    anyhit_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
-        sp, family, L.fb_list, nullptr, &L.ctr->fb_count, L.grp, nullptr, L.g_min_fb, L.state, &L.ctr->error_word,
-        prm, L.sc);
+    const AnyhitProblem fb{sp, family, L.fb_list, nullptr, &L.ctr->fb_count, L.grp, nullptr, L.g_min_fb, L.state,
+                           &L.ctr->error_word};
+    anyhit_certify_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(fb, prm, pools_at(L.sc), L.sc);
     P2C_CUDA(cudaGetLastError());
     calls_kernel<<<grid_for(cap, kThreads), kThreads, 0, s>>>(count, cap, G, K, L, evaluated, hit_out);
     P2C_CUDA(cudaGetLastError());

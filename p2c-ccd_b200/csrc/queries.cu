@@ -87,15 +87,17 @@ struct QueryProblem {
 };
 
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    certify_queries_kernel(QueryProblem prob, CertParams prm_pt, CertParams prm_ee, CertifyScratch* sc) {
+    certify_queries_kernel(const __grid_constant__ QueryProblem prob, const __grid_constant__ CertParams prm,
+                           int fetch_pt, int fetch_ee, CertifyScratch* sc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
   // no cross-warp pools here: the scratch stays one record per work item
-  const bool ok = run_engine<true, false, false>(prob, prm_pt, prm_ee, ee_first, sh, st, &sc->engine,
-                                                 EnginePools{}, t_start);
+  const EnginePools no_pools{};
+  const bool ok = run_engine<true, false, false>(prob, prm, fetch_pt, fetch_ee, ee_first, sh, st, &sc->engine,
+                                                 no_pools, t_start);
   flush_stats(st, ok, sc);
 }
 
@@ -241,7 +243,8 @@ int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const in
     prob.out[0] = pt_results_dev;
     prob.out[1] = ee_results_dev;
     prob.agg = agg;
-    certify_queries_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, ppt, pee, sc);
+    certify_queries_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, ppt, ppt.fetch_limit,
+                                                                           pee.fetch_limit, sc);
     P2C_CUDA(cudaGetLastError());
   }
   finalize_queries_kernel<<<(unsigned)((n_queries + 127) / 128), 128, 0, s>>>(

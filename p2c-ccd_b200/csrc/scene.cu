@@ -23,13 +23,19 @@ __host__ __device__ inline SceneAgg* scene_agg(void* ws) {
 // also feeds the scene reduction and, when undecided, the fallback queue.
 struct PairProblem {
   ScenePairs sp[2];
-  long long count[2];
+  long long cap[2];
+  const unsigned long long* counts;  // the broad phase's counts (device): n = min(count, cap)
+  unsigned family_mask;
   p2c_interval_result* out[2];
   SceneAgg* agg;
   unsigned long long* undecided_queue;
   unsigned long long undecided_cap;
   unsigned long long* error_word;
-  __device__ __forceinline__ long long n(int f) const { return pick(count, f); }
+  __device__ __forceinline__ long long n(int f) const {
+    if ((family_mask & (1u << (f - 1))) == 0u) return 0;
+    const long long c = (long long)counts[f - 1], k = pick(cap, f);
+    return c < k ? c : k;
+  }
   __device__ __forceinline__ bool skip(int, long long) const { return false; }
   __device__ __forceinline__ void load(int f, long long q, Geo& g, double& t0, double& t1, int& bad) const {
     const ScenePairs& s = pick(sp, f);
@@ -51,42 +57,26 @@ struct PairProblem {
 };
 
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
-    certify_scene_kernel(ScenePairs vf, long long vf_cap, ScenePairs ee, long long ee_cap,
-                         const unsigned long long* counts, unsigned family_mask, CertParams prm,
-                         p2c_interval_result* out_vf, p2c_interval_result* out_ee, unsigned long long* uq,
-                         unsigned long long uq_cap, CertifyScratch* scratch) {
+    certify_scene_kernel(const __grid_constant__ PairProblem prob, const __grid_constant__ CertParams prm,
+                         const __grid_constant__ EnginePools pools, CertifyScratch* scratch) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
   const unsigned long long t_start = global_ns();
-  const long long cvf = (long long)counts[0], cee = (long long)counts[1];
-  const long long n_vf = (family_mask & 1u) ? (cvf < vf_cap ? cvf : vf_cap) : 0;
-  const long long n_ee = (family_mask & 2u) ? (cee < ee_cap ? cee : ee_cap) : 0;
+  const long long n_vf = prob.n(1), n_ee = prob.n(2);
   // fetch width from the device-side sizes (the host did not see them)
   const long long warps = (long long)gridDim.x * kCertifyWarps;
-  CertParams p1 = prm, p2 = prm;
-  p1.fetch_limit = (int)min(32ll, max(1ll, (n_vf + warps - 1) / warps));
-  p2.fetch_limit = (int)min(32ll, max(1ll, (n_ee + warps - 1) / warps));
-  SceneAgg* agg = scene_agg(scratch);
-  PairProblem prob;
-  prob.sp[0] = vf;
-  prob.sp[1] = ee;
-  prob.count[0] = n_vf;
-  prob.count[1] = n_ee;
-  prob.out[0] = out_vf;
-  prob.out[1] = out_ee;
-  prob.agg = agg;
-  prob.undecided_queue = uq;
-  prob.undecided_cap = uq_cap;
-  prob.error_word = (unsigned long long*)&scratch->stats.error_word;
+  const int fetch_vf = (int)min(32ll, max(1ll, (n_vf + warps - 1) / warps));
+  const int fetch_ee = (int)min(32ll, max(1ll, (n_ee + warps - 1) / warps));
   const bool ee_first = ((blockIdx.x * kCertifyWarps + (threadIdx.x >> 5)) & 1u) != 0u;
-  const bool ok = run_engine<true, true, false>(prob, p1, p2, ee_first, sh, st, &scratch->engine, pools_at(scratch),
-                                                t_start);
+  const bool ok = run_engine<true, true, false>(prob, prm, fetch_vf, fetch_ee, ee_first, sh, st, &scratch->engine,
+                                                pools, t_start);
   flush_stats(st, ok, scratch);
   if (threadIdx.x == 0 && blockIdx.x == 0) {
-    agg->n_certified[0] = (unsigned long long)n_vf;
-    agg->n_certified[1] = (unsigned long long)n_ee;
-    if (cvf > vf_cap || cee > ee_cap) atomicOr((unsigned long long*)&scratch->stats.error_word, 2ull);
+    prob.agg->n_certified[0] = (unsigned long long)n_vf;
+    prob.agg->n_certified[1] = (unsigned long long)n_ee;
+    if ((long long)prob.counts[0] > prob.cap[0] || (long long)prob.counts[1] > prob.cap[1])
+      atomicOr((unsigned long long*)&scratch->stats.error_word, 2ull);
   }
 }
 
@@ -151,11 +141,20 @@ int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pa
   int rc = certify_shape(certify_scene_kernel, &shape);
   if (rc != P2C_OK) return rc;
   const CertParams prm = make_params(cfg, shape, 32ll * shape.grid * kCertifyWarps);
-  ScenePairs a{scene.v_t0, scene.v_t1, scene.faces, scene.edges, vf_pairs, T0, T1};
-  ScenePairs b{scene.v_t0, scene.v_t1, scene.faces, scene.edges, ee_pairs, T0, T1};
-  certify_scene_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(
-      a, vf_cap, b, ee_cap, counts, family_mask, prm, out_vf, out_ee, uq, (unsigned long long)(uq_cap > 0 ? uq_cap : 0),
-      sc);
+  PairProblem prob;
+  prob.sp[0] = ScenePairs{scene.v_t0, scene.v_t1, scene.faces, scene.edges, vf_pairs, T0, T1};
+  prob.sp[1] = ScenePairs{scene.v_t0, scene.v_t1, scene.faces, scene.edges, ee_pairs, T0, T1};
+  prob.cap[0] = vf_cap;
+  prob.cap[1] = ee_cap;
+  prob.counts = counts;
+  prob.family_mask = family_mask;
+  prob.out[0] = out_vf;
+  prob.out[1] = out_ee;
+  prob.agg = scene_agg(ws);
+  prob.undecided_queue = uq;
+  prob.undecided_cap = (unsigned long long)(uq_cap > 0 ? uq_cap : 0);
+  prob.error_word = (unsigned long long*)&sc->stats.error_word;
+  certify_scene_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, prm, pools_at(sc), sc);
   P2C_CUDA(cudaGetLastError());
   if (summary != nullptr) {
     const long long nmax = (vf_cap > ee_cap ? vf_cap : ee_cap);
