@@ -353,13 +353,15 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
   const SortedBoxes P = from_vertex ? V : F;
   const SortedBoxes Q = from_vertex ? F : V;
   Walker w;
+  Box6 pb{};
   double lo = 0.0;
   int32_t pid = 0, pobj = 0;
   if (live) {
     lo = P.lo[i];
     pid = P.id[i];
     pobj = P.obj[i];
-    walker_init(w, g, lo, P.hi[i], P.alo[i], P.ahi[i], P.blo[i], P.bhi[i], from_vertex ? g.reach1[1] : g.reach1[0],
+    pb = box_at(P, i);
+    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, from_vertex ? g.reach1[1] : g.reach1[0],
                 from_vertex ? g.reach2[1] : g.reach2[0]);
     live = w.next_cell(Q, g);
   }
@@ -371,7 +373,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
       const unsigned j = w.j;
       const double qlo = Q.lo[j];
       const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
-      if (own && overlap3(P, i, Q, j)) {
+      if (own && overlap3(pb, qlo, Q, j)) {
         const int32_t qobj = Q.obj[j];
         const int32_t vtx = from_vertex ? pid : Q.id[j];
         const int32_t fc = from_vertex ? Q.id[j] : pid;
@@ -406,6 +408,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
   if ((long long)blockIdx.x * blockDim.x >= ne) return;
   bool live = i < ne;
   Walker w;
+  Box6 pb{};
   double lo = 0.0;
   int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
   if (live) {
@@ -414,7 +417,8 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     eobj = E.obj[i];
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
-    walker_init(w, g, lo, E.hi[i], E.alo[i], E.ahi[i], E.blo[i], E.bhi[i], g.reach1[2], g.reach2[2]);
+    pb = box_at(E, i);
+    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2]);
     live = w.next_cell(E, g);
   }
   for (;;) {
@@ -426,7 +430,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
       const double qlo = E.lo[j];
       const int32_t oid = E.id[j];
       const bool own = qlo > lo || (qlo == lo && oid > eid);
-      if (own && overlap3(E, i, E, j)) {
+      if (own && overlap3(pb, qlo, E, j)) {
         bool ok = true;
         if (E.obj[j] == eobj) {
           if (exclude_self) ok = false;

@@ -174,9 +174,20 @@ __device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double lo,
   w.q_hi = quantise(hi, g);
 }
 
-__device__ __forceinline__ bool overlap3(const SortedBoxes& P, long long i, const SortedBoxes& Q, long long j) {
-  return P.lo[i] <= Q.hi[j] && Q.lo[j] <= P.hi[i] && P.alo[i] <= Q.ahi[j] && Q.alo[j] <= P.ahi[i] &&
-         P.blo[i] <= Q.bhi[j] && Q.blo[j] <= P.bhi[i];
+// A scanning box held in registers for the length of its walk.
+struct Box6 {
+  double lo, hi, alo, ahi, blo, bhi;
+};
+
+__device__ __forceinline__ Box6 box_at(const SortedBoxes& P, long long i) {
+  return Box6{P.lo[i], P.hi[i], P.alo[i], P.ahi[i], P.blo[i], P.bhi[i]};
+}
+
+// Inclusive overlap on all three axes (Overlap, :270-274); qlo is Q.lo[j],
+// already loaded by the caller's ownership test.
+__device__ __forceinline__ bool overlap3(const Box6& p, double qlo, const SortedBoxes& Q, long long j) {
+  return p.lo <= Q.hi[j] && qlo <= p.hi && p.alo <= Q.ahi[j] && Q.alo[j] <= p.ahi && p.blo <= Q.bhi[j] &&
+         Q.blo[j] <= p.bhi;
 }
 
 __device__ __forceinline__ unsigned long long pair_key(unsigned a, unsigned b, int pack_shift) {

@@ -530,6 +530,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
   }
   if (!__any_sync(kFull, live)) return;
   Walker w;
+  Box6 pb{};
   SortedBoxes Q{};
   Grid g{};
   double lo = 0.0;
@@ -546,7 +547,8 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
     lo = B.S.lo[i];
     pid = B.S.id[i];
     pobj = B.S.obj[i];
-    walker_init(w, g, lo, B.S.hi[i], B.S.alo[i], B.S.ahi[i], B.S.blo[i], B.S.bhi[i],
+    pb = box_at(B.S, (long long)i);
+    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi,
                 from_vertex ? g.reach1[1] : g.reach1[0], from_vertex ? g.reach2[1] : g.reach2[0]);
     live = w.next_cell(Q, g);
   }
@@ -558,7 +560,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
       const unsigned j = w.j;
       const double qlo = Q.lo[j];
       const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
-      if (own && overlap3(B.S, (long long)i, Q, j)) {
+      if (own && overlap3(pb, qlo, Q, j)) {
         const int32_t qobj = Q.obj[j];
         const int32_t vtx = from_vertex ? pid : Q.id[j];
         const int32_t fc = from_vertex ? Q.id[j] : pid;
@@ -596,6 +598,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
   }
   if (!__any_sync(kFull, live)) return;
   Walker w;
+  Box6 pb{};
   SortedBoxes E{};
   Grid g{};
   double lo = 0.0;
@@ -614,7 +617,8 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
     eobj = B.S.obj[i];
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
-    walker_init(w, g, lo, B.S.hi[i], B.S.alo[i], B.S.ahi[i], B.S.blo[i], B.S.bhi[i], g.reach1[2], g.reach2[2]);
+    pb = box_at(B.S, (long long)i);
+    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2]);
     live = w.next_cell(E, g);
   }
   for (;;) {
@@ -626,7 +630,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
       const double qlo = E.lo[j];
       const int32_t oid = E.id[j];
       const bool own = qlo > lo || (qlo == lo && oid > eid);
-      if (own && overlap3(B.S, (long long)i, E, j)) {
+      if (own && overlap3(pb, qlo, E, j)) {
         bool ok = true;
         if (E.obj[j] == eobj) {
           if (exclude_self) ok = false;
