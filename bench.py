@@ -415,7 +415,12 @@ class ClothWorkload:
 
         self.torch = torch
         self.seed = 20261203 + rank
-        self.scene = scenes.cloth_on_sphere(seed=self.seed)
+        if CLOTH_N == 513:
+            self.scene = scenes.cloth_on_sphere(seed=self.seed)
+        else:  # a smaller instance with the same proportions (profiling cases)
+            k = max(8, int(round(250 * CLOTH_N / 513)))
+            self.scene = scenes.cloth_on_sphere(n=CLOTH_N, sphere_lon=k, sphere_rings=max(6, (k * 4) // 5),
+                                                seed=self.seed)
         self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
         self.top_k = 4096
         self.pipe = ScenePipeline(self.scene, device, exclude_self=False, config=self.cfg, narrow="anyhit",
@@ -441,8 +446,9 @@ class ClothWorkload:
     def config(self) -> dict:
         sp = self.scene["spec"]
         s = self.first_summary
-        return {"workload": "dense-contact stress: 513 x 513 cloth grid (524,288 triangles) draped onto a "
-                            "100,000-triangle UV sphere (250 x 200 rings), 1e-4 initial gap, FP64, self pairs with "
+        return {"workload": f"dense-contact stress: {sp['cloth_n']} x {sp['cloth_n']} cloth grid "
+                            f"({sp['cloth_triangles']:,} triangles) draped onto a {sp['sphere_triangles']:,}-triangle "
+                            "UV sphere, 1e-4 initial gap, FP64, self pairs with "
                             "adjacency exclusion, swept-AABB candidates then scheduled any-hit with fallback replay "
                             "over object-pair groups (priorities from a seeded uniform scheduler stub, top-K "
                             f"{self.top_k}); a query is one exact call of the procedure",
@@ -947,6 +953,7 @@ def run_serve(args) -> dict:
 
 
 BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
+CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = configs[3])
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
 
@@ -1072,13 +1079,15 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--scenes", type=int, default=256, help="batch: number of scenes")
+    ap.add_argument("--cloth-n", type=int, default=513, help="cloth: grid vertices per side (513 = the stress config)")
     ap.add_argument("--autotune-reps", type=int, default=3,
                     help="batch: graph replays per autotuner trial (0: the library's default launch shape)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     args = ap.parse_args()
-    global BATCH_SCENES, AUTOTUNE_REPS
+    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N
     BATCH_SCENES, AUTOTUNE_REPS = max(1, args.scenes), max(0, args.autotune_reps)
+    CLOTH_N = max(9, args.cloth_n)
     if args.impl == "reference":
         line = run_reference(args)
     elif args.workload == "serve":
