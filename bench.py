@@ -655,14 +655,23 @@ def _barrier(world):
 
 
 def _max_over_ranks(world, value: float) -> float:
+    """The slowest rank's value (all ranks call this in the same order)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replica_rate(world: int, units_per_rank: float, ms_per_rank: float) -> tuple[float, float]:
+    """Whole-job rate of N replicas: all ranks' units over the slowest rank's
+    time (max over ranks), and that time.  Every rank calls it."""
+    ms = _max_over_ranks(world, ms_per_rank)
+    return units_per_rank * world / (ms * 1e-3), ms
 
 
 def time_steps(torch, fn, steps, flush, stream):
@@ -731,11 +740,8 @@ def run_b200(args) -> dict | None:
     e2e_times = time_steps(torch, wl.step_e2e, args.steps, flush, stream)
     torch.cuda.synchronize()
     ms = statistics.mean(times)
-    ms_max = _max_over_ranks(world, ms)
-    e2e_ms = _max_over_ranks(world, statistics.mean(e2e_times))
-    total_q = wl.queries * world
-    value = total_q / (ms_max * 1e-3)
-    e2e_value = total_q / (e2e_ms * 1e-3)
+    value, ms_max = replica_rate(world, wl.queries, ms)
+    e2e_value, e2e_ms = replica_rate(world, wl.queries, statistics.mean(e2e_times))
     n_kernels, kernel_names = count_kernels(torch, getattr(wl, "step_uncaptured", wl.step))
     census = wl.census()
     fp64_rate = certify.probe_fp64_rate(dev)
