@@ -34,6 +34,7 @@
 // Overlapping boxes of different objects imply overlapping object envelopes
 // (each box lies inside its object's envelope), so beyond culling only the
 // same-object rule remains.
+#include <cub/block/block_radix_sort.cuh>
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -465,6 +466,41 @@ __global__ void unpack_pairs_kernel(unsigned long long* p, long long n, int shif
   p[i] = ((k >> shift) << 32) | (k & ((1ull << shift) - 1ull));
 }
 
+// Pair lists that fit one block are sorted in ONE launch for both families
+// (block 0: vertex-face, block 1: edge-edge): padding, a block radix sort of
+// the packed keys and the unpack, instead of a fill, a device-wide sort and
+// an unpack launch per family.
+constexpr int kSmallSortThreads = 1024;
+constexpr int kSmallSortItems = 8;
+constexpr long long kSmallSortCap = (long long)kSmallSortThreads * kSmallSortItems;
+using SmallSort = cub::BlockRadixSort<unsigned long long, kSmallSortThreads, kSmallSortItems>;
+
+__global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
+    unsigned long long* vf, long long vf_cap, int vf_bits, int vf_shift, unsigned long long* ee, long long ee_cap,
+    int ee_bits, int ee_shift, const BroadScratch* sc) {
+  extern __shared__ __align__(16) unsigned char smem_sort[];
+  typename SmallSort::TempStorage& tmp = *reinterpret_cast<typename SmallSort::TempStorage*>(smem_sort);
+  const bool is_vf = blockIdx.x == 0;
+  unsigned long long* p = is_vf ? vf : ee;
+  const long long cap = is_vf ? vf_cap : ee_cap;
+  if (p == nullptr || cap <= 0) return;  // uniform per block
+  const int bits = is_vf ? vf_bits : ee_bits, shift = is_vf ? vf_shift : ee_shift;
+  const long long count = (long long)(is_vf ? sc->vf_count : sc->ee_count);
+  const long long n = count < cap ? count : cap;
+  unsigned long long k[kSmallSortItems];
+#pragma unroll
+  for (int u = 0; u < kSmallSortItems; ++u) {
+    const long long i = (long long)threadIdx.x * kSmallSortItems + u;
+    k[u] = i < n ? p[i] : ~0ull;
+  }
+  SmallSort(tmp).Sort(k, 0, bits);  // ~0 padding has every sorted bit set: it sorts last
+#pragma unroll
+  for (int u = 0; u < kSmallSortItems; ++u) {
+    const long long i = (long long)threadIdx.x * kSmallSortItems + u;
+    if (i < cap) p[i] = k[u] == ~0ull ? ~0ull : ((k[u] >> shift) << 32) | (k[u] & ((1ull << shift) - 1ull));
+  }
+}
+
 __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long* counts) {
   counts[0] = sc->vf_count;
   counts[1] = sc->ee_count;
@@ -645,8 +681,11 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   // with sorting, pairs are emitted packed so that the sort touches fewer bits
   const int vf_shift = sort_out ? std::max(1, bit_length(scene.nf)) : 0;
   const int ee_shift = sort_out ? std::max(1, bit_length(scene.ne)) : 0;
-  if (sort_out && vf_cap > 0) fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
-  if (sort_out && ee_cap > 0) fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
+  const bool small_sort = sort_out && vf_cap <= kSmallSortCap && ee_cap <= kSmallSortCap;
+  if (sort_out && !small_sort && vf_cap > 0)
+    fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
+  if (sort_out && !small_sort && ee_cap > 0)
+    fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
   if (scene.nv + scene.nf > 0 && vf_out != nullptr)
     sweep_vf_kernel<<<grid_for(scene.nv + scene.nf, kThreads), kThreads, 0, s>>>(
         L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out, (unsigned long long)vf_cap, L.sc);
@@ -655,7 +694,17 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
                                                                       ee_shift, ee_out, (unsigned long long)ee_cap,
                                                                       L.sc);
   P2C_CUDA(cudaGetLastError());
-  if (sort_out) {
+  if (small_sort) {
+    static bool attr_set = false;  // the block sort's storage is above the 48 KB static limit
+    if (!attr_set) {
+      P2C_CUDA(cudaFuncSetAttribute(small_sort_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)sizeof(SmallSort::TempStorage)));
+      attr_set = true;
+    }
+    small_sort_pairs_kernel<<<2, kSmallSortThreads, sizeof(SmallSort::TempStorage), s>>>(
+        vf_out, vf_cap, bit_length(scene.nv) + vf_shift, vf_shift, ee_out, ee_cap, bit_length(scene.ne) + ee_shift,
+        ee_shift, L.sc);
+  } else if (sort_out) {
     int rc = sort_pairs(vf_out, vf_cap, bit_length(scene.nv) + vf_shift, L, s);
     if (rc != P2C_OK) return rc;
     rc = sort_pairs(ee_out, ee_cap, bit_length(scene.ne) + ee_shift, L, s);

@@ -181,3 +181,30 @@ def test_undecided_queue_and_invalid_geometry(cuda_device, oracle_mod):
     pipe2 = ScenePipeline(bad, cuda_device, exclude_self=True, config=cfg)
     with pytest.raises(ValueError, match="finite"):
         pipe2.step_checked()
+
+
+@pytest.mark.parametrize("self_pairs", [False, True])
+def test_small_pair_buffers_sort_like_large_ones(cuda_device, self_pairs):
+    """Pair buffers of at most 8,192 entries take the one-launch block sort;
+    the lists, padding, summary and certificates equal the device-wide sort's."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.certify import CertConfig
+    from p2cccd_b200.scene import ScenePipeline
+
+    s = (scenes.cloth_on_sphere(n=17, sphere_lon=24, sphere_rings=16, gap=1e-3, drop=0.05) if self_pairs
+         else scenes.two_spheres(n_lon=40, n_rings=30))
+    cfg = CertConfig(1e-6, 1e-6, 32)
+    big = ScenePipeline(s, cuda_device, exclude_self=not self_pairs, config=cfg)
+    sb = big.step_checked()
+    small = ScenePipeline(s, cuda_device, exclude_self=not self_pairs, config=cfg)
+    small.step_checked()
+    small.fit_capacities(margin=1.0, slack=7)
+    assert small.vf_cap <= 8192 and small.ee_cap <= 8192 and big.vf_cap > 8192
+    ss = small.step_checked()
+    assert ss == sb
+    for a, b in zip(small.pairs(), big.pairs()):
+        assert np.array_equal(a, b)
+    for a, b in zip(small.results(), big.results()):
+        assert np.array_equal(_bytes(a), _bytes(b))
+    tail = small.vf_pairs[len(small.pairs()[0]):small.vf_cap].cpu().numpy().view(np.uint64)
+    assert len(tail) == 7 and (tail == np.uint64(0xFFFFFFFFFFFFFFFF)).all()
