@@ -433,6 +433,76 @@ int p2c_group_anyhit(const p2c_scene* scene, int family, const uint64_t* pairs_d
                      p2c_anyhit_summary* summary_dev, void* workspace_dev, size_t workspace_bytes,
                      void* stream);
 
+/* ---- proxy scenes: patch-level candidates with time slabs ---------------- */
+/* The proxy primitives of a built ProxyScene (rt_candidate/proxy_scene.h:29-46)
+ * as device arrays; proxy i has proxy_id i. */
+typedef struct p2c_proxy_scene {
+  uint64_t query_id;
+  int64_t n;                     /* proxy primitives */
+  const uint32_t* object_id;
+  const uint32_t* patch_id;
+  const uint32_t* slab_id;
+  const uint8_t* proxy_type;     /* 1 swept AABB, 2 capsule */
+  const double* t0;              /* slab interval */
+  const double* t1;
+  const double* bounds;          /* n x 6: min x, y, z, max x, y, z */
+  const double* motion_bound;    /* n x 4: translation_bound, rotation_angle, radial_motion_bound,
+                                    conservative_radius */
+} p2c_proxy_scene;
+
+/* RawCandidateHit (rt_candidate/candidate_buffer.h:19-31), 64 bytes. */
+typedef struct p2c_raw_candidate_hit {
+  uint64_t query_id;
+  uint64_t pair_key;             /* lo << 32 | hi proxy index */
+  uint32_t proxy_a_index, proxy_b_index;
+  uint32_t slab_id;
+  uint32_t rt_hit_count;
+  uint32_t flags;                /* 1 valid | 2 AABB overlap */
+  uint32_t reserved0;
+  float motion_bound[4];
+  uint32_t reserved1, reserved2;
+} p2c_raw_candidate_hit;
+
+/* CandidateRecord (common/runtime_contracts.h:41-56), 80 bytes. */
+typedef struct p2c_candidate_record {
+  uint32_t schema_version;
+  uint32_t pad0;
+  uint64_t candidate_id;
+  uint64_t query_id;
+  uint32_t slab_id;
+  uint32_t object_a_id, patch_a_id, object_b_id, patch_b_id;
+  uint8_t proxy_type_a, proxy_type_b;
+  uint8_t pad1[2];
+  uint32_t rt_hit_count;
+  float motion_bound[4];
+  uint32_t proxy_features_offset;
+  uint32_t flags;
+  uint32_t pad2;
+} p2c_candidate_record;
+
+size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap);
+
+/* Candidates of a proxy scene: GenerateRawCandidatesCpu then
+ * CompactRawCandidates (rt_candidate/candidate_buffer.cpp:144-227) on the
+ * device.  Raw hits are the proxy pairs of different objects in one slab
+ * whose time intervals and inclusive AABBs overlap, written in the
+ * reference's (i, j) order; candidates are the hits compacted by (slab,
+ * first (object, patch), second (object, patch), proxy types) with the first
+ * proxy the smaller (object, patch, proxy) tuple, in that key order, with
+ * candidate_id 1, 2, ..., hit counts summed, motion bounds maxed and flags
+ * or-ed.  counts_dev[0..2] = {raw hits, candidates, error word (1: a proxy
+ * fails ValidateProxyScene's per-proxy checks, rt_candidate/proxy_scene.cpp:
+ * 143-151: type, finite t0 < t1, finite ordered bounds; 2: a hit's float
+ * motion bound is negative or non-finite, which ValidateRawHit rejects in
+ * compaction, candidate_buffer.cpp:95-99; 4: raw_cap overflowed)}.  Proxy
+ * ids equal to the array index and the global slab partition (:58-85) are
+ * the caller's checks.  Raw hits beyond raw_cap are dropped (the count is
+ * the total); candidate capacity is raw_cap; raw_cap 0 only counts.  No host
+ * sync. */
+int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* raw_dev, int64_t raw_cap,
+                         p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
+                         size_t workspace_bytes, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

@@ -377,3 +377,84 @@ class RefToolScene:
         if T.ref_tool_time_all_exact(eps_time, eps_space, max_depth, _p(secs), _p(calls)):
             raise ValueError(T.ref_tool_last_error().decode())
         return {"candidates_s": float(secs[0]), "certify_s": float(secs[1]), "calls": int(calls[0])}
+
+
+# ---- proxy-scene candidates (rt_candidate/candidate_buffer.cpp) ----
+
+def _proxy_args(sc):
+    a = {k: np.ascontiguousarray(sc[k]) for k in ("object_id", "patch_id", "slab_id", "proxy_type", "t0", "t1",
+                                                   "bounds", "motion_bound")}
+    return a
+
+
+def ref_proxy_candidates(sc: dict):
+    """The reference's GenerateRawCandidatesCpu + CompactRawCandidates on a
+    proxy scene: (raw hits as 64-byte records, candidates as 80-byte records)."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_proxy_ready"):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        R.ref_proxy_candidates.argtypes = [ctypes.c_uint64, i64] + [vp] * 8 + [vp, i64, vp, i64, vp, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._proxy_ready = True
+    a = _proxy_args(sc)
+    n_raw, n_cand = ctypes.c_int64(0), ctypes.c_int64(0)
+    args = [int(sc["query_id"]), int(sc["n"])] + [_p(a[k]) for k in ("object_id", "patch_id", "slab_id",
+                                                                      "proxy_type", "t0", "t1", "bounds",
+                                                                      "motion_bound")]
+    if R.ref_proxy_candidates(*args, None, 0, None, 0, ctypes.byref(n_raw), ctypes.byref(n_cand)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    raw = np.zeros(max(1, n_raw.value), dtype=RAW_HIT_DTYPE)
+    cand = np.zeros(max(1, n_cand.value), dtype=CANDIDATE_RECORD_DTYPE)
+    R.ref_proxy_candidates(*args, _p(raw), n_raw.value, _p(cand), n_cand.value, ctypes.byref(n_raw),
+                           ctypes.byref(n_cand))
+    return raw[:n_raw.value], cand[:n_cand.value]
+
+
+def proxy_candidates(sc: dict):
+    """Restatement of GenerateRawCandidatesCpu (candidate_buffer.cpp:144-179)
+    and CompactRawCandidates (:181-227) in numpy: every pair i < j of
+    different objects in one slab whose time intervals and inclusive AABBs
+    overlap, in (i, j) order; then hits grouped by MakeCandidateKey (:104-124)
+    in key order with counts, float-max motion bounds and or-ed flags."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
+
+    a = _proxy_args(sc)
+    n = int(sc["n"])
+    obj, pat, slab, typ = a["object_id"], a["patch_id"], a["slab_id"], a["proxy_type"]
+    t0, t1, b, mb = a["t0"], a["t1"], a["bounds"], a["motion_bound"]
+    hits = []
+    for i in range(n):
+        j = np.arange(i + 1, n)
+        ok = (obj[j] != obj[i]) & (slab[j] == slab[i]) & (t0[i] < t1[j]) & (t0[j] < t1[i])
+        for ax in range(3):
+            ok &= ~((b[i, 3 + ax] < b[j, ax]) | (b[j, 3 + ax] < b[i, ax]))
+        hits.extend((i, int(x)) for x in j[ok])
+    raw = np.zeros(len(hits), dtype=RAW_HIT_DTYPE)
+    for k, (i, j) in enumerate(hits):
+        raw[k]["query_id"] = sc["query_id"]
+        raw[k]["pair_key"] = (i << 32) | j
+        raw[k]["proxy_a_index"], raw[k]["proxy_b_index"] = i, j
+        raw[k]["slab_id"] = slab[i]
+        raw[k]["rt_hit_count"] = 1
+        raw[k]["flags"] = 3
+        raw[k]["motion_bound"] = np.maximum(mb[i], mb[j]).astype(np.float32)
+    groups = {}
+    for k, (i, j) in enumerate(hits):
+        f, s2 = (i, j) if (obj[i], pat[i], i) <= (obj[j], pat[j], j) else (j, i)
+        key = (int(slab[i]), int(obj[f]), int(pat[f]), int(obj[s2]), int(pat[s2]), int(typ[f]), int(typ[s2]))
+        if key not in groups:
+            groups[key] = [0, raw[k]["motion_bound"].copy(), 0]
+        g = groups[key]
+        g[0] += 1
+        g[1] = np.maximum(g[1], raw[k]["motion_bound"])
+        g[2] |= int(raw[k]["flags"])
+    cand = np.zeros(len(groups), dtype=CANDIDATE_RECORD_DTYPE)
+    for cid, key in enumerate(sorted(groups)):
+        c = cand[cid]
+        c["schema_version"], c["candidate_id"], c["query_id"] = 1, cid + 1, sc["query_id"]
+        (c["slab_id"], c["object_a_id"], c["patch_a_id"], c["object_b_id"], c["patch_b_id"], c["proxy_type_a"],
+         c["proxy_type_b"]) = key
+        c["rt_hit_count"], c["motion_bound"], c["flags"] = groups[key]
+    return raw, cand

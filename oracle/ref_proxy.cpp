@@ -1,0 +1,103 @@
+// ref_proxy.cpp — C ABI over the reference's proxy-scene candidate
+// generation (rt_candidate/candidate_buffer.cpp: GenerateRawCandidatesCpu,
+// CompactRawCandidates; rt_candidate/proxy_scene.cpp: ValidateProxyScene),
+// compiled unchanged into oracle/_ref/libp2c_ref.so.
+//
+// TEST INFRASTRUCTURE ONLY: tests pin the device proxy candidates and the
+// restated checker to it; the product never loads it.
+#include "rt_candidate/candidate_buffer.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../include/p2c_b200.h"
+
+static_assert(sizeof(p2cccd::RawCandidateHit) == sizeof(p2c_raw_candidate_hit));
+static_assert(sizeof(p2cccd::CandidateRecord) == sizeof(p2c_candidate_record));
+static_assert(offsetof(p2cccd::CandidateRecord, candidate_id) == offsetof(p2c_candidate_record, candidate_id));
+static_assert(offsetof(p2cccd::CandidateRecord, proxy_type_a) == offsetof(p2c_candidate_record, proxy_type_a));
+static_assert(offsetof(p2cccd::CandidateRecord, rt_hit_count) == offsetof(p2c_candidate_record, rt_hit_count));
+static_assert(offsetof(p2cccd::CandidateRecord, flags) == offsetof(p2c_candidate_record, flags));
+static_assert(offsetof(p2cccd::RawCandidateHit, motion_bound) == offsetof(p2c_raw_candidate_hit, motion_bound));
+
+namespace {
+thread_local std::string g_proxy_error;
+}
+
+extern "C" {
+
+const char* ref_proxy_last_error(void) { return g_proxy_error.c_str(); }
+
+// Proxy arrays as p2c_proxy_scene lays them out (host memory).  Returns 0 and
+// the counts, or 1 with the reference's error message.  Outputs (may be NULL
+// for a sizing call) receive min(count, cap) records.
+int ref_proxy_candidates(uint64_t query_id, int64_t n, const uint32_t* object_id, const uint32_t* patch_id,
+                         const uint32_t* slab_id, const uint8_t* proxy_type, const double* t0, const double* t1,
+                         const double* bounds, const double* motion_bound, p2c_raw_candidate_hit* raw_out,
+                         int64_t raw_cap, p2c_candidate_record* cand_out, int64_t cand_cap, int64_t* n_raw,
+                         int64_t* n_cand) {
+  p2cccd::ProxyScene scene;
+  scene.query_id = query_id;
+  scene.primitives.resize(static_cast<std::size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    p2cccd::ProxyPrimitive& p = scene.primitives[static_cast<std::size_t>(i)];
+    p.proxy_id = static_cast<std::uint32_t>(i);
+    p.object_id = object_id[i];
+    p.patch_id = patch_id[i];
+    p.slab_id = slab_id[i];
+    p.proxy_type = static_cast<p2cccd::ProxyType>(proxy_type[i]);
+    p.t0 = t0[i];
+    p.t1 = t1[i];
+    for (int a = 0; a < 3; ++a) {
+      p.bounds.min[a] = bounds[6 * i + a];
+      p.bounds.max[a] = bounds[6 * i + 3 + a];
+    }
+    p.motion_bound.translation_bound = motion_bound[4 * i + 0];
+    p.motion_bound.rotation_angle = motion_bound[4 * i + 1];
+    p.motion_bound.radial_motion_bound = motion_bound[4 * i + 2];
+    p.motion_bound.conservative_radius = motion_bound[4 * i + 3];
+  }
+  p2cccd::RawCandidateBuffer raw;
+  p2cccd::Status st = p2cccd::GenerateRawCandidatesCpu(scene, query_id, &raw);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  std::vector<p2cccd::CandidateRecord> cands;
+  st = p2cccd::CompactRawCandidates(scene, raw, &cands);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  *n_raw = static_cast<int64_t>(raw.hits.size());
+  *n_cand = static_cast<int64_t>(cands.size());
+  if (raw_out != nullptr)
+    for (int64_t k = 0; k < *n_raw && k < raw_cap; ++k)
+      std::memcpy(&raw_out[k], &raw.hits[static_cast<std::size_t>(k)], sizeof(p2c_raw_candidate_hit));
+  if (cand_out != nullptr)
+    for (int64_t k = 0; k < *n_cand && k < cand_cap; ++k) {
+      std::memset(&cand_out[k], 0, sizeof(p2c_candidate_record));
+      const p2cccd::CandidateRecord& c = cands[static_cast<std::size_t>(k)];
+      p2c_candidate_record& o = cand_out[k];
+      o.schema_version = c.schema_version;
+      o.candidate_id = c.candidate_id;
+      o.query_id = c.query_id;
+      o.slab_id = c.slab_id;
+      o.object_a_id = c.object_a_id;
+      o.patch_a_id = c.patch_a_id;
+      o.object_b_id = c.object_b_id;
+      o.patch_b_id = c.patch_b_id;
+      o.proxy_type_a = static_cast<uint8_t>(c.proxy_type_a);
+      o.proxy_type_b = static_cast<uint8_t>(c.proxy_type_b);
+      o.rt_hit_count = c.rt_hit_count;
+      for (int a = 0; a < 4; ++a) o.motion_bound[a] = c.motion_bound[a];
+      o.proxy_features_offset = c.proxy_features_offset;
+      o.flags = c.flags;
+    }
+  return 0;
+}
+
+}  // extern "C"

@@ -60,6 +60,25 @@ CERTIFY_STATS_DTYPE = np.dtype([
     ("busy_lane_iterations", "<u8"),
 ])
 
+# RawCandidateHit (rt_candidate/candidate_buffer.h:19-31) and CandidateRecord
+# (common/runtime_contracts.h:41-56), the broad-phase output contracts.
+RAW_HIT_DTYPE = np.dtype({
+    "names": ["query_id", "pair_key", "proxy_a_index", "proxy_b_index", "slab_id", "rt_hit_count", "flags",
+              "reserved0", "motion_bound", "reserved1", "reserved2"],
+    "formats": ["<u8", "<u8", "<u4", "<u4", "<u4", "<u4", "<u4", "<u4", ("<f4", (4,)), "<u4", "<u4"],
+    "offsets": [0, 8, 16, 20, 24, 28, 32, 36, 40, 56, 60],
+    "itemsize": 64,
+})
+CANDIDATE_RECORD_DTYPE = np.dtype({
+    "names": ["schema_version", "candidate_id", "query_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id",
+              "patch_b_id", "proxy_type_a", "proxy_type_b", "rt_hit_count", "motion_bound",
+              "proxy_features_offset", "flags"],
+    "formats": ["<u4", "<u8", "<u8", "<u4", "<u4", "<u4", "<u4", "<u4", "u1", "u1", "<u4", ("<f4", (4,)), "<u4",
+                "<u4"],
+    "offsets": [0, 8, 16, 24, 28, 32, 36, 40, 44, 45, 48, 52, 68, 72],
+    "itemsize": 80,
+})
+
 assert POINT_TRIANGLE_DTYPE.itemsize == 240
 assert EDGE_EDGE_DTYPE.itemsize == 240
 assert INTERVAL_RESULT_DTYPE.itemsize == 72

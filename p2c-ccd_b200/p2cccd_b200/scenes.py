@@ -166,3 +166,48 @@ def uneven_batch(n_scenes: int = 256, tri_min: float = 1.0e3, tri_max: float = 2
                      "triangles": int(2 * len(f)), "contact_parameter": frac, "gap": gap, "seed": seed}
         out.append(s)
     return out
+
+
+def proxy_scene(n_objects: int = 6, patches_per_object: int = 40, n_slabs: int = 4, seed: int = 20261203,
+                query_id: int = 7, duplicates: float = 0.0) -> dict:
+    """A proxy scene (the arrays p2c_proxy_scene reads): every object's patches
+    as boxes in every time slab of a global partition of [0, 1], objects
+    drifting toward each other so that patches of different objects overlap
+    in some slabs; swept-AABB and capsule proxy types; motion bounds >= 0.
+    ``duplicates`` adds that fraction of extra proxies repeating an existing
+    (object, patch, slab) with other bounds, so that several raw hits
+    compact into one candidate."""
+    g = rng(seed)
+    edges = np.linspace(0.0, 1.0, n_slabs + 1)
+    rows = []
+    for o in range(n_objects):
+        center = g.uniform(-1.0, 1.0, 3)
+        vel = -center * g.uniform(0.5, 1.0)
+        ptype = 1 + (o % 2)
+        offs = g.normal(0.0, 0.25, (patches_per_object, 3))
+        half = g.uniform(0.02, 0.12, (patches_per_object, 3))
+        for sl in range(n_slabs):
+            t0, t1 = edges[sl], edges[sl + 1]
+            c0, c1 = center + vel * t0, center + vel * t1
+            for pch in range(patches_per_object):
+                lo = np.minimum(c0, c1) + offs[pch] - half[pch]
+                hi = np.maximum(c0, c1) + offs[pch] + half[pch]
+                mb = g.uniform(0.0, 0.2, 4)
+                rows.append((o, pch, sl, ptype, t0, t1, lo, hi, mb))
+                if g.random() < duplicates:
+                    d = g.normal(0.0, 0.03, 3)
+                    rows.append((o, pch, sl, ptype, t0, t1, lo + d, hi + d, g.uniform(0.0, 0.2, 4)))
+    n = len(rows)
+    out = {"query_id": query_id, "n": n,
+           "object_id": np.array([r[0] for r in rows], np.uint32),
+           "patch_id": np.array([r[1] for r in rows], np.uint32),
+           "slab_id": np.array([r[2] for r in rows], np.uint32),
+           "proxy_type": np.array([r[3] for r in rows], np.uint8),
+           "t0": np.array([r[4] for r in rows], np.float64),
+           "t1": np.array([r[5] for r in rows], np.float64),
+           "bounds": np.array([np.concatenate([r[6], r[7]]) for r in rows], np.float64).reshape(n, 6),
+           "motion_bound": np.array([r[8] for r in rows], np.float64).reshape(n, 4)}
+    perm = g.permutation(n)  # proxies in no particular order (proxy_id = index)
+    for k in ("object_id", "patch_id", "slab_id", "proxy_type", "t0", "t1", "bounds", "motion_bound"):
+        out[k] = np.ascontiguousarray(out[k][perm])
+    return out

@@ -806,3 +806,255 @@ def _materialize_host(scene: dict, pairs: np.ndarray, family: int) -> np.ndarray
         rec[names[2 + k]]["position_t0"] = scene["v_t0"][verts[:, k]]
         rec[names[2 + k]]["position_t1"] = scene["v_t1"][verts[:, k]]
     return rec
+
+
+# ---------------------------------------------------------------------------
+# proxy scenes: patch-level candidates (rt_candidate/, py_module.cpp:1541-1650,
+# 1863-1882).  Raw hits and compaction run on the GPU (p2c_proxy_candidates).
+
+
+class Aabb(_Struct):
+    _fields = (("min", lambda: [0.0, 0.0, 0.0]), ("max", lambda: [0.0, 0.0, 0.0]))
+
+
+class PatchMotionBound(_Struct):
+    _fields = (("patch_id", 0), ("t0", 0.0), ("t1", 1.0), ("center_t0", lambda: [0.0, 0.0, 0.0]),
+               ("center_t1", lambda: [0.0, 0.0, 0.0]), ("translation_bound", 0.0), ("rotation_angle", 0.0),
+               ("center_rotation_bound", 0.0), ("surface_rotation_bound", 0.0), ("radial_motion_bound", 0.0),
+               ("conservative_radius", 0.0))
+
+
+class CapsuleProxy(_Struct):
+    _fields = (("patch_id", 0), ("endpoint0", lambda: [0.0, 0.0, 0.0]), ("endpoint1", lambda: [0.0, 0.0, 0.0]),
+               ("radius", 0.0), ("motion_bound", PatchMotionBound))
+
+
+class ProxyPrimitive(_Struct):  # rt_candidate/proxy_scene.h:29-41
+    _fields = (("proxy_id", 0), ("object_id", 0), ("patch_id", 0), ("slab_id", 0), ("motion_segment_id", 0),
+               ("proxy_type", ProxyType.UNKNOWN), ("t0", 0.0), ("t1", 1.0), ("bounds", Aabb),
+               ("capsule", CapsuleProxy), ("motion_bound", PatchMotionBound))
+
+
+class ProxyScene(_Struct):  # :43-46
+    _fields = (("query_id", 0), ("primitives", list))
+
+
+class RawCandidateHit(_Struct):  # rt_candidate/candidate_buffer.h
+    _fields = (("query_id", 0), ("pair_key", 0), ("proxy_a_index", 0), ("proxy_b_index", 0), ("slab_id", 0),
+               ("rt_hit_count", 0), ("flags", 0), ("motion_bound", lambda: [0.0, 0.0, 0.0, 0.0]))
+
+
+class RawCandidateBuffer(_Struct):
+    _fields = (("hits", list),)
+
+
+class CandidateRecord(_Struct):  # common/runtime_contracts.h:41-56
+    _fields = (("schema_version", 1), ("candidate_id", 0), ("query_id", 0), ("slab_id", 0), ("object_a_id", 0),
+               ("patch_a_id", 0), ("object_b_id", 0), ("patch_b_id", 0), ("proxy_type_a", ProxyType.UNKNOWN),
+               ("proxy_type_b", ProxyType.UNKNOWN), ("rt_hit_count", 0),
+               ("motion_bound", lambda: [0.0, 0.0, 0.0, 0.0]), ("proxy_features_offset", 0), ("flags", 0))
+
+
+class RtCandidateTiming(_Struct):  # rt_candidate/candidate_generation_result.h:12-19
+    _fields = (("build_ms", 0.0), ("update_ms", 0.0), ("trace_ms", 0.0), ("compact_ms", 0.0), ("stats_ms", 0.0),
+               ("total_ms", 0.0))
+
+
+class CandidateDensityStats(_Struct):  # :21-37
+    _fields = (("schema_version", 1), ("query_id", 0), ("proxy_count", 0), ("object_count", 0), ("slab_count", 0),
+               ("cross_object_same_slab_pair_count", 0), ("raw_hit_count", 0), ("compact_candidate_count", 0),
+               ("raw_hits_per_proxy", 0.0), ("candidates_per_proxy", 0.0), ("candidates_per_slab", 0.0),
+               ("aabb_overlap_ratio", 0.0), ("avg_rt_hits_per_candidate", 0.0), ("timing", RtCandidateTiming),
+               ("backend_name", ""))
+
+
+class CandidateGenerationResult(_Struct):  # :39-45
+    _fields = (("backend_name", ""), ("raw_buffer", RawCandidateBuffer), ("candidates", list),
+               ("timing", RtCandidateTiming), ("density", CandidateDensityStats))
+
+
+def _time_tolerance(t0: float, t1: float) -> float:  # proxy_scene.cpp:41-43
+    return 1.0e-12 * max(1.0, abs(t0), abs(t1), abs(t1 - t0))
+
+
+def _proxy_arrays(scene) -> dict:
+    """The primitive list of a ProxyScene (or the equivalent dict of arrays)
+    as the column arrays p2c_proxy_candidates reads."""
+    if isinstance(scene, dict):
+        return scene
+    prims = scene.primitives
+    n = len(prims)
+    out = {"query_id": int(scene.query_id), "n": n,
+           "object_id": np.fromiter((p.object_id for p in prims), np.uint32, n),
+           "patch_id": np.fromiter((p.patch_id for p in prims), np.uint32, n),
+           "slab_id": np.fromiter((p.slab_id for p in prims), np.uint32, n),
+           "proxy_type": np.fromiter((int(p.proxy_type) for p in prims), np.uint8, n),
+           "t0": np.fromiter((p.t0 for p in prims), np.float64, n),
+           "t1": np.fromiter((p.t1 for p in prims), np.float64, n),
+           "bounds": np.array([[*p.bounds.min, *p.bounds.max] for p in prims], np.float64).reshape(n, 6),
+           "motion_bound": np.array([[p.motion_bound.translation_bound, p.motion_bound.rotation_angle,
+                                      p.motion_bound.radial_motion_bound, p.motion_bound.conservative_radius]
+                                     for p in prims], np.float64).reshape(n, 4)}
+    ids = np.fromiter((p.proxy_id for p in prims), np.int64, n)
+    if np.any(ids != np.arange(n)):  # proxy_scene.cpp:140-142
+        raise ValueError("proxy_id must match primitive array index")
+    return out
+
+
+def _validate_slab_partition(a: dict) -> None:
+    """ValidateGlobalSlabPartition (proxy_scene.cpp:58-85): one time interval
+    per slab id (within TimeTolerance of the first proxy's), and the slab
+    intervals, ordered by start then id, do not overlap."""
+    slab, t0, t1 = np.asarray(a["slab_id"]), np.asarray(a["t0"]), np.asarray(a["t1"])
+    if len(slab) == 0:
+        return
+    ids, first = np.unique(slab, return_index=True)
+    ft0, ft1 = t0[first], t1[first]
+    k = np.searchsorted(ids, slab)
+    tol = 1.0e-12 * np.maximum.reduce([np.ones_like(ft0), np.abs(ft0), np.abs(ft1), np.abs(ft1 - ft0)])
+    if np.any(np.abs(ft0[k] - t0) > tol[k]) or np.any(np.abs(ft1[k] - t1) > tol[k]):
+        raise ValueError("proxy scene slab_id must map to one global time interval")
+    order = np.lexsort((ids, ft0))
+    s0, s1, st = ft0[order], ft1[order], tol[order]
+    for i in range(1, len(order)):
+        t = max(st[i - 1], st[i])
+        if s0[i - 1] < s1[i] - t and s0[i] < s1[i - 1] - t:
+            raise ValueError("proxy scene global slab intervals must not overlap")
+
+
+def _validate_proxies(a: dict) -> None:
+    """ValidateProxyScene's per-proxy checks (proxy_scene.cpp:143-151) for the
+    host-side validator; the device repeats them while generating."""
+    if int(a["query_id"]) == 0:
+        raise ValueError("ProxyScene.query_id is required")
+    typ, t0, t1, b = (np.asarray(a[k]) for k in ("proxy_type", "t0", "t1", "bounds"))
+    if np.any((typ != 1) & (typ != 2)):
+        raise ValueError("proxy primitive has an unsupported proxy type")
+    if not (np.all(np.isfinite(t0)) and np.all(np.isfinite(t1)) and np.all(t0 < t1)):
+        raise ValueError("proxy primitive must satisfy finite t0 < t1")
+    b = b.reshape(-1, 6)
+    if not np.all(np.isfinite(b)):
+        raise ValueError("proxy bounds contain a non-finite value")
+    if np.any(b[:, :3] > b[:, 3:]):
+        raise ValueError("proxy bounds min cannot exceed max")
+
+
+def validate_proxy_scene(scene) -> bool:  # py_module.cpp:1314-1317
+    a = _proxy_arrays(scene)
+    _validate_proxies(a)
+    _validate_slab_partition(a)
+    return True
+
+
+def _run_proxy(scene, query_id: int, raw_only: bool):
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    a = _proxy_arrays(scene)
+    if query_id == 0:
+        raise ValueError("query_id is required")
+    _validate_slab_partition(a)
+    if int(a["query_id"]) == 0:
+        raise ValueError("ProxyScene.query_id is required")
+    if query_id != int(a["query_id"]):
+        raise ValueError("query_id must match ProxyScene.query_id")
+    return a, ProxyCandidates(a).run_checked(raw_only=raw_only)
+
+
+def _raw_objects(raw: np.ndarray) -> RawCandidateBuffer:
+    buf = RawCandidateBuffer()
+    for r in raw:
+        h = RawCandidateHit()
+        h.query_id, h.pair_key = int(r["query_id"]), int(r["pair_key"])
+        h.proxy_a_index, h.proxy_b_index = int(r["proxy_a_index"]), int(r["proxy_b_index"])
+        h.slab_id, h.rt_hit_count, h.flags = int(r["slab_id"]), int(r["rt_hit_count"]), int(r["flags"])
+        h.motion_bound = [float(x) for x in r["motion_bound"]]
+        buf.hits.append(h)
+    return buf
+
+
+def _candidate_objects(cand: np.ndarray) -> list:
+    out = []
+    for r in cand:
+        c = CandidateRecord()
+        for k in ("schema_version", "candidate_id", "query_id", "slab_id", "object_a_id", "patch_a_id",
+                  "object_b_id", "patch_b_id", "rt_hit_count", "proxy_features_offset", "flags"):
+            setattr(c, k, int(r[k]))
+        c.proxy_type_a, c.proxy_type_b = ProxyType(int(r["proxy_type_a"])), ProxyType(int(r["proxy_type_b"]))
+        c.motion_bound = [float(x) for x in r["motion_bound"]]
+        out.append(c)
+    return out
+
+
+def _density(a: dict, raw: np.ndarray, cand: np.ndarray, timing: RtCandidateTiming,
+             backend: str) -> CandidateDensityStats:
+    """ComputeCandidateDensityStats (candidate_stats.cpp:128-170); the pair
+    count of CountCrossObjectSameSlabPairs (:31-43) in closed form: pairs in
+    one slab minus pairs in one (slab, object)."""
+    def ratio(x, y):
+        return float(x) / float(y) if y else 0.0
+
+    slab, obj = np.asarray(a["slab_id"], np.int64), np.asarray(a["object_id"], np.int64)
+    _, per_slab = np.unique(slab, return_counts=True)
+    _, per_so = np.unique(np.stack([slab, obj], 1), axis=0, return_counts=True) if len(slab) else (None, per_slab)
+    d = CandidateDensityStats()
+    d.query_id, d.proxy_count = int(a["query_id"]), int(a["n"])
+    d.object_count, d.slab_count = len(np.unique(obj)), len(per_slab)
+    d.cross_object_same_slab_pair_count = int((per_slab * (per_slab - 1) // 2).sum() -
+                                              (per_so * (per_so - 1) // 2).sum())
+    d.raw_hit_count, d.compact_candidate_count = len(raw), len(cand)
+    d.raw_hits_per_proxy = ratio(d.raw_hit_count, d.proxy_count)
+    d.candidates_per_proxy = ratio(d.compact_candidate_count, d.proxy_count)
+    d.candidates_per_slab = ratio(d.compact_candidate_count, d.slab_count)
+    d.aabb_overlap_ratio = ratio(d.raw_hit_count, d.cross_object_same_slab_pair_count)
+    d.avg_rt_hits_per_candidate = ratio(int(cand["rt_hit_count"].sum()) if len(cand) else 0,
+                                        d.compact_candidate_count)
+    d.timing, d.backend_name = timing, backend
+    return d
+
+
+def generate_raw_candidates_cpu(scene, query_id: int = 0) -> RawCandidateBuffer:  # py_module.cpp:366-371
+    query_id = int(query_id) or int(_proxy_arrays(scene)["query_id"])
+    _, (raw, _cand) = _run_proxy(scene, query_id, raw_only=True)
+    return _raw_objects(raw)
+
+
+def generate_candidates_for_proxy_scene(scene, query_id: int = 0, backend_name: str = "cpu_reference",
+                                        allow_optix_cpu_fallback: bool = False) -> CandidateGenerationResult:
+    """GenerateCandidatesForProxyScene (py_module.cpp:103-116) through
+    CandidateGenerator::GenerateCandidates (candidate_generator.cpp:13-33).
+    The cpu_reference backends run the device path under their own name; the
+    OptiX backends behave as the reference built without OptiX
+    (optix_candidate_tracer.cpp:882-888): an error, or with
+    allow_optix_cpu_fallback the same generation named "optix_cpu_fallback"."""
+    import time
+
+    if backend_name in ("cpu_reference", "cpu_reference_rt"):
+        name = "cpu_reference"
+    elif backend_name in ("optix", "optix_compatible", "optix_rt"):
+        name = "optix_cpu_fallback"
+    else:
+        raise ValueError("unsupported candidate backend: " + str(backend_name))
+    start = time.perf_counter()
+    a = _proxy_arrays(scene)
+    qid = int(query_id) or int(a["query_id"])
+    if qid == 0:
+        raise ValueError("query_id is required")
+    if qid != int(a["query_id"]):
+        raise ValueError("query_id must match ProxyScene.query_id")
+    if name == "optix_cpu_fallback" and not allow_optix_cpu_fallback:
+        validate_proxy_scene(a)
+        raise ValueError("P2CCCD was built without OptiX support; configure with -DP2CCCD_ENABLE_OPTIX=ON")
+    timing = RtCandidateTiming()
+    t = time.perf_counter()
+    a, (raw, cand) = _run_proxy(a, qid, raw_only=False)
+    timing.trace_ms = (time.perf_counter() - t) * 1e3  # hits and compaction are one device call
+    timing.build_ms = (t - start) * 1e3
+    t = time.perf_counter()
+    res = CandidateGenerationResult()
+    res.backend_name = name
+    res.raw_buffer, res.candidates = _raw_objects(raw), _candidate_objects(cand)
+    res.density = _density(a, raw, cand, timing, name)
+    timing.stats_ms = (time.perf_counter() - t) * 1e3
+    timing.total_ms = (time.perf_counter() - start) * 1e3
+    res.timing = timing
+    return res
