@@ -503,6 +503,77 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
                          p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
                          size_t workspace_bytes, void* stream);
 
+/* ---- proxy scene build: patches x motion segments x time slabs --------------- */
+/* MotionSegment (geometry/motion.h:14-19): a rigid motion from pose_t0 at t0 to
+ * pose_t1 at t1; rotation quaternions are x, y, z, w. */
+typedef struct p2c_motion_segment {
+  double t0, t1;
+  double translation_t0[3];
+  double rotation_t0[4];
+  double translation_t1[3];
+  double rotation_t1[4];
+} p2c_motion_segment;
+
+/* ProxyObjectBuildInput (rt_candidate/proxy_scene.h:15-22).  Its patches are
+ * entries [patch_offset, patch_offset + n_patches) of the device patch
+ * arrays; its motion segments are a HOST array. */
+typedef struct p2c_proxy_object_input {
+  uint32_t object_id;
+  uint32_t proxy_type;               /* 1 swept AABB, 2 capsule */
+  uint32_t slabs_per_motion_segment;
+  uint32_t pad0;
+  double eps_proxy;
+  int64_t patch_offset, n_patches;
+  int64_t n_segments;
+  const p2c_motion_segment* segments; /* host */
+} p2c_proxy_object_input;
+
+/* Device outputs of p2c_proxy_scene_build, n proxies each (the inputs of
+ * p2c_proxy_candidates plus the rest of ProxyPrimitive).  motion_detail and
+ * capsule_radius may be NULL. */
+typedef struct p2c_proxy_build_out {
+  uint32_t* object_id;
+  uint32_t* patch_id;
+  uint32_t* slab_id;
+  uint32_t* motion_segment_id;
+  uint8_t* proxy_type;
+  double* t0;
+  double* t1;
+  double* bounds;          /* n x 6 */
+  double* motion_bound;    /* n x 4: translation_bound, rotation_angle, radial_motion_bound,
+                              conservative_radius */
+  double* motion_detail;   /* n x 8: center_t0 xyz, center_t1 xyz, center_rotation_bound,
+                              surface_rotation_bound */
+  double* capsule_radius;  /* n: the inflated radius of a capsule proxy, 0 for a swept AABB */
+} p2c_proxy_build_out;
+
+/* Proxies the objects expand to (sum of segments x slabs x patches), after
+ * the per-object checks of BuildProxyScene; -1 and the last error on an
+ * invalid input. */
+int64_t p2c_proxy_scene_count(const p2c_proxy_object_input* objects, int64_t n_objects);
+size_t p2c_proxy_scene_build_workspace_bytes(const p2c_proxy_object_input* objects, int64_t n_objects);
+
+/* BuildProxyScene (rt_candidate/proxy_scene.cpp:156-213): for each object,
+ * motion segment, uniform time slab and patch (in that order) one proxy with
+ * the patch's motion bound over the slab (ComputePatchMotionBound,
+ * geometry/motion_utils.cpp:269-325) and its swept-AABB or capsule bounds
+ * inflated by eps_proxy (geometry/proxy.cpp:70-131).  The rigid pose of each
+ * (object, segment, slab) end is computed on the host with the C library's
+ * acos/sin/cos, as the reference does; the per-patch transforms and bounds,
+ * all additions, products, quotients and square roots, run on the device.
+ * Object, segment and slab checks and the global slab partition
+ * (proxy_scene.cpp:58-85) fail the call with the reference's message;
+ * per-patch failures set bits of *error_word_dev (1 patch centre non-finite,
+ * 2 patch radius negative or non-finite, 4 swept AABB invalid before
+ * inflation, 8 capsule radius invalid, 16 final bounds invalid).
+ * Every object's patch range must lie inside the n_patch_entries patch
+ * entries.  proxy_cap must be at least p2c_proxy_scene_count.  No host sync. */
+int p2c_proxy_scene_build(uint64_t query_id, const p2c_proxy_object_input* objects, int64_t n_objects,
+                          const uint32_t* patch_id_dev, const double* patch_center_dev,
+                          const double* patch_radius_dev, int64_t n_patch_entries, int64_t proxy_cap,
+                          const p2c_proxy_build_out* out,
+                          uint64_t* error_word_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

@@ -17,6 +17,7 @@ this package.  The product library never does.
 from __future__ import annotations
 
 import ctypes
+import math
 import subprocess
 from pathlib import Path
 
@@ -458,3 +459,217 @@ def proxy_candidates(sc: dict):
          c["proxy_type_b"]) = key
         c["rt_hit_count"], c["motion_bound"], c["flags"] = groups[key]
     return raw, cand
+
+
+# ---- proxy-scene build (rt_candidate/proxy_scene.cpp, geometry/) ----
+
+def _build_flat(inp: dict):
+    objs = inp["objects"]
+    n_p = np.array([len(o["patch_id"]) for o in objs], np.int64)
+    n_s = np.array([len(o["segments"]) for o in objs], np.int64)
+    flat = {
+        "object_id": np.array([o["object_id"] for o in objs], np.uint32),
+        "proxy_type": np.array([o["proxy_type"] for o in objs], np.uint32),
+        "slabs": np.array([o["slabs_per_motion_segment"] for o in objs], np.uint32),
+        "eps": np.array([o["eps_proxy"] for o in objs], np.float64),
+        "patch_offset": np.concatenate([[0], np.cumsum(n_p)[:-1]]).astype(np.int64), "n_patches": n_p,
+        "segment_offset": np.concatenate([[0], np.cumsum(n_s)[:-1]]).astype(np.int64), "n_segments": n_s,
+        "patch_id": np.ascontiguousarray(np.concatenate([np.asarray(o["patch_id"], np.uint32) for o in objs])),
+        "patch_center": np.ascontiguousarray(np.concatenate([np.asarray(o["local_center"], np.float64).reshape(-1, 3)
+                                                             for o in objs])),
+        "patch_radius": np.ascontiguousarray(np.concatenate([np.asarray(o["radius"], np.float64) for o in objs])),
+        "segments": np.ascontiguousarray(np.concatenate([np.asarray(o["segments"], np.float64).reshape(-1, 16)
+                                                         for o in objs])),
+    }
+    return flat
+
+
+BUILT_FIELDS = (("object_id", np.uint32, ()), ("patch_id", np.uint32, ()), ("slab_id", np.uint32, ()),
+                ("motion_segment_id", np.uint32, ()), ("proxy_type", np.uint8, ()), ("t0", np.float64, ()),
+                ("t1", np.float64, ()), ("bounds", np.float64, (6,)), ("motion_bound", np.float64, (4,)),
+                ("motion_detail", np.float64, (8,)), ("capsule_radius", np.float64, ()))
+
+
+def ref_build_proxy_scene(inp: dict) -> dict:
+    """The reference's BuildProxyScene on a build input (the dict of
+    ``scenes.proxy_build_input``): the primitive arrays, or ValueError with
+    the reference's message."""
+    R = ref()
+    if not hasattr(R, "_build_ready"):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        R.ref_build_proxy_scene.argtypes = [ctypes.c_uint64, i64] + [vp] * 12 + [i64] + [vp] * 12
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._build_ready = True
+    f = _build_flat(inp)
+    n = ctypes.c_int64(0)
+    ins = [int(inp["query_id"]), len(inp["objects"])] + [_p(f[k]) for k in (
+        "object_id", "proxy_type", "slabs", "eps", "patch_offset", "n_patches", "segment_offset", "n_segments",
+        "patch_id", "patch_center", "patch_radius", "segments")]
+    if R.ref_build_proxy_scene(*ins, 0, *([None] * 11), ctypes.byref(n)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    out = {k: np.zeros((max(n.value, 1),) + sh, dt) for k, dt, sh in BUILT_FIELDS}
+    R.ref_build_proxy_scene(*ins, n.value, *[_p(out[k]) for k, _, _ in BUILT_FIELDS], ctypes.byref(n))
+    out = {k: v[:n.value] for k, v in out.items()}
+    out["query_id"], out["n"] = int(inp["query_id"]), n.value
+    return out
+
+
+def _norm4(q):
+    """NormalizeQuaternion (geometry/motion_utils.cpp:64-77)."""
+    if not all(math.isfinite(x) for x in q):
+        raise ValueError("quaternion contains a non-finite value")
+    nrm = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+    if not math.isfinite(nrm) or nrm <= 0.0:
+        raise ValueError("quaternion norm must be positive and finite")
+    return [q[0] / nrm, q[1] / nrm, q[2] / nrm, q[3] / nrm]
+
+
+def _clamp(v, lo, hi):
+    return lo if v < lo else (hi if hi < v else v)
+
+
+def _slerp(a, b, alpha):
+    """Slerp (:99-126), LerpAndNormalize (:87-97) past dot 0.9995."""
+    d = a[0] * b[0] + a[1] * b[1] + a[2] * b[2] + a[3] * b[3]
+    if d < 0.0:
+        b = [-x for x in b]
+        d = -d
+    d = _clamp(d, -1.0, 1.0)
+    if d > 0.9995:
+        q = [(1.0 - alpha) * a[k] + alpha * b[k] for k in range(4)]
+        nrm = math.sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3])
+        return [x / nrm for x in q]
+    th0 = math.acos(d)
+    th = th0 * alpha
+    st, st0 = math.sin(th), math.sin(th0)
+    s0 = math.cos(th) - d * st / st0
+    s1 = st / st0
+    return [s0 * a[k] + s1 * b[k] for k in range(4)]
+
+
+def _rotate(q, v):
+    """RotateVector (:128-135)."""
+    u0, u1, u2, s = q
+    k0 = 2.0 * (u0 * v[0] + u1 * v[1] + u2 * v[2])
+    k1 = s * s - (u0 * u0 + u1 * u1 + u2 * u2)
+    k2 = 2.0 * s
+    c = (u1 * v[2] - u2 * v[1], u2 * v[0] - u0 * v[2], u0 * v[1] - u1 * v[0])
+    return [(q[a] * k0 + v[a] * k1) + c[a] * k2 for a in range(3)]
+
+
+def _check_aabb(mn, mx, msg_finite, msg_order):
+    """ValidateAabb (geometry/proxy.cpp:21-31) / ValidateAabbBounds
+    (proxy_scene.cpp:25-35): axis by axis, finiteness then order."""
+    for a in range(3):
+        if not (math.isfinite(mn[a]) and math.isfinite(mx[a])):
+            raise ValueError(msg_finite)
+        if mn[a] > mx[a]:
+            raise ValueError(msg_order)
+
+
+def build_proxy_scene(inp: dict) -> dict:
+    """Restatement of BuildProxyScene (proxy_scene.cpp:156-213): per object,
+    motion segment, uniform slab (GenerateUniformTimeSlabs,
+    motion_utils.cpp:175-185) and patch one proxy; ComputePatchMotionBound
+    (:269-325) with the interpolated poses (InterpolateRigidMotion, :196-229)
+    and the swept-AABB / capsule bounds (geometry/proxy.cpp:70-131), then
+    ValidateProxyScene's slab partition (proxy_scene.cpp:58-85).  Python
+    floats and the math module (the C library's acos/sin/cos)."""
+    if int(inp["query_id"]) == 0:
+        raise ValueError("ProxySceneBuildInput.query_id is required")
+    if not inp["objects"]:
+        raise ValueError("ProxySceneBuildInput.objects is empty")
+    rows = []
+    for o in inp["objects"]:
+        if o["proxy_type"] not in (1, 2):
+            raise ValueError("ProxyObjectBuildInput.proxy_type must be concrete")
+        if len(o["patch_id"]) == 0:
+            raise ValueError("ProxyObjectBuildInput.patches is empty")
+        if len(o["segments"]) == 0:
+            raise ValueError("ProxyObjectBuildInput.motion_segments is empty")
+        S = int(o["slabs_per_motion_segment"])
+        if S == 0:
+            raise ValueError("slabs_per_motion_segment must be positive")
+        eps = float(o["eps_proxy"])
+        if not math.isfinite(eps) or eps < 0.0:
+            raise ValueError("eps_proxy must be finite and non-negative")
+        for si, seg in enumerate(np.asarray(o["segments"], np.float64).reshape(-1, 16).tolist()):
+            st0, st1 = seg[0], seg[1]
+            if not (math.isfinite(st0) and math.isfinite(st1)) or st0 >= st1:
+                raise ValueError("motion segment must satisfy finite t0 < t1")
+            for name, tr, rot in (("pose_t0", seg[2:5], seg[5:9]), ("pose_t1", seg[9:12], seg[12:16])):
+                if not all(math.isfinite(x) for x in tr):
+                    raise ValueError(f"{name}.translation contains a non-finite value")
+                _norm4(rot)
+            dt = (st1 - st0) / float(S)
+            for k in range(S):
+                t0 = st0 if k == 0 else st0 + dt * k
+                t1 = st1 if k + 1 == S else st0 + dt * (k + 1)
+                if not (math.isfinite(t0) and math.isfinite(t1)) or t0 >= t1:
+                    raise ValueError("time slab must satisfy finite t0 < t1")
+                tol = 1.0e-12 * max(1.0, st1 - st0)
+                if t0 < st0 - tol or t1 > st1 + tol:
+                    raise ValueError("time slab must lie inside the motion segment")
+                poses = []
+                for t in (t0, t1):
+                    alpha = (_clamp(t, st0, st1) - st0) / (st1 - st0)
+                    tr = [(1.0 - alpha) * seg[2 + a] + alpha * seg[9 + a] for a in range(3)]
+                    rot = _slerp(_norm4(seg[5:9]), _norm4(seg[12:16]), alpha)
+                    if not all(math.isfinite(x) for x in tr):
+                        raise ValueError("pose.translation contains a non-finite value")
+                    poses.append((tr, _norm4(rot)))
+                (tr0, q0), (tr1, q1) = poses
+                d = _clamp(abs(q0[0] * q1[0] + q0[1] * q1[1] + q0[2] * q1[2] + q0[3] * q1[3]), 0.0, 1.0)
+                angle = 2.0 * math.acos(d)
+                dx, dy, dz = tr0[0] - tr1[0], tr0[1] - tr1[1], tr0[2] - tr1[2]
+                tb = math.sqrt(dx * dx + dy * dy + dz * dz)
+                hs = math.sin(0.5 * angle)
+                for p_id, lc, rad in zip(np.asarray(o["patch_id"]).tolist(),
+                                         np.asarray(o["local_center"], np.float64).reshape(-1, 3).tolist(),
+                                         np.asarray(o["radius"], np.float64).tolist()):
+                    if not all(math.isfinite(x) for x in lc):
+                        raise ValueError("patch.local_center contains a non-finite value")
+                    if not math.isfinite(rad) or rad < 0.0:
+                        raise ValueError("patch.radius must be finite and non-negative")
+                    c0 = [x + y for x, y in zip(_rotate(q0, lc), tr0)]
+                    c1 = [x + y for x, y in zip(_rotate(q1, lc), tr1)]
+                    crb = 2.0 * math.sqrt(lc[0] * lc[0] + lc[1] * lc[1] + lc[2] * lc[2]) * hs
+                    srb = 2.0 * rad * hs
+                    cons = rad + crb
+                    lo = [c1[a] if c1[a] < c0[a] else c0[a] for a in range(3)]  # std::min(c0, c1)
+                    hi = [c1[a] if c0[a] < c1[a] else c0[a] for a in range(3)]  # std::max(c0, c1)
+                    if o["proxy_type"] == 1:
+                        mn = [lo[a] - cons for a in range(3)]
+                        mx = [hi[a] + cons for a in range(3)]
+                        _check_aabb(mn, mx, "AABB contains a non-finite bound", "AABB min cannot exceed max")
+                        mn = [x - eps for x in mn]
+                        mx = [x + eps for x in mx]
+                        cap_r = 0.0
+                    else:
+                        if not math.isfinite(cons) or cons < 0.0:
+                            raise ValueError("capsule radius must be finite and non-negative")
+                        cap_r = cons + eps
+                        mn = [lo[a] - cap_r for a in range(3)]
+                        mx = [hi[a] + cap_r for a in range(3)]
+                    _check_aabb(mn, mx, "proxy bounds contain a non-finite value",
+                                "proxy bounds min cannot exceed max")
+                    rows.append((o["object_id"], p_id, si * S + k, si, o["proxy_type"], t0, t1, mn + mx,
+                                 [tb, angle, tb + crb + srb, cons], c0 + c1 + [crb, srb], cap_r))
+    # ValidateGlobalSlabPartition (proxy_scene.cpp:58-85)
+    first = {}
+    for r in rows:
+        a, b = first.setdefault(r[2], (r[5], r[6]))
+        tol = 1.0e-12 * max(1.0, abs(a), abs(b), abs(b - a))
+        if not abs(a - r[5]) <= tol or not abs(b - r[6]) <= tol:
+            raise ValueError("proxy scene slab_id must map to one global time interval")
+    ordered = sorted(first.items(), key=lambda kv: (kv[1][0], kv[0]))
+    for (_, (a0, a1)), (_, (b0, b1)) in zip(ordered, ordered[1:]):
+        tol = max(1.0e-12 * max(1.0, abs(a0), abs(a1), abs(a1 - a0)),
+                  1.0e-12 * max(1.0, abs(b0), abs(b1), abs(b1 - b0)))
+        if a0 < b1 - tol and b0 < a1 - tol:
+            raise ValueError("proxy scene global slab intervals must not overlap")
+    n = len(rows)
+    out = {"query_id": int(inp["query_id"]), "n": n}
+    for j, (k, dt_, sh) in enumerate(BUILT_FIELDS):
+        out[k] = np.array([r[j] for r in rows], dt_).reshape((n,) + sh)
+    return out

@@ -1,12 +1,15 @@
-// ref_proxy.cpp — C ABI over the reference's proxy-scene candidate
-// generation (rt_candidate/candidate_buffer.cpp: GenerateRawCandidatesCpu,
-// CompactRawCandidates; rt_candidate/proxy_scene.cpp: ValidateProxyScene),
-// compiled unchanged into oracle/_ref/libp2c_ref.so.
+// ref_proxy.cpp — C ABI over the reference's proxy-scene build and candidate
+// generation (rt_candidate/proxy_scene.cpp: BuildProxyScene,
+// ValidateProxyScene; rt_candidate/candidate_buffer.cpp:
+// GenerateRawCandidatesCpu, CompactRawCandidates), compiled unchanged into
+// oracle/_ref/libp2c_ref.so.
 //
 // TEST INFRASTRUCTURE ONLY: tests pin the device proxy candidates and the
 // restated checker to it; the product never loads it.
 #include "rt_candidate/candidate_buffer.h"
+#include "rt_candidate/proxy_scene.h"
 
+#include <algorithm>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -97,6 +100,88 @@ int ref_proxy_candidates(uint64_t query_id, int64_t n, const uint32_t* object_id
       o.proxy_features_offset = c.proxy_features_offset;
       o.flags = c.flags;
     }
+  return 0;
+}
+
+// BuildProxyScene over a flattened ProxySceneBuildInput: per object its id,
+// type, slabs per segment, eps, and the ranges [patch_offset, +n_patches) of
+// the patch arrays and [segment_offset, +n_segments) of the segment array
+// (p2c_motion_segment layout).  Outputs n x {object, patch, slab, segment
+// ids, type, t0, t1, bounds[6], motion_bound[4] (translation, rotation,
+// radial, conservative), detail[8] (centre t0, centre t1, centre and surface
+// rotation bounds), capsule radius}; NULL outputs make it a sizing call.
+int ref_build_proxy_scene(uint64_t query_id, int64_t n_objects, const uint32_t* object_id,
+                          const uint32_t* proxy_type, const uint32_t* slabs_per_segment, const double* eps,
+                          const int64_t* patch_offset, const int64_t* n_patches, const int64_t* segment_offset,
+                          const int64_t* n_segments, const uint32_t* patch_id, const double* patch_center,
+                          const double* patch_radius, const p2c_motion_segment* segments, int64_t cap,
+                          uint32_t* o_object, uint32_t* o_patch, uint32_t* o_slab, uint32_t* o_segment,
+                          uint8_t* o_type, double* o_t0, double* o_t1, double* o_bounds, double* o_motion,
+                          double* o_detail, double* o_capsule_radius, int64_t* n_out) {
+  p2cccd::ProxySceneBuildInput in;
+  in.query_id = query_id;
+  for (int64_t k = 0; k < n_objects; ++k) {
+    p2cccd::ProxyObjectBuildInput o;
+    o.object_id = object_id[k];
+    o.proxy_type = static_cast<p2cccd::ProxyType>(proxy_type[k]);
+    o.slabs_per_motion_segment = slabs_per_segment[k];
+    o.eps_proxy = eps[k];
+    for (int64_t i = patch_offset[k]; i < patch_offset[k] + n_patches[k]; ++i) {
+      p2cccd::Patch pt;
+      pt.patch_id = patch_id[i];
+      pt.local_center = {patch_center[3 * i], patch_center[3 * i + 1], patch_center[3 * i + 2]};
+      pt.radius = patch_radius[i];
+      o.patches.push_back(pt);
+    }
+    for (int64_t i = segment_offset[k]; i < segment_offset[k] + n_segments[k]; ++i) {
+      const p2c_motion_segment& s = segments[i];
+      p2cccd::MotionSegment m;
+      m.t0 = s.t0;
+      m.t1 = s.t1;
+      for (int a = 0; a < 3; ++a) {
+        m.pose_t0.translation[a] = s.translation_t0[a];
+        m.pose_t1.translation[a] = s.translation_t1[a];
+      }
+      for (int a = 0; a < 4; ++a) {
+        m.pose_t0.rotation_xyzw[a] = s.rotation_t0[a];
+        m.pose_t1.rotation_xyzw[a] = s.rotation_t1[a];
+      }
+      o.motion_segments.push_back(m);
+    }
+    in.objects.push_back(std::move(o));
+  }
+  p2cccd::ProxyScene scene;
+  const p2cccd::Status st = p2cccd::BuildProxyScene(in, &scene);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  *n_out = static_cast<int64_t>(scene.primitives.size());
+  if (o_object == nullptr) return 0;
+  const int64_t n = std::min<int64_t>(*n_out, cap);
+  for (int64_t i = 0; i < n; ++i) {
+    const p2cccd::ProxyPrimitive& p = scene.primitives[i];
+    o_object[i] = p.object_id;
+    o_patch[i] = p.patch_id;
+    o_slab[i] = p.slab_id;
+    o_segment[i] = p.motion_segment_id;
+    o_type[i] = static_cast<uint8_t>(p.proxy_type);
+    o_t0[i] = p.t0;
+    o_t1[i] = p.t1;
+    for (int a = 0; a < 3; ++a) {
+      o_bounds[6 * i + a] = p.bounds.min[a];
+      o_bounds[6 * i + 3 + a] = p.bounds.max[a];
+      o_detail[8 * i + a] = p.motion_bound.center_t0[a];
+      o_detail[8 * i + 3 + a] = p.motion_bound.center_t1[a];
+    }
+    o_motion[4 * i + 0] = p.motion_bound.translation_bound;
+    o_motion[4 * i + 1] = p.motion_bound.rotation_angle;
+    o_motion[4 * i + 2] = p.motion_bound.radial_motion_bound;
+    o_motion[4 * i + 3] = p.motion_bound.conservative_radius;
+    o_detail[8 * i + 6] = p.motion_bound.center_rotation_bound;
+    o_detail[8 * i + 7] = p.motion_bound.surface_rotation_bound;
+    o_capsule_radius[i] = p.capsule.radius;
+  }
   return 0;
 }
 

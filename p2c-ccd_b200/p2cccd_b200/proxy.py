@@ -40,7 +40,13 @@ class ProxyCandidates:
         self.n = int(scene["n"])
         self.arrays = {}
         for k, dt in self.FIELDS:
-            a = np.ascontiguousarray(scene[k], dtype=dt)
+            v = scene[k]
+            if torch.is_tensor(v):  # already on the device (a built proxy scene)
+                if v.device != d or not v.is_contiguous() or v.element_size() != np.dtype(dt).itemsize:
+                    raise ValueError(f"proxy field {k}: expected a contiguous {np.dtype(dt)} tensor on {d}")
+                self.arrays[k] = v
+                continue
+            a = np.ascontiguousarray(v, dtype=dt)
             self.arrays[k] = torch.from_numpy(a.view(np.uint8).copy()).to(d) if dt == np.uint32 else \
                 torch.from_numpy(a).to(d)
         st = ProxySceneStruct()
@@ -90,3 +96,122 @@ class ProxyCandidates:
 
 def proxy_candidates(scene: dict, device: str | torch.device = "cuda") -> tuple[np.ndarray, np.ndarray]:
     return ProxyCandidates(scene, device).run_checked()
+
+
+# ---------------------------------------------------------------------------
+# proxy scene build (p2c_proxy_scene_build)
+
+BUILD_ERRORS = ((1, "patch.local_center contains a non-finite value"),
+                (2, "patch.radius must be finite and non-negative"),
+                (4, "AABB contains a non-finite bound or its min exceeds its max"),
+                (8, "capsule radius must be finite and non-negative"),
+                (16, "proxy bounds contain a non-finite value or min exceeds max"))
+
+
+class MotionSegmentStruct(ctypes.Structure):
+    _fields_ = [("t0", ctypes.c_double), ("t1", ctypes.c_double), ("translation_t0", ctypes.c_double * 3),
+                ("rotation_t0", ctypes.c_double * 4), ("translation_t1", ctypes.c_double * 3),
+                ("rotation_t1", ctypes.c_double * 4)]
+
+
+class ProxyObjectStruct(ctypes.Structure):
+    _fields_ = [("object_id", ctypes.c_uint32), ("proxy_type", ctypes.c_uint32),
+                ("slabs_per_motion_segment", ctypes.c_uint32), ("pad0", ctypes.c_uint32), ("eps_proxy", ctypes.c_double),
+                ("patch_offset", ctypes.c_int64), ("n_patches", ctypes.c_int64), ("n_segments", ctypes.c_int64),
+                ("segments", ctypes.c_void_p)]
+
+
+class ProxyBuildOutStruct(ctypes.Structure):
+    _fields_ = [(k, ctypes.c_void_p) for k in ("object_id", "patch_id", "slab_id", "motion_segment_id", "proxy_type",
+                                               "t0", "t1", "bounds", "motion_bound", "motion_detail",
+                                               "capsule_radius")]
+
+
+class ProxySceneBuild:
+    """A ProxySceneBuildInput built into a device-resident proxy scene.
+
+    ``inp`` is the dict of ``scenes.proxy_build_input``: ``query_id`` and
+    ``objects``, each with object_id, proxy_type, slabs_per_motion_segment,
+    eps_proxy, patch_id[P], local_center[P, 3], radius[P] and segments[M, 16]
+    (t0, t1, translation_t0, rotation_t0 xyzw, translation_t1, rotation_t1).
+    ``scene()`` returns the proxy arrays as device tensors, the input of
+    ``ProxyCandidates`` without a host round trip."""
+
+    def __init__(self, inp: dict, device: str | torch.device = "cuda", detail: bool = True):
+        self.lib = _lib.load()
+        self.device = d = torch.device(device)
+        self.query_id = int(inp["query_id"])
+        objs = inp["objects"]
+        k = len(objs)
+        self._segments = [np.ascontiguousarray(np.asarray(o["segments"], np.float64).reshape(-1, 16)) for o in objs]
+        arr = (ProxyObjectStruct * max(k, 1))()
+        off = 0
+        for i, o in enumerate(objs):
+            n_p = len(o["patch_id"])
+            arr[i].object_id, arr[i].proxy_type = int(o["object_id"]), int(o["proxy_type"])
+            arr[i].slabs_per_motion_segment, arr[i].eps_proxy = int(o["slabs_per_motion_segment"]), float(o["eps_proxy"])
+            arr[i].patch_offset, arr[i].n_patches = off, n_p
+            arr[i].n_segments = len(self._segments[i])
+            arr[i].segments = self._segments[i].ctypes.data if len(self._segments[i]) else None
+            off += n_p
+        self._objects, self.n_objects = arr, k
+        self.n_patch_entries = off
+        cat = (lambda key, dt, w: np.ascontiguousarray(np.concatenate(
+            [np.asarray(o[key], dt).reshape(-1, w) for o in objs]) if objs else np.zeros((0, w), dt)))
+        self.patch_id = torch.from_numpy(cat("patch_id", np.uint32, 1).view(np.int32).reshape(-1)).to(d)
+        self.patch_center = torch.from_numpy(cat("local_center", np.float64, 3)).to(d)
+        self.patch_radius = torch.from_numpy(cat("radius", np.float64, 1).reshape(-1)).to(d)
+        n = int(self.lib.p2c_proxy_scene_count(arr, k))
+        if n < 0:
+            raise ValueError(_lib.last_error())
+        self.n = n
+        self.out = {"object_id": torch.empty(n, dtype=torch.int32, device=d),
+                    "patch_id": torch.empty(n, dtype=torch.int32, device=d),
+                    "slab_id": torch.empty(n, dtype=torch.int32, device=d),
+                    "motion_segment_id": torch.empty(n, dtype=torch.int32, device=d),
+                    "proxy_type": torch.empty(n, dtype=torch.uint8, device=d),
+                    "t0": torch.empty(n, dtype=torch.float64, device=d),
+                    "t1": torch.empty(n, dtype=torch.float64, device=d),
+                    "bounds": torch.empty((n, 6), dtype=torch.float64, device=d),
+                    "motion_bound": torch.empty((n, 4), dtype=torch.float64, device=d)}
+        if detail:
+            self.out["motion_detail"] = torch.empty((n, 8), dtype=torch.float64, device=d)
+            self.out["capsule_radius"] = torch.empty(n, dtype=torch.float64, device=d)
+        st = ProxyBuildOutStruct()
+        for f, _ in ProxyBuildOutStruct._fields_:
+            setattr(st, f, self.out[f].data_ptr() if f in self.out else None)
+        self._out_struct = st
+        self.error_word = torch.zeros(1, dtype=torch.int64, device=d)
+        self.ws = torch.empty(int(self.lib.p2c_proxy_scene_build_workspace_bytes(arr, k)), dtype=torch.uint8, device=d)
+
+    def run(self) -> None:
+        """Enqueue the build on the current stream (no host sync); raises
+        ValueError for an invalid object, segment or slab partition."""
+        _lib.check(self.lib.p2c_proxy_scene_build(
+            self.query_id, self._objects, self.n_objects, self.patch_id.data_ptr(), self.patch_center.data_ptr(),
+            self.patch_radius.data_ptr(), self.n_patch_entries, self.n, ctypes.byref(self._out_struct),
+            self.error_word.data_ptr(), self.ws.data_ptr(), self.ws.numel(), _stream_ptr(self.device)))
+
+    def run_checked(self) -> dict:
+        """Build, then raise ValueError on a per-patch failure; returns
+        ``scene()``."""
+        self.run()
+        e = int(self.error_word.item())
+        for bit, msg in BUILD_ERRORS:
+            if e & bit:
+                raise ValueError(msg)
+        return self.scene()
+
+    def scene(self) -> dict:
+        """The built proxies as device tensors (uint32 fields as int32)."""
+        sc = {"query_id": self.query_id, "n": self.n}
+        sc.update(self.out)
+        return sc
+
+    def to_host(self) -> dict:
+        """The built proxies as numpy arrays with the reference's types."""
+        sc = {"query_id": self.query_id, "n": self.n}
+        for k, v in self.out.items():
+            a = v.cpu().numpy()
+            sc[k] = a.view(np.uint32) if a.dtype == np.int32 else a
+        return sc

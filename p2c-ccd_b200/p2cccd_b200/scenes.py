@@ -211,3 +211,52 @@ def proxy_scene(n_objects: int = 6, patches_per_object: int = 40, n_slabs: int =
     for k in ("object_id", "patch_id", "slab_id", "proxy_type", "t0", "t1", "bounds", "motion_bound"):
         out[k] = np.ascontiguousarray(out[k][perm])
     return out
+
+
+def _quat(axis, angle, scale=1.0):
+    """Quaternion (x, y, z, w) of a rotation by ``angle`` about ``axis``,
+    multiplied by ``scale`` (the builder normalises it)."""
+    axis = np.asarray(axis, np.float64)
+    axis = axis / np.linalg.norm(axis)
+    return np.concatenate([axis * np.sin(0.5 * angle), [np.cos(0.5 * angle)]]) * scale
+
+
+def proxy_build_input(n_objects: int = 6, patches_per_object: int = 60, n_segments: int = 2, slabs: int = 3,
+                      seed: int = 20261203, query_id: int = 11, eps_proxy: float = 1e-3) -> dict:
+    """A ProxySceneBuildInput as arrays: ``objects`` of rigid bodies whose
+    patches (centres on a sphere about the body origin, small radii) move
+    over piecewise rigid motion segments partitioning [0, 1] the same way for
+    every object (so the slab ids form one global partition).  Bodies drift
+    toward the origin while rotating; the rotations cover the slerp branch,
+    the near-parallel lerp branch (a still body and a tiny rotation), a
+    quaternion pair of opposite signs and quaternions of non-unit norm.
+    Segment rows are t0, t1, translation_t0, rotation_t0 (x, y, z, w),
+    translation_t1, rotation_t1."""
+    g = rng(seed)
+    cuts = np.linspace(0.0, 1.0, n_segments + 1)
+    objects = []
+    pid = 0
+    for o in range(n_objects):
+        start = g.uniform(-1.0, 1.0, 3)
+        vel = -start * g.uniform(0.6, 1.1)
+        axis = g.normal(size=3)
+        spin = [g.uniform(0.5, 3.0), 0.0, 1e-3, g.uniform(0.5, 3.0)][o % 4]
+        segs = np.zeros((n_segments, 16))
+        for s in range(n_segments):
+            a, b = cuts[s], cuts[s + 1]
+            segs[s, 0:2] = a, b
+            segs[s, 2:5] = start + vel * a
+            segs[s, 5:9] = _quat(axis, spin * a, g.uniform(0.5, 2.0))
+            segs[s, 9:12] = start + vel * b
+            q1 = _quat(axis, spin * b, g.uniform(0.5, 2.0))
+            segs[s, 12:16] = -q1 if o % 4 == 3 else q1  # same rotation, opposite sign
+        radius_body = g.uniform(0.15, 0.35)
+        d = g.normal(size=(patches_per_object, 3))
+        centers = d / np.linalg.norm(d, axis=1, keepdims=True) * radius_body
+        objects.append({"object_id": 100 + 3 * o, "proxy_type": 1 + (o % 2), "slabs_per_motion_segment": slabs,
+                        "eps_proxy": eps_proxy,
+                        "patch_id": np.arange(pid, pid + patches_per_object, dtype=np.uint32),
+                        "local_center": np.ascontiguousarray(centers),
+                        "radius": g.uniform(0.02, 0.08, patches_per_object), "segments": segs})
+        pid += patches_per_object
+    return {"query_id": query_id, "objects": objects}

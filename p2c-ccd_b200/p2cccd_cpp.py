@@ -1058,3 +1058,79 @@ def generate_candidates_for_proxy_scene(scene, query_id: int = 0, backend_name: 
     timing.total_ms = (time.perf_counter() - start) * 1e3
     res.timing = timing
     return res
+
+
+class PoseSample(_Struct):  # geometry/motion.h:9-12
+    _fields = (("translation", lambda: [0.0, 0.0, 0.0]), ("rotation_xyzw", lambda: [0.0, 0.0, 0.0, 1.0]))
+
+
+class MotionSegment(_Struct):  # :14-19
+    _fields = (("t0", 0.0), ("t1", 1.0), ("pose_t0", PoseSample), ("pose_t1", PoseSample))
+
+
+class Patch(_Struct):  # geometry/patch.h:9-16
+    _fields = (("patch_id", 0), ("triangle_ids", list), ("triangle_count", 0), ("area", 0.0),
+               ("local_center", lambda: [0.0, 0.0, 0.0]), ("radius", 0.0))
+
+
+class ProxyObjectBuildInput(_Struct):  # rt_candidate/proxy_scene.h:15-22
+    _fields = (("object_id", 0), ("proxy_type", ProxyType.SWEPT_AABB), ("patches", list), ("motion_segments", list),
+               ("slabs_per_motion_segment", 1), ("eps_proxy", 0.0))
+
+
+class ProxySceneBuildInput(_Struct):  # :24-27
+    _fields = (("query_id", 0), ("objects", list))
+
+
+def _build_input_arrays(inp) -> dict:
+    """A ProxySceneBuildInput as the arrays p2c_proxy_scene_build reads."""
+    if isinstance(inp, dict):
+        return inp
+    objs = []
+    for o in inp.objects:
+        segs = np.array([[s.t0, s.t1, *s.pose_t0.translation, *s.pose_t0.rotation_xyzw, *s.pose_t1.translation,
+                          *s.pose_t1.rotation_xyzw] for s in o.motion_segments], np.float64).reshape(-1, 16)
+        objs.append({"object_id": int(o.object_id), "proxy_type": int(o.proxy_type),
+                     "slabs_per_motion_segment": int(o.slabs_per_motion_segment), "eps_proxy": float(o.eps_proxy),
+                     "patch_id": np.array([p.patch_id for p in o.patches], np.uint32),
+                     "local_center": np.array([list(p.local_center) for p in o.patches], np.float64).reshape(-1, 3),
+                     "radius": np.array([p.radius for p in o.patches], np.float64), "segments": segs})
+    return {"query_id": int(inp.query_id), "objects": objs}
+
+
+def build_proxy_scene(input) -> ProxyScene:  # py_module.cpp:1868, proxy_scene.cpp:156-213
+    """BuildProxyScene on the device (p2c_proxy_scene_build): one proxy per
+    object, motion segment, slab and patch, with its motion bound, bounds and
+    (capsules) capsule; ValueError with the reference's message on an invalid
+    input."""
+    from p2cccd_b200.proxy import ProxySceneBuild
+
+    a = _build_input_arrays(input)
+    if int(a["query_id"]) == 0:
+        raise ValueError("ProxySceneBuildInput.query_id is required")
+    if not a["objects"]:
+        raise ValueError("ProxySceneBuildInput.objects is empty")
+    b = ProxySceneBuild(a)
+    b.run_checked()
+    h = b.to_host()
+    scene = ProxyScene()
+    scene.query_id = int(a["query_id"])
+    for i in range(h["n"]):
+        p = ProxyPrimitive()
+        p.proxy_id, p.object_id, p.patch_id = i, int(h["object_id"][i]), int(h["patch_id"][i])
+        p.slab_id, p.motion_segment_id = int(h["slab_id"][i]), int(h["motion_segment_id"][i])
+        p.proxy_type, p.t0, p.t1 = ProxyType(int(h["proxy_type"][i])), float(h["t0"][i]), float(h["t1"][i])
+        p.bounds.min, p.bounds.max = h["bounds"][i, :3].tolist(), h["bounds"][i, 3:].tolist()
+        m, det = p.motion_bound, h["motion_detail"][i].tolist()
+        m.patch_id, m.t0, m.t1 = p.patch_id, p.t0, p.t1
+        m.center_t0, m.center_t1 = det[0:3], det[3:6]
+        m.translation_bound, m.rotation_angle, m.radial_motion_bound, m.conservative_radius = \
+            h["motion_bound"][i].tolist()
+        m.center_rotation_bound, m.surface_rotation_bound = det[6], det[7]
+        if p.proxy_type == ProxyType.CAPSULE:
+            c = p.capsule
+            c.patch_id, c.endpoint0, c.endpoint1 = p.patch_id, list(m.center_t0), list(m.center_t1)
+            c.radius = float(h["capsule_radius"][i])
+            c.motion_bound = m
+        scene.primitives.append(p)
+    return scene

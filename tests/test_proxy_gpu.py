@@ -103,3 +103,87 @@ def test_motion_bound_error_only_in_compaction(cuda_device):
     assert len(hits) > 0 and all(h.motion_bound[2] == float("inf") for h in hits)
     with pytest.raises(ValueError, match="motion_bound"):
         cpp.generate_candidates_for_proxy_scene(sc)
+
+
+@pytest.mark.parametrize("seed,objs,patches,segs,slabs", [(1, 8, 30, 3, 2), (2, 5, 50, 1, 4), (7, 16, 120, 2, 3)])
+def test_device_build_matches_reference(cuda_device, oracle_mod, seed, objs, patches, segs, slabs):
+    """BuildProxyScene on the device: every output field byte for byte with
+    the reference, then the device candidates of the device-resident scene."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates, ProxySceneBuild
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    inp = scenes.proxy_build_input(n_objects=objs, patches_per_object=patches, n_segments=segs, slabs=slabs,
+                                   seed=seed)
+    ref = oracle_mod.ref_build_proxy_scene(inp)
+    b = ProxySceneBuild(inp, cuda_device)
+    dev_scene = b.run_checked()
+    got = b.to_host()
+    assert got["n"] == ref["n"]
+    for k, _, _ in oracle_mod.BUILT_FIELDS:
+        assert np.array_equal(np.ascontiguousarray(got[k]).view(np.uint8),
+                              np.ascontiguousarray(ref[k]).view(np.uint8)), k
+    raw, cand = ProxyCandidates(dev_scene, cuda_device).run_checked()
+    ref_raw, ref_cand = oracle_mod.ref_proxy_candidates(ref)
+    assert np.array_equal(raw.view(np.uint8), ref_raw.view(np.uint8))
+    assert np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
+
+
+def test_device_build_known_answers_and_mirror(cuda_device, oracle_mod):
+    """test_rt_candidate.cpp:98-156 through the p2cccd_cpp mirror objects."""
+    import p2cccd_cpp as cpp
+    from test_proxy_oracle import overlapping_build_input
+
+    a = overlapping_build_input()
+    inp = cpp.ProxySceneBuildInput()
+    inp.query_id = a["query_id"]
+    for o in a["objects"]:
+        ob = cpp.ProxyObjectBuildInput()
+        ob.object_id, ob.proxy_type = o["object_id"], cpp.ProxyType(o["proxy_type"])
+        ob.slabs_per_motion_segment, ob.eps_proxy = o["slabs_per_motion_segment"], o["eps_proxy"]
+        p = cpp.Patch()
+        p.patch_id, p.local_center, p.radius = int(o["patch_id"][0]), o["local_center"][0].tolist(), 0.2
+        ob.patches = [p]
+        m = cpp.MotionSegment()
+        m.pose_t0.translation = [0.0, 0.0, 0.0]
+        m.pose_t1.translation = [0.0, 0.0, 0.0]
+        ob.motion_segments = [m]
+        inp.objects.append(ob)
+    scene = cpp.build_proxy_scene(inp)
+    assert scene.query_id == 42 and len(scene.primitives) == 4
+    assert [p.proxy_id for p in scene.primitives] == [0, 1, 2, 3]
+    cap = scene.primitives[2]
+    assert cap.proxy_type == cpp.ProxyType.CAPSULE and cap.capsule.radius == 0.2 + 0.05
+    assert cap.capsule.endpoint0 == [0.25, 0.0, 0.0]
+    assert cpp.validate_proxy_scene(scene)
+    res = cpp.generate_candidates_for_proxy_scene(scene)
+    assert len(res.raw_buffer.hits) == 2 and len(res.candidates) == 2
+    assert all(c.object_a_id == 10 and c.object_b_id == 20 and c.rt_hit_count == 1 for c in res.candidates)
+    d = res.density
+    assert (d.proxy_count, d.object_count, d.slab_count, d.cross_object_same_slab_pair_count,
+            d.aabb_overlap_ratio) == (4, 2, 2, 2, 1.0)
+    ref = oracle_mod.ref_build_proxy_scene(a)
+    assert [p.bounds.min + p.bounds.max for p in scene.primitives] == ref["bounds"].tolist()
+    bad = cpp.ProxySceneBuildInput()
+    bad.query_id, bad.objects = 42, list(inp.objects)
+    bad.objects[1] = cpp.ProxyObjectBuildInput()
+    bad.objects[1].proxy_type, bad.objects[1].patches = cpp.ProxyType.UNKNOWN, [cpp.Patch()]
+    bad.objects[1].motion_segments = [cpp.MotionSegment()]
+    with pytest.raises(ValueError, match="concrete"):
+        cpp.build_proxy_scene(bad)
+
+
+def test_device_build_flags_bad_patches(cuda_device, oracle_mod):
+    from test_proxy_oracle import overlapping_build_input
+    from p2cccd_b200.proxy import ProxySceneBuild
+
+    for key, value, msg in (("local_center", np.array([[np.nan, 0.0, 0.0]]), "local_center"),
+                            ("radius", np.array([-0.1]), "radius")):
+        a = overlapping_build_input()
+        a["objects"][1][key] = value
+        if oracle_mod.ref_available():
+            with pytest.raises(ValueError, match=msg):
+                oracle_mod.ref_build_proxy_scene(a)
+        with pytest.raises(ValueError, match=msg):
+            ProxySceneBuild(a, cuda_device).run_checked()

@@ -110,3 +110,138 @@ def test_host_slab_validation_agrees_with_reference(oracle_mod):
         except ValueError:
             mine_ok = False
         assert mine_ok == ref_ok, stretch
+
+
+# ---- proxy scene build --------------------------------------------------------
+
+def overlapping_build_input():
+    """The reference's MakeOverlappingSceneInput (test_rt_candidate.cpp:49-94):
+    a swept-AABB patch at x = 0 (object 10) and a capsule patch at x = 0.25
+    (object 20), radius 0.2, both still over [0, 1] in 2 slabs, eps 0.05."""
+    still = np.array([[0.0, 1.0, 0, 0, 0, 0, 0, 0, 1, 0, 0, 0, 0, 0, 0, 1]], np.float64)
+    objs = []
+    for oid, typ, pid, x in ((10, 1, 1, 0.0), (20, 2, 2, 0.25)):
+        objs.append({"object_id": oid, "proxy_type": typ, "slabs_per_motion_segment": 2, "eps_proxy": 0.05,
+                     "patch_id": np.array([pid], np.uint32), "local_center": np.array([[x, 0.0, 0.0]]),
+                     "radius": np.array([0.2]), "segments": still.copy()})
+    return {"query_id": 42, "objects": objs}
+
+
+def _same(a, b, keys):
+    return [k for k in keys if not np.array_equal(np.ascontiguousarray(a[k]).view(np.uint8),
+                                                  np.ascontiguousarray(b[k]).view(np.uint8))]
+
+
+@pytest.mark.parametrize("seed,objs,patches,segs,slabs", [(1, 8, 30, 3, 2), (2, 5, 50, 1, 4), (3, 12, 10, 2, 3)])
+def test_build_restatement_matches_reference(oracle_mod, seed, objs, patches, segs, slabs):
+    from p2cccd_b200 import scenes
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    inp = scenes.proxy_build_input(n_objects=objs, patches_per_object=patches, n_segments=segs, slabs=slabs,
+                                   seed=seed)
+    r, m = oracle_mod.ref_build_proxy_scene(inp), oracle_mod.build_proxy_scene(inp)
+    assert r["n"] == m["n"] == objs * patches * segs * slabs
+    assert _same(r, m, [k for k, _, _ in oracle_mod.BUILT_FIELDS]) == []
+
+
+def test_build_known_answers(oracle_mod):
+    """test_rt_candidate.cpp:98-156 on the restated build and candidates."""
+    import p2cccd_cpp as cpp
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
+
+    sc = oracle_mod.build_proxy_scene(overlapping_build_input())
+    assert sc["query_id"] == 42 and sc["n"] == 4
+    assert cpp.validate_proxy_scene(sc)
+    raw, cand = oracle_mod.proxy_candidates(sc)
+    assert len(raw) == 2 and all(raw["flags"] & 3 == 3) and all(raw["motion_bound"][:, 3] > 0)
+    assert len(cand) == 2 and all(cand["object_a_id"] == 10) and all(cand["object_b_id"] == 20)
+    assert all(cand["rt_hit_count"] == 1) and all(cand["candidate_id"] != 0)
+    d = cpp._density(sc, raw, cand, cpp.RtCandidateTiming(), "cpu_reference")
+    assert (d.proxy_count, d.object_count, d.slab_count, d.cross_object_same_slab_pair_count, d.raw_hit_count,
+            d.compact_candidate_count, d.aabb_overlap_ratio) == (4, 2, 2, 2, 2, 2, 1.0)
+    if oracle_mod.ref_available():
+        r = oracle_mod.ref_build_proxy_scene(overlapping_build_input())
+        assert _same(r, sc, [k for k, _, _ in oracle_mod.BUILT_FIELDS]) == []
+
+
+def _mutations():
+    """(label, mutate(inp)) pairs, each an input BuildProxyScene rejects."""
+    def obj(k, key, v):
+        def f(inp):
+            inp["objects"][k][key] = v
+        return f
+
+    def seg(k, col, v):
+        def f(inp):
+            inp["objects"][k]["segments"][0, col] = v
+        return f
+
+    def quat_zero(inp):
+        inp["objects"][1]["segments"][0, 5:9] = 0.0
+
+    def query0(inp):
+        inp["query_id"] = 0
+
+    return [("unknown proxy type", obj(0, "proxy_type", 0)),
+            ("non-global slab grid", obj(1, "slabs_per_motion_segment", 3)),
+            ("zero slabs", obj(0, "slabs_per_motion_segment", 0)),
+            ("negative eps", obj(1, "eps_proxy", -1e-3)),
+            ("nan eps", obj(1, "eps_proxy", float("nan"))),
+            ("segment t0 >= t1", seg(0, 1, 0.0)),
+            ("non-finite translation", seg(1, 3, float("inf"))),
+            ("zero quaternion", quat_zero),
+            ("non-finite quaternion", seg(0, 14, float("nan"))),
+            ("query id 0", query0)]
+
+
+def _reject_message(fn, inp):
+    try:
+        fn(inp)
+    except ValueError as e:
+        return str(e)
+    return None
+
+
+def _library_host_check(inp):
+    """p2c_proxy_scene_build's host-side validation (it fails before any
+    device work on these inputs; the output pointers are never touched)."""
+    import ctypes
+
+    from p2cccd_b200 import _lib
+    from p2cccd_b200.proxy import ProxyBuildOutStruct, ProxyObjectStruct
+
+    L = _lib.load()
+    objs = inp["objects"]
+    arr = (ProxyObjectStruct * len(objs))()
+    keep, off = [], 0
+    for i, o in enumerate(objs):
+        s = np.ascontiguousarray(o["segments"], np.float64)
+        keep.append(s)
+        arr[i].object_id, arr[i].proxy_type = o["object_id"], o["proxy_type"]
+        arr[i].slabs_per_motion_segment, arr[i].eps_proxy = o["slabs_per_motion_segment"], o["eps_proxy"]
+        arr[i].patch_offset, arr[i].n_patches, arr[i].n_segments = off, len(o["patch_id"]), len(s)
+        arr[i].segments = s.ctypes.data
+        off += len(o["patch_id"])
+    out = ProxyBuildOutStruct(*([16] * 11))
+    rc = L.p2c_proxy_scene_build(int(inp["query_id"]), arr, len(objs), 16, 16, 16, off, 1 << 30, ctypes.byref(out),
+                                 16, 16, 1 << 30, None)
+    assert rc != 0, "expected a host-side rejection"
+    return _lib.last_error()
+
+
+def test_build_rejections_match_reference(oracle_mod):
+    import copy
+
+    import torch
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    for label, mutate in _mutations():
+        inp = copy.deepcopy(overlapping_build_input())
+        mutate(inp)
+        ref_msg = _reject_message(oracle_mod.ref_build_proxy_scene, inp)
+        assert ref_msg is not None, label
+        assert _reject_message(oracle_mod.build_proxy_scene, inp) == ref_msg, label
+        if not torch.cuda.is_available():  # the check never reaches the device; keep it off real devices anyway
+            assert _library_host_check(inp) == ref_msg, label
