@@ -1,14 +1,19 @@
 #!/usr/bin/env python
 """Benchmark of the B200 certification hot path (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scene|plain] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scene|plain|batch|cloth|serve|proxy] [--impl b200|reference]
 
 A step is one pass of the hot path over one batch of seeded synthetic input:
   * scene (default): two 40,960-triangle UV spheres (FP64, rigid translation
     toward contact + per-vertex N(0, 1e-3) jitter) -> swept-AABB candidates ->
     exact VF/EE certificates of every candidate;
-  * plain: 20,000 independent queries (10k VF + 10k EE).
+  * plain: 20,000 independent queries (10k VF + 10k EE);
+  * batch, cloth, serve: many uneven scenes in one launch, the dense cloth
+    any-hit stress case, a Poisson stream through the serving engine.
 metric: certified CCD queries/s (one query = one primitive certificate).
+  * proxy: a proxy scene (rigid bodies x patches x motion segments x time
+    slabs) built and its raw hits and compacted candidates generated;
+    metric: proxies/s.
 
 Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
 on the launching stream, with a 512 MB L2 flush between steps (outside the
@@ -958,6 +963,168 @@ def run_serve(args) -> dict:
     }
 
 
+PROXY_OBJECTS = 32  # rigid bodies of the proxy workload (--proxy-objects)
+PROXY_PATCHES, PROXY_SEGMENTS, PROXY_SLABS = 200, 2, 4
+
+
+def _proxy_input(objects: int, seed: int) -> dict:
+    """The proxy-scene workload: ``objects`` rigid bodies of 200 patches in a
+    box whose volume grows with the body count (constant density), 2 motion
+    segments x 4 slabs each, rotating and drifting (swept AABBs and capsules)."""
+    from p2cccd_b200 import scenes
+
+    spread = 2.0 * (objects / 64.0) ** (1.0 / 3.0)
+    return scenes.proxy_build_input(n_objects=objects, patches_per_object=PROXY_PATCHES, n_segments=PROXY_SEGMENTS,
+                                    slabs=PROXY_SLABS, seed=seed, spread=spread)
+
+
+def _proxy_config(inp: dict, n: int, raw: int, cand: int) -> dict:
+    return {"workload": f"proxy-scene candidates: {len(inp['objects'])} rigid bodies x {PROXY_PATCHES} patches x "
+                        f"{PROXY_SEGMENTS} motion segments x {PROXY_SLABS} time slabs, bodies rotating and drifting "
+                        "in a box of constant body density; BuildProxyScene (patch motion bounds, swept-AABB / "
+                        "capsule proxies) then raw hits and compacted candidates of the whole scene",
+            "proxies_per_step": n, "raw_hits": raw, "candidates": cand, "objects": len(inp["objects"]),
+            "seed": inp.get("seed")}
+
+
+def _proxy_reference(inp: dict, budget_s: float) -> dict:
+    """The reference's BuildProxyScene + GenerateRawCandidatesCpu +
+    CompactRawCandidates (oracle/_ref, unchanged sources, 1 thread as
+    written) on the same scene, whole scenes until budget_s has passed."""
+    import oracle
+
+    done, t0, runs = 0, time.perf_counter(), 0
+    while True:
+        sc = oracle.ref_build_proxy_scene(inp)
+        oracle.ref_proxy_candidates(sc)
+        done += sc["n"]
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return {"proxies": done, "seconds": el, "runs": runs}
+
+
+def run_proxy(args) -> dict | None:
+    import torch
+
+    from p2cccd_b200.proxy import ProxyCandidates, ProxySceneBuild
+
+    world, rank, local = _dist_setup(args)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    inp = _proxy_input(PROXY_OBJECTS, 20261203 + rank)
+    inp["seed"] = 20261203 + rank
+    build = ProxySceneBuild(inp, dev, detail=False)
+    scene = build.run_checked()
+    cands = ProxyCandidates(scene, dev)
+    raw, cand = cands.run_checked()
+    n_raw, n_cand = len(raw), len(cand)
+    cands.fit_capacity()  # buffers (and every sort over them) sized to the scene's hits
+
+    def step():
+        build.run()
+        cands.run()
+
+    # end-to-end: patch arrays from pinned host memory in, counts and records back
+    h_center = build.patch_center.cpu().pin_memory()
+    h_radius = build.patch_radius.cpu().pin_memory()
+    h_pid = build.patch_id.cpu().pin_memory()
+    h_raw = torch.empty_like(cands.raw, device="cpu").pin_memory()
+    h_cand = torch.empty_like(cands.cand, device="cpu").pin_memory()
+    h_counts = torch.empty_like(cands.counts, device="cpu").pin_memory()
+
+    def step_e2e():
+        build.patch_center.copy_(h_center, non_blocking=True)
+        build.patch_radius.copy_(h_radius, non_blocking=True)
+        build.patch_id.copy_(h_pid, non_blocking=True)
+        step()
+        h_counts.copy_(cands.counts, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+        nr, nc = int(h_counts[0]), int(h_counts[1])
+        h_raw[:nr].copy_(cands.raw[:nr], non_blocking=True)
+        h_cand[:nc].copy_(cands.cand[:nc], non_blocking=True)
+
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    sampler = ClockSampler(dev.index if world > 1 else 0)
+    sampler.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    t_begin = time.time()
+    times = time_steps(torch, step, args.steps, flush, stream)
+    torch.cuda.synchronize()
+    t_end = time.time()
+    _barrier(world)
+    clocks = sampler.stop((t_begin, t_end))
+    for _ in range(max(1, args.warmup)):
+        step_e2e()
+    e2e_times = time_steps(torch, step_e2e, args.steps, flush, stream)
+    # phases: build vs candidates
+    ev = []
+    for _ in range(args.steps):
+        flush.fill_(1)
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e[0].record()
+        build.run()
+        e[1].record()
+        cands.run()
+        e[2].record()
+        ev.append(e)
+    torch.cuda.synchronize()
+    build_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
+    cand_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
+    n = build.n
+    ms = statistics.mean(times)
+    value, ms_max = replica_rate(world, n, ms)
+    e2e_value, e2e_ms = replica_rate(world, n, statistics.mean(e2e_times))
+    n_kernels, kernel_names = count_kernels(torch, step)
+    peaks = _load_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "of fallback (6.65 TB/s)"
+    n_patch = int(build.n_patch_entries)
+    records = n // PROXY_PATCHES
+    build_bytes = 36 * n_patch + 200 * records + 113 * n
+    cand_bytes = 109 * n + 64 * n_raw + 80 * n_cand
+    rl = {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "traffic": None, "peak_source": hbm_src}
+    cand_roof = dict(rl, kernel="proxy candidates (sorts, slab sweep, raw hits, compaction)",
+                     achieved=cand_bytes / (cand_ms * 1e-3) / 1e9, frac=cand_bytes / (cand_ms * 1e-3) / 1e9 / hbm_peak,
+                     algorithmic_bytes_per_step=cand_bytes,
+                     bytes_per_unit="109 B read per proxy + 64 B per raw hit + 80 B per candidate written")
+    build_roof = dict(rl, kernel="build_kernel (patch motion bounds and proxy bounds)",
+                      achieved=build_bytes / (build_ms * 1e-3) / 1e9,
+                      frac=build_bytes / (build_ms * 1e-3) / 1e9 / hbm_peak, algorithmic_bytes_per_step=build_bytes,
+                      bytes_per_unit="36 B per patch + 200 B per slab record read, 113 B per proxy written")
+    roofline, secondary = (cand_roof, build_roof) if cand_ms >= build_ms else (build_roof, cand_roof)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = _proxy_reference(inp, args.cpu_budget)
+        cpu = {"value": r["proxies"] / r["seconds"], "unit": "proxies/s", "cores": 1, "kind": "reference",
+               "sample": f"the same {n}-proxy scene, {r['runs']} whole run(s) of the reference build + all-pairs "
+                         "candidates + compaction (1 thread as written)"}
+    if rank != 0:
+        return None
+    return {
+        "metric": "proxy-scene candidates: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "p50_ms": statistics.median(times), "p99_ms": sorted(times)[max(0, int(0.99 * len(times)) - 1)],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {**_proxy_config(inp, n, n_raw, n_cand),
+                   "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "proxies/s", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": h_center.numel() * 8 + h_radius.numel() * 8 + h_pid.numel() * 4,
+                "d2h_bytes_per_step": h_counts.numel() * 8 + 64 * n_raw + 80 * n_cand},
+        "gpu_launches": n_kernels * args.steps if n_kernels >= 0 else None,
+        "kernels_per_step": kernel_names,
+        "phases": {"build_ms": build_ms, "candidates_ms": cand_ms},
+        "roofline": roofline, "roofline_secondary": secondary,
+        "cpu_baseline": cpu, "clocks": clocks,
+    }
+
+
 BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
 CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = configs[3])
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
@@ -976,6 +1143,25 @@ def run_reference(args) -> dict | None:
 
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libp2c_ref.so was not built"}
+    if args.workload == "proxy":
+        inp = _proxy_input(PROXY_OBJECTS, 20261203)
+        inp["seed"] = 20261203
+        budget = REF_ARM_BUDGET_S / max(1, args.steps + args.warmup)
+        for _ in range(args.warmup):
+            _proxy_reference(inp, 0.0)
+        runs = [_proxy_reference(inp, budget) for _ in range(args.steps)]
+        n = sum(r["proxies"] for r in runs) / sum(r["runs"] for r in runs)
+        value = sum(r["proxies"] for r in runs) / sum(r["seconds"] for r in runs)
+        ms = sum(r["seconds"] for r in runs) / sum(r["runs"] for r in runs) * 1e3
+        return {"metric": "proxy-scene candidates: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {**_proxy_config(inp, int(n), -1, -1), "raw_hits": None, "candidates": None},
+                "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": "proxies/s", "cores": 1, "kind": "reference",
+                                 "sample": "whole scenes: BuildProxyScene + GenerateRawCandidatesCpu (all pairs) + "
+                                           "CompactRawCandidates, 1 thread as written"},
+                "e2e": {"value": value, "unit": "proxies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     threads = os.cpu_count() or 1
     cfg = certify.CertConfig(1e-6, 1e-6, 32)
     n_runs = max(1, args.steps + args.warmup)
@@ -1080,7 +1266,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS) + ["serve"])
+    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS) + ["serve", "proxy"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1090,14 +1276,18 @@ def main():
                     help="batch: graph replays per autotuner trial (0: the library's default launch shape)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
+    ap.add_argument("--proxy-objects", type=int, default=32, help="proxy: rigid bodies of 200 patches x 8 slabs")
     args = ap.parse_args()
-    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N
+    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS
+    PROXY_OBJECTS = max(2, args.proxy_objects)
     BATCH_SCENES, AUTOTUNE_REPS = max(1, args.scenes), max(0, args.autotune_reps)
     CLOTH_N = max(9, args.cloth_n)
     if args.impl == "reference":
         line = run_reference(args)
     elif args.workload == "serve":
         line = run_serve(args)
+    elif args.workload == "proxy":
+        line = run_proxy(args)
     else:
         line = run_b200(args)
     if line is not None:

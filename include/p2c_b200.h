@@ -448,6 +448,11 @@ typedef struct p2c_proxy_scene {
   const double* bounds;          /* n x 6: min x, y, z, max x, y, z */
   const double* motion_bound;    /* n x 4: translation_bound, rotation_angle, radial_motion_bound,
                                     conservative_radius */
+  /* Optional widths of the ids (0 = up to 32 bits): every slab id < 2^slab_bits, object id <
+   * 2^object_bits, patch id < 2^patch_bits.  Narrower sort keys; an id outside its width sets
+   * bit 8 of the error word and the results are void (run again without the hint). */
+  uint32_t slab_bits, object_bits, patch_bits;
+  uint32_t pad0;
 } p2c_proxy_scene;
 
 /* RawCandidateHit (rt_candidate/candidate_buffer.h:19-31), 64 bytes. */
@@ -494,7 +499,8 @@ size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap);
  * fails ValidateProxyScene's per-proxy checks, rt_candidate/proxy_scene.cpp:
  * 143-151: type, finite t0 < t1, finite ordered bounds; 2: a hit's float
  * motion bound is negative or non-finite, which ValidateRawHit rejects in
- * compaction, candidate_buffer.cpp:95-99; 4: raw_cap overflowed)}.  Proxy
+ * compaction, candidate_buffer.cpp:95-99; 4: raw_cap overflowed; 8: an id
+ * outside its width hint)}.  Proxy
  * ids equal to the array index and the global slab partition (:58-85) are
  * the caller's checks.  Raw hits beyond raw_cap are dropped (the count is
  * the total); candidate capacity is raw_cap; raw_cap 0 only counts.  No host

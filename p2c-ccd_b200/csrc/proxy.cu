@@ -3,18 +3,23 @@
 // (rt_candidate/candidate_buffer.cpp:144-227).
 //
 // The reference tests every proxy pair (O(n^2)).  Here:
-//   1. two stable radix sorts order the proxies by (slab, min x);
-//   2. a sweep: each proxy walks forward over its slab while the partner's
-//      min x is within its max x, and emits the pairs of different objects
-//      whose time intervals and inclusive AABBs overlap, as (lo << 32 | hi)
-//      keys (each pair once, from the proxy earlier in sweep order);
+//   1. one radix sort orders the proxies by (slab, column of the min corner
+//      over the two narrower axes, quantised min along the widest axis), and
+//      they are gathered into that order as struct-of-arrays;
+//   2. a column-subdivided sweep: each proxy scans the columns and the
+//      sweep-axis window its partners' min corners can lie in, and emits the
+//      pairs of different objects whose time intervals and inclusive AABBs
+//      overlap, as (lo << 32 | hi) keys, each pair once;
 //   3. one radix sort of the keys gives the reference's (i, j) hit order and
 //      the 64-byte RawCandidateHit records are written from the keys;
-//   4. three stable radix sorts of 64-bit key chunks order the hits by the
-//      reference's compaction key (slab, first object, first patch, second
-//      object, second patch, first type, second type), and the head of every
-//      run writes one CandidateRecord (ids 1, 2, ... in key order) with the
-//      run's hit count, the float maximum of its motion bounds and its flags.
+//   4. dense ranks of the slab ids and of the (object, patch) pairs keep the
+//      order of the reference's compaction key (slab, first object, first
+//      patch, second object, second patch, first type, second type), so two
+//      stable radix sorts of exact bit widths order the hits by it; the
+//      head of every run writes one CandidateRecord (ids 1, 2, ... in key
+//      order) with the run's hit count, the float maximum of its motion
+//      bounds and its flags.
+#include <cooperative_groups.h>
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_scan.cuh>
 
@@ -26,6 +31,8 @@
 
 namespace p2c {
 namespace {
+
+namespace cg = cooperative_groups;
 
 static_assert(sizeof(p2c_raw_candidate_hit) == 64, "RawCandidateHit layout");
 static_assert(sizeof(p2c_candidate_record) == 80, "CandidateRecord layout");
@@ -48,14 +55,35 @@ int bit_length(unsigned long long x) {
   return b;
 }
 
+struct ProxyStats {
+  unsigned long long lo_min[3], lo_max[3];  // order keys of the smallest / largest min corner per axis
+  unsigned long long ext_max[3];            // bit patterns of the largest extent per axis (>= 0)
+  double ext_sum[3];                        // sum of extents per axis (grid heuristic only)
+};
+
+// Columns over the two non-sweep axes (each box stored in the column of its
+// min corner) and a 16-bit quantiser of the sweep-axis min.
+struct ProxyGrid {
+  int axis, a1, a2, g1, g2;
+  double base0, scale0, base1, inv1, base2, inv2, reach1, reach2;
+};
+
 struct ProxyLayout {
   unsigned long long* counter;   // [0] raw hits, [1] error word
-  unsigned long long* xkey[2];   // n
-  unsigned* slabkey[2];          // n
-  unsigned* order[2];            // n
-  double* s_minx;                // n, sorted order
-  double* s_maxx;
-  unsigned* s_slab;
+  ProxyStats* stats;
+  ProxyGrid* grid;
+  unsigned long long* key[2];    // n: (slab << 30 | column << 16 | q), sorted copy
+  unsigned* order[2];            // n: proxy index, sorted copy
+  double* s_box;                 // 6 x n, sorted order, struct of arrays: lo, hi, alo, ahi, blo, bhi
+  double* s_t0;                  // n
+  double* s_t1;
+  unsigned* s_obj;
+  unsigned long long* okey[2];   // n: (object << 32 | patch), sorted copy
+  unsigned* oidx;                // n: proxy index in (object, patch) order
+  unsigned* flag;                // n: run heads of a sorted key
+  unsigned* scan;                // n: their inclusive sum
+  unsigned* rank_op;             // n: dense rank of the proxy's (object, patch)
+  unsigned* rank_slab;           // n: dense rank of the proxy's slab
   unsigned long long* pairs[2];  // raw_cap
   unsigned long long* ck[2];     // raw_cap: compaction key chunks
   unsigned* perm[2];             // raw_cap
@@ -69,14 +97,13 @@ struct ProxyLayout {
 
 size_t temp_bytes(long long n, long long cap) {
   const int nn = (int)std::max(n, 1ll), cc = (int)std::max(cap, 1ll);
-  size_t a = 0, b = 0, c = 0, d = 0;
+  size_t a = 0, c = 0, d = 0, e = 0;
   cub::DeviceRadixSort::SortPairs(nullptr, a, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                   (const unsigned*)nullptr, (unsigned*)nullptr, std::max(nn, cc));
-  cub::DeviceRadixSort::SortPairs(nullptr, b, (const unsigned*)nullptr, (unsigned*)nullptr, (const unsigned*)nullptr,
-                                  (unsigned*)nullptr, nn);
   cub::DeviceRadixSort::SortKeys(nullptr, c, (const unsigned long long*)nullptr, (unsigned long long*)nullptr, cc);
   cub::DeviceScan::ExclusiveSum(nullptr, d, (const unsigned*)nullptr, (unsigned*)nullptr, cc + 1);
-  return std::max(std::max(a, b), std::max(c, d));
+  cub::DeviceScan::InclusiveSum(nullptr, e, (const unsigned*)nullptr, (unsigned*)nullptr, nn);
+  return std::max(std::max(a, e), std::max(c, d));
 }
 
 ProxyLayout carve(void* base, long long n, long long cap) {
@@ -90,18 +117,26 @@ ProxyLayout carve(void* base, long long n, long long cap) {
   };
   const size_t N = (size_t)std::max(n, 1ll), C = (size_t)std::max(cap, 1ll);
   L.counter = static_cast<unsigned long long*>(take(16));
+  L.stats = static_cast<ProxyStats*>(take(sizeof(ProxyStats)));
+  L.grid = static_cast<ProxyGrid*>(take(sizeof(ProxyGrid)));
   for (int k = 0; k < 2; ++k) {
-    L.xkey[k] = static_cast<unsigned long long*>(take(8 * N));
-    L.slabkey[k] = static_cast<unsigned*>(take(4 * N));
+    L.key[k] = static_cast<unsigned long long*>(take(8 * N));
     L.order[k] = static_cast<unsigned*>(take(4 * N));
     L.pairs[k] = static_cast<unsigned long long*>(take(8 * C));
     L.ck[k] = static_cast<unsigned long long*>(take(8 * C));
     L.perm[k] = static_cast<unsigned*>(take(4 * C));
     L.gk[k] = static_cast<unsigned long long*>(take(8 * C));
   }
-  L.s_minx = static_cast<double*>(take(8 * N));
-  L.s_maxx = static_cast<double*>(take(8 * N));
-  L.s_slab = static_cast<unsigned*>(take(4 * N));
+  L.s_box = static_cast<double*>(take(6 * 8 * N));
+  L.s_t0 = static_cast<double*>(take(8 * N));
+  L.s_t1 = static_cast<double*>(take(8 * N));
+  L.s_obj = static_cast<unsigned*>(take(4 * N));
+  for (int k = 0; k < 2; ++k) L.okey[k] = static_cast<unsigned long long*>(take(8 * N));
+  L.oidx = static_cast<unsigned*>(take(4 * N));
+  L.flag = static_cast<unsigned*>(take(4 * N));
+  L.scan = static_cast<unsigned*>(take(4 * N));
+  L.rank_op = static_cast<unsigned*>(take(4 * N));
+  L.rank_slab = static_cast<unsigned*>(take(4 * N));
   L.head = static_cast<unsigned*>(take(4 * (C + 1)));
   L.seg = static_cast<unsigned*>(take(4 * (C + 1)));
   L.tmp_bytes = temp_bytes(n, cap);
@@ -110,34 +145,152 @@ ProxyLayout carve(void* base, long long n, long long cap) {
   return L;
 }
 
+__global__ void stats_init_kernel(ProxyLayout L) {
+  if (threadIdx.x != 0) return;
+  ProxyStats& S = *L.stats;
+  for (int a = 0; a < 3; ++a) {
+    S.lo_min[a] = ~0ull;
+    S.lo_max[a] = 0ull;
+    S.ext_max[a] = 0ull;
+    S.ext_sum[a] = 0.0;
+  }
+}
+
 // ValidateProxyScene's per-proxy checks (rt_candidate/proxy_scene.cpp:143-151:
-// concrete type, finite t0 < t1, finite bounds with min <= max) and the x sort
-// key.  Proxy ids (the array index here) and the global slab partition
-// (:58-85) are checked by the host, which holds one interval per slab.
+// concrete type, finite t0 < t1, finite bounds with min <= max) and the
+// statistics of the grid.  Proxy ids (the array index here) and the global
+// slab partition (:58-85) are checked by the host, which holds one interval
+// per slab.
 __global__ void keys_kernel(p2c_proxy_scene sc, ProxyLayout L) {
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool live = i < sc.n;
+  double lo[3] = {0, 0, 0}, ext[3] = {0, 0, 0};
+  bool ok = true;
+  if (live) {
+    const double* b = sc.bounds + 6 * i;
+    ok = (sc.proxy_type[i] == 1 || sc.proxy_type[i] == 2) && isfinite(sc.t0[i]) && isfinite(sc.t1[i]) &&
+         sc.t0[i] < sc.t1[i];
+    for (int a = 0; a < 3; ++a) {
+      ok = ok && isfinite(b[a]) && isfinite(b[3 + a]) && !(b[a] > b[3 + a]);
+      lo[a] = b[a];
+      ext[a] = b[3 + a] - b[a];
+    }
+    if (!ok) atomicOr(L.counter + 1, 1ull);
+    if ((sc.slab_bits && sc.slab_bits < 32 && (sc.slab_id[i] >> sc.slab_bits)) ||
+        (sc.object_bits && sc.object_bits < 32 && (sc.object_id[i] >> sc.object_bits)) ||
+        (sc.patch_bits && sc.patch_bits < 32 && (sc.patch_id[i] >> sc.patch_bits)))
+      atomicOr(L.counter + 1, 8ull);
+  }
+  // warp-reduced statistics of the valid boxes (an invalid scene fails as a whole)
+  const bool use = live && ok;
+  ProxyStats& S = *L.stats;
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    unsigned long long kmin = use ? order_key(lo[a]) : ~0ull, kmax = use ? order_key(lo[a]) : 0ull;
+    unsigned long long emax = use ? (unsigned long long)__double_as_longlong(ext[a]) : 0ull;
+    double esum = use ? ext[a] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      kmin = min(kmin, __shfl_xor_sync(kFull, kmin, o));
+      kmax = max(kmax, __shfl_xor_sync(kFull, kmax, o));
+      emax = max(emax, __shfl_xor_sync(kFull, emax, o));
+      esum += __shfl_xor_sync(kFull, esum, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+      if (kmin != ~0ull) atomicMin(&S.lo_min[a], kmin);
+      if (kmax != 0ull) atomicMax(&S.lo_max[a], kmax);
+      if (emax != 0ull) atomicMax(&S.ext_max[a], emax);
+      if (esum != 0.0) atomicAdd(&S.ext_sum[a], esum);
+    }
+  }
+}
+
+// Clamp to [0, hi], NaN to 0.
+__device__ __forceinline__ int clamp_index(double c, int hi) {
+  return !(c >= 0.0) ? 0 : (c >= (double)hi ? hi : (int)c);
+}
+
+// Sweep axis = the widest spread of min corners; columns over the other two
+// axes about twice the mean extent wide, at most kMaxColumns each.
+__global__ void grid_kernel(ProxyLayout L, long long n) {
+  if (threadIdx.x != 0) return;
+  const ProxyStats& S = *L.stats;
+  double base[3], range[3], mean[3], reach[3];
+  for (int a = 0; a < 3; ++a) {
+    const bool any = S.lo_min[a] != ~0ull;
+    base[a] = any ? unorder_key(S.lo_min[a]) : 0.0;
+    range[a] = any ? unorder_key(S.lo_max[a]) - base[a] : 0.0;
+    if (!(range[a] >= 0.0) || !isfinite(range[a])) range[a] = 0.0;
+    mean[a] = n > 0 ? S.ext_sum[a] / (double)n : 0.0;
+    reach[a] = __longlong_as_double((long long)S.ext_max[a]);
+    if (!isfinite(reach[a])) reach[a] = 0.0;
+  }
+  ProxyGrid g{};
+  g.axis = 0;
+  for (int a = 1; a < 3; ++a)
+    if (range[a] > range[g.axis]) g.axis = a;
+  g.a1 = g.axis == 0 ? 1 : 0;
+  g.a2 = g.axis == 2 ? 1 : 2;
+  const int ax[2] = {g.a1, g.a2};
+  int gg[2];
+  double inv[2];
+  for (int k = 0; k < 2; ++k) {
+    const int a = ax[k];
+    const double w = fmax(2.0 * mean[a], range[a] / kMaxColumns);
+    gg[k] = w > 0.0 ? clamp_index(floor(range[a] / w), kMaxColumns) : 1;
+    if (gg[k] < 1) gg[k] = 1;
+    inv[k] = range[a] > 0.0 ? (double)gg[k] / range[a] : 0.0;
+  }
+  g.g1 = gg[0];
+  g.g2 = gg[1];
+  g.base1 = base[g.a1];
+  g.inv1 = inv[0];
+  g.base2 = base[g.a2];
+  g.inv2 = inv[1];
+  g.reach1 = reach[g.a1];
+  g.reach2 = reach[g.a2];
+  g.base0 = base[g.axis];
+  g.scale0 = range[g.axis] > 0.0 ? 65535.0 / range[g.axis] : 0.0;
+  *L.grid = g;
+}
+
+__device__ __forceinline__ int proxy_column(double x, double base, double inv, int g) {
+  return clamp_index(floor((x - base) * inv), g - 1);
+}
+
+// Monotone (non-decreasing) in x.
+__device__ __forceinline__ unsigned proxy_quantise(double x, const ProxyGrid& g) {
+  return (unsigned)clamp_index(floor((x - g.base0) * g.scale0), 65535);
+}
+
+__global__ void cell_keys_kernel(p2c_proxy_scene sc, ProxyLayout L) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= sc.n) return;
+  const ProxyGrid g = *L.grid;
   const double* b = sc.bounds + 6 * i;
-  bool ok = (sc.proxy_type[i] == 1 || sc.proxy_type[i] == 2) && isfinite(sc.t0[i]) && isfinite(sc.t1[i]) &&
-            sc.t0[i] < sc.t1[i];
-  for (int a = 0; a < 3; ++a) ok = ok && isfinite(b[a]) && isfinite(b[3 + a]) && !(b[a] > b[3 + a]);
-  if (!ok) atomicOr(L.counter + 1, 1ull);
-  L.xkey[0][i] = order_key(b[0]);
+  const int c1 = proxy_column(b[g.a1], g.base1, g.inv1, g.g1);
+  const int c2 = proxy_column(b[g.a2], g.base2, g.inv2, g.g2);
+  const unsigned q = proxy_quantise(b[g.axis], g);
+  L.key[0][i] = ((unsigned long long)sc.slab_id[i] << 30) | ((unsigned long long)(c1 * g.g2 + c2) << 16) | q;
   L.order[0][i] = (unsigned)i;
 }
 
-__global__ void slab_keys_kernel(p2c_proxy_scene sc, ProxyLayout L) {
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (p < sc.n) L.slabkey[0][p] = sc.slab_id[L.order[1][p]];
-}
-
+// Proxies in (slab, column, q) order as struct-of-arrays.
 __global__ void gather_kernel(p2c_proxy_scene sc, ProxyLayout L) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= sc.n) return;
-  const unsigned i = L.order[0][p];
-  L.s_minx[p] = sc.bounds[6 * (long long)i];
-  L.s_maxx[p] = sc.bounds[6 * (long long)i + 3];
-  L.s_slab[p] = sc.slab_id[i];
+  const ProxyGrid g = *L.grid;
+  const long long n = sc.n;
+  const unsigned i = L.order[1][p];
+  const double* b = sc.bounds + 6 * (long long)i;
+  L.s_box[p] = b[g.axis];
+  L.s_box[n + p] = b[3 + g.axis];
+  L.s_box[2 * n + p] = b[g.a1];
+  L.s_box[3 * n + p] = b[3 + g.a1];
+  L.s_box[4 * n + p] = b[g.a2];
+  L.s_box[5 * n + p] = b[3 + g.a2];
+  L.s_t0[p] = sc.t0[i];
+  L.s_t1[p] = sc.t1[i];
+  L.s_obj[p] = sc.object_id[i];
 }
 
 __global__ void fill_kernel(unsigned long long* p, long long n) {
@@ -145,56 +298,113 @@ __global__ void fill_kernel(unsigned long long* p, long long n) {
   if (i < n) p[i] = ~0ull;
 }
 
-// Sweep over the proxies sorted by (slab, min x); the tests are
-// GenerateRawCandidatesCpu's (:158-173: different objects, same slab,
-// TimeOverlap, AabbOverlap).
-__global__ void sweep_kernel(p2c_proxy_scene sc, ProxyLayout L, unsigned long long cap) {
-  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long long n = sc.n;
-  bool live = p < n;
-  unsigned i = 0, slab = 0, obj = 0;
-  double maxx = 0.0, t0 = 0.0, t1 = 0.0, b[6] = {0, 0, 0, 0, 0, 0};
-  if (live) {
-    i = L.order[0][p];
-    slab = L.s_slab[p];
-    maxx = L.s_maxx[p];
-    obj = sc.object_id[i];
-    t0 = sc.t0[i];
-    t1 = sc.t1[i];
-    for (int a = 0; a < 6; ++a) b[a] = sc.bounds[6 * (long long)i + a];
+// First position in [0, n) whose key is >= k.
+__device__ __forceinline__ long long lower_bound(const unsigned long long* __restrict__ keys, long long n,
+                                                 unsigned long long k) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long m = (lo + hi) >> 1;
+    if (keys[m] < k) lo = m + 1;
+    else hi = m;
   }
-  long long q = p + 1;
-  for (;;) {
-    if (live && (q >= n || L.s_slab[q] != slab || L.s_minx[q] > maxx)) live = false;
-    if (!__any_sync(kFull, live)) break;
-    bool found = false;
-    unsigned long long key = 0;
-    if (live) {
-      const unsigned j = L.order[0][q];
-      if (sc.object_id[j] != obj && t0 < sc.t1[j] && sc.t0[j] < t1) {
-        const double* c = sc.bounds + 6 * (long long)j;
-        bool ov = true;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) ov = ov && !(b[3 + a] < c[a] || c[3 + a] < b[a]);
-        if (ov) {
-          found = true;
-          key = ((unsigned long long)min(i, j) << 32) | (unsigned long long)max(i, j);
-        }
-      }
-      ++q;
-    }
-    const unsigned mask = __ballot_sync(kFull, found);
-    if (mask) {
-      const int lane = threadIdx.x & 31, leader = __ffs((int)mask) - 1;
+  return lo;
+}
+
+// Column-subdivided sweep over the sorted proxies.  A box is stored in the
+// column of its min corner, so a partner overlapping box p on the two
+// column axes has its min corner in columns [col(min - reach), col(max)];
+// in each, the partners whose sweep-axis min lies in [p.min, p.max] are the
+// key window [q(p.min), q(p.max)] of p's slab.  A pair is emitted by the box
+// with the smaller (sweep min, index), so exactly once.  The tests are
+// GenerateRawCandidatesCpu's (candidate_buffer.cpp:158-173: different
+// objects, same slab, TimeOverlap, inclusive AabbOverlap).
+//
+// kSweepLanes lanes share one box and take its columns in turn: the work of
+// a box is a chain of dependent loads (a binary search per column, then the
+// window's walk), and splitting it shortens the chain and fills the SMs.
+constexpr int kSweepLanes = 8;
+
+__global__ void __launch_bounds__(kThreads) sweep_kernel(ProxyLayout L, long long n, unsigned long long cap,
+                                                         int rank_bits) {
+  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long p = t / kSweepLanes;
+  const int lane = (int)(t % kSweepLanes);
+  if (p >= n) return;
+  const ProxyGrid g = *L.grid;
+  const double* __restrict__ B = L.s_box;
+  const unsigned long long* __restrict__ K = L.key[1];
+  const double lo = B[p], hi = B[n + p], alo = B[2 * n + p], ahi = B[3 * n + p], blo = B[4 * n + p],
+               bhi = B[5 * n + p];
+  const unsigned obj = L.s_obj[p], id = L.order[1][p];
+  const double t0 = L.s_t0[p], t1 = L.s_t1[p];
+  const unsigned long long slab = K[p] >> 30;
+  // widen the lower columns by a relative 2^-40 so that the rounding of
+  // min - reach never skips the column of a partner's min corner
+  const int c1a = proxy_column(alo - g.reach1 - (fabs(alo) + g.reach1) * 0x1p-40, g.base1, g.inv1, g.g1);
+  const int c1b = proxy_column(ahi, g.base1, g.inv1, g.g1);
+  const int c2a = proxy_column(blo - g.reach2 - (fabs(blo) + g.reach2) * 0x1p-40, g.base2, g.inv2, g.g2);
+  const int c2b = proxy_column(bhi, g.base2, g.inv2, g.g2);
+  const int n2 = c2b - c2a + 1, n_cells = (c1b - c1a + 1) * n2;
+  const unsigned q_lo = proxy_quantise(lo, g), q_hi = proxy_quantise(hi, g);
+  for (int k = lane; k < n_cells; k += kSweepLanes) {
+    const int c1 = c1a + k / n2, c2 = c2a + k % n2;
+    const unsigned long long cell = (slab << 30) | ((unsigned long long)(c1 * g.g2 + c2) << 16);
+    const unsigned long long k_end = cell | q_hi;
+    for (long long j = lower_bound(K, n, cell | q_lo); j < n && K[j] <= k_end; ++j) {
+      const double lj = B[j];
+      const unsigned idj = L.order[1][j];
+      if (lj < lo || (lj == lo && idj <= id) || lj > hi) continue;  // owned by the other box / no overlap
+      if (B[3 * n + j] < alo || ahi < B[2 * n + j] || B[5 * n + j] < blo || bhi < B[4 * n + j]) continue;
+      if (L.s_obj[j] == obj || !(t0 < L.s_t1[j] && L.s_t0[j] < t1)) continue;
+      const cg::coalesced_group grp = cg::coalesced_threads();
       unsigned long long base = 0;
-      if (lane == leader) base = atomicAdd(L.counter, (unsigned long long)__popc(mask));
-      base = __shfl_sync(kFull, base, leader);
-      if (found) {
-        const unsigned long long slot = base + (unsigned long long)__popc(mask & ((1u << lane) - 1u));
-        if (slot < cap) L.pairs[0][slot] = key;
-      }
+      if (grp.thread_rank() == 0) base = atomicAdd(L.counter, (unsigned long long)grp.size());
+      base = grp.shfl(base, 0);
+      const unsigned long long slot = base + grp.thread_rank();
+      if (slot < cap)
+        L.pairs[0][slot] = ((unsigned long long)min(id, idj) << rank_bits) | (unsigned long long)max(id, idj);
     }
   }
+}
+
+// Dense ranks that preserve the compaction key's order
+// (MakeCandidateKey, candidate_buffer.cpp:104-124, compared field by field):
+// the slab id's rank among the scene's slabs and the (object, patch) pair's
+// rank among the scene's pairs.  Equal ranks <=> equal fields, so the key
+// (slab, first (object, patch), second (object, patch), types) sorts as
+// (slab rank, first rank, second rank, types) in few radix passes.
+__global__ void slab_flags_kernel(ProxyLayout L, long long n) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) L.flag[p] = (p == 0 || (L.key[1][p] >> 30) != (L.key[1][p - 1] >> 30)) ? 1u : 0u;
+}
+
+__global__ void slab_rank_kernel(ProxyLayout L, long long n) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) L.rank_slab[L.order[1][p]] = L.scan[p] - 1u;
+}
+
+__global__ void op_keys_kernel(p2c_proxy_scene sc, ProxyLayout L, int patch_bits) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc.n) return;
+  L.okey[0][i] = ((unsigned long long)sc.object_id[i] << patch_bits) | sc.patch_id[i];
+  L.order[0][i] = (unsigned)i;
+}
+
+__global__ void op_flags_kernel(ProxyLayout L, long long n) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) L.flag[p] = (p == 0 || L.okey[1][p] != L.okey[1][p - 1]) ? 1u : 0u;
+}
+
+__global__ void op_rank_kernel(ProxyLayout L, long long n) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p < n) L.rank_op[L.oidx[p]] = L.scan[p] - 1u;
+}
+
+// The first / second proxy of a hit: the smaller (object, patch, proxy id)
+// tuple first (MakeCandidateKey).
+__device__ __forceinline__ bool hit_swapped(const p2c_proxy_scene& sc, unsigned i, unsigned j) {
+  const unsigned fo = sc.object_id[i], so = sc.object_id[j], fp = sc.patch_id[i], sp = sc.patch_id[j];
+  return fo > so || (fo == so && (fp > sp || (fp == sp && i > j)));
 }
 
 // static_cast<float>(std::max(lhs, rhs)) with IEEE round to nearest: a double
@@ -210,11 +420,18 @@ __device__ __forceinline__ bool bound_valid(float v) {
   return (__float_as_uint(v) & 0x7f800000u) != 0x7f800000u && !(v < 0.0f);
 }
 
-// Raw hit records in (i, j) order, and the compaction key chunks of each hit
-// (MakeCandidateKey, :104-124: the first proxy is the smaller (object, patch,
-// proxy) tuple).
+// Raw hit records in (i, j) order, and the compaction key of each hit from
+// the dense ranks (slab rank D, first and second (object, patch) ranks, the
+// two proxy types 1 / 2 as one bit each): one key (D, first, second, types)
+// when it fits 64 bits, else two chunks (second, types) and (D, first).
+struct CompactionKey {
+  int rank_bits;  // bits of a proxy index and of an (object, patch) rank
+  int d_bits;     // bits of a slab rank
+  bool single;    // the whole key fits one 64-bit chunk
+};
+
 __global__ void raw_hits_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned long long* sorted,
-                                unsigned long long cap, p2c_raw_candidate_hit* raw) {
+                                unsigned long long cap, CompactionKey ck, p2c_raw_candidate_hit* raw) {
   const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= (long long)cap) return;
   const unsigned long long k = sorted[h];
@@ -222,15 +439,14 @@ __global__ void raw_hits_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigne
   if (k == ~0ull) {  // past the hits: sorts last in every pass
     L.ck[0][h] = ~0ull;
     L.ck[1][h] = ~0ull;
-    L.pairs[0][h] = ~0ull;
     return;
   }
-  const unsigned i = (unsigned)(k >> 32), j = (unsigned)(k & 0xffffffffull);
+  const unsigned i = (unsigned)(k >> ck.rank_bits), j = (unsigned)(k & ((1ull << ck.rank_bits) - 1ull));
   const double* ma = sc.motion_bound + 4 * (long long)i;
   const double* mb = sc.motion_bound + 4 * (long long)j;
   p2c_raw_candidate_hit r{};
   r.query_id = sc.query_id;
-  r.pair_key = k;
+  r.pair_key = ((unsigned long long)i << 32) | j;  // PairKey
   r.proxy_a_index = i;
   r.proxy_b_index = j;
   r.slab_id = sc.slab_id[i];
@@ -244,25 +460,18 @@ __global__ void raw_hits_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigne
   // ValidateRawHit (:95-99), which CompactRawCandidates applies to every hit
   if (!bound_ok) atomicOr(L.counter + 1, 2ull);
   raw[h] = r;
-  // first / second proxy by (object, patch, proxy id)
-  unsigned fo = sc.object_id[i], fp = sc.patch_id[i], so = sc.object_id[j], sp = sc.patch_id[j];
-  unsigned ft = sc.proxy_type[i], st = sc.proxy_type[j];
-  const bool swap = fo > so || (fo == so && (fp > sp || (fp == sp && i > j)));
-  if (swap) {
-    unsigned t = fo;
-    fo = so;
-    so = t;
-    t = fp;
-    fp = sp;
-    sp = t;
-    t = ft;
-    ft = st;
-    st = t;
+  const bool sw = hit_swapped(sc, i, j);
+  const unsigned f = sw ? j : i, t = sw ? i : j;
+  const unsigned long long types = ((unsigned long long)((sc.proxy_type[f] - 1u) & 1u) << 1) |
+                                   ((sc.proxy_type[t] - 1u) & 1u);
+  const unsigned long long lo = ((unsigned long long)L.rank_op[t] << 2) | types;  // rank_bits + 2 bits
+  const unsigned long long hi = ((unsigned long long)L.rank_slab[i] << ck.rank_bits) | L.rank_op[f];
+  if (ck.single) {
+    L.ck[0][h] = (hi << (ck.rank_bits + 2)) | lo;
+  } else {
+    L.ck[0][h] = lo;
+    L.ck[1][h] = hi;
   }
-  // three chunks, most significant last: (slab, fo) (fp, so) (sp, ft, st)
-  L.ck[0][h] = ((unsigned long long)sp << 16) | ((unsigned long long)ft << 8) | st;
-  L.ck[1][h] = ((unsigned long long)fp << 32) | so;
-  L.pairs[0][h] = ((unsigned long long)r.slab_id << 32) | fo;  // third chunk (the raw keys moved to pairs[1])
 }
 
 __global__ void gather_chunk_kernel(const unsigned long long* chunk, const unsigned* perm, unsigned long long* out,
@@ -273,7 +482,7 @@ __global__ void gather_chunk_kernel(const unsigned long long* chunk, const unsig
 
 // Run heads of the compaction key over the hits in key order.
 __global__ void heads_kernel(ProxyLayout L, const unsigned* perm, const unsigned long long* k0,
-                             const unsigned long long* k1, const unsigned long long* k2, long long cap) {
+                             const unsigned long long* k1, long long cap) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (p > cap) return;
   const long long n_hits = (long long)min(L.counter[0], (unsigned long long)cap);
@@ -283,16 +492,15 @@ __global__ void heads_kernel(ProxyLayout L, const unsigned* perm, const unsigned
     hd = p == 0 ? 1u : 0u;
     if (p > 0) {
       const unsigned b = perm[p - 1];
-      hd = (k0[a] != k0[b] || k1[a] != k1[b] || k2[a] != k2[b]) ? 1u : 0u;
+      hd = (k0[a] != k0[b] || k1[a] != k1[b]) ? 1u : 0u;
     }
   }
   L.head[p] = hd;
 }
 
 __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned* perm,
-                               const p2c_raw_candidate_hit* raw, const unsigned long long* k0,
-                               const unsigned long long* k1, const unsigned long long* k2, long long cap,
-                               p2c_candidate_record* out, unsigned long long* counts) {
+                               const p2c_raw_candidate_hit* raw, long long cap, p2c_candidate_record* out,
+                               unsigned long long* counts) {
   const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long n_hits = (long long)min(L.counter[0], (unsigned long long)cap);
   if (p == 0) {
@@ -306,13 +514,16 @@ __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned
   r.schema_version = 1u;
   r.candidate_id = (unsigned long long)L.seg[p] + 1ull;
   r.query_id = sc.query_id;
-  r.slab_id = (unsigned)(k2[a] >> 32);
-  r.object_a_id = (unsigned)(k2[a] & 0xffffffffull);
-  r.patch_a_id = (unsigned)(k1[a] >> 32);
-  r.object_b_id = (unsigned)(k1[a] & 0xffffffffull);
-  r.patch_b_id = (unsigned)(k0[a] >> 16);
-  r.proxy_type_a = (uint8_t)((k0[a] >> 8) & 0xffull);
-  r.proxy_type_b = (uint8_t)(k0[a] & 0xffull);
+  const unsigned i = raw[a].proxy_a_index, j = raw[a].proxy_b_index;
+  const bool sw = hit_swapped(sc, i, j);
+  const unsigned f = sw ? j : i, t = sw ? i : j;
+  r.slab_id = raw[a].slab_id;
+  r.object_a_id = sc.object_id[f];
+  r.patch_a_id = sc.patch_id[f];
+  r.object_b_id = sc.object_id[t];
+  r.patch_b_id = sc.patch_id[t];
+  r.proxy_type_a = sc.proxy_type[f];
+  r.proxy_type_b = sc.proxy_type[t];
   unsigned count = 0u, flags = 0u;
   float mb[4] = {0.f, 0.f, 0.f, 0.f};
   for (long long q = p; q < n_hits && (q == p || !L.head[q]); ++q) {
@@ -365,48 +576,70 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
   cudaStream_t s = as_stream(stream);
   const p2c_proxy_scene sc = *scene;
   const long long cap = raw_cap;
+  const int rank_bits = std::max(1, bit_length((unsigned long long)std::max(n - 1, 1ll)));  // indices, ranks < n
+  const int slab_bits = sc.slab_bits > 0 && sc.slab_bits < 32 ? (int)sc.slab_bits : 32;
+  const int object_bits = sc.object_bits > 0 && sc.object_bits < 32 ? (int)sc.object_bits : 32;
+  const int patch_bits = sc.patch_bits > 0 && sc.patch_bits < 32 ? (int)sc.patch_bits : 32;
   P2C_CUDA(cudaMemsetAsync(L.counter, 0, 16, s));
   if (n > 0) {
+    stats_init_kernel<<<1, 32, 0, s>>>(L);
     keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
+    grid_kernel<<<1, 32, 0, s>>>(L, n);
+    cell_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
     size_t tb = L.tmp_bytes;
-    // (slab, min x): stable sort by min x, then stable sort by slab
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.xkey[0], L.xkey[1], L.order[0], L.order[1], (int)n, 0, 64,
-                                             s));
-    slab_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
-    tb = L.tmp_bytes;
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.slabkey[0], L.slabkey[1], L.order[1], L.order[0], (int)n,
-                                             0, 32, s));
+    // (slab, column, quantised min) order, ties in proxy order
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key[0], L.key[1], L.order[0], L.order[1], (int)n, 0,
+                                             30 + slab_bits, s));
     gather_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
+    // dense slab ranks from the sorted keys; dense (object, patch) ranks from one more sort
+    slab_flags_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
+    tb = L.tmp_bytes;
+    P2C_CUDA(cub::DeviceScan::InclusiveSum(L.tmp, tb, L.flag, L.scan, (int)n, s));
+    slab_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
+    op_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, patch_bits);
+    tb = L.tmp_bytes;
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.okey[0], L.okey[1], L.order[0], L.oidx, (int)n, 0,
+                                             object_bits + patch_bits, s));
+    op_flags_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
+    tb = L.tmp_bytes;
+    P2C_CUDA(cub::DeviceScan::InclusiveSum(L.tmp, tb, L.flag, L.scan, (int)n, s));
+    op_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
   }
   if (cap > 0) fill_kernel<<<grid_for(cap), kThreads, 0, s>>>(L.pairs[0], cap);
   // the sweep counts every hit, also past the capacity (writes only below it)
-  if (n > 0) sweep_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, (unsigned long long)cap);
+  if (n > 0) sweep_kernel<<<grid_for(n * kSweepLanes), kThreads, 0, s>>>(L, n, (unsigned long long)cap, rank_bits);
   if (cap > 0) {
     size_t tb = L.tmp_bytes;
-    const int pair_bits = 32 + std::max(1, bit_length((unsigned long long)std::max(n - 1, 1ll)));
+    CompactionKey ckey;
+    ckey.rank_bits = rank_bits;
+    ckey.d_bits = std::min(rank_bits, slab_bits);  // slab ranks < min(n, 2^slab_bits)
+    ckey.single = ckey.d_bits + 2 * rank_bits + 2 <= 64;
     // the hits in (i, j) order
-    P2C_CUDA(cub::DeviceRadixSort::SortKeys(L.tmp, tb, L.pairs[0], L.pairs[1], (int)cap, 0,
-                                            std::min(64, pair_bits), s));
-    raw_hits_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, L.pairs[1], (unsigned long long)cap, raw_dev);
+    P2C_CUDA(cub::DeviceRadixSort::SortKeys(L.tmp, tb, L.pairs[0], L.pairs[1], (int)cap, 0, 2 * rank_bits, s));
+    raw_hits_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, L.pairs[1], (unsigned long long)cap, ckey, raw_dev);
     P2C_CUDA(cudaGetLastError());
     // compaction key order: stable sorts by the chunks, least significant first
-    const unsigned long long* chunk[3] = {L.ck[0], L.ck[1], L.pairs[0]};
+    const int n_chunks = ckey.single ? 1 : 2;
+    const unsigned long long* chunk[2] = {L.ck[0], L.ck[1]};
+    const int chunk_bits[2] = {ckey.single ? ckey.d_bits + 2 * rank_bits + 2 : rank_bits + 2,
+                               ckey.d_bits + rank_bits};
     unsigned* perm_in = L.perm[0];
     unsigned* perm_out = L.perm[1];
-    for (int c = 0; c < 3; ++c) {
+    for (int c = 0; c < n_chunks; ++c) {
       gather_chunk_kernel<<<grid_for(cap), kThreads, 0, s>>>(chunk[c], perm_in, L.gk[0], cap);
       tb = L.tmp_bytes;
-      P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.gk[0], L.gk[1], perm_in, perm_out, (int)cap, 0, 64, s));
+      P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.gk[0], L.gk[1], perm_in, perm_out, (int)cap, 0,
+                                               chunk_bits[c], s));
       std::swap(perm_in, perm_out);
     }
-    heads_kernel<<<grid_for(cap + 1), kThreads, 0, s>>>(L, perm_in, chunk[0], chunk[1], chunk[2], cap);
+    heads_kernel<<<grid_for(cap + 1), kThreads, 0, s>>>(L, perm_in, chunk[0], ckey.single ? chunk[0] : chunk[1], cap);
     tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceScan::ExclusiveSum(L.tmp, tb, L.head, L.seg, (int)(cap + 1), s));
-    records_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, perm_in, raw_dev, chunk[0], chunk[1], chunk[2], cap,
-                                                      candidates_dev, reinterpret_cast<unsigned long long*>(counts_dev));
+    records_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, perm_in, raw_dev, cap, candidates_dev,
+                                                      reinterpret_cast<unsigned long long*>(counts_dev));
     P2C_CUDA(cudaGetLastError());
   } else {
-    records_kernel<<<1, kThreads, 0, s>>>(sc, L, L.perm[0], raw_dev, L.ck[0], L.ck[1], L.pairs[0], 0, candidates_dev,
+    records_kernel<<<1, kThreads, 0, s>>>(sc, L, L.perm[0], raw_dev, 0, candidates_dev,
                                           reinterpret_cast<unsigned long long*>(counts_dev));
     P2C_CUDA(cudaGetLastError());
   }

@@ -17,14 +17,20 @@ from . import _lib
 from .certify import _stream_ptr
 from .records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
 
-ERR_INVALID_PROXY, ERR_MOTION_BOUND, ERR_OVERFLOW = 1, 2, 4
+ERR_INVALID_PROXY, ERR_MOTION_BOUND, ERR_OVERFLOW, ERR_ID_BITS = 1, 2, 4, 8
+
+
+def _bits(max_id: int) -> int:
+    """Width hint for ids up to max_id (at least 1 bit)."""
+    return max(1, int(max_id).bit_length())
 
 
 class ProxySceneStruct(ctypes.Structure):
     _fields_ = [("query_id", ctypes.c_uint64), ("n", ctypes.c_int64), ("object_id", ctypes.c_void_p),
                 ("patch_id", ctypes.c_void_p), ("slab_id", ctypes.c_void_p), ("proxy_type", ctypes.c_void_p),
                 ("t0", ctypes.c_void_p), ("t1", ctypes.c_void_p), ("bounds", ctypes.c_void_p),
-                ("motion_bound", ctypes.c_void_p)]
+                ("motion_bound", ctypes.c_void_p), ("slab_bits", ctypes.c_uint32), ("object_bits", ctypes.c_uint32),
+                ("patch_bits", ctypes.c_uint32), ("pad0", ctypes.c_uint32)]
 
 
 class ProxyCandidates:
@@ -53,6 +59,12 @@ class ProxyCandidates:
         st.query_id, st.n = self.query_id, self.n
         for k, _ in self.FIELDS:
             setattr(st, k, self.arrays[k].data_ptr())
+        # id widths: from the scene's own hint, or from host arrays; none for other device arrays
+        hint = scene.get("id_bits")
+        if hint is None and self.n and not any(torch.is_tensor(scene[k]) for k in ("slab_id", "object_id",
+                                                                                   "patch_id")):
+            hint = tuple(_bits(np.max(scene[k])) for k in ("slab_id", "object_id", "patch_id"))
+        st.slab_bits, st.object_bits, st.patch_bits = hint or (0, 0, 0)
         self._struct = st
         self.counts = torch.zeros(4, dtype=torch.int64, device=d)
         self._alloc(max(1024, 4 * self.n) if raw_capacity is None else raw_capacity)
@@ -65,6 +77,14 @@ class ProxyCandidates:
         self.ws = torch.empty(int(self.lib.p2c_proxy_candidates_workspace_bytes(self.n, self.cap)), dtype=torch.uint8,
                               device=d)
 
+    def fit_capacity(self, margin: float = 1.25, slack: int = 1024) -> int:
+        """Size the raw-hit and candidate buffers to the last run's raw hit
+        count (x margin + slack): every sort and pass of the next runs covers
+        that many entries.  Returns the new capacity."""
+        n_raw = int(self.counts[0].item())
+        self._alloc(int(n_raw * margin) + slack)
+        return self.cap
+
     def run(self) -> None:
         """Enqueue candidate generation on the current stream (no host sync)."""
         _lib.check(self.lib.p2c_proxy_candidates(ctypes.byref(self._struct), self.raw.data_ptr(), self.cap,
@@ -76,10 +96,13 @@ class ProxyCandidates:
         scene, and unless ``raw_only`` on a hit whose motion bound the
         reference's compaction rejects.  Returns (raw hits, candidates) as
         host record arrays (candidates empty when ``raw_only``)."""
-        for _ in range(max_retries + 1):
+        for _ in range(max_retries + 2):
             self.run()
             c = self.counts.cpu().numpy()
             n_raw, n_cand, err = int(c[0]), int(c[1]), int(c[2])
+            if err & ERR_ID_BITS:  # a width hint was wrong: the run is void, drop the hints
+                self._struct.slab_bits = self._struct.object_bits = self._struct.patch_bits = 0
+                continue
             if err & ERR_INVALID_PROXY:
                 raise ValueError("proxy scene fails validation (proxy type, finite t0 < t1, finite ordered bounds)")
             if err & ERR_MOTION_BOUND and not raw_only:
@@ -156,6 +179,11 @@ class ProxySceneBuild:
             off += n_p
         self._objects, self.n_objects = arr, k
         self.n_patch_entries = off
+        max_slab = max((len(self._segments[i]) * int(o["slabs_per_motion_segment"]) - 1 for i, o in enumerate(objs)),
+                       default=0)
+        max_obj = max((int(o["object_id"]) for o in objs), default=0)
+        max_patch = max((int(np.max(o["patch_id"])) for o in objs if len(o["patch_id"])), default=0)
+        self.id_bits = (_bits(max(max_slab, 0)), _bits(max_obj), _bits(max_patch))
         cat = (lambda key, dt, w: np.ascontiguousarray(np.concatenate(
             [np.asarray(o[key], dt).reshape(-1, w) for o in objs]) if objs else np.zeros((0, w), dt)))
         self.patch_id = torch.from_numpy(cat("patch_id", np.uint32, 1).view(np.int32).reshape(-1)).to(d)
@@ -203,8 +231,9 @@ class ProxySceneBuild:
         return self.scene()
 
     def scene(self) -> dict:
-        """The built proxies as device tensors (uint32 fields as int32)."""
-        sc = {"query_id": self.query_id, "n": self.n}
+        """The built proxies as device tensors (uint32 fields as int32), with
+        the widths of their slab, object and patch ids."""
+        sc = {"query_id": self.query_id, "n": self.n, "id_bits": self.id_bits}
         sc.update(self.out)
         return sc
 

@@ -222,7 +222,8 @@ def _quat(axis, angle, scale=1.0):
 
 
 def proxy_build_input(n_objects: int = 6, patches_per_object: int = 60, n_segments: int = 2, slabs: int = 3,
-                      seed: int = 20261203, query_id: int = 11, eps_proxy: float = 1e-3) -> dict:
+                      seed: int = 20261203, query_id: int = 11, eps_proxy: float = 1e-3,
+                      spread: float | None = None) -> dict:
     """A ProxySceneBuildInput as arrays: ``objects`` of rigid bodies whose
     patches (centres on a sphere about the body origin, small radii) move
     over piecewise rigid motion segments partitioning [0, 1] the same way for
@@ -231,14 +232,21 @@ def proxy_build_input(n_objects: int = 6, patches_per_object: int = 60, n_segmen
     the near-parallel lerp branch (a still body and a tiny rotation), a
     quaternion pair of opposite signs and quaternions of non-unit norm.
     Segment rows are t0, t1, translation_t0, rotation_t0 (x, y, z, w),
-    translation_t1, rotation_t1."""
+    translation_t1, rotation_t1.  With ``spread`` the bodies start anywhere
+    in [-spread, spread]^3 and drift 0.1-0.4 in a random direction instead,
+    a sparse scene where only neighbours meet."""
     g = rng(seed)
     cuts = np.linspace(0.0, 1.0, n_segments + 1)
     objects = []
     pid = 0
     for o in range(n_objects):
-        start = g.uniform(-1.0, 1.0, 3)
-        vel = -start * g.uniform(0.6, 1.1)
+        if spread is None:
+            start = g.uniform(-1.0, 1.0, 3)
+            vel = -start * g.uniform(0.6, 1.1)
+        else:
+            start = g.uniform(-spread, spread, 3)
+            vel = g.normal(size=3)
+            vel *= g.uniform(0.1, 0.4) / np.linalg.norm(vel)
         axis = g.normal(size=3)
         spin = [g.uniform(0.5, 3.0), 0.0, 1e-3, g.uniform(0.5, 3.0)][o % 4]
         segs = np.zeros((n_segments, 16))

@@ -187,3 +187,36 @@ def test_device_build_flags_bad_patches(cuda_device, oracle_mod):
                 oracle_mod.ref_build_proxy_scene(a)
         with pytest.raises(ValueError, match=msg):
             ProxySceneBuild(a, cuda_device).run_checked()
+
+
+def test_fitted_capacity_keeps_results(cuda_device, oracle_mod):
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    sc = scenes.proxy_scene(n_objects=7, patches_per_object=90, n_slabs=5, seed=12, duplicates=0.3)
+    ref_raw, ref_cand = oracle_mod.proxy_candidates(sc)
+    pc = ProxyCandidates(sc, cuda_device)
+    raw0, cand0 = pc.run_checked()
+    assert pc.fit_capacity(margin=1.0, slack=0) == len(ref_raw)  # exactly full: no overflow
+    raw1, cand1 = pc.run_checked()
+    for raw, cand in ((raw0, cand0), (raw1, cand1)):
+        assert np.array_equal(raw.view(np.uint8), ref_raw.view(np.uint8))
+        assert np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
+
+
+def test_wrong_id_width_hint_falls_back(cuda_device, oracle_mod):
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ERR_ID_BITS, ProxyCandidates
+
+    sc = scenes.proxy_scene(n_objects=5, patches_per_object=50, n_slabs=6, seed=21, duplicates=0.2)
+    ref_raw, ref_cand = oracle_mod.proxy_candidates(sc)
+    for hint in ((2, 3, 6), (3, 1, 6), (3, 3, 4)):  # slab, object, patch ids wider than claimed
+        pc = ProxyCandidates(dict(sc, id_bits=hint), cuda_device)
+        pc.run()
+        assert int(pc.counts[2].item()) & ERR_ID_BITS
+        raw, cand = pc.run_checked()
+        assert np.array_equal(raw.view(np.uint8), ref_raw.view(np.uint8))
+        assert np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
+    exact = ProxyCandidates(dict(sc, id_bits=(3, 3, 6)), cuda_device)  # max ids 5, 4, 49
+    raw, cand = exact.run_checked()
+    assert exact._struct.slab_bits == 3 and np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
