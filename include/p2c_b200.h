@@ -485,7 +485,10 @@ typedef struct p2c_candidate_record {
   uint32_t pad2;
 } p2c_candidate_record;
 
-size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap);
+/* Workspace of p2c_proxy_candidates for n proxies, raw_cap hits and the
+ * scene's slab_bits hint (0: none; a hint of at most 6 bits adds a direct
+ * (slab, column) table of 2^(slab_bits + 14) x 16 bytes). */
+size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap, uint32_t slab_bits);
 
 /* Candidates of a proxy scene: GenerateRawCandidatesCpu then
  * CompactRawCandidates (rt_candidate/candidate_buffer.cpp:144-227) on the

@@ -78,12 +78,19 @@ struct ProxyLayout {
   double* s_t0;                  // n
   double* s_t1;
   unsigned* s_obj;
+  float4* s_f;                   // n: column-axis bounds rounded outward (a float prefilter)
   unsigned long long* okey[2];   // n: (object << 32 | patch), sorted copy
   unsigned* oidx;                // n: proxy index in (object, patch) order
   unsigned* flag;                // n: run heads of a sorted key
   unsigned* scan;                // n: their inclusive sum
   unsigned* rank_op;             // n: dense rank of the proxy's (object, patch)
   unsigned* rank_slab;           // n: dense rank of the proxy's slab
+  // direct (slab, column) table, when the slab ids are known to be narrow:
+  // per run {first entry, one past the last, float keys of the largest max
+  // corner along the two column axes}
+  int table_bits;                // slab id bits of the table (0: no table, binary search)
+  uint4* cells;                  // [2^(table_bits + 14)]
+  size_t table_bytes;
   unsigned long long* pairs[2];  // raw_cap
   unsigned long long* ck[2];     // raw_cap: compaction key chunks
   unsigned* perm[2];             // raw_cap
@@ -106,7 +113,15 @@ size_t temp_bytes(long long n, long long cap) {
   return std::max(std::max(a, e), std::max(c, d));
 }
 
-ProxyLayout carve(void* base, long long n, long long cap) {
+// The direct (slab, column) table is used for slab ids of at most this many
+// bits (2^(6 + 14) runs of 16 bytes, 16 MB).
+constexpr int kTableSlabBits = 6;
+
+int table_bits_for(uint32_t slab_bits) {
+  return slab_bits > 0 && slab_bits <= (uint32_t)kTableSlabBits ? (int)slab_bits : 0;
+}
+
+ProxyLayout carve(void* base, long long n, long long cap, int table_bits) {
   ProxyLayout L{};
   size_t off = 0;
   char* b = static_cast<char*>(base);
@@ -137,6 +152,11 @@ ProxyLayout carve(void* base, long long n, long long cap) {
   L.scan = static_cast<unsigned*>(take(4 * N));
   L.rank_op = static_cast<unsigned*>(take(4 * N));
   L.rank_slab = static_cast<unsigned*>(take(4 * N));
+  L.s_f = static_cast<float4*>(take(sizeof(float4) * N));
+  L.table_bits = table_bits;
+  const size_t T = table_bits > 0 ? (size_t)1 << (table_bits + kCellBits) : 0;
+  L.table_bytes = sizeof(uint4) * T;
+  L.cells = static_cast<uint4*>(take(L.table_bytes));
   L.head = static_cast<unsigned*>(take(4 * (C + 1)));
   L.seg = static_cast<unsigned*>(take(4 * (C + 1)));
   L.tmp_bytes = temp_bytes(n, cap);
@@ -181,9 +201,11 @@ __global__ void keys_kernel(p2c_proxy_scene sc, ProxyLayout L) {
         (sc.patch_bits && sc.patch_bits < 32 && (sc.patch_id[i] >> sc.patch_bits)))
       atomicOr(L.counter + 1, 8ull);
   }
-  // warp-reduced statistics of the valid boxes (an invalid scene fails as a whole)
+  // block-reduced statistics of the valid boxes (an invalid scene fails as a whole)
   const bool use = live && ok;
-  ProxyStats& S = *L.stats;
+  __shared__ unsigned long long s_kmin[kThreads / 32][3], s_kmax[kThreads / 32][3], s_emax[kThreads / 32][3];
+  __shared__ double s_esum[kThreads / 32][3];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     unsigned long long kmin = use ? order_key(lo[a]) : ~0ull, kmax = use ? order_key(lo[a]) : 0ull;
@@ -195,12 +217,29 @@ __global__ void keys_kernel(p2c_proxy_scene sc, ProxyLayout L) {
       emax = max(emax, __shfl_xor_sync(kFull, emax, o));
       esum += __shfl_xor_sync(kFull, esum, o);
     }
-    if ((threadIdx.x & 31) == 0) {
-      if (kmin != ~0ull) atomicMin(&S.lo_min[a], kmin);
-      if (kmax != 0ull) atomicMax(&S.lo_max[a], kmax);
-      if (emax != 0ull) atomicMax(&S.ext_max[a], emax);
-      if (esum != 0.0) atomicAdd(&S.ext_sum[a], esum);
+    if (lane == 0) {
+      s_kmin[warp][a] = kmin;
+      s_kmax[warp][a] = kmax;
+      s_emax[warp][a] = emax;
+      s_esum[warp][a] = esum;
     }
+  }
+  __syncthreads();
+  if (threadIdx.x < 3) {
+    const int a = threadIdx.x;
+    unsigned long long kmin = ~0ull, kmax = 0ull, emax = 0ull;
+    double esum = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) {
+      kmin = min(kmin, s_kmin[w][a]);
+      kmax = max(kmax, s_kmax[w][a]);
+      emax = max(emax, s_emax[w][a]);
+      esum += s_esum[w][a];
+    }
+    ProxyStats& S = *L.stats;
+    if (kmin != ~0ull) atomicMin(&S.lo_min[a], kmin);
+    if (kmax != 0ull) atomicMax(&S.lo_max[a], kmax);
+    if (emax != 0ull) atomicMax(&S.ext_max[a], emax);
+    if (esum != 0.0) atomicAdd(&S.ext_sum[a], esum);
   }
 }
 
@@ -210,8 +249,10 @@ __device__ __forceinline__ int clamp_index(double c, int hi) {
 }
 
 // Sweep axis = the widest spread of min corners; columns over the other two
-// axes about twice the mean extent wide, at most kMaxColumns each.
+// axes one (direct table: a column costs one 16-byte load) or two (binary
+// search) mean extents wide, at most kMaxColumns each.
 __global__ void grid_kernel(ProxyLayout L, long long n) {
+  const double width_mult = L.table_bits > 0 ? 1.0 : 2.0;
   if (threadIdx.x != 0) return;
   const ProxyStats& S = *L.stats;
   double base[3], range[3], mean[3], reach[3];
@@ -235,7 +276,7 @@ __global__ void grid_kernel(ProxyLayout L, long long n) {
   double inv[2];
   for (int k = 0; k < 2; ++k) {
     const int a = ax[k];
-    const double w = fmax(2.0 * mean[a], range[a] / kMaxColumns);
+    const double w = fmax(width_mult * mean[a], range[a] / kMaxColumns);
     gg[k] = w > 0.0 ? clamp_index(floor(range[a] / w), kMaxColumns) : 1;
     if (gg[k] < 1) gg[k] = 1;
     inv[k] = range[a] > 0.0 ? (double)gg[k] / range[a] : 0.0;
@@ -291,6 +332,24 @@ __global__ void gather_kernel(p2c_proxy_scene sc, ProxyLayout L) {
   L.s_t0[p] = sc.t0[i];
   L.s_t1[p] = sc.t1[i];
   L.s_obj[p] = sc.object_id[i];
+  L.s_f[p] = make_float4(__double2float_rd(b[g.a1]), __double2float_ru(b[3 + g.a1]), __double2float_rd(b[g.a2]),
+                         __double2float_ru(b[3 + g.a2]));
+}
+
+// Begin / end of every (slab, column) run of the sorted keys and the float
+// keys (rounded up) of the largest max corner of its boxes on the two column
+// axes.
+__global__ void table_kernel(ProxyLayout L, long long n) {
+  const long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= n) return;
+  const unsigned long long* K = L.key[1];
+  const unsigned long long run = K[p] >> 16;  // slab << 14 | column
+  if ((K[p] >> 30) >> L.table_bits) return;   // a slab id past its width hint (error word bit 8)
+  uint4* c = L.cells + run;
+  if (p == 0 || (K[p - 1] >> 16) != run) c->x = (unsigned)p;
+  if (p == n - 1 || (K[p + 1] >> 16) != run) c->y = (unsigned)(p + 1);
+  atomicMax(&c->z, fkey_up(L.s_box[3 * n + p]));
+  atomicMax(&c->w, fkey_up(L.s_box[5 * n + p]));
 }
 
 __global__ void fill_kernel(unsigned long long* p, long long n) {
@@ -320,8 +379,12 @@ __device__ __forceinline__ long long lower_bound(const unsigned long long* __res
 // objects, same slab, TimeOverlap, inclusive AabbOverlap).
 //
 // kSweepLanes lanes share one box and take its columns in turn: the work of
-// a box is a chain of dependent loads (a binary search per column, then the
-// window's walk), and splitting it shortens the chain and fills the SMs.
+// a box is a chain of dependent loads (a column lookup, a search for the
+// window's start, then the window's walk), and splitting it shortens the
+// chain and fills the SMs.  With narrow slab ids a direct (slab, column)
+// table gives each column's run and lets columns whose boxes cannot reach
+// the scanning box be skipped; otherwise a binary search over all keys
+// finds each window.
 constexpr int kSweepLanes = 8;
 
 __global__ void __launch_bounds__(kThreads) sweep_kernel(ProxyLayout L, long long n, unsigned long long cap,
@@ -346,24 +409,50 @@ __global__ void __launch_bounds__(kThreads) sweep_kernel(ProxyLayout L, long lon
   const int c2b = proxy_column(bhi, g.base2, g.inv2, g.g2);
   const int n2 = c2b - c2a + 1, n_cells = (c1b - c1a + 1) * n2;
   const unsigned q_lo = proxy_quantise(lo, g), q_hi = proxy_quantise(hi, g);
+  // column-axis bounds rounded outward: a pair that overlaps in doubles
+  // overlaps in these floats, so they reject most entries with one load
+  const float f_alo = __double2float_rd(alo), f_ahi = __double2float_ru(ahi), f_blo = __double2float_rd(blo),
+              f_bhi = __double2float_ru(bhi);
+  // one partner entry j: prefilter, ownership, exact overlap, object and time tests, then append
+  auto visit = [&](long long j) {
+    const float4 f = L.s_f[j];
+    if (f.y < f_alo || f_ahi < f.x || f.w < f_blo || f_bhi < f.z) return;
+    const double lj = B[j];
+    const unsigned idj = L.order[1][j];
+    if (lj < lo || (lj == lo && idj <= id) || lj > hi) return;  // owned by the other box / no overlap
+    if (B[3 * n + j] < alo || ahi < B[2 * n + j] || B[5 * n + j] < blo || bhi < B[4 * n + j]) return;
+    if (L.s_obj[j] == obj || !(t0 < L.s_t1[j] && L.s_t0[j] < t1)) return;
+    const cg::coalesced_group grp = cg::coalesced_threads();
+    unsigned long long base = 0;
+    if (grp.thread_rank() == 0) base = atomicAdd(L.counter, (unsigned long long)grp.size());
+    base = grp.shfl(base, 0);
+    const unsigned long long slot = base + grp.thread_rank();
+    if (slot < cap)
+      L.pairs[0][slot] = ((unsigned long long)min(id, idj) << rank_bits) | (unsigned long long)max(id, idj);
+  };
+  if (L.table_bits > 0) {
+    if (slab >> L.table_bits) return;  // past the slab width hint (error word bit 8)
+    const unsigned k_alo = fkey_down(alo), k_blo = fkey_down(blo);
+    for (int k = lane; k < n_cells; k += kSweepLanes) {
+      const int c1 = c1a + k / n2, c2 = c2a + k % n2;
+      const uint4 c = L.cells[(slab << kCellBits) | (unsigned long long)(c1 * g.g2 + c2)];
+      // empty, or no box of this column reaches the scanning box on a column axis
+      if (c.x >= c.y || c.z < k_alo || c.w < k_blo) continue;
+      unsigned b = c.x, r = c.y;
+      while (b < r) {  // first entry of the column with q >= q_lo
+        const unsigned m = (b + r) >> 1;
+        if ((unsigned)(K[m] & 0xffffull) < q_lo) b = m + 1;
+        else r = m;
+      }
+      for (unsigned j = b; j < c.y && (unsigned)(K[j] & 0xffffull) <= q_hi; ++j) visit(j);
+    }
+    return;
+  }
   for (int k = lane; k < n_cells; k += kSweepLanes) {
     const int c1 = c1a + k / n2, c2 = c2a + k % n2;
     const unsigned long long cell = (slab << 30) | ((unsigned long long)(c1 * g.g2 + c2) << 16);
     const unsigned long long k_end = cell | q_hi;
-    for (long long j = lower_bound(K, n, cell | q_lo); j < n && K[j] <= k_end; ++j) {
-      const double lj = B[j];
-      const unsigned idj = L.order[1][j];
-      if (lj < lo || (lj == lo && idj <= id) || lj > hi) continue;  // owned by the other box / no overlap
-      if (B[3 * n + j] < alo || ahi < B[2 * n + j] || B[5 * n + j] < blo || bhi < B[4 * n + j]) continue;
-      if (L.s_obj[j] == obj || !(t0 < L.s_t1[j] && L.s_t0[j] < t1)) continue;
-      const cg::coalesced_group grp = cg::coalesced_threads();
-      unsigned long long base = 0;
-      if (grp.thread_rank() == 0) base = atomicAdd(L.counter, (unsigned long long)grp.size());
-      base = grp.shfl(base, 0);
-      const unsigned long long slot = base + grp.thread_rank();
-      if (slot < cap)
-        L.pairs[0][slot] = ((unsigned long long)min(id, idj) << rank_bits) | (unsigned long long)max(id, idj);
-    }
+    for (long long j = lower_bound(K, n, cell | q_lo); j < n && K[j] <= k_end; ++j) visit(j);
   }
 }
 
@@ -548,9 +637,9 @@ __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned
 
 extern "C" {
 
-size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap) {
+size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap, uint32_t slab_bits) {
   if (n_proxies < 0 || raw_cap < 0) return 0;
-  return p2c::carve(nullptr, n_proxies, raw_cap).total + 256;
+  return p2c::carve(nullptr, n_proxies, raw_cap, p2c::table_bits_for(slab_bits)).total + 256;
 }
 
 int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* raw_dev, int64_t raw_cap,
@@ -569,10 +658,11 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
                 scene->proxy_type == nullptr || scene->t0 == nullptr || scene->t1 == nullptr ||
                 scene->bounds == nullptr || scene->motion_bound == nullptr))
     return fail(P2C_ERR_INVALID, "proxy scene arrays are null");
-  const size_t need = carve(nullptr, n, raw_cap).total;
+  const int table_bits = table_bits_for(scene->slab_bits);
+  const size_t need = carve(nullptr, n, raw_cap, table_bits).total;
   if (workspace_dev == nullptr || workspace_bytes < need)
     return fail(P2C_ERR_INVALID, "proxy candidate workspace too small: %zu < %zu bytes", workspace_bytes, need);
-  ProxyLayout L = carve(workspace_dev, n, raw_cap);
+  ProxyLayout L = carve(workspace_dev, n, raw_cap, table_bits);
   cudaStream_t s = as_stream(stream);
   const p2c_proxy_scene sc = *scene;
   const long long cap = raw_cap;
@@ -591,6 +681,10 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key[0], L.key[1], L.order[0], L.order[1], (int)n, 0,
                                              30 + slab_bits, s));
     gather_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
+    if (L.table_bits > 0) {
+      P2C_CUDA(cudaMemsetAsync(L.cells, 0, L.table_bytes, s));
+      table_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
+    }
     // dense slab ranks from the sorted keys; dense (object, patch) ranks from one more sort
     slab_flags_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
     tb = L.tmp_bytes;

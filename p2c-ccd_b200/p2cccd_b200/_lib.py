@@ -79,7 +79,7 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_refinement_children": (_int, [_i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_uint16, _f64,
                                        ctypes.c_uint64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                        _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p]),
-    "p2c_proxy_candidates_workspace_bytes": (_size, [_i64, _i64]),
+    "p2c_proxy_candidates_workspace_bytes": (_size, [_i64, _i64, ctypes.c_uint32]),
     "p2c_proxy_candidates": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p]),
     "p2c_proxy_scene_count": (_i64, [_c_void_p, _i64]),
     "p2c_proxy_scene_build_workspace_bytes": (_size, [_c_void_p, _i64]),

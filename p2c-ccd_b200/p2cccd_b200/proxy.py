@@ -69,13 +69,14 @@ class ProxyCandidates:
         self.counts = torch.zeros(4, dtype=torch.int64, device=d)
         self._alloc(max(1024, 4 * self.n) if raw_capacity is None else raw_capacity)
 
+
     def _alloc(self, cap: int) -> None:
         d = self.device
         self.cap = max(0, int(cap))  # 0: only count the hits
         self.raw = torch.empty((self.cap, 64), dtype=torch.uint8, device=d)
         self.cand = torch.empty((self.cap, 80), dtype=torch.uint8, device=d)
-        self.ws = torch.empty(int(self.lib.p2c_proxy_candidates_workspace_bytes(self.n, self.cap)), dtype=torch.uint8,
-                              device=d)
+        ws = int(self.lib.p2c_proxy_candidates_workspace_bytes(self.n, self.cap, self._struct.slab_bits))
+        self.ws = torch.empty(ws, dtype=torch.uint8, device=d)
 
     def fit_capacity(self, margin: float = 1.25, slack: int = 1024) -> int:
         """Size the raw-hit and candidate buffers to the last run's raw hit

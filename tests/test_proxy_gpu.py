@@ -220,3 +220,24 @@ def test_wrong_id_width_hint_falls_back(cuda_device, oracle_mod):
     exact = ProxyCandidates(dict(sc, id_bits=(3, 3, 6)), cuda_device)  # max ids 5, 4, 49
     raw, cand = exact.run_checked()
     assert exact._struct.slab_bits == 3 and np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
+
+
+@pytest.mark.parametrize("mode", ["table", "no_hint", "wide_slabs"])
+def test_sweep_paths_agree(cuda_device, oracle_mod, mode):
+    """The direct (slab, column) table (narrow slab ids) and the binary
+    search over the sorted keys (no hint, or slab ids wider than the table)
+    give the reference's hits."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    for seed, dups in ((31, 0.0), (32, 0.4)):
+        sc = scenes.proxy_scene(n_objects=9, patches_per_object=70, n_slabs=5, seed=seed, duplicates=dups)
+        if mode == "wide_slabs":
+            sc["slab_id"] = (sc["slab_id"].astype(np.uint64) * 40_000_003 % (1 << 32)).astype(np.uint32)
+        ref_raw, ref_cand = oracle_mod.proxy_candidates(sc)
+        pc = ProxyCandidates(dict(sc, id_bits=(0, 0, 0)) if mode == "no_hint" else sc, cuda_device)
+        raw, cand = pc.run_checked()
+        table = 0 < pc._struct.slab_bits <= 6
+        assert table == (mode == "table")
+        assert np.array_equal(raw.view(np.uint8), ref_raw.view(np.uint8))
+        assert np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
