@@ -583,6 +583,52 @@ int p2c_proxy_scene_build(uint64_t query_id, const p2c_proxy_object_input* objec
                           const p2c_proxy_build_out* out,
                           uint64_t* error_word_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* ---- proposal feature rows (the learned scheduler's inputs) -------------- */
+/* CandidateDensityStats (rt_candidate/candidate_generation_result.h:21-37)
+ * without its timing and backend name, 96 bytes. */
+typedef struct p2c_candidate_density {
+  uint64_t query_id;
+  uint64_t proxy_count, object_count, slab_count, cross_object_same_slab_pair_count;
+  uint64_t raw_hit_count, compact_candidate_count;
+  double raw_hits_per_proxy, candidates_per_proxy, candidates_per_slab, aabb_overlap_ratio;
+  double avg_rt_hits_per_candidate;
+} p2c_candidate_density;
+
+/* ProposalFeatureRow (proposal/proposal_features.h:27-43), 256 bytes. */
+typedef struct p2c_proposal_feature_row {
+  uint32_t schema_version;
+  uint32_t pad0;
+  uint64_t query_id;
+  uint64_t candidate_id;
+  uint32_t slab_id;
+  uint32_t object_a_id, patch_a_id, object_b_id, patch_b_id;
+  float features[32];
+  float interval_targets[8];
+  float family_targets[8];
+  float priority_target, cost_target, uncertainty_target;
+  uint32_t target_mask;
+  uint32_t pad1;
+} p2c_proposal_feature_row;
+
+size_t p2c_proposal_feature_rows_workspace_bytes(int64_t n_proxies);
+
+/* The density stats and proposal feature rows of a proxy scene's candidates,
+ * on the device: ComputeCandidateDensityStats (rt_candidate/
+ * candidate_stats.cpp:128-170) into *density_dev and ExtractProposalFeatureRows
+ * (proposal/proposal_features.cpp:236-259, rows by FillFeatureRow :122-205)
+ * into rows_dev[0 .. min(counts_dev[1], cap)).  counts_dev and candidates_dev
+ * are p2c_proxy_candidates' outputs for the same scene (no host sync between
+ * the calls).  Each candidate side maps to the first proxy in scene order with
+ * its (slab, object, patch, type).  *error_word_dev: bit 1 a candidate fails
+ * ValidateCandidateRecord (common/validators.cpp:160-181), bit 2 a candidate
+ * side maps to no proxy; such rows are zero.  The scene's id width hints
+ * narrow the sorts (an id beyond its hint voids the results, as for
+ * p2c_proxy_candidates).  No host sync. */
+int p2c_proposal_feature_rows(const p2c_proxy_scene* scene, const p2c_candidate_record* candidates_dev,
+                              int64_t cap, const uint64_t* counts_dev, p2c_candidate_density* density_dev,
+                              p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* workspace_dev,
+                              size_t workspace_bytes, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

@@ -673,3 +673,126 @@ def build_proxy_scene(inp: dict) -> dict:
     for j, (k, dt_, sh) in enumerate(BUILT_FIELDS):
         out[k] = np.array([r[j] for r in rows], dt_).reshape((n,) + sh)
     return out
+
+
+
+# ---- proposal feature rows (proposal/proposal_features.cpp) ----
+
+def ref_proposal_feature_rows(sc: dict):
+    """The reference's ComputeCandidateDensityStats and ExtractProposalFeatureRows
+    for the candidates of a proxy scene: (density record, feature rows)."""
+    from p2cccd_b200.records import DENSITY_DTYPE, FEATURE_ROW_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_rows_ready"):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        R.ref_proposal_feature_rows.argtypes = [ctypes.c_uint64, i64] + [vp] * 8 + [vp, vp, i64, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._rows_ready = True
+    a = _proxy_args(sc)
+    args = [int(sc["query_id"]), int(sc["n"])] + [_p(a[k]) for k in ("object_id", "patch_id", "slab_id",
+                                                                      "proxy_type", "t0", "t1", "bounds",
+                                                                      "motion_bound")]
+    dens = np.zeros(1, DENSITY_DTYPE)
+    n_rows = ctypes.c_int64(0)
+    if R.ref_proposal_feature_rows(*args, _p(dens), None, 0, ctypes.byref(n_rows)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    rows = np.zeros(max(1, n_rows.value), FEATURE_ROW_DTYPE)
+    R.ref_proposal_feature_rows(*args, _p(dens), _p(rows), n_rows.value, ctypes.byref(n_rows))
+    return dens[0], rows[:n_rows.value]
+
+
+def candidate_density(sc: dict, raw, cand):
+    """Restatement of ComputeCandidateDensityStats (candidate_stats.cpp:128-170,
+    pair count :31-43 by its definition) without timing / backend name."""
+    from p2cccd_b200.records import DENSITY_DTYPE
+
+    n = int(sc["n"])
+    obj, slab = np.asarray(sc["object_id"]), np.asarray(sc["slab_id"])
+    pairs = 0
+    for s_id in np.unique(slab):
+        o = obj[slab == s_id]
+        _, per = np.unique(o, return_counts=True)
+        m = len(o)
+        pairs += m * (m - 1) // 2 - int((per * (per - 1) // 2).sum())
+    def ratio(x, y):
+        return float(x) / float(y) if y else 0.0
+    d = np.zeros(1, DENSITY_DTYPE)[0]
+    d["query_id"], d["proxy_count"] = int(sc["query_id"]), n
+    d["object_count"], d["slab_count"] = len(np.unique(obj)), len(np.unique(slab))
+    d["cross_object_same_slab_pair_count"] = pairs
+    d["raw_hit_count"], d["compact_candidate_count"] = len(raw), len(cand)
+    d["raw_hits_per_proxy"] = ratio(len(raw), n)
+    d["candidates_per_proxy"] = ratio(len(cand), n)
+    d["candidates_per_slab"] = ratio(len(cand), d["slab_count"])
+    d["aabb_overlap_ratio"] = ratio(len(raw), pairs)
+    d["avg_rt_hits_per_candidate"] = ratio(int(cand["rt_hit_count"].astype(np.uint64).sum()) if len(cand) else 0,
+                                           len(cand))
+    return d
+
+
+def _clamp_feature(v: float) -> np.float32:
+    """ClampFeature (proposal_features.cpp:82-88)."""
+    if not math.isfinite(v):
+        return np.float32(0.0)
+    return np.float32(-1.0e6 if v < -1.0e6 else (1.0e6 if 1.0e6 < v else v))
+
+
+def proposal_feature_rows(sc: dict, cand, density):
+    """Restatement of ExtractProposalFeatureRows / FillFeatureRow
+    (proposal_features.cpp:122-205, 236-259): per candidate, the first proxy
+    (in scene order) matching each side's (slab, object, patch, type), then
+    the 32 features and the targets."""
+    from p2cccd_b200.records import FEATURE_ROW_DTYPE
+
+    a = _proxy_args(sc)
+    first = {}
+    for i in range(int(sc["n"])):
+        key = (int(a["slab_id"][i]), int(a["object_id"][i]), int(a["patch_id"][i]), int(a["proxy_type"][i]))
+        first.setdefault(key, i)
+    rows = np.zeros(len(cand), FEATURE_ROW_DTYPE)
+    ext = lambda b, k: max(0.0, b[3 + k] - b[k])
+    vol = lambda b: ext(b, 0) * ext(b, 1) * ext(b, 2)
+    def area(b):
+        x, y, z = ext(b, 0), ext(b, 1), ext(b, 2)
+        return 2.0 * (x * y + y * z + z * x)
+    def ov(l, r, k):
+        return max(0.0, min(l[3 + k], r[3 + k]) - max(l[k], r[k]))
+    for r, c in zip(rows, cand):
+        if not (c["schema_version"] == 1 and c["candidate_id"] and c["query_id"] and c["proxy_type_a"] in (1, 2)
+                and c["proxy_type_b"] in (1, 2) and c["rt_hit_count"]):
+            raise ValueError("invalid CandidateRecord")
+        ia = first.get((int(c["slab_id"]), int(c["object_a_id"]), int(c["patch_a_id"]), int(c["proxy_type_a"])))
+        ib = first.get((int(c["slab_id"]), int(c["object_b_id"]), int(c["patch_b_id"]), int(c["proxy_type_b"])))
+        if ia is None or ib is None:
+            raise ValueError("candidate does not map to proxy primitives")
+        A, B = a["bounds"][ia].tolist(), a["bounds"][ib].tolist()
+        ma, mb = a["motion_bound"][ia].tolist(), a["motion_bound"][ib].tolist()
+        t0, t1 = float(a["t0"][ia]), float(a["t1"][ia])
+        va, vb = vol(A), vol(B)
+        ovol = ov(A, B, 0) * ov(A, B, 1) * ov(A, B, 2)
+        uvol = max(0.0, va + vb - ovol)
+        ca = [0.5 * (A[k] + A[3 + k]) for k in range(3)]
+        cb = [0.5 * (B[k] + B[3 + k]) for k in range(3)]
+        dx, dy, dz = ca[0] - cb[0], ca[1] - cb[1], ca[2] - cb[2]
+        mbc = [float(x) for x in c["motion_bound"]]
+        f = [t0, t1, max(0.0, t1 - t0), float(c["rt_hit_count"]), float(c["proxy_type_a"]),
+             float(c["proxy_type_b"]), *mbc, ext(A, 0), ext(A, 1), ext(A, 2), ext(B, 0), ext(B, 1), ext(B, 2),
+             va, vb, ovol, ovol / uvol if uvol > 0.0 else 0.0, math.sqrt(dx * dx + dy * dy + dz * dz), area(A),
+             area(B), ma[3], mb[3], ma[0], mb[0], ma[1], mb[1], float(density["candidates_per_proxy"]),
+             float(density["aabb_overlap_ratio"]), float(density["avg_rt_hits_per_candidate"])]
+        feats = np.array([_clamp_feature(v) for v in f], np.float32)
+        r["schema_version"], r["query_id"], r["candidate_id"] = 1, c["query_id"], c["candidate_id"]
+        for k in ("slab_id", "object_a_id", "patch_a_id", "object_b_id", "patch_b_id"):
+            r[k] = c[k]
+        r["features"] = feats
+        center = 0.5 * (t0 + t1)
+        center = 0.0 if center < 0.0 else (math.nextafter(1.0, 0.0) if math.nextafter(1.0, 0.0) < center else center)
+        r["interval_targets"][int(center * 8)] = 1.0
+        r["family_targets"][0] = r["family_targets"][1] = 1.0
+        r["priority_target"] = _clamp_feature(0.5 * float(c["rt_hit_count"]) +
+                                              0.5 * float(density["candidates_per_proxy"]))
+        r["cost_target"] = _clamp_feature(1.0 + mbc[3])
+        r["uncertainty_target"] = _clamp_feature(1.0 - min(1.0, float(feats[19])))
+        r["target_mask"] = 31
+    return rows

@@ -1,12 +1,16 @@
-// ref_proxy.cpp — C ABI over the reference's proxy-scene build and candidate
-// generation (rt_candidate/proxy_scene.cpp: BuildProxyScene,
-// ValidateProxyScene; rt_candidate/candidate_buffer.cpp:
-// GenerateRawCandidatesCpu, CompactRawCandidates), compiled unchanged into
+// ref_proxy.cpp — C ABI over the reference's proxy-scene build, candidate
+// generation and proposal feature rows (rt_candidate/proxy_scene.cpp:
+// BuildProxyScene, ValidateProxyScene; rt_candidate/candidate_buffer.cpp:
+// GenerateRawCandidatesCpu, CompactRawCandidates; rt_candidate/
+// candidate_stats.cpp: ComputeCandidateDensityStats; proposal/
+// proposal_features.cpp: ExtractProposalFeatureRows), compiled unchanged into
 // oracle/_ref/libp2c_ref.so.
 //
 // TEST INFRASTRUCTURE ONLY: tests pin the device proxy candidates and the
 // restated checker to it; the product never loads it.
+#include "proposal/proposal_features.h"
 #include "rt_candidate/candidate_buffer.h"
+#include "rt_candidate/candidate_stats.h"
 #include "rt_candidate/proxy_scene.h"
 
 #include <algorithm>
@@ -25,23 +29,19 @@ static_assert(offsetof(p2cccd::CandidateRecord, proxy_type_a) == offsetof(p2c_ca
 static_assert(offsetof(p2cccd::CandidateRecord, rt_hit_count) == offsetof(p2c_candidate_record, rt_hit_count));
 static_assert(offsetof(p2cccd::CandidateRecord, flags) == offsetof(p2c_candidate_record, flags));
 static_assert(offsetof(p2cccd::RawCandidateHit, motion_bound) == offsetof(p2c_raw_candidate_hit, motion_bound));
+static_assert(sizeof(p2cccd::ProposalFeatureRow) == sizeof(p2c_proposal_feature_row));
+static_assert(offsetof(p2cccd::ProposalFeatureRow, features) == offsetof(p2c_proposal_feature_row, features));
+static_assert(offsetof(p2cccd::ProposalFeatureRow, target_mask) == offsetof(p2c_proposal_feature_row, target_mask));
 
 namespace {
 thread_local std::string g_proxy_error;
 }
 
-extern "C" {
+static p2cccd::ProxyScene make_scene(uint64_t query_id, int64_t n, const uint32_t* object_id,
+                                     const uint32_t* patch_id, const uint32_t* slab_id, const uint8_t* proxy_type,
+                                     const double* t0, const double* t1, const double* bounds,
+                                     const double* motion_bound) {
 
-const char* ref_proxy_last_error(void) { return g_proxy_error.c_str(); }
-
-// Proxy arrays as p2c_proxy_scene lays them out (host memory).  Returns 0 and
-// the counts, or 1 with the reference's error message.  Outputs (may be NULL
-// for a sizing call) receive min(count, cap) records.
-int ref_proxy_candidates(uint64_t query_id, int64_t n, const uint32_t* object_id, const uint32_t* patch_id,
-                         const uint32_t* slab_id, const uint8_t* proxy_type, const double* t0, const double* t1,
-                         const double* bounds, const double* motion_bound, p2c_raw_candidate_hit* raw_out,
-                         int64_t raw_cap, p2c_candidate_record* cand_out, int64_t cand_cap, int64_t* n_raw,
-                         int64_t* n_cand) {
   p2cccd::ProxyScene scene;
   scene.query_id = query_id;
   scene.primitives.resize(static_cast<std::size_t>(n));
@@ -63,6 +63,23 @@ int ref_proxy_candidates(uint64_t query_id, int64_t n, const uint32_t* object_id
     p.motion_bound.radial_motion_bound = motion_bound[4 * i + 2];
     p.motion_bound.conservative_radius = motion_bound[4 * i + 3];
   }
+  return scene;
+}
+
+extern "C" {
+
+const char* ref_proxy_last_error(void) { return g_proxy_error.c_str(); }
+
+// Proxy arrays as p2c_proxy_scene lays them out (host memory).  Returns 0 and
+// the counts, or 1 with the reference's error message.  Outputs (may be NULL
+// for a sizing call) receive min(count, cap) records.
+int ref_proxy_candidates(uint64_t query_id, int64_t n, const uint32_t* object_id, const uint32_t* patch_id,
+                         const uint32_t* slab_id, const uint8_t* proxy_type, const double* t0, const double* t1,
+                         const double* bounds, const double* motion_bound, p2c_raw_candidate_hit* raw_out,
+                         int64_t raw_cap, p2c_candidate_record* cand_out, int64_t cand_cap, int64_t* n_raw,
+                         int64_t* n_cand) {
+  p2cccd::ProxyScene scene =
+      make_scene(query_id, n, object_id, patch_id, slab_id, proxy_type, t0, t1, bounds, motion_bound);
   p2cccd::RawCandidateBuffer raw;
   p2cccd::Status st = p2cccd::GenerateRawCandidatesCpu(scene, query_id, &raw);
   if (!st.ok) {
@@ -181,6 +198,46 @@ int ref_build_proxy_scene(uint64_t query_id, int64_t n_objects, const uint32_t* 
     o_detail[8 * i + 6] = p.motion_bound.center_rotation_bound;
     o_detail[8 * i + 7] = p.motion_bound.surface_rotation_bound;
     o_capsule_radius[i] = p.capsule.radius;
+  }
+  return 0;
+}
+
+// The reference's density stats (ComputeCandidateDensityStats, zero timing)
+// and ExtractProposalFeatureRows for the candidates GenerateRawCandidatesCpu
+// + CompactRawCandidates give on the same proxy arrays.  rows may be NULL (a
+// sizing call); *n_rows receives the candidate count.
+int ref_proposal_feature_rows(uint64_t query_id, int64_t n, const uint32_t* object_id, const uint32_t* patch_id,
+                              const uint32_t* slab_id, const uint8_t* proxy_type, const double* t0,
+                              const double* t1, const double* bounds, const double* motion_bound,
+                              p2c_candidate_density* density, p2c_proposal_feature_row* rows, int64_t rows_cap,
+                              int64_t* n_rows) {
+  p2cccd::ProxyScene scene =
+      make_scene(query_id, n, object_id, patch_id, slab_id, proxy_type, t0, t1, bounds, motion_bound);
+  p2cccd::CandidateGenerationResult gen;
+  gen.backend_name = "cpu_reference";
+  p2cccd::Status st = p2cccd::GenerateRawCandidatesCpu(scene, query_id, &gen.raw_buffer);
+  if (st.ok) st = p2cccd::CompactRawCandidates(scene, gen.raw_buffer, &gen.candidates);
+  if (st.ok)
+    st = p2cccd::ComputeCandidateDensityStats(scene, gen.raw_buffer, gen.candidates, gen.timing, gen.backend_name,
+                                              &gen.density);
+  std::vector<p2cccd::ProposalFeatureRow> out;
+  if (st.ok) st = p2cccd::ExtractProposalFeatureRows(scene, gen, &out);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  const p2cccd::CandidateDensityStats& d = gen.density;
+  *density = p2c_candidate_density{d.query_id, d.proxy_count, d.object_count, d.slab_count,
+                                   d.cross_object_same_slab_pair_count, d.raw_hit_count, d.compact_candidate_count,
+                                   d.raw_hits_per_proxy, d.candidates_per_proxy, d.candidates_per_slab,
+                                   d.aabb_overlap_ratio, d.avg_rt_hits_per_candidate};
+  *n_rows = static_cast<int64_t>(out.size());
+  if (rows != nullptr) {
+    const int64_t m = std::min<int64_t>(*n_rows, rows_cap);
+    for (int64_t i = 0; i < m; ++i) {
+      std::memcpy(rows + i, &out[static_cast<std::size_t>(i)], sizeof(p2c_proposal_feature_row));
+      rows[i].pad0 = rows[i].pad1 = 0;  // padding bytes of the reference struct are indeterminate
+    }
   }
   return 0;
 }

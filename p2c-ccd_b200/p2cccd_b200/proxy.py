@@ -15,7 +15,7 @@ import torch
 
 from . import _lib
 from .certify import _stream_ptr
-from .records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
+from .records import CANDIDATE_RECORD_DTYPE, DENSITY_DTYPE, FEATURE_ROW_DTYPE, RAW_HIT_DTYPE
 
 ERR_INVALID_PROXY, ERR_MOTION_BOUND, ERR_OVERFLOW, ERR_ID_BITS = 1, 2, 4, 8
 
@@ -116,6 +116,39 @@ class ProxyCandidates:
                 return raw, cand
             self._alloc(int(n_raw * 1.25) + 1024)
         raise _lib.P2CError("raw candidate buffer kept overflowing")
+
+    def feature_rows_async(self) -> tuple[torch.Tensor, torch.Tensor, torch.Tensor]:
+        """Enqueue the density stats and proposal feature rows of the last
+        run's candidates (p2c_proposal_feature_rows, no host sync).  Returns
+        device tensors (density 96 B, rows cap x 256 B, error word); rows
+        [0, candidate count) are valid."""
+        d = self.device
+        if getattr(self, "_rows_cap", -1) != self.cap:
+            self.rows = torch.empty((max(self.cap, 1), 256), dtype=torch.uint8, device=d)
+            self.density = torch.empty(96, dtype=torch.uint8, device=d)
+            self.feature_error = torch.zeros(1, dtype=torch.int64, device=d)
+            self.feature_ws = torch.empty(int(self.lib.p2c_proposal_feature_rows_workspace_bytes(self.n)),
+                                          dtype=torch.uint8, device=d)
+            self._rows_cap = self.cap
+        _lib.check(self.lib.p2c_proposal_feature_rows(
+            ctypes.byref(self._struct), self.cand.data_ptr(), self.cap, self.counts.data_ptr(),
+            self.density.data_ptr(), self.rows.data_ptr(), self.feature_error.data_ptr(), self.feature_ws.data_ptr(),
+            self.feature_ws.numel(), _stream_ptr(d)))
+        return self.density, self.rows, self.feature_error
+
+    def feature_rows(self) -> tuple[np.void, np.ndarray]:
+        """Density stats (a DENSITY_DTYPE record) and proposal feature rows
+        (FEATURE_ROW_DTYPE) of the last checked run's candidates; ValueError
+        on an invalid candidate or one that maps to no proxy."""
+        density, rows, err = self.feature_rows_async()
+        n_cand = int(self.counts[1].item())
+        e = int(err.item())
+        if e & 1:
+            raise ValueError("a CandidateRecord fails validation")
+        if e & 2:
+            raise ValueError("candidate does not map to proxy primitives")
+        dens = density.cpu().numpy().view(DENSITY_DTYPE)[0]
+        return dens, rows[:n_cand].cpu().numpy().view(FEATURE_ROW_DTYPE).reshape(-1)
 
 
 def proxy_candidates(scene: dict, device: str | torch.device = "cuda") -> tuple[np.ndarray, np.ndarray]:

@@ -128,3 +128,25 @@ def unpack_positions(rec: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     p0 = np.stack([rec[names[2 + k]]["position_t0"] for k in range(4)], axis=1)
     p1 = np.stack([rec[names[2 + k]]["position_t1"] for k in range(4)], axis=1)
     return p0, p1
+
+
+# CandidateDensityStats without timing / backend name (p2c_candidate_density, 96 bytes)
+DENSITY_DTYPE = np.dtype({
+    "names": ["query_id", "proxy_count", "object_count", "slab_count", "cross_object_same_slab_pair_count",
+              "raw_hit_count", "compact_candidate_count", "raw_hits_per_proxy", "candidates_per_proxy",
+              "candidates_per_slab", "aabb_overlap_ratio", "avg_rt_hits_per_candidate"],
+    "formats": ["<u8"] * 7 + ["<f8"] * 5,
+    "offsets": [8 * k for k in range(12)],
+    "itemsize": 96,
+})
+
+# ProposalFeatureRow (proposal/proposal_features.h:27-43), 256 bytes
+FEATURE_ROW_DTYPE = np.dtype({
+    "names": ["schema_version", "query_id", "candidate_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id",
+              "patch_b_id", "features", "interval_targets", "family_targets", "priority_target", "cost_target",
+              "uncertainty_target", "target_mask"],
+    "formats": ["<u4", "<u8", "<u8", "<u4", "<u4", "<u4", "<u4", "<u4", ("<f4", (32,)), ("<f4", (8,)),
+                ("<f4", (8,)), "<f4", "<f4", "<f4", "<u4"],
+    "offsets": [0, 8, 16, 24, 28, 32, 36, 40, 44, 172, 204, 236, 240, 244, 248],
+    "itemsize": 256,
+})

@@ -241,3 +241,60 @@ def test_sweep_paths_agree(cuda_device, oracle_mod, mode):
         assert table == (mode == "table")
         assert np.array_equal(raw.view(np.uint8), ref_raw.view(np.uint8))
         assert np.array_equal(cand.view(np.uint8), ref_cand.view(np.uint8))
+
+
+@pytest.mark.parametrize("seed,dups,hint", [(1, 0.0, True), (2, 0.5, True), (4, 0.4, False), (5, 0.0, False)])
+def test_device_feature_rows_match_reference(cuda_device, oracle_mod, seed, dups, hint):
+    """p2c_proposal_feature_rows: density stats and every 256-byte row byte for
+    byte with the reference's ComputeCandidateDensityStats +
+    ExtractProposalFeatureRows, with and without the id width hints."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=6, patches_per_object=40, n_slabs=4, seed=seed, duplicates=dups)
+    d_ref, rows_ref = oracle_mod.ref_proposal_feature_rows(sc)
+    pc = ProxyCandidates(sc if hint else dict(sc, id_bits=(0, 0, 0)), cuda_device)
+    pc.run_checked()
+    dens, rows = pc.feature_rows()
+    assert dens.tobytes() == d_ref.tobytes()
+    assert len(rows) == len(rows_ref) > 0
+    assert np.array_equal(rows.view(np.uint8), rows_ref.view(np.uint8))
+
+
+def test_device_feature_rows_of_a_built_scene(cuda_device, oracle_mod):
+    """Build, candidates and feature rows all on the device, against the
+    reference's build + generation + ExtractProposalFeatureRows."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates, ProxySceneBuild
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    inp = scenes.proxy_build_input(n_objects=10, patches_per_object=40, n_segments=2, slabs=3, seed=8)
+    ref_scene = oracle_mod.ref_build_proxy_scene(inp)
+    d_ref, rows_ref = oracle_mod.ref_proposal_feature_rows(ref_scene)
+    pc = ProxyCandidates(ProxySceneBuild(inp, cuda_device).run_checked(), cuda_device)
+    pc.run_checked()
+    dens, rows = pc.feature_rows()
+    assert dens.tobytes() == d_ref.tobytes()
+    assert np.array_equal(rows.view(np.uint8), rows_ref.view(np.uint8))
+
+
+def test_device_feature_rows_flag_bad_candidates(cuda_device):
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    sc = scenes.proxy_scene(n_objects=4, patches_per_object=20, n_slabs=2, seed=3)
+    pc = ProxyCandidates(sc, cuda_device)
+    pc.run_checked()
+    pc.cand[0, 32:36] = 255  # patch_a_id of candidate 0: no proxy has it
+    with pytest.raises(ValueError, match="map to proxy"):
+        pc.feature_rows()
+    pc.run_checked()
+    pc.cand[1, 0] = 7  # schema_version of candidate 1
+    with pytest.raises(ValueError, match="validation"):
+        pc.feature_rows()
+    pc.run_checked()
+    dens, rows = pc.feature_rows()
+    assert len(rows) == int(dens["compact_candidate_count"]) > 0

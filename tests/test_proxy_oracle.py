@@ -245,3 +245,40 @@ def test_build_rejections_match_reference(oracle_mod):
         assert _reject_message(oracle_mod.build_proxy_scene, inp) == ref_msg, label
         if not torch.cuda.is_available():  # the check never reaches the device; keep it off real devices anyway
             assert _library_host_check(inp) == ref_msg, label
+
+
+# ---- proposal feature rows ---------------------------------------------------
+
+@pytest.mark.parametrize("seed,dups,slabs", [(1, 0.0, 3), (2, 0.5, 3), (3, 0.2, 1), (4, 0.4, 6)])
+def test_feature_rows_restatement_matches_reference(oracle_mod, seed, dups, slabs):
+    """Density stats (ComputeCandidateDensityStats) and feature rows
+    (ExtractProposalFeatureRows) restated, byte for byte with the reference;
+    repeated patches exercise the first-proxy-in-scene-order lookup."""
+    from p2cccd_b200 import scenes
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=5, patches_per_object=30, n_slabs=slabs, seed=seed, duplicates=dups)
+    d_ref, rows_ref = oracle_mod.ref_proposal_feature_rows(sc)
+    raw, cand = oracle_mod.proxy_candidates(sc)
+    d = oracle_mod.candidate_density(sc, raw, cand)
+    rows = oracle_mod.proposal_feature_rows(sc, cand, d)
+    assert len(rows_ref) == len(cand) > 0
+    assert d.tobytes() == d_ref.tobytes()
+    assert np.array_equal(rows.view(np.uint8), rows_ref.view(np.uint8))
+
+
+def test_feature_rows_known_properties(oracle_mod):
+    """test_proposal_features.cpp:101-118 on the overlapping scene: one row per
+    candidate, schema 1, the scene's query id, a one-hot interval target, both
+    family targets set, a non-zero target mask, finite features."""
+    sc = oracle_mod.build_proxy_scene(overlapping_build_input())
+    raw, cand = oracle_mod.proxy_candidates(sc)
+    rows = oracle_mod.proposal_feature_rows(sc, cand, oracle_mod.candidate_density(sc, raw, cand))
+    assert len(rows) == len(cand) == 2
+    assert all(rows["schema_version"] == 1) and all(rows["query_id"] == 42)
+    assert np.array_equal(rows["interval_targets"].sum(1), np.ones(2, np.float32))
+    assert np.all(rows["family_targets"][:, :2] == 1.0) and np.all(rows["target_mask"] != 0)
+    assert np.all(np.isfinite(rows["features"]))
+    # the two slabs of [0, 1]: interval bins 2 and 6 (centres 0.25 and 0.75)
+    assert sorted(np.argmax(rows["interval_targets"], 1).tolist()) == [2, 6]
