@@ -629,6 +629,20 @@ int p2c_proposal_feature_rows(const p2c_proxy_scene* scene, const p2c_candidate_
                               p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* workspace_dev,
                               size_t workspace_bytes, void* stream);
 
+/* BuildProposalFeatureRowsFromRuntimeCandidates (proposal/
+ * proposal_policy.cpp:568-592, rows by :184-226): rows from n candidate
+ * records alone, the density ratios of primitive_count / raw_hit_count /
+ * compact_candidate_count (MakeRuntimeDensityDerivedStats :44-58) and each
+ * query's conservative family mask (n_masks query ids in ascending order with
+ * their masks; a query absent or with mask 0 gets both families).  Bit 1 of
+ * *error_word_dev: a candidate fails ValidateCandidateRecord (its row is
+ * zero).  primitive_count 0 fails the call with the reference's message.  No
+ * host sync. */
+int p2c_runtime_feature_rows(const p2c_candidate_record* candidates_dev, int64_t n, uint64_t primitive_count,
+                             uint64_t raw_hit_count, uint64_t compact_candidate_count,
+                             const uint64_t* mask_query_ids_dev, const uint32_t* masks_dev, int64_t n_masks,
+                             p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

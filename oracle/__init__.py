@@ -796,3 +796,70 @@ def proposal_feature_rows(sc: dict, cand, density):
         r["uncertainty_target"] = _clamp_feature(1.0 - min(1.0, float(feats[19])))
         r["target_mask"] = 31
     return rows
+
+
+
+def ref_runtime_feature_rows(cand, primitive_count: int, raw_hit_count: int, compact_candidate_count: int,
+                             masks: dict | None = None):
+    """The reference's BuildProposalFeatureRowsFromRuntimeCandidates (with the
+    binding's MakeRuntimeDensityStats) on CANDIDATE_RECORD_DTYPE records."""
+    from p2cccd_b200.records import FEATURE_ROW_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_rt_rows_ready"):
+        vp, i64, u64 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_uint64
+        R.ref_runtime_feature_rows.argtypes = [vp, i64, u64, u64, u64, vp, vp, i64, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._rt_rows_ready = True
+    cand = np.ascontiguousarray(cand)
+    keys = np.array(sorted((masks or {}).keys()), np.uint64)
+    vals = np.array([masks[int(k)] for k in keys], np.uint32)
+    rows = np.zeros(max(1, len(cand)), FEATURE_ROW_DTYPE)
+    if R.ref_runtime_feature_rows(_p(cand), len(cand), primitive_count, raw_hit_count, compact_candidate_count,
+                                  _p(keys) if len(keys) else None, _p(vals) if len(vals) else None, len(keys),
+                                  _p(rows)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    return rows[:len(cand)]
+
+
+def runtime_feature_rows(cand, primitive_count: int, raw_hit_count: int, compact_candidate_count: int,
+                         masks: dict | None = None):
+    """Restatement of BuildRuntimeFeatureRowFromDerived (proposal_policy.cpp:
+    184-226) with MakeRuntimeDensityDerivedStats (:44-58)."""
+    from p2cccd_b200.records import FEATURE_ROW_DTYPE
+
+    if primitive_count == 0:
+        raise ValueError("CandidateDensityStats.proxy_count must be non-zero")
+    def ratio(x, y):
+        return float(x) / float(y) if y else 0.0
+    cpp = ratio(compact_candidate_count, primitive_count)
+    aor = ratio(raw_hit_count, primitive_count // 2 if primitive_count >= 2 else 1)
+    avg = ratio(raw_hit_count, compact_candidate_count)
+    rows = np.zeros(len(cand), FEATURE_ROW_DTYPE)
+    for r, c in zip(rows, cand):
+        if not (c["schema_version"] == 1 and c["candidate_id"] and c["query_id"] and c["proxy_type_a"] in (1, 2)
+                and c["proxy_type_b"] in (1, 2) and c["rt_hit_count"]
+                and all(math.isfinite(float(x)) and x >= 0 for x in c["motion_bound"])):
+            raise ValueError("invalid CandidateRecord")
+        mask = (masks or {}).get(int(c["query_id"]), 0) or 3
+        for k in ("query_id", "candidate_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id", "patch_b_id"):
+            r[k] = c[k]
+        r["schema_version"] = 1
+        rt = float(c["rt_hit_count"])
+        f = np.zeros(32, np.float32)
+        f[1] = f[2] = 1.0
+        f[3], f[4], f[5] = _clamp_feature(rt), _clamp_feature(float(c["proxy_type_a"])), \
+            _clamp_feature(float(c["proxy_type_b"]))
+        for k in range(4):
+            f[6 + k] = _clamp_feature(float(c["motion_bound"][k]))
+        f[19] = _clamp_feature(min(1.0, aor))
+        f[29], f[30], f[31] = _clamp_feature(cpp), _clamp_feature(aor), _clamp_feature(avg)
+        r["features"] = f
+        r["interval_targets"][0] = 1.0
+        r["family_targets"][0] = 1.0 if mask & 1 else 0.0
+        r["family_targets"][1] = 1.0 if mask & 2 else 0.0
+        r["priority_target"] = _clamp_feature(min(1.0, 0.5 * rt + 0.5 * cpp))
+        r["cost_target"] = _clamp_feature(max(1.0, 1.0 + rt))
+        r["uncertainty_target"] = 0.25 if mask == 3 else 0.0
+        r["target_mask"] = 31
+    return rows

@@ -9,6 +9,7 @@
 // TEST INFRASTRUCTURE ONLY: tests pin the device proxy candidates and the
 // restated checker to it; the product never loads it.
 #include "proposal/proposal_features.h"
+#include "proposal/proposal_policy.h"
 #include "rt_candidate/candidate_buffer.h"
 #include "rt_candidate/candidate_stats.h"
 #include "rt_candidate/proxy_scene.h"
@@ -18,6 +19,7 @@
 #include <cstdint>
 #include <cstring>
 #include <string>
+#include <unordered_map>
 #include <vector>
 
 #include "../include/p2c_b200.h"
@@ -238,6 +240,34 @@ int ref_proposal_feature_rows(uint64_t query_id, int64_t n, const uint32_t* obje
       std::memcpy(rows + i, &out[static_cast<std::size_t>(i)], sizeof(p2c_proposal_feature_row));
       rows[i].pad0 = rows[i].pad1 = 0;  // padding bytes of the reference struct are indeterminate
     }
+  }
+  return 0;
+}
+
+// BuildProposalFeatureRowsFromRuntimeCandidates with the density of
+// MakeRuntimeDensityStats (the binding's, py_module.cpp:508-531) and a
+// query id -> family mask map.
+int ref_runtime_feature_rows(const p2c_candidate_record* cands, int64_t n, uint64_t primitive_count,
+                             uint64_t raw_hit_count, uint64_t compact_candidate_count, const uint64_t* mask_query_ids,
+                             const uint32_t* masks, int64_t n_masks, p2c_proposal_feature_row* rows) {
+  std::vector<p2cccd::CandidateRecord> cand(static_cast<std::size_t>(n));
+  for (int64_t i = 0; i < n; ++i) std::memcpy(&cand[static_cast<std::size_t>(i)], cands + i, sizeof(p2c_candidate_record));
+  p2cccd::CandidateDensityStats density;
+  density.query_id = cand.empty() ? 1U : cand.front().query_id;
+  density.proxy_count = primitive_count;
+  density.raw_hit_count = raw_hit_count;
+  density.compact_candidate_count = compact_candidate_count;
+  std::unordered_map<std::uint64_t, std::uint32_t> mask_map;
+  for (int64_t i = 0; i < n_masks; ++i) mask_map[mask_query_ids[i]] = masks[i];
+  std::vector<p2cccd::ProposalFeatureRow> out;
+  const p2cccd::Status st = p2cccd::BuildProposalFeatureRowsFromRuntimeCandidates(cand, density, mask_map, &out);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  for (int64_t i = 0; i < n; ++i) {
+    std::memcpy(rows + i, &out[static_cast<std::size_t>(i)], sizeof(p2c_proposal_feature_row));
+    rows[i].pad0 = rows[i].pad1 = 0;
   }
   return 0;
 }

@@ -13,6 +13,8 @@
 //      and every candidate side finds its proxy by binary search;
 //   3. one thread per candidate forms the row with the reference's double
 //      arithmetic (bit-identical with --fmad=false) and float clamps.
+// p2c_runtime_feature_rows is the runtime form without a scene
+// (BuildProposalFeatureRowsFromRuntimeCandidates, proposal_policy.cpp:568-592).
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
@@ -282,10 +284,101 @@ __global__ void rows_kernel(p2c_proxy_scene sc, FeatureLayout L, const p2c_candi
   rows[c] = row;
 }
 
+// BuildRuntimeFeatureRowFromDerived (proposal/proposal_policy.cpp:184-226):
+// a row from the candidate alone, the three density ratios and the query's
+// conservative family mask (sorted query ids with their masks; absent or 0:
+// both families).
+struct RuntimeDerived {
+  double candidates_per_proxy, aabb_overlap_ratio, avg_hits;
+};
+
+__global__ void runtime_rows_kernel(const p2c_candidate_record* cand, long long n, RuntimeDerived dv,
+                                    const unsigned long long* mask_query_ids, const unsigned* masks, long long n_masks,
+                                    p2c_proposal_feature_row* rows, unsigned long long* err) {
+  const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= n) return;
+  const p2c_candidate_record r = cand[c];
+  p2c_proposal_feature_row row{};
+  bool ok = r.schema_version == 1u && r.candidate_id != 0 && r.query_id != 0 &&
+            (r.proxy_type_a == 1 || r.proxy_type_a == 2) && (r.proxy_type_b == 1 || r.proxy_type_b == 2) &&
+            r.rt_hit_count != 0;
+  for (int k = 0; k < 4; ++k) ok = ok && isfinite(r.motion_bound[k]) && !(r.motion_bound[k] < 0.0f);
+  if (!ok) {
+    atomicOr(err, 1ull);
+    rows[c] = row;
+    return;
+  }
+  unsigned mask = 3u;  // kFeatureFamilyPointTriangle | kFeatureFamilyEdgeEdge
+  long long lo = 0, hi = n_masks;
+  while (lo < hi) {
+    const long long m = (lo + hi) >> 1;
+    if (mask_query_ids[m] < r.query_id) lo = m + 1;
+    else hi = m;
+  }
+  if (lo < n_masks && mask_query_ids[lo] == r.query_id && masks[lo] != 0u) mask = masks[lo];
+  row.schema_version = 1u;
+  row.query_id = r.query_id;
+  row.candidate_id = r.candidate_id;
+  row.slab_id = r.slab_id;
+  row.object_a_id = r.object_a_id;
+  row.patch_a_id = r.patch_a_id;
+  row.object_b_id = r.object_b_id;
+  row.patch_b_id = r.patch_b_id;
+  float* f = row.features;
+  f[1] = 1.0f;
+  f[2] = 1.0f;
+  f[3] = clamp_feature((double)r.rt_hit_count);
+  f[4] = clamp_feature((double)r.proxy_type_a);
+  f[5] = clamp_feature((double)r.proxy_type_b);
+  for (int k = 0; k < 4; ++k) f[6 + k] = clamp_feature((double)r.motion_bound[k]);
+  f[19] = clamp_feature(dv.aabb_overlap_ratio < 1.0 ? dv.aabb_overlap_ratio : 1.0);
+  f[29] = clamp_feature(dv.candidates_per_proxy);
+  f[30] = clamp_feature(dv.aabb_overlap_ratio);
+  f[31] = clamp_feature(dv.avg_hits);
+  row.interval_targets[0] = 1.0f;
+  row.family_targets[0] = (mask & 1u) ? 1.0f : 0.0f;
+  row.family_targets[1] = (mask & 2u) ? 1.0f : 0.0f;
+  const double pr = 0.5 * (double)r.rt_hit_count + 0.5 * dv.candidates_per_proxy;
+  row.priority_target = clamp_feature(pr < 1.0 ? pr : 1.0);
+  const double cost = 1.0 + (double)r.rt_hit_count;
+  row.cost_target = clamp_feature(1.0 < cost ? cost : 1.0);
+  row.uncertainty_target = mask == 3u ? 0.25f : 0.0f;
+  row.target_mask = 31u;
+  rows[c] = row;
+}
+
 }  // namespace
 }  // namespace p2c
 
 extern "C" {
+
+int p2c_runtime_feature_rows(const p2c_candidate_record* candidates_dev, int64_t n, uint64_t primitive_count,
+                             uint64_t raw_hit_count, uint64_t compact_candidate_count,
+                             const uint64_t* mask_query_ids_dev, const uint32_t* masks_dev, int64_t n_masks,
+                             p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* stream) {
+  using namespace p2c;
+  if (primitive_count == 0) return fail(P2C_ERR_INVALID, "CandidateDensityStats.proxy_count must be non-zero");
+  if (n < 0 || n >= (1ll << 31) || n_masks < 0) return fail(P2C_ERR_INVALID, "row or mask count out of range");
+  if (error_word_dev == nullptr || (n > 0 && (candidates_dev == nullptr || rows_dev == nullptr)) ||
+      (n_masks > 0 && (mask_query_ids_dev == nullptr || masks_dev == nullptr)))
+    return fail(P2C_ERR_INVALID, "candidate, row, mask or error word pointer is null");
+  // MakeRuntimeDensityDerivedStats (proposal_policy.cpp:44-58)
+  auto ratio = [](uint64_t num, uint64_t den) { return den == 0 ? 0.0 : (double)num / (double)den; };
+  RuntimeDerived dv;
+  dv.candidates_per_proxy = ratio(compact_candidate_count, primitive_count);
+  dv.aabb_overlap_ratio = ratio(raw_hit_count, primitive_count >= 2 ? primitive_count / 2 : 1);
+  dv.avg_hits = ratio(raw_hit_count, compact_candidate_count);
+  cudaStream_t s = as_stream(stream);
+  P2C_CUDA(cudaMemsetAsync(error_word_dev, 0, sizeof(uint64_t), s));
+  if (n > 0)
+    runtime_rows_kernel<<<grid_for(n), kThreads, 0, s>>>(candidates_dev, n, dv,
+                                                         reinterpret_cast<const unsigned long long*>(mask_query_ids_dev),
+                                                         masks_dev, n_masks, rows_dev,
+                                                         reinterpret_cast<unsigned long long*>(error_word_dev));
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
 
 size_t p2c_proposal_feature_rows_workspace_bytes(int64_t n_proxies) {
   if (n_proxies < 0) return 0;

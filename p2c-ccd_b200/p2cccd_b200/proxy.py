@@ -278,3 +278,32 @@ class ProxySceneBuild:
             a = v.cpu().numpy()
             sc[k] = a.view(np.uint32) if a.dtype == np.int32 else a
         return sc
+
+
+def runtime_feature_rows(candidates, primitive_count: int, raw_hit_count: int, compact_candidate_count: int,
+                         masks: dict | None = None, device: str | torch.device = "cuda") -> np.ndarray:
+    """Proposal feature rows from candidate records alone (the runtime form,
+    p2c_runtime_feature_rows).  ``candidates``: CANDIDATE_RECORD_DTYPE records
+    or a (n, 80) uint8 device tensor; ``masks``: query id -> conservative
+    family mask.  Returns FEATURE_ROW_DTYPE records; ValueError on an invalid
+    candidate or a zero primitive count."""
+    lib = _lib.load()
+    d = torch.device(device)
+    if torch.is_tensor(candidates):
+        cand = candidates.to(d).contiguous()
+    else:
+        a = np.ascontiguousarray(candidates).view(np.uint8).reshape(-1, 80)
+        cand = torch.from_numpy(a.copy()).to(d)
+    n = cand.shape[0]
+    keys = sorted(int(k) for k in (masks or {}))
+    mq = torch.tensor(np.array(keys, np.uint64).view(np.int64), device=d) if keys else None
+    mv = torch.tensor(np.array([int(masks[k]) for k in keys], np.uint32).view(np.int32), device=d) if keys else None
+    rows = torch.empty((max(n, 1), 256), dtype=torch.uint8, device=d)
+    err = torch.zeros(1, dtype=torch.int64, device=d)
+    _lib.check(lib.p2c_runtime_feature_rows(cand.data_ptr() if n else None, n, int(primitive_count), int(raw_hit_count),
+                                            int(compact_candidate_count), mq.data_ptr() if keys else None,
+                                            mv.data_ptr() if keys else None, len(keys), rows.data_ptr(), err.data_ptr(),
+                                            _stream_ptr(d)))
+    if int(err.item()) & 1:
+        raise ValueError("a CandidateRecord fails validation")
+    return rows[:n].cpu().numpy().view(FEATURE_ROW_DTYPE).reshape(-1)

@@ -1134,3 +1134,98 @@ def build_proxy_scene(input) -> ProxyScene:  # py_module.cpp:1868, proxy_scene.c
             c.motion_bound = m
         scene.primitives.append(p)
     return scene
+
+
+# ---------------------------------------------------------------------------
+# proposal feature rows (proposal/proposal_features.h:27-43, py_module.cpp:639-753, 1895-1908)
+
+
+class ProposalFeatureRow(_Struct):
+    _fields = (("schema_version", 1), ("query_id", 0), ("candidate_id", 0), ("slab_id", 0), ("object_a_id", 0),
+               ("patch_a_id", 0), ("object_b_id", 0), ("patch_b_id", 0), ("features", lambda: [0.0] * 32),
+               ("interval_targets", lambda: [0.0] * 8), ("family_targets", lambda: [0.0] * 8),
+               ("priority_target", 0.0), ("cost_target", 0.0), ("uncertainty_target", 0.0), ("target_mask", 0))
+
+
+def _candidate_array(candidates) -> np.ndarray:
+    """CandidateRecord objects (or records) as CANDIDATE_RECORD_DTYPE records."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE
+
+    if isinstance(candidates, np.ndarray):
+        return np.ascontiguousarray(candidates, dtype=CANDIDATE_RECORD_DTYPE)
+    out = np.zeros(len(candidates), CANDIDATE_RECORD_DTYPE)
+    for r, c in zip(out, candidates):
+        for k in ("schema_version", "candidate_id", "query_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id",
+                  "patch_b_id", "rt_hit_count", "proxy_features_offset", "flags"):
+            r[k] = int(getattr(c, k))
+        r["proxy_type_a"], r["proxy_type_b"] = int(c.proxy_type_a), int(c.proxy_type_b)
+        mb = list(c.motion_bound)
+        if len(mb) != 4:
+            raise ValueError("CandidateRecord.motion_bound must have length 4")
+        r["motion_bound"] = mb
+    return out
+
+
+def _row_objects(rows: np.ndarray) -> list:
+    out = []
+    for r in rows:
+        o = ProposalFeatureRow()
+        for k in ("schema_version", "query_id", "candidate_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id",
+                  "patch_b_id", "target_mask"):
+            setattr(o, k, int(r[k]))
+        for k in ("features", "interval_targets", "family_targets"):
+            setattr(o, k, [float(x) for x in r[k]])
+        o.priority_target, o.cost_target = float(r["priority_target"]), float(r["cost_target"])
+        o.uncertainty_target = float(r["uncertainty_target"])
+        out.append(o)
+    return out
+
+
+def _runtime_rows(candidates, primitive_count, raw_hit_count, compact_candidate_count, masks) -> np.ndarray:
+    from p2cccd_b200.proxy import runtime_feature_rows
+
+    return runtime_feature_rows(_candidate_array(candidates), primitive_count, raw_hit_count,
+                                compact_candidate_count, dict(masks or {}))
+
+
+def build_runtime_proposal_feature_rows(candidates, primitive_count: int, raw_hit_count: int,
+                                        compact_candidate_count: int,
+                                        conservative_family_masks_by_query_id) -> list:  # py_module.cpp:639-652
+    """BuildProposalFeatureRowsFromRuntimeCandidates (proposal_policy.cpp:568-592)
+    on the GPU: one ProposalFeatureRow per candidate."""
+    return _row_objects(_runtime_rows(candidates, primitive_count, raw_hit_count, compact_candidate_count,
+                                      conservative_family_masks_by_query_id))
+
+
+def build_runtime_proposal_feature_arrays(candidates, primitive_count: int, raw_hit_count: int,
+                                          compact_candidate_count: int,
+                                          conservative_family_masks_by_query_id) -> dict:  # py_module.cpp:654-753
+    """The same rows as a dict of numpy arrays (the reference's keys)."""
+    rows = _runtime_rows(candidates, primitive_count, raw_hit_count, compact_candidate_count,
+                         conservative_family_masks_by_query_id)
+    out = {"schema_version": int(rows["schema_version"][0]) if len(rows) else 1}
+    for k in ("query_id", "candidate_id", "slab_id", "object_a_id", "patch_a_id", "object_b_id", "patch_b_id",
+              "features", "interval_targets", "family_targets", "priority_target", "cost_target",
+              "uncertainty_target", "target_mask"):
+        out[k] = np.ascontiguousarray(rows[k])
+    return out
+
+
+def extract_proposal_feature_rows(scene, generation_result) -> list:
+    """ExtractProposalFeatureRows (proposal_features.cpp:236-259) on the GPU for a
+    ProxyScene and the CandidateGenerationResult of generate_candidates_for_proxy_scene:
+    candidates regenerated on the device for the scene (identical to the
+    result's; checked), density stats and rows from p2c_proposal_feature_rows."""
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    a = _proxy_arrays(scene)
+    validate_proxy_scene(a)
+    if int(generation_result.density.query_id) != int(a["query_id"]):
+        raise ValueError("candidate density query_id must match proxy scene query_id")
+    pc = ProxyCandidates(a)
+    _, cand = pc.run_checked()
+    given = _candidate_array(generation_result.candidates)
+    if cand.tobytes() != given.tobytes():
+        raise ValueError("generation_result candidates do not belong to this scene")
+    _, rows = pc.feature_rows()
+    return _row_objects(rows)

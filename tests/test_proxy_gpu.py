@@ -298,3 +298,57 @@ def test_device_feature_rows_flag_bad_candidates(cuda_device):
     pc.run_checked()
     dens, rows = pc.feature_rows()
     assert len(rows) == int(dens["compact_candidate_count"]) > 0
+
+
+@pytest.mark.parametrize("masks", [None, {7: 1}, {7: 2}, {7: 0}])
+def test_device_runtime_feature_rows_match_reference(cuda_device, oracle_mod, masks):
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates, runtime_feature_rows
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=6, patches_per_object=40, n_slabs=4, seed=6, duplicates=0.3)
+    pc = ProxyCandidates(sc, cuda_device)
+    raw, cand = pc.run_checked()
+    ref = oracle_mod.ref_runtime_feature_rows(cand, int(sc["n"]), len(raw), len(cand), masks)
+    got = runtime_feature_rows(cand, int(sc["n"]), len(raw), len(cand), masks, cuda_device)
+    assert np.array_equal(got.view(np.uint8), ref.view(np.uint8))
+    # straight from the device candidates of the run
+    got_dev = runtime_feature_rows(pc.cand[:len(cand)], int(sc["n"]), len(raw), len(cand), masks, cuda_device)
+    assert np.array_equal(got_dev.view(np.uint8), ref.view(np.uint8))
+    bad = cand.copy()
+    bad["rt_hit_count"][2] = 0
+    with pytest.raises(ValueError, match="validation"):
+        runtime_feature_rows(bad, int(sc["n"]), len(raw), len(cand), masks, cuda_device)
+
+
+def test_mirror_feature_row_functions(cuda_device, oracle_mod):
+    import p2cccd_cpp as cpp
+    from p2cccd_b200 import scenes
+    from test_proxy_oracle import _scene_object
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=4, patches_per_object=25, n_slabs=3, seed=9, duplicates=0.3)
+    obj = _scene_object(sc)
+    res = cpp.generate_candidates_for_proxy_scene(obj)
+    _, ref_rows = oracle_mod.ref_proposal_feature_rows(sc)
+    rows = cpp.extract_proposal_feature_rows(obj, res)
+    assert len(rows) == len(ref_rows)
+    for o, r in zip(rows, ref_rows):
+        assert o.candidate_id == int(r["candidate_id"]) and o.features == [float(x) for x in r["features"]]
+        assert o.interval_targets == [float(x) for x in r["interval_targets"]]
+        assert (o.priority_target, o.cost_target, o.uncertainty_target) == \
+            (float(r["priority_target"]), float(r["cost_target"]), float(r["uncertainty_target"]))
+    masks = {int(sc["query_id"]): 2}
+    n_raw, n_cand = len(res.raw_buffer.hits), len(res.candidates)
+    ref_rt = oracle_mod.ref_runtime_feature_rows(cpp._candidate_array(res.candidates), int(sc["n"]), n_raw, n_cand,
+                                                 masks)
+    arrays = cpp.build_runtime_proposal_feature_arrays(res.candidates, int(sc["n"]), n_raw, n_cand, masks)
+    assert arrays["schema_version"] == 1
+    for k in ("features", "family_targets", "priority_target", "cost_target", "uncertainty_target", "candidate_id"):
+        assert np.array_equal(arrays[k], ref_rt[k]), k
+    rt_rows = cpp.build_runtime_proposal_feature_rows(res.candidates, int(sc["n"]), n_raw, n_cand, masks)
+    assert [o.family_targets[:2] for o in rt_rows] == [[0.0, 1.0]] * n_cand
+    with pytest.raises(ValueError, match="non-zero"):
+        cpp.build_runtime_proposal_feature_rows(res.candidates, 0, n_raw, n_cand, masks)

@@ -282,3 +282,39 @@ def test_feature_rows_known_properties(oracle_mod):
     assert np.all(np.isfinite(rows["features"]))
     # the two slabs of [0, 1]: interval bins 2 and 6 (centres 0.25 and 0.75)
     assert sorted(np.argmax(rows["interval_targets"], 1).tolist()) == [2, 6]
+
+
+@pytest.mark.parametrize("masks", [None, {7: 1}, {7: 2}, {7: 0}, {8: 1}])
+def test_runtime_feature_rows_restatement_matches_reference(oracle_mod, masks):
+    """BuildProposalFeatureRowsFromRuntimeCandidates restated, byte for byte:
+    no mask, point-triangle only, edge-edge only, a zero mask (both
+    families) and another query's mask."""
+    from p2cccd_b200 import scenes
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=5, patches_per_object=30, n_slabs=3, seed=2, duplicates=0.5)
+    raw, cand = oracle_mod.proxy_candidates(sc)
+    a = oracle_mod.ref_runtime_feature_rows(cand, int(sc["n"]), len(raw), len(cand), masks)
+    b = oracle_mod.runtime_feature_rows(cand, int(sc["n"]), len(raw), len(cand), masks)
+    assert np.array_equal(a.view(np.uint8), b.view(np.uint8))
+    # one proxy: overlap denominator 1; no candidates: ratios 0
+    a1 = oracle_mod.ref_runtime_feature_rows(cand[:3], 1, 5, 0, masks)
+    b1 = oracle_mod.runtime_feature_rows(cand[:3], 1, 5, 0, masks)
+    assert np.array_equal(a1.view(np.uint8), b1.view(np.uint8))
+
+
+def test_runtime_feature_rows_reject_zero_primitives(oracle_mod):
+    import torch
+
+    from p2cccd_b200 import _lib
+
+    msg = "CandidateDensityStats.proxy_count must be non-zero"
+    if oracle_mod.ref_available():
+        with pytest.raises(ValueError, match=msg):
+            oracle_mod.ref_runtime_feature_rows(np.zeros(0, np.uint8), 0, 0, 0)
+    with pytest.raises(ValueError, match=msg):
+        oracle_mod.runtime_feature_rows([], 0, 0, 0)
+    if not torch.cuda.is_available():  # host-side check, before any device work
+        with pytest.raises(ValueError, match=msg):
+            _lib.check(_lib.load().p2c_runtime_feature_rows(None, 0, 0, 0, 0, None, None, 0, None, 16, None))
