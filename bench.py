@@ -12,8 +12,8 @@ A step is one pass of the hot path over one batch of seeded synthetic input:
     any-hit stress case, a Poisson stream through the serving engine.
 metric: certified CCD queries/s (one query = one primitive certificate).
   * proxy: a proxy scene (rigid bodies x patches x motion segments x time
-    slabs) built and its raw hits and compacted candidates generated;
-    metric: proxies/s.
+    slabs) built, its raw hits and compacted candidates generated and the
+    proposal feature rows of every candidate formed; metric: proxies/s.
 
 Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
 on the launching stream, with a 512 MB L2 flush between steps (outside the
@@ -979,24 +979,26 @@ def _proxy_input(objects: int, seed: int) -> dict:
 
 
 def _proxy_config(inp: dict, n: int, raw: int, cand: int) -> dict:
-    return {"workload": f"proxy-scene candidates: {len(inp['objects'])} rigid bodies x {PROXY_PATCHES} patches x "
+    return {"workload": f"proxy-scene proposal data: {len(inp['objects'])} rigid bodies x {PROXY_PATCHES} patches x "
                         f"{PROXY_SEGMENTS} motion segments x {PROXY_SLABS} time slabs, bodies rotating and drifting "
                         "in a box of constant body density; BuildProxyScene (patch motion bounds, swept-AABB / "
-                        "capsule proxies) then raw hits and compacted candidates of the whole scene",
+                        "capsule proxies), raw hits and compacted candidates of the whole scene, density stats and "
+                        "the 32-feature proposal rows of every candidate",
             "proxies_per_step": n, "raw_hits": raw, "candidates": cand, "objects": len(inp["objects"]),
             "seed": inp.get("seed")}
 
 
 def _proxy_reference(inp: dict, budget_s: float) -> dict:
     """The reference's BuildProxyScene + GenerateRawCandidatesCpu +
-    CompactRawCandidates (oracle/_ref, unchanged sources, 1 thread as
+    CompactRawCandidates + ComputeCandidateDensityStats +
+    ExtractProposalFeatureRows (oracle/_ref, unchanged sources, 1 thread as
     written) on the same scene, whole scenes until budget_s has passed."""
     import oracle
 
     done, t0, runs = 0, time.perf_counter(), 0
     while True:
         sc = oracle.ref_build_proxy_scene(inp)
-        oracle.ref_proxy_candidates(sc)
+        oracle.ref_proposal_feature_rows(sc)
         done += sc["n"]
         runs += 1
         el = time.perf_counter() - t0
@@ -1020,10 +1022,12 @@ def run_proxy(args) -> dict | None:
     raw, cand = cands.run_checked()
     n_raw, n_cand = len(raw), len(cand)
     cands.fit_capacity()  # buffers (and every sort over them) sized to the scene's hits
+    cands.run_checked()
 
     def step():
         build.run()
         cands.run()
+        cands.feature_rows_async()
 
     # end-to-end: patch arrays from pinned host memory in, counts and records back
     h_center = build.patch_center.cpu().pin_memory()
@@ -1032,6 +1036,8 @@ def run_proxy(args) -> dict | None:
     h_raw = torch.empty_like(cands.raw, device="cpu").pin_memory()
     h_cand = torch.empty_like(cands.cand, device="cpu").pin_memory()
     h_counts = torch.empty_like(cands.counts, device="cpu").pin_memory()
+    cands.feature_rows()  # allocates the row buffers; checks the rows
+    h_rows = torch.empty_like(cands.rows, device="cpu").pin_memory()
 
     def step_e2e():
         build.patch_center.copy_(h_center, non_blocking=True)
@@ -1043,6 +1049,7 @@ def run_proxy(args) -> dict | None:
         nr, nc = int(h_counts[0]), int(h_counts[1])
         h_raw[:nr].copy_(cands.raw[:nr], non_blocking=True)
         h_cand[:nc].copy_(cands.cand[:nc], non_blocking=True)
+        h_rows[:nc].copy_(cands.rows[:nc], non_blocking=True)
 
     stream = torch.cuda.current_stream(dev)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
@@ -1066,16 +1073,19 @@ def run_proxy(args) -> dict | None:
     ev = []
     for _ in range(args.steps):
         flush.fill_(1)
-        e = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        e = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
         e[0].record()
         build.run()
         e[1].record()
         cands.run()
         e[2].record()
+        cands.feature_rows_async()
+        e[3].record()
         ev.append(e)
     torch.cuda.synchronize()
-    build_ms = statistics.mean(a.elapsed_time(b) for a, b, _ in ev)
-    cand_ms = statistics.mean(b.elapsed_time(c) for _, b, c in ev)
+    build_ms = statistics.mean(e[0].elapsed_time(e[1]) for e in ev)
+    cand_ms = statistics.mean(e[1].elapsed_time(e[2]) for e in ev)
+    feat_ms = statistics.mean(e[2].elapsed_time(e[3]) for e in ev)
     n = build.n
     ms = statistics.mean(times)
     value, ms_max = replica_rate(world, n, ms)
@@ -1097,17 +1107,23 @@ def run_proxy(args) -> dict | None:
                       achieved=build_bytes / (build_ms * 1e-3) / 1e9,
                       frac=build_bytes / (build_ms * 1e-3) / 1e9 / hbm_peak, algorithmic_bytes_per_step=build_bytes,
                       bytes_per_unit="36 B per patch + 200 B per slab record read, 113 B per proxy written")
-    roofline, secondary = (cand_roof, build_roof) if cand_ms >= build_ms else (build_roof, cand_roof)
+    feat_bytes = 528 * n_cand
+    feat_roof = dict(rl, kernel="proposal feature rows (density sorts, first-proxy lookup, rows_kernel)",
+                     achieved=feat_bytes / (feat_ms * 1e-3) / 1e9, frac=feat_bytes / (feat_ms * 1e-3) / 1e9 / hbm_peak,
+                     algorithmic_bytes_per_step=feat_bytes,
+                     bytes_per_unit="80 B candidate + 2 x 96 B proxy read, 256 B row written per candidate")
+    ranked = sorted(((cand_ms, cand_roof), (build_ms, build_roof), (feat_ms, feat_roof)), key=lambda x: -x[0])
+    roofline, secondary = ranked[0][1], [r for _, r in ranked[1:]]
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         r = _proxy_reference(inp, args.cpu_budget)
         cpu = {"value": r["proxies"] / r["seconds"], "unit": "proxies/s", "cores": 1, "kind": "reference",
                "sample": f"the same {n}-proxy scene, {r['runs']} whole run(s) of the reference build + all-pairs "
-                         "candidates + compaction (1 thread as written)"}
+                         "candidates + compaction + density stats + feature rows (1 thread as written)"}
     if rank != 0:
         return None
     return {
-        "metric": "proxy-scene candidates: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
+        "metric": "proxy-scene proposal data: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
         "p50_ms": statistics.median(times), "p99_ms": sorted(times)[max(0, int(0.99 * len(times)) - 1)],
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
@@ -1116,10 +1132,10 @@ def run_proxy(args) -> dict | None:
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": e2e_value, "unit": "proxies/s", "ms_per_step": e2e_ms,
                 "h2d_bytes_per_step": h_center.numel() * 8 + h_radius.numel() * 8 + h_pid.numel() * 4,
-                "d2h_bytes_per_step": h_counts.numel() * 8 + 64 * n_raw + 80 * n_cand},
+                "d2h_bytes_per_step": h_counts.numel() * 8 + 64 * n_raw + 80 * n_cand + 256 * n_cand},
         "gpu_launches": n_kernels * args.steps if n_kernels >= 0 else None,
         "kernels_per_step": kernel_names,
-        "phases": {"build_ms": build_ms, "candidates_ms": cand_ms},
+        "phases": {"build_ms": build_ms, "candidates_ms": cand_ms, "feature_rows_ms": feat_ms},
         "roofline": roofline, "roofline_secondary": secondary,
         "cpu_baseline": cpu, "clocks": clocks,
     }
@@ -1153,14 +1169,15 @@ def run_reference(args) -> dict | None:
         n = sum(r["proxies"] for r in runs) / sum(r["runs"] for r in runs)
         value = sum(r["proxies"] for r in runs) / sum(r["seconds"] for r in runs)
         ms = sum(r["seconds"] for r in runs) / sum(r["runs"] for r in runs) * 1e3
-        return {"metric": "proxy-scene candidates: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
+        return {"metric": "proxy-scene proposal data: proxies/s", "value": value, "unit": "proxies/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "config": {**_proxy_config(inp, int(n), -1, -1), "raw_hits": None, "candidates": None},
                 "impl": "reference",
                 "cpu_baseline": {"value": value, "unit": "proxies/s", "cores": 1, "kind": "reference",
                                  "sample": "whole scenes: BuildProxyScene + GenerateRawCandidatesCpu (all pairs) + "
-                                           "CompactRawCandidates, 1 thread as written"},
+                                           "CompactRawCandidates + ComputeCandidateDensityStats + "
+                                           "ExtractProposalFeatureRows, 1 thread as written"},
                 "e2e": {"value": value, "unit": "proxies/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     threads = os.cpu_count() or 1
     cfg = certify.CertConfig(1e-6, 1e-6, 32)

@@ -73,6 +73,7 @@ class ProxyCandidates:
     def _alloc(self, cap: int) -> None:
         d = self.device
         self.cap = max(0, int(cap))  # 0: only count the hits
+        self._filled = False  # no run has written the new buffers yet
         self.raw = torch.empty((self.cap, 64), dtype=torch.uint8, device=d)
         self.cand = torch.empty((self.cap, 80), dtype=torch.uint8, device=d)
         ws = int(self.lib.p2c_proxy_candidates_workspace_bytes(self.n, self.cap, self._struct.slab_bits))
@@ -91,6 +92,7 @@ class ProxyCandidates:
         _lib.check(self.lib.p2c_proxy_candidates(ctypes.byref(self._struct), self.raw.data_ptr(), self.cap,
                                                  self.cand.data_ptr(), self.counts.data_ptr(), self.ws.data_ptr(),
                                                  self.ws.numel(), _stream_ptr(self.device)))
+        self._filled = True
 
     def run_checked(self, max_retries: int = 3, raw_only: bool = False) -> tuple[np.ndarray, np.ndarray]:
         """Run; grow the buffers and re-run on overflow; raise on an invalid
@@ -122,6 +124,8 @@ class ProxyCandidates:
         run's candidates (p2c_proposal_feature_rows, no host sync).  Returns
         device tensors (density 96 B, rows cap x 256 B, error word); rows
         [0, candidate count) are valid."""
+        if not self._filled:
+            raise RuntimeError("run() the candidates after (re)sizing the buffers before forming feature rows")
         d = self.device
         if getattr(self, "_rows_cap", -1) != self.cap:
             self.rows = torch.empty((max(self.cap, 1), 256), dtype=torch.uint8, device=d)

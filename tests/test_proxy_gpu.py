@@ -352,3 +352,19 @@ def test_mirror_feature_row_functions(cuda_device, oracle_mod):
     assert [o.family_targets[:2] for o in rt_rows] == [[0.0, 1.0]] * n_cand
     with pytest.raises(ValueError, match="non-zero"):
         cpp.build_runtime_proposal_feature_rows(res.candidates, 0, n_raw, n_cand, masks)
+
+
+def test_feature_rows_need_a_run_after_resizing(cuda_device):
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    pc = ProxyCandidates(scenes.proxy_scene(n_objects=3, patches_per_object=10, n_slabs=2, seed=4), cuda_device)
+    with pytest.raises(RuntimeError):
+        pc.feature_rows()
+    pc.run_checked()
+    pc.fit_capacity()
+    with pytest.raises(RuntimeError):
+        pc.feature_rows()
+    pc.run_checked()
+    dens, rows = pc.feature_rows()
+    assert len(rows) == int(dens["compact_candidate_count"])
