@@ -621,9 +621,11 @@ size_t p2c_proposal_feature_rows_workspace_bytes(int64_t n_proxies);
  * the calls).  Each candidate side maps to the first proxy in scene order with
  * its (slab, object, patch, type).  *error_word_dev: bit 1 a candidate fails
  * ValidateCandidateRecord (common/validators.cpp:160-181), bit 2 a candidate
- * side maps to no proxy; such rows are zero.  The scene's id width hints
- * narrow the sorts (an id beyond its hint voids the results, as for
- * p2c_proxy_candidates).  No host sync. */
+ * side maps to no proxy; such rows are zero; bit 4 a proxy id beyond its
+ * width hint (results void; p2c_proxy_candidates flags the same scene).  The
+ * scene's id width hints narrow the sorts, and when all three are set and
+ * slab, type, object and patch fit one 64-bit word the first-proxy lookup is
+ * one sort and one binary search per side.  No host sync. */
 int p2c_proposal_feature_rows(const p2c_proxy_scene* scene, const p2c_candidate_record* candidates_dev,
                               int64_t cap, const uint64_t* counts_dev, p2c_candidate_density* density_dev,
                               p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* workspace_dev,

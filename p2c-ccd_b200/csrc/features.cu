@@ -163,6 +163,35 @@ __global__ void lookup_gather_kernel(p2c_proxy_scene sc, FeatureLayout L, int pa
   L.ko[p] = ((unsigned long long)sc.object_id[i] << patch_bits) | sc.patch_id[i];
 }
 
+// Packed lookup key (all width hints set and fitting 64 bits): slab, type,
+// object, patch in one word.  Ids past their hints flag bit 4 (the packing
+// would alias them).
+struct PackedKey {
+  int ob, pb;  // bits of the object and patch fields (slab above type above object above patch)
+  __device__ __forceinline__ unsigned long long make(unsigned slab, unsigned type, unsigned object,
+                                                    unsigned patch) const {
+    return ((((((unsigned long long)slab << 8) | type) << ob) | object) << pb) | patch;
+  }
+  __device__ __forceinline__ bool fits(unsigned slab, unsigned object, unsigned patch, int sb) const {
+    return (sb >= 32 || !(slab >> sb)) && (ob >= 32 || !(object >> ob)) && (pb >= 32 || !(patch >> pb));
+  }
+};
+
+__global__ void packed_keys_kernel(p2c_proxy_scene sc, FeatureLayout L, PackedKey pk, int sb,
+                                   unsigned long long* err) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= sc.n) return;
+  const unsigned slab = sc.slab_id[i], obj = sc.object_id[i], patch = sc.patch_id[i];
+  if (!pk.fits(slab, obj, patch, sb)) atomicOr(err, 4ull);
+  L.key[0][i] = pk.make(slab, sc.proxy_type[i], obj, patch);
+  L.val[0][i] = (unsigned)i;
+}
+
+__device__ __forceinline__ long long find_proxy_packed(const FeatureLayout& L, long long n, unsigned long long k) {
+  const long long lo = lower_bound(L.k2, n, k);
+  return (lo < n && L.k2[lo] == k) ? (long long)L.val[1][lo] : -1;
+}
+
 // FindCandidatePrimitive (:103-112): the smallest proxy index whose
 // (slab, type, object, patch) equals the candidate side's; -1 if none.
 __device__ __forceinline__ long long find_proxy(const FeatureLayout& L, long long n, unsigned long long k2,
@@ -200,7 +229,8 @@ __device__ __forceinline__ double overlap(const double* l, const double* r, int 
 
 __global__ void rows_kernel(p2c_proxy_scene sc, FeatureLayout L, const p2c_candidate_record* cand, long long cap,
                             const uint64_t* counts, const p2c_candidate_density* density,
-                            p2c_proposal_feature_row* rows, unsigned long long* err) {
+                            p2c_proposal_feature_row* rows, unsigned long long* err, bool packed, PackedKey pk,
+                            int sb) {
   const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long m = (long long)min((unsigned long long)counts[1], (unsigned long long)cap);
   if (c >= m) return;
@@ -213,10 +243,20 @@ __global__ void rows_kernel(p2c_proxy_scene sc, FeatureLayout L, const p2c_candi
   for (int k = 0; k < 4; ++k) ok = ok && isfinite(r.motion_bound[k]) && !(r.motion_bound[k] < 0.0f);
   const long long n = sc.n;
   const int pb = id_bits(sc.patch_bits);
-  const long long ia = find_proxy(L, n, ((unsigned long long)r.slab_id << 8) | r.proxy_type_a,
-                                  ((unsigned long long)r.object_a_id << pb) | r.patch_a_id);
-  const long long ib = find_proxy(L, n, ((unsigned long long)r.slab_id << 8) | r.proxy_type_b,
-                                  ((unsigned long long)r.object_b_id << pb) | r.patch_b_id);
+  long long ia, ib;
+  if (packed) {  // a side with ids past the hints matches no proxy (all proxies fit them)
+    ia = pk.fits(r.slab_id, r.object_a_id, r.patch_a_id, sb)
+             ? find_proxy_packed(L, n, pk.make(r.slab_id, r.proxy_type_a, r.object_a_id, r.patch_a_id))
+             : -1;
+    ib = pk.fits(r.slab_id, r.object_b_id, r.patch_b_id, sb)
+             ? find_proxy_packed(L, n, pk.make(r.slab_id, r.proxy_type_b, r.object_b_id, r.patch_b_id))
+             : -1;
+  } else {
+    ia = find_proxy(L, n, ((unsigned long long)r.slab_id << 8) | r.proxy_type_a,
+                    ((unsigned long long)r.object_a_id << pb) | r.patch_a_id);
+    ib = find_proxy(L, n, ((unsigned long long)r.slab_id << 8) | r.proxy_type_b,
+                    ((unsigned long long)r.object_b_id << pb) | r.patch_b_id);
+  }
   if (!ok || ia < 0 || ib < 0) {
     atomicOr(err, (!ok ? 1ull : 0ull) | (ia < 0 || ib < 0 ? 2ull : 0ull));
     rows[c] = row;
@@ -424,6 +464,18 @@ int p2c_proposal_feature_rows(const p2c_proxy_scene* scene, const p2c_candidate_
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key[0], L.key[1], L.val[0], L.val[1], (int)n, 0, ob + sb,
                                              s));
     runs_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n, 1, 3, sb);
+  }
+  const bool packed = sc.slab_bits > 0 && sc.object_bits > 0 && sc.patch_bits > 0 && sb + 8 + ob + pb <= 64;
+  PackedKey pk{ob, pb};
+  if (n > 0 && packed) {
+    // lookup order in one sort of (slab, type, object, patch) words, ties by proxy index (stable)
+    size_t tb = L.tmp_bytes;
+    packed_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, pk, sb,
+                                                         reinterpret_cast<unsigned long long*>(error_word_dev));
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key[0], L.k2, L.val[0], L.val[1], (int)n, 0,
+                                             sb + 8 + ob + pb, s));
+  } else if (n > 0) {
+    size_t tb;
     // lookup order: (slab, type, object, patch), ties by proxy index (stable passes)
     lookup_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, pb);
     tb = L.tmp_bytes;
@@ -437,7 +489,8 @@ int p2c_proposal_feature_rows(const p2c_proxy_scene* scene, const p2c_candidate_
   density_kernel<<<1, 32, 0, s>>>(sc, L, counts_dev, density_dev);
   if (cap > 0)
     rows_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, candidates_dev, cap, counts_dev, density_dev, rows_dev,
-                                                  reinterpret_cast<unsigned long long*>(error_word_dev));
+                                                  reinterpret_cast<unsigned long long*>(error_word_dev), packed, pk,
+                                                  sb);
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;
 }

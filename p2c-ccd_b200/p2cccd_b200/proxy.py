@@ -151,6 +151,8 @@ class ProxyCandidates:
             raise ValueError("a CandidateRecord fails validation")
         if e & 2:
             raise ValueError("candidate does not map to proxy primitives")
+        if e & 4:
+            raise RuntimeError("a proxy id exceeds the scene's width hint")
         dens = density.cpu().numpy().view(DENSITY_DTYPE)[0]
         return dens, rows[:n_cand].cpu().numpy().view(FEATURE_ROW_DTYPE).reshape(-1)
 
