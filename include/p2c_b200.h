@@ -645,6 +645,46 @@ int p2c_runtime_feature_rows(const p2c_candidate_record* candidates_dev, int64_t
                              const uint64_t* mask_query_ids_dev, const uint32_t* masks_dev, int64_t n_masks,
                              p2c_proposal_feature_row* rows_dev, uint64_t* error_word_dev, void* stream);
 
+/* ---- audit rows of an exact work queue ------------------------------------- */
+/* The ExactWorkItem fields (common/runtime_contracts.h:67-81) an audit row
+ * reads, 56 bytes; candidate_id is the item's parent_candidate_id. */
+typedef struct p2c_audit_item {
+  uint64_t query_id, candidate_id, work_item_id;
+  double interval_t0, interval_t1;
+  float priority_score;
+  uint32_t feature_family_mask;
+  uint16_t depth;
+  uint16_t pad[3];
+} p2c_audit_item;
+
+/* AuditLogRow (common/runtime_contracts.h:101-114), 80 bytes. */
+typedef struct p2c_audit_row {
+  uint64_t event_id, query_id, candidate_id, work_item_id;
+  uint8_t stage;                 /* AuditStage: 2 exact (dequeue), 4 certify */
+  uint8_t pad0;
+  uint16_t action;               /* 1 dequeued, 2 collision, 3 separation, 4 undecided, 5 invalid input */
+  uint16_t depth;
+  uint16_t pad1;
+  double interval_t0, interval_t1;
+  uint64_t timestamp_us;
+  double aux_value0, aux_value1;
+} p2c_audit_row;
+
+/* The audit log ProcessExactWorkQueueCpu (certificate/certificate_engine.cpp:
+ * 593-661) writes for n certified work items, from their certificates on the
+ * device (p2c_certify_queries' output): per item, with emit_dequeue_events a
+ * dequeue row (stage exact, action dequeued, aux = priority score, family
+ * mask), then a certify row (stage certify, action from the status and
+ * reason code, aux = safe_margin_lb for a separation else toi_upper, and the
+ * next refinement mode); event ids and timestamps count up from
+ * first_event_id / first_timestamp_us in that order (rows_dev holds n x 2 or
+ * n rows).  error_dev[0] bit 1: a row fails ValidateAuditLogRow
+ * (common/validators.cpp:295-315), error_dev[1] the first such row.  No host
+ * sync. */
+int p2c_audit_rows(const p2c_audit_item* items_dev, const p2c_query_certificate* certs_dev, int64_t n,
+                   uint64_t first_event_id, uint64_t first_timestamp_us, int emit_dequeue_events,
+                   p2c_audit_row* rows_dev, uint64_t* error_dev, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

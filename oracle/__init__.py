@@ -863,3 +863,58 @@ def runtime_feature_rows(cand, primitive_count: int, raw_hit_count: int, compact
         r["uncertainty_target"] = 0.25 if mask == 3 else 0.0
         r["target_mask"] = 31
     return rows
+
+
+
+# ---- exact work queue audit rows (certificate_engine.cpp:593-661) ----
+
+def ref_process_queue(items, pts, pt_off, ees, ee_off, eps_time=1e-6, eps_space=1e-6, max_depth=32,
+                      first_event_id=1, first_timestamp_us=1, emit_dequeue=True):
+    """The reference's ProcessExactWorkQueueCpu: (certificates as QUERY_CERT
+    records, audit rows as AUDIT_ROW_DTYPE records)."""
+    from p2cccd_b200.records import AUDIT_ROW_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_queue_ready"):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        R.ref_process_queue.argtypes = [vp, i64, vp, vp, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                        ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, vp, vp, vp]
+        R._queue_ready = True
+    items = np.ascontiguousarray(items)
+    n = len(items)
+    certs = np.zeros(max(n, 1), QUERY_CERT)
+    rows = np.zeros(max(2 * n, 1), AUDIT_ROW_DTYPE)
+    n_rows = ctypes.c_int64(0)
+    a, b = np.ascontiguousarray(pts), np.ascontiguousarray(ees)
+    po, eo = np.ascontiguousarray(pt_off, np.int64), np.ascontiguousarray(ee_off, np.int64)
+    if R.ref_process_queue(_p(items), n, _p(a), _p(po), _p(b), _p(eo), eps_time, eps_space, max_depth,
+                           first_event_id, first_timestamp_us, 1 if emit_dequeue else 0, _p(certs), _p(rows),
+                           ctypes.byref(n_rows)):
+        raise ValueError(ref().ref_last_error().decode())
+    return certs[:n], rows[:n_rows.value]
+
+
+def audit_rows(items, certs, first_event_id=1, first_timestamp_us=1, emit_dequeue=True):
+    """Restatement of the audit rows of ProcessExactWorkQueueCpu (:593-661,
+    MakeAuditRow :456-477, AuditActionForCertificate :443-454)."""
+    from p2cccd_b200.records import AUDIT_ROW_DTYPE
+
+    rows = []
+    ev, ts = int(first_event_id), int(first_timestamp_us)
+    for it, c in zip(items, certs):
+        def row(stage, action, aux0, aux1):
+            return (ev, it["query_id"], it["candidate_id"], it["work_item_id"], stage, action, it["depth"],
+                    it["interval_t0"], it["interval_t1"], ts, aux0, aux1)
+        if emit_dequeue:
+            rows.append(row(2, 1, float(it["priority_score"]), float(it["feature_family_mask"])))
+            ev, ts = ev + 1, ts + 1
+        st = int(c["status"])
+        action = 2 if st == 0 else (3 if st == 1 else (5 if int(c["reason_code"]) == 3 else 4))
+        rows.append(row(4, action, float(c["safe_margin_lb"] if st == 1 else c["toi_upper"]),
+                        float(c["next_refinement_mode"])))
+        ev, ts = ev + 1, ts + 1
+    out = np.zeros(len(rows), AUDIT_ROW_DTYPE)
+    for o, r in zip(out, rows):
+        for k, v in zip(AUDIT_ROW_DTYPE.names, r):
+            o[k] = v
+    return out

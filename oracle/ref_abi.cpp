@@ -28,6 +28,7 @@ using p2cccd::PointTriangleIntervalPrimitive;
 using p2cccd::PrimitiveIntervalResult;
 
 // The ABI records are the reference's host structs byte for byte.
+static_assert(sizeof(p2cccd::AuditLogRow) == sizeof(p2c_audit_row), "AuditLogRow layout");
 static_assert(sizeof(PointTriangleIntervalPrimitive) == sizeof(p2c_point_triangle));
 static_assert(sizeof(EdgeEdgeIntervalPrimitive) == sizeof(p2c_edge_edge));
 static_assert(sizeof(PrimitiveIntervalResult) == sizeof(p2c_interval_result));
@@ -290,6 +291,79 @@ int ref_refinement_children(double t0, double t1, std::uint16_t depth, std::uint
     c1[i] = children[i].interval_t1;
   }
   return static_cast<int>(children.size());
+}
+
+// ProcessExactWorkQueueCpu on n work items (the p2c_audit_item fields; slab
+// and patch ids 0, source raw) with CSR primitive lists: certificates (the
+// p2c_query_certificate fields) and the audit log (*n_rows rows).
+int ref_process_queue(const p2c_audit_item* items, std::int64_t n, const p2c_point_triangle* pts,
+                      const std::int64_t* pt_off, const p2c_edge_edge* ees, const std::int64_t* ee_off,
+                      double eps_time, double eps_space, int max_depth, std::uint64_t first_event_id,
+                      std::uint64_t first_timestamp_us, int emit_dequeue, p2c_query_certificate* certs_out,
+                      p2c_audit_row* rows_out, std::int64_t* n_rows) {
+  std::vector<p2cccd::ExactCertificateQuery> queue(static_cast<std::size_t>(n));
+  for (std::int64_t k = 0; k < n; ++k) {
+    p2cccd::ExactCertificateQuery& q = queue[static_cast<std::size_t>(k)];
+    const p2c_audit_item& it = items[k];
+    q.work_item.work_item_id = it.work_item_id;
+    q.work_item.parent_candidate_id = it.candidate_id;
+    q.work_item.query_id = it.query_id;
+    q.work_item.interval_t0 = it.interval_t0;
+    q.work_item.interval_t1 = it.interval_t1;
+    q.work_item.feature_family_mask = it.feature_family_mask;
+    q.work_item.depth = it.depth;
+    q.work_item.priority_score = it.priority_score;
+    q.config = MakeConfig(eps_time, eps_space, max_depth);
+    const std::int64_t np = pt_off[k + 1] - pt_off[k], ne = ee_off[k + 1] - ee_off[k];
+    q.point_triangle_primitives.resize(static_cast<std::size_t>(np));
+    q.edge_edge_primitives.resize(static_cast<std::size_t>(ne));
+    if (np) std::memcpy(static_cast<void*>(q.point_triangle_primitives.data()), pts + pt_off[k], sizeof(p2c_point_triangle) * np);
+    if (ne) std::memcpy(static_cast<void*>(q.edge_edge_primitives.data()), ees + ee_off[k], sizeof(p2c_edge_edge) * ne);
+  }
+  p2cccd::ExactWorkQueueConfig cfg;
+  cfg.first_event_id = first_event_id;
+  cfg.first_timestamp_us = first_timestamp_us;
+  cfg.emit_dequeue_events = emit_dequeue != 0;
+  p2cccd::ExactWorkQueueResult res;
+  const auto st = p2cccd::ProcessExactWorkQueueCpu(queue, cfg, &res);
+  if (!st.ok) {
+    g_error = st.message;
+    return 1;
+  }
+  for (std::size_t k = 0; k < res.certificates.size(); ++k) {
+    const p2cccd::CertificateResult& r = res.certificates[k];
+    p2c_query_certificate& o = certs_out[k];
+    std::memset(&o, 0, sizeof(o));
+    o.status = static_cast<std::uint8_t>(r.status);
+    o.witness_family = r.witness_family;
+    o.reason_code = r.reason_code;
+    o.covered_feature_mask = r.covered_feature_mask;
+    o.toi_upper = r.toi_upper;
+    o.safe_margin_lb = r.safe_margin_lb;
+    o.witness_id_a = r.witness_id_a;
+    o.witness_id_b = r.witness_id_b;
+    o.witness_index = -1;
+    o.next_refinement_mode = static_cast<std::uint8_t>(r.next_refinement_mode);
+  }
+  *n_rows = static_cast<std::int64_t>(res.audit_log.size());
+  for (std::size_t k = 0; k < res.audit_log.size(); ++k) {
+    const p2cccd::AuditLogRow& a = res.audit_log[k];
+    p2c_audit_row& o = rows_out[k];
+    std::memset(&o, 0, sizeof(o));
+    o.event_id = a.event_id;
+    o.query_id = a.query_id;
+    o.candidate_id = a.candidate_id;
+    o.work_item_id = a.work_item_id;
+    o.stage = static_cast<std::uint8_t>(a.stage);
+    o.action = a.action;
+    o.depth = a.depth;
+    o.interval_t0 = a.interval_t0;
+    o.interval_t1 = a.interval_t1;
+    o.timestamp_us = a.timestamp_us;
+    o.aux_value0 = a.aux_value0;
+    o.aux_value1 = a.aux_value1;
+  }
+  return 0;
 }
 
 }  // extern "C"

@@ -66,3 +66,44 @@ def certify_work_items(pt_records: np.ndarray, pt_offsets: np.ndarray, ee_record
 
 def empty_records(family: int) -> np.ndarray:
     return np.zeros(0, dtype=POINT_TRIANGLE_DTYPE if family == 1 else EDGE_EDGE_DTYPE)
+
+
+
+def audit_rows(items, certs, first_event_id: int = 1, first_timestamp_us: int = 1, emit_dequeue: bool = True,
+               device: str | torch.device = "cuda") -> np.ndarray:
+    """The audit log of a certified queue, written on the device
+    (p2c_audit_rows).  ``items``: AUDIT_ITEM_DTYPE records; ``certs``:
+    QUERY_CERTIFICATE_DTYPE records or their (n, 64) uint8 device tensor.
+    Returns AUDIT_ROW_DTYPE records; ValueError (with the first failing row
+    index) when a row fails the reference's audit row validation."""
+    from .records import AUDIT_ROW_DTYPE
+
+    lib = _lib.load()
+    dev = torch.device(device)
+    items = np.ascontiguousarray(items)
+    n = len(items)
+    d_items = torch.from_numpy(items.view(np.uint8).reshape(-1).copy()).to(dev) if n else None
+    if torch.is_tensor(certs):
+        d_certs = certs.to(dev).contiguous()
+    else:
+        c = np.ascontiguousarray(certs)
+        d_certs = torch.from_numpy(c.view(np.uint8).reshape(-1).copy()).to(dev) if n else None
+    per = 2 if emit_dequeue else 1
+    rows = torch.empty((max(per * n, 1), AUDIT_ROW_DTYPE.itemsize), dtype=torch.uint8, device=dev)
+    err = torch.zeros(2, dtype=torch.int64, device=dev)
+    _lib.check(lib.p2c_audit_rows(d_items.data_ptr() if n else None, d_certs.data_ptr() if n else None, n,
+                                  int(first_event_id), int(first_timestamp_us), 1 if emit_dequeue else 0,
+                                  rows.data_ptr(), err.data_ptr(), _stream_ptr(dev)))
+    e = err.cpu().numpy().view(np.uint64)
+    out = rows[:per * n].cpu().numpy().view(AUDIT_ROW_DTYPE).reshape(-1)
+    if e[0] & 1:
+        raise AuditRowError(int(e[1]), out)
+    return out
+
+
+class AuditRowError(ValueError):
+    """A row fails the reference's ValidateAuditLogRow; ``row`` is the first."""
+
+    def __init__(self, row: int, rows: np.ndarray):
+        super().__init__(f"audit row {row} fails validation")
+        self.row, self.rows = row, rows

@@ -150,3 +150,22 @@ FEATURE_ROW_DTYPE = np.dtype({
     "offsets": [0, 8, 16, 24, 28, 32, 36, 40, 44, 172, 204, 236, 240, 244, 248],
     "itemsize": 256,
 })
+
+
+# the ExactWorkItem fields an audit row reads (p2c_audit_item, 56 bytes)
+AUDIT_ITEM_DTYPE = np.dtype({
+    "names": ["query_id", "candidate_id", "work_item_id", "interval_t0", "interval_t1", "priority_score",
+              "feature_family_mask", "depth"],
+    "formats": ["<u8", "<u8", "<u8", "<f8", "<f8", "<f4", "<u4", "<u2"],
+    "offsets": [0, 8, 16, 24, 32, 40, 44, 48],
+    "itemsize": 56,
+})
+
+# AuditLogRow (common/runtime_contracts.h:101-114), 80 bytes
+AUDIT_ROW_DTYPE = np.dtype({
+    "names": ["event_id", "query_id", "candidate_id", "work_item_id", "stage", "action", "depth", "interval_t0",
+              "interval_t1", "timestamp_us", "aux_value0", "aux_value1"],
+    "formats": ["<u8", "<u8", "<u8", "<u8", "u1", "<u2", "<u2", "<f8", "<f8", "<u8", "<f8", "<f8"],
+    "offsets": [0, 8, 16, 24, 32, 34, 36, 40, 48, 56, 64, 72],
+    "itemsize": 80,
+})

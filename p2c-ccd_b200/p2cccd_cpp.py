@@ -582,28 +582,14 @@ class CertificateEngine:
         return evaluate_certificate_query_cpu(query)
 
 
-def _audit_action(c: CertificateResult) -> int:  # :443-454
-    if c.status == CertificateStatus.COLLISION:
-        return EXACT_AUDIT_COLLISION
-    if c.status == CertificateStatus.SEPARATION:
-        return EXACT_AUDIT_SEPARATION
-    return EXACT_AUDIT_INVALID_INPUT if c.reason_code == CERTIFICATE_REASON_INVALID_INPUT else EXACT_AUDIT_UNDECIDED
-
-
-def _audit_row(event_id, ts, item, stage, action, aux0, aux1) -> AuditLogRow:  # :456-477
-    r = AuditLogRow()
-    r.event_id, r.query_id, r.candidate_id, r.work_item_id = event_id, item.query_id, item.parent_candidate_id, \
-        item.work_item_id
-    r.stage, r.action, r.depth = stage, action, item.depth
-    r.interval_t0, r.interval_t1, r.timestamp_us = item.interval_t0, item.interval_t1, ts
-    r.aux_value0, r.aux_value1 = float(aux0), float(aux1)
-    return r
-
-
 def process_exact_work_queue_cpu(work_queue: Sequence[ExactCertificateQuery],
                                  config: ExactWorkQueueConfig) -> ExactWorkQueueResult:
     """ProcessExactWorkQueueCpu (:593-661): every work item certified in one
-    GPU launch per config; audit rows and the coverage guard on the host."""
+    GPU launch per config; the audit log written on the GPU (p2c_audit_rows);
+    work item / certificate validation and the coverage guard on the host."""
+    from p2cccd_b200 import queue as _queue
+    from p2cccd_b200.records import AUDIT_ITEM_DTYPE, QUERY_CERTIFICATE_DTYPE
+
     if int(config.first_event_id) == 0:
         raise ValueError("ExactWorkQueueConfig.first_event_id must be non-zero")
     if int(config.first_timestamp_us) == 0:
@@ -613,14 +599,9 @@ def process_exact_work_queue_cpu(work_queue: Sequence[ExactCertificateQuery],
         validate_exact_work_item(q.work_item)
     certs = _certify_queries(queue_list)
     result = ExactWorkQueueResult()
-    ev, ts = int(config.first_event_id), int(config.first_timestamp_us)
-    for q, c in zip(queue_list, certs):
-        if config.emit_dequeue_events:
-            row = _audit_row(ev, ts, q.work_item, AuditStage.EXACT, EXACT_AUDIT_DEQUEUED,
-                             float(np.float32(q.work_item.priority_score)), float(q.work_item.feature_family_mask))
-            validate_audit_log_row(row)
-            result.audit_log.append(row)
-            ev, ts = ev + 1, ts + 1
+    items = np.zeros(len(queue_list), AUDIT_ITEM_DTYPE)
+    crec = np.zeros(len(queue_list), QUERY_CERTIFICATE_DTYPE)
+    for k, (q, c) in enumerate(zip(queue_list, certs)):
         if isinstance(c, Exception):  # MakeInvalidInputCertificate, :426-431
             c = _base_certificate(q.work_item, q.config)
             c.reason_code = CERTIFICATE_REASON_INVALID_INPUT
@@ -628,16 +609,34 @@ def process_exact_work_queue_cpu(work_queue: Sequence[ExactCertificateQuery],
             c.safe_margin_lb = 0.0
             c.covered_feature_mask = 0
         validate_certificate_result(c)
-        aux0 = c.safe_margin_lb if c.status == CertificateStatus.SEPARATION else c.toi_upper
-        row = _audit_row(ev, ts, q.work_item, AuditStage.CERTIFY, _audit_action(c), aux0,
-                         float(int(c.next_refinement_mode)))
-        validate_audit_log_row(row)
-        ev, ts = ev + 1, ts + 1
+        w = q.work_item
+        items[k] = (w.query_id, w.parent_candidate_id, w.work_item_id, w.interval_t0, w.interval_t1,
+                    w.priority_score, w.feature_family_mask, w.depth)
+        r = crec[k]
+        r["status"], r["reason_code"] = int(c.status), int(c.reason_code)
+        r["toi_upper"], r["safe_margin_lb"] = float(c.toi_upper), float(c.safe_margin_lb)
+        r["next_refinement_mode"] = int(c.next_refinement_mode)
         result.certificates.append(c)
-        result.audit_log.append(row)
-        result.processed_count += 1
+    try:
+        rows = _queue.audit_rows(items, crec, int(config.first_event_id), int(config.first_timestamp_us),
+                                 bool(config.emit_dequeue_events))
+    except _queue.AuditRowError as exc:  # the reference's message for the first failing row
+        validate_audit_log_row(_audit_row_object(exc.rows[exc.row]))
+        raise
+    result.audit_log = [_audit_row_object(r) for r in rows]
+    result.processed_count = len(queue_list)
     validate_exact_work_queue_coverage(queue_list, result)
     return result
+
+
+def _audit_row_object(r) -> AuditLogRow:
+    row = AuditLogRow()
+    for k in ("event_id", "query_id", "candidate_id", "work_item_id", "action", "depth", "timestamp_us"):
+        setattr(row, k, int(r[k]))
+    row.stage = AuditStage(int(r["stage"]))
+    for k in ("interval_t0", "interval_t1", "aux_value0", "aux_value1"):
+        setattr(row, k, float(r[k]))
+    return row
 
 
 def validate_exact_work_queue_coverage(work_queue, result) -> bool:  # :553-591

@@ -368,3 +368,60 @@ def test_feature_rows_need_a_run_after_resizing(cuda_device):
     pc.run_checked()
     dens, rows = pc.feature_rows()
     assert len(rows) == int(dens["compact_candidate_count"])
+
+
+@pytest.mark.parametrize("emit", [True, False])
+def test_device_audit_rows_match_reference(cuda_device, oracle_mod, emit):
+    """Certificates from the device queue path, then p2c_audit_rows: every
+    80-byte AuditLogRow equal to the reference ProcessExactWorkQueueCpu's."""
+    from audit_queue import make_queue
+    from p2cccd_b200 import queue
+    from p2cccd_b200.certify import CertConfig
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    items, pts, pt_off, ees, ee_off = make_queue()
+    ref_certs, ref_rows = oracle_mod.ref_process_queue(items, pts, pt_off, ees, ee_off, 1e-6, 1e-6, 32, 500, 800,
+                                                       emit)
+    res = queue.certify_work_items(pts, pt_off, ees, ee_off, items["interval_t0"], items["interval_t1"],
+                                   items["feature_family_mask"], CertConfig(1e-6, 1e-6, 32), cuda_device)
+    certs = res["certs"]
+    for k in ("status", "reason_code", "toi_upper", "safe_margin_lb", "next_refinement_mode"):
+        assert np.array_equal(certs[k], ref_certs[k]), k
+    rows = queue.audit_rows(items, certs, 500, 800, emit, cuda_device)
+    assert np.array_equal(rows.view(np.uint8), ref_rows.view(np.uint8))
+
+
+def test_mirror_queue_audit_log_matches_reference(cuda_device, oracle_mod):
+    import p2cccd_cpp as cpp
+    from audit_queue import make_queue
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    items, pts, pt_off, ees, ee_off = make_queue(n_items=40, seed=6)
+    _, ref_rows = oracle_mod.ref_process_queue(items, pts, pt_off, ees, ee_off, 1e-6, 1e-6, 32, 7, 9, True)
+    queries = []
+    pt_objs = cpp._from_records(pts, 1)
+    ee_objs = cpp._from_records(ees, 2)
+    for k, it in enumerate(items):
+        q = cpp.ExactCertificateQuery()
+        w = q.work_item
+        w.work_item_id, w.parent_candidate_id, w.query_id = (int(it[f]) for f in ("work_item_id", "candidate_id",
+                                                                                  "query_id"))
+        w.interval_t0, w.interval_t1 = float(it["interval_t0"]), float(it["interval_t1"])
+        w.feature_family_mask, w.depth = int(it["feature_family_mask"]), int(it["depth"])
+        w.priority_score = float(it["priority_score"])
+        q.config.eps_time, q.config.eps_space, q.config.max_subdivision_depth = 1e-6, 1e-6, 32
+        q.point_triangle_primitives = pt_objs[pt_off[k]:pt_off[k + 1]]
+        q.edge_edge_primitives = ee_objs[ee_off[k]:ee_off[k + 1]]
+        queries.append(q)
+    cfg = cpp.ExactWorkQueueConfig()
+    cfg.first_event_id, cfg.first_timestamp_us, cfg.emit_dequeue_events = 7, 9, True
+    res = cpp.process_exact_work_queue_cpu(queries, cfg)
+    assert len(res.audit_log) == len(ref_rows)
+    for o, r in zip(res.audit_log, ref_rows):
+        assert (o.event_id, o.query_id, o.candidate_id, o.work_item_id, int(o.stage), o.action, o.depth,
+                o.timestamp_us) == tuple(int(r[k]) for k in ("event_id", "query_id", "candidate_id", "work_item_id",
+                                                             "stage", "action", "depth", "timestamp_us"))
+        assert (o.interval_t0, o.interval_t1, o.aux_value0, o.aux_value1) == \
+            tuple(float(r[k]) for k in ("interval_t0", "interval_t1", "aux_value0", "aux_value1"))

@@ -318,3 +318,20 @@ def test_runtime_feature_rows_reject_zero_primitives(oracle_mod):
     if not torch.cuda.is_available():  # host-side check, before any device work
         with pytest.raises(ValueError, match=msg):
             _lib.check(_lib.load().p2c_runtime_feature_rows(None, 0, 0, 0, 0, None, None, 0, None, 16, None))
+
+
+# ---- audit rows ---------------------------------------------------------------
+
+@pytest.mark.parametrize("emit", [True, False])
+def test_audit_rows_restatement_matches_reference(oracle_mod, emit):
+    from audit_queue import make_queue
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    items, pts, pt_off, ees, ee_off = make_queue()
+    certs, rows = oracle_mod.ref_process_queue(items, pts, pt_off, ees, ee_off, first_event_id=500,
+                                               first_timestamp_us=800, emit_dequeue=emit)
+    assert len(rows) == len(items) * (2 if emit else 1)
+    assert (certs["reason_code"] == 3).sum() == 1  # the NaN primitive's item
+    mine = oracle_mod.audit_rows(items, certs, 500, 800, emit)
+    assert np.array_equal(mine.view(np.uint8), rows.view(np.uint8))
