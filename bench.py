@@ -807,7 +807,47 @@ def run_b200(args) -> dict | None:
     if phases is not None:
         line["phases"] = phases
         line["roofline_secondary"] = secondary
+    if args.benchmark_rows:
+        _write_benchmark_rows(args, wl, times, phases, census, line, dev)
     return line
+
+
+def _write_benchmark_rows(args, wl, times, phases, census, line, dev) -> None:
+    """The run as a BenchmarkRowV2 (the reference's export schema) in
+    DIR/benchmark_v2.jsonl and .csv, from the device counters of the census
+    launch and the per-step CUDA-event times."""
+    import hashlib
+
+    import torch
+
+    from p2cccd_b200 import rows
+
+    keys = ("collisions", "separations", "undecided", "vf_certified", "ee_certified")
+    if isinstance(getattr(wl, "summaries", None), list):
+        tot = {k: sum(int(x.get(k, 0)) for x in wl.summaries) for k in keys}
+    elif getattr(wl, "first_summary", None) is not None:
+        tot = {k: int(wl.first_summary.get(k, 0)) for k in keys}
+    else:  # independent queries: the families of the batch
+        tot = dict.fromkeys(keys, 0)
+        tot["vf_certified"], tot["ee_certified"] = len(wl.host["vf"]), len(wl.host["ee"])
+    extra = {}
+    if tot["vf_certified"] + tot["ee_certified"] != wl.queries:  # exact calls not split by family (any-hit)
+        tot["vf_certified"] = tot["ee_certified"] = 0
+        extra = {"family_unknown_exact_calls": int(wl.queries), "exact_calls_total": int(wl.queries)}
+    cfg = json.dumps(line["config"], sort_keys=True, default=str)
+    row = rows.benchmark_row_v2(
+        run_id=f"{args.workload}-{int(time.time())}", dataset_name="synthetic", scene_name=args.workload,
+        method_name="b200", config_hash=hashlib.sha1(cfg.encode()).hexdigest()[:16],
+        seed=int(line["config"].get("seed") or 0), query_count=int(wl.queries), latencies_ms=times,
+        exact_ms=(phases or {}).get("narrow_ms", statistics.mean(times)), rt_ms=(phases or {}).get("broad_ms", 0.0),
+        pt_exact_calls=tot["vf_certified"], ee_exact_calls=tot["ee_certified"],
+        distance_evals=int(census.get("distance_evals", 0)), collisions=tot["collisions"],
+        separations=tot["separations"], undecided=tot["undecided"],
+        candidate_bytes=8 * int(wl.queries), vram_peak_bytes=torch.cuda.max_memory_allocated(dev), **extra)
+    out = Path(args.benchmark_rows)
+    rows.write_benchmark_v2_jsonl(out / "benchmark_v2.jsonl", [row])
+    out.mkdir(parents=True, exist_ok=True)
+    (out / "benchmark_v2.csv").write_text(rows.benchmark_csv([row]))
 
 
 # --------------------------------------------------------------------------
@@ -1294,6 +1334,8 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     ap.add_argument("--proxy-objects", type=int, default=32, help="proxy: rigid bodies of 200 patches x 8 slabs")
+    ap.add_argument("--benchmark-rows", default=None, metavar="DIR",
+                    help="also write the run as BenchmarkRowV2 JSONL / CSV (the reference's export schema) to DIR")
     args = ap.parse_args()
     global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS
     PROXY_OBJECTS = max(2, args.proxy_objects)
