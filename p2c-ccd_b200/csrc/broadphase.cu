@@ -337,8 +337,13 @@ __device__ __forceinline__ void append_pair(bool found, unsigned long long key, 
   }
 }
 
-// Vertex-face pairs: threads [0, nv) scan faces from a vertex and own the
-// pairs whose face minimum is >= the vertex minimum; threads [nv, nv + nf)
+// Lanes that share one scanning box in the scene sweeps (its columns are
+// taken in turn): a box's walk is a chain of dependent loads, and splitting
+// it shortens the chain and puts more warps on the SMs.
+constexpr int kSceneSweepLanes = 8;
+
+// Vertex-face pairs: boxes [0, nv) scan faces from a vertex and own the
+// pairs whose face minimum is >= the vertex minimum; boxes [nv, nv + nf)
 // scan vertices from a face and own the others.  Keys (vertex, face).
 __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
                                                             const int32_t* __restrict__ faces, int exclude_self,
@@ -346,14 +351,16 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
                                                             unsigned long long cap, BroadScratch* sc) {
   const Grid& g = sc->grid;
   const long long nv = (long long)(g.seg[1] - g.seg[0]), nf = (long long)(g.seg[2] - g.seg[1]);
-  const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((long long)blockIdx.x * blockDim.x >= nv + nf) return;  // whole block beyond the work
+  const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long t = tt / kSceneSweepLanes;
+  const int lane = (int)(tt % kSceneSweepLanes);
+  if ((long long)blockIdx.x * blockDim.x >= (nv + nf) * kSceneSweepLanes) return;  // whole block beyond the work
   const bool from_vertex = t < nv;
   const long long i = from_vertex ? t : t - nv;
   bool live = from_vertex || i < nf;
   const SortedBoxes P = from_vertex ? V : F;
   const SortedBoxes Q = from_vertex ? F : V;
-  Walker w;
+  StridedWalker w;
   Box6 pb{};
   double lo = 0.0;
   int32_t pid = 0, pobj = 0;
@@ -362,8 +369,8 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
     pid = P.id[i];
     pobj = P.obj[i];
     pb = box_at(P, i);
-    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, from_vertex ? g.reach1[1] : g.reach1[0],
-                from_vertex ? g.reach2[1] : g.reach2[0]);
+    strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, from_vertex ? g.reach1[1] : g.reach1[0],
+                        from_vertex ? g.reach2[1] : g.reach2[0], lane, kSceneSweepLanes);
     live = w.next_cell(Q, g);
   }
   for (;;) {
@@ -405,10 +412,12 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
                                                             unsigned long long cap, BroadScratch* sc) {
   const Grid& g = sc->grid;
   const long long ne = (long long)(g.seg[3] - g.seg[2]);
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if ((long long)blockIdx.x * blockDim.x >= ne) return;
+  const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long long i = tt / kSceneSweepLanes;
+  const int lane = (int)(tt % kSceneSweepLanes);
+  if ((long long)blockIdx.x * blockDim.x >= ne * kSceneSweepLanes) return;
   bool live = i < ne;
-  Walker w;
+  StridedWalker w;
   Box6 pb{};
   double lo = 0.0;
   int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
@@ -419,7 +428,8 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
     pb = box_at(E, i);
-    walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2]);
+    strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
+                        kSceneSweepLanes);
     live = w.next_cell(E, g);
   }
   for (;;) {
@@ -687,10 +697,10 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   if (sort_out && !small_sort && ee_cap > 0)
     fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
   if (scene.nv + scene.nf > 0 && vf_out != nullptr)
-    sweep_vf_kernel<<<grid_for(scene.nv + scene.nf, kThreads), kThreads, 0, s>>>(
+    sweep_vf_kernel<<<grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads), kThreads, 0, s>>>(
         L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out, (unsigned long long)vf_cap, L.sc);
   if (scene.ne > 0 && ee_out != nullptr)
-    sweep_ee_kernel<<<grid_for(scene.ne, kThreads), kThreads, 0, s>>>(L.B[2].s, scene.edges, scene.exclude_self,
+    sweep_ee_kernel<<<grid_for(scene.ne * kSceneSweepLanes, kThreads), kThreads, 0, s>>>(L.B[2].s, scene.edges, scene.exclude_self,
                                                                       ee_shift, ee_out, (unsigned long long)ee_cap,
                                                                       L.sc);
   P2C_CUDA(cudaGetLastError());

@@ -174,6 +174,48 @@ __device__ __forceinline__ void walker_init(Walker& w, const Grid& g, double lo,
   w.q_hi = quantise(hi, g);
 }
 
+// The same walk with the columns of one box shared by several lanes: lane l
+// of a group of `step` takes columns l, l + step, ... of the box's
+// rectangle (row-major over [c1, c1_end] x [c2_begin, c2_end]).
+struct StridedWalker {
+  int c1a, c2a, n2, n_cells, k, step;
+  unsigned j, j_end, q_lo, q_hi;
+
+  __device__ __forceinline__ bool next_cell(const SortedBoxes& Q, const Grid& g) {
+    for (;;) {
+      k += step;
+      if (k >= n_cells) return false;
+      const int cell = (c1a + k / n2) * g.g2 + (c2a + k % n2);
+      unsigned b = Q.cell_begin[cell], e = Q.cell_end[cell];
+      const unsigned end = e;
+      while (b < e) {  // first entry with q >= q_lo
+        const unsigned m = (b + e) >> 1;
+        if (Q.q[m] < q_lo) b = m + 1;
+        else e = m;
+      }
+      j = b;
+      j_end = end;
+      if (j < j_end && Q.q[j] <= q_hi) return true;
+    }
+  }
+};
+
+__device__ __forceinline__ void strided_walker_init(StridedWalker& w, const Grid& g, double lo, double hi, double alo,
+                                                    double ahi, double blo, double bhi, double reach1, double reach2,
+                                                    int lane, int step) {
+  Walker v;
+  walker_init(v, g, lo, hi, alo, ahi, blo, bhi, reach1, reach2);
+  w.c1a = v.c1;
+  w.c2a = v.c2_begin;
+  w.n2 = v.c2_end - v.c2_begin + 1;
+  w.n_cells = (v.c1_end - v.c1 + 1) * w.n2;
+  w.step = step;
+  w.k = lane - step;
+  w.j = w.j_end = 0;
+  w.q_lo = v.q_lo;
+  w.q_hi = v.q_hi;
+}
+
 // A scanning box held in registers for the length of its walk.
 struct Box6 {
   double lo, hi, alo, ahi, blo, bhi;
