@@ -685,6 +685,76 @@ int p2c_audit_rows(const p2c_audit_item* items_dev, const p2c_query_certificate*
                    uint64_t first_event_id, uint64_t first_timestamp_us, int emit_dequeue_events,
                    p2c_audit_row* rows_dev, uint64_t* error_dev, void* stream);
 
+/* ---- runtime exact work queue from proposals ------------------------------- */
+/* ProposalOutput (common/runtime_contracts.h:58-65), 88 bytes. */
+typedef struct p2c_proposal_output {
+  uint64_t candidate_id;
+  float interval_scores[8];
+  float family_scores[8];
+  float priority_score, cost_score, uncertainty_score;
+  uint32_t pad0;
+} p2c_proposal_output;
+
+/* ExactWorkItem (common/runtime_contracts.h:67-81), 80 bytes. */
+typedef struct p2c_exact_work_item {
+  uint64_t work_item_id, parent_candidate_id, query_id;
+  uint32_t slab_id, patch_a_id, patch_b_id, pad0;
+  double interval_t0, interval_t1;
+  uint32_t feature_family_mask, topk_feature_ids_offset;
+  uint16_t depth;
+  uint16_t pad1;
+  float priority_score;
+  uint8_t source;                /* ProposalSource: 0 raw, 1 refined, 2 fallback */
+  uint8_t pad2[7];
+} p2c_exact_work_item;
+
+/* ProposalSchedulingConfig (proposal/proposal_policy.h:13-23). */
+typedef struct p2c_scheduling_config {
+  uint64_t first_work_item_id;
+  uint32_t conservative_feature_family_mask;
+  uint32_t preserve_candidate_order;
+  double fallback_interval_t0, fallback_interval_t1;
+  float family_score_threshold, uncertainty_fallback_threshold, ood_abs_feature_threshold;
+  uint32_t pad0;
+} p2c_scheduling_config;
+
+/* ProposalScheduleStats (proposal/proposal_policy.h:25-36); monotonic_safe 0/1. */
+typedef struct p2c_schedule_stats {
+  uint64_t raw_candidate_count, proposal_output_count, work_item_count, fallback_count;
+  uint64_t missing_proposal_fallback_count, invalid_proposal_fallback_count, ood_fallback_count;
+  uint64_t high_uncertainty_fallback_count, reordered_count, monotonic_safe;
+} p2c_schedule_stats;
+
+size_t p2c_schedule_work_items_workspace_bytes(int64_t n_candidates, int64_t n_rows, int64_t n_outputs);
+
+/* The ordered exact work queue from proposals.  mode 0:
+ * ScheduleRuntimeExactWorkItemsFromProposals (proposal/proposal_policy.cpp:
+ * 595-742): per candidate its feature row and proposal output found by
+ * candidate id; mode 1: the binding's aligned-array form (bindings/
+ * py_module.cpp:1088-1174): rows and outputs at the same position, the
+ * candidate fields from the row and a fallback priority of features[3].  A
+ * candidate falls back (conservative family mask, rt-hit priority, source
+ * fallback) on a missing, invalid, out-of-distribution or high-uncertainty
+ * proposal; otherwise it takes the predicted families and the proposal's
+ * priority (source refined).  Unless preserve_candidate_order, the queue is
+ * stable-sorted by priority, descending; work item ids count up from
+ * first_work_item_id in queue order.  The config is checked on the host
+ * (the reference's messages); *error_dev bits: 1 a candidate fails
+ * ValidateCandidateRecord, 2 a row id is zero or repeated, 4 an output id is
+ * zero or repeated, 8 repeated candidate ids, 16 a work item fails
+ * ValidateExactWorkItem, 32 a work item has no exact family, 64 unknown
+ * family bits (mode 0), 128 aligned arrays out of candidate order (mode 1);
+ * error_dev[1] / [2]: the first queue position with no family / with unknown
+ * bits (~0 if none; the reference reports the earlier one).  Family masks per
+ * query: n_masks ascending query ids with their masks.  No host sync. */
+int p2c_schedule_work_items(int mode, const p2c_candidate_record* candidates_dev, int64_t n_candidates,
+                            const p2c_proposal_feature_row* rows_dev, int64_t n_rows,
+                            const p2c_proposal_output* outputs_dev, int64_t n_outputs,
+                            const uint64_t* mask_query_ids_dev, const uint32_t* masks_dev, int64_t n_masks,
+                            const p2c_scheduling_config* config, p2c_exact_work_item* items_dev,
+                            p2c_schedule_stats* stats_dev, uint64_t* error_dev, void* workspace_dev,
+                            size_t workspace_bytes, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

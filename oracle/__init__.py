@@ -918,3 +918,133 @@ def audit_rows(items, certs, first_event_id=1, first_timestamp_us=1, emit_dequeu
         for k, v in zip(AUDIT_ROW_DTYPE.names, r):
             o[k] = v
     return out
+
+
+
+# ---- runtime exact work queue from proposals (proposal_policy.cpp:595-742) ----
+
+SCHED_DEFAULTS = dict(first_work_item_id=1, conservative_feature_family_mask=3, fallback_interval_t0=0.0,
+                      fallback_interval_t1=1.0, family_score_threshold=0.5, uncertainty_fallback_threshold=0.95,
+                      ood_abs_feature_threshold=1.0e5, preserve_candidate_order=False)
+
+
+def ref_schedule_runtime(cand, rows, outs, masks=None, **cfg):
+    """The reference's ScheduleRuntimeExactWorkItemsFromProposals: (work items
+    as EXACT_WORK_ITEM_DTYPE records, stats as SCHEDULE_STATS_DTYPE)."""
+    from p2cccd_b200.records import EXACT_WORK_ITEM_DTYPE, SCHEDULE_STATS_DTYPE
+
+    c = dict(SCHED_DEFAULTS, **cfg)
+    R = ref()
+    if not hasattr(R, "_sched_ready"):
+        vp, i64, f32, f64 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_float, ctypes.c_double
+        R.ref_schedule_runtime.argtypes = [vp, i64, vp, i64, vp, i64, vp, vp, i64, ctypes.c_uint64, ctypes.c_uint32,
+                                           f64, f64, f32, f32, f32, ctypes.c_int, vp, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._sched_ready = True
+    cand, rows, outs = (np.ascontiguousarray(x) for x in (cand, rows, outs))
+    keys = np.array(sorted((masks or {}).keys()), np.uint64)
+    vals = np.array([masks[int(k)] for k in keys], np.uint32)
+    items = np.zeros(max(1, len(cand)), EXACT_WORK_ITEM_DTYPE)
+    stats = np.zeros(1, SCHEDULE_STATS_DTYPE)
+    if R.ref_schedule_runtime(_p(cand), len(cand), _p(rows), len(rows), _p(outs), len(outs),
+                              _p(keys) if len(keys) else None, _p(vals) if len(vals) else None, len(keys),
+                              c["first_work_item_id"], c["conservative_feature_family_mask"],
+                              c["fallback_interval_t0"], c["fallback_interval_t1"], c["family_score_threshold"],
+                              c["uncertainty_fallback_threshold"], c["ood_abs_feature_threshold"],
+                              1 if c["preserve_candidate_order"] else 0, _p(items), _p(stats)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    return items[:len(cand)], stats[0]
+
+
+def schedule_runtime(cand, rows, outs, masks=None, mode=0, **cfg):
+    """Restatement of ScheduleRuntimeExactWorkItemsFromProposals
+    (proposal_policy.cpp:595-742; mode 0) and of the binding's aligned-array
+    form (py_module.cpp:1088-1174; mode 1: rows / outputs paired by position,
+    candidate fields from the row, fallback priority features[3]).  Returns
+    (work items, stats) or raises ValueError."""
+    from p2cccd_b200.records import EXACT_WORK_ITEM_DTYPE, SCHEDULE_STATS_DTYPE
+
+    c = dict(SCHED_DEFAULTS, **cfg)
+    f32 = np.float32
+    def fin(x):
+        return bool(np.isfinite(x))
+    def invalid(o):
+        vals = list(o["interval_scores"]) + list(o["family_scores"]) + [o["priority_score"], o["cost_score"],
+                                                                       o["uncertainty_score"]]
+        return int(o["candidate_id"]) == 0 or not all(fin(v) for v in vals) or o["cost_score"] < 0 or \
+            o["uncertainty_score"] < 0
+    def ood(r):
+        return r is None or any((not fin(v)) or abs(f32(v)) > f32(c["ood_abs_feature_threshold"]) for v in r["features"])
+    n = len(cand) if mode == 0 else len(rows)
+    if mode == 0:
+        rows_by = {}
+        for r in rows:
+            if int(r["candidate_id"]) == 0 or int(r["candidate_id"]) in rows_by:
+                raise ValueError("proposal feature row candidate_id zero or repeated")
+            rows_by[int(r["candidate_id"])] = r
+        outs_by = {}
+        for o in outs:
+            if int(o["candidate_id"]) == 0 or int(o["candidate_id"]) in outs_by:
+                raise ValueError("proposal output candidate_id zero or repeated")
+            outs_by[int(o["candidate_id"])] = o
+    stats = np.zeros(1, SCHEDULE_STATS_DTYPE)[0]
+    items = np.zeros(n, EXACT_WORK_ITEM_DTYPE)
+    for i in range(n):
+        if mode == 0:
+            cd = cand[i]
+            ok = cd["schema_version"] == 1 and cd["candidate_id"] and cd["query_id"] and \
+                cd["proxy_type_a"] in (1, 2) and cd["proxy_type_b"] in (1, 2) and cd["rt_hit_count"] and \
+                all(fin(v) and v >= 0 for v in cd["motion_bound"])
+            if not ok:
+                raise ValueError("invalid CandidateRecord")
+            src = cd
+            r, o = rows_by.get(int(cd["candidate_id"])), outs_by.get(int(cd["candidate_id"]))
+            fb_prio = f32(int(cd["rt_hit_count"]))
+        else:
+            r, o = rows[i], outs[i]
+            if int(r["candidate_id"]) == 0 or int(o["candidate_id"]) != int(r["candidate_id"]):
+                raise ValueError("proposal arrays must preserve candidate_id order")
+            src = r
+            fb_prio = f32(r["features"][3])
+        miss = o is None
+        inv = not miss and invalid(o)
+        od = ood(r)
+        unc = not miss and fin(o["uncertainty_score"]) and f32(o["uncertainty_score"]) >= f32(c["uncertainty_fallback_threshold"])
+        fb = miss or inv or od or unc
+        stats["fallback_count"] += fb
+        stats["missing_proposal_fallback_count"] += miss
+        stats["invalid_proposal_fallback_count"] += inv
+        stats["ood_fallback_count"] += od
+        stats["high_uncertainty_fallback_count"] += unc
+        base = (masks or {}).get(int(src["query_id"]), 0) or c["conservative_feature_family_mask"]
+        it = items[i]
+        it["parent_candidate_id"], it["query_id"] = src["candidate_id"], src["query_id"]
+        it["slab_id"], it["patch_a_id"], it["patch_b_id"] = src["slab_id"], src["patch_a_id"], src["patch_b_id"]
+        it["interval_t0"], it["interval_t1"] = c["fallback_interval_t0"], c["fallback_interval_t1"]
+        it["feature_family_mask"], it["priority_score"], it["source"] = base, fb_prio, 2
+        if not fb:
+            pred = (1 if f32(o["family_scores"][0]) >= f32(c["family_score_threshold"]) else 0) | \
+                (2 if f32(o["family_scores"][1]) >= f32(c["family_score_threshold"]) else 0)
+            it["feature_family_mask"], it["priority_score"], it["source"] = base | pred, o["priority_score"], 1
+    if not c["preserve_candidate_order"]:
+        order = sorted(range(n), key=lambda k: -float(items[k]["priority_score"]))  # stable
+        items = items[order]
+    originals = (cand if mode == 0 else rows)["candidate_id"]
+    for i in range(n):
+        items[i]["work_item_id"] = c["first_work_item_id"] + i
+        stats["reordered_count"] += int(items[i]["parent_candidate_id"] != originals[i])
+        if not (items[i]["parent_candidate_id"] and items[i]["query_id"] and items[i]["feature_family_mask"]
+                and fin(items[i]["priority_score"])):
+            raise ValueError("invalid ExactWorkItem")
+    if mode == 0:
+        if len(set(int(x) for x in cand["candidate_id"])) != n:
+            raise ValueError("runtime candidates contain duplicate candidate_id")
+        for it in items:
+            if not int(it["feature_family_mask"]) & 3 or int(it["feature_family_mask"]) & 0xFFFFFFFC:
+                raise ValueError("runtime scheduled work item family bits")
+    stats["raw_candidate_count"], stats["proposal_output_count"], stats["work_item_count"] = n, len(outs), n
+    stats["monotonic_safe"] = 1
+    clean = np.zeros(n, EXACT_WORK_ITEM_DTYPE)  # zero padding between the fields
+    for k in EXACT_WORK_ITEM_DTYPE.names:
+        clean[k] = items[k]
+    return clean, stats

@@ -32,6 +32,11 @@ static_assert(offsetof(p2cccd::CandidateRecord, rt_hit_count) == offsetof(p2c_ca
 static_assert(offsetof(p2cccd::CandidateRecord, flags) == offsetof(p2c_candidate_record, flags));
 static_assert(offsetof(p2cccd::RawCandidateHit, motion_bound) == offsetof(p2c_raw_candidate_hit, motion_bound));
 static_assert(sizeof(p2cccd::ProposalFeatureRow) == sizeof(p2c_proposal_feature_row));
+static_assert(sizeof(p2cccd::ProposalOutput) == sizeof(p2c_proposal_output));
+static_assert(offsetof(p2cccd::ProposalOutput, uncertainty_score) == offsetof(p2c_proposal_output, uncertainty_score));
+static_assert(sizeof(p2cccd::ExactWorkItem) == sizeof(p2c_exact_work_item));
+static_assert(offsetof(p2cccd::ExactWorkItem, source) == offsetof(p2c_exact_work_item, source));
+static_assert(offsetof(p2cccd::ExactWorkItem, priority_score) == offsetof(p2c_exact_work_item, priority_score));
 static_assert(offsetof(p2cccd::ProposalFeatureRow, features) == offsetof(p2c_proposal_feature_row, features));
 static_assert(offsetof(p2cccd::ProposalFeatureRow, target_mask) == offsetof(p2c_proposal_feature_row, target_mask));
 
@@ -269,6 +274,64 @@ int ref_runtime_feature_rows(const p2c_candidate_record* cands, int64_t n, uint6
     std::memcpy(rows + i, &out[static_cast<std::size_t>(i)], sizeof(p2c_proposal_feature_row));
     rows[i].pad0 = rows[i].pad1 = 0;
   }
+  return 0;
+}
+
+// ScheduleRuntimeExactWorkItemsFromProposals on candidate / row / output
+// records, a query id -> family mask map and the config fields.
+int ref_schedule_runtime(const p2c_candidate_record* cands, int64_t n, const p2c_proposal_feature_row* rows,
+                         int64_t n_rows, const p2c_proposal_output* outs, int64_t n_outs, const uint64_t* mask_qids,
+                         const uint32_t* masks, int64_t n_masks, uint64_t first_work_item_id, uint32_t conservative,
+                         double t0, double t1, float family_threshold, float uncertainty_threshold,
+                         float ood_threshold, int preserve, p2c_exact_work_item* items_out, uint64_t* stats_out) {
+  std::vector<p2cccd::CandidateRecord> cand(static_cast<std::size_t>(n));
+  for (int64_t i = 0; i < n; ++i) std::memcpy(&cand[static_cast<std::size_t>(i)], cands + i, sizeof(p2c_candidate_record));
+  std::vector<p2cccd::ProposalFeatureRow> rv(static_cast<std::size_t>(n_rows));
+  for (int64_t i = 0; i < n_rows; ++i) std::memcpy(&rv[static_cast<std::size_t>(i)], rows + i, sizeof(p2c_proposal_feature_row));
+  std::vector<p2cccd::ProposalOutput> ov(static_cast<std::size_t>(n_outs));
+  for (int64_t i = 0; i < n_outs; ++i) std::memcpy(&ov[static_cast<std::size_t>(i)], outs + i, sizeof(p2c_proposal_output));
+  std::unordered_map<std::uint64_t, std::uint32_t> mask_map;
+  for (int64_t i = 0; i < n_masks; ++i) mask_map[mask_qids[i]] = masks[i];
+  p2cccd::ProposalSchedulingConfig cfg;
+  cfg.first_work_item_id = first_work_item_id;
+  cfg.conservative_feature_family_mask = conservative;
+  cfg.fallback_interval_t0 = t0;
+  cfg.fallback_interval_t1 = t1;
+  cfg.family_score_threshold = family_threshold;
+  cfg.uncertainty_fallback_threshold = uncertainty_threshold;
+  cfg.ood_abs_feature_threshold = ood_threshold;
+  cfg.preserve_candidate_order = preserve != 0;
+  std::vector<p2cccd::ExactWorkItem> queue;
+  p2cccd::ProposalScheduleStats st;
+  const p2cccd::Status status =
+      p2cccd::ScheduleRuntimeExactWorkItemsFromProposals(cand, rv, ov, mask_map, cfg, &queue, &st);
+  if (!status.ok) {
+    g_proxy_error = status.message;
+    return 1;
+  }
+  for (std::size_t i = 0; i < queue.size(); ++i) {
+    std::memset(items_out + i, 0, sizeof(p2c_exact_work_item));
+    const p2cccd::ExactWorkItem& w = queue[i];
+    p2c_exact_work_item& o = items_out[i];
+    o.work_item_id = w.work_item_id;
+    o.parent_candidate_id = w.parent_candidate_id;
+    o.query_id = w.query_id;
+    o.slab_id = w.slab_id;
+    o.patch_a_id = w.patch_a_id;
+    o.patch_b_id = w.patch_b_id;
+    o.interval_t0 = w.interval_t0;
+    o.interval_t1 = w.interval_t1;
+    o.feature_family_mask = w.feature_family_mask;
+    o.topk_feature_ids_offset = w.topk_feature_ids_offset;
+    o.depth = w.depth;
+    o.priority_score = w.priority_score;
+    o.source = static_cast<uint8_t>(w.source);
+  }
+  const uint64_t s[10] = {st.raw_candidate_count, st.proposal_output_count, st.work_item_count, st.fallback_count,
+                          st.missing_proposal_fallback_count, st.invalid_proposal_fallback_count,
+                          st.ood_fallback_count, st.high_uncertainty_fallback_count, st.reordered_count,
+                          st.monotonic_safe ? 1u : 0u};
+  std::memcpy(stats_out, s, sizeof(s));
   return 0;
 }
 

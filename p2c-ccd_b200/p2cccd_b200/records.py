@@ -169,3 +169,28 @@ AUDIT_ROW_DTYPE = np.dtype({
     "offsets": [0, 8, 16, 24, 32, 34, 36, 40, 48, 56, 64, 72],
     "itemsize": 80,
 })
+
+
+# ProposalOutput (common/runtime_contracts.h:58-65), 88 bytes
+PROPOSAL_OUTPUT_DTYPE = np.dtype({
+    "names": ["candidate_id", "interval_scores", "family_scores", "priority_score", "cost_score",
+              "uncertainty_score"],
+    "formats": ["<u8", ("<f4", (8,)), ("<f4", (8,)), "<f4", "<f4", "<f4"],
+    "offsets": [0, 8, 40, 72, 76, 80],
+    "itemsize": 88,
+})
+
+# ExactWorkItem (common/runtime_contracts.h:67-81), 80 bytes
+EXACT_WORK_ITEM_DTYPE = np.dtype({
+    "names": ["work_item_id", "parent_candidate_id", "query_id", "slab_id", "patch_a_id", "patch_b_id",
+              "interval_t0", "interval_t1", "feature_family_mask", "topk_feature_ids_offset", "depth",
+              "priority_score", "source"],
+    "formats": ["<u8", "<u8", "<u8", "<u4", "<u4", "<u4", "<f8", "<f8", "<u4", "<u4", "<u2", "<f4", "u1"],
+    "offsets": [0, 8, 16, 24, 28, 32, 40, 48, 56, 60, 64, 68, 72],
+    "itemsize": 80,
+})
+
+SCHEDULE_STATS_FIELDS = ("raw_candidate_count", "proposal_output_count", "work_item_count", "fallback_count",
+                         "missing_proposal_fallback_count", "invalid_proposal_fallback_count", "ood_fallback_count",
+                         "high_uncertainty_fallback_count", "reordered_count", "monotonic_safe")
+SCHEDULE_STATS_DTYPE = np.dtype([(k, "<u8") for k in SCHEDULE_STATS_FIELDS])

@@ -1228,3 +1228,145 @@ def extract_proposal_feature_rows(scene, generation_result) -> list:
         raise ValueError("generation_result candidates do not belong to this scene")
     _, rows = pc.feature_rows()
     return _row_objects(rows)
+
+
+# ---------------------------------------------------------------------------
+# the runtime exact work queue from proposals (proposal_policy.cpp:595-742, py_module.cpp:1035-1174, 1918-1937)
+
+
+class ProposalOutput(_Struct):  # runtime_contracts.h:58-65
+    _fields = (("candidate_id", 0), ("interval_scores", lambda: [0.0] * 8), ("family_scores", lambda: [0.0] * 8),
+               ("priority_score", 0.0), ("cost_score", 0.0), ("uncertainty_score", 0.0))
+
+
+class ProposalSchedulingConfig(_Struct):  # proposal_policy.h:13-23
+    _fields = (("first_work_item_id", 1), ("conservative_feature_family_mask", 3), ("fallback_interval_t0", 0.0),
+               ("fallback_interval_t1", 1.0), ("family_score_threshold", 0.5),
+               ("uncertainty_fallback_threshold", 0.95), ("ood_abs_feature_threshold", 1.0e5),
+               ("preserve_candidate_order", False))
+
+
+class ProposalScheduleStats(_Struct):  # proposal_policy.h:25-36
+    _fields = (("raw_candidate_count", 0), ("proposal_output_count", 0), ("work_item_count", 0),
+               ("fallback_count", 0), ("missing_proposal_fallback_count", 0), ("invalid_proposal_fallback_count", 0),
+               ("ood_fallback_count", 0), ("high_uncertainty_fallback_count", 0), ("reordered_count", 0),
+               ("monotonic_safe", False))
+
+
+def _row_array(rows) -> np.ndarray:
+    from p2cccd_b200.records import FEATURE_ROW_DTYPE
+
+    if isinstance(rows, np.ndarray):
+        return np.ascontiguousarray(rows, dtype=FEATURE_ROW_DTYPE)
+    out = np.zeros(len(rows), FEATURE_ROW_DTYPE)
+    for r, o in zip(out, rows):
+        for k in ("schema_version", "query_id", "candidate_id", "slab_id", "object_a_id", "patch_a_id",
+                  "object_b_id", "patch_b_id", "priority_target", "cost_target", "uncertainty_target",
+                  "target_mask"):
+            r[k] = getattr(o, k)
+        for k, m in (("features", 32), ("interval_targets", 8), ("family_targets", 8)):
+            v = list(getattr(o, k))
+            if len(v) != m:
+                raise ValueError(f"ProposalFeatureRow.{k} must have length {m}")
+            r[k] = v
+    return out
+
+
+def _output_array(outputs) -> np.ndarray:
+    from p2cccd_b200.records import PROPOSAL_OUTPUT_DTYPE
+
+    out = np.zeros(len(outputs), PROPOSAL_OUTPUT_DTYPE)
+    for r, o in zip(out, outputs):
+        r["candidate_id"] = int(o.candidate_id)
+        for k in ("interval_scores", "family_scores"):
+            v = list(getattr(o, k))
+            if len(v) != 8:
+                raise ValueError(f"ProposalOutput.{k} must have length 8")
+            r[k] = v
+        r["priority_score"], r["cost_score"], r["uncertainty_score"] = o.priority_score, o.cost_score, \
+            o.uncertainty_score
+    return out
+
+
+def _require(arrays: dict, key: str, shape: tuple, dtype) -> np.ndarray:  # py_module.cpp:756-790
+    if key not in arrays:
+        raise ValueError(f"missing or invalid array field: {key}")
+    a = np.ascontiguousarray(arrays[key], dtype=dtype)
+    if a.shape != shape:
+        raise ValueError(f"{key} must have shape [{', '.join(str(x) for x in shape)}]")
+    return a
+
+
+def _rows_from_arrays(fa: dict) -> np.ndarray:  # ParseProposalFeatureRowsFromArrays, :792-852
+    from p2cccd_b200.records import FEATURE_ROW_DTYPE
+
+    n = len(fa["query_id"])
+    out = np.zeros(n, FEATURE_ROW_DTYPE)
+    out["schema_version"] = int(fa["schema_version"])
+    for k, dt in (("candidate_id", np.uint64), ("query_id", np.uint64), ("slab_id", np.uint32),
+                  ("object_a_id", np.uint32), ("patch_a_id", np.uint32), ("object_b_id", np.uint32),
+                  ("patch_b_id", np.uint32), ("priority_target", np.float32), ("cost_target", np.float32),
+                  ("uncertainty_target", np.float32), ("target_mask", np.uint32)):
+        out[k] = _require(fa, k, (n,), dt)
+    for k, m in (("features", 32), ("interval_targets", 8), ("family_targets", 8)):
+        out[k] = _require(fa, k, (n, m), np.float32)
+    return out
+
+
+def _outputs_from_arrays(fa: dict, pa: dict) -> np.ndarray:  # ParseProposalOutputsFromArrays, :853-890
+    from p2cccd_b200.records import PROPOSAL_OUTPUT_DTYPE
+
+    n = len(fa["query_id"])
+    out = np.zeros(n, PROPOSAL_OUTPUT_DTYPE)
+    out["candidate_id"] = _require(fa, "candidate_id", (n,), np.uint64)
+    for k in ("interval_scores", "family_scores"):
+        out[k] = _require(pa, k, (n, 8), np.float32)
+    for k in ("priority_score", "cost_score", "uncertainty_score"):
+        out[k] = _require(pa, k, (n,), np.float32)
+    return out
+
+
+def _schedule(cand, rows, outs, masks, config, mode) -> tuple:
+    from p2cccd_b200.schedule import schedule_work_items
+
+    cfg = {k: getattr(config, k) for k, _ in ProposalSchedulingConfig._fields}
+    items, stats = schedule_work_items(cand, rows, outs, dict(masks or {}), mode, **cfg)
+    queue = []
+    for r in items:
+        w = ExactWorkItem()
+        for k in ("work_item_id", "parent_candidate_id", "query_id", "slab_id", "patch_a_id", "patch_b_id",
+                  "feature_family_mask", "topk_feature_ids_offset", "depth"):
+            setattr(w, k, int(r[k]))
+        w.interval_t0, w.interval_t1 = float(r["interval_t0"]), float(r["interval_t1"])
+        w.priority_score = float(r["priority_score"])
+        w.source = ProposalSource(int(r["source"]))
+        queue.append(w)
+    st = ProposalScheduleStats()
+    for k, _ in ProposalScheduleStats._fields:
+        setattr(st, k, bool(stats[k]) if k == "monotonic_safe" else int(stats[k]))
+    return queue, st
+
+
+def schedule_runtime_exact_work_items(candidates, rows, proposal_outputs, conservative_family_masks_by_query_id,
+                                      config: ProposalSchedulingConfig) -> tuple:  # py_module.cpp:1035-1059
+    """ScheduleRuntimeExactWorkItemsFromProposals on the GPU: (work queue, stats)."""
+    return _schedule(_candidate_array(candidates), _row_array(rows), _output_array(proposal_outputs),
+                     conservative_family_masks_by_query_id, config, 0)
+
+
+def schedule_runtime_exact_work_items_from_arrays(candidates, feature_arrays, prediction_arrays,
+                                                  conservative_family_masks_by_query_id,
+                                                  config: ProposalSchedulingConfig) -> tuple:  # :1061-1086
+    return _schedule(_candidate_array(candidates), _rows_from_arrays(feature_arrays),
+                     _outputs_from_arrays(feature_arrays, prediction_arrays), conservative_family_masks_by_query_id,
+                     config, 0)
+
+
+def schedule_runtime_exact_work_items_from_proposal_arrays(feature_arrays, prediction_arrays,
+                                                           conservative_family_masks_by_query_id,
+                                                           config: ProposalSchedulingConfig) -> tuple:  # :1088-1174
+    rows = _rows_from_arrays(feature_arrays)
+    outs = _outputs_from_arrays(feature_arrays, prediction_arrays)
+    if len(rows) != len(outs):
+        raise ValueError("feature row and proposal output array lengths must match")
+    return _schedule(None, rows, outs, conservative_family_masks_by_query_id, config, 1)

@@ -425,3 +425,98 @@ def test_mirror_queue_audit_log_matches_reference(cuda_device, oracle_mod):
                                                              "stage", "action", "depth", "timestamp_us"))
         assert (o.interval_t0, o.interval_t1, o.aux_value0, o.aux_value1) == \
             tuple(float(r[k]) for k in ("interval_t0", "interval_t1", "aux_value0", "aux_value1"))
+
+
+@pytest.mark.parametrize("cfg", [{}, {"preserve_candidate_order": True}, {"family_score_threshold": 0.6,
+                                                                           "uncertainty_fallback_threshold": 0.5,
+                                                                           "first_work_item_id": 1000,
+                                                                           "conservative_feature_family_mask": 2,
+                                                                           "fallback_interval_t0": 0.25,
+                                                                           "fallback_interval_t1": 0.75}])
+def test_device_schedule_matches_reference(cuda_device, oracle_mod, cfg):
+    """p2c_schedule_work_items: every 80-byte ExactWorkItem and the stats equal
+    to the reference's ScheduleRuntimeExactWorkItemsFromProposals (candidate
+    form), and the aligned-array form equal to it on paired inputs."""
+    from p2cccd_b200.schedule import schedule_work_items
+    from sched_inputs import make_inputs
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    cand, rows, outs, outs_all = make_inputs()
+    masks = {7: 1, 99: 2}
+    ref_items, ref_stats = oracle_mod.ref_schedule_runtime(cand, rows, outs, masks, **cfg)
+    items, stats = schedule_work_items(cand, rows, outs, masks, 0, cuda_device, **cfg)
+    assert np.array_equal(items.view(np.uint8), ref_items.view(np.uint8))
+    assert stats.tobytes() == ref_stats.tobytes()
+    ref_items, ref_stats = oracle_mod.ref_schedule_runtime(cand, rows, outs_all, masks, **cfg)
+    items, stats = schedule_work_items(None, rows, outs_all, masks, 1, cuda_device, **cfg)
+    assert np.array_equal(items.view(np.uint8), ref_items.view(np.uint8))
+    assert stats.tobytes() == ref_stats.tobytes()
+
+
+def test_device_schedule_rejections(cuda_device, oracle_mod):
+    from p2cccd_b200.schedule import schedule_work_items
+    from sched_inputs import make_inputs
+
+    cand, rows, outs, outs_all = make_inputs(seed=5)
+    cases = []
+    bad = rows.copy(); bad["candidate_id"][1] = bad["candidate_id"][0]; cases.append((cand, bad, outs, {}, "rows"))
+    bad = outs.copy(); bad["candidate_id"][2] = 0; cases.append((cand, rows, bad, {}, "outputs"))
+    bad = cand.copy(); bad["rt_hit_count"][4] = 0; cases.append((bad, rows, outs, {}, "CandidateRecord"))
+    bad = cand.copy(); bad["candidate_id"][5] = bad["candidate_id"][6]; cases.append((bad, rows, outs, {}, "duplicate"))
+    cases.append((cand, rows, outs, {7: 4}, "feature family"))
+    cases.append((cand, rows, outs, {7: 5}, "feature-family bits"))
+    for c, r, o, m, msg in cases:
+        with pytest.raises(ValueError, match=msg):
+            schedule_work_items(c, r, o, m, 0, cuda_device)
+        if oracle_mod.ref_available() and "family" in msg:  # the reference's own message for the same input
+            with pytest.raises(ValueError) as ref_err:
+                oracle_mod.ref_schedule_runtime(c, r, o, m)
+            with pytest.raises(ValueError) as dev_err:
+                schedule_work_items(c, r, o, m, 0, cuda_device)
+            assert str(dev_err.value) == str(ref_err.value)
+    swapped = outs_all.copy()
+    swapped[[0, 1]] = swapped[[1, 0]]
+    with pytest.raises(ValueError, match="preserve candidate_id order"):
+        schedule_work_items(None, rows, swapped, {}, 1, cuda_device)
+    with pytest.raises(ValueError, match="ood_abs_feature_threshold"):
+        schedule_work_items(cand, rows, outs, {}, 0, cuda_device, ood_abs_feature_threshold=0.0)
+
+
+def test_mirror_schedule_functions(cuda_device, oracle_mod):
+    import p2cccd_cpp as cpp
+    from sched_inputs import make_inputs
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    cand, rows, outs, outs_all = make_inputs(seed=6)
+    masks = {7: 2}
+    ref_items, ref_stats = oracle_mod.ref_schedule_runtime(cand, rows, outs, masks)
+    cfg = cpp.ProposalSchedulingConfig()
+    cand_objs = cpp._candidate_objects(cand)
+    row_objs = cpp._row_objects(rows)
+    out_objs = []
+    for r in outs:
+        o = cpp.ProposalOutput()
+        o.candidate_id, o.interval_scores, o.family_scores = int(r["candidate_id"]), r["interval_scores"].tolist(), \
+            r["family_scores"].tolist()
+        o.priority_score, o.cost_score, o.uncertainty_score = (float(r[k]) for k in ("priority_score", "cost_score",
+                                                                                     "uncertainty_score"))
+        out_objs.append(o)
+    queue, stats = cpp.schedule_runtime_exact_work_items(cand_objs, row_objs, out_objs, masks, cfg)
+    assert [w.parent_candidate_id for w in queue] == [int(x) for x in ref_items["parent_candidate_id"]]
+    assert [int(w.source) for w in queue] == [int(x) for x in ref_items["source"]]
+    assert stats.fallback_count == int(ref_stats["fallback_count"]) and stats.monotonic_safe
+    fa = cpp.build_runtime_proposal_feature_arrays(cand_objs, 100, 200, len(cand), masks)
+    fa["features"] = rows["features"]  # the test rows (with out-of-distribution features)
+    pa = {k: outs_all[k] for k in ("interval_scores", "family_scores", "priority_score", "cost_score",
+                                   "uncertainty_score")}
+    ref2, _ = oracle_mod.ref_schedule_runtime(cand, rows, outs_all, masks)
+    q2, _ = cpp.schedule_runtime_exact_work_items_from_arrays(cand_objs, fa, pa, masks, cfg)
+    assert [w.parent_candidate_id for w in q2] == [int(x) for x in ref2["parent_candidate_id"]]
+    q3, s3 = cpp.schedule_runtime_exact_work_items_from_proposal_arrays(fa, pa, masks, cfg)
+    assert [(w.parent_candidate_id, w.feature_family_mask, w.priority_score) for w in q3] == \
+        [(int(r["parent_candidate_id"]), int(r["feature_family_mask"]), float(r["priority_score"])) for r in ref2]
+    with pytest.raises(ValueError, match="must have shape"):
+        cpp.schedule_runtime_exact_work_items_from_proposal_arrays(fa, dict(pa, priority_score=pa["priority_score"][:-1]),
+                                                                   masks, cfg)

@@ -335,3 +335,64 @@ def test_audit_rows_restatement_matches_reference(oracle_mod, emit):
     assert (certs["reason_code"] == 3).sum() == 1  # the NaN primitive's item
     mine = oracle_mod.audit_rows(items, certs, 500, 800, emit)
     assert np.array_equal(mine.view(np.uint8), rows.view(np.uint8))
+
+
+# ---- runtime exact work queue from proposals ---------------------------------
+
+@pytest.mark.parametrize("cfg", [{}, {"preserve_candidate_order": True}, {"family_score_threshold": 0.6,
+                                                                           "uncertainty_fallback_threshold": 0.5,
+                                                                           "first_work_item_id": 1000,
+                                                                           "conservative_feature_family_mask": 2,
+                                                                           "fallback_interval_t0": 0.25,
+                                                                           "fallback_interval_t1": 0.75}])
+def test_schedule_restatement_matches_reference(oracle_mod, cfg):
+    from sched_inputs import make_inputs
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    cand, rows, outs, _ = make_inputs()
+    masks = {7: 1, 99: 2}
+    ref_items, ref_stats = oracle_mod.ref_schedule_runtime(cand, rows, outs, masks, **cfg)
+    items, stats = oracle_mod.schedule_runtime(cand, rows, outs, masks, 0, **cfg)
+    assert np.array_equal(items.view(np.uint8), ref_items.view(np.uint8))
+    assert stats.tobytes() == ref_stats.tobytes()
+    assert ref_stats["missing_proposal_fallback_count"] == 6 and ref_stats["invalid_proposal_fallback_count"] >= 5
+    assert ref_stats["ood_fallback_count"] >= 3 and ref_stats["high_uncertainty_fallback_count"] > 0
+    if not cfg.get("preserve_candidate_order"):
+        assert ref_stats["reordered_count"] > 0
+
+
+def test_aligned_schedule_equals_candidate_schedule(oracle_mod):
+    """The binding's aligned-array form on rows whose features[3] is the hit
+    count (runtime rows) and outputs paired with them gives the reference's
+    candidate-form queue."""
+    from sched_inputs import make_inputs
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    cand, rows, _, outs_all = make_inputs(seed=4)
+    ref_items, ref_stats = oracle_mod.ref_schedule_runtime(cand, rows, outs_all, {})
+    items, stats = oracle_mod.schedule_runtime(cand, rows, outs_all, {}, 1)
+    assert np.array_equal(items.view(np.uint8), ref_items.view(np.uint8))
+    assert stats.tobytes() == ref_stats.tobytes()
+
+
+def test_schedule_rejections_match_reference(oracle_mod):
+    from sched_inputs import make_inputs
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    cand, rows, outs, _ = make_inputs(seed=5)
+    cases = []
+    bad = rows.copy(); bad["candidate_id"][1] = bad["candidate_id"][0]; cases.append((cand, bad, outs, {}))
+    bad = outs.copy(); bad["candidate_id"][2] = 0; cases.append((cand, rows, bad, {}))
+    bad = cand.copy(); bad["rt_hit_count"][4] = 0; cases.append((bad, rows, outs, {}))
+    bad = cand.copy(); bad["candidate_id"][5] = bad["candidate_id"][6]; cases.append((bad, rows, outs, {}))
+    cases.append((cand, rows, outs, {7: 4}))  # unknown family bit
+    for c, r, o, m in cases:
+        with pytest.raises(ValueError):
+            oracle_mod.ref_schedule_runtime(c, r, o, m)
+        with pytest.raises(ValueError):
+            oracle_mod.schedule_runtime(c, r, o, m, 0)
+    with pytest.raises(ValueError, match="first_work_item_id"):
+        oracle_mod.ref_schedule_runtime(cand, rows, outs, {}, first_work_item_id=0)
