@@ -1048,3 +1048,43 @@ def schedule_runtime(cand, rows, outs, masks=None, mode=0, **cfg):
     for k in EXACT_WORK_ITEM_DTYPE.names:
         clean[k] = items[k]
     return clean, stats
+
+
+
+# ---- external batch candidates (rt_candidate/external_batch_candidate.cpp) ----
+
+def _external_args(batch: dict):
+    n = len(batch["query_id"])
+    return (n, np.ascontiguousarray(batch["query_id"], np.uint64),
+            np.ascontiguousarray(batch["source_query_index"], np.uint32),
+            np.ascontiguousarray(batch["family"], np.uint8),
+            np.ascontiguousarray(batch["vertices_t0"], np.float64).reshape(n, 12),
+            np.ascontiguousarray(batch["vertices_t1"], np.float64).reshape(n, 12),
+            np.ascontiguousarray(batch["ground_truth"], np.int8), np.ascontiguousarray(batch["has_box"], np.uint8),
+            np.ascontiguousarray(batch["box_pair"], np.uint32).reshape(n, 2))
+
+
+def ref_external_batch(batch: dict):
+    """The reference's GenerateCandidatesForExternalBatch: (candidates,
+    runtime query ids, counts {primitives, raw hits, candidates}, recall)."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_ext_ready"):
+        vp = ctypes.c_void_p
+        R.ref_external_batch.argtypes = [ctypes.c_int64] + [vp] * 12
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._ext_ready = True
+    a = _external_args(batch)
+    n = a[0]
+    cand = np.zeros(max(1, n), CANDIDATE_RECORD_DTYPE)
+    rid = np.zeros(max(1, n), np.uint64)
+    counts = np.zeros(3, np.uint64)
+    recall = np.zeros(1, np.float64)
+    if R.ref_external_batch(n, *[_p(x) for x in a[1:]], _p(cand), _p(rid), _p(counts), _p(recall)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    cand = cand[:int(counts[2])]
+    clean = np.zeros(len(cand), cand.dtype)  # the reference struct's padding bytes are indeterminate
+    for f in cand.dtype.names:
+        clean[f] = cand[f]
+    return clean, rid[:n], counts, float(recall[0])

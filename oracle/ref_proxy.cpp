@@ -12,6 +12,7 @@
 #include "proposal/proposal_policy.h"
 #include "rt_candidate/candidate_buffer.h"
 #include "rt_candidate/candidate_stats.h"
+#include "rt_candidate/external_batch_candidate.h"
 #include "rt_candidate/proxy_scene.h"
 
 #include <algorithm>
@@ -332,6 +333,48 @@ int ref_schedule_runtime(const p2c_candidate_record* cands, int64_t n, const p2c
                           st.ood_fallback_count, st.high_uncertainty_fallback_count, st.reordered_count,
                           st.monotonic_safe ? 1u : 0u};
   std::memcpy(stats_out, s, sizeof(s));
+  return 0;
+}
+
+// GenerateCandidatesForExternalBatch (CPU reference backend) on n external
+// queries: family 0 vertex-face / 1 edge-edge, 4 vertices at t0 and t1
+// (n x 12 doubles each), ground truth -1 none / 0 / 1, box pairs (has_box
+// 0/1, n x 2 ids).  Outputs: candidates (capacity n), the runtime query id
+// of every query, counts {primitives, raw hits, candidates} and the recall.
+int ref_external_batch(int64_t n, const uint64_t* source_id, const uint32_t* source_index, const uint8_t* family,
+                       const double* v_t0, const double* v_t1, const int8_t* ground_truth, const uint8_t* has_box,
+                       const uint32_t* box_pair, p2c_candidate_record* cand_out, uint64_t* runtime_ids,
+                       uint64_t* counts, double* recall) {
+  std::vector<p2cccd::ExternalBatchQuery> queries(static_cast<std::size_t>(n));
+  for (int64_t k = 0; k < n; ++k) {
+    p2cccd::ExternalBatchQuery& q = queries[static_cast<std::size_t>(k)];
+    q.source_query_id = source_id[k];
+    q.source_query_index = source_index[k];
+    q.family = family[k] ? p2cccd::ExternalQueryFamily::kEdgeEdge : p2cccd::ExternalQueryFamily::kVertexFace;
+    for (int v = 0; v < 4; ++v)
+      for (int a = 0; a < 3; ++a) {
+        q.vertices_t0[v][a] = v_t0[12 * k + 3 * v + a];
+        q.vertices_t1[v][a] = v_t1[12 * k + 3 * v + a];
+      }
+    q.has_ground_truth = ground_truth[k] >= 0;
+    q.ground_truth_collides = ground_truth[k] > 0;
+    q.has_box_pair = has_box[k] != 0;
+    if (q.has_box_pair) q.box_pair = {box_pair[2 * k], box_pair[2 * k + 1]};
+  }
+  p2cccd::CandidateGeneratorConfig cfg;
+  p2cccd::ExternalBatchCandidateResult res;
+  const p2cccd::Status st = p2cccd::GenerateCandidatesForExternalBatch(queries, cfg, &res);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  for (std::size_t i = 0; i < res.candidates.size(); ++i)
+    std::memcpy(cand_out + i, &res.candidates[i], sizeof(p2c_candidate_record));
+  for (std::size_t i = 0; i < res.runtime_query_ids.size(); ++i) runtime_ids[i] = res.runtime_query_ids[i].runtime_query_id;
+  counts[0] = res.primitive_count;
+  counts[1] = res.raw_hit_count;
+  counts[2] = res.compact_candidate_count;
+  *recall = res.candidate_recall;
   return 0;
 }
 

@@ -1027,12 +1027,7 @@ def generate_candidates_for_proxy_scene(scene, query_id: int = 0, backend_name: 
     allow_optix_cpu_fallback the same generation named "optix_cpu_fallback"."""
     import time
 
-    if backend_name in ("cpu_reference", "cpu_reference_rt"):
-        name = "cpu_reference"
-    elif backend_name in ("optix", "optix_compatible", "optix_rt"):
-        name = "optix_cpu_fallback"
-    else:
-        raise ValueError("unsupported candidate backend: " + str(backend_name))
+    name = _backend(backend_name)
     start = time.perf_counter()
     a = _proxy_arrays(scene)
     qid = int(query_id) or int(a["query_id"])
@@ -1056,6 +1051,103 @@ def generate_candidates_for_proxy_scene(scene, query_id: int = 0, backend_name: 
     timing.stats_ms = (time.perf_counter() - t) * 1e3
     timing.total_ms = (time.perf_counter() - start) * 1e3
     res.timing = timing
+    return res
+
+
+class RuntimeQueryIdMapping(_Struct):  # rt_candidate/external_batch_candidate.h
+    _fields = (("source_query_id", 0), ("runtime_query_id", 0))
+
+
+class ExternalBatchCandidateResult(_Struct):  # py_module.cpp:1657-1667
+    _fields = (("backend_name", ""), ("timing", RtCandidateTiming), ("primitive_count", 0), ("raw_hit_count", 0),
+               ("compact_candidate_count", 0), ("candidate_recall", 0.0), ("candidates", list),
+               ("runtime_query_ids", list))
+
+
+def _vertex_array(v, field: str) -> list:  # ParseVertexArray, py_module.cpp:129-146
+    if len(v) != 4:
+        raise ValueError(field + " must contain four vertices")
+    out = []
+    for p in v:
+        if len(p) != 3:
+            raise ValueError(field + " vertices must be 3D")
+        out.append([float(x) for x in p])
+    return out
+
+
+def _external_batch(batch) -> dict:
+    """ParseExternalBatchQueries (py_module.cpp:148-181): ``batch.queries``
+    items with query_id, source_query_index, family ("vf" / "ee"),
+    vertices_t0 / vertices_t1 (4 x 3), ground_truth_collides (None or bool)
+    and box_pair (None or two ids).  A dict of column arrays
+    (``p2cccd_b200.external.batch_arrays``) passes through."""
+    from p2cccd_b200.external import batch_arrays
+
+    if isinstance(batch, dict):
+        return batch
+    qid, sidx, fam, v0, v1, gt, has, pairs = [], [], [], [], [], [], [], []
+    for item in batch.queries:
+        qid.append(int(item.query_id))
+        sidx.append(int(item.source_query_index))
+        f = str(item.family)
+        if f not in ("vf", "ee"):
+            raise ValueError("unsupported external CCD query family: " + f)
+        fam.append(0 if f == "vf" else 1)
+        v0.append(_vertex_array(item.vertices_t0, "vertices_t0"))
+        v1.append(_vertex_array(item.vertices_t1, "vertices_t1"))
+        g = item.ground_truth_collides
+        gt.append(-1 if g is None else int(bool(g)))
+        bp = item.box_pair
+        if bp is None:
+            has.append(0)
+            pairs.append((0, 0))
+        else:
+            if len(bp) != 2:
+                raise ValueError("box_pair must contain exactly two object ids")
+            has.append(1)
+            pairs.append((int(bp[0]), int(bp[1])))
+    n = len(qid)
+    return batch_arrays(np.array(qid, np.uint64), sidx, fam, np.array(v0, np.float64).reshape(n, 4, 3),
+                        np.array(v1, np.float64).reshape(n, 4, 3), gt, np.array(pairs, np.uint32).reshape(n, 2), has)
+
+
+def _backend(backend_name: str) -> str:  # ParseCandidateBackend
+    if backend_name in ("cpu_reference", "cpu_reference_rt"):
+        return "cpu_reference"
+    if backend_name in ("optix", "optix_compatible", "optix_rt"):
+        return "optix_cpu_fallback"
+    raise ValueError("unsupported candidate backend: " + str(backend_name))
+
+
+def generate_candidates_for_external_batch(batch, backend_name: str = "cpu_reference",
+                                           allow_optix_cpu_fallback: bool = False) -> ExternalBatchCandidateResult:
+    """GenerateCandidatesForExternalBatch (external_batch_candidate.cpp:231-339,
+    py_module.cpp:183-200): the queries packed into one x-tiled proxy scene,
+    its candidates from the device proxy path, translated back to the
+    queries.  OptiX backends behave as in a reference built without OptiX."""
+    from p2cccd_b200 import external
+
+    name = _backend(backend_name)
+    b = _external_batch(batch)
+    if name == "optix_cpu_fallback" and not allow_optix_cpu_fallback:
+        n = len(b["query_id"])
+        if n == 0:
+            raise ValueError("external batch candidate generation requires at least one query")
+        external._first_error(b)
+        raise ValueError("P2CCCD was built without OptiX support; configure with -DP2CCCD_ENABLE_OPTIX=ON")
+    r = external.generate(b)
+    res = ExternalBatchCandidateResult()
+    res.backend_name = name
+    res.primitive_count, res.raw_hit_count = r["primitive_count"], r["raw_hit_count"]
+    res.compact_candidate_count, res.candidate_recall = r["compact_candidate_count"], r["candidate_recall"]
+    res.candidates = _candidate_objects(r["candidates"])
+    for s, t in zip(b["query_id"].tolist(), r["runtime_query_ids"].tolist()):
+        m = RuntimeQueryIdMapping()
+        m.source_query_id, m.runtime_query_id = int(s), int(t)
+        res.runtime_query_ids.append(m)
+    t = res.timing
+    t.build_ms, t.trace_ms, t.compact_ms = r["encode_ms"], r["generate_ms"], r["compact_ms"]
+    t.total_ms = t.build_ms + t.update_ms + t.trace_ms + t.compact_ms
     return res
 
 
