@@ -755,6 +755,62 @@ int p2c_schedule_work_items(int mode, const p2c_candidate_record* candidates_dev
                             p2c_schedule_stats* stats_dev, uint64_t* error_dev, void* workspace_dev,
                             size_t workspace_bytes, void* stream);
 
+/* ---- candidate-group early-stop replay ----------------------------------- */
+/* DenseGroupEarlyStopConfig (cpp/common/group_scheduler.h:24-29) plus the
+ * width of the query ids (bits above it must be zero; 0 = 64). */
+typedef struct p2c_dense_group_config {
+  float uncertainty_fallback_threshold;
+  uint32_t representative_attempt_limit;
+  double interval_miss_penalty_scale;
+  int32_t preserve_input_order;
+  int32_t query_bits;
+} p2c_dense_group_config;
+
+/* DenseGroupEarlyStopStats (group_scheduler.h:31-61) without the host
+ * timings, and the first invalid row: error_kind 1 a zero query or candidate
+ * id, 2 a non-finite field (group_scheduler.cpp:81-88), at row error_row
+ * (-1 none; the totals are then meaningless). */
+typedef struct p2c_dense_group_stats {
+  uint64_t candidate_count;
+  uint64_t group_count;
+  uint64_t positive_group_count;
+  uint64_t no_proposal_exact_calls;
+  double no_proposal_exact_work;
+  uint64_t learned_exact_calls;
+  uint64_t learned_fallback_calls;
+  uint64_t learned_interval_hit_count;
+  uint64_t learned_interval_miss_count;
+  double learned_exact_work;
+  double first_positive_rank_sum;
+  double cost_before_first_positive_sum;
+  uint64_t tp;
+  uint64_t tn;
+  uint64_t fp;
+  uint64_t fn;
+  uint64_t reordered_count;
+  uint64_t high_uncertainty_group_count;
+  int64_t error_row;
+  int32_t error_kind;
+  int32_t pad;
+} p2c_dense_group_stats;
+
+size_t p2c_dense_group_early_stop_workspace_bytes(int64_t n);
+
+/* RunNativeDenseGroupExactEarlyStopOrThrow (cpp/bindings/py_module.cpp:
+ * 1179-1311) over RunDenseGroupExactEarlyStop (common/group_scheduler.cpp:
+ * 60-239) for n device rows: query_id, candidate_id, cost_target,
+ * oracle_trace (n x 8 doubles), interval_scores (n x 8 floats) and the
+ * priority, cost and uncertainty scores.  Writes *stats_dev (device); every
+ * total, the double ones included, equals the reference's bit for bit.
+ * Invalid configurations return P2C_ERR_INVALID with the reference's
+ * messages.  No host sync. */
+int p2c_dense_group_early_stop(int64_t n, const uint64_t* query_id_dev, const uint64_t* candidate_id_dev,
+                               const float* cost_target_dev, const double* oracle_trace_dev,
+                               const float* interval_scores_dev, const float* priority_score_dev,
+                               const float* cost_score_dev, const float* uncertainty_score_dev,
+                               const p2c_dense_group_config* config, p2c_dense_group_stats* stats_dev,
+                               void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

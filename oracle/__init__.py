@@ -1088,3 +1088,148 @@ def ref_external_batch(batch: dict):
     for f in cand.dtype.names:
         clean[f] = cand[f]
     return clean, rid[:n], counts, float(recall[0])
+
+
+# ---- candidate-group early-stop replay (common/group_scheduler.cpp) ----
+
+DENSE_KEYS = ("query_id", "candidate_id", "cost_target", "oracle_trace", "interval_scores", "priority_score",
+              "cost_score", "uncertainty_score")
+
+
+def _dense_arrays(rows: dict):
+    return (np.ascontiguousarray(rows["query_id"], np.uint64), np.ascontiguousarray(rows["candidate_id"], np.uint64),
+            np.ascontiguousarray(rows["cost_target"], np.float32),
+            np.ascontiguousarray(rows["oracle_trace"], np.float64).reshape(-1, 8),
+            np.ascontiguousarray(rows["interval_scores"], np.float32).reshape(-1, 8),
+            np.ascontiguousarray(rows["priority_score"], np.float32),
+            np.ascontiguousarray(rows["cost_score"], np.float32),
+            np.ascontiguousarray(rows["uncertainty_score"], np.float32))
+
+
+def ref_dense_group(rows: dict, threshold=0.75, limit=3, penalty=0.22, preserve=False) -> np.ndarray:
+    """The reference's RunDenseGroupExactEarlyStop on rows parsed as its
+    binding parses them: one DENSE_GROUP_STATS_DTYPE record."""
+    from p2cccd_b200.records import DENSE_GROUP_STATS_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_dense_ready"):
+        vp = ctypes.c_void_p
+        R.ref_dense_group.argtypes = [ctypes.c_int64] + [vp] * 8 + [ctypes.c_float, ctypes.c_uint32, ctypes.c_double,
+                                                                    ctypes.c_int, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._dense_ready = True
+    a = _dense_arrays(rows)
+    out = np.zeros(1, DENSE_GROUP_STATS_DTYPE)
+    if R.ref_dense_group(len(a[0]), *[_p(x) for x in a], float(np.float32(threshold)), int(limit), float(penalty),
+                         int(bool(preserve)), _p(out)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    return out[0]
+
+
+def dense_group(rows: dict, threshold=0.75, limit=3, penalty=0.22, preserve=False) -> dict:
+    """Restatement of RunDenseGroupExactEarlyStop (group_scheduler.cpp:60-239)
+    after the binding's parse (py_module.cpp:1212-1244), in plain Python over
+    the rows: the same order (stable by query id, then priority desc, cost
+    asc, index) and the same additions in the same order."""
+    qid, cid, ct, tr, isc, pr, cs, unc = _dense_arrays(rows)
+    n = len(qid)
+    thr = np.float32(threshold)
+    if limit == 0:
+        raise ValueError("representative_attempt_limit must be positive")
+    if not np.isfinite(thr) or thr < 0:
+        raise ValueError("uncertainty_fallback_threshold must be finite and non-negative")
+    if not math.isfinite(penalty) or penalty < 0:
+        raise ValueError("interval_miss_penalty_scale must be finite and non-negative")
+    cand = []
+    for i in range(n):
+        best, bs = 0, isc[i, 0]
+        for k in range(1, 8):
+            if isc[i, k] > bs:
+                best, bs = k, isc[i, k]
+        full = float(tr[i, 5])
+        ratio = float(ct[i])
+        narrow = max(1e-12, full * ratio) if (math.isfinite(ratio) and ratio > 0.0) else full
+        t0 = 0.125 * best
+        t1 = min(1.0, t0 + 0.125)
+        cand.append(dict(q=int(qid[i]), c=int(cid[i]), full=full, narrow=narrow, t0=t0, t1=t1, c0=float(tr[i, 6]),
+                         c1=float(tr[i, 7]), pr=np.float32(pr[i]), cs=np.float32(cs[i]), unc=np.float32(unc[i]),
+                         coll=bool(tr[i, 0] > 0.5)))
+    for c in cand:
+        if c["q"] == 0 or c["c"] == 0:
+            raise ValueError("dense group candidate ids must be non-zero")
+        if not all(math.isfinite(float(c[k])) for k in ("full", "narrow", "t0", "t1", "c0", "c1", "pr", "cs", "unc")):
+            raise ValueError("dense group candidate contains a non-finite field")
+
+    def pos_cost(v, fb):
+        return fb if (not math.isfinite(v) or v <= 0.0) else v
+
+    if preserve:
+        order = sorted(range(n), key=lambda i: (cand[i]["q"], i))
+    else:  # -0 == +0 in float comparisons; Python's sort is stable
+        order = sorted(range(n), key=lambda i: (cand[i]["q"], -float(cand[i]["pr"]), float(cand[i]["cs"]), i))
+    out = dict(candidate_count=n, group_count=0, positive_group_count=0, no_proposal_exact_calls=0,
+               no_proposal_exact_work=0.0, learned_exact_calls=0, learned_fallback_calls=0,
+               learned_interval_hit_count=0, learned_interval_miss_count=0, learned_exact_work=0.0,
+               first_positive_rank_sum=0.0, cost_before_first_positive_sum=0.0, tp=0, tn=0, fp=0, fn=0,
+               reordered_count=sum(1 for i, o in enumerate(order) if o != i), high_uncertainty_group_count=0)
+    b = 0
+    while b < n:
+        e = b + 1
+        while e < n and cand[order[e]]["q"] == cand[order[b]]["q"]:
+            e += 1
+        out["group_count"] += 1
+        truth, gwork = False, 0.0
+        for p in range(b, e):
+            c = cand[order[p]]
+            truth = truth or c["coll"]
+            gwork += pos_cost(c["full"], 1.0)
+        out["positive_group_count"] += truth
+        out["no_proposal_exact_calls"] += e - b
+        out["no_proposal_exact_work"] += gwork
+        predicted, resolved, high, wb = False, False, False, 0.0
+        for p in range(b, e):
+            c = cand[order[p]]
+            full = pos_cost(c["full"], 1.0)
+            nar = pos_cost(c["narrow"], full)
+            if c["unc"] >= thr:
+                high = True
+                for fp in range(p, e):  # run_full_fallback
+                    f = cand[order[fp]]
+                    fc = pos_cost(f["full"], 1.0)
+                    out["learned_exact_calls"] += 1
+                    out["learned_fallback_calls"] += 1
+                    out["learned_exact_work"] += fc
+                    if f["coll"]:
+                        predicted = True
+                        out["first_positive_rank_sum"] += fp - b + 1
+                        out["cost_before_first_positive_sum"] += wb + fc
+                        break
+                    wb += fc
+                break
+            out["learned_exact_calls"] += 1
+            out["learned_exact_work"] += nar
+            if c["coll"]:
+                if max(c["t0"], c["c0"]) <= min(c["t1"], c["c1"]):
+                    out["learned_interval_hit_count"] += 1
+                    predicted = True
+                    out["first_positive_rank_sum"] += p - b + 1
+                    out["cost_before_first_positive_sum"] += wb + nar
+                    break
+                out["learned_interval_miss_count"] += 1
+                out["learned_exact_work"] += full * penalty
+                if p - b + 1 >= limit:
+                    out["learned_exact_calls"] += 1
+                    out["learned_fallback_calls"] += 1
+                    out["learned_exact_work"] += full
+                    predicted = True
+                    out["first_positive_rank_sum"] += p - b + 1
+                    out["cost_before_first_positive_sum"] += wb + nar + full
+                    break
+                wb += nar + full * penalty
+                continue
+            wb += nar
+        out["high_uncertainty_group_count"] += high
+        key = ("tp" if predicted else "fn") if truth else ("fp" if predicted else "tn")
+        out[key] += 1
+        b = e
+    return out

@@ -12,10 +12,12 @@
 #include "proposal/proposal_policy.h"
 #include "rt_candidate/candidate_buffer.h"
 #include "rt_candidate/candidate_stats.h"
+#include "common/group_scheduler.h"
 #include "rt_candidate/external_batch_candidate.h"
 #include "rt_candidate/proxy_scene.h"
 
 #include <algorithm>
+#include <cmath>
 #include <cstddef>
 #include <cstdint>
 #include <cstring>
@@ -375,6 +377,76 @@ int ref_external_batch(int64_t n, const uint64_t* source_id, const uint32_t* sou
   counts[1] = res.raw_hit_count;
   counts[2] = res.compact_candidate_count;
   *recall = res.candidate_recall;
+  return 0;
+}
+
+// RunDenseGroupExactEarlyStop on n rows, parsed as the binding parses its
+// arrays (py_module.cpp:1212-1244): arg-max interval bin with strict >,
+// full cost trace[5], narrow cost max(1e-12, full * cost_target) for a
+// finite positive cost_target, contact trace[6:8], label trace[0] > 0.5.
+// Writes 18 totals in p2c_dense_group_stats order (doubles as their bits).
+int ref_dense_group(int64_t n, const uint64_t* query_id, const uint64_t* candidate_id, const float* cost_target,
+                    const double* trace, const float* interval_scores, const float* priority, const float* cost_score,
+                    const float* uncertainty, float threshold, uint32_t limit, double penalty, int preserve,
+                    p2c_dense_group_stats* out) {
+  std::vector<p2cccd::DenseGroupCandidateInput> rows(static_cast<std::size_t>(n));
+  for (int64_t i = 0; i < n; ++i) {
+    const float* sc = interval_scores + 8 * i;
+    int best = 0;
+    float best_score = sc[0];
+    for (int k = 1; k < 8; ++k)
+      if (sc[k] > best_score) {
+        best_score = sc[k];
+        best = k;
+      }
+    const double width = 1.0 / 8.0;
+    const double full = trace[8 * i + 5];
+    const double ratio = cost_target[i];
+    p2cccd::DenseGroupCandidateInput& r = rows[static_cast<std::size_t>(i)];
+    r.query_id = query_id[i];
+    r.candidate_id = candidate_id[i];
+    r.full_exact_cost = full;
+    r.narrow_exact_cost = std::isfinite(ratio) && ratio > 0.0 ? std::max(1.0e-12, full * ratio) : full;
+    r.interval_t0 = width * static_cast<double>(best);
+    r.interval_t1 = std::min(1.0, r.interval_t0 + width);
+    r.contact_t0 = trace[8 * i + 6];
+    r.contact_t1 = trace[8 * i + 7];
+    r.priority_score = priority[i];
+    r.cost_score = cost_score[i];
+    r.uncertainty_score = uncertainty[i];
+    r.candidate_collides = trace[8 * i] > 0.5;
+  }
+  p2cccd::DenseGroupEarlyStopConfig cfg;
+  cfg.uncertainty_fallback_threshold = threshold;
+  cfg.representative_attempt_limit = limit;
+  cfg.interval_miss_penalty_scale = penalty;
+  cfg.preserve_input_order = preserve != 0;
+  p2cccd::DenseGroupEarlyStopStats st;
+  const p2cccd::Status status = p2cccd::RunDenseGroupExactEarlyStop(rows, cfg, &st);
+  if (!status.ok) {
+    g_proxy_error = status.message;
+    return 1;
+  }
+  std::memset(out, 0, sizeof(*out));
+  out->candidate_count = st.candidate_count;
+  out->group_count = st.group_count;
+  out->positive_group_count = st.positive_group_count;
+  out->no_proposal_exact_calls = st.no_proposal_exact_calls;
+  out->no_proposal_exact_work = st.no_proposal_exact_work;
+  out->learned_exact_calls = st.learned_exact_calls;
+  out->learned_fallback_calls = st.learned_fallback_calls;
+  out->learned_interval_hit_count = st.learned_interval_hit_count;
+  out->learned_interval_miss_count = st.learned_interval_miss_count;
+  out->learned_exact_work = st.learned_exact_work;
+  out->first_positive_rank_sum = st.first_positive_rank_sum;
+  out->cost_before_first_positive_sum = st.cost_before_first_positive_sum;
+  out->tp = st.tp;
+  out->tn = st.tn;
+  out->fp = st.fp;
+  out->fn = st.fn;
+  out->reordered_count = st.reordered_count;
+  out->high_uncertainty_group_count = st.high_uncertainty_group_count;
+  out->error_row = -1;
   return 0;
 }
 

@@ -95,6 +95,9 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_schedule_work_items_workspace_bytes": (_size, [_i64, _i64, _i64]),
     "p2c_schedule_work_items": (_int, [_int, _c_void_p, _i64, _c_void_p, _i64, _c_void_p, _i64, _c_void_p, _c_void_p,
                                        _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p]),
+    "p2c_dense_group_early_stop_workspace_bytes": (_size, [_i64]),
+    "p2c_dense_group_early_stop": (_int, [_i64] + [_c_void_p] * 8 + [_c_void_p, _c_void_p, _c_void_p, _size,
+                                                                     _c_void_p]),
     "p2c_probe_fp64": (_int, [_c_void_p, _int, ctypes.POINTER(ctypes.c_longlong), _c_void_p]),
     "p2c_certify_census": (_int, [_c_void_p, _i64, _c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig),
                                   _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),

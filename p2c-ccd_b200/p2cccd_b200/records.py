@@ -194,3 +194,15 @@ SCHEDULE_STATS_FIELDS = ("raw_candidate_count", "proposal_output_count", "work_i
                          "missing_proposal_fallback_count", "invalid_proposal_fallback_count", "ood_fallback_count",
                          "high_uncertainty_fallback_count", "reordered_count", "monotonic_safe")
 SCHEDULE_STATS_DTYPE = np.dtype([(k, "<u8") for k in SCHEDULE_STATS_FIELDS])
+
+# p2c_dense_group_stats (DenseGroupEarlyStopStats without host timings, plus
+# the first invalid row)
+DENSE_GROUP_STATS_DTYPE = np.dtype([
+    ("candidate_count", "<u8"), ("group_count", "<u8"), ("positive_group_count", "<u8"),
+    ("no_proposal_exact_calls", "<u8"), ("no_proposal_exact_work", "<f8"), ("learned_exact_calls", "<u8"),
+    ("learned_fallback_calls", "<u8"), ("learned_interval_hit_count", "<u8"),
+    ("learned_interval_miss_count", "<u8"), ("learned_exact_work", "<f8"), ("first_positive_rank_sum", "<f8"),
+    ("cost_before_first_positive_sum", "<f8"), ("tp", "<u8"), ("tn", "<u8"), ("fp", "<u8"), ("fn", "<u8"),
+    ("reordered_count", "<u8"), ("high_uncertainty_group_count", "<u8"), ("error_row", "<i8"),
+    ("error_kind", "<i4"), ("pad", "<i4")])
+assert DENSE_GROUP_STATS_DTYPE.itemsize == 160

@@ -1462,3 +1462,21 @@ def schedule_runtime_exact_work_items_from_proposal_arrays(feature_arrays, predi
     if len(rows) != len(outs):
         raise ValueError("feature row and proposal output array lengths must match")
     return _schedule(None, rows, outs, conservative_family_masks_by_query_id, config, 1)
+
+
+# ---------------------------------------------------------------------------
+# the candidate-group interface (common/group_scheduler.cpp, py_module.cpp:1179-1311, 1938-1945)
+
+def run_native_dense_group_exact_early_stop(feature_arrays: dict, prediction_arrays: dict,
+                                            uncertainty_fallback_threshold: float = 0.75,
+                                            representative_attempt_limit: int = 3,
+                                            interval_miss_penalty_scale: float = 0.22,
+                                            preserve_input_order: bool = False) -> dict:
+    """RunNativeDenseGroupExactEarlyStopOrThrow: the label replay of a learned
+    group schedule (first hit per query group, uncertainty fallback, interval
+    miss penalties) on the GPU; the counts and work totals equal the
+    reference's bit for bit."""
+    from p2cccd_b200 import dense_groups
+
+    return dense_groups.early_stop(feature_arrays, prediction_arrays, uncertainty_fallback_threshold,
+                                   representative_attempt_limit, interval_miss_penalty_scale, preserve_input_order)
