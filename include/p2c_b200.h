@@ -755,6 +755,25 @@ int p2c_schedule_work_items(int mode, const p2c_candidate_record* candidates_dev
                             p2c_schedule_stats* stats_dev, uint64_t* error_dev, void* workspace_dev,
                             size_t workspace_bytes, void* stream);
 
+/* RunDummyProposalScheduleFromRuntimeCandidates (cpp/proposal/
+ * proposal_policy.cpp:744-858; binding py_module.cpp:1009-1033) for n device
+ * candidates (bypass == 0): the density-derived dummy proposals, the
+ * out-of-distribution fallback, a stable sort by priority (unless the config
+ * preserves candidate order) and the checks.  With rows_dev and outputs_dev
+ * non-NULL the artifacts are materialized too (rows as
+ * p2c_runtime_feature_rows; outputs from them).  bypass != 0 is the raw
+ * queue of GenerateExternalBatchDummyProposalScheduleOrThrow
+ * (py_module.cpp:290-318): one kRaw item per candidate in order, its query's
+ * mask, priority rt_hit_count, no config check.  Workspace:
+ * p2c_schedule_work_items_workspace_bytes(n, 0, 0).  error_dev[0] as for
+ * p2c_schedule_work_items (bits 1 and 16).  No host sync. */
+int p2c_dummy_schedule(int bypass, const p2c_candidate_record* candidates_dev, int64_t n, uint64_t primitive_count,
+                       uint64_t raw_hit_count, uint64_t compact_candidate_count, const uint64_t* mask_query_ids_dev,
+                       const uint32_t* masks_dev, int64_t n_masks, const p2c_scheduling_config* config,
+                       p2c_proposal_feature_row* rows_dev, p2c_proposal_output* outputs_dev,
+                       p2c_exact_work_item* items_dev, p2c_schedule_stats* stats_dev, uint64_t* error_dev,
+                       void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- candidate-group early-stop replay ----------------------------------- */
 /* DenseGroupEarlyStopConfig (cpp/common/group_scheduler.h:24-29) plus the
  * width of the query ids (bits above it must be zero; 0 = 64). */

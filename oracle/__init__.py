@@ -1233,3 +1233,144 @@ def dense_group(rows: dict, threshold=0.75, limit=3, penalty=0.22, preserve=Fals
         out[key] += 1
         b = e
     return out
+
+
+# ---- dummy proposal schedules (proposal_policy.cpp:744-858, py_module.cpp:269-361) ----
+
+def _sched_args(c: dict):
+    return (c["first_work_item_id"], c["conservative_feature_family_mask"], c["fallback_interval_t0"],
+            c["fallback_interval_t1"], c["family_score_threshold"], c["uncertainty_fallback_threshold"],
+            c["ood_abs_feature_threshold"], 1 if c["preserve_candidate_order"] else 0)
+
+
+def _sched_argtypes():
+    return [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_double, ctypes.c_double, ctypes.c_float, ctypes.c_float,
+            ctypes.c_float, ctypes.c_int]
+
+
+def _schedule_buffers(n: int):
+    from p2cccd_b200.records import (EXACT_WORK_ITEM_DTYPE, FEATURE_ROW_DTYPE, PROPOSAL_OUTPUT_DTYPE,
+                                     SCHEDULE_STATS_DTYPE)
+
+    m = max(1, n)
+    return (np.zeros(m, EXACT_WORK_ITEM_DTYPE), np.zeros(1, SCHEDULE_STATS_DTYPE), np.zeros(m, FEATURE_ROW_DTYPE),
+            np.zeros(m, PROPOSAL_OUTPUT_DTYPE), np.zeros(4, np.int64))
+
+
+def ref_dummy_schedule(cand, primitive_count, raw_hit_count, compact_candidate_count, masks=None, materialize=True,
+                       **cfg):
+    """The reference's RunDummyProposalScheduleFromRuntimeCandidates with the
+    binding's density: (work items, stats, feature rows, proposal outputs)."""
+    c = dict(SCHED_DEFAULTS, **cfg)
+    R = ref()
+    if not hasattr(R, "_dummy_ready"):
+        vp, i64, u64 = ctypes.c_void_p, ctypes.c_int64, ctypes.c_uint64
+        R.ref_dummy_schedule.argtypes = [vp, i64, u64, u64, u64, vp, vp, i64] + _sched_argtypes() + \
+            [ctypes.c_int, vp, vp, vp, vp, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._dummy_ready = True
+    cand = np.ascontiguousarray(cand)
+    keys = np.array(sorted((masks or {}).keys()), np.uint64)
+    vals = np.array([masks[int(k)] for k in keys], np.uint32)
+    items, stats, rows, outs, sizes = _schedule_buffers(len(cand))
+    if R.ref_dummy_schedule(_p(cand), len(cand), int(primitive_count), int(raw_hit_count),
+                            int(compact_candidate_count), _p(keys) if len(keys) else None,
+                            _p(vals) if len(vals) else None, len(keys), *_sched_args(c), int(bool(materialize)),
+                            _p(items), _p(stats), _p(rows), _p(outs), _p(sizes)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    return items[:sizes[0]], stats[0], rows[:sizes[1]], outs[:sizes[2]]
+
+
+def ref_external_dummy(batch: dict, materialize=False, **cfg):
+    """The binding's GenerateExternalBatchDummyProposalSchedule restated over
+    the reference's functions: (candidates, work items, stats, rows, outputs)."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE
+
+    c = dict(SCHED_DEFAULTS, **cfg)
+    R = ref()
+    if not hasattr(R, "_ext_dummy_ready"):
+        vp = ctypes.c_void_p
+        R.ref_external_dummy.argtypes = [ctypes.c_int64] + [vp] * 8 + _sched_argtypes() + [ctypes.c_int] + [vp] * 6
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._ext_dummy_ready = True
+    a = _external_args(batch)
+    n = a[0]
+    cand = np.zeros(max(1, n), CANDIDATE_RECORD_DTYPE)
+    items, stats, rows, outs, sizes = _schedule_buffers(n)
+    if R.ref_external_dummy(n, *[_p(x) for x in a[1:]], *_sched_args(c), int(bool(materialize)), _p(cand),
+                            _p(items), _p(stats), _p(rows), _p(outs), _p(sizes)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    clean = np.zeros(int(sizes[3]), CANDIDATE_RECORD_DTYPE)  # padding bytes of the reference struct are indeterminate
+    for f in CANDIDATE_RECORD_DTYPE.names:
+        clean[f] = cand[:int(sizes[3])][f]
+    return clean, items[:sizes[0]], stats[0], rows[:sizes[1]], outs[:sizes[2]]
+
+
+def dummy_schedule(cand, primitive_count, raw_hit_count, compact_candidate_count, masks=None, materialize=True,
+                   **cfg):
+    """Restatement of RunDummyProposalScheduleFromRuntimeCandidates
+    (proposal_policy.cpp:744-858): runtime rows and dummy outputs, the OOD
+    fallback, a stable priority sort, ids and checks."""
+    from p2cccd_b200.records import EXACT_WORK_ITEM_DTYPE, PROPOSAL_OUTPUT_DTYPE, SCHEDULE_STATS_DTYPE
+
+    c = dict(SCHED_DEFAULTS, **cfg)
+    f32 = np.float32
+    if primitive_count == 0:
+        raise ValueError("CandidateDensityStats.proxy_count must be non-zero")
+    def ratio(x, y):
+        return float(x) / float(y) if y else 0.0
+    cpp = ratio(compact_candidate_count, primitive_count)
+    aor = ratio(raw_hit_count, primitive_count // 2 if primitive_count >= 2 else 1)
+    avg = ratio(raw_hit_count, compact_candidate_count)
+    thr = f32(c["ood_abs_feature_threshold"])
+    rows = runtime_feature_rows(cand, primitive_count, raw_hit_count, compact_candidate_count, masks)
+    n = len(cand)
+    outs = np.zeros(n, PROPOSAL_OUTPUT_DTYPE)
+    staged = np.zeros(n, EXACT_WORK_ITEM_DTYPE)
+    stats = np.zeros(1, SCHEDULE_STATS_DTYPE)[0]
+    for i, r in enumerate(cand):
+        base = (masks or {}).get(int(r["query_id"]), 0) or 3
+        scal = [1.0, float(r["rt_hit_count"]), float(r["proxy_type_a"]), float(r["proxy_type_b"]), min(1.0, aor),
+                cpp, aor, avg]
+        ood = any((not math.isfinite(v)) or abs(v) > float(thr) for v in scal) or \
+            any((not np.isfinite(v)) or abs(f32(v)) > thr for v in r["motion_bound"])
+        stats["fallback_count"] += ood
+        stats["ood_fallback_count"] += ood
+        act = [k for k in (0, 1) if base & (1 << k)] or [0, 1]
+        w = f32(1.0) / f32(len(act))
+        fam = [w if k in act else f32(0.0) for k in (0, 1)]
+        row = rows[i]
+        o = outs[i]
+        o["candidate_id"] = r["candidate_id"]
+        o["interval_scores"] = row["interval_targets"]
+        o["family_scores"][0], o["family_scores"][1] = fam
+        o["priority_score"] = max(f32(0.0), row["priority_target"])
+        o["cost_score"] = max(f32(0.0), row["cost_target"])
+        o["uncertainty_score"] = f32(1.0) if ood else max(f32(0.0), row["uncertainty_target"])
+        it = staged[i]
+        for k in ("query_id", "slab_id", "patch_a_id", "patch_b_id"):
+            it[k] = r[k]
+        it["parent_candidate_id"] = r["candidate_id"]
+        it["interval_t0"], it["interval_t1"] = c["fallback_interval_t0"], c["fallback_interval_t1"]
+        if ood:
+            it["feature_family_mask"], it["priority_score"], it["source"] = base, f32(r["rt_hit_count"]), 2
+        else:
+            m = base | (1 if fam[0] >= f32(c["family_score_threshold"]) else 0) | \
+                (2 if fam[1] >= f32(c["family_score_threshold"]) else 0)
+            it["feature_family_mask"] = m
+            it["priority_score"] = max(f32(0.0), _clamp_feature(min(1.0, 0.5 * float(r["rt_hit_count"]) + 0.5 * cpp)))
+            it["source"] = 1
+    order = list(range(n))
+    if not c["preserve_candidate_order"]:
+        order.sort(key=lambda i: -float(staged[i]["priority_score"]))  # stable
+    items = staged[order]
+    items["work_item_id"] = np.arange(n, dtype=np.uint64) + np.uint64(c["first_work_item_id"])
+    stats["raw_candidate_count"] = stats["proposal_output_count"] = stats["work_item_count"] = n
+    stats["reordered_count"] = int(np.sum(items["parent_candidate_id"] != np.asarray(cand["candidate_id"])))
+    stats["monotonic_safe"] = 1
+    clean = np.zeros(n, EXACT_WORK_ITEM_DTYPE)  # zero padding after the fancy-index copy
+    for f in EXACT_WORK_ITEM_DTYPE.names:
+        clean[f] = items[f]
+    if not materialize:
+        rows, outs = rows[:0], outs[:0]
+    return clean, stats, rows, outs

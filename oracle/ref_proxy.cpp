@@ -13,6 +13,7 @@
 #include "rt_candidate/candidate_buffer.h"
 #include "rt_candidate/candidate_stats.h"
 #include "common/group_scheduler.h"
+#include "common/validators.h"
 #include "rt_candidate/external_batch_candidate.h"
 #include "rt_candidate/proxy_scene.h"
 
@@ -335,6 +336,206 @@ int ref_schedule_runtime(const p2c_candidate_record* cands, int64_t n, const p2c
                           st.ood_fallback_count, st.high_uncertainty_fallback_count, st.reordered_count,
                           st.monotonic_safe ? 1u : 0u};
   std::memcpy(stats_out, s, sizeof(s));
+  return 0;
+}
+
+namespace {
+
+p2cccd::ProposalSchedulingConfig sched_config(uint64_t first_work_item_id, uint32_t conservative, double t0,
+                                              double t1, float family_threshold, float uncertainty_threshold,
+                                              float ood_threshold, int preserve) {
+  p2cccd::ProposalSchedulingConfig cfg;
+  cfg.first_work_item_id = first_work_item_id;
+  cfg.conservative_feature_family_mask = conservative;
+  cfg.fallback_interval_t0 = t0;
+  cfg.fallback_interval_t1 = t1;
+  cfg.family_score_threshold = family_threshold;
+  cfg.uncertainty_fallback_threshold = uncertainty_threshold;
+  cfg.ood_abs_feature_threshold = ood_threshold;
+  cfg.preserve_candidate_order = preserve != 0;
+  return cfg;
+}
+
+void write_schedule(const p2cccd::ProposalRuntimeScheduleResult& r, p2c_exact_work_item* items_out,
+                    uint64_t* stats_out, p2c_proposal_feature_row* rows_out, p2c_proposal_output* outs_out,
+                    int64_t* sizes_out) {
+  for (std::size_t i = 0; i < r.work_queue.size(); ++i) {
+    std::memset(items_out + i, 0, sizeof(p2c_exact_work_item));
+    const p2cccd::ExactWorkItem& w = r.work_queue[i];
+    p2c_exact_work_item& o = items_out[i];
+    o.work_item_id = w.work_item_id;
+    o.parent_candidate_id = w.parent_candidate_id;
+    o.query_id = w.query_id;
+    o.slab_id = w.slab_id;
+    o.patch_a_id = w.patch_a_id;
+    o.patch_b_id = w.patch_b_id;
+    o.interval_t0 = w.interval_t0;
+    o.interval_t1 = w.interval_t1;
+    o.feature_family_mask = w.feature_family_mask;
+    o.topk_feature_ids_offset = w.topk_feature_ids_offset;
+    o.depth = w.depth;
+    o.priority_score = w.priority_score;
+    o.source = static_cast<uint8_t>(w.source);
+  }
+  for (std::size_t i = 0; i < r.feature_rows.size(); ++i)
+    std::memcpy(rows_out + i, &r.feature_rows[i], sizeof(p2c_proposal_feature_row));
+  for (std::size_t i = 0; i < r.proposal_outputs.size(); ++i)
+    std::memcpy(outs_out + i, &r.proposal_outputs[i], sizeof(p2c_proposal_output));
+  const p2cccd::ProposalScheduleStats& st = r.stats;
+  const uint64_t s[10] = {st.raw_candidate_count, st.proposal_output_count, st.work_item_count, st.fallback_count,
+                          st.missing_proposal_fallback_count, st.invalid_proposal_fallback_count,
+                          st.ood_fallback_count, st.high_uncertainty_fallback_count, st.reordered_count,
+                          st.monotonic_safe ? 1u : 0u};
+  std::memcpy(stats_out, s, sizeof(s));
+  sizes_out[0] = static_cast<int64_t>(r.work_queue.size());
+  sizes_out[1] = static_cast<int64_t>(r.feature_rows.size());
+  sizes_out[2] = static_cast<int64_t>(r.proposal_outputs.size());
+}
+
+// MakeRuntimeDensityStats (py_module.cpp:508-531)
+p2cccd::CandidateDensityStats runtime_density(const std::vector<p2cccd::CandidateRecord>& c, uint64_t primitives,
+                                              uint64_t raw, uint64_t compact) {
+  p2cccd::CandidateDensityStats d;
+  d.query_id = c.empty() ? 1U : c.front().query_id;
+  d.proxy_count = primitives;
+  d.raw_hit_count = raw;
+  d.compact_candidate_count = compact;
+  d.candidates_per_proxy = primitives == 0U ? 0.0 : static_cast<double>(compact) / static_cast<double>(primitives);
+  const uint64_t den = primitives >= 2U ? primitives / 2U : 1U;
+  d.aabb_overlap_ratio = static_cast<double>(raw) / static_cast<double>(den);
+  d.avg_rt_hits_per_candidate = compact == 0U ? 0.0 : static_cast<double>(raw) / static_cast<double>(compact);
+  return d;
+}
+
+}  // namespace
+
+// RunDummyProposalScheduleFromRuntimeCandidates through its binding
+// (py_module.cpp:1009-1033).  sizes_out: {items, rows, outputs}.
+int ref_dummy_schedule(const p2c_candidate_record* cands, int64_t n, uint64_t primitives, uint64_t raw,
+                       uint64_t compact, const uint64_t* mask_qids, const uint32_t* masks, int64_t n_masks,
+                       uint64_t first_work_item_id, uint32_t conservative, double t0, double t1,
+                       float family_threshold, float uncertainty_threshold, float ood_threshold, int preserve,
+                       int materialize, p2c_exact_work_item* items_out, uint64_t* stats_out,
+                       p2c_proposal_feature_row* rows_out, p2c_proposal_output* outs_out, int64_t* sizes_out) {
+  std::vector<p2cccd::CandidateRecord> cand(static_cast<std::size_t>(n));
+  for (int64_t i = 0; i < n; ++i) std::memcpy(&cand[static_cast<std::size_t>(i)], cands + i, sizeof(p2c_candidate_record));
+  std::unordered_map<std::uint64_t, std::uint32_t> mask_map;
+  for (int64_t i = 0; i < n_masks; ++i) mask_map[mask_qids[i]] = masks[i];
+  const auto cfg = sched_config(first_work_item_id, conservative, t0, t1, family_threshold, uncertainty_threshold,
+                                ood_threshold, preserve);
+  p2cccd::ProposalRuntimeScheduleResult result;
+  const p2cccd::Status status = p2cccd::RunDummyProposalScheduleFromRuntimeCandidates(
+      cand, runtime_density(cand, primitives, raw, compact), mask_map, cfg, materialize != 0, &result);
+  if (!status.ok) {
+    g_proxy_error = status.message;
+    return 1;
+  }
+  write_schedule(result, items_out, stats_out, rows_out, outs_out, sizes_out);
+  return 0;
+}
+
+// GenerateExternalBatchDummyProposalScheduleOrThrow (py_module.cpp:269-361)
+// restated over the reference's own functions: the batch's candidates, a
+// conservative mask per runtime query id from its family (:213-246), the
+// raw bypass when every candidate has its own query and a single-family
+// mask (:248-267, :290-318), else the dummy schedule with the binding's
+// density (:320-349).  Batch arguments as ref_external_batch; candidates
+// (capacity n) are written too.  sizes_out: {items, rows, outputs, cands}.
+int ref_external_dummy(int64_t n, const uint64_t* source_id, const uint32_t* source_index, const uint8_t* family,
+                       const double* v_t0, const double* v_t1, const int8_t* ground_truth, const uint8_t* has_box,
+                       const uint32_t* box_pair, uint64_t first_work_item_id, uint32_t conservative, double t0,
+                       double t1, float family_threshold, float uncertainty_threshold, float ood_threshold,
+                       int preserve, int materialize, p2c_candidate_record* cand_out, p2c_exact_work_item* items_out,
+                       uint64_t* stats_out, p2c_proposal_feature_row* rows_out, p2c_proposal_output* outs_out,
+                       int64_t* sizes_out) {
+  std::vector<p2cccd::ExternalBatchQuery> queries(static_cast<std::size_t>(n));
+  for (int64_t k = 0; k < n; ++k) {
+    p2cccd::ExternalBatchQuery& q = queries[static_cast<std::size_t>(k)];
+    q.source_query_id = source_id[k];
+    q.source_query_index = source_index[k];
+    q.family = family[k] ? p2cccd::ExternalQueryFamily::kEdgeEdge : p2cccd::ExternalQueryFamily::kVertexFace;
+    for (int v = 0; v < 4; ++v)
+      for (int a = 0; a < 3; ++a) {
+        q.vertices_t0[v][a] = v_t0[12 * k + 3 * v + a];
+        q.vertices_t1[v][a] = v_t1[12 * k + 3 * v + a];
+      }
+    q.has_ground_truth = ground_truth[k] >= 0;
+    q.ground_truth_collides = ground_truth[k] > 0;
+    q.has_box_pair = has_box[k] != 0;
+    if (q.has_box_pair) q.box_pair = {box_pair[2 * k], box_pair[2 * k + 1]};
+  }
+  p2cccd::CandidateGeneratorConfig gen_cfg;
+  p2cccd::ExternalBatchCandidateResult cr;
+  p2cccd::Status status = p2cccd::GenerateCandidatesForExternalBatch(queries, gen_cfg, &cr);
+  if (!status.ok) {
+    g_proxy_error = status.message;
+    return 1;
+  }
+  std::unordered_map<std::uint64_t, std::uint32_t> source_masks, runtime_masks;
+  for (const auto& q : queries)
+    source_masks.emplace(q.source_query_id, q.family == p2cccd::ExternalQueryFamily::kVertexFace ? 1u : 2u);
+  for (const auto& m : cr.runtime_query_ids) {
+    const auto it = source_masks.find(m.source_query_id);
+    runtime_masks.emplace(m.runtime_query_id, it != source_masks.end() ? it->second : 3u);
+  }
+  bool bypass = true;
+  {
+    std::unordered_map<std::uint64_t, std::uint8_t> seen;
+    for (const auto& c : cr.candidates) {
+      if (!seen.emplace(c.query_id, 1U).second) {
+        bypass = false;
+        break;
+      }
+      const auto it = runtime_masks.find(c.query_id);
+      const uint32_t m = it != runtime_masks.end() ? it->second : 3u;
+      if (m == 0u || (m & (m - 1u)) != 0u) {
+        bypass = false;
+        break;
+      }
+    }
+  }
+  const auto cfg = sched_config(first_work_item_id, conservative, t0, t1, family_threshold, uncertainty_threshold,
+                                ood_threshold, preserve);
+  p2cccd::ProposalRuntimeScheduleResult result;
+  if (bypass) {
+    result.stats.raw_candidate_count = cr.candidates.size();
+    result.stats.work_item_count = cr.candidates.size();
+    result.stats.monotonic_safe = true;
+    for (std::size_t i = 0; i < cr.candidates.size(); ++i) {
+      const p2cccd::CandidateRecord& c = cr.candidates[i];
+      p2cccd::ExactWorkItem item;
+      item.work_item_id = cfg.first_work_item_id + i;
+      item.parent_candidate_id = c.candidate_id;
+      item.query_id = c.query_id;
+      item.slab_id = c.slab_id;
+      item.patch_a_id = c.patch_a_id;
+      item.patch_b_id = c.patch_b_id;
+      item.interval_t0 = cfg.fallback_interval_t0;
+      item.interval_t1 = cfg.fallback_interval_t1;
+      item.feature_family_mask = runtime_masks.at(c.query_id);
+      item.topk_feature_ids_offset = 0U;
+      item.depth = 0U;
+      item.priority_score = static_cast<float>(c.rt_hit_count);
+      item.source = p2cccd::ProposalSource::kRaw;
+      status = p2cccd::ValidateExactWorkItem(item);
+      if (!status.ok) break;
+      result.work_queue.push_back(item);
+    }
+  } else {
+    std::vector<p2cccd::CandidateRecord> cand = cr.candidates;
+    p2cccd::CandidateDensityStats d = runtime_density(cand, cr.primitive_count, cr.raw_hit_count,
+                                                      cr.compact_candidate_count);
+    status = p2cccd::RunDummyProposalScheduleFromRuntimeCandidates(cand, d, runtime_masks, cfg, materialize != 0,
+                                                                   &result);
+  }
+  if (!status.ok) {
+    g_proxy_error = status.message;
+    return 1;
+  }
+  for (std::size_t i = 0; i < cr.candidates.size(); ++i)
+    std::memcpy(cand_out + i, &cr.candidates[i], sizeof(p2c_candidate_record));
+  write_schedule(result, items_out, stats_out, rows_out, outs_out, sizes_out);
+  sizes_out[3] = static_cast<int64_t>(cr.candidates.size());
   return 0;
 }
 

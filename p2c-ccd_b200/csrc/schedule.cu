@@ -160,10 +160,61 @@ __device__ __forceinline__ unsigned priority_key(float p) {
 }
 
 struct SchedParams {
-  int mode;  // 0: candidates with lookups, 1: aligned rows / outputs
+  int mode;  // 0: candidates with lookups, 1: aligned rows / outputs, 2: dummy proposals, 3: raw bypass
   p2c_scheduling_config cfg;
   long long n, n_rows, n_outputs, n_masks;
+  double candidates_per_proxy, aabb_overlap_ratio, avg_hits;  // mode 2: RuntimeDensityDerivedStats
 };
+
+// ClampRuntimeFeature (proposal_policy.cpp:30-35)
+__device__ __forceinline__ float runtime_clamp(double v) {
+  if (!isfinite(v)) return 0.0f;
+  const double c = v < -1.0e6 ? -1.0e6 : (1.0e6 < v ? 1.0e6 : v);
+  return __double2float_rn(c);
+}
+
+// The query's conservative mask from the sorted (query id, mask) table:
+// BaseFamilyMaskForRuntimeQuery's two-argument form (:135-144) when
+// `nonzero_only` (a zero mask counts as absent), else unordered_map::at.
+__device__ __forceinline__ unsigned query_mask(const unsigned long long* qids, const unsigned* masks, long long n,
+                                               unsigned long long q, bool nonzero_only) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long m = (lo + hi) >> 1;
+    if (qids[m] < q) lo = m + 1;
+    else hi = m;
+  }
+  if (lo < n && qids[lo] == q && (!nonzero_only || masks[lo] != 0u)) return masks[lo];
+  return 3u;
+}
+
+// NormalizedDummyFamilyScores (:156-175): equal weights over the mask's families.
+__device__ __forceinline__ void dummy_family_scores(unsigned base, float* s0, float* s1) {
+  bool a0 = (base & 1u) != 0u, a1 = (base & 2u) != 0u;
+  if (!a0 && !a1) a0 = a1 = true;
+  const float w = 1.0f / (float)((a0 ? 1 : 0) + (a1 ? 1 : 0));
+  *s0 = a0 ? w : 0.0f;
+  *s1 = a1 ? w : 0.0f;
+}
+
+// IsRuntimeCandidateOod (:245-270)
+__device__ __forceinline__ bool runtime_ood(const p2c_candidate_record& r, const SchedParams& P) {
+  const double thr = (double)P.cfg.ood_abs_feature_threshold;
+  const double capped = P.aabb_overlap_ratio < 1.0 ? P.aabb_overlap_ratio : 1.0;
+  const double v[8] = {1.0, (double)r.rt_hit_count, (double)r.proxy_type_a, (double)r.proxy_type_b,
+                       capped, P.candidates_per_proxy, P.aabb_overlap_ratio, P.avg_hits};
+  bool ood = false;
+  for (int k = 0; k < 8; ++k) ood = ood || !isfinite(v[k]) || fabs(v[k]) > thr;
+  for (int k = 0; k < 4; ++k)
+    ood = ood || !isfinite(r.motion_bound[k]) || fabsf(r.motion_bound[k]) > P.cfg.ood_abs_feature_threshold;
+  return ood;
+}
+
+// RuntimePriorityTarget (:237-241)
+__device__ __forceinline__ float runtime_priority(const p2c_candidate_record& r, const SchedParams& P) {
+  const double x = 0.5 * (double)r.rt_hit_count + 0.5 * P.candidates_per_proxy;
+  return runtime_clamp(x < 1.0 ? x : 1.0);
+}
 
 __device__ __forceinline__ void warp_add(unsigned long long* dst, unsigned long long v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
@@ -176,7 +227,41 @@ __global__ void decide_kernel(SchedParams P, const p2c_candidate_record* cand, c
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool live = i < P.n;
   unsigned long long f_missing = 0, f_invalid = 0, f_ood = 0, f_unc = 0, f_any = 0;
-  if (live) {
+  if (live && P.mode >= 2) {  // RunDummyProposalScheduleFromRuntimeCandidates (:744-858) / the raw bypass
+    const p2c_candidate_record r = cand[i];
+    if (!candidate_ok(r)) atomicOr(L.acc + 10, kErrCandidate);
+    p2c_exact_work_item it{};
+    it.parent_candidate_id = r.candidate_id;
+    it.query_id = r.query_id;
+    it.slab_id = r.slab_id;
+    it.patch_a_id = r.patch_a_id;
+    it.patch_b_id = r.patch_b_id;
+    it.interval_t0 = P.cfg.fallback_interval_t0;
+    it.interval_t1 = P.cfg.fallback_interval_t1;
+    const unsigned base = query_mask(mask_qids, masks, P.n_masks, r.query_id, P.mode == 2);
+    it.feature_family_mask = base;
+    it.priority_score = (float)r.rt_hit_count;
+    it.source = 0;  // ProposalSource::kRaw
+    if (P.mode == 2) {
+      const bool ood = runtime_ood(r, P);
+      f_any = f_ood = ood;
+      it.source = kSourceFallback;
+      if (!ood) {
+        float s0, s1;
+        dummy_family_scores(base, &s0, &s1);
+        unsigned m = base;
+        if (s0 >= P.cfg.family_score_threshold) m |= 1u;
+        if (s1 >= P.cfg.family_score_threshold) m |= 2u;
+        it.feature_family_mask = m;
+        const float pr = runtime_priority(r, P);
+        it.priority_score = 0.0f < pr ? pr : 0.0f;  // std::max(0.0F, ...)
+        it.source = kSourceRefined;
+      }
+    }
+    L.staged[i] = it;
+    L.pkey[0][i] = priority_key(it.priority_score);
+    L.order[0][i] = (unsigned)i;
+  } else if (live) {
     const p2c_scheduling_config& c = P.cfg;
     long long ir = -1, io = -1;
     p2c_exact_work_item it{};
@@ -257,9 +342,11 @@ __global__ void write_kernel(SchedParams P, const unsigned* order, const p2c_can
   if (p < P.n) {
     p2c_exact_work_item it = L.staged[order[p]];
     it.work_item_id = P.cfg.first_work_item_id + (unsigned long long)p;
-    const unsigned long long original = P.mode == 0 ? cand[p].candidate_id : rows[p].candidate_id;
+    const unsigned long long original = P.mode == 1 ? rows[p].candidate_id : cand[p].candidate_id;
     reordered = it.parent_candidate_id != original ? 1ull : 0ull;
-    const bool ok = it.work_item_id != 0 && it.parent_candidate_id != 0 && it.query_id != 0 &&
+    const bool interval_ok = isfinite(it.interval_t0) && isfinite(it.interval_t1) && !(it.interval_t0 < 0.0) &&
+                             !(it.interval_t1 > 1.0) && !(it.interval_t0 > it.interval_t1);  // ValidateUnitInterval
+    const bool ok = it.work_item_id != 0 && it.parent_candidate_id != 0 && it.query_id != 0 && interval_ok &&
                     it.feature_family_mask != 0 && finite_f(it.priority_score);
     unsigned long long e = ok ? 0ull : kErrWorkItem;
     if (P.mode == 0) {  // per item the reference checks a missing family first, then unknown bits
@@ -294,6 +381,27 @@ __global__ void stats_kernel(SchedParams P, SchedLayout L, p2c_schedule_stats* s
   err[0] = L.acc[10];
   err[1] = L.acc[11];
   err[2] = L.acc[12];
+}
+
+// The dummy proposal outputs of materialized rows (:787-800): the row's
+// interval targets, the normalized family scores, non-negative priority and
+// cost targets, uncertainty 1 for an out-of-distribution candidate.
+__global__ void dummy_outputs_kernel(SchedParams P, const p2c_candidate_record* cand,
+                                     const p2c_proposal_feature_row* rows, const unsigned long long* mask_qids,
+                                     const unsigned* masks, p2c_proposal_output* outs) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= P.n) return;
+  const p2c_candidate_record r = cand[i];
+  const p2c_proposal_feature_row& row = rows[i];
+  p2c_proposal_output o{};
+  o.candidate_id = r.candidate_id;
+  for (int k = 0; k < 8; ++k) o.interval_scores[k] = row.interval_targets[k];
+  dummy_family_scores(query_mask(mask_qids, masks, P.n_masks, r.query_id, true), &o.family_scores[0],
+                      &o.family_scores[1]);
+  o.priority_score = 0.0f < row.priority_target ? row.priority_target : 0.0f;
+  o.cost_score = 0.0f < row.cost_target ? row.cost_target : 0.0f;
+  o.uncertainty_score = runtime_ood(r, P) ? 1.0f : (0.0f < row.uncertainty_target ? row.uncertainty_target : 0.0f);
+  outs[i] = o;
 }
 
 __global__ void init_acc_kernel(SchedLayout L) {
@@ -394,6 +502,60 @@ int p2c_schedule_work_items(int mode, const p2c_candidate_record* candidates_dev
       order = L.order[1];
     }
     write_kernel<<<grid_for(n), kThreads, 0, s>>>(P, order, candidates_dev, rows_dev, items_dev, L);
+  }
+  stats_kernel<<<1, 32, 0, s>>>(P, L, stats_dev, error_dev);
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+int p2c_dummy_schedule(int bypass, const p2c_candidate_record* candidates_dev, int64_t n, uint64_t primitive_count,
+                       uint64_t raw_hit_count, uint64_t compact_candidate_count, const uint64_t* mask_query_ids_dev,
+                       const uint32_t* masks_dev, int64_t n_masks, const p2c_scheduling_config* config,
+                       p2c_proposal_feature_row* rows_dev, p2c_proposal_output* outputs_dev,
+                       p2c_exact_work_item* items_dev, p2c_schedule_stats* stats_dev, uint64_t* error_dev,
+                       void* workspace_dev, size_t workspace_bytes, void* stream) {
+  using namespace p2c;
+  if (config == nullptr) return fail(P2C_ERR_INVALID, "scheduling config pointer is null");
+  if (!bypass) {
+    if (int rc = check_config(*config)) return rc;
+    if (primitive_count == 0) return fail(P2C_ERR_INVALID, "CandidateDensityStats.proxy_count must be non-zero");
+  }
+  if (n < 0 || n >= (1ll << 31) || n_masks < 0) return fail(P2C_ERR_INVALID, "counts must lie in [0, 2^31)");
+  if (stats_dev == nullptr || error_dev == nullptr || (n > 0 && (items_dev == nullptr || candidates_dev == nullptr)) ||
+      (n_masks > 0 && (mask_query_ids_dev == nullptr || masks_dev == nullptr)) ||
+      ((rows_dev == nullptr) != (outputs_dev == nullptr)))
+    return fail(P2C_ERR_INVALID, "input or output pointer is null");
+  const size_t need = carve(nullptr, n, 0, 0).total;
+  if (workspace_dev == nullptr || workspace_bytes < need)
+    return fail(P2C_ERR_INVALID, "scheduling workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  SchedLayout L = carve(workspace_dev, n, 0, 0);
+  cudaStream_t s = as_stream(stream);
+  const double P_ = (double)primitive_count;
+  const unsigned long long overlap_den = primitive_count >= 2 ? primitive_count / 2 : 1;  // :44-58
+  SchedParams P{bypass ? 3 : 2, *config, n, 0, bypass ? 0 : n, n_masks,
+                primitive_count == 0 ? 0.0 : (double)compact_candidate_count / P_,
+                (double)raw_hit_count / (double)overlap_den,
+                compact_candidate_count == 0 ? 0.0 : (double)raw_hit_count / (double)compact_candidate_count};
+  P2C_CUDA(cudaMemsetAsync(L.acc, 0, 16 * 8, s));
+  init_acc_kernel<<<1, 32, 0, s>>>(L);
+  const auto* mq = reinterpret_cast<const unsigned long long*>(mask_query_ids_dev);
+  if (n > 0) {
+    if (!bypass && rows_dev != nullptr) {  // the artifacts: runtime feature rows, then the dummy outputs
+      if (int rc = p2c_runtime_feature_rows(candidates_dev, n, primitive_count, raw_hit_count,
+                                            compact_candidate_count, mask_query_ids_dev, masks_dev, n_masks,
+                                            rows_dev, reinterpret_cast<uint64_t*>(L.acc + 13), stream))
+        return rc;
+      dummy_outputs_kernel<<<grid_for(n), kThreads, 0, s>>>(P, candidates_dev, rows_dev, mq, masks_dev, outputs_dev);
+    }
+    decide_kernel<<<grid_for(n), kThreads, 0, s>>>(P, candidates_dev, nullptr, nullptr, mq, masks_dev, L);
+    const unsigned* order = L.order[0];
+    if (!bypass && !config->preserve_candidate_order) {
+      size_t tb = L.tmp_bytes;
+      P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.pkey[0], L.pkey[1], L.order[0], L.order[1], (int)n, 0,
+                                               32, s));
+      order = L.order[1];
+    }
+    write_kernel<<<grid_for(n), kThreads, 0, s>>>(P, order, candidates_dev, nullptr, items_dev, L);
   }
   stats_kernel<<<1, 32, 0, s>>>(P, L, stats_dev, error_dev);
   P2C_CUDA(cudaGetLastError());

@@ -1135,7 +1135,10 @@ def generate_candidates_for_external_batch(batch, backend_name: str = "cpu_refer
             raise ValueError("external batch candidate generation requires at least one query")
         external._first_error(b)
         raise ValueError("P2CCCD was built without OptiX support; configure with -DP2CCCD_ENABLE_OPTIX=ON")
-    r = external.generate(b)
+    return _external_result(b, external.generate(b), name)
+
+
+def _external_result(b: dict, r: dict, name: str) -> ExternalBatchCandidateResult:
     res = ExternalBatchCandidateResult()
     res.backend_name = name
     res.primitive_count, res.raw_hit_count = r["primitive_count"], r["raw_hit_count"]
@@ -1423,6 +1426,10 @@ def _schedule(cand, rows, outs, masks, config, mode) -> tuple:
 
     cfg = {k: getattr(config, k) for k, _ in ProposalSchedulingConfig._fields}
     items, stats = schedule_work_items(cand, rows, outs, dict(masks or {}), mode, **cfg)
+    return _queue_objects(items), _stats_object(stats)
+
+
+def _queue_objects(items: np.ndarray) -> list:
     queue = []
     for r in items:
         w = ExactWorkItem()
@@ -1433,10 +1440,104 @@ def _schedule(cand, rows, outs, masks, config, mode) -> tuple:
         w.priority_score = float(r["priority_score"])
         w.source = ProposalSource(int(r["source"]))
         queue.append(w)
+    return queue
+
+
+def _stats_object(stats) -> ProposalScheduleStats:
     st = ProposalScheduleStats()
     for k, _ in ProposalScheduleStats._fields:
         setattr(st, k, bool(stats[k]) if k == "monotonic_safe" else int(stats[k]))
-    return queue, st
+    return st
+
+
+def _output_objects(outs: np.ndarray) -> list:
+    res = []
+    for r in outs:
+        o = ProposalOutput()
+        o.candidate_id = int(r["candidate_id"])
+        o.interval_scores = [float(x) for x in r["interval_scores"]]
+        o.family_scores = [float(x) for x in r["family_scores"]]
+        o.priority_score, o.cost_score = float(r["priority_score"]), float(r["cost_score"])
+        o.uncertainty_score = float(r["uncertainty_score"])
+        res.append(o)
+    return res
+
+
+class ProposalRuntimeScheduleResult(_Struct):  # proposal_policy.h:38-43
+    _fields = (("feature_rows", list), ("proposal_outputs", list), ("work_queue", list),
+               ("stats", ProposalScheduleStats))
+
+
+class ExternalBatchDummyProposalScheduleResult(_Struct):  # py_module.cpp:202-209
+    _fields = (("candidate_result", ExternalBatchCandidateResult), ("feature_rows", list),
+               ("proposal_outputs", list), ("work_queue", list), ("stats", ProposalScheduleStats),
+               ("proposal_elapsed_ms", 0.0))
+
+
+def _config_dict(config) -> dict:
+    config = config if config is not None else ProposalSchedulingConfig()
+    return {k: getattr(config, k) for k, _ in ProposalSchedulingConfig._fields}
+
+
+def run_dummy_runtime_proposal_schedule(candidates, primitive_count: int, raw_hit_count: int,
+                                        compact_candidate_count: int, conservative_family_masks_by_query_id,
+                                        config=None, materialize_artifacts: bool = True
+                                        ) -> ProposalRuntimeScheduleResult:  # py_module.cpp:1009-1033
+    """RunDummyProposalScheduleFromRuntimeCandidates on the GPU: the runtime
+    feature rows, density-derived dummy proposals and the ordered queue."""
+    from p2cccd_b200.schedule import dummy_schedule
+
+    items, stats, rows, outs = dummy_schedule(_candidate_array(candidates), primitive_count, raw_hit_count,
+                                              compact_candidate_count, dict(conservative_family_masks_by_query_id or {}),
+                                              materialize_artifacts, **_config_dict(config))
+    res = ProposalRuntimeScheduleResult()
+    res.feature_rows, res.proposal_outputs = _row_objects(rows), _output_objects(outs)
+    res.work_queue, res.stats = _queue_objects(items), _stats_object(stats)
+    return res
+
+
+def external_batch_dummy_schedule(b: dict, r: dict, config=None, materialize_artifacts: bool = False) -> tuple:
+    """The schedule half of GenerateExternalBatchDummyProposalScheduleOrThrow
+    (py_module.cpp:284-360) on the device, for a batch (column arrays) and its
+    candidates from ``external.generate``: a mask per runtime query id from
+    its query's family (:213-246), then the raw bypass when every candidate
+    has its own query and a single-family mask (:248-318), else the dummy
+    schedule with the batch's counts (:320-349).  Returns (items, stats,
+    rows, outputs)."""
+    from p2cccd_b200.schedule import dummy_schedule
+
+    cand = r["candidates"]
+    masks = dict(zip(r["runtime_query_ids"].tolist(), np.where(b["family"] == 0, 1, 2).tolist()))
+    q = cand["query_id"]
+    fam = np.array([masks.get(int(x), 3) for x in q], np.int64) if len(q) else np.zeros(0, np.int64)
+    bypass = len(np.unique(q)) == len(q) and bool(np.all((fam != 0) & ((fam & (fam - 1)) == 0)))
+    return dummy_schedule(cand, r["primitive_count"], r["raw_hit_count"], r["compact_candidate_count"], masks,
+                          materialize_artifacts, bypass=bypass, **_config_dict(config))
+
+
+def generate_external_batch_dummy_proposal_schedule(batch, backend_name: str = "cpu_reference",
+                                                    allow_optix_cpu_fallback: bool = False, config=None,
+                                                    materialize_artifacts: bool = False
+                                                    ) -> ExternalBatchDummyProposalScheduleResult:
+    """GenerateExternalBatchDummyProposalScheduleOrThrow (py_module.cpp:269-361):
+    the batch's candidates, then its exact work queue, on the GPU."""
+    import time
+
+    from p2cccd_b200 import external
+
+    name = _backend(backend_name)
+    b = _external_batch(batch)
+    if name == "optix_cpu_fallback" and not allow_optix_cpu_fallback:
+        generate_candidates_for_external_batch(b, backend_name, allow_optix_cpu_fallback)  # raises its error
+    r = external.generate(b)
+    res = ExternalBatchDummyProposalScheduleResult()
+    res.candidate_result = _external_result(b, r, name)
+    start = time.perf_counter()
+    items, stats, rows, outs = external_batch_dummy_schedule(b, r, config, materialize_artifacts)
+    res.proposal_elapsed_ms = (time.perf_counter() - start) * 1e3
+    res.feature_rows, res.proposal_outputs = _row_objects(rows), _output_objects(outs)
+    res.work_queue, res.stats = _queue_objects(items), _stats_object(stats)
+    return res
 
 
 def schedule_runtime_exact_work_items(candidates, rows, proposal_outputs, conservative_family_masks_by_query_id,
