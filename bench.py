@@ -1,7 +1,8 @@
 #!/usr/bin/env python
 """Benchmark of the B200 certification hot path (one JSON line on rank 0).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scene|plain|batch|cloth|serve|proxy] [--impl b200|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload scene|plain|batch|cloth|serve|proxy|groups]
+                    [--impl b200|reference]
 
 A step is one pass of the hot path over one batch of seeded synthetic input:
   * scene (default): two 40,960-triangle UV spheres (FP64, rigid translation
@@ -14,6 +15,8 @@ metric: certified CCD queries/s (one query = one primitive certificate).
   * proxy: a proxy scene (rigid bodies x patches x motion segments x time
     slabs) built, its raw hits and compacted candidates generated and the
     proposal feature rows of every candidate formed; metric: proxies/s.
+  * groups: the candidate-group interface (run_native_dense_group_exact_early_stop)
+    over 1M candidate rows in query groups; metric: rows/s.
 
 Timing: W untimed warm-up steps, then K steps each bracketed by CUDA events
 on the launching stream, with a 512 MB L2 flush between steps (outside the
@@ -1181,6 +1184,125 @@ def run_proxy(args) -> dict | None:
     }
 
 
+GROUP_ROWS = 1_000_000  # rows of the candidate-group workload (--group-rows)
+GROUP_CFG = {"threshold": 0.75, "limit": 3, "penalty": 0.22}  # the binding's defaults
+
+
+def _groups_config(rows: dict, n_groups: int) -> dict:
+    return {"workload": f"candidate-group interface: run_native_dense_group_exact_early_stop over "
+                        f"{len(rows['query_id'])} candidate rows in {n_groups} query groups of log-uniform size "
+                        f"1-256 (rows shuffled), 20% positive labels; uncertainty threshold 0.75, attempt limit 3, "
+                        f"miss penalty 0.22 (the binding's defaults)",
+            "rows_per_step": len(rows["query_id"]), "groups": n_groups}
+
+
+def _groups_reference(rows: dict, budget_s: float) -> dict:
+    """The reference's RunDenseGroupExactEarlyStop after its binding's row
+    parse (oracle/_ref, unchanged sources, 1 thread as written), whole row
+    sets until budget_s has passed."""
+    import oracle
+
+    done, runs, t0 = 0, 0, time.perf_counter()
+    while True:
+        oracle.ref_dense_group(rows, **GROUP_CFG)
+        done += len(rows["query_id"])
+        runs += 1
+        el = time.perf_counter() - t0
+        if el >= budget_s:
+            break
+    return {"rows": done, "seconds": el, "runs": runs}
+
+
+def run_groups(args) -> dict | None:
+    import numpy as np
+    import torch
+
+    from p2cccd_b200 import workloads
+    from p2cccd_b200.dense_groups import DenseGroupEarlyStop, _ORDER, _query_bits, upload
+
+    world, rank, local = _dist_setup(args)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    rows = workloads.dense_group_rows(GROUP_ROWS, 20261203 + rank)
+    n = len(rows["query_id"])
+    qbits = _query_bits(rows["query_id"])
+    tens = upload(rows, dev)
+    runner = DenseGroupEarlyStop(n, dev)
+
+    def step():
+        runner.run(tens, n, query_bits=qbits, **GROUP_CFG)
+
+    step()
+    st = runner.result()
+    n_groups = int(st["group_count"])
+    host = {k: torch.from_numpy(rows[k].view(np.int64) if rows[k].dtype == np.uint64 else rows[k]).pin_memory()
+            for k in _ORDER}
+    h_stats = torch.empty_like(runner.stats, device="cpu").pin_memory()
+
+    def step_e2e():  # rows from pinned host memory in, the stats back
+        for k in _ORDER:
+            tens[k].copy_(host[k], non_blocking=True)
+        step()
+        h_stats.copy_(runner.stats, non_blocking=True)
+        torch.cuda.current_stream(dev).synchronize()
+
+    stream = torch.cuda.current_stream(dev)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=dev)
+    sampler = ClockSampler(dev.index if world > 1 else 0)
+    sampler.start()
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    _barrier(world)
+    torch.cuda.synchronize()
+    t_begin = time.time()
+    times = time_steps(torch, step, args.steps, flush, stream)
+    torch.cuda.synchronize()
+    t_end = time.time()
+    _barrier(world)
+    clocks = sampler.stop((t_begin, t_end))
+    for _ in range(max(1, args.warmup)):
+        step_e2e()
+    e2e_times = time_steps(torch, step_e2e, args.steps, flush, stream)
+    ms = statistics.mean(times)
+    value, ms_max = replica_rate(world, n, ms)
+    e2e_value, e2e_ms = replica_rate(world, n, statistics.mean(e2e_times))
+    n_kernels, kernel_names = count_kernels(torch, step)
+    peaks = _load_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm_src = "of measured (MEASURED_PEAKS.json hbm_gbs)" if "hbm_gbs" in peaks else "of fallback (6.65 TB/s)"
+    row_bytes = 128 * n  # query + candidate id, cost target, 8 trace doubles, 8 scores, 3 scores
+    roofline = {"bound": "hbm", "peak": hbm_peak, "unit": "GB/s", "traffic": None, "peak_source": hbm_src,
+                "kernel": "whole replay (parse, two stable sorts, gather, group walk, ordered folds)",
+                "achieved": row_bytes / (ms * 1e-3) / 1e9, "frac": row_bytes / (ms * 1e-3) / 1e9 / hbm_peak,
+                "algorithmic_bytes_per_step": row_bytes,
+                "bytes_per_unit": "128 B per candidate row read once",
+                "note": "the work totals are folded one term at a time in the reference's order "
+                        "(bit-exact doubles): a dependent FP64 add chain per total"}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        r = _groups_reference(rows, args.cpu_budget)
+        cpu = {"value": r["rows"] / r["seconds"], "unit": "rows/s", "cores": 1, "kind": "reference",
+               "sample": f"the same {n} rows, {r['runs']} whole run(s) of the binding's parse + "
+                         "RunDenseGroupExactEarlyStop (1 thread as written)"}
+    if rank != 0:
+        return None
+    return {
+        "metric": "candidate-group early stop: rows/s", "value": value, "unit": "rows/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
+        "p50_ms": statistics.median(times), "p99_ms": sorted(times)[max(0, int(0.99 * len(times)) - 1)],
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {**_groups_config(rows, n_groups), "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write)",
+                   "parallelism": f"replicas x{world}"},
+        "e2e": {"value": e2e_value, "unit": "rows/s", "ms_per_step": e2e_ms, "h2d_bytes_per_step": row_bytes,
+                "d2h_bytes_per_step": int(h_stats.numel())},
+        "gpu_launches": n_kernels * args.steps if n_kernels >= 0 else None,
+        "kernels_per_step": kernel_names,
+        "result": {"groups": n_groups, "learned_exact_calls": int(st["learned_exact_calls"]),
+                   "learned_exact_work": float(st["learned_exact_work"]), "tp": int(st["tp"]), "fn": int(st["fn"])},
+        "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
+    }
+
+
 BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
 CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = configs[3])
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
@@ -1199,6 +1321,25 @@ def run_reference(args) -> dict | None:
 
     if not oracle.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref/libp2c_ref.so was not built"}
+    if args.workload == "groups":
+        from p2cccd_b200 import workloads as wl
+
+        rows = wl.dense_group_rows(GROUP_ROWS, 20261203)
+        budget = REF_ARM_BUDGET_S / max(1, args.steps + args.warmup)
+        for _ in range(args.warmup):
+            _groups_reference(rows, 0.0)
+        runs = [_groups_reference(rows, budget) for _ in range(args.steps)]
+        value = sum(r["rows"] for r in runs) / sum(r["seconds"] for r in runs)
+        ms = sum(r["seconds"] for r in runs) / sum(r["runs"] for r in runs) * 1e3
+        n_groups = int(oracle.ref_dense_group(rows, **GROUP_CFG)["group_count"])
+        return {"metric": "candidate-group early stop: rows/s", "value": value, "unit": "rows/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": _groups_config(rows, n_groups), "impl": "reference",
+                "cpu_baseline": {"value": value, "unit": "rows/s", "cores": 1, "kind": "reference",
+                                 "sample": "whole row sets: the binding's row parse + RunDenseGroupExactEarlyStop, "
+                                           "1 thread as written"},
+                "e2e": {"value": value, "unit": "rows/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     if args.workload == "proxy":
         inp = _proxy_input(PROXY_OBJECTS, 20261203)
         inp["seed"] = 20261203
@@ -1323,7 +1464,7 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=2000)
     ap.add_argument("--warmup", type=int, default=20)
-    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS) + ["serve", "proxy"])
+    ap.add_argument("--workload", default="scene", choices=sorted(WORKLOADS) + ["serve", "proxy", "groups"])
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--cpu-budget", type=float, default=10.0, help="seconds of reference CPU work")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -1334,11 +1475,13 @@ def main():
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     ap.add_argument("--proxy-objects", type=int, default=32, help="proxy: rigid bodies of 200 patches x 8 slabs")
+    ap.add_argument("--group-rows", type=int, default=1_000_000, help="groups: candidate rows per step")
     ap.add_argument("--benchmark-rows", default=None, metavar="DIR",
                     help="also write the run as BenchmarkRowV2 JSONL / CSV (the reference's export schema) to DIR")
     args = ap.parse_args()
-    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS
+    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS, GROUP_ROWS
     PROXY_OBJECTS = max(2, args.proxy_objects)
+    GROUP_ROWS = max(1, args.group_rows)
     BATCH_SCENES, AUTOTUNE_REPS = max(1, args.scenes), max(0, args.autotune_reps)
     CLOTH_N = max(9, args.cloth_n)
     if args.impl == "reference":
@@ -1347,6 +1490,8 @@ def main():
         line = run_serve(args)
     elif args.workload == "proxy":
         line = run_proxy(args)
+    elif args.workload == "groups":
+        line = run_groups(args)
     else:
         line = run_b200(args)
     if line is not None:

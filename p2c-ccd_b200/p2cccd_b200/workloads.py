@@ -122,3 +122,36 @@ def plain_queries(spec: PlainSpec = PlainSpec()) -> dict:
     vf, vf_cat, _ = _vf(g, spec)
     ee, ee_cat, _ = _ee(g, spec)
     return {"vf": vf, "ee": ee, "vf_cat": vf_cat, "ee_cat": ee_cat, "spec": spec}
+
+
+def dense_group_rows(n_rows: int, seed: int = DEFAULT_SEED, max_group: int = 256) -> dict:
+    """Rows of the candidate-group interface (the arrays
+    run_native_dense_group_exact_early_stop reads) for ``n_rows`` candidates
+    in query groups of log-uniform size 1..``max_group``, rows shuffled:
+    labels (oracle_trace[:, 0]) positive for ~20% of candidates, full exact
+    costs gamma-distributed (some zero or negative: replaced by 1 on the
+    path), contact intervals inside [0, 1], eight interval scores, and
+    priority / cost / uncertainty scores as a proposal model would emit."""
+    g = rng(seed)
+    sizes = []
+    total = 0
+    while total < n_rows:
+        s = int(np.exp(g.uniform(0.0, np.log(max_group + 1.0))))
+        s = max(1, min(s, n_rows - total))
+        sizes.append(s)
+        total += s
+    q = np.repeat(np.arange(1, len(sizes) + 1, dtype=np.uint64) * np.uint64(7919), sizes)
+    q = q[g.permutation(n_rows)]
+    trace = np.zeros((n_rows, 8))
+    trace[:, 0] = (g.random(n_rows) < 0.2).astype(np.float64)
+    trace[:, 5] = g.gamma(2.0, 40.0, n_rows)
+    trace[g.random(n_rows) < 0.01, 5] = 0.0
+    c0 = g.random(n_rows)
+    trace[:, 6] = c0
+    trace[:, 7] = np.minimum(1.0, c0 + g.random(n_rows) * 0.25)
+    return {"query_id": q, "candidate_id": np.arange(1, n_rows + 1, dtype=np.uint64),
+            "cost_target": g.random(n_rows).astype(np.float32), "oracle_trace": trace,
+            "interval_scores": g.normal(0.0, 1.0, (n_rows, 8)).astype(np.float32),
+            "priority_score": g.normal(0.0, 1.0, n_rows).astype(np.float32),
+            "cost_score": g.random(n_rows).astype(np.float32),
+            "uncertainty_score": g.beta(2.0, 5.0, n_rows).astype(np.float32)}
