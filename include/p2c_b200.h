@@ -830,6 +830,13 @@ int p2c_dense_group_early_stop(int64_t n, const uint64_t* query_id_dev, const ui
                                const p2c_dense_group_config* config, p2c_dense_group_stats* stats_dev,
                                void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* The left-to-right double sum of n non-negative terms (NaN-free; +inf
+ * allowed), bit-identical to `s = 0; for (i) s += terms[i];`: the ordered
+ * accumulation RunDenseGroupExactEarlyStop makes (group_scheduler.cpp:
+ * 128-230), computed with block scans instead of one dependent add per term.
+ * Writes *out_dev; one block; no host sync. */
+int p2c_ordered_sum(const double* terms_dev, int64_t n, double* out_dev, void* stream);
+
 /* ---- refinement children ------------------------------------------------- */
 size_t p2c_refinement_children_workspace_bytes(int64_t n_parents);
 

@@ -44,7 +44,6 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned char kColl = 1, kOverlap = 2, kHighUnc = 4;
-constexpr int kFoldTile = 2048;  // doubles per shared-memory tile of the fold
 
 // Integer totals, in p2c_dense_group_stats order of the counters below.
 enum {
@@ -377,49 +376,201 @@ __global__ void __launch_bounds__(kThreads) group_kernel(long long n, unsigned l
 
 struct FoldJob {
   const double* src[3];
-  const int* count[3];  // device counts
+  const int* count[3];   // device counts, or null: the fixed counts
+  long long fixed[3];
   double* out[3];
 };
 
-// One block per total: warp 0 adds the values in order from one shared tile
-// while the other warps load the next.
-__global__ void __launch_bounds__(kThreads) fold_kernel(FoldJob job) {
-  __shared__ double buf[2][kFoldTile];
+// ---- the ordered fold ------------------------------------------------------
+//
+// A sum s of non-negative doubles, added one term at a time in a fixed order
+// with round-to-nearest-even, reproduced exactly with block-wide scans.
+// While s stays below the top of its binade, s = S * u with u its unit in the
+// last place and S an integer below 2^53, and adding a term x gives
+// S + floor(x / u) + r, where r = 1 when the remainder of x / u is above one
+// half, 0 below, and on an exact half the bit that makes the result even:
+// r depends on S only through its parity.  Each term is therefore a pair of
+// increments (for an even and for an odd S), pairs compose associatively
+// ((a then b)[p] = a[p] + b[(p + a[p]) mod 2]), and a block scan gives every
+// term the S in front of it.  The first term whose exact sum could reach the
+// top of the binade (or an infinite term) is added with the hardware DADD;
+// the fold then continues from it in the new binade.  Each such step at least
+// doubles s, so there are at most a few dozen of them.  A zero-start sum
+// takes its first non-zero term exactly.
+
+constexpr int kFoldThreads = 512;
+constexpr int kFoldPerThread = 8;  // consecutive terms per thread
+constexpr int kFoldChunk = kFoldThreads * kFoldPerThread;
+constexpr int kFoldWarps = kFoldThreads / 32;
+constexpr unsigned long long kTwo53 = 1ull << 53;
+
+struct IncPair {
+  unsigned long long e, o;  // increments of S for an even / an odd S
+};
+
+__device__ __forceinline__ IncPair compose(const IncPair& a, const IncPair& b) {  // a, then b
+  IncPair c;
+  c.e = a.e + ((a.e & 1ull) ? b.o : b.e);
+  c.o = a.o + ((a.o & 1ull) ? b.e : b.o);
+  return c;
+}
+
+__device__ __forceinline__ IncPair shfl_up_pair(const IncPair& v, int o) {
+  IncPair r;
+  r.e = __shfl_up_sync(0xffffffffu, v.e, o);
+  r.o = __shfl_up_sync(0xffffffffu, v.o, o);
+  return r;
+}
+
+__device__ __forceinline__ IncPair warp_inclusive(IncPair v, int lane) {
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const IncPair up = shfl_up_pair(v, o);
+    if (lane >= o) v = compose(up, v);
+  }
+  return v;
+}
+
+struct FoldShared {
+  unsigned long long we[32], wo[32];
+  double s;
+  long long pos;
+  int first;
+};
+
+// One block per total.
+__global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
+  __shared__ FoldShared sh;
   const int b = blockIdx.x;  // selects without indexing the parameter arrays dynamically
   const double* src = b == 0 ? job.src[0] : (b == 1 ? job.src[1] : job.src[2]);
-  const long long cnt = *(b == 0 ? job.count[0] : (b == 1 ? job.count[1] : job.count[2]));
-  const int tid = threadIdx.x;
-  for (long long k = tid; k < min((long long)kFoldTile, cnt); k += kThreads) buf[0][k] = src[k];
+  const int* cp = b == 0 ? job.count[0] : (b == 1 ? job.count[1] : job.count[2]);
+  const long long cnt = cp ? (long long)*cp : (b == 0 ? job.fixed[0] : (b == 1 ? job.fixed[1] : job.fixed[2]));
+  const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+  const IncPair zero{0ull, 0ull};
+  if (t == 0) {
+    sh.s = 0.0;
+    sh.pos = 0;
+  }
   __syncthreads();
-  double s = 0.0;
-  int cur = 0;
-  for (long long base = 0; base < cnt; base += kFoldTile) {
-    const long long next = base + kFoldTile;
-    if (tid >= 32) {
-      const long long m = min((long long)kFoldTile, cnt - next);
-      for (long long k = tid - 32; k < m; k += kThreads - 32) buf[cur ^ 1][k] = src[next + k];
-    } else {
-      const int m = (int)min((long long)kFoldTile, cnt - base);
-      const double* b = buf[cur];
-      int k = 0;
-      for (; k + 8 <= m; k += 8) {
-        const double v0 = b[k], v1 = b[k + 1], v2 = b[k + 2], v3 = b[k + 3];
-        const double v4 = b[k + 4], v5 = b[k + 5], v6 = b[k + 6], v7 = b[k + 7];
-        s += v0;
-        s += v1;
-        s += v2;
-        s += v3;
-        s += v4;
-        s += v5;
-        s += v6;
-        s += v7;
+  double x[kFoldPerThread];
+  long long loaded = -1;  // chunk start the registers hold
+  while (true) {
+    const double s = sh.s;
+    const long long pos = sh.pos;
+    if (pos >= cnt || isinf(s)) break;
+    const int len = (int)min((long long)kFoldChunk, cnt - pos);
+    if (loaded != pos) {
+#pragma unroll
+      for (int k = 0; k < kFoldPerThread; ++k) {
+        const int i = t * kFoldPerThread + k;
+        x[k] = i < len ? src[pos + i] : 0.0;
       }
-      for (; k < m; ++k) s += b[k];
+    }
+    double nx[kFoldPerThread];  // the next chunk, in case this one has no binade step
+#pragma unroll
+    for (int k = 0; k < kFoldPerThread; ++k) {
+      const long long i = pos + len + t * kFoldPerThread + k;
+      nx[k] = i < cnt ? src[i] : 0.0;
+    }
+    if (t == 0) sh.first = len;
+    __syncthreads();  // everyone read s and pos; first is reset
+    if (s == 0.0) {  // 0 + x == x: the first non-zero term starts the sum
+#pragma unroll
+      for (int k = 0; k < kFoldPerThread; ++k) {
+        const int i = t * kFoldPerThread + k;
+        if (i < len && x[k] != 0.0) {
+          atomicMin(&sh.first, i);
+          break;
+        }
+      }
+      __syncthreads();
+      const int f = sh.first;
+#pragma unroll
+      for (int k = 0; k < kFoldPerThread; ++k)
+        if (t * kFoldPerThread + k == f) sh.s = x[k];
+      if (t == 0) sh.pos = pos + (f < len ? f + 1 : len);
+      loaded = -1;
+      __syncthreads();
+      continue;
+    }
+    const int ue = max(ilogb(s), -1022) - 52;
+    const unsigned long long S = (unsigned long long)ldexp(s, -ue);
+    IncPair inc[kFoldPerThread];
+    unsigned long long m[kFoldPerThread];
+    bool big[kFoldPerThread];
+    IncPair local = zero;
+#pragma unroll
+    for (int k = 0; k < kFoldPerThread; ++k) {
+      const bool in = t * kFoldPerThread + k < len;
+      const double q = ldexp(x[k], -ue);
+      big[k] = in && !(q < 9007199254740992.0);
+      const double mf = big[k] || !in ? 0.0 : floor(q);
+      const double f = big[k] || !in ? 0.0 : q - mf;
+      m[k] = (unsigned long long)mf;
+      const bool above = f > 0.5, tie = f == 0.5;
+      inc[k].e = m[k] + (above ? 1ull : (tie ? (m[k] & 1ull) : 0ull));
+      inc[k].o = m[k] + (above ? 1ull : (tie ? ((m[k] + 1ull) & 1ull) : 0ull));
+      if (big[k]) inc[k] = IncPair{kTwo53, kTwo53};  // never applied: the binade step comes first
+      local = compose(local, inc[k]);
+    }
+    const IncPair incl = warp_inclusive(local, lane);
+    if (lane == 31) {
+      sh.we[w] = incl.e;
+      sh.wo[w] = incl.o;
     }
     __syncthreads();
-    cur ^= 1;
+    if (w == 0) {
+      const IncPair v = warp_inclusive(lane < kFoldWarps ? IncPair{sh.we[lane], sh.wo[lane]} : zero, lane);
+      IncPair ex = shfl_up_pair(v, 1);
+      if (lane == 0) ex = zero;
+      __syncwarp();
+      sh.we[lane] = ex.e;
+      sh.wo[lane] = ex.o;
+    }
+    __syncthreads();
+    IncPair ein = shfl_up_pair(incl, 1);
+    if (lane == 0) ein = zero;
+    const IncPair wp{sh.we[w], sh.wo[w]};
+    const IncPair ex = compose(wp, ein);
+    unsigned long long P = S + ((S & 1ull) ? ex.o : ex.e);
+    int mine = len;
+    unsigned long long P_at = 0;
+#pragma unroll
+    for (int k = 0; k < kFoldPerThread; ++k) {
+      const bool in = t * kFoldPerThread + k < len;
+      if (in && mine == len) {
+        if (big[k] || P >= kTwo53 || P + m[k] >= kTwo53) {
+          mine = t * kFoldPerThread + k;
+          P_at = P;
+        } else {
+          P += (P & 1ull) ? inc[k].o : inc[k].e;
+        }
+      }
+    }
+    if (mine < len) atomicMin(&sh.first, mine);
+    __syncthreads();
+    const int c = sh.first;
+    if (c == len) {  // no binade step: the last thread holds the end of the chunk
+      if (t == (len - 1) / kFoldPerThread) {
+        sh.s = ldexp((double)P, ue);
+        sh.pos = pos + len;
+      }
+    } else if (mine == c) {
+#pragma unroll
+      for (int k = 0; k < kFoldPerThread; ++k)
+        if (t * kFoldPerThread + k == c) sh.s = ldexp((double)P_at, ue) + x[k];
+      sh.pos = pos + c + 1;
+    }
+    __syncthreads();
+    if (sh.pos == pos + len) {
+#pragma unroll
+      for (int k = 0; k < kFoldPerThread; ++k) x[k] = nx[k];
+      loaded = pos + len;
+    } else {
+      loaded = -1;
+    }
   }
-  if (tid == 0) *(b == 0 ? job.out[0] : (b == 1 ? job.out[1] : job.out[2])) = s;
+  if (t == 0) *(b == 0 ? job.out[0] : (b == 1 ? job.out[1] : job.out[2])) = sh.s;
 }
 
 __global__ void finish_kernel(long long n, DenseLayout L, p2c_dense_group_stats* st) {
@@ -520,11 +671,22 @@ int p2c_dense_group_early_stop(int64_t n, const uint64_t* query_id_dev, const ui
     P2C_CUDA(cub::DeviceSelect::If(L.tmp, tb, L.terms, L.compact, &L.acc->n_terms, (int)(3 * n), NonZeroTerm{}, s));
     FoldJob job{{L.compact, L.g_full, L.g_cost},
                 {&L.acc->n_terms, &L.acc->n_groups, &L.acc->n_groups},
+                {0, 0, 0},
                 {&stats_dev->learned_exact_work, &stats_dev->no_proposal_exact_work,
                  &stats_dev->cost_before_first_positive_sum}};
-    fold_kernel<<<3, kThreads, 0, s>>>(job);
+    fold_kernel<<<3, kFoldThreads, 0, s>>>(job);
   }
   finish_kernel<<<1, 32, 0, s>>>(n, L, stats_dev);
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+int p2c_ordered_sum(const double* terms_dev, int64_t n, double* out_dev, void* stream) {
+  using namespace p2c;
+  if (n < 0) return fail(P2C_ERR_INVALID, "term count must be non-negative");
+  if (out_dev == nullptr || (n > 0 && terms_dev == nullptr)) return fail(P2C_ERR_INVALID, "term or output pointer is null");
+  FoldJob job{{terms_dev, terms_dev, terms_dev}, {nullptr, nullptr, nullptr}, {n, 0, 0}, {out_dev, out_dev, out_dev}};
+  fold_kernel<<<1, kFoldThreads, 0, as_stream(stream)>>>(job);
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;
 }

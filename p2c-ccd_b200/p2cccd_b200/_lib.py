@@ -98,6 +98,7 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_dummy_schedule": (_int, [_int, _c_void_p, _i64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64,
                                   _c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                   _c_void_p, _c_void_p, _size, _c_void_p]),
+    "p2c_ordered_sum": (_int, [_c_void_p, _i64, _c_void_p, _c_void_p]),
     "p2c_dense_group_early_stop_workspace_bytes": (_size, [_i64]),
     "p2c_dense_group_early_stop": (_int, [_i64] + [_c_void_p] * 8 + [_c_void_p, _c_void_p, _c_void_p, _size,
                                                                      _c_void_p]),

@@ -153,3 +153,17 @@ def result_dict(st: np.void, parse_ms: float = 0.0, native_ms: float = 0.0, uplo
     out["exact_call_reduction"] = 0.0 if npc == 0 else 1.0 - float(lec) / float(npc)
     out["exact_work_reduction"] = 0.0 if npw <= 0.0 else 1.0 - lew / npw
     return out
+
+
+def ordered_sum(terms: torch.Tensor) -> torch.Tensor:
+    """p2c_ordered_sum: the left-to-right double sum of non-negative terms (a
+    CUDA float64 tensor), bit-identical to a sequential loop; returns a
+    one-element device tensor (no host sync)."""
+    lib = _lib.load()
+    t = terms.contiguous()
+    if t.dtype != torch.float64 or not t.is_cuda:
+        raise TypeError("terms must be a CUDA float64 tensor")
+    out = torch.empty(1, dtype=torch.float64, device=t.device)
+    _lib.check(lib.p2c_ordered_sum(t.data_ptr() if t.numel() else None, t.numel(), out.data_ptr(),
+                                   _stream_ptr(t.device)))
+    return out

@@ -157,3 +157,47 @@ def test_large_replay_against_reference(oracle_mod):
     r = DenseGroupEarlyStop(200_000)
     r.run(upload(rows), 200_000, threshold=0.93, limit=4, query_bits=_query_bits(rows["query_id"]))
     assert _same(r.result(), want) == []
+
+
+def _ordered_cases():
+    """Non-negative term sequences that stress the ordered sum: wide dynamic
+    range, exact half-ulp ties, runs of zeros (also in front), subnormals,
+    terms that jump several binades, sums that round up to a power of two,
+    an infinite term, and lengths around the 4,096-term chunk."""
+    rng = np.random.default_rng(5)
+    cases = [np.zeros(0), np.zeros(10), np.array([0.0, 0.0, 3.5]), np.array([2.0 ** -1074] * 5000)]
+    for n in (1, 31, 4095, 4096, 4097, 12289, 50000):
+        cases.append(rng.gamma(2.0, 3.0, n))
+        cases.append(np.exp(rng.uniform(-40.0, 40.0, n)))
+        cases.append(rng.integers(0, 64, n) * 2.0 ** rng.integers(-60, 10, n).astype(np.float64))
+        z = rng.random(n)
+        z[rng.random(n) < 0.4] = 0.0
+        cases.append(z)
+        cases.append(rng.integers(0, 3, n) * 0.5 + 2.0 ** 52 * (rng.random(n) < 0.05))
+    ups = np.full(9000, 1.0)  # 2^53 + 1 + 1 + ... ties-to-even at every step
+    ups[0] = 2.0 ** 53
+    cases.append(ups)
+    w = rng.random(6000) * 1e292
+    w[0], w[3000], w[3001] = 1e300, 1e308, 1e308  # overflow to inf
+    cases.append(w)
+    w = rng.random(6000)
+    w[4500] = np.inf
+    cases.append(w)
+    return cases
+
+
+@pytest.mark.gpu
+def test_ordered_sum_is_the_sequential_sum():
+    import math
+
+    import torch
+
+    from p2cccd_b200.dense_groups import ordered_sum
+
+    for i, c in enumerate(_ordered_cases()):
+        want = 0.0
+        for x in c.tolist():
+            want += x
+        got = float(ordered_sum(torch.from_numpy(np.ascontiguousarray(c, np.float64)).cuda()).item())
+        assert (got == want and math.copysign(1.0, got) == math.copysign(1.0, want)) or \
+            (math.isnan(got) and math.isnan(want)), (i, len(c), got, want)
