@@ -394,14 +394,16 @@ struct FoldJob {
 // ((a then b)[p] = a[p] + b[(p + a[p]) mod 2]), and a block scan gives every
 // term the S in front of it.  The first term whose exact sum could reach the
 // top of the binade (or an infinite term) is added with the hardware DADD;
-// the fold then continues from it in the new binade.  Each such step at least
-// doubles s, so there are at most a few dozen of them.  A zero-start sum
-// takes its first non-zero term exactly.
+// the fold then continues from it in the new binade, with a short chunk that
+// doubles while no step comes (steps come every few terms while s is small).
+// Each such step at least doubles s, so there are at most a few dozen of
+// them.  A zero-start sum takes its first non-zero term exactly.
 
 constexpr int kFoldThreads = 512;
 constexpr int kFoldPerThread = 8;  // consecutive terms per thread
 constexpr int kFoldChunk = kFoldThreads * kFoldPerThread;
 constexpr int kFoldWarps = kFoldThreads / 32;
+constexpr int kFoldSmall = 64;  // chunk after a binade step; doubles up to kFoldChunk while none comes
 constexpr unsigned long long kTwo53 = 1ull << 53;
 
 struct IncPair {
@@ -436,6 +438,7 @@ struct FoldShared {
   double s;
   long long pos;
   int first;
+  int len;  // terms the next iteration takes
 };
 
 // One block per total.
@@ -450,6 +453,7 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
   if (t == 0) {
     sh.s = 0.0;
     sh.pos = 0;
+    sh.len = kFoldSmall;
   }
   __syncthreads();
   double x[kFoldPerThread];
@@ -458,7 +462,9 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
     const double s = sh.s;
     const long long pos = sh.pos;
     if (pos >= cnt || isinf(s)) break;
-    const int len = (int)min((long long)kFoldChunk, cnt - pos);
+    const int want = sh.len;
+    const int len = (int)min((long long)want, cnt - pos);
+    const int next_len = min(kFoldChunk, 2 * want);
     if (loaded != pos) {
 #pragma unroll
       for (int k = 0; k < kFoldPerThread; ++k) {
@@ -469,8 +475,8 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
     double nx[kFoldPerThread];  // the next chunk, in case this one has no binade step
 #pragma unroll
     for (int k = 0; k < kFoldPerThread; ++k) {
-      const long long i = pos + len + t * kFoldPerThread + k;
-      nx[k] = i < cnt ? src[i] : 0.0;
+      const int i = t * kFoldPerThread + k;
+      nx[k] = (i < next_len && pos + len + i < cnt) ? src[pos + len + i] : 0.0;
     }
     if (t == 0) sh.first = len;
     __syncthreads();  // everyone read s and pos; first is reset
@@ -488,7 +494,10 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
 #pragma unroll
       for (int k = 0; k < kFoldPerThread; ++k)
         if (t * kFoldPerThread + k == f) sh.s = x[k];
-      if (t == 0) sh.pos = pos + (f < len ? f + 1 : len);
+      if (t == 0) {
+        sh.pos = pos + (f < len ? f + 1 : len);
+        sh.len = f < len ? kFoldSmall : next_len;
+      }
       loaded = -1;
       __syncthreads();
       continue;
@@ -501,16 +510,23 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
     IncPair local = zero;
 #pragma unroll
     for (int k = 0; k < kFoldPerThread; ++k) {
-      const bool in = t * kFoldPerThread + k < len;
-      const double q = ldexp(x[k], -ue);
-      big[k] = in && !(q < 9007199254740992.0);
-      const double mf = big[k] || !in ? 0.0 : floor(q);
-      const double f = big[k] || !in ? 0.0 : q - mf;
-      m[k] = (unsigned long long)mf;
-      const bool above = f > 0.5, tie = f == 0.5;
-      inc[k].e = m[k] + (above ? 1ull : (tie ? (m[k] & 1ull) : 0ull));
-      inc[k].o = m[k] + (above ? 1ull : (tie ? ((m[k] + 1ull) & 1ull) : 0ull));
-      if (big[k]) inc[k] = IncPair{kTwo53, kTwo53};  // never applied: the binade step comes first
+      inc[k] = zero;
+      m[k] = 0;
+      big[k] = false;
+      if (t * kFoldPerThread + k < len) {
+        const double q = ldexp(x[k], -ue);
+        big[k] = !(q < 9007199254740992.0);
+        if (big[k]) {
+          inc[k] = IncPair{kTwo53, kTwo53};  // never applied: the binade step comes first
+        } else {
+          const double mf = floor(q);
+          const double f = q - mf;
+          m[k] = (unsigned long long)mf;
+          const bool above = f > 0.5, tie = f == 0.5;
+          inc[k].e = m[k] + (above ? 1ull : (tie ? (m[k] & 1ull) : 0ull));
+          inc[k].o = m[k] + (above ? 1ull : (tie ? ((m[k] + 1ull) & 1ull) : 0ull));
+        }
+      }
       local = compose(local, inc[k]);
     }
     const IncPair incl = warp_inclusive(local, lane);
@@ -554,12 +570,14 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
       if (t == (len - 1) / kFoldPerThread) {
         sh.s = ldexp((double)P, ue);
         sh.pos = pos + len;
+        sh.len = next_len;
       }
     } else if (mine == c) {
 #pragma unroll
       for (int k = 0; k < kFoldPerThread; ++k)
         if (t * kFoldPerThread + k == c) sh.s = ldexp((double)P_at, ue) + x[k];
       sh.pos = pos + c + 1;
+      sh.len = kFoldSmall;
     }
     __syncthreads();
     if (sh.pos == pos + len) {
