@@ -394,8 +394,8 @@ struct FoldJob {
 // ((a then b)[p] = a[p] + b[(p + a[p]) mod 2]), and a block scan gives every
 // term the S in front of it.  The first term whose exact sum could reach the
 // top of the binade (or an infinite term) is added with the hardware DADD;
-// the fold then continues from it in the new binade, with a short chunk that
-// doubles while no step comes (steps come every few terms while s is small).
+// the fold then continues from it in the new binade, with a chunk as long as
+// the terms taken so far (steps come every few terms while s is small).
 // Each such step at least doubles s, so there are at most a few dozen of
 // them.  A zero-start sum takes its first non-zero term exactly.
 
@@ -403,7 +403,7 @@ constexpr int kFoldThreads = 512;
 constexpr int kFoldPerThread = 8;  // consecutive terms per thread
 constexpr int kFoldChunk = kFoldThreads * kFoldPerThread;
 constexpr int kFoldWarps = kFoldThreads / 32;
-constexpr int kFoldSmall = 64;  // chunk after a binade step; doubles up to kFoldChunk while none comes
+constexpr int kFoldSmall = 64;  // shortest chunk after a binade step
 constexpr unsigned long long kTwo53 = 1ull << 53;
 
 struct IncPair {
@@ -577,7 +577,9 @@ __global__ void __launch_bounds__(kFoldThreads) fold_kernel(FoldJob job) {
       for (int k = 0; k < kFoldPerThread; ++k)
         if (t * kFoldPerThread + k == c) sh.s = ldexp((double)P_at, ue) + x[k];
       sh.pos = pos + c + 1;
-      sh.len = kFoldSmall;
+      // s grows about linearly in the terms taken, so the next step is about
+      // as many terms away as have been taken so far
+      sh.len = (int)max((long long)kFoldSmall, min((long long)kFoldChunk, pos + c + 1));
     }
     __syncthreads();
     if (sh.pos == pos + len) {
