@@ -1459,6 +1459,20 @@ def run_reference(args) -> dict | None:
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def _host_cpu() -> dict:
+    """The host's CPU model and hardware threads (for the CPU baseline)."""
+    model = ""
+    try:
+        with open("/proc/cpuinfo", encoding="utf-8") as f:
+            for ln in f:
+                if ln.startswith("model name"):
+                    model = ln.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model or None, "host_threads": os.cpu_count()}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -1495,6 +1509,8 @@ def main():
     else:
         line = run_b200(args)
     if line is not None:
+        if isinstance(line.get("cpu_baseline"), dict):
+            line["cpu_baseline"].update(_host_cpu())
         print(json.dumps(line), flush=True)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1 and args.impl == "b200":
         import torch.distributed as dist
