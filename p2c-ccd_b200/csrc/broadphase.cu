@@ -648,6 +648,34 @@ size_t broadphase_workspace_bytes(long long nv, long long nf, long long ne, long
   return carve(nullptr, nv, nf, ne, pair_cap, true).total;
 }
 
+// A second stream (per host thread and device) the vertex-face and edge-edge
+// sweeps fork onto: both read the sorted boxes and append to their own pair
+// lists, so they run side by side and fill each other's tail waves.  Created
+// outside stream capture only; while none exists the sweeps run in order.
+struct SweepFork {
+  cudaStream_t stream = nullptr;
+  cudaEvent_t fork = nullptr, join = nullptr;
+};
+
+SweepFork* sweep_fork(cudaStream_t s) {
+  constexpr int kMaxDevices = 64;
+  static thread_local SweepFork forks[kMaxDevices];
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) return nullptr;
+  SweepFork& f = forks[dev];
+  if (f.stream == nullptr) {
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(s, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) return nullptr;
+    if (cudaStreamCreateWithFlags(&f.stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f.fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&f.join, cudaEventDisableTiming) != cudaSuccess) {
+      f.stream = nullptr;
+      return nullptr;
+    }
+  }
+  return &f;
+}
+
 // Candidate generation; counts_dev receives {vf_count, ee_count, error_word,
 // axis | g1 << 8 | g2 << 24 | kept boxes << 40}.
 int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long long vf_cap,
@@ -701,13 +729,23 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     fill_u64_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, ~0ull);
   if (sort_out && !small_sort && ee_cap > 0)
     fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
-  if (scene.nv + scene.nf > 0 && vf_out != nullptr)
+  const bool do_vf = scene.nv + scene.nf > 0 && vf_out != nullptr;
+  const bool do_ee = scene.ne > 0 && ee_out != nullptr;
+  SweepFork* fk = do_vf && do_ee ? sweep_fork(s) : nullptr;
+  cudaStream_t ee_stream = s;
+  if (fk != nullptr) {
+    P2C_CUDA(cudaEventRecord(fk->fork, s));
+    P2C_CUDA(cudaStreamWaitEvent(fk->stream, fk->fork, 0));
+    ee_stream = fk->stream;
+  }
+  if (do_ee)
+    sweep_ee_kernel<<<grid_for(scene.ne * kSceneSweepLanes, kThreads), kThreads, 0, ee_stream>>>(
+        L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out, (unsigned long long)ee_cap, L.sc);
+  if (fk != nullptr) P2C_CUDA(cudaEventRecord(fk->join, fk->stream));
+  if (do_vf)
     sweep_vf_kernel<<<grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads), kThreads, 0, s>>>(
         L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out, (unsigned long long)vf_cap, L.sc);
-  if (scene.ne > 0 && ee_out != nullptr)
-    sweep_ee_kernel<<<grid_for(scene.ne * kSceneSweepLanes, kThreads), kThreads, 0, s>>>(L.B[2].s, scene.edges, scene.exclude_self,
-                                                                      ee_shift, ee_out, (unsigned long long)ee_cap,
-                                                                      L.sc);
+  if (fk != nullptr) P2C_CUDA(cudaStreamWaitEvent(s, fk->join, 0));
   P2C_CUDA(cudaGetLastError());
   if (small_sort) {
     static bool attr_set = false;  // the block sort's storage is above the 48 KB static limit
