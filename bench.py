@@ -311,6 +311,10 @@ class SceneWorkload:
             end.synchronize()
             times.append(start.elapsed_time(end))
         drain = times.pop()
+        if steps >= 2:  # the two pipelines certified the same frames: their read-backs agree byte for byte
+            for a, b in zip(host_out[0], host_out[1]):
+                if not torch.equal(a, b):
+                    raise RuntimeError("the alternating pipelines returned different certificates")
         return [t + drain / steps for t in times]
 
     def io_bytes(self) -> tuple[int, int]:
