@@ -78,6 +78,8 @@ __global__ void init_scratch_kernel(BroadScratch* sc) {
 __global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restrict__ v_t0,
                                                          const double* __restrict__ v_t1, Lists L,
                                                          double thickness, int cull_objects, BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   __shared__ double red[9][kThreads / 32];
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
@@ -158,6 +160,8 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restric
 // list size the column grid.
 __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_objects,
                                                             unsigned char* __restrict__ active, BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool keep = false;
   int l = 3;
@@ -217,6 +221,8 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
 
 // Sweep axis, column grid, sweep-axis quantiser and list segments (one thread).
 __global__ void grid_kernel(BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const double n = sc->count > 0 ? (double)sc->count : 1.0;
   int axis = 0;
   double best = INFINITY;
@@ -278,6 +284,8 @@ __global__ void grid_kernel(BroadScratch* sc) {
 __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned char* __restrict__ active,
                                                         unsigned* __restrict__ keys, unsigned* __restrict__ vals,
                                                         const BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= L.off[3]) return;
   const Grid& G = sc->grid;
@@ -297,6 +305,8 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned 
 __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigned* __restrict__ keys,
                                                           const unsigned* __restrict__ order, SortedBoxes s0,
                                                           SortedBoxes s1, SortedBoxes s2, const BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const Grid& G = sc->grid;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)G.seg[3]) return;
@@ -349,6 +359,8 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
                                                             const int32_t* __restrict__ faces, int exclude_self,
                                                             int pack_shift, unsigned long long* out,
                                                             unsigned long long cap, BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const Grid& g = sc->grid;
   const long long nv = (long long)(g.seg[1] - g.seg[0]), nf = (long long)(g.seg[2] - g.seg[1]);
   const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -410,6 +422,8 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
 __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
                                                             int exclude_self, int pack_shift, unsigned long long* out,
                                                             unsigned long long cap, BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   const Grid& g = sc->grid;
   const long long ne = (long long)(g.seg[3] - g.seg[2]);
   const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -493,6 +507,8 @@ using SmallSort = cub::BlockRadixSort<unsigned long long, kSmallSortThreads, kSm
 __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
     unsigned long long* vf, long long vf_cap, int vf_bits, int vf_shift, unsigned long long* ee, long long ee_cap,
     int ee_bits, int ee_shift, const BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_sort[];
   typename SmallSort::TempStorage& tmp = *reinterpret_cast<typename SmallSort::TempStorage*>(smem_sort);
   const bool is_vf = blockIdx.x == 0;
@@ -517,6 +533,8 @@ __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
 }
 
 __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long* counts) {
+  pdl_wait();
+  pdl_trigger();
   counts[0] = sc->vf_count;
   counts[1] = sc->ee_count;
   counts[2] = sc->error_word;
@@ -704,22 +722,22 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
   init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
   if (n > 0) {
-    boxes_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(scene.v_t0, scene.v_t1, lists, scene.thickness, cull,
-                                                            L.sc);
-    classify_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, cull, L.active, L.sc);
+    P2C_CUDA(launch_pdl(boxes_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
+                        lists, scene.thickness, cull, L.sc));
+    P2C_CUDA(launch_pdl(classify_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists, cull, L.active,
+                        L.sc));
   }
-  grid_kernel<<<1, 1, 0, s>>>(L.sc);
-  P2C_CUDA(cudaGetLastError());
+  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc));
   if (n > 0) {
-    keys_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, L.active, L.keys[0], L.vals[0], L.sc);
-    P2C_CUDA(cudaGetLastError());
+    P2C_CUDA(launch_pdl(keys_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
+                        (const unsigned char*)L.active, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));
     cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
     cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
     size_t tb = L.sort_tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, 32, s));
-    gather_kernel<<<grid_for(n, kThreads), kThreads, 0, s>>>(lists, k.Current(), v.Current(), L.B[0].s, L.B[1].s,
-                                                             L.B[2].s, L.sc);
-    P2C_CUDA(cudaGetLastError());
+    P2C_CUDA(launch_pdl(gather_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
+                        (const unsigned*)k.Current(), (const unsigned*)v.Current(), L.B[0].s, L.B[1].s, L.B[2].s,
+                        (const BroadScratch*)L.sc));
   }
   // with sorting, pairs are emitted packed so that the sort touches fewer bits
   const int vf_shift = sort_out ? std::max(1, bit_length(scene.nf)) : 0;
@@ -739,12 +757,14 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     ee_stream = fk->stream;
   }
   if (do_ee)
-    sweep_ee_kernel<<<grid_for(scene.ne * kSceneSweepLanes, kThreads), kThreads, 0, ee_stream>>>(
-        L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out, (unsigned long long)ee_cap, L.sc);
+    P2C_CUDA(launch_pdl(sweep_ee_kernel, dim3(grid_for(scene.ne * kSceneSweepLanes, kThreads)), dim3(kThreads), 0,
+                        ee_stream, L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out,
+                        (unsigned long long)ee_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaEventRecord(fk->join, fk->stream));
   if (do_vf)
-    sweep_vf_kernel<<<grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads), kThreads, 0, s>>>(
-        L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out, (unsigned long long)vf_cap, L.sc);
+    P2C_CUDA(launch_pdl(sweep_vf_kernel, dim3(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads)),
+                        dim3(kThreads), 0, s, L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out,
+                        (unsigned long long)vf_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaStreamWaitEvent(s, fk->join, 0));
   P2C_CUDA(cudaGetLastError());
   if (small_sort) {
@@ -754,9 +774,9 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
                                     (int)sizeof(SmallSort::TempStorage)));
       attr_set = true;
     }
-    small_sort_pairs_kernel<<<2, kSmallSortThreads, sizeof(SmallSort::TempStorage), s>>>(
-        vf_out, vf_cap, bit_length(scene.nv) + vf_shift, vf_shift, ee_out, ee_cap, bit_length(scene.ne) + ee_shift,
-        ee_shift, L.sc);
+    P2C_CUDA(launch_pdl(small_sort_pairs_kernel, dim3(2), dim3(kSmallSortThreads), sizeof(SmallSort::TempStorage), s,
+                        vf_out, vf_cap, bit_length(scene.nv) + vf_shift, vf_shift, ee_out, ee_cap,
+                        bit_length(scene.ne) + ee_shift, ee_shift, (const BroadScratch*)L.sc));
   } else if (sort_out) {
     int rc = sort_pairs(vf_out, vf_cap, bit_length(scene.nv) + vf_shift, L, s);
     if (rc != P2C_OK) return rc;
@@ -765,7 +785,7 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     if (vf_cap > 0) unpack_pairs_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, vf_shift);
     if (ee_cap > 0) unpack_pairs_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ee_shift);
   }
-  export_counts_kernel<<<1, 1, 0, s>>>(L.sc, counts_dev);
+  P2C_CUDA(launch_pdl(export_counts_kernel, dim3(1), dim3(1), 0, s, (const BroadScratch*)L.sc, counts_dev));
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;
 }

@@ -59,6 +59,8 @@ struct PairProblem {
 __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
     certify_scene_kernel(const __grid_constant__ PairProblem prob, const __grid_constant__ CertParams prm,
                          const __grid_constant__ EnginePools pools, CertifyScratch* scratch) {
+  pdl_wait();
+  pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   EngineShared& sh = reinterpret_cast<EngineShared*>(smem_raw)[threadIdx.x >> 5];
   WarpStats st;
@@ -80,7 +82,10 @@ __global__ void __launch_bounds__(kCertifyThreads, kCertifyMinBlocks)
   }
 }
 
-__global__ void init_scene_agg_kernel(SceneAgg* a) { scene_agg_init(*a); }
+__global__ void init_scene_agg_kernel(SceneAgg* a) {
+  pdl_trigger();  // the certification launch behind it may be scheduled now
+  scene_agg_init(*a);
+}
 
 // CertificateEngine::Evaluate over (VF list, EE list) from the reduced flags;
 // the collision witness is the candidate whose key won the atomicMin.
@@ -88,6 +93,8 @@ __global__ void scene_summary_kernel(const CertifyScratch* sc, const SceneAgg* a
                                      const unsigned long long* ee_pairs, const p2c_interval_result* out_vf,
                                      const p2c_interval_result* out_ee, unsigned family_mask, double T1,
                                      p2c_scene_summary* summary) {
+  pdl_wait();
+  pdl_trigger();
   const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   scene_witness(*agg, t, vf_pairs, ee_pairs, out_vf, out_ee, summary);
   if (t == 0) scene_summary_fields(*agg, family_mask, T1, sc->stats.error_word, summary);
@@ -154,14 +161,13 @@ int launch_scene_certify(const p2c_scene& scene, const unsigned long long* vf_pa
   prob.undecided_queue = uq;
   prob.undecided_cap = (unsigned long long)(uq_cap > 0 ? uq_cap : 0);
   prob.error_word = (unsigned long long*)&sc->stats.error_word;
-  certify_scene_kernel<<<shape.grid, kCertifyThreads, shape.smem, s>>>(prob, prm, pools_at(sc), sc);
-  P2C_CUDA(cudaGetLastError());
+  P2C_CUDA(launch_pdl(certify_scene_kernel, dim3(shape.grid), dim3(kCertifyThreads), shape.smem, s, prob, prm,
+                      pools_at(sc), sc));
   if (summary != nullptr) {
     const long long nmax = (vf_cap > ee_cap ? vf_cap : ee_cap);
     const unsigned grid = (unsigned)((nmax + 255) / 256 > 0 ? (nmax + 255) / 256 : 1);
-    scene_summary_kernel<<<grid, 256, 0, s>>>(sc, scene_agg(ws), vf_pairs, ee_pairs, out_vf, out_ee, family_mask,
-                                              T1, summary);
-    P2C_CUDA(cudaGetLastError());
+    P2C_CUDA(launch_pdl(scene_summary_kernel, dim3(grid), dim3(256), 0, s, sc, scene_agg(ws), vf_pairs, ee_pairs,
+                        out_vf, out_ee, family_mask, T1, summary));
   }
   return P2C_OK;
 }
