@@ -130,7 +130,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
   unsigned exhausted = (n1 == 0 ? 1u : 0u) | (n2 == 0 ? 2u : 0u);  // bit f-1: family f's queue is empty
   bool hungry = false;                     // this warp is counted in es->hungry
   bool helper = false;                     // this warp is counted in es->helpers
-  unsigned backoff = 256;                  // ns slept per idle poll (doubles up to 4 us)
+  unsigned backoff = 256;                  // ns slept per idle poll (doubles up to 512 ns)
   unsigned long long pool_hungry = 0, pool_size = 0;
   bool ok = true;
 
@@ -395,7 +395,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
           if (!helper) break;
         }
         __nanosleep(backoff);
-        backoff = min(backoff * 2u, 4096u);
+        backoff = min(backoff * 2u, 512u);
       }
       continue;
     }
