@@ -644,7 +644,8 @@ int p2c_dense_group_early_stop(int64_t n, const uint64_t* query_id_dev, const ui
     return fail(P2C_ERR_INVALID, "uncertainty_fallback_threshold must be finite and non-negative");
   if (!std::isfinite(config->interval_miss_penalty_scale) || config->interval_miss_penalty_scale < 0.0)
     return fail(P2C_ERR_INVALID, "interval_miss_penalty_scale must be finite and non-negative");
-  if (n < 0 || n >= (1ll << 30)) return fail(P2C_ERR_INVALID, "row count must lie in [0, 2^30)");
+  if (n < 0 || n >= (1ll << 29))  // the 3n work-term slots are counted in int by the compaction
+    return fail(P2C_ERR_INVALID, "row count must lie in [0, 2^29)");
   if (n > 0 && (query_id_dev == nullptr || candidate_id_dev == nullptr || cost_target_dev == nullptr ||
                 oracle_trace_dev == nullptr || interval_scores_dev == nullptr || priority_score_dev == nullptr ||
                 cost_score_dev == nullptr || uncertainty_score_dev == nullptr))
