@@ -130,12 +130,13 @@ def test_device_dummy_schedule_errors(oracle_mod):
 @pytest.mark.parametrize("seed,n,materialize", [(71, 60, False), (72, 500, True), (73, 1, False)])
 def test_device_external_dummy_matches_reference(oracle_mod, seed, n, materialize):
     import p2cccd_cpp as cpp
+    from p2cccd_b200.records import EXACT_WORK_ITEM_DTYPE
 
     b = make_batch(n, seed, miss=0.3)
     cfg = cpp.ProposalSchedulingConfig()
     cfg.first_work_item_id = 77
     res = cpp.generate_external_batch_dummy_proposal_schedule(b, config=cfg, materialize_artifacts=materialize)
-    items = np.zeros(len(res.work_queue), dtype=__import__("p2cccd_b200.records", fromlist=["x"]).EXACT_WORK_ITEM_DTYPE)
+    items = np.zeros(len(res.work_queue), dtype=EXACT_WORK_ITEM_DTYPE)
     for r, w in zip(items, res.work_queue):
         for k in ("work_item_id", "parent_candidate_id", "query_id", "slab_id", "patch_a_id", "patch_b_id",
                   "interval_t0", "interval_t1", "feature_family_mask", "topk_feature_ids_offset", "depth",

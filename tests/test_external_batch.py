@@ -175,15 +175,15 @@ def test_device_batch_candidates_match_reference(oracle_mod, seed, n, kw):
 @pytest.mark.gpu
 def test_mirror_external_batch_objects(oracle_mod):
     import p2cccd_cpp as cpp
+    from p2cccd_b200 import external as ex
 
     b = make_batch(50, 41, touching=True)
     res = cpp.generate_candidates_for_external_batch(_objects(b))
     fb = cpp.generate_candidates_for_external_batch(_objects(b), backend_name="optix", allow_optix_cpu_fallback=True)
     assert res.backend_name == "cpu_reference" and fb.backend_name == "optix_cpu_fallback"
     assert cpp._candidate_array(res.candidates).tobytes() == cpp._candidate_array(fb.candidates).tobytes()
-    sc = __import__("p2cccd_b200.external", fromlist=["x"])
-    raw, cand = oracle_mod.proxy_candidates(sc.encode_scene(b))
-    want, _ = sc.translate(cand, b, sc.runtime_query_ids(b["query_id"]))
+    raw, cand = oracle_mod.proxy_candidates(ex.encode_scene(b))
+    want, _ = ex.translate(cand, b, ex.runtime_query_ids(b["query_id"]))
     assert cpp._candidate_array(res.candidates).tobytes() == want.tobytes()
     assert [m.source_query_id for m in res.runtime_query_ids] == b["query_id"].tolist()
     assert res.primitive_count == 100 and res.raw_hit_count == len(raw)
