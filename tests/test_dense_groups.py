@@ -183,6 +183,10 @@ def _ordered_cases():
     w = rng.random(6000)
     w[4500] = np.inf
     cases.append(w)
+    w = rng.random(5000)
+    w[::7] = -0.0  # negative zeros add nothing
+    w[:3] = -0.0
+    cases.append(w)
     return cases
 
 
