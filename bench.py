@@ -165,6 +165,35 @@ class PlainWorkload:
         self.h_out_pt.copy_(self.out_pt, non_blocking=True)
         self.h_out_ee.copy_(self.out_ee, non_blocking=True)
 
+    def e2e_pipelined(self, steps: int, flush, stream) -> list[float]:
+        """End-to-end steps with the transfers overlapped (``overlapped_e2e``)
+        over two sets of device records and results; the read-backs of both
+        sets are checked to agree."""
+        torch = self.torch
+        if getattr(self, "set2", None) is None:
+            self.set2 = (torch.empty_like(self.pt), torch.empty_like(self.ee), torch.empty_like(self.out_pt),
+                         torch.empty_like(self.out_ee), self.certify.Workspace(self.dev))
+        sets = ((self.pt, self.ee, self.out_pt, self.out_ee, self.ws), self.set2)
+        host_out = [(self.h_out_pt, self.h_out_ee),
+                    (torch.empty_like(self.h_out_pt).pin_memory(), torch.empty_like(self.h_out_ee).pin_memory())]
+
+        def copy_in(i):
+            sets[i][0].copy_(self.h_pt, non_blocking=True)
+            sets[i][1].copy_(self.h_ee, non_blocking=True)
+
+        def compute(i):
+            pt, ee, opt, oee, ws = sets[i]
+            self.certify.certify_batch2(pt, ee, 0.0, 1.0, self.cfg, opt, oee, ws)
+
+        def copy_out(i):
+            host_out[i][0].copy_(sets[i][2], non_blocking=True)
+            host_out[i][1].copy_(sets[i][3], non_blocking=True)
+
+        times = overlapped_e2e(torch, steps, flush, stream, copy_in, compute, copy_out)
+        if steps >= 2 and not all(torch.equal(a, b) for a, b in zip(host_out[0], host_out[1])):
+            raise RuntimeError("the alternating buffer sets returned different certificates")
+        return times
+
     def io_bytes(self) -> tuple[int, int]:
         return self.h_pt.numel() + self.h_ee.numel(), self.h_out_pt.numel() + self.h_out_ee.numel()
 
@@ -257,14 +286,9 @@ class SceneWorkload:
         self.h_summary.copy_(self.pipe.summary, non_blocking=True)
 
     def e2e_pipelined(self, steps: int, flush, stream) -> list[float]:
-        """End-to-end steps with the transfers overlapped: two captured
-        pipelines alternate, and while step k's graph runs, step k+1's frames
-        come in from pinned host memory (into the other pipeline's inputs) and
-        step k-1's certificates and summary go out, on a copy stream.  Every
-        copy is issued after the start event of the step it overlaps and
-        waited for before that step's end event, so each timed region holds
-        its share of the transfers; a last region drains the final step's
-        results and is spread over the steps.  Returns per-step milliseconds."""
+        """End-to-end steps with the transfers overlapped (``overlapped_e2e``):
+        two captured pipelines alternate; the read-backs of both are checked
+        to agree (the same frames give the same certificates)."""
         torch = self.torch
         from p2cccd_b200.scene import ScenePipeline
 
@@ -276,47 +300,26 @@ class SceneWorkload:
             p2.capture()
             self.pipe2 = p2
         pipes = (self.pipe, self.pipe2)
-        cs = torch.cuda.Stream(self.pipe.v_t0.device)
         host_out = [(self.h_vf, self.h_ee, self.h_summary),
                     tuple(torch.empty_like(t, device="cpu").pin_memory()
                           for t in (self.pipe2.vf_results, self.pipe2.ee_results, self.pipe2.summary))]
-        ev_in = [torch.cuda.Event(), torch.cuda.Event()]
-        with torch.cuda.stream(cs):
-            pipes[0].v_t0.copy_(self.h_t0, non_blocking=True)
-            pipes[0].v_t1.copy_(self.h_t1, non_blocking=True)
-            ev_in[0].record(cs)
-        times = []
-        for k in range(steps + 1):
-            flush.fill_(1)
-            start, end, ev_x = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
-                                torch.cuda.Event())
-            start.record(stream)
-            cs.wait_event(start)
-            with torch.cuda.stream(cs):
-                if k >= 1:  # step k-1's results out of the pipeline that ran it
-                    q = pipes[(k - 1) % 2]
-                    for d, src in zip(host_out[(k - 1) % 2], (q.vf_results, q.ee_results, q.summary)):
-                        d.copy_(src, non_blocking=True)
-                if k + 1 < steps:  # step k+1's frames into the other pipeline (step k-1 is done with them)
-                    q = pipes[(k + 1) % 2]
-                    q.v_t0.copy_(self.h_t0, non_blocking=True)
-                    q.v_t1.copy_(self.h_t1, non_blocking=True)
-                    ev_in[(k + 1) % 2].record(cs)
-                ev_x.record(cs)
-            if k < steps:
-                stream.wait_event(ev_in[k % 2])
-                pipes[k % 2].replay()
-            stream.wait_event(ev_x)
-            end.record(stream)
-            end.synchronize()
-            times.append(start.elapsed_time(end))
-        drain = times.pop()
+
+        def copy_in(i):
+            pipes[i].v_t0.copy_(self.h_t0, non_blocking=True)
+            pipes[i].v_t1.copy_(self.h_t1, non_blocking=True)
+
+        def copy_out(i):
+            q = pipes[i]
+            for d, src in zip(host_out[i], (q.vf_results, q.ee_results, q.summary)):
+                d.copy_(src, non_blocking=True)
+
+        times = overlapped_e2e(torch, steps, flush, stream, copy_in, lambda i: pipes[i].replay(), copy_out)
         if steps >= 2:  # the two pipelines certified the same frames: their certificates agree byte for byte
             rows = (self.n_vf, self.n_ee, None)  # result buffers hold spare capacity beyond the counts
             for name, r, a, b in zip(("vf", "ee", "summary"), rows, host_out[0], host_out[1]):
                 if not torch.equal(a[:r] if r is not None else a, b[:r] if r is not None else b):
                     raise RuntimeError(f"the alternating pipelines returned different {name} results")
-        return [t + drain / steps for t in times]
+        return times
 
     def io_bytes(self) -> tuple[int, int]:
         return (self.h_t0.numel() * 8 + self.h_t1.numel() * 8,
@@ -758,6 +761,45 @@ def time_steps(torch, fn, steps, flush, stream):
     return times
 
 
+def overlapped_e2e(torch, steps, flush, stream, copy_in, compute, copy_out) -> list[float]:
+    """End-to-end steps with the transfers overlapped on a copy stream, two
+    buffer sets alternating: while step k computes on set k % 2, step k+1's
+    inputs come in to the other set (``copy_in(slot)``) and step k-1's
+    results go out of it (``copy_out(slot)``).  Every copy is issued after
+    the start event of the step it overlaps and waited for before that step's
+    end event, so each timed region holds its share of the transfers; a last
+    region drains the final step's results and is spread over the steps.
+    Returns per-step milliseconds."""
+    cs = torch.cuda.Stream(stream.device)
+    ev_in = [torch.cuda.Event(), torch.cuda.Event()]
+    with torch.cuda.stream(cs):
+        copy_in(0)
+        ev_in[0].record(cs)
+    times = []
+    for k in range(steps + 1):
+        flush.fill_(1)
+        start, end, ev_x = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True),
+                            torch.cuda.Event())
+        start.record(stream)
+        cs.wait_event(start)
+        with torch.cuda.stream(cs):
+            if k >= 1:
+                copy_out((k - 1) % 2)
+            if k + 1 < steps:  # the set step k-1 used, which is done with it
+                copy_in((k + 1) % 2)
+                ev_in[(k + 1) % 2].record(cs)
+            ev_x.record(cs)
+        if k < steps:
+            stream.wait_event(ev_in[k % 2])
+            compute(k % 2)
+        stream.wait_event(ev_x)
+        end.record(stream)
+        end.synchronize()
+        times.append(start.elapsed_time(end))
+    drain = times.pop()
+    return [t + drain / steps for t in times]
+
+
 def count_kernels(torch, fn) -> tuple[int, dict]:
     """Kernels one call of fn launches (torch profiler / CUPTI), by name."""
     try:
@@ -869,9 +911,9 @@ def run_b200(args) -> dict | None:
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms, "pipelined": e2e_times is not e2e_serial_times,
                 "serial_ms_per_step": statistics.mean(e2e_serial_times),
-                "method": ("two captured pipelines alternate; frames in and results out on a copy stream, "
-                           "overlapped with the neighbouring steps' graphs; each transfer inside the timed region of "
-                           "the step it overlaps"
+                "method": ("two buffer sets (captured pipelines for the scene) alternate; inputs in and results "
+                           "out on a copy stream, overlapped with the neighbouring steps' compute; each transfer "
+                           "inside the timed region of the step it overlaps"
                            if e2e_times is not e2e_serial_times else
                            "copy in, step, copy out, in order on one stream")},
         "gpu_launches": n_kernels * args.steps if n_kernels >= 0 else None,
