@@ -512,6 +512,25 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
                          p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
                          size_t workspace_bytes, void* stream);
 
+/* Workspace of p2c_compact_raw_candidates (as p2c_proxy_candidates with
+ * raw_cap = n_raw). */
+size_t p2c_compact_raw_candidates_workspace_bytes(int64_t n_proxies, int64_t n_raw, uint32_t slab_bits);
+
+/* CompactRawCandidates (rt_candidate/candidate_buffer.cpp:181-227) on n_raw
+ * given hits of a proxy scene (from any tracer): each hit checked as
+ * ValidateRawHit does (:71-101), then the same compaction, order and ids as
+ * p2c_proxy_candidates.  candidates_dev holds n_raw records.
+ * counts_dev[0..3] = {n_raw, candidates, error word (1: a proxy fails the
+ * per-proxy checks; 16: a candidate's summed rt_hit_count overflows 32
+ * bits), the first invalid hit as (hit index << 4 | check) or ~0: check 1 not
+ * marked valid, 2 zero query id, 3 query id differs from the scene's, 4 proxy
+ * index out of range, 5 the same proxy twice, 6 pair_key mismatch, 7 one
+ * object, 8 slab mismatch, 9 motion bound negative or non-finite}.  With an
+ * invalid hit the records are meaningless.  No host sync. */
+int p2c_compact_raw_candidates(const p2c_proxy_scene* scene, const p2c_raw_candidate_hit* raw_dev, int64_t n_raw,
+                               p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
+                               size_t workspace_bytes, void* stream);
+
 /* ---- proxy scene build: patches x motion segments x time slabs --------------- */
 /* MotionSegment (geometry/motion.h:14-19): a rigid motion from pose_t0 at t0 to
  * pose_t1 at t1; rotation quaternions are x, y, z, w. */

@@ -1374,3 +1374,24 @@ def dummy_schedule(cand, primitive_count, raw_hit_count, compact_candidate_count
     if not materialize:
         rows, outs = rows[:0], outs[:0]
     return clean, stats, rows, outs
+
+
+def ref_compact_raw(sc: dict, raw):
+    """The reference's CompactRawCandidates on given raw hits of a proxy scene."""
+    from p2cccd_b200.records import CANDIDATE_RECORD_DTYPE, RAW_HIT_DTYPE
+
+    R = ref()
+    if not hasattr(R, "_compact_ready"):
+        vp, i64 = ctypes.c_void_p, ctypes.c_int64
+        R.ref_compact_raw.argtypes = [ctypes.c_uint64, i64] + [vp] * 8 + [vp, i64, vp, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._compact_ready = True
+    a = _proxy_args(sc)
+    raw = np.ascontiguousarray(raw, dtype=RAW_HIT_DTYPE)
+    cand = np.zeros(max(1, len(raw)), CANDIDATE_RECORD_DTYPE)
+    n_cand = ctypes.c_int64(0)
+    args = [int(sc["query_id"]), int(sc["n"])] + [_p(a[k]) for k in ("object_id", "patch_id", "slab_id", "proxy_type",
+                                                                     "t0", "t1", "bounds", "motion_bound")]
+    if R.ref_compact_raw(*args, _p(raw) if len(raw) else None, len(raw), _p(cand), ctypes.byref(n_cand)):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    return cand[:n_cand.value]

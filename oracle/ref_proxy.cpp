@@ -539,6 +539,47 @@ int ref_external_dummy(int64_t n, const uint64_t* source_id, const uint32_t* sou
   return 0;
 }
 
+// CompactRawCandidates on n_raw given hits (64-byte records) of the scene.
+// Writes the candidates (capacity n_raw) and their count.
+int ref_compact_raw(uint64_t query_id, int64_t n, const uint32_t* object_id, const uint32_t* patch_id,
+                    const uint32_t* slab_id, const uint8_t* proxy_type, const double* t0, const double* t1,
+                    const double* bounds, const double* motion_bound, const p2c_raw_candidate_hit* raw_in,
+                    int64_t n_raw, p2c_candidate_record* cand_out, int64_t* n_cand) {
+  p2cccd::ProxyScene scene =
+      make_scene(query_id, n, object_id, patch_id, slab_id, proxy_type, t0, t1, bounds, motion_bound);
+  p2cccd::RawCandidateBuffer raw;
+  raw.hits.resize(static_cast<std::size_t>(n_raw));
+  for (int64_t k = 0; k < n_raw; ++k)
+    std::memcpy(&raw.hits[static_cast<std::size_t>(k)], raw_in + k, sizeof(p2c_raw_candidate_hit));
+  std::vector<p2cccd::CandidateRecord> cands;
+  const p2cccd::Status st = p2cccd::CompactRawCandidates(scene, raw, &cands);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  *n_cand = static_cast<int64_t>(cands.size());
+  for (std::size_t k = 0; k < cands.size(); ++k) {
+    std::memset(&cand_out[k], 0, sizeof(p2c_candidate_record));
+    const p2cccd::CandidateRecord& c = cands[k];
+    p2c_candidate_record& o = cand_out[k];
+    o.schema_version = c.schema_version;
+    o.candidate_id = c.candidate_id;
+    o.query_id = c.query_id;
+    o.slab_id = c.slab_id;
+    o.object_a_id = c.object_a_id;
+    o.patch_a_id = c.patch_a_id;
+    o.object_b_id = c.object_b_id;
+    o.patch_b_id = c.patch_b_id;
+    o.proxy_type_a = static_cast<uint8_t>(c.proxy_type_a);
+    o.proxy_type_b = static_cast<uint8_t>(c.proxy_type_b);
+    o.rt_hit_count = c.rt_hit_count;
+    for (int m = 0; m < 4; ++m) o.motion_bound[m] = c.motion_bound[static_cast<std::size_t>(m)];
+    o.proxy_features_offset = c.proxy_features_offset;
+    o.flags = c.flags;
+  }
+  return 0;
+}
+
 // GenerateCandidatesForExternalBatch (CPU reference backend) on n external
 // queries: family 0 vertex-face / 1 edge-edge, 4 vertices at t0 and t1
 // (n x 12 doubles each), ground truth -1 none / 0 / 1, box pairs (has_box

@@ -40,6 +40,7 @@ static_assert(sizeof(p2c_candidate_record) == 80, "CandidateRecord layout");
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr uint32_t kHitFlags = 3u;  // kRawCandidateValid | kRawCandidateAabbOverlap
+constexpr unsigned long long kErrHitCountOverflow = 16ull;  // a candidate's summed rt_hit_count exceeds 32 bits
 
 unsigned grid_for(long long n) {
   const long long b = (n + kThreads - 1) / kThreads;
@@ -69,7 +70,7 @@ struct ProxyGrid {
 };
 
 struct ProxyLayout {
-  unsigned long long* counter;   // [0] raw hits, [1] error word
+  unsigned long long* counter;   // [0] raw hits, [1] error word, [2] first invalid given hit (hit << 4 | check)
   ProxyStats* stats;
   ProxyGrid* grid;
   unsigned long long* key[2];    // n: (slab << 30 | column << 16 | q), sorted copy
@@ -131,7 +132,7 @@ ProxyLayout carve(void* base, long long n, long long cap, int table_bits) {
     return p;
   };
   const size_t N = (size_t)std::max(n, 1ll), C = (size_t)std::max(cap, 1ll);
-  L.counter = static_cast<unsigned long long*>(take(16));
+  L.counter = static_cast<unsigned long long*>(take(24));
   L.stats = static_cast<ProxyStats*>(take(sizeof(ProxyStats)));
   L.grid = static_cast<ProxyGrid*>(take(sizeof(ProxyGrid)));
   for (int k = 0; k < 2; ++k) {
@@ -590,6 +591,65 @@ __global__ void heads_kernel(ProxyLayout L, const unsigned* perm, const unsigned
   L.head[p] = hd;
 }
 
+// Given raw hits: ValidateRawHit (candidate_buffer.cpp:71-101) on each, the
+// first failing hit's first failing check kept as (hit << 4 | check) in
+// counter[2]; then the compaction key chunks as raw_hits_kernel forms them,
+// from the hit's own proxy indices.
+__global__ void external_hits_kernel(p2c_proxy_scene sc, ProxyLayout L, const p2c_raw_candidate_hit* raw,
+                                     long long n_raw, CompactionKey ck) {
+  const long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= n_raw) return;
+  L.perm[0][h] = (unsigned)h;
+  const p2c_raw_candidate_hit r = raw[h];
+  const unsigned long long n = (unsigned long long)sc.n;
+  unsigned check = 0u;
+  if ((r.flags & 1u) == 0u) check = 1;
+  else if (r.query_id == 0ull) check = 2;
+  else if (r.query_id != sc.query_id) check = 3;
+  else if (r.proxy_a_index >= n || r.proxy_b_index >= n) check = 4;
+  else if (r.proxy_a_index == r.proxy_b_index) check = 5;
+  else {
+    const unsigned a = r.proxy_a_index, b = r.proxy_b_index;
+    const unsigned long long pk = ((unsigned long long)(a < b ? a : b) << 32) | (a < b ? b : a);
+    bool bound_ok = true;
+    for (int c = 0; c < 4; ++c) bound_ok = bound_ok && bound_valid(r.motion_bound[c]);
+    if (r.pair_key != pk) check = 6;
+    else if (sc.object_id[a] == sc.object_id[b]) check = 7;
+    else if (sc.slab_id[a] != sc.slab_id[b] || r.slab_id != sc.slab_id[a]) check = 8;
+    else if (!bound_ok) check = 9;
+  }
+  if (check != 0u) {
+    atomicMin(L.counter + 2, ((unsigned long long)h << 4) | check);
+    L.ck[0][h] = ~0ull;
+    L.ck[1][h] = ~0ull;
+    return;
+  }
+  const unsigned i = r.proxy_a_index, j = r.proxy_b_index;
+  const bool sw = hit_swapped(sc, i, j);
+  const unsigned f = sw ? j : i, t = sw ? i : j;
+  const unsigned long long types = ((unsigned long long)((sc.proxy_type[f] - 1u) & 1u) << 1) |
+                                   ((sc.proxy_type[t] - 1u) & 1u);
+  const unsigned long long lo = ((unsigned long long)L.rank_op[t] << 2) | types;
+  const unsigned long long hi = ((unsigned long long)L.rank_slab[i] << ck.rank_bits) | L.rank_op[f];
+  if (ck.single) {
+    L.ck[0][h] = (hi << (ck.rank_bits + 2)) | lo;
+  } else {
+    L.ck[0][h] = lo;
+    L.ck[1][h] = hi;
+  }
+}
+
+__global__ void first_invalid_kernel(ProxyLayout L, uint64_t* counts) {
+  if (threadIdx.x == 0) counts[3] = L.counter[2];
+}
+
+__global__ void set_hits_kernel(ProxyLayout L, long long n_raw) {
+  if (threadIdx.x == 0) {
+    L.counter[0] = (unsigned long long)n_raw;
+    L.counter[2] = ~0ull;
+  }
+}
+
 __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned* perm,
                                const p2c_raw_candidate_hit* raw, long long cap, p2c_candidate_record* out,
                                unsigned long long* counts) {
@@ -607,6 +667,7 @@ __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned
   r.candidate_id = (unsigned long long)L.seg[p] + 1ull;
   r.query_id = sc.query_id;
   const unsigned i = raw[a].proxy_a_index, j = raw[a].proxy_b_index;
+  if ((long long)i >= sc.n || (long long)j >= sc.n) return;  // an invalid given hit (reported, not compacted)
   const bool sw = hit_swapped(sc, i, j);
   const unsigned f = sw ? j : i, t = sw ? i : j;
   r.slab_id = raw[a].slab_id;
@@ -616,7 +677,8 @@ __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned
   r.patch_b_id = sc.patch_id[t];
   r.proxy_type_a = sc.proxy_type[f];
   r.proxy_type_b = sc.proxy_type[t];
-  unsigned count = 0u, flags = 0u;
+  unsigned long long count = 0ull;
+  unsigned flags = 0u;
   float mb[4] = {0.f, 0.f, 0.f, 0.f};
   for (long long q = p; q < n_hits && (q == p || !L.head[q]); ++q) {
     const p2c_raw_candidate_hit& h = raw[perm[q]];
@@ -628,7 +690,8 @@ __global__ void records_kernel(p2c_proxy_scene sc, ProxyLayout L, const unsigned
     count += h.rt_hit_count;
     flags |= h.flags;
   }
-  r.rt_hit_count = count;
+  if (count > 0xffffffffull) atomicOr(L.counter + 1, kErrHitCountOverflow);  // the reference's u32 sum overflows
+  r.rt_hit_count = (unsigned)count;
   for (int c = 0; c < 4; ++c) r.motion_bound[c] = mb[c];
   r.proxy_features_offset = 0u;
   r.flags = flags;
@@ -645,35 +708,36 @@ size_t p2c_proxy_candidates_workspace_bytes(int64_t n_proxies, int64_t raw_cap, 
   return p2c::carve(nullptr, n_proxies, raw_cap, p2c::table_bits_for(slab_bits)).total + 256;
 }
 
-int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* raw_dev, int64_t raw_cap,
-                         p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
-                         size_t workspace_bytes, void* stream) {
-  using namespace p2c;
+}  // extern "C"
+
+namespace p2c {
+namespace {
+
+struct ProxyRun {
+  p2c_proxy_scene sc;
+  ProxyLayout L;
+  long long n = 0;
+  int rank_bits = 1, slab_bits = 32, object_bits = 32, patch_bits = 32;
+};
+
+int proxy_checks(const p2c_proxy_scene* scene) {
   if (scene == nullptr) return fail(P2C_ERR_INVALID, "proxy scene pointer is null");
   if (scene->query_id == 0) return fail(P2C_ERR_INVALID, "ProxyScene.query_id is required");
   if (scene->n < 0 || scene->n >= (1ll << 31)) return fail(P2C_ERR_INVALID, "proxy count must lie in [0, 2^31)");
-  if (raw_cap < 0 || raw_cap >= (1ll << 31)) return fail(P2C_ERR_INVALID, "raw capacity must lie in [0, 2^31)");
-  if (counts_dev == nullptr) return fail(P2C_ERR_INVALID, "counts pointer is null");
-  if (raw_cap > 0 && (raw_dev == nullptr || candidates_dev == nullptr))
-    return fail(P2C_ERR_INVALID, "raw hit or candidate output pointer is null");
-  const long long n = scene->n;
-  if (n > 0 && (scene->object_id == nullptr || scene->patch_id == nullptr || scene->slab_id == nullptr ||
-                scene->proxy_type == nullptr || scene->t0 == nullptr || scene->t1 == nullptr ||
-                scene->bounds == nullptr || scene->motion_bound == nullptr))
+  if (scene->n > 0 && (scene->object_id == nullptr || scene->patch_id == nullptr || scene->slab_id == nullptr ||
+                       scene->proxy_type == nullptr || scene->t0 == nullptr || scene->t1 == nullptr ||
+                       scene->bounds == nullptr || scene->motion_bound == nullptr))
     return fail(P2C_ERR_INVALID, "proxy scene arrays are null");
-  const int table_bits = table_bits_for(scene->slab_bits);
-  const size_t need = carve(nullptr, n, raw_cap, table_bits).total;
-  if (workspace_dev == nullptr || workspace_bytes < need)
-    return fail(P2C_ERR_INVALID, "proxy candidate workspace too small: %zu < %zu bytes", workspace_bytes, need);
-  ProxyLayout L = carve(workspace_dev, n, raw_cap, table_bits);
-  cudaStream_t s = as_stream(stream);
-  const p2c_proxy_scene sc = *scene;
-  const long long cap = raw_cap;
-  const int rank_bits = std::max(1, bit_length((unsigned long long)std::max(n - 1, 1ll)));  // indices, ranks < n
-  const int slab_bits = sc.slab_bits > 0 && sc.slab_bits < 32 ? (int)sc.slab_bits : 32;
-  const int object_bits = sc.object_bits > 0 && sc.object_bits < 32 ? (int)sc.object_bits : 32;
-  const int patch_bits = sc.patch_bits > 0 && sc.patch_bits < 32 ? (int)sc.patch_bits : 32;
-  P2C_CUDA(cudaMemsetAsync(L.counter, 0, 16, s));
+  return P2C_OK;
+}
+
+// Validation, the sorted proxy layout of the sweep and the dense slab and
+// (object, patch) ranks the compaction keys are built from.
+int prepare(ProxyRun& R, cudaStream_t s) {
+  const p2c_proxy_scene& sc = R.sc;
+  ProxyLayout& L = R.L;
+  const long long n = R.n;
+  P2C_CUDA(cudaMemsetAsync(L.counter, 0, 24, s));
   if (n > 0) {
     stats_init_kernel<<<1, 32, 0, s>>>(L);
     keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
@@ -682,7 +746,7 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
     size_t tb = L.tmp_bytes;
     // (slab, column, quantised min) order, ties in proxy order
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.key[0], L.key[1], L.order[0], L.order[1], (int)n, 0,
-                                             30 + slab_bits, s));
+                                             30 + R.slab_bits, s));
     gather_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L);
     if (L.table_bits > 0) {
       P2C_CUDA(cudaMemsetAsync(L.cells, 0, L.table_bytes, s));
@@ -693,53 +757,136 @@ int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* ra
     tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceScan::InclusiveSum(L.tmp, tb, L.flag, L.scan, (int)n, s));
     slab_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
-    op_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, patch_bits);
+    op_keys_kernel<<<grid_for(n), kThreads, 0, s>>>(sc, L, R.patch_bits);
     tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.okey[0], L.okey[1], L.order[0], L.oidx, (int)n, 0,
-                                             object_bits + patch_bits, s));
+                                             R.object_bits + R.patch_bits, s));
     op_flags_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
     tb = L.tmp_bytes;
     P2C_CUDA(cub::DeviceScan::InclusiveSum(L.tmp, tb, L.flag, L.scan, (int)n, s));
     op_rank_kernel<<<grid_for(n), kThreads, 0, s>>>(L, n);
   }
+  return P2C_OK;
+}
+
+// Compaction of the hits [0, cap) whose key chunks and identity permutation
+// are written: stable sorts by the chunks, run heads, candidate ids, records.
+int compact(ProxyRun& R, const CompactionKey& ckey, const p2c_raw_candidate_hit* raw, long long cap,
+            p2c_candidate_record* candidates_dev, uint64_t* counts_dev, cudaStream_t s) {
+  ProxyLayout& L = R.L;
+  const int rank_bits = ckey.rank_bits;
+  const int n_chunks = ckey.single ? 1 : 2;
+  const unsigned long long* chunk[2] = {L.ck[0], L.ck[1]};
+  const int chunk_bits[2] = {ckey.single ? ckey.d_bits + 2 * rank_bits + 2 : rank_bits + 2, ckey.d_bits + rank_bits};
+  unsigned* perm_in = L.perm[0];
+  unsigned* perm_out = L.perm[1];
+  size_t tb;
+  for (int c = 0; c < n_chunks; ++c) {
+    gather_chunk_kernel<<<grid_for(cap), kThreads, 0, s>>>(chunk[c], perm_in, L.gk[0], cap);
+    tb = L.tmp_bytes;
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.gk[0], L.gk[1], perm_in, perm_out, (int)cap, 0,
+                                             chunk_bits[c], s));
+    std::swap(perm_in, perm_out);
+  }
+  heads_kernel<<<grid_for(cap + 1), kThreads, 0, s>>>(L, perm_in, chunk[0], ckey.single ? chunk[0] : chunk[1], cap);
+  tb = L.tmp_bytes;
+  P2C_CUDA(cub::DeviceScan::ExclusiveSum(L.tmp, tb, L.head, L.seg, (int)(cap + 1), s));
+  records_kernel<<<grid_for(cap), kThreads, 0, s>>>(R.sc, L, perm_in, raw, cap, candidates_dev,
+                                                    reinterpret_cast<unsigned long long*>(counts_dev));
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+CompactionKey compaction_key(const ProxyRun& R) {
+  CompactionKey ckey;
+  ckey.rank_bits = R.rank_bits;
+  ckey.d_bits = std::min(R.rank_bits, R.slab_bits);  // slab ranks < min(n, 2^slab_bits)
+  ckey.single = ckey.d_bits + 2 * R.rank_bits + 2 <= 64;
+  return ckey;
+}
+
+int setup(const p2c_proxy_scene* scene, long long raw_cap, void* workspace_dev, size_t workspace_bytes,
+          ProxyRun& R) {
+  R.sc = *scene;
+  R.n = scene->n;
+  const int table_bits = table_bits_for(scene->slab_bits);
+  const size_t need = carve(nullptr, R.n, raw_cap, table_bits).total;
+  if (workspace_dev == nullptr || workspace_bytes < need)
+    return fail(P2C_ERR_INVALID, "proxy candidate workspace too small: %zu < %zu bytes", workspace_bytes, need);
+  R.L = carve(workspace_dev, R.n, raw_cap, table_bits);
+  R.rank_bits = std::max(1, bit_length((unsigned long long)std::max(R.n - 1, 1ll)));  // indices, ranks < n
+  R.slab_bits = R.sc.slab_bits > 0 && R.sc.slab_bits < 32 ? (int)R.sc.slab_bits : 32;
+  R.object_bits = R.sc.object_bits > 0 && R.sc.object_bits < 32 ? (int)R.sc.object_bits : 32;
+  R.patch_bits = R.sc.patch_bits > 0 && R.sc.patch_bits < 32 ? (int)R.sc.patch_bits : 32;
+  return P2C_OK;
+}
+
+}  // namespace
+}  // namespace p2c
+
+extern "C" {
+
+int p2c_proxy_candidates(const p2c_proxy_scene* scene, p2c_raw_candidate_hit* raw_dev, int64_t raw_cap,
+                         p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
+                         size_t workspace_bytes, void* stream) {
+  using namespace p2c;
+  if (int rc = proxy_checks(scene)) return rc;
+  if (raw_cap < 0 || raw_cap >= (1ll << 31)) return fail(P2C_ERR_INVALID, "raw capacity must lie in [0, 2^31)");
+  if (counts_dev == nullptr) return fail(P2C_ERR_INVALID, "counts pointer is null");
+  if (raw_cap > 0 && (raw_dev == nullptr || candidates_dev == nullptr))
+    return fail(P2C_ERR_INVALID, "raw hit or candidate output pointer is null");
+  ProxyRun R;
+  if (int rc = setup(scene, raw_cap, workspace_dev, workspace_bytes, R)) return rc;
+  cudaStream_t s = as_stream(stream);
+  if (int rc = prepare(R, s)) return rc;
+  ProxyLayout& L = R.L;
+  const long long n = R.n, cap = raw_cap;
   if (cap > 0) fill_kernel<<<grid_for(cap), kThreads, 0, s>>>(L.pairs[0], cap);
   // the sweep counts every hit, also past the capacity (writes only below it)
-  if (n > 0) sweep_kernel<<<grid_for(n * kSweepLanes), kThreads, 0, s>>>(L, n, (unsigned long long)cap, rank_bits);
+  if (n > 0) sweep_kernel<<<grid_for(n * kSweepLanes), kThreads, 0, s>>>(L, n, (unsigned long long)cap, R.rank_bits);
   if (cap > 0) {
     size_t tb = L.tmp_bytes;
-    CompactionKey ckey;
-    ckey.rank_bits = rank_bits;
-    ckey.d_bits = std::min(rank_bits, slab_bits);  // slab ranks < min(n, 2^slab_bits)
-    ckey.single = ckey.d_bits + 2 * rank_bits + 2 <= 64;
+    const CompactionKey ckey = compaction_key(R);
     // the hits in (i, j) order
-    P2C_CUDA(cub::DeviceRadixSort::SortKeys(L.tmp, tb, L.pairs[0], L.pairs[1], (int)cap, 0, 2 * rank_bits, s));
-    raw_hits_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, L.pairs[1], (unsigned long long)cap, ckey, raw_dev);
+    P2C_CUDA(cub::DeviceRadixSort::SortKeys(L.tmp, tb, L.pairs[0], L.pairs[1], (int)cap, 0, 2 * R.rank_bits, s));
+    raw_hits_kernel<<<grid_for(cap), kThreads, 0, s>>>(R.sc, L, L.pairs[1], (unsigned long long)cap, ckey, raw_dev);
     P2C_CUDA(cudaGetLastError());
-    // compaction key order: stable sorts by the chunks, least significant first
-    const int n_chunks = ckey.single ? 1 : 2;
-    const unsigned long long* chunk[2] = {L.ck[0], L.ck[1]};
-    const int chunk_bits[2] = {ckey.single ? ckey.d_bits + 2 * rank_bits + 2 : rank_bits + 2,
-                               ckey.d_bits + rank_bits};
-    unsigned* perm_in = L.perm[0];
-    unsigned* perm_out = L.perm[1];
-    for (int c = 0; c < n_chunks; ++c) {
-      gather_chunk_kernel<<<grid_for(cap), kThreads, 0, s>>>(chunk[c], perm_in, L.gk[0], cap);
-      tb = L.tmp_bytes;
-      P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.tmp, tb, L.gk[0], L.gk[1], perm_in, perm_out, (int)cap, 0,
-                                               chunk_bits[c], s));
-      std::swap(perm_in, perm_out);
-    }
-    heads_kernel<<<grid_for(cap + 1), kThreads, 0, s>>>(L, perm_in, chunk[0], ckey.single ? chunk[0] : chunk[1], cap);
-    tb = L.tmp_bytes;
-    P2C_CUDA(cub::DeviceScan::ExclusiveSum(L.tmp, tb, L.head, L.seg, (int)(cap + 1), s));
-    records_kernel<<<grid_for(cap), kThreads, 0, s>>>(sc, L, perm_in, raw_dev, cap, candidates_dev,
-                                                      reinterpret_cast<unsigned long long*>(counts_dev));
-    P2C_CUDA(cudaGetLastError());
-  } else {
-    records_kernel<<<1, kThreads, 0, s>>>(sc, L, L.perm[0], raw_dev, 0, candidates_dev,
-                                          reinterpret_cast<unsigned long long*>(counts_dev));
-    P2C_CUDA(cudaGetLastError());
+    return compact(R, ckey, raw_dev, cap, candidates_dev, counts_dev, s);
   }
+  records_kernel<<<1, kThreads, 0, s>>>(R.sc, L, L.perm[0], raw_dev, 0, candidates_dev,
+                                        reinterpret_cast<unsigned long long*>(counts_dev));
+  P2C_CUDA(cudaGetLastError());
+  return P2C_OK;
+}
+
+size_t p2c_compact_raw_candidates_workspace_bytes(int64_t n_proxies, int64_t n_raw, uint32_t slab_bits) {
+  return p2c_proxy_candidates_workspace_bytes(n_proxies, n_raw, slab_bits);
+}
+
+int p2c_compact_raw_candidates(const p2c_proxy_scene* scene, const p2c_raw_candidate_hit* raw_dev, int64_t n_raw,
+                               p2c_candidate_record* candidates_dev, uint64_t* counts_dev, void* workspace_dev,
+                               size_t workspace_bytes, void* stream) {
+  using namespace p2c;
+  if (int rc = proxy_checks(scene)) return rc;
+  if (n_raw < 0 || n_raw >= (1ll << 31)) return fail(P2C_ERR_INVALID, "raw hit count must lie in [0, 2^31)");
+  if (counts_dev == nullptr) return fail(P2C_ERR_INVALID, "counts pointer is null");
+  if (n_raw > 0 && (raw_dev == nullptr || candidates_dev == nullptr))
+    return fail(P2C_ERR_INVALID, "raw hit or candidate pointer is null");
+  ProxyRun R;
+  if (int rc = setup(scene, n_raw, workspace_dev, workspace_bytes, R)) return rc;
+  cudaStream_t s = as_stream(stream);
+  if (int rc = prepare(R, s)) return rc;
+  set_hits_kernel<<<1, 32, 0, s>>>(R.L, n_raw);
+  if (n_raw == 0) {
+    records_kernel<<<1, kThreads, 0, s>>>(R.sc, R.L, R.L.perm[0], raw_dev, 0, candidates_dev,
+                                          reinterpret_cast<unsigned long long*>(counts_dev));
+  } else {
+    const CompactionKey ckey = compaction_key(R);
+    external_hits_kernel<<<grid_for(n_raw), kThreads, 0, s>>>(R.sc, R.L, raw_dev, n_raw, ckey);
+    if (int rc = compact(R, ckey, raw_dev, n_raw, candidates_dev, counts_dev, s)) return rc;
+  }
+  first_invalid_kernel<<<1, 32, 0, s>>>(R.L, counts_dev);
+  P2C_CUDA(cudaGetLastError());
   return P2C_OK;
 }
 

@@ -81,6 +81,9 @@ SIGNATURES: dict[str, tuple] = {
                                        _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p]),
     "p2c_proxy_candidates_workspace_bytes": (_size, [_i64, _i64, ctypes.c_uint32]),
     "p2c_proxy_candidates": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p]),
+    "p2c_compact_raw_candidates_workspace_bytes": (_size, [_i64, _i64, ctypes.c_uint32]),
+    "p2c_compact_raw_candidates": (_int, [_c_void_p, _c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _size,
+                                          _c_void_p]),
     "p2c_proxy_scene_count": (_i64, [_c_void_p, _i64]),
     "p2c_proxy_scene_build_workspace_bytes": (_size, [_c_void_p, _i64]),
     "p2c_proxy_scene_build": (_int, [ctypes.c_uint64, _c_void_p, _i64, _c_void_p, _c_void_p, _c_void_p, _i64, _i64,

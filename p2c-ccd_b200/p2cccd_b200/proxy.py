@@ -17,7 +17,18 @@ from . import _lib
 from .certify import _stream_ptr
 from .records import CANDIDATE_RECORD_DTYPE, DENSITY_DTYPE, FEATURE_ROW_DTYPE, RAW_HIT_DTYPE
 
-ERR_INVALID_PROXY, ERR_MOTION_BOUND, ERR_OVERFLOW, ERR_ID_BITS = 1, 2, 4, 8
+ERR_INVALID_PROXY, ERR_MOTION_BOUND, ERR_OVERFLOW, ERR_ID_BITS, ERR_HIT_COUNT_OVERFLOW = 1, 2, 4, 8, 16
+
+# ValidateRawHit's messages (rt_candidate/candidate_buffer.cpp:71-101) by the
+# check number p2c_compact_raw_candidates reports
+RAW_HIT_ERRORS = {1: "raw candidate hit is not marked valid", 2: "raw candidate query_id is required",
+                  3: "raw candidate query_id must match ProxyScene.query_id",
+                  4: "raw candidate proxy index is out of range",
+                  5: "raw candidate cannot reference the same proxy twice",
+                  6: "raw candidate pair_key does not match proxy indices",
+                  7: "raw candidate must reference two different objects",
+                  8: "raw candidate slab_id must match both proxy primitives",
+                  9: "raw candidate motion_bound must be finite and non-negative"}
 
 
 def _bits(max_id: int) -> int:
@@ -93,6 +104,37 @@ class ProxyCandidates:
                                                  self.cand.data_ptr(), self.counts.data_ptr(), self.ws.data_ptr(),
                                                  self.ws.numel(), _stream_ptr(self.device)))
         self._filled = True
+
+    def compact(self, raw: np.ndarray) -> np.ndarray:
+        """CompactRawCandidates on given raw hits of this scene
+        (p2c_compact_raw_candidates): their candidate records, or ValueError
+        with the reference's message for the first invalid hit."""
+        hits = np.ascontiguousarray(raw, dtype=RAW_HIT_DTYPE)
+        n = len(hits)
+        d = self.device
+        dh = torch.from_numpy(hits.view(np.uint8).reshape(-1).copy()).to(d) if n else None
+        out = torch.empty((max(n, 1), 80), dtype=torch.uint8, device=d)
+        counts = torch.zeros(4, dtype=torch.int64, device=d)
+        ws = torch.empty(int(self.lib.p2c_compact_raw_candidates_workspace_bytes(self.n, n, self._struct.slab_bits)),
+                         dtype=torch.uint8, device=d)
+        _lib.check(self.lib.p2c_compact_raw_candidates(ctypes.byref(self._struct), dh.data_ptr() if n else None, n,
+                                                       out.data_ptr(), counts.data_ptr(), ws.data_ptr(), ws.numel(),
+                                                       _stream_ptr(d)))
+        c = counts.cpu().numpy().view(np.uint64)
+        if int(c[2]) & ERR_ID_BITS:  # a width hint was wrong: again without hints
+            hint = (self._struct.slab_bits, self._struct.object_bits, self._struct.patch_bits)
+            self._struct.slab_bits = self._struct.object_bits = self._struct.patch_bits = 0
+            try:
+                return self.compact(raw)
+            finally:
+                self._struct.slab_bits, self._struct.object_bits, self._struct.patch_bits = hint
+        if int(c[2]) & ERR_INVALID_PROXY:
+            raise ValueError("proxy scene fails validation (proxy type, finite t0 < t1, finite ordered bounds)")
+        if n and int(c[3]) != 0xFFFFFFFFFFFFFFFF:
+            raise ValueError(RAW_HIT_ERRORS[int(c[3]) & 15])
+        if int(c[2]) & ERR_HIT_COUNT_OVERFLOW:
+            raise ValueError("candidate rt_hit_count overflow during compaction")
+        return out[:int(c[1])].cpu().numpy().view(CANDIDATE_RECORD_DTYPE).reshape(-1)
 
     def run_checked(self, max_retries: int = 3, raw_only: bool = False) -> tuple[np.ndarray, np.ndarray]:
         """Run; grow the buffers and re-run on overflow; raise on an invalid

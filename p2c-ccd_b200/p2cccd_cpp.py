@@ -1017,6 +1017,36 @@ def generate_raw_candidates_cpu(scene, query_id: int = 0) -> RawCandidateBuffer:
     return _raw_objects(raw)
 
 
+def _raw_array(raw_buffer) -> np.ndarray:
+    """RawCandidateBuffer (or its hits, or RAW_HIT_DTYPE records) as records."""
+    from p2cccd_b200.records import RAW_HIT_DTYPE
+
+    if isinstance(raw_buffer, np.ndarray):
+        return np.ascontiguousarray(raw_buffer, dtype=RAW_HIT_DTYPE)
+    hits = raw_buffer.hits if hasattr(raw_buffer, "hits") else raw_buffer
+    out = np.zeros(len(hits), RAW_HIT_DTYPE)
+    for r, h in zip(out, hits):
+        for k in ("query_id", "pair_key", "proxy_a_index", "proxy_b_index", "slab_id", "rt_hit_count", "flags"):
+            r[k] = int(getattr(h, k))
+        mb = list(h.motion_bound)
+        if len(mb) != 4:
+            raise ValueError("RawCandidateHit.motion_bound must have length 4")
+        r["motion_bound"] = mb
+    return out
+
+
+def compact_raw_candidates(scene, raw_buffer) -> list:  # py_module.cpp:373-379, 1873-1876
+    """CompactRawCandidates (rt_candidate/candidate_buffer.cpp:181-227) on the
+    GPU for any raw hits of the scene (from generate_raw_candidates_cpu or
+    another tracer): ValidateProxyScene, ValidateRawHit on every hit, then the
+    compacted CandidateRecords in key order with ids 1, 2, ..."""
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    a = _proxy_arrays(scene)
+    validate_proxy_scene(a)
+    return _candidate_objects(ProxyCandidates(a, raw_capacity=0).compact(_raw_array(raw_buffer)))
+
+
 def generate_candidates_for_proxy_scene(scene, query_id: int = 0, backend_name: str = "cpu_reference",
                                         allow_optix_cpu_fallback: bool = False) -> CandidateGenerationResult:
     """GenerateCandidatesForProxyScene (py_module.cpp:103-116) through

@@ -520,3 +520,90 @@ def test_mirror_schedule_functions(cuda_device, oracle_mod):
     with pytest.raises(ValueError, match="must have shape"):
         cpp.schedule_runtime_exact_work_items_from_proposal_arrays(fa, dict(pa, priority_score=pa["priority_score"][:-1]),
                                                                    masks, cfg)
+
+
+def _given_hits(oracle_mod, seed=11):
+    from p2cccd_b200 import scenes
+
+    sc = scenes.proxy_scene(n_objects=6, patches_per_object=40, n_slabs=3, seed=seed, duplicates=0.3)
+    raw, _ = oracle_mod.proxy_candidates(sc)
+    g = np.random.default_rng(seed)
+    hits = np.concatenate([raw, raw[g.choice(len(raw), len(raw) // 3)]])  # repeated hits sum their counts
+    hits = hits[g.permutation(len(hits))]  # the order of the hits does not matter
+    hits["rt_hit_count"] = g.integers(1, 5, len(hits))
+    hits["flags"] |= g.choice([0, 4, 8], len(hits)).astype(np.uint32)
+    hits["motion_bound"] *= g.uniform(1.0, 2.0, (len(hits), 4)).astype(np.float32)
+    return sc, hits
+
+
+@pytest.mark.gpu
+def test_device_compaction_of_given_hits(oracle_mod):
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    sc, hits = _given_hits(oracle_mod)
+    got = ProxyCandidates(sc, raw_capacity=0).compact(hits)
+    if oracle_mod.ref_available():
+        want = oracle_mod.ref_compact_raw(sc, hits)
+        assert got.tobytes() == want.tobytes()
+    assert got["rt_hit_count"].sum() == hits["rt_hit_count"].sum()
+    raw, cand = oracle_mod.proxy_candidates(sc)  # the scene's own hits give its candidates
+    assert ProxyCandidates(sc, raw_capacity=0).compact(raw).tobytes() == cand.tobytes()
+    assert len(ProxyCandidates(sc, raw_capacity=0).compact(hits[:0])) == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("fault", ["flags", "zero_query", "query", "index", "same", "pair_key", "object", "slab",
+                                   "bound", "two", "overflow"])
+def test_device_compaction_rejects_hits_like_reference(oracle_mod, fault):
+    from p2cccd_b200.proxy import ProxyCandidates
+
+    sc, hits = _given_hits(oracle_mod, seed=12)
+    k = len(hits) // 2
+    h = hits[k]
+    obj = np.asarray(sc["object_id"])
+    if fault == "flags":
+        hits["flags"][k] &= ~np.uint32(1)
+    elif fault == "zero_query":
+        hits["query_id"][k] = 0
+    elif fault == "query":
+        hits["query_id"][k] = int(sc["query_id"]) + 1
+    elif fault == "index":
+        hits["proxy_b_index"][k] = int(sc["n"]) + 3
+    elif fault == "same":
+        hits["proxy_b_index"][k] = h["proxy_a_index"]
+        hits["pair_key"][k] = (int(h["proxy_a_index"]) << 32) | int(h["proxy_a_index"])
+    elif fault == "pair_key":
+        hits["pair_key"][k] ^= 1
+    elif fault == "object":
+        a = int(h["proxy_a_index"])
+        b = int(np.nonzero((obj == obj[a]) & (np.arange(len(obj)) != a))[0][0])
+        hits["proxy_b_index"][k] = b
+        hits["pair_key"][k] = (min(a, b) << 32) | max(a, b)
+    elif fault == "slab":
+        hits["slab_id"][k] += 1
+    elif fault == "bound":
+        hits["motion_bound"][k, 2] = -1.0
+    elif fault == "two":  # the first invalid hit decides
+        hits["motion_bound"][k, 0] = np.inf
+        hits["flags"][k + 3] = 0
+    else:  # summed counts beyond 32 bits
+        dup = hits[k:k + 1].copy()
+        dup["rt_hit_count"] = 0xFFFFFFFF
+        hits = np.concatenate([hits, dup])
+    with pytest.raises(ValueError) as err:
+        ProxyCandidates(sc, raw_capacity=0).compact(hits)
+    if oracle_mod.ref_available():
+        with pytest.raises(ValueError) as ref_err:
+            oracle_mod.ref_compact_raw(sc, hits)
+        assert str(err.value) == str(ref_err.value)
+
+
+@pytest.mark.gpu
+def test_mirror_compact_raw_candidates(oracle_mod):
+    import p2cccd_cpp as cpp
+
+    sc, _ = _given_hits(oracle_mod, seed=13)
+    buf = cpp.generate_raw_candidates_cpu(sc)
+    got = cpp.compact_raw_candidates(sc, buf)
+    want = cpp.generate_candidates_for_proxy_scene(sc).candidates
+    assert cpp._candidate_array(got).tobytes() == cpp._candidate_array(want).tobytes()

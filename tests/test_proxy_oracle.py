@@ -396,3 +396,16 @@ def test_schedule_rejections_match_reference(oracle_mod):
             oracle_mod.schedule_runtime(c, r, o, m, 0)
     with pytest.raises(ValueError, match="first_work_item_id"):
         oracle_mod.ref_schedule_runtime(cand, rows, outs, {}, first_work_item_id=0)
+
+
+def test_reference_compaction_of_its_own_hits(oracle_mod):
+    """The compaction wrapper over given hits reproduces the reference's
+    generated candidates when handed the reference's raw hits."""
+    from p2cccd_b200 import scenes
+
+    if not oracle_mod.ref_available():
+        pytest.skip("reference library not built")
+    sc = scenes.proxy_scene(n_objects=5, patches_per_object=30, n_slabs=3, seed=7, duplicates=0.3)
+    raw, cand = oracle_mod.ref_proxy_candidates(sc)
+    got = oracle_mod.ref_compact_raw(sc, raw)
+    assert got.tobytes() == cand.tobytes()
