@@ -639,8 +639,13 @@ __global__ void external_hits_kernel(p2c_proxy_scene sc, ProxyLayout L, const p2
   }
 }
 
+// After the records: the error bits they set (a count overflow) and the
+// first invalid given hit.
 __global__ void first_invalid_kernel(ProxyLayout L, uint64_t* counts) {
-  if (threadIdx.x == 0) counts[3] = L.counter[2];
+  if (threadIdx.x == 0) {
+    counts[2] |= L.counter[1];
+    counts[3] = L.counter[2];
+  }
 }
 
 __global__ void set_hits_kernel(ProxyLayout L, long long n_raw) {
