@@ -1395,3 +1395,24 @@ def ref_compact_raw(sc: dict, raw):
     if R.ref_compact_raw(*args, _p(raw) if len(raw) else None, len(raw), _p(cand), ctypes.byref(n_cand)):
         raise ValueError(R.ref_proxy_last_error().decode())
     return cand[:n_cand.value]
+
+
+def ref_load_mesh(path: str, center: bool = False):
+    """The reference's LoadTriangleMesh (and CenterMeshAtAabbCenter): (vertices,
+    triangles, patch ids[, center]) or ValueError with its message."""
+    R = ref()
+    if not hasattr(R, "_mesh_ready"):
+        vp = ctypes.c_void_p
+        R.ref_load_mesh.argtypes = [ctypes.c_char_p, vp, vp, vp, vp, vp]
+        R.ref_proxy_last_error.restype = ctypes.c_char_p
+        R._mesh_ready = True
+    counts = np.zeros(3, np.int64)
+    if R.ref_load_mesh(str(path).encode(), _p(counts), None, None, None, None):
+        raise ValueError(R.ref_proxy_last_error().decode())
+    v = np.zeros((max(1, counts[0]), 3))
+    t = np.zeros((max(1, counts[1]), 3), np.uint32)
+    pid = np.zeros(max(1, counts[2]), np.uint32)
+    c = np.zeros(3)
+    R.ref_load_mesh(str(path).encode(), _p(counts), _p(v), _p(t), _p(pid), _p(c) if center else None)
+    out = (v[:counts[0]], t[:counts[1]], pid[:counts[2]])
+    return out + (c,) if center else out

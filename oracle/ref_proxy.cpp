@@ -13,11 +13,13 @@
 #include "rt_candidate/candidate_buffer.h"
 #include "rt_candidate/candidate_stats.h"
 #include "common/group_scheduler.h"
+#include "geometry/mesh_io.h"
 #include "common/validators.h"
 #include "rt_candidate/external_batch_candidate.h"
 #include "rt_candidate/proxy_scene.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstddef>
 #include <cstdint>
@@ -536,6 +538,43 @@ int ref_external_dummy(int64_t n, const uint64_t* source_id, const uint32_t* sou
     std::memcpy(cand_out + i, &cr.candidates[i], sizeof(p2c_candidate_record));
   write_schedule(result, items_out, stats_out, rows_out, outs_out, sizes_out);
   sizes_out[3] = static_cast<int64_t>(cr.candidates.size());
+  return 0;
+}
+
+// LoadTriangleMesh on a file: counts {vertices, triangles, patch ids} and,
+// when the outputs are given, the arrays (vertices n x 3 doubles, triangles
+// n x 3 u32, patch ids u32).  With center != NULL also CenterMeshAtAabbCenter
+// of the loaded mesh (vertices then centered, center written).
+int ref_load_mesh(const char* path, int64_t* counts, double* vertices, uint32_t* triangles, uint32_t* patch_ids,
+                  double* center) {
+  p2cccd::Mesh mesh;
+  p2cccd::Status st = p2cccd::LoadTriangleMesh(path, &mesh);
+  if (!st.ok) {
+    g_proxy_error = st.message;
+    return 1;
+  }
+  if (center != nullptr) {
+    p2cccd::Mesh centered;
+    std::array<double, 3> c{};
+    st = p2cccd::CenterMeshAtAabbCenter(mesh, &centered, &c);
+    if (!st.ok) {
+      g_proxy_error = st.message;
+      return 1;
+    }
+    mesh = centered;
+    for (int a = 0; a < 3; ++a) center[a] = c[static_cast<std::size_t>(a)];
+  }
+  counts[0] = static_cast<int64_t>(mesh.vertices_ref.size());
+  counts[1] = static_cast<int64_t>(mesh.triangles.size());
+  counts[2] = static_cast<int64_t>(mesh.patch_ids.size());
+  if (vertices != nullptr)
+    for (std::size_t i = 0; i < mesh.vertices_ref.size(); ++i)
+      for (int a = 0; a < 3; ++a) vertices[3 * i + static_cast<std::size_t>(a)] = mesh.vertices_ref[i][static_cast<std::size_t>(a)];
+  if (triangles != nullptr)
+    for (std::size_t i = 0; i < mesh.triangles.size(); ++i)
+      for (int a = 0; a < 3; ++a) triangles[3 * i + static_cast<std::size_t>(a)] = mesh.triangles[i][static_cast<std::size_t>(a)];
+  if (patch_ids != nullptr)
+    for (std::size_t i = 0; i < mesh.patch_ids.size(); ++i) patch_ids[i] = mesh.patch_ids[i];
   return 0;
 }
 

@@ -706,6 +706,219 @@ def generate_conservative_refinement_work_items(parent: ExactWorkItem, certifica
 # mesh-pair query (cpp/certificate/mesh_exact_query.cpp:143-327)
 
 
+class BenchmarkRow(_Struct):  # common/runtime_contracts.h (BenchmarkRow), py_module.cpp:1433-1447
+    _fields = (("query_count", 0), ("fn_count", 0), ("fp_count", 0), ("candidate_recall", 0.0),
+               ("avg_candidates", 0.0), ("avg_exact_evals", 0.0), ("avg_subdivision_depth", 0.0),
+               ("fallback_ratio", 0.0), ("rt_ms", 0.0), ("proposal_ms", 0.0), ("exact_ms", 0.0), ("total_ms", 0.0),
+               ("qps", 0.0))
+
+
+def validate_benchmark_row(row) -> bool:  # validators.cpp:317-357
+    if int(row.query_count) == 0:
+        raise ValueError("BenchmarkRow.query_count is required")
+    if int(row.fn_count) > int(row.query_count):
+        raise ValueError("BenchmarkRow.fn_count cannot exceed query_count")
+    for k in ("candidate_recall", "fallback_ratio"):  # ValidateRatio
+        v = float(getattr(row, k))
+        if not math.isfinite(v):
+            raise ValueError(f"BenchmarkRow.{k} must be finite")
+        if not (0.0 <= v <= 1.0):
+            raise ValueError(f"BenchmarkRow.{k} must be in [0, 1]")
+    for k in ("avg_candidates", "avg_exact_evals", "avg_subdivision_depth", "rt_ms", "proposal_ms", "exact_ms",
+              "total_ms", "qps"):  # RequireNonNegative
+        v = float(getattr(row, k))
+        if not math.isfinite(v):
+            raise ValueError(f"BenchmarkRow.{k} must be finite")
+        if not v >= 0.0:
+            raise ValueError(f"BenchmarkRow.{k} must be non-negative")
+    return True
+
+
+def validate_candidate_record(record) -> bool:  # validators.cpp:160-181, py_module.cpp:488-491
+    from p2cccd_b200.schedule import candidate_record_error
+
+    msg = candidate_record_error(_candidate_array([record])[0])
+    if msg:
+        raise ValueError(msg)
+    return True
+
+
+# ---- triangle meshes (geometry/mesh_io.cpp) --------------------------------
+
+def _area2(v, t) -> float:  # TriangleAreaSquared (:113-119): 0.25 * |e0 x e1|^2, the reference's op order
+    a, b, c = v[t[0]], v[t[1]], v[t[2]]
+    e0 = (b[0] - a[0], b[1] - a[1], b[2] - a[2])
+    e1 = (c[0] - a[0], c[1] - a[1], c[2] - a[2])
+    x = (e0[1] * e1[2] - e0[2] * e1[1], e0[2] * e1[0] - e0[0] * e1[2], e0[0] * e1[1] - e0[1] * e1[0])
+    return 0.25 * (x[0] * x[0] + x[1] * x[1] + x[2] * x[2])
+
+
+def validate_triangle_mesh(mesh) -> bool:  # ValidateTriangleMesh, mesh_io.cpp:306-340
+    v, t, p = list(mesh.vertices_ref), list(mesh.triangles), list(mesh.patch_ids)
+    if not v:
+        raise ValueError("mesh has no vertices")
+    if not t:
+        raise ValueError("mesh has no triangles")
+    if p and len(p) != len(t):
+        raise ValueError("mesh patch_ids must be empty or match triangle count")
+    for vert in v:
+        if not all(math.isfinite(float(x)) for x in vert):
+            raise ValueError("mesh vertex contains a non-finite coordinate")
+    vf = [tuple(float(x) for x in vert) for vert in v]
+    for tri in t:
+        i = [int(x) for x in tri]
+        if i[0] == i[1] or i[0] == i[2] or i[1] == i[2]:
+            raise ValueError("mesh triangle contains duplicate vertex indices")
+        if any(x >= len(v) for x in i):
+            raise ValueError("mesh triangle references a vertex outside the vertex array")
+        if _area2(vf, i) <= 0.0:
+            raise ValueError("mesh triangle has zero area")
+    return True
+
+
+def center_mesh_at_aabb_center(mesh) -> tuple:  # CenterMeshAtAabbCenter, mesh_io.cpp:423-456
+    validate_triangle_mesh(mesh)
+    v = [tuple(float(x) for x in vert) for vert in mesh.vertices_ref]
+    lo, hi = list(v[0]), list(v[0])
+    for vert in v:
+        for a in range(3):
+            lo[a] = vert[a] if vert[a] < lo[a] else lo[a]  # std::min
+            hi[a] = vert[a] if hi[a] < vert[a] else hi[a]  # std::max
+    center = [0.5 * (lo[a] + hi[a]) for a in range(3)]
+    out = Mesh()
+    out.vertices_ref = [[vert[0] - center[0], vert[1] - center[1], vert[2] - center[2]] for vert in v]
+    out.triangles = [list(t) for t in mesh.triangles]
+    out.patch_ids = list(mesh.patch_ids)
+    return out, center
+
+
+def _obj_index(token: str, count: int) -> int:  # ParseObjVertexIndex, :52-91
+    text = token.split("/", 1)[0]
+    if not text:
+        raise ValueError("OBJ face token has empty vertex index")
+    body = text[1:] if text[:1] in "+-" else text
+    if not body or not body.isdigit():
+        if not body or not body[:1].isdigit():
+            raise ValueError("OBJ face token has invalid vertex index")
+        raise ValueError("OBJ vertex index must be a non-zero integer")
+    k = int(text)
+    if abs(k) > (1 << 63) - 1:  # std::stoll's range
+        raise ValueError("OBJ face token has invalid vertex index")
+    if k == 0:
+        raise ValueError("OBJ vertex index must be a non-zero integer")
+    z = k - 1 if k > 0 else count + k
+    if z < 0 or z >= count:
+        raise ValueError("OBJ face references a vertex outside the loaded vertex range")
+    return z
+
+
+def _load_obj(path: str) -> Mesh:  # LoadTriangleMeshObj, :342-409 (default options: triangulate, one patch)
+    import re
+
+    num = re.compile(r"^[+-]?(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?")  # what operator>> reads as a double
+    m = Mesh()
+    try:
+        text = open(path, encoding="utf-8", errors="replace").read().splitlines()
+    except OSError:
+        raise ValueError("failed to open OBJ file: " + str(path)) from None
+    for ln, line in enumerate(text, 1):
+        toks = line.split("#", 1)[0].split()
+        if not toks:
+            continue
+        if toks[0] == "v":
+            vals = []
+            for tok in toks[1:4]:  # operator>> reads the leading number of each token
+                mm = num.match(tok)
+                if not mm:
+                    break
+                vals.append(float(mm.group(0)))
+                if mm.end() != len(tok):
+                    break
+            if len(vals) < 3:
+                raise ValueError(f"invalid OBJ vertex at line {ln}")
+            m.vertices_ref.append(vals)
+        elif toks[0] == "f":
+            try:
+                face = [_obj_index(tok, len(m.vertices_ref)) for tok in toks[1:]]
+                if len(face) < 3:
+                    raise ValueError("OBJ face must have at least 3 vertices")
+                for i in range(1, len(face) - 1):  # AddFaceTriangles (:121-140): a fan from the first vertex
+                    if face[0] == face[i] or face[0] == face[i + 1] or face[i] == face[i + 1]:
+                        raise ValueError("OBJ face creates a degenerate triangle with duplicate indices")
+                    m.triangles.append([face[0], face[i], face[i + 1]])
+                    m.patch_ids.append(0)
+            except ValueError as e:
+                raise ValueError(f"{e} at line {ln}") from None
+    validate_triangle_mesh(m)
+    return m
+
+
+def _dedup_vertices(xyz: np.ndarray) -> tuple:
+    """AddOrGetVertexIndex (:164-188): float vertices numbered in first-seen
+    order, equal floats (+0 and -0 alike) sharing one index."""
+    key = np.where(xyz == 0, np.float32(0.0), xyz).view(np.uint32)  # +0 and -0 compare equal
+    flat = key.reshape(-1, 3)
+    _, first, inv = np.unique(flat, axis=0, return_index=True, return_inverse=True)
+    order = np.argsort(first, kind="stable")
+    rank = np.empty(len(order), np.int64)
+    rank[order] = np.arange(len(order))
+    idx = rank[inv.reshape(-1)]
+    verts = xyz.reshape(-1, 3)[np.sort(first)].astype(np.float64)
+    return verts, idx
+
+
+def _stl_mesh(xyz: np.ndarray) -> Mesh:
+    verts, idx = _dedup_vertices(xyz.astype(np.float32))
+    tri = idx.reshape(-1, 3)
+    keep = (tri[:, 0] != tri[:, 1]) & (tri[:, 0] != tri[:, 2]) & (tri[:, 1] != tri[:, 2])
+    m = Mesh()
+    m.vertices_ref = verts.tolist()
+    m.triangles = tri[keep].tolist()
+    validate_triangle_mesh(m)
+    return m
+
+
+def _load_stl(path: str) -> Mesh:  # LooksLikeBinaryStl + the binary / ASCII loaders, :142-300
+    import os
+
+    try:
+        size = os.path.getsize(path)
+        raw = open(path, "rb").read()
+    except OSError:
+        raise ValueError("failed to open STL file: " + str(path)) from None
+    if size >= 84 and 84 + int(np.frombuffer(raw[80:84], "<u4")[0]) * 50 == size:
+        n = int(np.frombuffer(raw[80:84], "<u4")[0])
+        rec = np.frombuffer(raw[84:], dtype=np.dtype([("f", "<f4", (12,)), ("a", "<u2")]), count=n)
+        return _stl_mesh(rec["f"][:, 3:12].reshape(-1, 3))
+    rows = []
+    for line in raw.decode("utf-8", errors="replace").splitlines():
+        toks = line.split()
+        if not toks or toks[0] not in ("vertex", "VERTEX"):
+            continue
+        try:
+            rows.append([np.float32(t) for t in toks[1:4]])
+        except ValueError:
+            raise ValueError("invalid ASCII STL vertex row in " + str(path)) from None
+        if len(rows[-1]) < 3:
+            raise ValueError("invalid ASCII STL vertex row in " + str(path))
+    if len(rows) % 3:
+        raise ValueError("ASCII STL ended with a partial triangle")
+    return _stl_mesh(np.array(rows, np.float32).reshape(-1, 3))
+
+
+def load_triangle_mesh(path) -> Mesh:  # LoadTriangleMesh, mesh_io.cpp:411-421
+    """OBJ (fan-triangulated polygons, one patch) or STL (binary or ASCII,
+    float vertices merged by value) into a Mesh, validated."""
+    import os
+
+    ext = os.path.splitext(str(path))[1]
+    if ext in (".obj", ".OBJ"):
+        return _load_obj(str(path))
+    if ext in (".stl", ".STL"):
+        return _load_stl(str(path))
+    raise ValueError("unsupported triangle mesh format: " + ext)
+
+
 def _mesh_arrays(mesh: Mesh):
     v = np.asarray(mesh.vertices_ref, dtype=np.float64).reshape(-1, 3)
     f = np.asarray(mesh.triangles, dtype=np.int64).reshape(-1, 3)
