@@ -1230,6 +1230,41 @@ def generate_raw_candidates_cpu(scene, query_id: int = 0) -> RawCandidateBuffer:
     return _raw_objects(raw)
 
 
+RAW_CANDIDATE_VALID = 1  # RawCandidateFlags (rt_candidate/candidate_buffer.h:14-17)
+RAW_CANDIDATE_AABB_OVERLAP = 2
+
+
+class CandidateBackend(enum.IntEnum):  # rt_candidate/candidate_generator.h:13-16
+    CPU_REFERENCE = 0
+    OPTIX = 1
+
+
+class CandidateGeneratorConfig(_Struct):  # :18-21
+    _fields = (("backend", CandidateBackend.CPU_REFERENCE), ("allow_optix_cpu_fallback", False))
+
+
+class CandidateGenerator:  # :23-38, py_module.cpp:1821-1829
+    """The candidate generator of a backend config; both backends run the
+    device proxy path (OptiX as the reference built without it)."""
+
+    def __init__(self, config: CandidateGeneratorConfig | None = None):
+        self.config = config if config is not None else CandidateGeneratorConfig()
+
+    def trace_candidates_for_proxy_scene(self, scene, query_id: int = 0) -> list:
+        """TraceCandidates (candidate_generator.cpp:40-47): the candidates, or
+        an empty list where generation fails."""
+        name = "optix" if CandidateBackend(self.config.backend) == CandidateBackend.OPTIX else "cpu_reference"
+        try:
+            return generate_candidates_for_proxy_scene(scene, query_id, name,
+                                                       bool(self.config.allow_optix_cpu_fallback)).candidates
+        except ValueError:
+            return []
+
+
+class ObjLoadOptions(_Struct):  # geometry/mesh_io.h:10-13
+    _fields = (("triangulate_polygon_faces", True), ("use_object_groups_as_patch_ids", False))
+
+
 def _raw_array(raw_buffer) -> np.ndarray:
     """RawCandidateBuffer (or its hits, or RAW_HIT_DTYPE records) as records."""
     from p2cccd_b200.records import RAW_HIT_DTYPE

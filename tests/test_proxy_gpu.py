@@ -607,3 +607,19 @@ def test_mirror_compact_raw_candidates(oracle_mod):
     got = cpp.compact_raw_candidates(sc, buf)
     want = cpp.generate_candidates_for_proxy_scene(sc).candidates
     assert cpp._candidate_array(got).tobytes() == cpp._candidate_array(want).tobytes()
+
+
+@pytest.mark.gpu
+def test_mirror_candidate_generator(oracle_mod):
+    import p2cccd_cpp as cpp
+
+    sc, _ = _given_hits(oracle_mod, seed=14)
+    want = cpp._candidate_array(cpp.generate_candidates_for_proxy_scene(sc).candidates)
+    gen = cpp.CandidateGenerator()
+    assert cpp._candidate_array(gen.trace_candidates_for_proxy_scene(sc)).tobytes() == want.tobytes()
+    cfg = cpp.CandidateGeneratorConfig()
+    cfg.backend = cpp.CandidateBackend.OPTIX
+    assert cpp.CandidateGenerator(cfg).trace_candidates_for_proxy_scene(sc) == []  # built without OptiX
+    cfg.allow_optix_cpu_fallback = True
+    got = cpp.CandidateGenerator(cfg).trace_candidates_for_proxy_scene(sc)
+    assert cpp._candidate_array(got).tobytes() == want.tobytes()
