@@ -1090,7 +1090,7 @@ def run_serve(args) -> dict:
     seed = 20261203 + rank
     cfg = certify.CertConfig(1e-6, 1e-6, 32)
     pool = _serve_pool(seed)
-    eng = ServeEngine(dev, config=cfg, slots=4, max_group=16)
+    eng = ServeEngine(dev, config=cfg, slots=SERVE_SLOTS, max_group=SERVE_MAX_GROUP)
     host = {}
     for key, s, excl in pool:
         eng.register_mesh(key, s, exclude_self=excl)
@@ -1372,6 +1372,7 @@ def run_proxy(args) -> dict | None:
 
 
 GROUP_ROWS = 1_000_000  # rows of the candidate-group workload (--group-rows)
+SERVE_SLOTS, SERVE_MAX_GROUP = 4, 16  # serving engine: groups in flight, requests per group
 GROUP_CFG = {"threshold": 0.75, "limit": 3, "penalty": 0.22}  # the binding's defaults
 
 
@@ -1677,11 +1678,14 @@ def main():
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     ap.add_argument("--proxy-objects", type=int, default=32, help="proxy: rigid bodies of 200 patches x 8 slabs")
     ap.add_argument("--group-rows", type=int, default=1_000_000, help="groups: candidate rows per step")
+    ap.add_argument("--serve-slots", type=int, default=4, help="serving: request groups in flight")
+    ap.add_argument("--serve-max-group", type=int, default=16, help="serving: requests admitted per group")
     ap.add_argument("--benchmark-rows", default=None, metavar="DIR",
                     help="also write the run as BenchmarkRowV2 JSONL / CSV (the reference's export schema) to DIR")
     args = ap.parse_args()
-    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS, GROUP_ROWS
+    global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS, GROUP_ROWS, SERVE_SLOTS, SERVE_MAX_GROUP
     PROXY_OBJECTS = max(2, args.proxy_objects)
+    SERVE_SLOTS, SERVE_MAX_GROUP = max(1, args.serve_slots), max(1, args.serve_max_group)
     GROUP_ROWS = max(1, args.group_rows)
     BATCH_SCENES, AUTOTUNE_REPS = max(1, args.scenes), max(0, args.autotune_reps)
     CLOTH_N = max(9, args.cloth_n)
