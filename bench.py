@@ -1494,7 +1494,7 @@ def run_groups(args) -> dict | None:
 
 
 BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
-CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = configs[3])
+CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = the dense-contact stress case)
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
 
