@@ -250,15 +250,7 @@ class SceneWorkload:
         self.launches_per_step = None
 
     def config(self) -> dict:
-        sp = self.scene["spec"]
-        return {"workload": "single-scene broad+narrow: two UV spheres of 40,960 triangles each (160 x 128 rings; "
-                            "40,960 is not an icosphere level), FP64, B translating toward A "
-                            f"(gap {sp['gap']}, approach {sp['approach']} per step) + per-vertex N(0,{sp['jitter']}) "
-                            "jitter, swept-AABB candidates (A x B) then exact VF/EE certificates of every candidate",
-                "vertices": int(len(self.scene["v_t0"])), "triangles": int(len(self.scene["faces"])),
-                "edges": int(len(self.scene["edges"])), "vf_candidates": self.n_vf, "ee_candidates": self.n_ee,
-                "queries_per_step": self.queries, "eps_time": self.cfg.eps_time, "eps_space": self.cfg.eps_space,
-                "max_subdivision_depth": self.cfg.max_subdivision_depth, "seed": sp["seed"]}
+        return scene_config(self.scene, self.cfg)
 
     def step(self):
         self.pipe.replay()  # the captured step: one graph launch
@@ -339,7 +331,62 @@ class SceneWorkload:
         return 48 * len(s["v_t0"]) + 12 * len(s["faces"]) + 8 * len(s["edges"]) + 8 * self.queries
 
     def cpu_reference(self, threads: int, budget_s: float) -> dict:
-        return _scene_reference_sample(self.scene, self.cfg, budget_s, threads)
+        ref = ToolSceneStep(self.scene, self.cfg)
+        q_sum, s_sum, rounds = 0, 0.0, 0
+        t_start = time.perf_counter()
+        while True:
+            q, sec = ref.run()
+            q_sum, s_sum, rounds = q_sum + q, s_sum + sec, rounds + 1
+            if time.perf_counter() - t_start >= budget_s:
+                break
+        return {"queries": q_sum / rounds, "seconds": s_sum / rounds, "threads": 1,
+                "sample": ref.describe() + f"; {rounds} whole step(s)"}
+
+
+def scene_config(scene: dict, cfg) -> dict:
+    """The scene workload's config, identical in both arms: built from the
+    seeded scene alone (the candidate counts are reported per arm, beside it)."""
+    sp = scene["spec"]
+    return {"workload": "single-scene broad+narrow: two UV spheres of 40,960 triangles each (160 x 128 rings; "
+                        "40,960 is not an icosphere level), FP64, B translating toward A "
+                        f"(gap {sp['gap']}, approach {sp['approach']} per step) + per-vertex N(0,{sp['jitter']}) "
+                        "jitter, swept-AABB candidates (A x B) then exact VF/EE certificates of every candidate",
+            "vertices": int(len(scene["v_t0"])), "triangles": int(len(scene["faces"])),
+            "edges": int(len(scene["edges"])), "eps_time": cfg.eps_time, "eps_space": cfg.eps_space,
+            "max_subdivision_depth": cfg.max_subdivision_depth, "seed": sp["seed"]}
+
+
+class ToolSceneStep:
+    """One step of the reference's own scene path on the identical scene:
+    the scene tool (tools/scene_object_envelope_native_ti_walltime.cpp, compiled
+    unchanged) builds its candidates with SweepPairs / BuildVFCandidates /
+    BuildEECandidates (:603-696) and certifies every candidate with its
+    RunAllExactRows (:1239-1281), whose exact kernel answers with the reference
+    certifier.  Single-threaded, as the tool is written.  PrepareScene (PLY
+    frames in, swept boxes, edge list) runs once, outside the timed step."""
+
+    def __init__(self, scene, cfg, exclude_self: bool = True):
+        import oracle
+
+        self.cfg = cfg
+        t0 = time.perf_counter()
+        self.tool = oracle.RefToolScene(scene["v_t0"], scene["v_t1"], scene["faces"], 0.0, exclude_self)
+        self.prepare_s = time.perf_counter() - t0
+        self.last = None
+
+    def run(self) -> tuple[int, float]:
+        c = self.cfg
+        r = self.tool.time_all_exact(c.eps_time, c.eps_space, c.max_subdivision_depth)
+        self.last = r
+        return r["calls"], r["candidates_s"] + r["certify_s"]
+
+    def describe(self) -> str:
+        r = self.last or {}
+        return ("the identical scene through the reference scene tool compiled unchanged: SweepPairs candidates + "
+                "RunAllExactRows certificates of every candidate (reference certifier), 1 thread as written; "
+                f"last step {r.get('candidates_s', 0.0):.3f} s candidates + {r.get('certify_s', 0.0):.4f} s "
+                f"certificates, {r.get('calls', 0)} candidates; PrepareScene ({self.prepare_s:.2f} s incl. PLY "
+                "frames) outside the step")
 
 
 class BatchWorkload:
@@ -982,6 +1029,7 @@ def run_b200(args) -> dict | None:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {**wl.config(), "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write)",
                    "parallelism": f"replicas x{world}"},
+        "queries_per_step": wl.queries,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms, "pipelined": e2e_times is not e2e_serial_times,
                 "serial_ms_per_step": statistics.mean(e2e_serial_times),
@@ -1497,6 +1545,7 @@ BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
 CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = the dense-contact stress case)
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
+REF_ARM_CAP_S = 600.0  # hard cap on a reference arm of whole steps (the scene tool's step is ~4 s)
 
 
 def run_reference(args) -> dict | None:
@@ -1567,7 +1616,7 @@ def run_reference(args) -> dict | None:
             return nq, time.perf_counter() - t0
         conf = {"workload": "plain exact CCD: 10,000 VF + 10,000 EE seeded FP64 queries"}
         sample = f"the full {nq}-query batch per step, {threads} threads over the reference certifier"
-    elif args.workload == "scene":
+    elif args.workload == "scene" and args.scene_reference == "builder":
         scene = scenes.two_spheres()
         probe = SceneReferenceSample(scene, cfg, threads, 1)
         t0 = time.perf_counter()
@@ -1579,8 +1628,17 @@ def run_reference(args) -> dict | None:
             q, b, c = ref.run(i)
             return q, b + c
         conf = {"workload": "single-scene broad+narrow: two 40,960-triangle UV spheres, translation-only form "
-                            "(the reference mesh builder takes rigid translations only)"}
+                            "(the reference mesh builder takes rigid translations only); EXTRAPOLATED from slices"}
         sample = ref.describe() + "; one slice per step"
+    elif args.workload == "scene":
+        scene = scenes.two_spheres()
+        ref = ToolSceneStep(scene, cfg)
+
+        def step(i):
+            return ref.run()
+        conf = scene_config(scene, cfg)
+        threads = 1
+        sample = None  # filled from the tool's last step
     elif args.workload in ("batch", "serve"):
         if args.workload == "batch":
             batch = scenes.uneven_batch(BATCH_SCENES)
@@ -1630,6 +1688,7 @@ def run_reference(args) -> dict | None:
                   f"the {n} x {n} cloth instance ({n_tris} triangles; the full instance has 624,288), the largest "
                   f"whose step fits {per_step_s * 1e3:.0f} ms of wall time")
         threads = 1
+    t_arm = time.perf_counter()
     for i in range(args.warmup):
         step(i)
     times, qs = [], []
@@ -1637,16 +1696,22 @@ def run_reference(args) -> dict | None:
         q, sec = step(args.warmup + i)
         times.append(sec)
         qs.append(q)
+        if time.perf_counter() - t_arm > REF_ARM_CAP_S:
+            break  # bounded run: the line reports how many steps were timed
     ms = statistics.mean(times) * 1e3
     value = sum(qs) / sum(times)
-    conf["queries_per_step"] = statistics.mean(qs)
-    return {"metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+    if sample is None:
+        sample = ref.describe() + f"; {len(times)} whole step(s) timed"
+    line = {"metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
+            "steps": len(times), "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": conf,
-            "impl": "reference",
+            "queries_per_step": statistics.mean(qs), "impl": "reference",
             "cpu_baseline": {"value": value, "unit": "queries/s", "cores": threads, "kind": "reference",
                              "sample": sample},
             "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    if len(times) < args.steps:
+        line["steps_requested"] = args.steps
+    return line
 
 
 def _host_cpu() -> dict:
@@ -1682,6 +1747,9 @@ def main():
     ap.add_argument("--group-rows", type=int, default=1_000_000, help="groups: candidate rows per step")
     ap.add_argument("--serve-slots", type=int, default=4, help="serving: request groups in flight")
     ap.add_argument("--serve-max-group", type=int, default=16, help="serving: requests admitted per group")
+    ap.add_argument("--scene-reference", default="tool", choices=["tool", "builder"],
+                    help="reference arm of the scene: the scene tool's own SweepPairs path on the identical scene "
+                         "(default) or the translation-only mesh builder, extrapolated from slices")
     ap.add_argument("--benchmark-rows", default=None, metavar="DIR",
                     help="also write the run as BenchmarkRowV2 JSONL / CSV (the reference's export schema) to DIR")
     args = ap.parse_args()

@@ -291,8 +291,9 @@ typedef struct p2c_scene_summary {
   p2c_query_certificate query;
   uint64_t collisions, separations, undecided;
   uint64_t vf_certified, ee_certified;
-  uint64_t undecided_queued;                /* entries written to the undecided queue */
-  uint64_t error_word;                      /* 1: time budget, 2: pair overflow, 4: invalid geometry */
+  uint64_t undecided_queued;                /* this scene's undecided entries (written or dropped) */
+  uint64_t error_word;                      /* 1: time budget, 2: pair overflow, 4: invalid geometry,
+                                               8: undecided queue full (entries of this scene dropped) */
 } p2c_scene_summary;
 
 size_t p2c_scene_certify_workspace_bytes(void);
@@ -303,7 +304,9 @@ size_t p2c_scene_certify_workspace_bytes(void);
  * the device, so this can follow p2c_scene_candidates without a host sync.
  * Results are positional with the pair lists.  Undecided candidates are
  * appended to undecided_queue_dev as (family << 63 | pair position) when it is
- * non-NULL (capacity undecided_cap).  summary_dev may be NULL. */
+ * non-NULL (capacity undecided_cap); entries past the capacity are counted in
+ * undecided_queued but not written, and set bit 8 of the summary's error word
+ * (the caller re-runs with a larger queue).  summary_dev may be NULL. */
 int p2c_scene_certify(const p2c_scene* scene, const uint64_t* vf_pairs_dev, int64_t vf_cap,
                       const uint64_t* ee_pairs_dev, int64_t ee_cap, const uint64_t* counts_dev,
                       double interval_t0, double interval_t1, const p2c_cert_config* config,
@@ -377,9 +380,14 @@ size_t p2c_batch_certify_workspace_bytes(int32_t n_scenes);
  * queues that all warps drain together, so small and large scenes share the
  * GPU.  Per scene, summaries_dev[s] (may be NULL) receives the
  * CertificateEngine::Evaluate reduction exactly as p2c_scene_certify writes
- * it; undecided candidates are appended to undecided_queue_dev (may be NULL)
- * as (scene << 40 | (family - 1) << 39 | pair position).  No host sync; the
- * sizes are read on the device.  tuning may be NULL (defaults). */
+ * it; undecided candidates of all scenes are appended to the one queue
+ * undecided_queue_dev (may be NULL), in completion order, as
+ * (scene << 40 | (family - 1) << 39 | pair position): slots come from one
+ * launch-wide counter, summaries_dev[s].undecided_queued counts scene s's
+ * entries, and the queue holds the first min(sum, undecided_cap) of them.  A
+ * scene with an entry past the capacity gets bit 8 in its summary's error
+ * word.  No host sync; the sizes are read on the device.  tuning may be NULL
+ * (defaults). */
 int p2c_batch_certify(const p2c_batch_scene* scenes_dev, int32_t n_scenes, double interval_t0, double interval_t1,
                       const p2c_cert_config* config, uint32_t family_mask, p2c_scene_summary* summaries_dev,
                       uint64_t* undecided_queue_dev, int64_t undecided_cap, const p2c_batch_tuning* tuning,

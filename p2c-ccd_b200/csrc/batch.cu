@@ -30,6 +30,7 @@ struct BatchLayout {
   CertifyScratch* sc = nullptr;
   unsigned long long* off[2] = {nullptr, nullptr};  // n_scenes + 1 prefix offsets per family
   SceneAgg* aggs = nullptr;
+  unsigned long long* uq_slots = nullptr;  // entries of the shared undecided queue (all scenes)
   size_t total = 0;
 };
 
@@ -46,6 +47,7 @@ BatchLayout carve(void* base, long long n_scenes) {
   L.off[0] = static_cast<unsigned long long*>(take((size_t)(n_scenes + 1) * 8));
   L.off[1] = static_cast<unsigned long long*>(take((size_t)(n_scenes + 1) * 8));
   L.aggs = static_cast<SceneAgg*>(take((size_t)std::max(n_scenes, 1ll) * sizeof(SceneAgg)));
+  L.uq_slots = static_cast<unsigned long long*>(take(sizeof(unsigned long long)));
   L.total = off;
   return L;
 }
@@ -65,6 +67,7 @@ __global__ void __launch_bounds__(kPrepThreads) batch_prep_kernel(const p2c_batc
   __shared__ typename Scan::TempStorage tmp;
   __shared__ unsigned long long carry[2];
   if (threadIdx.x < 2) carry[threadIdx.x] = 0ull;
+  if (threadIdx.x == 0) *L.uq_slots = 0ull;
   __syncthreads();
   for (int base = 0; base < n_scenes; base += kPrepThreads) {
     const int s = base + (int)threadIdx.x;
@@ -108,6 +111,7 @@ struct BatchProblem {
   SceneAgg* aggs;
   unsigned long long* uq;
   unsigned long long uq_cap;
+  unsigned long long* uq_slots;  // one slot counter for every scene's entries
   unsigned long long* error_word;
   double T0, T1;
   __device__ __forceinline__ long long n(int f) const { return (long long)pick(off, f)[n_scenes]; }
@@ -135,7 +139,7 @@ struct BatchProblem {
     const unsigned long long key = (f == 1 ? d.vf_pairs : d.ee_pairs)[local];
     store_interval_result((f == 1 ? d.vf_results : d.ee_results) + local, f, o, (long long)(key >> 32),
                           (long long)(key & 0xffffffffull));
-    scene_agg_record(aggs + s, f, key, o, uq, uq_cap,
+    scene_agg_record(aggs + s, f, key, o, uq, uq_cap, uq_slots,
                      ((unsigned long long)s << 40) | ((unsigned long long)(f - 1) << 39) | (unsigned long long)local);
   }
   __device__ __forceinline__ void invalid(int f, long long q, int, double t0, double t1) const {
@@ -224,6 +228,7 @@ int launch_batch_certify(const p2c_batch_scene* scenes, int n_scenes, double T0,
   prob.aggs = L.aggs;
   prob.uq = uq;
   prob.uq_cap = (unsigned long long)(uq_cap > 0 ? uq_cap : 0);
+  prob.uq_slots = L.uq_slots;
   prob.error_word = (unsigned long long*)&L.sc->stats.error_word;
   prob.T0 = T0;
   prob.T1 = T1;
@@ -269,3 +274,16 @@ int p2c_batch_certify(const p2c_batch_scene* scenes_dev, int32_t n_scenes, doubl
 }
 
 }  // extern "C"
+
+#ifdef P2C_ENGINE_PROFILE
+// Measurement build only: the engine phase clock of this file's kernels (see
+// certify_engine.cuh), read and cleared by the host.
+extern "C" int p2c_engine_profile_batch(unsigned long long* out16, int clear) {
+  if (cudaMemcpyFromSymbol(out16, p2c::g_engine_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return 2;
+  if (clear) {
+    static const unsigned long long zero[16] = {};
+    if (cudaMemcpyToSymbol(p2c::g_engine_prof, zero, sizeof(zero)) != cudaSuccess) return 2;
+  }
+  return 0;
+}
+#endif

@@ -236,3 +236,16 @@ int p2c_certify_census(const p2c_point_triangle* pt_dev, int64_t n_pt, const p2c
 }
 
 }  // extern "C"
+
+#ifdef P2C_ENGINE_PROFILE
+// Measurement build only: the engine phase clock of this file's kernels (see
+// certify_engine.cuh), read and cleared by the host.
+extern "C" int p2c_engine_profile_certify(unsigned long long* out16, int clear) {
+  if (cudaMemcpyFromSymbol(out16, p2c::g_engine_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return 2;
+  if (clear) {
+    static const unsigned long long zero[16] = {};
+    if (cudaMemcpyToSymbol(p2c::g_engine_prof, zero, sizeof(zero)) != cudaSuccess) return 2;
+  }
+  return 0;
+}
+#endif

@@ -75,6 +75,38 @@ struct EnginePools {
 
 constexpr int kMaxTreeDepth = 63;  // leaf keys need one bit below the deepest level
 
+// Phase clock of one warp iteration, compiled only with -DP2C_ENGINE_PROFILE
+// (a measurement build; the library is built without it): lane 0 of every
+// warp adds the SM clock cycles spent in each phase of the loop below to
+// g_engine_prof (0 fetch, 1 donation, 2 pool take, 3 idle wait, 4 distance
+// sample, 5 classify, 6 record, 7 move to the next node, 8 export,
+// 9 finalise, 10 budget check, 11 iterations).
+#ifdef P2C_ENGINE_PROFILE
+static __device__ unsigned long long g_engine_prof[16];
+#define P2C_PROF_DECL              \
+  unsigned long long prof_t = 0;   \
+  unsigned long long prof_acc[12]; \
+  for (int _k = 0; _k < 12; ++_k) prof_acc[_k] = 0ull;
+#define P2C_PROF_START() prof_t = clock64();
+#define P2C_PROF_MARK(k)                               \
+  {                                                    \
+    __syncwarp();                                      \
+    const unsigned long long _now = clock64();         \
+    prof_acc[k] += _now - prof_t;                      \
+    prof_t = _now;                                     \
+  }
+#define P2C_PROF_FLUSH()                                                               \
+  if ((threadIdx.x & 31) == 0)                                                         \
+    for (int _k = 0; _k < 12; ++_k) atomicAdd(&g_engine_prof[_k], prof_acc[_k]);
+#define P2C_PROF_COUNT(k) prof_acc[k] += 1ull;
+#else
+#define P2C_PROF_DECL
+#define P2C_PROF_START()
+#define P2C_PROF_MARK(k)
+#define P2C_PROF_FLUSH()
+#define P2C_PROF_COUNT(k)
+#endif
+
 __device__ __forceinline__ unsigned long long leaf_key(unsigned long long path, int depth) {
   return path | (1ull << (63 - depth));
 }
@@ -135,6 +167,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
   bool ok = true;
 
   auto queues_done = [&]() { return exhausted == 3u; };
+  P2C_PROF_DECL
 
   // Finish a tree: one result for query (f, q).
   auto finalize = [&](int f, long long q, const Outcome& o) {
@@ -170,6 +203,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
     return o;
   };
 
+  P2C_PROF_START()
   for (unsigned iter = 0;; ++iter) {
     if ((iter & 63u) == 0u && prm.budget_ns != 0ull) {
       int over = 0;
@@ -179,6 +213,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         break;
       }
     }
+    P2C_PROF_MARK(10)
     // ---- (A) new queries from the per-family queues -------------------------
     unsigned idle = __ballot_sync(FULL, slot < 0);
     if (idle != 0u && !queues_done()) {
@@ -244,6 +279,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         __syncwarp();
       }
     }
+    P2C_PROF_MARK(0)
     // ---- (B) donation inside the warp ---------------------------------------
     if (kDonate) {
       idle = __ballot_sync(FULL, slot < 0);
@@ -294,6 +330,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         }
       }
     }
+    P2C_PROF_MARK(1)
     // ---- (C) subtrees from the global pool ------------------------------------
     if (kExport) {
       idle = __ballot_sync(FULL, slot < 0);
@@ -379,6 +416,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         hungry = want;
       }
     }
+    P2C_PROF_MARK(2)
     const unsigned busy = __ballot_sync(FULL, slot >= 0);
     if (busy == 0u) {
       if (queues_done()) {
@@ -397,8 +435,10 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         __nanosleep(backoff);
         backoff = min(backoff * 2u, 512u);
       }
+      P2C_PROF_MARK(3)
       continue;
     }
+    P2C_PROF_COUNT(11)
     backoff = 256u;
     st.iters += 1;
     st.busy += (unsigned long long)__popc(busy);
@@ -417,6 +457,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
       if (phase == 0 || (phase == 2 && depth > 0)) st.nodes += 1;
       if (kCount) ops.add(phase == 2 ? 2 : 0);
     }
+    P2C_PROF_MARK(4)
     // ---- (F) classify: 0 none, 1 collision, 2 separation, 3 undecided ---------
     int leaf = 0;
     double toi = 0.0, margin = 0.0;
@@ -454,6 +495,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         }
       }
     }
+    P2C_PROF_MARK(5)
     // ---- (G) record leaves ------------------------------------------------------
     bool root_collision = false;
     if (leaf != 0) {
@@ -475,6 +517,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
       }
     }
     __syncwarp();
+    P2C_PROF_MARK(6)
     // ---- (H) after a leaf, move to the deepest pending right sibling ---------
     if (leaf != 0 && !root_collision) {
       const unsigned long long pend = pending_levels(path, donated, depth, sub_depth);
@@ -493,6 +536,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         phase = 2;
       }
     }
+    P2C_PROF_MARK(7)
     // ---- (I) export pending subtrees to hungry warps ---------------------------
     if (kExport) {
       if ((iter & 7u) == 0u) {
@@ -553,6 +597,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         __syncwarp();
       }
     }
+    P2C_PROF_MARK(8)
     // ---- (J) a finished lane leaves its tree; the last unit finalises it ------
     unsigned freed = 0u;
     if (root_collision) {
@@ -585,7 +630,9 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
     }
     free_mask |= __reduce_or_sync(FULL, freed);
     __syncwarp();
+    P2C_PROF_MARK(9)
   }
+  P2C_PROF_FLUSH()
   if (kExport && hungry && lane == 0) atomicAdd(&es->hungry.v, ~0ull);
   if (kCount) st.ops += ops.n;
   return ok;

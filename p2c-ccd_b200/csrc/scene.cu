@@ -46,7 +46,7 @@ struct PairProblem {
   __device__ __forceinline__ void finish(int fam, long long q, const Outcome& o) const {
     const unsigned long long key = pick(sp, fam).pairs[q];
     store_interval_result(pick(out, fam) + q, fam, o, (long long)(key >> 32), (long long)(key & 0xffffffffull));
-    scene_agg_record(agg, fam, key, o, undecided_queue, undecided_cap,
+    scene_agg_record(agg, fam, key, o, undecided_queue, undecided_cap, nullptr,
                      ((unsigned long long)(fam - 1) << 63) | (unsigned long long)q);
   }
   __device__ __forceinline__ void invalid(int fam, long long q, int bad, double t0, double t1) const {
@@ -228,3 +228,16 @@ int p2c_scene_materialize(const p2c_scene* scene, const uint64_t* vf_pairs_dev, 
 }
 
 }  // extern "C"
+
+#ifdef P2C_ENGINE_PROFILE
+// Measurement build only: the engine phase clock of this file's kernels (see
+// certify_engine.cuh), read and cleared by the host.
+extern "C" int p2c_engine_profile_scene(unsigned long long* out16, int clear) {
+  if (cudaMemcpyFromSymbol(out16, p2c::g_engine_prof, 16 * sizeof(unsigned long long)) != cudaSuccess) return 2;
+  if (clear) {
+    static const unsigned long long zero[16] = {};
+    if (cudaMemcpyToSymbol(p2c::g_engine_prof, zero, sizeof(zero)) != cudaSuccess) return 2;
+  }
+  return 0;
+}
+#endif

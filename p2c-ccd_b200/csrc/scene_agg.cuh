@@ -14,6 +14,7 @@ struct SceneAgg {
   unsigned int any_undecided[2];
   unsigned long long collisions, separations, undecided, queued;
   unsigned long long n_certified[2];
+  unsigned int dropped;  // an undecided entry of this scene found the queue full
 };
 
 __device__ __forceinline__ void scene_agg_init(SceneAgg& a) {
@@ -25,12 +26,17 @@ __device__ __forceinline__ void scene_agg_init(SceneAgg& a) {
 
 // One finished certificate of family fam (1: VF, 2: EE) with pair key `key`;
 // an undecided one is appended to the undecided (fallback-replay) queue as
-// `entry` when the queue exists.
+// `entry` when the queue exists.  Queue slots come from `uq_slots`, the
+// counter of everything written to that queue: a queue shared by several
+// scenes passes one launch-wide counter (each scene still counts its own
+// entries in agg->queued); nullptr means the queue is this scene's alone and
+// agg->queued is the slot counter.  An entry past uq_cap is counted but not
+// written, and marks the scene (error bit 8 of its summary).
 // Lanes that finish together add their counts with one atomic per (scene,
 // status); a minimum is only written when it can still decrease.
 __device__ __forceinline__ void scene_agg_record(SceneAgg* agg, int fam, unsigned long long key, const Outcome& o,
                                                  unsigned long long* uq, unsigned long long uq_cap,
-                                                 unsigned long long entry) {
+                                                 unsigned long long* uq_slots, unsigned long long entry) {
   const int f = fam - 1;
   const unsigned act = __activemask();
   const unsigned m = __match_any_sync(act, (reinterpret_cast<unsigned long long>(agg) << 2) | o.status);
@@ -49,8 +55,10 @@ __device__ __forceinline__ void scene_agg_record(SceneAgg* agg, int fam, unsigne
     if (agg->any_undecided[f] == 0u) atomicExch(&agg->any_undecided[f], 1u);
     if (leader) atomicAdd(&agg->undecided, n);
     if (uq != nullptr) {
-      const unsigned long long slot = atomicAdd(&agg->queued, 1ull);
+      const unsigned long long slot = atomicAdd(uq_slots != nullptr ? uq_slots : &agg->queued, 1ull);
+      if (uq_slots != nullptr) atomicAdd(&agg->queued, 1ull);
       if (slot < uq_cap) uq[slot] = entry;
+      else atomicExch(&agg->dropped, 1u);
     }
   }
 }
@@ -96,7 +104,7 @@ __device__ __forceinline__ void scene_summary_fields(const SceneAgg& a, unsigned
   summary->vf_certified = (unsigned long long)n_vf;
   summary->ee_certified = (unsigned long long)n_ee;
   summary->undecided_queued = a.queued;
-  summary->error_word = error_word;
+  summary->error_word = error_word | (a.dropped ? 8ull : 0ull);
   if (a.coll_key != ~0ull) return;
   p2c_query_certificate q{};
   q.witness_id_a = -1;

@@ -27,7 +27,7 @@ import torch
 from . import _lib
 from .certify import CertConfig, _stream_ptr
 from .records import INTERVAL_RESULT_DTYPE, QUERY_CERTIFICATE_DTYPE
-from .scene import SUMMARY_DTYPE, SceneStruct
+from .scene import ERR_UNDECIDED_FULL, SUMMARY_DTYPE, SceneStruct, UndecidedOverflow
 
 BATCH_SCENE_DTYPE = np.dtype([
     ("v_t0", "<u8"), ("v_t1", "<u8"), ("faces", "<u8"), ("edges", "<u8"), ("vf_pairs", "<u8"),
@@ -43,6 +43,15 @@ def scene_row(st, vf_pairs: int, ee_pairs: int, vf_cap: int, ee_cap: int, counts
     """One p2c_batch_scene row from a SceneStruct and the scene's buffers."""
     return (st.v_t0, st.v_t1, st.faces, st.edges, vf_pairs, ee_pairs, vf_cap, ee_cap, counts, vf_results,
             ee_results, st.v_obj, st.f_obj, st.e_obj, st.nv, st.nf, st.ne, st.thickness, st.exclude_self, st.n_obj)
+
+
+def decode_batch_undecided(raw: np.ndarray) -> np.ndarray:
+    """Entries (scene << 40 | (family - 1) << 39 | position) of a batch
+    undecided queue as int64 rows (scene, family 1/2, pair position)."""
+    u = np.asarray(raw).view(np.uint64)
+    return np.stack([(u >> np.uint64(40)).astype(np.int64),
+                     ((u >> np.uint64(39)) & np.uint64(1)).astype(np.int64) + 1,
+                     (u & np.uint64((1 << 39) - 1)).astype(np.int64)], 1).reshape(-1, 3)
 
 
 class BatchTuning(ctypes.Structure):
@@ -133,13 +142,16 @@ class BatchPipeline:
         self.summaries = torch.zeros((self.n, SUMMARY_DTYPE.itemsize), dtype=torch.uint8, device=d)
         self.cert_ws = torch.empty(int(self.lib.p2c_batch_certify_workspace_bytes(self.n)), dtype=torch.uint8,
                                    device=d)
-        self.undecided_capacity = int(undecided_capacity)
-        self.undecided_queue = torch.empty(max(1, self.undecided_capacity), dtype=torch.int64, device=d)
-        self.graph = None
+        self._alloc_undecided(undecided_capacity)
         # first sizing of the pair buffers: about one candidate per triangle
         self._alloc([max(1024, x) for x in nf], [max(1024, 2 * x) for x in nf])
 
     # -- buffers ---------------------------------------------------------
+    def _alloc_undecided(self, capacity: int) -> None:
+        self.undecided_capacity = max(1, int(capacity))
+        self.undecided_queue = torch.empty(self.undecided_capacity, dtype=torch.int64, device=self.device)
+        self.graph = None
+
     def _alloc(self, vf_caps: list[int], ee_caps: list[int]) -> None:
         d = self.device
         self.vf_caps = [max(1, int(c)) for c in vf_caps]
@@ -234,7 +246,8 @@ class BatchPipeline:
         return self.counts.cpu().numpy()
 
     def step_checked(self, max_retries: int = 3) -> list[dict]:
-        """Run a step; grow the pair buffers of scenes that overflowed and re-run."""
+        """Run a step; grow the pair buffers of scenes that overflowed, or
+        the shared undecided queue, and re-run."""
         for _ in range(max_retries + 1):
             self.step()
             c = self.read_counts()
@@ -246,12 +259,16 @@ class BatchPipeline:
                 summ = self.read_summaries()
                 if any(s["error_word"] & 1 for s in summ):
                     raise _lib.P2CError("certification exceeded the device time budget (P2C_DEVICE_BUDGET_MS)")
+                queued = sum(s["undecided_queued"] for s in summ)
+                if queued > self.undecided_capacity or any(s["error_word"] & ERR_UNDECIDED_FULL for s in summ):
+                    self._alloc_undecided(int(queued * 1.25) + 1024)
+                    continue
                 return summ
             self._alloc([max(cap, int(n * 1.25) + 1024) if o else cap
                          for cap, n, o in zip(self.vf_caps, c[:, 0], over_vf)],
                         [max(cap, int(n * 1.25) + 1024) if o else cap
                          for cap, n, o in zip(self.ee_caps, c[:, 1], over_ee)])
-        raise _lib.P2CError("pair buffers kept overflowing")
+        raise _lib.P2CError("pair buffers or the undecided queue kept overflowing")
 
     def fit_capacities(self, margin: float = 1.25, slack: int = 256) -> None:
         """Resize every scene's pair buffers to its last candidate count x
@@ -298,6 +315,16 @@ class BatchPipeline:
             _stream_ptr(self.device)))
         return (a[:n_vf].cpu().numpy().view(POINT_TRIANGLE_DTYPE).reshape(-1),
                 b[:n_ee].cpu().numpy().view(EDGE_EDGE_DTYPE).reshape(-1))
+
+    def undecided_entries(self) -> np.ndarray:
+        """The step's undecided (fallback-replay) entries of all scenes as
+        (scene, family, pair position) rows, in queue order.  Raises
+        ``UndecidedOverflow`` when the shared queue was too small."""
+        summ = self.read_summaries()
+        n = sum(s["undecided_queued"] for s in summ)
+        if n > self.undecided_capacity or any(s["error_word"] & ERR_UNDECIDED_FULL for s in summ):
+            raise UndecidedOverflow(f"undecided queue overflow: {n} entries, capacity {self.undecided_capacity}")
+        return decode_batch_undecided(self.undecided_queue[:n].cpu().numpy())
 
     def certified_per_step(self) -> int:
         s = self.read_summaries()

@@ -35,7 +35,13 @@ SUMMARY_DTYPE = np.dtype({
     "itemsize": 112,
 })
 
-ERR_BUDGET, ERR_OVERFLOW, ERR_GEOMETRY = 1, 2, 4
+ERR_BUDGET, ERR_OVERFLOW, ERR_GEOMETRY, ERR_UNDECIDED_FULL = 1, 2, 4, 8
+
+
+class UndecidedOverflow(_lib.P2CError):
+    """The undecided (fallback-replay) queue was too small: entries were
+    counted but not written, so a replay list read from it would be
+    incomplete.  ``step_checked`` re-runs with a larger queue instead."""
 
 
 @dataclass
@@ -91,8 +97,7 @@ class ScenePipeline:
         self.counts = torch.zeros(4, dtype=torch.int64, device=d)
         self.summary = torch.zeros(SUMMARY_DTYPE.itemsize, dtype=torch.uint8, device=d)
         self.cert_ws = torch.empty(int(self.lib.p2c_scene_certify_workspace_bytes()), dtype=torch.uint8, device=d)
-        self.undecided_capacity = int(undecided_capacity)
-        self.undecided_queue = torch.empty(max(1, self.undecided_capacity), dtype=torch.int64, device=d)
+        self._alloc_undecided(undecided_capacity)
         if narrow not in ("certify", "anyhit"):
             raise ValueError("narrow must be 'certify' or 'anyhit'")
         self.narrow = narrow
@@ -103,6 +108,11 @@ class ScenePipeline:
         self._alloc(vf_capacity, ee_capacity)
 
     # -- buffers ---------------------------------------------------------
+    def _alloc_undecided(self, capacity: int) -> None:
+        self.undecided_capacity = max(1, int(capacity))
+        self.undecided_queue = torch.empty(self.undecided_capacity, dtype=torch.int64, device=self.device)
+        self.graph = None
+
     def _refresh_struct(self):
         s = self._struct
         s.v_t0, s.v_t1 = self.v_t0.data_ptr(), self.v_t1.data_ptr()
@@ -198,8 +208,10 @@ class ScenePipeline:
         return int(c[0]), int(c[1]), int(c[2])
 
     def step_checked(self, max_retries: int = 3) -> dict:
-        """Run a step, grow the pair buffers and re-run if they overflowed;
-        raise on non-finite geometry or an exhausted time budget."""
+        """Run a step; grow the pair buffers or the undecided queue and re-run
+        if they overflowed; raise on non-finite geometry or an exhausted time
+        budget.  Every returned step certified every candidate and queued
+        every undecided one."""
         for _ in range(max_retries + 1):
             self.step()
             n_vf, n_ee, err = self.read_counts()
@@ -209,9 +221,12 @@ class ScenePipeline:
                 summ = self.read_summary() if self.narrow == "certify" else self.read_anyhit_summary()
                 if summ["error_word"] & ERR_BUDGET:
                     raise _lib.P2CError("certification exceeded the device time budget (P2C_DEVICE_BUDGET_MS)")
+                if self.narrow == "certify" and summ["error_word"] & ERR_UNDECIDED_FULL:
+                    self._alloc_undecided(int(summ["undecided_queued"] * 1.25) + 1024)
+                    continue
                 return summ
             self._alloc(max(self.vf_cap, int(n_vf * 1.25) + 1024), max(self.ee_cap, int(n_ee * 1.25) + 1024))
-        raise _lib.P2CError("pair buffers kept overflowing")
+        raise _lib.P2CError("pair buffers or the undecided queue kept overflowing")
 
     def read_anyhit_summary(self) -> dict:
         """Both families' any-hit summaries plus their sums."""
@@ -267,6 +282,11 @@ class ScenePipeline:
 
     @property
     def undecided_entries(self) -> np.ndarray:
-        """Undecided (fallback-replay) queue: (family - 1) << 63 | pair position."""
-        n = min(self.read_summary()["undecided_queued"], self.undecided_capacity)
+        """Undecided (fallback-replay) queue: (family - 1) << 63 | pair position.
+        Raises ``UndecidedOverflow`` when the queue was too small for the
+        step (the list would miss undecided candidates)."""
+        summ = self.read_summary()
+        n = summ["undecided_queued"]
+        if summ["error_word"] & ERR_UNDECIDED_FULL or n > self.undecided_capacity:
+            raise UndecidedOverflow(f"undecided queue overflow: {n} entries, capacity {self.undecided_capacity}")
         return self.undecided_queue[:n].cpu().numpy().view(np.uint64)

@@ -62,16 +62,47 @@ def test_batch_matches_single_scene_and_oracle(cuda_device, oracle_mod, depth):
             assert st.sum() == 0
             assert np.array_equal(_bytes(cpu), _bytes(res)), (i, kind)
         total_undecided += summ[i]["undecided"]
-    # undecided queue: (scene << 40 | family << 39 | position), one entry per undecided certificate
-    n_q = min(sum(x["undecided_queued"] for x in summ), bp.undecided_capacity)
-    assert n_q == total_undecided
-    entries = bp.undecided_queue[:n_q].cpu().numpy().view(np.uint64)
-    for e in entries[:200]:
-        sc, fam, pos = int(e >> np.uint64(40)), int((e >> np.uint64(39)) & np.uint64(1)), int(e & np.uint64((1 << 39) - 1))
-        res = bp.results(sc)[fam]
-        assert res[pos]["status"] == 2
+    # undecided queue: (scene << 40 | family << 39 | position), one entry per
+    # undecided certificate of every scene, none twice (one queue shared by all scenes)
+    assert sum(x["undecided_queued"] for x in summ) == total_undecided
+    got = {tuple(int(v) for v in row) for row in bp.undecided_entries()}
+    assert len(got) == total_undecided
+    assert got == _undecided_set(bp)
     if depth == 4:
-        assert total_undecided > 0
+        assert sum(1 for x in summ if x["undecided"] > 0) >= 2  # several scenes share the queue
+
+
+def _undecided_set(bp):
+    out = set()
+    for i in range(bp.n):
+        for fam, res in ((1, bp.results(i)[0]), (2, bp.results(i)[1])):
+            out |= {(i, fam, int(p)) for p in np.nonzero(res["status"] == 2)[0]}
+    return out
+
+
+def test_batch_undecided_queue_overflow_reruns(cuda_device):
+    """A shared undecided queue smaller than the step's undecided
+    certificates: the device marks the scenes whose entries were dropped
+    (error bit 8), reading the queue raises, and step_checked re-runs with a
+    larger queue so that the replay list is complete."""
+    from p2cccd_b200.batch import BatchPipeline
+    from p2cccd_b200.certify import CertConfig
+    from p2cccd_b200.scene import ERR_UNDECIDED_FULL, UndecidedOverflow
+
+    cfg = CertConfig(1e-2, 1e-6, 4)  # coarse: many undecided certificates
+    bp = BatchPipeline(_small_batch(), cuda_device, config=cfg, undecided_capacity=8)
+    bp.step()
+    summ = bp.read_summaries()
+    queued = sum(x["undecided_queued"] for x in summ)
+    assert queued > 8
+    assert any(x["error_word"] & ERR_UNDECIDED_FULL for x in summ)
+    with pytest.raises(UndecidedOverflow):
+        bp.undecided_entries()
+    summ = bp.step_checked()
+    assert bp.undecided_capacity >= queued
+    assert not any(x["error_word"] & ERR_UNDECIDED_FULL for x in summ)
+    got = {tuple(int(v) for v in row) for row in bp.undecided_entries()}
+    assert got == _undecided_set(bp) and len(got) == queued
 
 
 def test_batch_autotune_keeps_results(cuda_device, tmp_path):

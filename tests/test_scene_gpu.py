@@ -175,6 +175,19 @@ def test_undecided_queue_and_invalid_geometry(cuda_device, oracle_mod):
                     [(1 << 63) | int(i) for i in np.nonzero(ee_res["status"] == 2)[0]])
     assert summ["undecided"] == len(expect) > 0
     np.testing.assert_array_equal(np.sort(pipe.undecided_entries), np.array(expect, dtype=np.uint64))
+    # a queue too small for the step: entries dropped, flagged, and the
+    # checked step re-runs with a larger queue
+    from p2cccd_b200.scene import ERR_UNDECIDED_FULL, UndecidedOverflow
+
+    tiny = ScenePipeline(s, cuda_device, exclude_self=True, config=cfg, undecided_capacity=4)
+    tiny.step()
+    raw = tiny.read_summary()
+    assert raw["undecided_queued"] == len(expect) and raw["error_word"] & ERR_UNDECIDED_FULL
+    with pytest.raises(UndecidedOverflow):
+        tiny.undecided_entries
+    again = tiny.step_checked()
+    assert again == summ and tiny.undecided_capacity >= len(expect)
+    np.testing.assert_array_equal(np.sort(tiny.undecided_entries), np.array(expect, dtype=np.uint64))
     bad = dict(s)
     bad["v_t1"] = s["v_t1"].copy()
     bad["v_t1"][5, 1] = np.nan
