@@ -9,6 +9,7 @@ accept / reject verdict on a set of invalid benchmark rows.
 from __future__ import annotations
 
 import json
+import os
 import sys
 import tempfile
 from pathlib import Path
@@ -79,4 +80,4 @@ def main(reference: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    main(sys.argv[1] if len(sys.argv) > 1 else os.environ.get("P2C_REFERENCE_ROOT", "/root/reference"))
