@@ -272,9 +272,26 @@ __device__ __forceinline__ unsigned long long pending_levels(unsigned long long 
 }
 
 // Endpoints of the node (path, depth) under root [T0, T1], recomputed with the
-// recursion's own roundings.
+// recursion's own roundings.  Under the root [0, 1] every bisection is exact:
+// the endpoints at depth d are multiples of 2^-d, so a + b needs at most d + 1
+// significant bits and 0.5 * (a + b) is exact for d <= 52.  The node at depth
+// d with path bits k (its first d levels read as a binary number) is then
+// [k * 2^-d, (k + 1) * 2^-d], bit for bit what the recursion computes, without
+// the d dependent steps.
 __device__ __forceinline__ void replay(double T0, double T1, unsigned long long path, int depth,
                                        double& a, double& b) {
+  if (T0 == 0.0 && T1 == 1.0 && depth <= 52) {
+    if (depth <= 0) {
+      a = 0.0;
+      b = 1.0;
+      return;
+    }
+    const unsigned long long k = path >> (64 - depth);
+    const double u = __longlong_as_double((long long)(1023 - depth) << 52);  // 2^-depth
+    a = __dmul_rn(__ull2double_rn(k), u);
+    b = __dmul_rn(__ull2double_rn(k + 1ull), u);
+    return;
+  }
   a = T0;
   b = T1;
   for (int l = 1; l <= depth; ++l) {

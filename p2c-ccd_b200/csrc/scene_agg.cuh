@@ -42,13 +42,16 @@ __device__ __forceinline__ void scene_agg_record(SceneAgg* agg, int fam, unsigne
   const unsigned m = __match_any_sync(act, (reinterpret_cast<unsigned long long>(agg) << 2) | o.status);
   const bool leader = (int)(threadIdx.x & 31) == __ffs((int)m) - 1;
   const unsigned long long n = (unsigned long long)__popc(m);
+  // The minima only decrease, so a stale (L1-cached) copy is an upper bound
+  // of the current value: skipping the atomic when the new value is not below
+  // it never loses a minimum, and the read rarely leaves the SM.
   if (o.status == P2C_STATUS_COLLISION) {
     const unsigned long long k = ((unsigned long long)f << 63) | key;
-    if (k < *reinterpret_cast<volatile unsigned long long*>(&agg->coll_key)) atomicMin(&agg->coll_key, k);
+    if (k < __ldca(&agg->coll_key)) atomicMin(&agg->coll_key, k);
     if (leader) atomicAdd(&agg->collisions, n);
   } else if (o.status == P2C_STATUS_SEPARATION) {
     const unsigned long long mb = (unsigned long long)__double_as_longlong(o.margin);
-    if (mb < *reinterpret_cast<volatile unsigned long long*>(&agg->margin_bits)) atomicMin(&agg->margin_bits, mb);
+    if (mb < __ldca(&agg->margin_bits)) atomicMin(&agg->margin_bits, mb);
     if (agg->any_sep[f] == 0u) atomicExch(&agg->any_sep[f], 1u);
     if (leader) atomicAdd(&agg->separations, n);
   } else {
