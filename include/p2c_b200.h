@@ -441,6 +441,41 @@ int p2c_group_anyhit(const p2c_scene* scene, int family, const uint64_t* pairs_d
                      p2c_anyhit_summary* summary_dev, void* workspace_dev, size_t workspace_bytes,
                      void* stream);
 
+/* The seeded scheduler stub: scores_dev[i] = a uniform score in [0, 1) of
+ * (seed, family, pairs_dev[i]) for i < min(*count_dev, cap) (count_dev may be
+ * NULL: all cap entries), 0 beyond.  A score depends only on the candidate's
+ * identity (family and pair key), so a candidate is ranked the same alone and
+ * in any batch.  It stands in for the learned scheduler's output (the
+ * reference tool's "random" policy, ScoreCandidate
+ * tools/scene_object_envelope_native_ti_walltime.cpp:1102-1106, plays the
+ * same role); callers with a scheduler pass its scores instead. */
+int p2c_stub_scores(const uint64_t* pairs_dev, const uint64_t* count_dev, int64_t cap, int family, uint64_t seed,
+                    double* scores_dev, void* stream);
+
+/* Workspace of p2c_batch_anyhit for the scenes of a host table. */
+size_t p2c_batch_anyhit_workspace_bytes(const p2c_batch_scene* scenes_host, int32_t n_scenes, uint32_t family_mask);
+
+/* p2c_group_anyhit for every (scene, family) of a batch in one launch
+ * sequence (about twenty launches whatever the number of scenes): groups are
+ * the object pairs of one scene and one family, so every scene gets exactly
+ * what p2c_group_anyhit gives it alone with the same scores and top_k.
+ * Candidates are each scene's first min(counts[f], cap) pairs (read on the
+ * device, so this can follow p2c_batch_candidates without a host sync).
+ * Scores: scores_dev (device array of 2 * n_scenes device pointers, entry
+ * 2 * s + family - 1 positional over that list's capacity), or, when NULL,
+ * the scheduler stub of p2c_stub_scores with seed seeds_dev[s] (seeds_dev
+ * NULL: seed 0).  Outputs (each optional): summaries_dev[2 * s + family - 1]
+ * (p2c_anyhit_summary of that scene and family); group_detected_dev, one byte
+ * per group, and evaluated_dev / hit_dev, one byte per candidate slot, in the
+ * batch's index spaces (family-major, then scene: segment k = (family - 1) *
+ * n_scenes + s holds that list's capacity of candidate slots and n_obj^2
+ * groups).  scenes_host is read on the host for sizes (caps, n_obj). */
+int p2c_batch_anyhit(const p2c_batch_scene* scenes_host, const p2c_batch_scene* scenes_dev, int32_t n_scenes,
+                     uint32_t family_mask, const double* const* scores_dev, const uint64_t* seeds_dev, int64_t top_k,
+                     double interval_t0, double interval_t1, const p2c_cert_config* config,
+                     p2c_anyhit_summary* summaries_dev, uint8_t* group_detected_dev, uint8_t* evaluated_dev,
+                     uint8_t* hit_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
+
 /* ---- proxy scenes: patch-level candidates with time slabs ---------------- */
 /* The proxy primitives of a built ProxyScene (rt_candidate/proxy_scene.h:29-46)
  * as device arrays; proxy i has proxy_id i. */

@@ -51,3 +51,21 @@ __device__ __forceinline__ bool load_pair(const ScenePairs& s, int family, unsig
 }
 
 }  // namespace p2c
+
+namespace p2c {
+
+// The seeded scheduler stub: a uniform score in [0, 1) from (seed, family,
+// pair key), mixed by the splitmix64 finaliser (Steele, Lea and Flood,
+// "Fast splittable pseudorandom number generators", OOPSLA 2014).  It depends
+// only on the candidate's identity, so a candidate scores the same alone and
+// in any batch, whatever its position in the candidate list.
+__host__ __device__ inline double stub_score(unsigned long long seed, int family, unsigned long long key) {
+  unsigned long long x = seed ^ (key * 0x9e3779b97f4a7c15ull) ^ ((unsigned long long)family << 62);
+  x += 0x9e3779b97f4a7c15ull;
+  x = (x ^ (x >> 30)) * 0xbf58476d1ce4e5b9ull;
+  x = (x ^ (x >> 27)) * 0x94d049bb133111ebull;
+  x ^= x >> 31;
+  return (double)(x >> 11) * (1.0 / 9007199254740992.0);
+}
+
+}  // namespace p2c

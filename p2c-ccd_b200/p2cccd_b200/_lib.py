@@ -75,6 +75,11 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_group_anyhit": (_int, [_c_void_p, _int, _c_void_p, _i64, _c_void_p, _c_void_p, _i64, _f64, _f64,
                                 ctypes.POINTER(CertConfig), _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                 _c_void_p, _c_void_p, _size, _c_void_p]),
+    "p2c_stub_scores": (_int, [_c_void_p, _c_void_p, _i64, _int, ctypes.c_uint64, _c_void_p, _c_void_p]),
+    "p2c_batch_anyhit_workspace_bytes": (_size, [_c_void_p, ctypes.c_int32, ctypes.c_uint32]),
+    "p2c_batch_anyhit": (_int, [_c_void_p, _c_void_p, ctypes.c_int32, ctypes.c_uint32, _c_void_p, _c_void_p, _i64,
+                                _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p, _c_void_p, _c_void_p, _c_void_p,
+                                _c_void_p, _size, _c_void_p]),
     "p2c_refinement_children_workspace_bytes": (_size, [_i64]),
     "p2c_refinement_children": (_int, [_i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_uint16, _f64,
                                        ctypes.c_uint64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,

@@ -73,7 +73,9 @@ class ScenePipeline:
         narrow = "anyhit": candidates are grouped by object pair and run
         through the scheduled any-hit with fallback replay
         (p2c_group_anyhit) with proposal size top_k and priority scores from
-        a seeded scheduler stub (uniform random, positional per candidate)."""
+        the seeded scheduler stub (p2c_stub_scores: a uniform score per
+        candidate identity, so a candidate ranks the same here and in a
+        served batch)."""
         if isinstance(scene, dict):
             scene = SceneArrays.from_dict(scene)
         self.lib = _lib.load()
@@ -136,9 +138,8 @@ class ScenePipeline:
         if self.narrow == "anyhit":
             from .anyhit import GroupAnyHit
 
-            gen = torch.Generator(device=d).manual_seed(self.scheduler_seed)
-            self.vf_scores = torch.rand(self.vf_cap, dtype=torch.float64, device=d, generator=gen)
-            self.ee_scores = torch.rand(self.ee_cap, dtype=torch.float64, device=d, generator=gen)
+            self.vf_scores = torch.zeros(self.vf_cap, dtype=torch.float64, device=d)
+            self.ee_scores = torch.zeros(self.ee_cap, dtype=torch.float64, device=d)
             self.anyhit_vf = GroupAnyHit(self._struct, self.n_obj, "vf", self.vf_cap, d)
             self.anyhit_ee = GroupAnyHit(self._struct, self.n_obj, "ee", self.ee_cap, d)
 
@@ -165,7 +166,14 @@ class ScenePipeline:
             self.undecided_capacity, self.summary.data_ptr(), self.cert_ws.data_ptr(), self.cert_ws.numel(), stream))
 
     def anyhit(self) -> None:
-        """Scheduled any-hit with fallback replay of both families (async)."""
+        """Scheduled any-hit with fallback replay of both families (async),
+        scores from the scheduler stub."""
+        from .anyhit import stub_scores
+
+        if self.family_mask & 1:
+            stub_scores(self.vf_pairs, self.counts[0:1], 1, self.scheduler_seed, self.vf_scores)
+        if self.family_mask & 2:
+            stub_scores(self.ee_pairs, self.counts[1:2], 2, self.scheduler_seed, self.ee_scores)
         if self.family_mask & 1:
             self.anyhit_vf.run(self.vf_pairs, self.counts[0:1], self.vf_scores, self.top_k, self.config,
                                self.interval)
