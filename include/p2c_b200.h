@@ -476,6 +476,115 @@ int p2c_batch_anyhit(const p2c_batch_scene* scenes_host, const p2c_batch_scene* 
                      p2c_anyhit_summary* summaries_dev, uint8_t* group_detected_dev, uint8_t* evaluated_dev,
                      uint8_t* hit_dev, void* workspace_dev, size_t workspace_bytes, void* stream);
 
+/* ---- serving: continuous batching of CCD steps on one GPU ---------------- */
+/* A server keeps registered meshes (topology, object ids) resident on its
+ * device together with their candidate state (pair capacities fitted to the
+ * last step), and one device arena of memory_budget bytes allocated at
+ * creation.  Requests are CCD steps of a registered mesh (the vertex
+ * trajectories of one step, host memory).  p2c_serve_poll retires finished
+ * groups and admits waiting requests, in admission order, into free slots:
+ * the requests admitted together form a group on the slot's own stream
+ * (trajectories in; candidates of every request in one p2c_batch_candidates
+ * sequence; then either the certificates of every candidate, one
+ * p2c_batch_certify launch, or the scheduled any-hit with fallback replay of
+ * every request, one p2c_batch_anyhit sequence; summaries out), as long as
+ * the group's memory fits a free range of the arena.  Groups on different
+ * slots overlap on the device.  A request whose candidates outgrew its
+ * buffers (or, certifying every candidate, the undecided queue) is re-run
+ * with larger ones, so every result is the complete answer for its step: the
+ * one the step gets alone.  The reference has no serving layer; the
+ * ownership model of each step is RunCudaBatch's (certificate_cuda.cu:456-552:
+ * host arrays in, host results out) with device memory held across steps.
+ * One host thread drives a server (the calls are not re-entrant). */
+#define P2C_SERVE_CERTIFY 0  /* certificates of every candidate */
+#define P2C_SERVE_ANYHIT 1   /* scheduled any-hit with fallback replay per object-pair group */
+
+typedef struct p2c_serve_config {
+  int32_t slots;              /* groups in flight (one CUDA stream each), >= 1 */
+  int32_t max_group;          /* requests admitted into one group, >= 1 */
+  int32_t narrow;             /* P2C_SERVE_CERTIFY or P2C_SERVE_ANYHIT */
+  int32_t top_k;              /* any-hit proposals per group (RunScheduledAnyHitRows' proposal_top_k) */
+  int64_t memory_budget;      /* device arena bytes; 0: half the free device memory at creation */
+  int64_t undecided_capacity; /* first size of a group's undecided queue (certify mode), grows on overflow */
+  p2c_cert_config cert;       /* CertificateEngineConfig of every certificate */
+  double interval_t0, interval_t1;
+} p2c_serve_config;
+
+typedef struct p2c_serve p2c_serve;  /* opaque */
+
+/* A mesh: host arrays copied to the device at registration. */
+typedef struct p2c_serve_mesh {
+  const int32_t* faces;  /* nf x 3 */
+  const int32_t* edges;  /* ne x 2 */
+  const int32_t* v_obj;  /* nv */
+  const int32_t* f_obj;  /* nf */
+  const int32_t* e_obj;  /* ne */
+  int64_t nv, nf, ne;
+  int32_t n_obj;          /* object ids < n_obj; candidate groups are object pairs */
+  int32_t exclude_self;   /* 1: no candidates between primitives of one object */
+  double thickness;
+  int64_t vf_capacity, ee_capacity;  /* first pair capacities (0: from the face count) */
+} p2c_serve_mesh;
+
+/* A CCD step.  v_t0 / v_t1 (nv x 3 doubles, host memory; page-locked memory
+ * lets the copies overlap) must stay valid until the request's result is
+ * returned.  Optional host outputs, filled before the result is returned:
+ * vf_results / ee_results (certify mode: the certificates of the first
+ * results_cap candidates of each list), undecided (certify mode: (family -
+ * 1) << 63 | pair position of each undecided certificate, the fallback-replay
+ * list, up to undecided_cap entries), group_detected (any-hit mode: n_obj^2
+ * bytes for the VF groups then n_obj^2 for the EE groups, index lo * n_obj +
+ * hi, up to groups_cap bytes).  seed is the scheduler stub's seed (any-hit). */
+typedef struct p2c_serve_request {
+  int32_t mesh_id;
+  int32_t pad;
+  const double* v_t0;
+  const double* v_t1;
+  uint64_t seed;
+  p2c_interval_result* vf_results;
+  p2c_interval_result* ee_results;
+  int64_t results_cap;
+  uint64_t* undecided;
+  int64_t undecided_cap;
+  uint8_t* group_detected;
+  int64_t groups_cap;
+} p2c_serve_request;
+
+typedef struct p2c_serve_result {
+  int64_t request_id;
+  int32_t status;        /* P2C_OK, or the error code that failed this request (p2c_last_error) */
+  int32_t reruns;        /* re-runs after a buffer overflow */
+  double latency_ms;     /* device clock: admission to the completion of its group */
+  uint64_t vf_candidates, ee_candidates;
+  uint64_t undecided_entries;        /* certify mode: entries of its fallback-replay list */
+  uint64_t truncated;                /* bits: 1 results, 2 undecided list, 4 group decisions beyond the caps */
+  p2c_scene_summary certify;         /* certify mode: the Evaluate reduction of its candidates */
+  p2c_anyhit_summary anyhit[2];      /* any-hit mode: VF and EE summaries */
+} p2c_serve_result;
+
+typedef struct p2c_serve_stats {
+  uint64_t admitted, completed, failed, groups, reruns;
+  uint64_t pending, in_flight;
+  uint64_t candidates;       /* candidates of completed requests */
+  uint64_t calls;            /* certificates the procedure called (certify: all candidates) */
+  uint64_t arena_bytes, arena_in_use, arena_peak;
+} p2c_serve_stats;
+
+/* Create a server on the current device (allocates its arena, streams and
+ * events); *out receives the handle. */
+int p2c_serve_create(const p2c_serve_config* config, p2c_serve** out);
+/* Wait for groups in flight, then free everything the server holds. */
+int p2c_serve_destroy(p2c_serve* server);
+/* Copy a mesh to the device; *mesh_id receives its id. */
+int p2c_serve_register_mesh(p2c_serve* server, const p2c_serve_mesh* mesh, int32_t* mesh_id);
+/* A request arrives: it waits for admission (the next poll).  Its arrival is
+ * stamped on the device clock now; *request_id receives its id. */
+int p2c_serve_admit(p2c_serve* server, const p2c_serve_request* request, int64_t* request_id);
+/* Retire finished groups, launch waiting requests into free slots, and
+ * return up to max_results finished requests (the rest at later polls). */
+int p2c_serve_poll(p2c_serve* server, p2c_serve_result* results, int32_t max_results, int32_t* n_results);
+int p2c_serve_read_stats(p2c_serve* server, p2c_serve_stats* stats);
+
 /* ---- proxy scenes: patch-level candidates with time slabs ---------------- */
 /* The proxy primitives of a built ProxyScene (rt_candidate/proxy_scene.h:29-46)
  * as device arrays; proxy i has proxy_id i. */

@@ -80,6 +80,12 @@ SIGNATURES: dict[str, tuple] = {
     "p2c_batch_anyhit": (_int, [_c_void_p, _c_void_p, ctypes.c_int32, ctypes.c_uint32, _c_void_p, _c_void_p, _i64,
                                 _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p, _c_void_p, _c_void_p, _c_void_p,
                                 _c_void_p, _size, _c_void_p]),
+    "p2c_serve_create": (_int, [_c_void_p, _c_void_p]),
+    "p2c_serve_destroy": (_int, [_c_void_p]),
+    "p2c_serve_register_mesh": (_int, [_c_void_p, _c_void_p, _c_void_p]),
+    "p2c_serve_admit": (_int, [_c_void_p, _c_void_p, _c_void_p]),
+    "p2c_serve_poll": (_int, [_c_void_p, _c_void_p, ctypes.c_int32, _c_void_p]),
+    "p2c_serve_read_stats": (_int, [_c_void_p, _c_void_p]),
     "p2c_refinement_children_workspace_bytes": (_size, [_i64]),
     "p2c_refinement_children": (_int, [_i64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, ctypes.c_uint16, _f64,
                                        ctypes.c_uint64, _c_void_p, _c_void_p, _c_void_p, _c_void_p, _c_void_p,

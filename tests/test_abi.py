@@ -73,3 +73,39 @@ def test_record_layouts_match_header():
     assert oracle.PT.itemsize == 240 and oracle.EE.itemsize == 240
     rec = np.zeros(1, dtype=records.POINT_TRIANGLE_DTYPE)
     assert rec.dtype.fields["triangle_v2"][1] == 16 + 3 * 56
+
+
+def test_serving_struct_layouts_match_header(tmp_path):
+    """The Python mirror's ctypes / numpy layouts of the serving structs
+    equal the C header's (sizes and offsets printed by a C compiler)."""
+    import shutil
+    import subprocess
+
+    from p2cccd_b200 import serve
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "layout.c"
+    src.write_text("""
+#include <stddef.h>
+#include <stdio.h>
+#include "p2c_b200.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu\\n", sizeof(p2c_serve_config), sizeof(p2c_serve_mesh), sizeof(p2c_serve_request),
+         sizeof(p2c_serve_result), sizeof(p2c_serve_stats));
+  printf("%zu %zu %zu %zu\\n", offsetof(p2c_serve_result, latency_ms), offsetof(p2c_serve_result, certify),
+         offsetof(p2c_serve_result, anyhit), offsetof(p2c_serve_config, cert));
+  return 0;
+}
+""")
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-std=c11", f"-I{ROOT / 'include'}", str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    sizes = [int(v) for v in out]
+    assert sizes[:5] == [ctypes.sizeof(serve.ServeConfigC), ctypes.sizeof(serve.ServeMeshC),
+                         ctypes.sizeof(serve.ServeRequestC), serve.SERVE_RESULT_DTYPE.itemsize,
+                         serve.SERVE_STATS_DTYPE.itemsize]
+    f = serve.SERVE_RESULT_DTYPE.fields
+    assert sizes[5:8] == [f["latency_ms"][1], f["certify"][1], f["anyhit"][1]]
+    assert sizes[8] == serve.ServeConfigC.cert.offset
