@@ -222,7 +222,8 @@ class ServeEngine:
             if r.keep_results:
                 if int(x["truncated"]):
                     raise _lib.P2CError(f"request {r.rid}: outputs truncated ({int(x['truncated'])})")
-                r.results = (r._out["vf"][:n_vf].copy(), r._out["ee"][:n_ee].copy())
+                raw = lambda a, n: a.view(np.uint8).reshape(-1, 72)[:n].copy().view(INTERVAL_RESULT_DTYPE).reshape(-1)
+                r.results = (raw(r._out["vf"], n_vf), raw(r._out["ee"], n_ee))  # bytes as written, padding too
                 u = r._out["uq"][:int(x["undecided_entries"])]
                 r.undecided = np.stack([(u >> np.uint64(63)).astype(np.int64) + 1,
                                         (u & np.uint64((1 << 63) - 1)).astype(np.int64)], 1)
