@@ -325,8 +325,16 @@ class SceneWorkload:
                               certify.records_to_device(ee_rec, self.pipe.device), 0.0, 1.0, self.cfg)["stats"]
 
     def broad_phase_bytes(self) -> int:
-        """Algorithmic bytes of candidate generation: read every vertex
-        trajectory (48 B), face (12 B) and edge (8 B) once, write every pair (8 B)."""
+        """Algorithmic bytes of candidate generation, B_bp = 48 V + 24 F + 16 E
+        + 120 S + 8 P (S = V + F + E, P = pairs): vertex t0/t1 read, index
+        read/write, box write, sort-key read/write and box re-read, pair write."""
+        s = self.scene
+        v, f, e = len(s["v_t0"]), len(s["faces"]), len(s["edges"])
+        return 48 * v + 24 * f + 16 * e + 120 * (v + f + e) + 8 * self.queries
+
+    def fused_ideal_bytes(self) -> int:
+        """The floor of a fused broad phase that reads the scene once and
+        writes the pairs: 48 B per vertex, 12 per face, 8 per edge, 8 per pair."""
         s = self.scene
         return 48 * len(s["v_t0"]) + 12 * len(s["faces"]) + 8 * len(s["edges"]) + 8 * self.queries
 
@@ -1004,7 +1012,9 @@ def run_b200(args) -> dict | None:
         broad_roof = {"bound": "hbm", "achieved": bp_bytes / (bp * 1e-3) / 1e9, "peak": hbm_peak, "unit": "GB/s",
                       "frac": bp_bytes / (bp * 1e-3) / 1e9 / hbm_peak, "traffic": None,
                       "peak_source": hbm_src, "kernel": "candidate generation (boxes, sort, sweep)",
-                      "algorithmic_bytes_per_step": bp_bytes}
+                      "algorithmic_bytes_per_step": bp_bytes, "bytes_formula": "48V + 24F + 16E + 120(V+F+E) + 8P"}
+        if hasattr(wl, "fused_ideal_bytes"):
+            broad_roof["fused_ideal_bytes_per_step"] = wl.fused_ideal_bytes()
         narrow = dict(fp64_roof, kernel=getattr(wl, "narrow_kernel", "certify_scene_kernel"),
                       achieved=census["fp64_ops"] / (npm * 1e-3) / 1e12,
                       frac=census["fp64_ops"] / (npm * 1e-3) / fp64_rate)
@@ -1019,6 +1029,9 @@ def run_b200(args) -> dict | None:
         r = wl.cpu_reference(threads, args.cpu_budget)
         cpu = {"value": r["queries"] / r["seconds"], "unit": "queries/s", "cores": r.get("threads", threads),
                "kind": "reference", "sample": r["sample"]}
+    served = None
+    if args.workload == "scene" and not args.no_served:
+        served = serve_bench(args, dev, rank, args.cpu_budget if (cpu is not None) else None)
     if rank != 0:
         return None
     h2d, d2h = wl.io_bytes()
@@ -1047,6 +1060,8 @@ def run_b200(args) -> dict | None:
     if phases is not None:
         line["phases"] = phases
         line["roofline_secondary"] = secondary
+    if served is not None:
+        line["served"] = served
     if args.benchmark_rows:
         _write_benchmark_rows(args, wl, times, phases, census, line, dev)
     return line
@@ -1127,7 +1142,44 @@ def _serve_pool(seed: int) -> list[tuple[str, dict, bool]]:
     return pool
 
 
-def run_serve(args) -> dict:
+def _served_run(eng, reqs, torch) -> tuple[list, float]:
+    """One stream through a server: wall seconds from the start to the last result."""
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    done = eng.run(reqs)
+    return done, time.perf_counter() - t0
+
+
+def _tool_serve_sample(pool, cfg, budget_s: float) -> dict:
+    """The reference scene tool (compiled unchanged: SweepPairs candidates +
+    RunScheduledAnyHitRows with its random policy, top-K 4096, 1 thread as
+    written) on whole steps of the serving meshes, smallest first, while the
+    budget lasts."""
+    import oracle
+
+    done, secs, cands, calls, t_start = [], 0.0, 0, 0, time.perf_counter()
+    for key, s, excl in sorted(pool, key=lambda p: len(p[1]["faces"])):
+        tool = oracle.RefToolScene(s["v_t0"], s["v_t1"], s["faces"], 0.0, excl)
+        r = tool.time_step(4096, cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth)
+        done.append((key, len(s["faces"]), r["candidates_s"] + r["anyhit_vf_s"] + r["anyhit_ee_s"]))
+        secs += done[-1][2]
+        cands += r["candidates"]
+        calls += r["calls"]
+        if time.perf_counter() - t_start > budget_s:
+            break
+    return {"value": len(done) / secs, "unit": "steps/s", "cores": 1, "kind": "reference",
+            "candidates_per_s": cands / secs, "exact_calls_per_s": calls / secs,
+            "sample": "the reference scene tool (SweepPairs + RunScheduledAnyHitRows, random policy, top-K 4096, "
+                      "1 thread as written) on one whole step of each of the smallest serving meshes: " +
+                      ", ".join(f"{k} ({t} tris, {sec:.2f} s)" for k, t, sec in done)}
+
+
+def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
+    """The serving stream: Poisson arrivals of CCD steps drawn from the
+    two-sphere, rigid uneven-scene and cloth-on-sphere kinds at 10k-600k
+    triangles, through the native server (p2c_serve_*), beside the plain path
+    (each step alone through the single-scene pipeline, every candidate
+    certified, host sync per step) on the same requests."""
     import numpy as np
     import torch
 
@@ -1135,111 +1187,133 @@ def run_serve(args) -> dict:
     from p2cccd_b200.scene import ScenePipeline
     from p2cccd_b200.serve import Request, ServeEngine, latency_stats
 
-    world, rank, local = _dist_setup(args)
-    dev = torch.device("cuda", local if world > 1 else 0)
     seed = 20261203 + rank
     cfg = certify.CertConfig(1e-6, 1e-6, 32)
     pool = _serve_pool(seed)
-    eng = ServeEngine(dev, config=cfg, slots=SERVE_SLOTS, max_group=SERVE_MAX_GROUP)
     host = {}
     for key, s, excl in pool:
-        eng.register_mesh(key, s, exclude_self=excl)
         host[key] = (torch.from_numpy(np.ascontiguousarray(s["v_t0"])).pin_memory(),
                      torch.from_numpy(np.ascontiguousarray(s["v_t1"])).pin_memory(), len(s["faces"]), excl, s)
-    rng = np.random.default_rng(seed)
-    n_req = args.serve_requests
     keys = [k for k, _, _ in pool]
+    rng = np.random.default_rng(seed)
+    n_req = max(1, args.serve_requests)
+    picks = [keys[int(rng.integers(len(keys)))] for _ in range(n_req)]
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, n_req))
 
-    def stream(rate: float):
-        t, out = 0.0, []
-        for i in range(n_req):
-            t += float(rng.exponential(1.0 / rate))
-            k = keys[int(rng.integers(len(keys)))]
-            out.append(Request(rid=i, mesh=k, v_t0=host[k][0], v_t1=host[k][1], arrival_s=t))
-        return out
+    def stream(times):
+        return [Request(rid=i, mesh=picks[i], v_t0=host[picks[i]][0], v_t1=host[picks[i]][1],
+                        arrival_s=float(times[i]), seed=1000003 * i + 7) for i in range(n_req)]
 
-    # warm-up: every mesh once (sizes the candidate state), then a short stream
-    eng.run([Request(rid=-1 - i, mesh=k, v_t0=host[k][0], v_t1=host[k][1], arrival_s=0.0) for i, k in enumerate(keys)])
-    for _ in range(max(0, args.warmup)):
-        eng.start()
-        eng.run(stream(args.serve_rate)[: max(8, n_req // 8)])
-    sampler = ClockSampler(dev.index if world > 1 else 0)
+    def engine(narrow):
+        eng = ServeEngine(dev, config=cfg, slots=SERVE_SLOTS, max_group=SERVE_MAX_GROUP, narrow=narrow, top_k=4096,
+                          memory_budget=int(args.serve_memory_gb * (1 << 30)))
+        for key, s, excl in pool:
+            eng.register_mesh(key, s, exclude_self=excl)
+        warm = [Request(rid=-1 - i, mesh=k, v_t0=host[k][0], v_t1=host[k][1], arrival_s=0.0, seed=i)
+                for i, k in enumerate(keys)]
+        for _ in range(2):  # sizes every mesh's candidate state
+            eng.run(warm)
+        return eng
+
+    sampler = ClockSampler(dev.index or 0)
     sampler.start()
-    torch.cuda.synchronize()
-    results = []
     t_begin = time.time()
-    for _ in range(args.steps):
-        reqs = stream(args.serve_rate)
-        eng.start()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        e0.record()
-        done = eng.run(reqs)
-        e1.record()
-        torch.cuda.synchronize()
-        results.append((done, e0.elapsed_time(e1)))
+    out = {}
+    for narrow in ("anyhit", "certify"):
+        eng = engine(narrow)
+        for _ in range(max(1, args.warmup // 2)):
+            eng.run(stream(np.zeros(n_req))[: max(8, n_req // 8)])
+        done, wall = _served_run(eng, stream(np.zeros(n_req)), torch)  # saturated: capacity
+        st = eng.stats()
+        cap = {"steps_per_s": n_req / wall, "candidates_per_s": sum(r.queries for r in done) / wall,
+               "exact_calls_per_s": sum(r.calls for r in done) / wall, "wall_s": wall,
+               "groups_run": st["groups"], "reruns": st["reruns"], "arena_peak_bytes": st["arena_peak"]}
+        res = {"capacity": cap}
+        if narrow == "anyhit":
+            for tag, times in (("offered", arrivals),
+                               ("sustainable", arrivals * max(1.0, args.serve_rate / (0.7 * cap["steps_per_s"])))):
+                done_r, wall_r = _served_run(eng, stream(times), torch)
+                tris = np.array([host[r.mesh][2] for r in done_r], dtype=np.float64)
+                lat = np.array([r.latency_ms for r in done_r])
+                per = lat / np.maximum(tris / 1e5, 1e-9)
+                res[tag] = {"arrival_rate_per_s": n_req / float(times[-1]), "steps_per_s": n_req / wall_r,
+                            **latency_stats(done_r),
+                            "p50_ms_per_100k_tris": float(np.percentile(per, 50)),
+                            "p99_ms_per_100k_tris": float(np.percentile(per, 99)),
+                            "admission_lag_p99_ms": float(np.percentile([r.admit_lag_ms for r in done_r], 99))}
+        eng.close()
+        out[narrow] = res
     t_end = time.time()
     clocks = sampler.stop((t_begin, t_end))
-    done_all = [r for d, _ in results for r in d]
-    q_total = sum(r.queries for r in done_all)
-    ms_total = sum(ms for _, ms in results)
-    stats = latency_stats(done_all)
-    tris = np.array([host[r.mesh][2] for r in done_all], dtype=np.float64)
-    lat = np.array([r.latency_ms for r in done_all])
-    per100k = lat / np.maximum(tris / 1e5, 1e-9)
-    # the plain per-step path: each request alone, synchronously, through ScenePipeline
-    plain_ms, plain_q = 0.0, 0
-    pipes = {}
-    for r in results[-1][0]:
-        v0, v1, _, excl, s = host[r.mesh]
-        if r.mesh not in pipes:
-            pipes[r.mesh] = ScenePipeline(s, dev, exclude_self=excl, config=cfg,
-                                          vf_capacity=eng.meshes[r.mesh].vf_cap,
-                                          ee_capacity=eng.meshes[r.mesh].ee_cap)
-            pipes[r.mesh].step_checked()
-        p = pipes[r.mesh]
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        p.v_t0.copy_(v0, non_blocking=True)
-        p.v_t1.copy_(v1, non_blocking=True)
-        summ = p.step_checked()
-        plain_ms += (time.perf_counter() - t0) * 1e3
-        plain_q += summ["vf_certified"] + summ["ee_certified"]
-    value = q_total / (ms_total * 1e-3)
-    plain_value = plain_q / (plain_ms * 1e-3)
-    h2d = int(sum(2 * host[r.mesh][0].numel() * 8 for r in done_all) / max(1, args.steps))
-    d2h = int(sum(112 + 32 for _ in done_all) / max(1, args.steps))
-    census_q = {}
-    return {
-        "metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_total / args.steps,
-        "p50_ms": stats["p50_ms"], "p99_ms": stats["p99_ms"], "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "serving stream: Poisson arrivals of CCD steps drawn from the two-sphere, rigid "
-                               "uneven-scene and cloth-on-sphere kinds at 10k-600k triangles, admitted by slots and "
-                               "device memory into continuous batches (one candidate launch sequence + one "
-                               "certification launch per batch), every candidate certified; a step of this line "
-                               f"is one stream of {n_req} requests",
-                   "arrival_rate_per_s": args.serve_rate, "requests_per_step": n_req,
-                   "meshes": {k: int(host[k][2]) for k in keys},
-                   "latency_ms": stats, "latency_ms_per_100k_triangles": {
-                       "p50": float(np.percentile(per100k, 50)), "p99": float(np.percentile(per100k, 99))},
-                   "served_requests_per_s": len(done_all) / (ms_total * 1e-3),
-                   "groups_run": eng.groups_run, "reruns": int(sum(r.reruns for r in done_all)),
-                   "plain_path": {"value": plain_value, "unit": "queries/s",
-                                  "what": "the same requests one at a time through ScenePipeline.step_checked "
-                                          "(host sync per step)"},
-                   "served_over_plain": value / plain_value,
-                   "eps_time": cfg.eps_time, "eps_space": cfg.eps_space,
-                   "max_subdivision_depth": cfg.max_subdivision_depth, "seed": seed,
-                   "l2": "requests stream fresh trajectories from host memory", "parallelism": f"replicas x{world}"},
-        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                "what": "the serving loop is end to end: trajectories copied from pinned host memory, summaries "
-                        "and counts copied back, per request"},
-        "gpu_launches": None,
-        "roofline": None,
-        "cpu_baseline": None,
+    # the plain path: each step alone, one at a time, every candidate certified
+    plain_ms = {}
+    for key, s, excl in pool:
+        if key not in picks:
+            continue
+        p = ScenePipeline(s, dev, exclude_self=excl, config=cfg)
+        p.step_checked()
+        p.fit_capacities()
+        p.step_checked()
+        ts = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            p.v_t0.copy_(host[key][0], non_blocking=True)
+            p.v_t1.copy_(host[key][1], non_blocking=True)
+            p.step_checked()
+            ts.append((time.perf_counter() - t0) * 1e3)
+        plain_ms[key] = (statistics.median(ts), p.read_counts()[0] + p.read_counts()[1])
+        del p
+    plain_s = sum(plain_ms[k][0] for k in picks) * 1e-3
+    plain = {"steps_per_s": n_req / plain_s, "candidates_per_s": sum(plain_ms[k][1] for k in picks) / plain_s,
+             "what": "each request alone, one at a time, through ScenePipeline.step_checked (single-scene broad "
+                     "phase + certificates of every candidate, trajectories copied in from page-locked memory, "
+                     "counts and summary read back: a host sync per step); per-mesh median of 3 steps, summed "
+                     "over the stream's requests",
+             "ms_per_step_by_mesh": {k: v[0] for k, v in plain_ms.items()}}
+    block = {
+        "workload": "serving stream: Poisson arrivals of CCD steps drawn uniformly from 9 meshes of the two-sphere, "
+                    "rigid uneven-scene and cloth-on-sphere kinds (10k-600k triangles), through the native "
+                    "continuous-batching server (p2c_serve_*): admission by slots and a device arena, one batched "
+                    "candidate generation per group, then the scheduled any-hit with fallback replay (scores from "
+                    "the seeded scheduler stub, top-K 4096) or certificates of every candidate",
+        "requests": n_req, "offered_rate_per_s": args.serve_rate,
+        "meshes": {k: int(host[k][2]) for k in keys}, "slots": SERVE_SLOTS, "max_group": SERVE_MAX_GROUP,
+        "anyhit": out["anyhit"], "certify_all": out["certify"], "plain_path": plain,
+        "served_over_plain": out["anyhit"]["capacity"]["steps_per_s"] / plain["steps_per_s"],
+        "served_certify_all_over_plain": out["certify"]["capacity"]["steps_per_s"] / plain["steps_per_s"],
+        "ratio_unit": "CCD steps/s on the same requests (capacity: every request arrives at once)",
+        "e2e": "every served number is end to end: trajectories from page-locked host memory, summaries back",
         "clocks": clocks,
+    }
+    if cpu_budget is not None:
+        block["cpu_baseline"] = _tool_serve_sample(pool, cfg, cpu_budget)
+    return block
+
+
+def run_serve(args) -> dict:
+    import torch
+
+    world, rank, local = _dist_setup(args)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    blk = serve_bench(args, dev, rank, None if (args.no_cpu_baseline or rank != 0) else args.cpu_budget)
+    cap = blk["anyhit"]["capacity"]
+    value, ms = replica_rate(world, cap["candidates_per_s"] * cap["wall_s"], cap["wall_s"] * 1e3)
+    if rank != 0:
+        return None
+    off = blk["anyhit"]["offered"]
+    return {
+        "metric": "served CCD candidates/s (every candidate decided: certified, or covered by its group's hit)",
+        "value": value, "unit": "candidates/s", "n_gpus": world, "steps": 1, "warmup": args.warmup,
+        "ms_per_step": ms, "p50_ms": off["p50_ms"], "p99_ms": off["p99_ms"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": blk["workload"], "requests_per_step": blk["requests"],
+                   "arrival_rate_per_s": args.serve_rate, "parallelism": f"replicas x{world}",
+                   "l2": "requests stream fresh trajectories from host memory"},
+        "served": blk,
+        "e2e": {"value": value, "unit": "candidates/s", "h2d_bytes_per_step": None, "d2h_bytes_per_step": None,
+                "what": blk["e2e"]},
+        "gpu_launches": None, "roofline": None, "cpu_baseline": blk.get("cpu_baseline"), "clocks": blk["clocks"],
     }
 
 
@@ -1743,6 +1817,8 @@ def main():
                     help="batch: graph replays per autotuner trial (0: the library's default launch shape)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
+    ap.add_argument("--serve-memory-gb", type=float, default=32.0, help="serving: the server's device arena (GB)")
+    ap.add_argument("--no-served", action="store_true", help="scene: leave out the serving block")
     ap.add_argument("--proxy-objects", type=int, default=32, help="proxy: rigid bodies of 200 patches x 8 slabs")
     ap.add_argument("--group-rows", type=int, default=1_000_000, help="groups: candidate rows per step")
     ap.add_argument("--serve-slots", type=int, default=4, help="serving: request groups in flight")

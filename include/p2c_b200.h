@@ -186,6 +186,21 @@ int p2c_certify_ee_batch_host(const p2c_edge_edge* prims_host, int64_t n,
                               const p2c_cert_config* config,
                               p2c_interval_result* results_host);
 
+/* The library's CPU certifier, the CPU side of CrossCheckCpuCudaExact
+ * (certificate_cuda.cu:616-679): EvaluatePointTriangleInterval /
+ * EvaluateEdgeEdgeInterval (certificate_engine.cpp:300-386, 481-551) on the
+ * host's cores, host arrays in and out.  Same validation messages as the GPU
+ * entry points.  It shares only the distance and motion formulas with the
+ * device; the GPU entry points never call it. */
+int p2c_certify_pt_batch_cpu(const p2c_point_triangle* prims_host, int64_t n,
+                             double interval_t0, double interval_t1,
+                             const p2c_cert_config* config,
+                             p2c_interval_result* results_host);
+int p2c_certify_ee_batch_cpu(const p2c_edge_edge* prims_host, int64_t n,
+                             double interval_t0, double interval_t1,
+                             const p2c_cert_config* config,
+                             p2c_interval_result* results_host);
+
 /* Census launch: the same certifier with lane-local depth-first order (the
  * reference's node set exactly) and FP64 operation counting.  Used to state the
  * algorithmic FP64 work of a batch; not a production path. */

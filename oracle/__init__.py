@@ -27,6 +27,7 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libccd_oracle.so"
 REF_SO = HERE / "_ref" / "libp2c_ref.so"
 REF_TOOL_SO = HERE / "_ref" / "libp2c_ref_tool.so"
+REF_CUDA_SO = HERE / "_ref" / "libp2c_ref_cuda.so"
 
 TRAJ = np.dtype([("feature_id", "<i8"), ("position_t0", "<f8", (3,)), ("position_t1", "<f8", (3,))])
 PT = np.dtype([("point_id", "<i8"), ("triangle_id", "<i8"), ("point", TRAJ), ("triangle_v0", TRAJ),
@@ -97,6 +98,49 @@ def lib() -> ctypes.CDLL:
 
 def ref_available() -> bool:
     return REF_SO.exists()
+
+
+_ref_cuda = None
+
+
+def ref_cuda_available() -> bool:
+    return REF_CUDA_SO.exists()
+
+
+def ref_cuda() -> ctypes.CDLL:
+    """The reference's CUDA batch certifier compiled unchanged
+    (certificate_cuda.cu, oracle/ref_cuda.cpp): needs a GPU to run."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        if not REF_CUDA_SO.exists():
+            raise FileNotFoundError(f"{REF_CUDA_SO} is not built (reference CUDA sources or nvcc absent)")
+        _ref_cuda = ctypes.CDLL(str(REF_CUDA_SO))
+        C = _ref_cuda
+        vp, i64, f64, ci = ctypes.c_void_p, ctypes.c_int64, ctypes.c_double, ctypes.c_int
+        C.ref_cuda_last_error.restype = ctypes.c_char_p
+        C.ref_cuda_eval_batch.argtypes = [ci, vp, i64, f64, f64, f64, f64, ci, vp]
+        C.ref_cuda_cross_check.argtypes = [vp, i64, vp, i64, f64, f64, f64, f64, ci, f64]
+    return _ref_cuda
+
+
+def ref_cuda_eval_batch(records: np.ndarray, t0: float, t1: float, eps_time: float, eps_space: float,
+                        max_depth: int) -> np.ndarray:
+    """EvaluatePointTriangleBatchCuda / EvaluateEdgeEdgeBatchCuda of the
+    reference (host records in, results out; the family from the dtype)."""
+    C = ref_cuda()
+    fam = 1 if records.dtype.names[0] == "point_id" else 2
+    out = np.zeros(len(records), dtype=RESULT)
+    if C.ref_cuda_eval_batch(fam, _p(records), len(records), t0, t1, eps_time, eps_space, max_depth, _p(out)):
+        raise RuntimeError(C.ref_cuda_last_error().decode())
+    return out
+
+
+def ref_cuda_cross_check(pt: np.ndarray, ee: np.ndarray, t0: float, t1: float, eps_time: float, eps_space: float,
+                         max_depth: int, eps_cert: float) -> tuple[bool, str]:
+    """The reference's CrossCheckCpuCudaExact: (agree, message)."""
+    C = ref_cuda()
+    rc = C.ref_cuda_cross_check(_p(pt), len(pt), _p(ee), len(ee), t0, t1, eps_time, eps_space, max_depth, eps_cert)
+    return rc == 0, C.ref_cuda_last_error().decode()
 
 
 def ref() -> ctypes.CDLL:

@@ -25,6 +25,7 @@
 // known collision are pruned (the serial recursion never visits them).
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <type_traits>
 
@@ -34,52 +35,89 @@ namespace p2c {
 
 constexpr double kNumEps = 1.0e-14;  // kNumericalEpsilon, certificate_engine.cpp:20
 
-// ---- optional FP64 operation census ---------------------------------------
-struct NoCount {
-  static constexpr unsigned long long n = 0;
-  __device__ __forceinline__ void add(int) {}
-};
-struct OpCount {
-  unsigned long long n = 0;
-  __device__ __forceinline__ void add(int k) { n += (unsigned long long)k; }
-};
-
 struct V3 {
   double x, y, z;
 };
 
-__device__ __forceinline__ double mul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double add(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double sub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double dvd(double a, double b) { return __ddiv_rn(a, b); }
+// Every operation is rounded once, to nearest: the explicitly rounded
+// intrinsics on the device; on the host (the library's CPU certifier, built
+// with -ffp-contract=off and no FMA target) the plain IEEE operators, which
+// round the same way.
+#define P2C_HD __host__ __device__ __forceinline__
+P2C_HD double mul(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dmul_rn(a, b);
+#else
+  return a * b;
+#endif
+}
+P2C_HD double add(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dadd_rn(a, b);
+#else
+  return a + b;
+#endif
+}
+P2C_HD double sub(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __dsub_rn(a, b);
+#else
+  return a - b;
+#endif
+}
+P2C_HD double dvd(double a, double b) {
+#ifdef __CUDA_ARCH__
+  return __ddiv_rn(a, b);
+#else
+  return a / b;
+#endif
+}
+P2C_HD double sqrt_rn(double a) {
+#ifdef __CUDA_ARCH__
+  return __dsqrt_rn(a);
+#else
+  return std::sqrt(a);
+#endif
+}
 
-__device__ __forceinline__ V3 vadd(V3 a, V3 b) { return {add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)}; }
-__device__ __forceinline__ V3 vsub(V3 a, V3 b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
-__device__ __forceinline__ V3 vscale(V3 a, double s) { return {mul(a.x, s), mul(a.y, s), mul(a.z, s)}; }
+// ---- optional FP64 operation census ---------------------------------------
+struct NoCount {
+  static constexpr unsigned long long n = 0;
+  P2C_HD void add(int) {}
+};
+struct OpCount {
+  unsigned long long n = 0;
+  P2C_HD void add(int k) { n += (unsigned long long)k; }
+};
+
+
+P2C_HD V3 vadd(V3 a, V3 b) { return {add(a.x, b.x), add(a.y, b.y), add(a.z, b.z)}; }
+P2C_HD V3 vsub(V3 a, V3 b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
+P2C_HD V3 vscale(V3 a, double s) { return {mul(a.x, s), mul(a.y, s), mul(a.z, s)}; }
 // a.x*b.x + a.y*b.y + a.z*b.z, left to right
-__device__ __forceinline__ double vdot(V3 a, V3 b) {
+P2C_HD double vdot(V3 a, V3 b) {
   return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z));
 }
-__device__ __forceinline__ V3 vcross(V3 a, V3 b) {
+P2C_HD V3 vcross(V3 a, V3 b) {
   return {sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)),
           sub(mul(a.x, b.y), mul(a.y, b.x))};
 }
 // std::clamp(v, lo, hi) as libstdc++ evaluates it
-__device__ __forceinline__ double clamp_std(double v, double lo, double hi) {
+P2C_HD double clamp_std(double v, double lo, double hi) {
   return (v < lo) ? lo : ((hi < v) ? hi : v);
 }
-__device__ __forceinline__ double max_std(double a, double b) { return (a < b) ? b : a; }
-__device__ __forceinline__ double min_std(double a, double b) { return (b < a) ? b : a; }
+P2C_HD double max_std(double a, double b) { return (a < b) ? b : a; }
+P2C_HD double min_std(double a, double b) { return (b < a) ? b : a; }
 
 template <class C>
-__device__ __forceinline__ double dist_pp(V3 a, V3 b, C& c) {  // :78-80
+P2C_HD double dist_pp(V3 a, V3 b, C& c) {  // :78-80
   c.add(9);
   const V3 d = vsub(a, b);
-  return __dsqrt_rn(vdot(d, d));
+  return sqrt_rn(vdot(d, d));
 }
 
 template <class C>
-__device__ __forceinline__ double dist_point_segment(V3 p, V3 a, V3 b, C& c) {  // :82-90
+P2C_HD double dist_point_segment(V3 p, V3 a, V3 b, C& c) {  // :82-90
   const V3 ab = vsub(b, a);
   const double ab2 = vdot(ab, ab);
   c.add(8);
@@ -91,7 +129,7 @@ __device__ __forceinline__ double dist_point_segment(V3 p, V3 a, V3 b, C& c) {  
 
 // DistancePointTriangle, certificate_engine.cpp:133-184
 template <class C>
-__device__ __forceinline__ double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C& c) {
+P2C_HD double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C& c) {
   const V3 ab = vsub(b, a);
   const V3 ac = vsub(cc, a);
   const V3 n = vcross(ab, ac);
@@ -142,7 +180,7 @@ __device__ __forceinline__ double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C
     c.add(11);
     return dist_pp(p, vadd(b, vscale(vsub(cc, b), w)), c);
   }
-  const double nn = __dsqrt_rn(vdot(n, n));
+  const double nn = sqrt_rn(vdot(n, n));
   const double sd = dvd(vdot(ap, n), nn);
   c.add(12);
   return fabs(sd);
@@ -150,7 +188,7 @@ __device__ __forceinline__ double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C
 
 // DistanceSegmentSegment, certificate_engine.cpp:92-131
 template <class C>
-__device__ __forceinline__ double dist_segment_segment(V3 p1, V3 q1, V3 p2, V3 q2, C& c) {
+P2C_HD double dist_segment_segment(V3 p1, V3 q1, V3 p2, V3 q2, C& c) {
   const V3 d1 = vsub(q1, p1);
   const V3 d2 = vsub(q2, p2);
   const V3 r = vsub(p1, p2);
@@ -213,7 +251,7 @@ struct SlotGeo {
 
 // PositionAt (:67-69) for the 4 vertices, then the family's distance.
 template <int kFamily, class G, class C>
-__device__ __forceinline__ double distance_at(const G& g, double t, C& c) {
+P2C_HD double distance_at(const G& g, double t, C& c) {
   V3 x[4];
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -229,12 +267,12 @@ __device__ __forceinline__ double distance_at(const G& g, double t, C& c) {
 // Norm(Sub(p1, p0)) of each trajectory: constant per query, hoisted out of
 // MaxDisplacementFromMidpoint (:71-76); the same rounded value either way.
 template <class G, class C>
-__device__ __forceinline__ void motion_norms(const G& g, double nrm[4], C& c) {
+P2C_HD void motion_norms(const G& g, double nrm[4], C& c) {
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const V3 d = vsub(V3{g.p1(3 * i), g.p1(3 * i + 1), g.p1(3 * i + 2)},
                       V3{g.p0(3 * i), g.p0(3 * i + 1), g.p0(3 * i + 2)});
-    nrm[i] = __dsqrt_rn(vdot(d, d));
+    nrm[i] = sqrt_rn(vdot(d, d));
   }
   c.add(36);
 }
@@ -242,7 +280,7 @@ __device__ __forceinline__ void motion_norms(const G& g, double nrm[4], C& c) {
 // PointTriangleMotionRadius / EdgeEdgeMotionRadius (:200-222); each
 // MaxDisplacementFromMidpoint is (0.5 * max(0, t1 - t0)) * norm.
 template <int kFamily, class C>
-__device__ __forceinline__ double motion_radius(const double nrm[4], double t0, double t1, C& c) {
+P2C_HD double motion_radius(const double nrm[4], double t0, double t1, C& c) {
   const double h = mul(0.5, max_std(0.0, sub(t1, t0)));
   const double m0 = mul(h, nrm[0]), m1 = mul(h, nrm[1]), m2 = mul(h, nrm[2]), m3 = mul(h, nrm[3]);
   c.add(7);

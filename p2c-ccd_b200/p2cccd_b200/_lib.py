@@ -47,6 +47,8 @@ SIGNATURES: dict[str, tuple] = {
                                     _c_void_p, _size, _c_void_p, _c_void_p]),
     "p2c_certify_pt_batch_host": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
     "p2c_certify_ee_batch_host": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
+    "p2c_certify_pt_batch_cpu": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
+    "p2c_certify_ee_batch_cpu": (_int, [_c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig), _c_void_p]),
     "p2c_certify_batch2": (_int, [_c_void_p, _i64, _c_void_p, _i64, _f64, _f64, ctypes.POINTER(CertConfig),
                                   _c_void_p, _c_void_p, _c_void_p, _size, _c_void_p, _c_void_p]),
     "p2c_certify_queries_workspace_bytes": (_size, [_i64]),

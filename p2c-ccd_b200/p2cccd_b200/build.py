@@ -33,7 +33,7 @@ LIB_DIGEST = LIB.with_name(LIB.name + ".sha256")
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-lineinfo", "-O3", "--fmad=false", "-std=c++17",
-    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2",
+    "-Xcompiler", "-fPIC", "-Xcompiler", "-O2", "-Xcompiler", "-ffp-contract=off",
     "--expt-relaxed-constexpr",
 ]
 

@@ -144,6 +144,20 @@ def certify_batch_host(records: np.ndarray, interval_t0: float = 0.0, interval_t
     return out
 
 
+def certify_batch_cpu(records: np.ndarray, interval_t0: float = 0.0, interval_t1: float = 1.0,
+                      config: CertConfig = CertConfig()) -> np.ndarray:
+    """The library's CPU certifier (p2c_certify_*_batch_cpu) on host records:
+    the CPU side of the CPU/CUDA cross-check.  Never a fallback of the GPU path."""
+    lib = _lib.load()
+    rec = np.ascontiguousarray(records)
+    fn = lib.p2c_certify_pt_batch_cpu if rec.dtype.names[0] == "point_id" else lib.p2c_certify_ee_batch_cpu
+    out = np.zeros(len(rec), dtype=INTERVAL_RESULT_DTYPE)
+    cfg = config.c()
+    _lib.check(fn(rec.ctypes.data if len(rec) else None, len(rec), float(interval_t0), float(interval_t1),
+                  ctypes.byref(cfg), out.ctypes.data if len(rec) else None))
+    return out
+
+
 def census(pt: torch.Tensor | None, ee: torch.Tensor | None, interval_t0: float = 0.0,
            interval_t1: float = 1.0, config: CertConfig = CertConfig()) -> dict:
     """Run the lane-local depth-first census launch (the reference's node set)

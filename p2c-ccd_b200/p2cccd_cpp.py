@@ -450,13 +450,12 @@ def _compare(a: np.ndarray, b: np.ndarray, eps_cert: float, label: str) -> None:
 
 
 def cross_check_cpu_cuda_exact(point_triangles, edge_edges, interval_t0, interval_t1, config, eps_cert) -> bool:
-    """The reference cross-checks its CUDA kernel against its CPU recursion
-    (certificate_cuda.cu:616-679).  Here both sides run on the GPU: the
-    production warp-cooperative launch against the census launch, whose lanes
-    walk each interval tree depth-first exactly as the CPU recursion does; the
-    comparison rules are the reference's."""
-    import torch
-
+    """CrossCheckCpuCudaExact (certificate_cuda.cu:616-679): the GPU engine's
+    certificates (the production launch, as evaluate_*_batch_cuda returns
+    them) against the library's CPU certifier (p2c_certify_*_batch_cpu, an
+    independent host evaluation of the recursion), with the reference's
+    comparison rules; raises ValueError with the reference's message on the
+    first mismatch, returns True otherwise."""
     from p2cccd_b200 import certify
 
     if not math.isfinite(float(eps_cert)) or float(eps_cert) < 0.0:
@@ -464,15 +463,12 @@ def cross_check_cpu_cuda_exact(point_triangles, edge_edges, interval_t0, interva
     cfg = _config(config)
     pt = _to_records(list(point_triangles), 1)
     ee = _to_records(list(edge_edges), 2)
-    fast_pt = certify.certify_batch_host(pt, interval_t0, interval_t1, cfg)
-    fast_ee = certify.certify_batch_host(ee, interval_t0, interval_t1, cfg)
-    if len(pt) + len(ee) == 0:
-        return True
-    dev = torch.device("cuda", torch.cuda.current_device())
-    cen = certify.census(certify.records_to_device(pt, dev) if len(pt) else None,
-                         certify.records_to_device(ee, dev) if len(ee) else None, interval_t0, interval_t1, cfg)
-    _compare(certify.results_to_numpy(cen["pt"]), fast_pt, float(eps_cert), "point-triangle CPU/CUDA cross-check")
-    _compare(certify.results_to_numpy(cen["ee"]), fast_ee, float(eps_cert), "edge-edge CPU/CUDA cross-check")
+    gpu_pt = certify.certify_batch_host(pt, interval_t0, interval_t1, cfg)
+    cpu_pt = certify.certify_batch_cpu(pt, interval_t0, interval_t1, cfg)
+    _compare(cpu_pt, gpu_pt, float(eps_cert), "point-triangle CPU/CUDA cross-check")
+    gpu_ee = certify.certify_batch_host(ee, interval_t0, interval_t1, cfg)
+    cpu_ee = certify.certify_batch_cpu(ee, interval_t0, interval_t1, cfg)
+    _compare(cpu_ee, gpu_ee, float(eps_cert), "edge-edge CPU/CUDA cross-check")
     return True
 
 
