@@ -200,6 +200,32 @@ class PlainWorkload:
     def census(self) -> dict:
         return self.certify.census(self.pt, self.ee, 0.0, 1.0, self.cfg)["stats"]
 
+    def reference_gpu(self, steps: int) -> dict | None:
+        """The reference's own GPU path on this batch: certificate_cuda.cu
+        compiled unchanged for sm_100a (oracle/_ref), called the way its batch
+        API runs (host records in, cudaMalloc + cudaMemcpy + one thread per
+        primitive + cudaDeviceSynchronize + copy back + cudaFree per family)."""
+        import oracle
+
+        if not oracle.ref_cuda_available():
+            return None
+        c = self.cfg
+        run = lambda fam: oracle.ref_cuda_eval_batch(self.host[fam], 0.0, 1.0, c.eps_time, c.eps_space,
+                                                     c.max_subdivision_depth)
+        for _ in range(2):
+            run("vf"), run("ee")
+        ts = []
+        for _ in range(max(1, steps)):
+            t0 = time.perf_counter()
+            run("vf")
+            run("ee")
+            ts.append(time.perf_counter() - t0)
+        ms = statistics.median(ts) * 1e3
+        return {"value": self.queries / (ms * 1e-3), "unit": "queries/s", "ms_per_step": ms,
+                "what": "the reference's CUDA batch certifier (certificate_cuda.cu, compiled unchanged for sm_100a: "
+                        "malloc, copy, one thread per primitive, sync, copy back, free per call) on the same 20,000 "
+                        "host records; its certificates are not parity truth (it stops at the first undecided leaf)"}
+
     def cpu_reference(self, threads: int, budget_s: float) -> dict:
         """Reference C++ certifier (oracle/_ref, unchanged sources) on host cores."""
         import oracle
@@ -1029,6 +1055,8 @@ def run_b200(args) -> dict | None:
         r = wl.cpu_reference(threads, args.cpu_budget)
         cpu = {"value": r["queries"] / r["seconds"], "unit": "queries/s", "cores": r.get("threads", threads),
                "kind": "reference", "sample": r["sample"]}
+        if hasattr(wl, "reference_gpu"):  # the reference's GPU path, a comparison row beside the CPU one
+            cpu["reference_gpu"] = wl.reference_gpu(min(args.steps, 20))
     served = None
     if args.workload == "scene" and not args.no_served:
         served = serve_bench(args, dev, rank, args.cpu_budget if (cpu is not None) else None)
