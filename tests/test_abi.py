@@ -109,3 +109,13 @@ int main(void) {
     f = serve.SERVE_RESULT_DTYPE.fields
     assert sizes[5:8] == [f["latency_ms"][1], f["certify"][1], f["anyhit"][1]]
     assert sizes[8] == serve.ServeConfigC.cert.offset
+
+
+def test_reference_checker_libraries_load():
+    """Every checker library under oracle/_ref resolves all its symbols (a
+    missing one would only show on the GPU box otherwise)."""
+    import oracle
+
+    for so in (oracle.REF_SO, oracle.REF_TOOL_SO, oracle.REF_CUDA_SO):
+        if so.exists():
+            ctypes.CDLL(str(so))
