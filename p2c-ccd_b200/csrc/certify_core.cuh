@@ -127,14 +127,23 @@ P2C_HD double dist_point_segment(V3 p, V3 a, V3 b, C& c) {  // :82-90
   return dist_pp(p, vadd(a, vscale(ab, t)), c);
 }
 
-// DistancePointTriangle, certificate_engine.cpp:133-184
+// DistancePointTriangle, certificate_engine.cpp:133-184.  The Voronoi region
+// is found with the reference's tests, in its order, on the quantities it
+// computes; every region then ends in one of three forms: a vertex
+// (|p - v|), an edge (v = num / den, |p - (base + dir * v)|) or the face
+// (|dot(ap, n) / |n||).  Evaluating the tails after the region is known, one
+// form at a time, lets a warp whose lanes sit in different regions issue at
+// most one division and two square roots instead of one of each per region
+// present; every lane still performs exactly its region's operations, in the
+// reference's order, so the value is the same bit for bit.
 template <class C>
 P2C_HD double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C& c) {
   const V3 ab = vsub(b, a);
   const V3 ac = vsub(cc, a);
   const V3 n = vcross(ab, ac);
   c.add(20);
-  if (vdot(n, n) <= kNumEps) {
+  const double nn2 = vdot(n, n);
+  if (nn2 <= kNumEps) {
     double m = dist_point_segment(p, a, b, c);
     const double m1 = dist_point_segment(p, b, cc, c);
     const double m2 = dist_point_segment(p, cc, a, c);
@@ -146,44 +155,76 @@ P2C_HD double dist_point_triangle(V3 p, V3 a, V3 b, V3 cc, C& c) {
   const double d1 = vdot(ab, ap);
   const double d2 = vdot(ac, ap);
   c.add(13);
-  if (d1 <= 0.0 && d2 <= 0.0) return dist_pp(p, a, c);
-  const V3 bp = vsub(p, b);
-  const double d3 = vdot(ab, bp);
-  const double d4 = vdot(ac, bp);
-  c.add(13);
-  if (d3 >= 0.0 && d4 <= d3) return dist_pp(p, b, c);
-  const double vc = sub(mul(d1, d4), mul(d3, d2));
-  c.add(3);
-  if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
-    const double v = dvd(d1, sub(d1, d3));
-    c.add(8);
-    return dist_pp(p, vadd(a, vscale(ab, v)), c);
+  int form;  // 0 vertex, 1 edge, 2 face
+  V3 base = a, dir = ab;
+  double num = 0.0, den = 1.0;
+  if (d1 <= 0.0 && d2 <= 0.0) {
+    form = 0;  // vertex a
+  } else {
+    const V3 bp = vsub(p, b);
+    const double d3 = vdot(ab, bp);
+    const double d4 = vdot(ac, bp);
+    c.add(13);
+    if (d3 >= 0.0 && d4 <= d3) {
+      form = 0;  // vertex b
+      base = b;
+    } else {
+      const double vc = sub(mul(d1, d4), mul(d3, d2));
+      c.add(3);
+      if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+        form = 1;  // edge ab: v = d1 / (d1 - d3)
+        num = d1;
+        den = sub(d1, d3);
+        c.add(8);
+      } else {
+        const V3 cp = vsub(p, cc);
+        const double d5 = vdot(ab, cp);
+        const double d6 = vdot(ac, cp);
+        c.add(13);
+        if (d6 >= 0.0 && d5 <= d6) {
+          form = 0;  // vertex c
+          base = cc;
+        } else {
+          const double vb = sub(mul(d5, d2), mul(d1, d6));
+          c.add(3);
+          if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+            form = 1;  // edge ac: w = d2 / (d2 - d6)
+            dir = ac;
+            num = d2;
+            den = sub(d2, d6);
+            c.add(8);
+          } else {
+            const double va = sub(mul(d3, d6), mul(d5, d4));
+            const double d43 = sub(d4, d3);
+            const double d56 = sub(d5, d6);
+            c.add(5);
+            if (va <= 0.0 && d43 >= 0.0 && d56 >= 0.0) {
+              form = 1;  // edge bc: w = d43 / (d43 + d56), from b along c - b
+              base = b;
+              dir = vsub(cc, b);
+              num = d43;
+              den = add(d43, d56);
+              c.add(11);
+            } else {
+              form = 2;  // face: dot(ap, n) / |n|
+              c.add(12);
+            }
+          }
+        }
+      }
+    }
   }
-  const V3 cp = vsub(p, cc);
-  const double d5 = vdot(ab, cp);
-  const double d6 = vdot(ac, cp);
-  c.add(13);
-  if (d6 >= 0.0 && d5 <= d6) return dist_pp(p, cc, c);
-  const double vb = sub(mul(d5, d2), mul(d1, d6));
-  c.add(3);
-  if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
-    const double w = dvd(d2, sub(d2, d6));
-    c.add(8);
-    return dist_pp(p, vadd(a, vscale(ac, w)), c);
+  if (form == 2) {
+    num = vdot(ap, n);
+    den = sqrt_rn(nn2);
   }
-  const double va = sub(mul(d3, d6), mul(d5, d4));
-  const double d43 = sub(d4, d3);
-  const double d56 = sub(d5, d6);
-  c.add(5);
-  if (va <= 0.0 && d43 >= 0.0 && d56 >= 0.0) {
-    const double w = dvd(d43, add(d43, d56));
-    c.add(11);
-    return dist_pp(p, vadd(b, vscale(vsub(cc, b), w)), c);
-  }
-  const double nn = sqrt_rn(vdot(n, n));
-  const double sd = dvd(vdot(ap, n), nn);
-  c.add(12);
-  return fabs(sd);
+  double v = 0.0;
+  if (form != 0) v = dvd(num, den);
+  if (form == 2) return fabs(v);
+  const V3 q = form == 1 ? vadd(base, vscale(dir, v)) : base;
+  c.add(9);
+  const V3 d = vsub(p, q);
+  return sqrt_rn(vdot(d, d));
 }
 
 // DistanceSegmentSegment, certificate_engine.cpp:92-131
