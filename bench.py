@@ -441,8 +441,17 @@ class BatchWorkload:
         from p2cccd_b200.batch import BatchPipeline
 
         self.torch = torch
-        self.seed = 20261203 + rank
-        self.scenes = scenes.uneven_batch(BATCH_SCENES, seed=self.seed)
+        world = int(os.environ.get("WORLD_SIZE", "1"))
+        if BATCH_PARTITION == "lpt":  # one batch split over the ranks by triangle count (strong scaling)
+            from p2cccd_b200.batch import lpt_partition
+
+            self.seed = 20261203
+            everything = scenes.uneven_batch(BATCH_SCENES, seed=self.seed)
+            self.share = lpt_partition([len(x["faces"]) for x in everything], world)[rank]
+            self.scenes = [everything[i] for i in self.share]
+        else:  # every rank its own batch (weak scaling)
+            self.seed = 20261203 + rank
+            self.scenes = scenes.uneven_batch(BATCH_SCENES, seed=self.seed)
         self.cfg = certify.CertConfig(1e-6, 1e-6, 32)
         self.bp = BatchPipeline(self.scenes, device, exclude_self=True, config=self.cfg, streams=8)
         self.bp.step_checked()
@@ -895,6 +904,27 @@ def _max_over_ranks(world, value: float) -> float:
     return float(t.item())
 
 
+def _sum_over_ranks(world, value: float) -> float:
+    """All ranks' values added (all ranks call this in the same order)."""
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def partition_rate(world: int, units_this_rank: float, ms_this_rank: float) -> tuple[float, float]:
+    """Whole-job rate of one job split over N ranks (LPT): every rank's
+    units over the slowest rank's time.  Every rank calls it."""
+    units = _sum_over_ranks(world, units_this_rank)
+    ms = _max_over_ranks(world, ms_this_rank)
+    return units / (ms * 1e-3), ms
+
+
 def replica_rate(world: int, units_per_rank: float, ms_per_rank: float) -> tuple[float, float]:
     """Whole-job rate of N replicas: all ranks' units over the slowest rank's
     time (max over ranks), and that time.  Every rank calls it."""
@@ -1012,8 +1042,10 @@ def run_b200(args) -> dict | None:
         e2e_times = wl.e2e_pipelined(args.steps, flush, stream)
         torch.cuda.synchronize()
     ms = statistics.mean(times)
-    value, ms_max = replica_rate(world, wl.queries, ms)
-    e2e_value, e2e_ms = replica_rate(world, wl.queries, statistics.mean(e2e_times))
+    split = args.workload == "batch" and BATCH_PARTITION == "lpt"
+    rate = partition_rate if split else replica_rate
+    value, ms_max = rate(world, wl.queries, ms)
+    e2e_value, e2e_ms = rate(world, wl.queries, statistics.mean(e2e_times))
     n_kernels, kernel_names = count_kernels(torch, getattr(wl, "step_uncaptured", wl.step))
     census = wl.census()
     fp64_rate = certify.probe_fp64_rate(dev)
@@ -1067,9 +1099,11 @@ def run_b200(args) -> dict | None:
         "metric": "certified CCD queries/s", "value": value, "unit": "queries/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_max,
         "p50_ms": statistics.median(times), "p99_ms": sorted(times)[max(0, int(0.99 * len(times)) - 1)],
-        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "higher_is_better": True, "scaling": "strong" if split else "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
         "config": {**wl.config(), "l2": f"flushed between timed steps ({L2_FLUSH_BYTES >> 20} MB write)",
-                   "parallelism": f"replicas x{world}"},
+                   "parallelism": (f"one batch LPT-packed over {world} ranks by triangle count" if split
+                                   else f"replicas x{world}")},
         "queries_per_step": wl.queries,
         "e2e": {"value": e2e_value, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "ms_per_step": e2e_ms, "pipelined": e2e_times is not e2e_serial_times,
@@ -1644,6 +1678,7 @@ def run_groups(args) -> dict | None:
 
 
 BATCH_SCENES = 256  # scenes of the batch workload (--scenes)
+BATCH_PARTITION = "replica"  # --partition: "replica" (each rank its own batch) or "lpt" (one batch split by LPT)
 CLOTH_N = 513  # cloth grid of the cloth workload (--cloth-n; 513 = the dense-contact stress case)
 AUTOTUNE_REPS = 3  # graph replays per autotuner trial of the batch workload (--autotune-reps; 0 = defaults)
 REF_ARM_BUDGET_S = 150.0  # wall seconds of the whole reference arm (warm-up + timed steps)
@@ -1843,6 +1878,9 @@ def main():
     ap.add_argument("--cloth-n", type=int, default=513, help="cloth: grid vertices per side (513 = the stress config)")
     ap.add_argument("--autotune-reps", type=int, default=3,
                     help="batch: graph replays per autotuner trial (0: the library's default launch shape)")
+    ap.add_argument("--partition", default="replica", choices=["replica", "lpt"],
+                    help="batch with --gpus N: every rank its own batch (weak scaling) or one batch packed onto the "
+                         "ranks longest-processing-time first by triangle count (strong scaling)")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="serving: mean arrivals per second")
     ap.add_argument("--serve-requests", type=int, default=400, help="serving: requests per stream")
     ap.add_argument("--serve-memory-gb", type=float, default=32.0, help="serving: the server's device arena (GB)")
@@ -1858,6 +1896,8 @@ def main():
                     help="also write the run as BenchmarkRowV2 JSONL / CSV (the reference's export schema) to DIR")
     args = ap.parse_args()
     global BATCH_SCENES, AUTOTUNE_REPS, CLOTH_N, PROXY_OBJECTS, GROUP_ROWS, SERVE_SLOTS, SERVE_MAX_GROUP
+    global BATCH_PARTITION
+    BATCH_PARTITION = args.partition
     PROXY_OBJECTS = max(2, args.proxy_objects)
     SERVE_SLOTS, SERVE_MAX_GROUP = max(1, args.serve_slots), max(1, args.serve_max_group)
     GROUP_ROWS = max(1, args.group_rows)

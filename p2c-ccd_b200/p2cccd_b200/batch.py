@@ -45,6 +45,26 @@ def scene_row(st, vf_pairs: int, ee_pairs: int, vf_cap: int, ee_cap: int, counts
             ee_results, st.v_obj, st.f_obj, st.e_obj, st.nv, st.nf, st.ne, st.thickness, st.exclude_self, st.n_obj)
 
 
+def lpt_partition(weights: list[float] | np.ndarray, n_bins: int) -> list[list[int]]:
+    """Longest-processing-time-first packing of independent scenes onto
+    n_bins GPUs: scenes by decreasing weight (triangle count), each to the
+    least-loaded bin so far (ties: the lower bin); each bin's scenes in index
+    order.  The most-loaded bin holds at most 4/3 of the optimum.  Every rank
+    computes the same packing from the same weights, so no exchange is needed."""
+    import heapq
+
+    w = np.asarray(weights, dtype=np.float64)
+    if n_bins < 1:
+        raise ValueError("n_bins must be at least 1")
+    heap = [(0.0, b) for b in range(n_bins)]
+    bins: list[list[int]] = [[] for _ in range(n_bins)]
+    for i in sorted(range(len(w)), key=lambda k: (-w[k], k)):
+        load, b = heapq.heappop(heap)
+        bins[b].append(i)
+        heapq.heappush(heap, (load + float(w[i]), b))
+    return [sorted(x) for x in bins]
+
+
 def decode_batch_undecided(raw: np.ndarray) -> np.ndarray:
     """Entries (scene << 40 | (family - 1) << 39 | position) of a batch
     undecided queue as int64 rows (scene, family 1/2, pair position)."""

@@ -24,9 +24,11 @@ def _rank_main(rank: int, world: int, port: int, out):
         bench._barrier(world)
         # rank r "took" 2 + r ms for 1,000 units: the job is as slow as rank 1
         rate, ms = bench.replica_rate(world, 1000.0, 2.0 + rank)
+        # one job split over the ranks: rank r did 100 * (r + 1) units
+        prate, pms = bench.partition_rate(world, 100.0 * (rank + 1), 2.0 + rank)
         args = type("A", (), {"steps": 1, "warmup": 0, "workload": "plain"})()
         ref = bench.run_reference(args) if rank != 0 else "rank0"
-        out.put((rank, rate, ms, ref))
+        out.put((rank, rate, ms, ref, prate, pms))
     finally:
         dist.destroy_process_group()
 
@@ -42,7 +44,30 @@ def test_two_gloo_ranks_aggregate_like_the_driver():
         p.join(120)
         assert p.exitcode == 0
     res = sorted(q.get(timeout=5) for _ in range(2))
-    for rank, rate, ms, ref in res:
+    for rank, rate, ms, ref, prate, pms in res:
         assert ms == pytest.approx(3.0)                     # max over ranks
         assert rate == pytest.approx(2000.0 / 3.0e-3)       # all units / slowest time
+        assert pms == pytest.approx(3.0) and prate == pytest.approx(300.0 / 3.0e-3)
     assert res[1][3] is None                                # rank 1 of the reference arm prints nothing
+
+
+def test_lpt_partition_packs_scenes_by_triangles():
+    """The batch's longest-processing-time packing: every scene on exactly
+    one rank, each rank's load within the LPT bound (4/3 of the optimum, so
+    within the largest scene of the mean), the same packing on every rank."""
+    import numpy as np
+
+    from p2cccd_b200.batch import lpt_partition
+
+    rng = np.random.default_rng(0)
+    w = np.exp(rng.uniform(np.log(1e3), np.log(2e5), 256))
+    for n in (1, 2, 3, 8):
+        bins = lpt_partition(w, n)
+        flat = sorted(i for b in bins for i in b)
+        assert flat == list(range(256))
+        loads = [w[b].sum() for b in bins]
+        assert max(loads) <= w.sum() / n + w.max() + 1e-6
+        assert max(loads) <= 4.0 / 3.0 * max(w.sum() / n, w.max()) + 1e-6
+        assert lpt_partition(w, n) == bins
+    with pytest.raises(ValueError):
+        lpt_partition(w, 0)

@@ -81,3 +81,70 @@ def test_batch_of_256_uneven_scenes_full_size(cuda_device, oracle_mod):
             first = rvf if (rvf["status"] == 0).any() else ree
             k = int(np.nonzero(first["status"] == 0)[0][0])
             assert summ[i]["query"]["witness_index"] == k and summ[i]["query"]["status"] == 0
+
+
+def _summary_vs_row(summ, row):
+    assert summ["proposal_calls"] == row["proposal_exact_calls"]
+    assert summ["fallback_calls"] == row["fallback_exact_calls"]
+    assert summ["detected_groups"] == row["hit_count"]
+    assert summ["groups"] == row["group_count"]
+    assert summ["fallback_groups"] == row["fallback_groups"]
+    assert summ["first_hit_rank_sum"] == row["positive_first_hit_rank_sum"]
+
+
+def test_cloth_on_sphere_full_size_anyhit(cuda_device, oracle_mod):
+    """Vertex-face: the reference scene tool itself (its candidates, its
+    random-policy scores, its RunScheduledAnyHitRows) against the device
+    any-hit on the same candidates and scores.  Edge-edge (2.5 M candidates,
+    whose tool sweep alone takes minutes on one core): the device's own
+    candidates and the scheduler stub's scores, against the restated
+    procedure (pinned to the tool on smaller scenes) over the reference
+    certifier's decision for every candidate."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.anyhit import GroupAnyHit, stub_scores
+    from p2cccd_b200.certify import CertConfig
+    from p2cccd_b200.scene import ScenePipeline
+
+    if not oracle_mod.REF_TOOL_SO.exists():
+        pytest.skip("reference scene tool library not built")
+    cfg = CertConfig(A.CFG["eps_time"], A.CFG["eps_space"], A.CFG["max_depth"])
+    s = scenes.cloth_on_sphere()
+    assert len(s["faces"]) == 624_288
+    tool = oracle_mod.RefToolScene(s["v_t0"], s["v_t1"], s["faces"], 0.0, False)
+    d = dict(s)
+    d.update(edges=tool.edges, e_obj=tool.e_obj, v_obj=tool.v_obj, f_obj=tool.f_obj, n_obj=tool.n_obj)
+    pipe = ScenePipeline(d, cuda_device, exclude_self=False, config=cfg, vf_capacity=1 << 20, ee_capacity=1 << 22)
+    # vertex-face through the tool
+    vf = tool.candidates("vf")
+    scores = tool.random_scores("vf", len(vf))
+    row = tool.anyhit("vf", 4096, A.CFG["eps_time"], A.CFG["eps_space"], A.CFG["max_depth"])
+    keys = ((vf[:, 0].astype(np.int64) << 32) | vf[:, 1].astype(np.int64))
+    ah = GroupAnyHit(pipe._struct, pipe.n_obj, "vf", len(vf), cuda_device)
+    ah.run(torch.from_numpy(keys).to(cuda_device), torch.tensor([len(vf)], device=cuda_device),
+           torch.from_numpy(scores).to(cuda_device), 4096, cfg)
+    torch.cuda.synchronize(cuda_device)
+    summ = ah.read_summary()
+    assert summ["candidates"] == len(vf) == row["all_exact_calls"] and summ["error_word"] == 0
+    _summary_vs_row(summ, row)
+    # edge-edge through the device broad phase, the stub and the restated procedure
+    pipe.step_checked()
+    n_ee = int(pipe.read_counts()[1])
+    pairs = pipe.ee_pairs[:n_ee]
+    sc = torch.empty(n_ee, dtype=torch.float64, device=cuda_device)
+    stub_scores(pairs, None, 2, 97, sc)
+    ah2 = GroupAnyHit(pipe._struct, pipe.n_obj, "ee", n_ee, cuda_device)
+    ah2.run(pairs.contiguous(), torch.tensor([n_ee], device=cuda_device), sc, 4096, cfg)
+    torch.cuda.synchronize(cuda_device)
+    cands = _cands(pairs.cpu().numpy().view(np.uint64))
+    rec = A.primitives(d, tool.edges, cands, "ee")
+    res, st = oracle_mod.ref_eval_batch(rec, 0.0, 1.0, cfg.eps_time, cfg.eps_space, cfg.max_subdivision_depth,
+                                        threads=16)
+    hit = ((res["status"] != 1) | (st != 0)).astype(np.uint8)
+    groups = A.groups_of(tool, cands, "ee")
+    exp = A.expected(oracle_mod, groups, hit, sc.cpu().numpy(), tool.n_obj ** 2, 4096)
+    summ2 = ah2.read_summary()
+    assert summ2["candidates"] == n_ee > 2_000_000 and summ2["error_word"] == 0
+    _summary_vs_row(summ2, exp["row"])
+    det, pc, fc = ah2.read_groups()
+    assert np.array_equal(det, exp["detected"]) and np.array_equal(pc, exp["proposal_calls"])
+    assert np.array_equal(fc, exp["fallback_calls"])
