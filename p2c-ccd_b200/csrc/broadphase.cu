@@ -323,6 +323,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigne
   s.blo[k] = b[G.a2];
   s.bhi[k] = b[3 + G.a2];
   s.q[k] = key & kQMax;
+  s.fb[k] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
   s.id[k] = (int32_t)j;
   s.obj[k] = L.obj[l][j];
   const unsigned head = key >> kQBits;  // list and column
@@ -374,6 +375,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
   const SortedBoxes Q = from_vertex ? F : V;
   StridedWalker w;
   Box6 pb{};
+  FBox pf{};
   double lo = 0.0;
   int32_t pid = 0, pobj = 0;
   if (live) {
@@ -381,6 +383,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
     pid = P.id[i];
     pobj = P.obj[i];
     pb = box_at(P, i);
+    pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, from_vertex ? g.reach1[1] : g.reach1[0],
                         from_vertex ? g.reach2[1] : g.reach2[0], lane, kSceneSweepLanes);
     live = w.next_cell(Q, g);
@@ -391,9 +394,10 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
     unsigned long long key = 0;
     if (live) {
       const unsigned j = w.j;
+      const float4 qf = Q.fb[j];
       const double qlo = Q.lo[j];
       const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
-      if (own && overlap3(pb, qlo, Q, j)) {
+      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, Q, j)) {
         const int32_t qobj = Q.obj[j];
         const int32_t vtx = from_vertex ? pid : Q.id[j];
         const int32_t fc = from_vertex ? Q.id[j] : pid;
@@ -433,6 +437,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
   bool live = i < ne;
   StridedWalker w;
   Box6 pb{};
+  FBox pf{};
   double lo = 0.0;
   int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
   if (live) {
@@ -442,6 +447,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
     pb = box_at(E, i);
+    pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
                         kSceneSweepLanes);
     live = w.next_cell(E, g);
@@ -452,10 +458,11 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     unsigned long long key = 0;
     if (live) {
       const unsigned j = w.j;
+      const float4 qf = E.fb[j];
       const double qlo = E.lo[j];
       const int32_t oid = E.id[j];
       const bool own = qlo > lo || (qlo == lo && oid > eid);
-      if (own && overlap3(pb, qlo, E, j)) {
+      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, E, j)) {
         bool ok = true;
         if (E.obj[j] == eobj) {
           if (exclude_self) ok = false;
@@ -596,6 +603,7 @@ void carve_list(Carver& c, BoxList& L, long long n) {
   L.s.blo = c.take<double>(n);
   L.s.bhi = c.take<double>(n);
   L.s.q = c.take<unsigned>(n);
+  L.s.fb = c.take<float4>(n);
   L.s.id = c.take<int32_t>(n);
   L.s.obj = c.take<int32_t>(n);
 }

@@ -41,6 +41,7 @@ struct SortedBoxes {
   double* blo;    // min / max along the second non-sweep axis
   double* bhi;
   unsigned* q;    // quantised min along the sweep axis (the sort key's low bits)
+  float4* fb;     // the non-sweep bounds rounded outward to float: (alo down, ahi up, blo down, bhi up)
   int32_t* id;    // primitive index in the scene
   int32_t* obj;   // object id
   unsigned* cell_begin;  // [kMaxColumns^2] first entry of each column
@@ -223,6 +224,27 @@ struct Box6 {
 
 __device__ __forceinline__ Box6 box_at(const SortedBoxes& P, long long i) {
   return Box6{P.lo[i], P.hi[i], P.alo[i], P.ahi[i], P.blo[i], P.bhi[i]};
+}
+
+// A box's non-sweep bounds rounded outward to float, for the prefilter below.
+struct FBox {
+  float alo, ahi, blo, bhi;
+};
+
+__device__ __forceinline__ FBox fbox_of(const Box6& b) {
+  return FBox{__double2float_rd(b.alo), __double2float_ru(b.ahi), __double2float_rd(b.blo), __double2float_ru(b.bhi)};
+}
+
+__device__ __forceinline__ float4 fbox_entry(double alo, double ahi, double blo, double bhi) {
+  return make_float4(__double2float_rd(alo), __double2float_ru(ahi), __double2float_rd(blo), __double2float_ru(bhi));
+}
+
+// Conservative prefilter on the two non-sweep axes from one 16-byte load:
+// false only when the double boxes are disjoint there (a lower bound rounded
+// down above an upper bound rounded up orders the doubles the same way), so
+// every pair the exact test accepts passes it.
+__device__ __forceinline__ bool fmay_overlap(const FBox& p, const float4 q) {
+  return !(p.alo > q.y || q.x > p.ahi || p.blo > q.w || q.z > p.bhi);
 }
 
 // Inclusive overlap on all three axes (Overlap, :270-274); qlo is Q.lo[j],

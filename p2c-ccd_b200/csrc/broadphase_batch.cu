@@ -465,6 +465,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const un
   B.S.blo[i] = b[G.a2];
   B.S.bhi[i] = b[3 + G.a2];
   B.S.q[i] = (unsigned)(key & kBatchQMax);
+  B.S.fb[i] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
   B.S.id[i] = (int32_t)j;
   B.S.obj[i] = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[j];
   const unsigned long long head = key >> kBatchQBits;  // scene, list and column
@@ -538,6 +539,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
   if (!__any_sync(kFull, live)) return;
   StridedWalker w;
   Box6 pb{};
+  FBox pf{};
   SortedBoxes Q{};
   Grid g{};
   double lo = 0.0;
@@ -555,6 +557,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
     pid = B.S.id[i];
     pobj = B.S.obj[i];
     pb = box_at(B.S, (long long)i);
+    pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi,
                         from_vertex ? g.reach1[1] : g.reach1[0], from_vertex ? g.reach2[1] : g.reach2[0], lane,
                         kBatchSweepLanes);
@@ -566,9 +569,10 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
     unsigned long long key = 0;
     if (live) {
       const unsigned j = w.j;
+      const float4 qf = Q.fb[j];
       const double qlo = Q.lo[j];
       const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
-      if (own && overlap3(pb, qlo, Q, j)) {
+      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, Q, j)) {
         const int32_t qobj = Q.obj[j];
         const int32_t vtx = from_vertex ? pid : Q.id[j];
         const int32_t fc = from_vertex ? Q.id[j] : pid;
@@ -609,6 +613,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
   if (!__any_sync(kFull, live)) return;
   StridedWalker w;
   Box6 pb{};
+  FBox pf{};
   SortedBoxes E{};
   Grid g{};
   double lo = 0.0;
@@ -628,6 +633,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
     a0 = __ldg(edges + 2 * (long long)eid);
     a1 = __ldg(edges + 2 * (long long)eid + 1);
     pb = box_at(B.S, (long long)i);
+    pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
                         kBatchSweepLanes);
     live = w.next_cell(E, g);
@@ -638,10 +644,11 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
     unsigned long long key = 0;
     if (live) {
       const unsigned j = w.j;
+      const float4 qf = E.fb[j];
       const double qlo = E.lo[j];
       const int32_t oid = E.id[j];
       const bool own = qlo > lo || (qlo == lo && oid > eid);
-      if (own && overlap3(pb, qlo, E, j)) {
+      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, E, j)) {
         bool ok = true;
         if (E.obj[j] == eobj) {
           if (exclude_self) ok = false;
@@ -765,6 +772,7 @@ Carve carve(void* base, const p2c_batch_scene* scenes_dev, int n, const Totals& 
   B.S.blo = static_cast<double*>(take(8 * P));
   B.S.bhi = static_cast<double*>(take(8 * P));
   B.S.q = static_cast<unsigned*>(take(4 * P));
+  B.S.fb = static_cast<float4*>(take(16 * P));
   B.S.id = static_cast<int32_t*>(take(4 * P));
   B.S.obj = static_cast<int32_t*>(take(4 * P));
   B.cell_begin = static_cast<unsigned*>(take(4 * 3 * (size_t)t.cells));
