@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned 
     const double* b = L.box[l] + 6 * (g - L.off[l]);
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
-    key = ((unsigned)l << 30) | (c << kQBits) | quantise(b[G.axis], G);
+    key = ((unsigned)l << kListShift) | (c << kQBits) | quantise(b[G.axis], G);
   }
   keys[g] = key;
   vals[g] = (unsigned)g;
@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigne
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)G.seg[3]) return;
   const unsigned key = keys[i];
-  const int l = (int)(key >> 30);
+  const int l = (int)(key >> kListShift);
   const SortedBoxes s = l == 0 ? s0 : (l == 1 ? s1 : s2);
   const long long k = i - (long long)G.seg[l];
   const long long j = (long long)order[i] - L.off[l];
@@ -503,13 +503,41 @@ __global__ void unpack_pairs_kernel(unsigned long long* p, long long n, int shif
 // an unpack launch per family.
 // 512 threads x 16 keys with 7-bit digits (5 passes over a 34-bit pair key,
 // 130 KB of shared memory): measured against 1024 x 8 with 4-, 5- and 6-bit
-// digits, the fastest on the two-sphere scene.
+// digits, the fastest on the two-sphere scene.  Each block sorts only the
+// smallest power-of-two tile (512 x 2, 4, 8 or 16 keys) that holds its list's
+// count, read on the device, and writes the padding beyond it directly: a
+// radix pass costs in proportion to the keys it ranks.
 constexpr int kSmallSortThreads = 512;
 constexpr int kSmallSortItems = 16;
 constexpr int kSmallSortRadixBits = 7;
 constexpr long long kSmallSortCap = (long long)kSmallSortThreads * kSmallSortItems;
-using SmallSort = cub::BlockRadixSort<unsigned long long, kSmallSortThreads, kSmallSortItems, cub::NullType,
-                                      kSmallSortRadixBits>;
+template <int kItems>
+using SmallSortT = cub::BlockRadixSort<unsigned long long, kSmallSortThreads, kItems, cub::NullType,
+                                       kSmallSortRadixBits>;
+using SmallSort = SmallSortT<kSmallSortItems>;
+constexpr size_t kSmallSortSmem =
+    std::max(std::max(sizeof(SmallSortT<16>::TempStorage), sizeof(SmallSortT<8>::TempStorage)),
+             std::max(sizeof(SmallSortT<4>::TempStorage), sizeof(SmallSortT<2>::TempStorage)));
+
+template <int kItems>
+__device__ __forceinline__ void small_sort_tile(unsigned long long* p, long long cap, long long n, int bits, int shift,
+                                                unsigned char* smem) {
+  typename SmallSortT<kItems>::TempStorage& tmp = *reinterpret_cast<typename SmallSortT<kItems>::TempStorage*>(smem);
+  unsigned long long k[kItems];
+#pragma unroll
+  for (int u = 0; u < kItems; ++u) {
+    const long long i = (long long)threadIdx.x * kItems + u;
+    k[u] = i < n ? p[i] : ~0ull;
+  }
+  SmallSortT<kItems>(tmp).Sort(k, 0, bits);  // ~0 padding has every sorted bit set: it sorts last
+#pragma unroll
+  for (int u = 0; u < kItems; ++u) {
+    const long long i = (long long)threadIdx.x * kItems + u;
+    if (i < cap) p[i] = k[u] == ~0ull ? ~0ull : ((k[u] >> shift) << 32) | (k[u] & ((1ull << shift) - 1ull));
+  }
+  for (long long i = (long long)kSmallSortThreads * kItems + threadIdx.x; i < cap; i += kSmallSortThreads)
+    p[i] = ~0ull;  // padding beyond the tile
+}
 
 __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
     unsigned long long* vf, long long vf_cap, int vf_bits, int vf_shift, unsigned long long* ee, long long ee_cap,
@@ -517,7 +545,6 @@ __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
   pdl_wait();
   pdl_trigger();
   extern __shared__ __align__(16) unsigned char smem_sort[];
-  typename SmallSort::TempStorage& tmp = *reinterpret_cast<typename SmallSort::TempStorage*>(smem_sort);
   const bool is_vf = blockIdx.x == 0;
   unsigned long long* p = is_vf ? vf : ee;
   const long long cap = is_vf ? vf_cap : ee_cap;
@@ -525,18 +552,10 @@ __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
   const int bits = is_vf ? vf_bits : ee_bits, shift = is_vf ? vf_shift : ee_shift;
   const long long count = (long long)(is_vf ? sc->vf_count : sc->ee_count);
   const long long n = count < cap ? count : cap;
-  unsigned long long k[kSmallSortItems];
-#pragma unroll
-  for (int u = 0; u < kSmallSortItems; ++u) {
-    const long long i = (long long)threadIdx.x * kSmallSortItems + u;
-    k[u] = i < n ? p[i] : ~0ull;
-  }
-  SmallSort(tmp).Sort(k, 0, bits);  // ~0 padding has every sorted bit set: it sorts last
-#pragma unroll
-  for (int u = 0; u < kSmallSortItems; ++u) {
-    const long long i = (long long)threadIdx.x * kSmallSortItems + u;
-    if (i < cap) p[i] = k[u] == ~0ull ? ~0ull : ((k[u] >> shift) << 32) | (k[u] & ((1ull << shift) - 1ull));
-  }
+  if (n <= 2 * kSmallSortThreads) small_sort_tile<2>(p, cap, n, bits, shift, smem_sort);
+  else if (n <= 4 * kSmallSortThreads) small_sort_tile<4>(p, cap, n, bits, shift, smem_sort);
+  else if (n <= 8 * kSmallSortThreads) small_sort_tile<8>(p, cap, n, bits, shift, smem_sort);
+  else small_sort_tile<16>(p, cap, n, bits, shift, smem_sort);
 }
 
 __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long* counts) {
@@ -742,7 +761,7 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
     cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
     size_t tb = L.sort_tmp_bytes;
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, 32, s));
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, kListShift + 2, s));
     P2C_CUDA(launch_pdl(gather_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
                         (const unsigned*)k.Current(), (const unsigned*)v.Current(), L.B[0].s, L.B[1].s, L.B[2].s,
                         (const BroadScratch*)L.sc));
@@ -779,10 +798,10 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     static bool attr_set = false;  // the block sort's storage is above the 48 KB static limit
     if (!attr_set) {
       P2C_CUDA(cudaFuncSetAttribute(small_sort_pairs_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)sizeof(SmallSort::TempStorage)));
+                                    (int)kSmallSortSmem));
       attr_set = true;
     }
-    P2C_CUDA(launch_pdl(small_sort_pairs_kernel, dim3(2), dim3(kSmallSortThreads), sizeof(SmallSort::TempStorage), s,
+    P2C_CUDA(launch_pdl(small_sort_pairs_kernel, dim3(2), dim3(kSmallSortThreads), kSmallSortSmem, s,
                         vf_out, vf_cap, bit_length(scene.nv) + vf_shift, vf_shift, ee_out, ee_cap,
                         bit_length(scene.ne) + ee_shift, ee_shift, (const BroadScratch*)L.sc));
   } else if (sort_out) {

@@ -12,8 +12,12 @@ namespace p2c {
 constexpr int kMaxCullObjects = 64;  // object-envelope culling up to this many objects
 constexpr int kMaxColumns = 128;     // columns per non-sweep axis (cell id < 2^14)
 constexpr int kCellBits = 14;
-constexpr int kQBits = 16;           // quantised sweep-axis minimum
+#ifndef P2C_SCENE_QBITS
+#define P2C_SCENE_QBITS 16
+#endif
+constexpr int kQBits = P2C_SCENE_QBITS;  // quantised sweep-axis minimum
 constexpr unsigned kQMax = (1u << kQBits) - 1u;
+constexpr int kListShift = kCellBits + kQBits;  // sort key: list << kListShift | cell << kQBits | quantised min
 
 // Order-preserving maps to unsigned integers (radix-sortable keys).
 __device__ __forceinline__ unsigned long long order_key(double x) {
