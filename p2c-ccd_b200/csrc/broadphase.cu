@@ -23,10 +23,10 @@
 //      object's envelope cannot have a candidate (the scene tool's object-pair
 //      permission, PrepareScene :521-545, used as a filter);
 //   3. device-side choice of the sweep axis (smallest mean extent relative to
-//      the spread of centres), the column grid and a 16-bit quantiser of the
+//      the spread of centres), the column grid and an 8-bit quantiser of the
 //      sweep-axis minimum;
-//   4. ONE CUB radix sort of all three lists on a 32-bit key
-//      (list << 30 | column << 16 | quantised minimum; 4 onesweep passes) and
+//   4. ONE CUB radix sort of all three lists on a 24-bit key
+//      (list << 22 | column << 8 | quantised minimum; 3 onesweep passes) and
 //      a gather into per-list struct-of-arrays;
 //   5. sweeps over monotone quantised windows with exact double tests and an
 //      ownership rule so that every pair is emitted once; pairs are compacted

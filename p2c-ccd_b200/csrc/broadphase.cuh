@@ -13,7 +13,7 @@ constexpr int kMaxCullObjects = 64;  // object-envelope culling up to this many 
 constexpr int kMaxColumns = 128;     // columns per non-sweep axis (cell id < 2^14)
 constexpr int kCellBits = 14;
 #ifndef P2C_SCENE_QBITS
-#define P2C_SCENE_QBITS 16
+#define P2C_SCENE_QBITS 8
 #endif
 constexpr int kQBits = P2C_SCENE_QBITS;  // quantised sweep-axis minimum
 constexpr unsigned kQMax = (1u << kQBits) - 1u;

@@ -15,8 +15,9 @@
 //   4. one thread per scene: sweep axis, column grid (at most
 //      max(64, n/4) cells for a scene of n primitives, 128 x 128 at most),
 //      quantiser;
-//   5. ONE radix sort of 64-bit keys (scene, list, column, 14-bit quantised
-//      min: 30 + scene bits, 5 passes for up to 256 scenes) over all primitives, a gather into one struct-of-arrays in sorted
+//   5. ONE radix sort of 64-bit keys (scene, list, column, 8-bit quantised
+//      min: 24 + scene bits, 4 passes for up to 256 scenes) over all
+//      primitives, a gather into one struct-of-arrays in sorted
 //      order and per-scene column tables holding sorted positions;
 //   6. sweeps that walk only their own scene's columns, appending pairs as
 //      (scene << w | packed pair), w the widest scene's packed pair, into a buffer of the scenes' summed
@@ -44,8 +45,13 @@ constexpr int kThreads = 256;
 constexpr int kPrepThreads = 1024;
 constexpr unsigned kFull = 0xffffffffu;
 constexpr long long kMaxScenePrims = 1ll << 22;  // packed pairs of one scene stay below 2^44
-constexpr int kBatchQBits = 14;                 // quantiser of the batched key (5 radix passes)
+#ifndef P2C_BATCH_QBITS
+#define P2C_BATCH_QBITS 8
+#endif
+constexpr int kBatchQBits = P2C_BATCH_QBITS;     // quantiser of the batched key
 constexpr unsigned kBatchQMax = (1u << kBatchQBits) - 1u;
+constexpr int kBatchListShift = kCellBits + kBatchQBits;  // key: scene | list | column | quantised min
+constexpr int kBatchSceneShift = kBatchListShift + 2;
 
 inline unsigned grid_for(long long n, int threads) {
   const long long g = (n + threads - 1) / threads;
@@ -432,7 +438,8 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned l
     const double* b = B.box + 6 * g;
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
-    key = ((unsigned long long)s << 30) | ((unsigned long long)l << 28) | ((unsigned long long)c << kBatchQBits) |
+    key = ((unsigned long long)s << kBatchSceneShift) | ((unsigned long long)l << kBatchListShift) |
+          ((unsigned long long)c << kBatchQBits) |
           quantise(b[G.axis], G);
   }
   B.keys[0][g] = key;
@@ -450,8 +457,8 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const un
   if (i >= P) return;
   const unsigned long long key = keys[i];
   if (key == ~0ull) return;  // culled entries sort last
-  const int s = (int)(key >> 30);
-  const int l = (int)((key >> 28) & 3ull);
+  const int s = (int)(key >> kBatchSceneShift);
+  const int l = (int)((key >> kBatchListShift) & 3ull);
   const p2c_batch_scene& d = B.scenes[s];
   const Grid& G = B.sc[s].grid;
   const unsigned long long g = order[i];
@@ -531,9 +538,9 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
   bool from_vertex = false;
   if (i < P) {
     const unsigned long long key = keys[i];
-    const int l = key == ~0ull ? 3 : (int)((key >> 28) & 3ull);
+    const int l = key == ~0ull ? 3 : (int)((key >> kBatchListShift) & 3ull);
     live = l <= 1;
-    s = (int)(key >> 30);
+    s = (int)(key >> kBatchSceneShift);
     from_vertex = l == 0;
   }
   if (!__any_sync(kFull, live)) return;
@@ -607,8 +614,8 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
   int s = 0;
   if (i < P) {
     const unsigned long long key = keys[i];
-    live = key != ~0ull && ((key >> 28) & 3ull) == 2ull;
-    s = (int)(key >> 30);
+    live = key != ~0ull && ((key >> kBatchListShift) & 3ull) == 2ull;
+    s = (int)(key >> kBatchSceneShift);
   }
   if (!__any_sync(kFull, live)) return;
   StridedWalker w;
@@ -837,7 +844,7 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
     P2C_CUDA(cudaGetLastError());
     size_t tb = C.tmp_bytes;
     P2C_CUDA(cub::DeviceRadixSort::SortPairs(C.tmp, tb, B.keys[0], B.keys[1], B.vals[0], B.vals[1], (int)P, 0,
-                                             30 + scene_bits, s));
+                                             kBatchSceneShift + scene_bits, s));
     gather_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, B.keys[1], B.vals[1], P);
     P2C_CUDA(cudaGetLastError());
   }
