@@ -23,10 +23,10 @@
 //      object's envelope cannot have a candidate (the scene tool's object-pair
 //      permission, PrepareScene :521-545, used as a filter);
 //   3. device-side choice of the sweep axis (smallest mean extent relative to
-//      the spread of centres), the column grid and an 8-bit quantiser of the
-//      sweep-axis minimum;
-//   4. ONE CUB radix sort of all three lists on a 24-bit key
-//      (list << 22 | column << 8 | quantised minimum; 3 onesweep passes) and
+//      the spread of centres), the column grid and an 8- or 16-bit quantiser
+//      of the sweep-axis minimum (by scene size);
+//   4. ONE CUB radix sort of all three lists on a 24- or 32-bit key
+//      (list | column | quantised minimum; 3 or 4 onesweep passes) and
 //      a gather into per-list struct-of-arrays;
 //   5. sweeps over monotone quantised windows with exact double tests and an
 //      ownership rule so that every pair is emitted once; pairs are compacted
@@ -220,7 +220,7 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
 }
 
 // Sweep axis, column grid, sweep-axis quantiser and list segments (one thread).
-__global__ void grid_kernel(BroadScratch* sc) {
+__global__ void grid_kernel(BroadScratch* sc, int qbits) {
   pdl_wait();
   pdl_trigger();
   const double n = sc->count > 0 ? (double)sc->count : 1.0;
@@ -239,7 +239,8 @@ __global__ void grid_kernel(BroadScratch* sc) {
   g.axis = axis;
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
-  g.qmax = kQMax;
+  g.qbits = qbits;
+  g.qmax = (1u << qbits) - 1u;
   const int ax[3] = {g.a1, g.a2, axis};
   double base[3], inv[3];
   int cols[2] = {1, 1};
@@ -263,7 +264,7 @@ __global__ void grid_kernel(BroadScratch* sc) {
       cols[k] = c < 1 ? 1 : c;
       inv[k] = 1.0 / width;
     } else {
-      inv[k] = (range > 0.0 && isfinite(range)) ? (double)kQMax / range : 0.0;
+      inv[k] = (range > 0.0 && isfinite(range)) ? (double)g.qmax / range : 0.0;
     }
   }
   g.base1 = base[0];
@@ -295,7 +296,7 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned 
     const double* b = L.box[l] + 6 * (g - L.off[l]);
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
-    key = ((unsigned)l << kListShift) | (c << kQBits) | quantise(b[G.axis], G);
+    key = ((unsigned)l << (kCellBits + G.qbits)) | (c << G.qbits) | quantise(b[G.axis], G);
   }
   keys[g] = key;
   vals[g] = (unsigned)g;
@@ -311,7 +312,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigne
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= (long long)G.seg[3]) return;
   const unsigned key = keys[i];
-  const int l = (int)(key >> kListShift);
+  const int l = (int)(key >> (kCellBits + G.qbits));
   const SortedBoxes s = l == 0 ? s0 : (l == 1 ? s1 : s2);
   const long long k = i - (long long)G.seg[l];
   const long long j = (long long)order[i] - L.off[l];
@@ -322,14 +323,14 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigne
   s.ahi[k] = b[3 + G.a1];
   s.blo[k] = b[G.a2];
   s.bhi[k] = b[3 + G.a2];
-  s.q[k] = key & kQMax;
+  s.q[k] = key & G.qmax;
   s.fb[k] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
   s.id[k] = (int32_t)j;
   s.obj[k] = L.obj[l][j];
-  const unsigned head = key >> kQBits;  // list and column
+  const unsigned head = key >> G.qbits;  // list and column
   const unsigned cell = head & ((1u << kCellBits) - 1u);
-  if (i == (long long)G.seg[l] || (keys[i - 1] >> kQBits) != head) s.cell_begin[cell] = (unsigned)k;
-  if (i + 1 == (long long)G.seg[l + 1] || (keys[i + 1] >> kQBits) != head) s.cell_end[cell] = (unsigned)(k + 1);
+  if (i == (long long)G.seg[l] || (keys[i - 1] >> G.qbits) != head) s.cell_begin[cell] = (unsigned)k;
+  if (i + 1 == (long long)G.seg[l + 1] || (keys[i + 1] >> G.qbits) != head) s.cell_end[cell] = (unsigned)(k + 1);
 }
 
 // Warp-aggregated append of the pairs found by this iteration.
@@ -754,14 +755,15 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     P2C_CUDA(launch_pdl(classify_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists, cull, L.active,
                         L.sc));
   }
-  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc));
+  const int qbits = n <= kSmallSceneQPrims ? kQBitsSmall : kQBitsLarge;
+  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits));
   if (n > 0) {
     P2C_CUDA(launch_pdl(keys_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
                         (const unsigned char*)L.active, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));
     cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
     cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
     size_t tb = L.sort_tmp_bytes;
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, kListShift + 2, s));
+    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, kCellBits + qbits + 2, s));
     P2C_CUDA(launch_pdl(gather_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
                         (const unsigned*)k.Current(), (const unsigned*)v.Current(), L.B[0].s, L.B[1].s, L.B[2].s,
                         (const BroadScratch*)L.sc));

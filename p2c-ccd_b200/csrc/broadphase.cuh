@@ -12,12 +12,13 @@ namespace p2c {
 constexpr int kMaxCullObjects = 64;  // object-envelope culling up to this many objects
 constexpr int kMaxColumns = 128;     // columns per non-sweep axis (cell id < 2^14)
 constexpr int kCellBits = 14;
-#ifndef P2C_SCENE_QBITS
-#define P2C_SCENE_QBITS 8
-#endif
-constexpr int kQBits = P2C_SCENE_QBITS;  // quantised sweep-axis minimum
-constexpr unsigned kQMax = (1u << kQBits) - 1u;
-constexpr int kListShift = kCellBits + kQBits;  // sort key: list << kListShift | cell << kQBits | quantised min
+// Width of the quantised sweep-axis minimum in a scene's sort key
+// (list << (14 + q) | cell << q | quantised min): 8 bits keep the key at 24
+// bits (3 radix passes) for scenes up to kSmallSceneQPrims primitives, 16
+// bits (4 passes) give larger scenes - dense flat sheets above all - tighter
+// sweep windows.  Chosen on the host from the primitive count.
+constexpr int kQBitsSmall = 8, kQBitsLarge = 16;
+constexpr long long kSmallSceneQPrims = 1000000;
 
 // Order-preserving maps to unsigned integers (radix-sortable keys).
 __device__ __forceinline__ unsigned long long order_key(double x) {
@@ -68,6 +69,7 @@ struct ListStats {
 struct Grid {
   int axis, a1, a2, g1, g2;
   unsigned qmax;                    // largest quantised value (the key's quantiser field is full)
+  int qbits;                        // width of the quantiser field (scene keys)
   double base1, base2, inv1, inv2;  // column = floor((x - base) * inv)
   double base0, scale0;             // quantiser of the sweep axis: floor((x - base0) * scale0)
   double reach1[3], reach2[3];      // per list: the largest extent along a1 / a2
