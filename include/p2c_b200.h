@@ -245,7 +245,8 @@ int p2c_certify_queries(const p2c_point_triangle* pt_dev, int64_t n_pt, const in
  * holds until exit, so at most P2C_STATIC_QUEUE_MAX_QUERIES work items per call
  * (larger queues return P2C_ERR_INVALID).  The first call on a device resolves
  * the array's device address (cudaGetSymbolAddress); make that first call before
- * any stream capture.  Each call clears the scratch it uses before reading it,
+ * any stream capture.  Later calls made outside capture resolve it again (a
+ * device reset can move the array).  Each call clears the scratch it uses before reading it,
  * but all calls on a device share the one array: calls that overlap on the GPU
  * (different streams, or host threads without ordering) race and must not be
  * issued.  It calls no cudaMalloc, cudaFree or allocating library routine. */

@@ -190,9 +190,11 @@ __global__ void finalize_queries_kernel(const QueryAgg* agg, long long n_queries
 
 }  // namespace
 
-size_t queries_workspace_bytes(long long n_queries) {
+constexpr size_t queries_workspace_bytes_for(long long n_queries) {
   return ((sizeof(CertifyScratch) + 255) & ~size_t(255)) + sizeof(QueryAgg) * (size_t)(n_queries > 0 ? n_queries : 1);
 }
+
+size_t queries_workspace_bytes(long long n_queries) { return queries_workspace_bytes_for(n_queries); }
 
 }  // namespace p2c
 
@@ -270,18 +272,26 @@ namespace {
 constexpr size_t kStaticQueueScratchBytes = 1u << 20;  // 1 MiB per device, held until exit
 static __device__ __align__(256) unsigned char g_static_queue_scratch[kStaticQueueScratchBytes];
 static_assert(P2C_STATIC_QUEUE_MAX_QUERIES > 0, "capacity must be positive");
+static_assert(queries_workspace_bytes_for(P2C_STATIC_QUEUE_MAX_QUERIES) <= kStaticQueueScratchBytes,
+              "the stated maximum queue must fit the static scratch");
 
 std::mutex g_static_mu;
 void* g_static_ptr[64] = {};
 
-// Device address of the array on the current device, resolved once per
-// device (the array's host-side name is only a stand-in for it).
-int static_queue_scratch(void** out) {
+// Device address of the array on the current device (the array's host-side
+// name is only a stand-in for it).  It is resolved at the first call on a
+// device and again at every later call made outside stream capture, so a
+// device reset, which reloads the module and can move the array, never
+// leaves a stale address behind; a call under capture uses the address of
+// the last call made outside it.
+int static_queue_scratch(cudaStream_t s, void** out) {
   int dev = 0;
   P2C_CUDA(cudaGetDevice(&dev));
   if (dev < 0 || dev >= 64) return fail(P2C_ERR_CUDA, "device ordinal %d out of range", dev);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  P2C_CUDA(cudaStreamIsCapturing(s, &cap));
   std::lock_guard<std::mutex> lock(g_static_mu);
-  if (g_static_ptr[dev] == nullptr) {
+  if (g_static_ptr[dev] == nullptr || cap == cudaStreamCaptureStatusNone) {
     void* p = nullptr;
     const cudaError_t e = cudaGetSymbolAddress(&p, g_static_queue_scratch);
     if (e != cudaSuccess) return fail(P2C_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
@@ -310,7 +320,7 @@ extern "C" int p2c_certify_queries_static(const p2c_point_triangle* pt_dev, int6
   if (p2c::queries_workspace_bytes(n_queries) > p2c::kStaticQueueScratchBytes)
     return p2c::fail(P2C_ERR_INVALID, "static scratch too small for %lld work items", (long long)n_queries);
   void* scratch = nullptr;
-  const int rc = p2c::static_queue_scratch(&scratch);
+  const int rc = p2c::static_queue_scratch(p2c::as_stream(stream), &scratch);
   if (rc != P2C_OK) return rc;
   // the existing entry point clears the counters and the per-item records
   // it needs at the start of every call

@@ -90,6 +90,15 @@ def test_static_scratch_matches_workspace_entry_point_twice(cuda_device):
         assert (want[0][:, 0] <= 2).all()  # every work item got a certificate
 
 
+def test_static_scratch_at_its_stated_maximum(cuda_device):
+    """Exactly P2C_STATIC_QUEUE_MAX_QUERIES work items fit the array."""
+    queue = _queue(53, P2C_STATIC_QUEUE_MAX_QUERIES)
+    want = _run(cuda_device, queue, static=False)
+    got = _run(cuda_device, queue, static=True)
+    for a, b in zip(want, got):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_static_scratch_refuses_oversized_queue(cuda_device):
     import torch
 
