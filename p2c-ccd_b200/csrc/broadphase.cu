@@ -163,7 +163,7 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
   pdl_wait();
   pdl_trigger();
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool keep = false;
+  bool keep = false, other = false;
   int l = 3;
   double b[6] = {0, 0, 0, 0, 0, 0};
   if (g < L.off[3]) {
@@ -188,7 +188,9 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
       keep = near_other;
     }
     active[g] = keep ? 1 : 0;
+    other = keep && o != 0 && o != 1;
   }
+  if (__any_sync(kFull, other) && (threadIdx.x & 31) == 0) atomicOr(&sc->obj_other, 1ull);
   // per-list reductions; most warps hold one list only
   const int l0 = __shfl_sync(kFull, l, 0);
   const bool uniform = __all_sync(kFull, l == l0);
@@ -219,8 +221,10 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
   }
 }
 
-// Sweep axis, column grid, sweep-axis quantiser and list segments (one thread).
-__global__ void grid_kernel(BroadScratch* sc, int qbits) {
+// Sweep axis, column grid, sweep-axis quantiser and list segments (one
+// thread).  two_body: self pairs are excluded and the scene has two objects,
+// so the keys split by object unless an id other than 0 and 1 was kept.
+__global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
   pdl_wait();
   pdl_trigger();
   const double n = sc->count > 0 ? (double)sc->count : 1.0;
@@ -240,7 +244,9 @@ __global__ void grid_kernel(BroadScratch* sc, int qbits) {
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
   g.qbits = qbits;
-  g.qmax = (1u << qbits) - 1u;
+  const bool split = two_body != 0 && sc->obj_other == 0ull;
+  g.split_shift = split ? qbits - 1 : -1;
+  g.qmax = (1u << (split ? qbits - 1 : qbits)) - 1u;
   const int ax[3] = {g.a1, g.a2, axis};
   double base[3], inv[3];
   int cols[2] = {1, 1};
@@ -293,10 +299,12 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned 
   unsigned key = ~0u;
   if (active[g]) {
     const int l = L.list_of(g);
-    const double* b = L.box[l] + 6 * (g - L.off[l]);
+    const long long i = g - L.off[l];
+    const double* b = L.box[l] + 6 * i;
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
-    key = ((unsigned)l << (kCellBits + G.qbits)) | (c << G.qbits) | quantise(b[G.axis], G);
+    const int32_t o = G.split_shift >= 0 ? L.obj[l][i] : 0;
+    key = ((unsigned)l << (kCellBits + G.qbits)) | (c << G.qbits) | split_field(G, o, quantise(b[G.axis], G));
   }
   keys[g] = key;
   vals[g] = (unsigned)g;
@@ -323,7 +331,7 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigne
   s.ahi[k] = b[3 + G.a1];
   s.blo[k] = b[G.a2];
   s.bhi[k] = b[3 + G.a2];
-  s.q[k] = key & G.qmax;
+  s.q[k] = key & ((1u << G.qbits) - 1u);  // quantised min, with the object bit when split
   s.fb[k] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
   s.id[k] = (int32_t)j;
   s.obj[k] = L.obj[l][j];
@@ -386,7 +394,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
     pb = box_at(P, i);
     pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, from_vertex ? g.reach1[1] : g.reach1[0],
-                        from_vertex ? g.reach2[1] : g.reach2[0], lane, kSceneSweepLanes);
+                        from_vertex ? g.reach2[1] : g.reach2[0], lane, kSceneSweepLanes, split_prefix(g, pobj));
     live = w.next_cell(Q, g);
   }
   for (;;) {
@@ -450,7 +458,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     pb = box_at(E, i);
     pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
-                        kSceneSweepLanes);
+                        kSceneSweepLanes, split_prefix(g, eobj));
     live = w.next_cell(E, g);
   }
   for (;;) {
@@ -756,7 +764,8 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
                         L.sc));
   }
   const int qbits = n <= kSmallSceneQPrims ? kQBitsSmall : kQBitsLarge;
-  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits));
+  const int two_body = scene.exclude_self && scene.n_obj == 2 ? 1 : 0;
+  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
   if (n > 0) {
     P2C_CUDA(launch_pdl(keys_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
                         (const unsigned char*)L.active, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));

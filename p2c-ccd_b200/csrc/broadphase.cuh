@@ -68,8 +68,14 @@ struct ListStats {
 
 struct Grid {
   int axis, a1, a2, g1, g2;
-  unsigned qmax;                    // largest quantised value (the key's quantiser field is full)
-  int qbits;                        // width of the quantiser field (scene keys)
+  unsigned qmax;                    // largest quantised value
+  int qbits;                        // width of the key's low field (scene keys)
+  // Two-body split: with self pairs excluded and exactly two objects (ids 0
+  // and 1), the low field is (object << (qbits - 1)) | quantised min, so a
+  // column's entries of each object form their own sorted run and a box
+  // walks only the other object's run.  split_shift is qbits - 1 then, else
+  // -1 (the low field is the quantised min alone).
+  int split_shift;
   double base1, base2, inv1, inv2;  // column = floor((x - base) * inv)
   double base0, scale0;             // quantiser of the sweep axis: floor((x - base0) * scale0)
   double reach1[3], reach2[3];      // per list: the largest extent along a1 / a2
@@ -86,7 +92,18 @@ struct BroadScratch {
   unsigned long long vf_count;
   unsigned long long ee_count;
   unsigned long long error_word;  // bit 0: non-finite coordinate
+  unsigned long long obj_other;   // non-zero: a kept primitive's object id is neither 0 nor 1
 };
+
+// Prefix of the partner object's run in a split low field (0 unsplit): a
+// box of object o (0 or 1) walks the entries of object 1 - o.
+__device__ __forceinline__ unsigned split_prefix(const Grid& g, int32_t obj) {
+  return g.split_shift >= 0 ? (unsigned)(1 - obj) << g.split_shift : 0u;
+}
+// The low field of an entry of object obj with quantised min q.
+__device__ __forceinline__ unsigned split_field(const Grid& g, int32_t obj, unsigned q) {
+  return g.split_shift >= 0 ? ((unsigned)obj << g.split_shift) | q : q;
+}
 
 
 // ---- device helpers shared by the single-scene and batched sweeps ---------
@@ -209,7 +226,7 @@ struct StridedWalker {
 
 __device__ __forceinline__ void strided_walker_init(StridedWalker& w, const Grid& g, double lo, double hi, double alo,
                                                     double ahi, double blo, double bhi, double reach1, double reach2,
-                                                    int lane, int step) {
+                                                    int lane, int step, unsigned prefix) {
   Walker v;
   walker_init(v, g, lo, hi, alo, ahi, blo, bhi, reach1, reach2);
   w.c1a = v.c1;
@@ -219,8 +236,8 @@ __device__ __forceinline__ void strided_walker_init(StridedWalker& w, const Grid
   w.step = step;
   w.k = lane - step;
   w.j = w.j_end = 0;
-  w.q_lo = v.q_lo;
-  w.q_hi = v.q_hi;
+  w.q_lo = v.q_lo + prefix;
+  w.q_hi = v.q_hi + prefix;
 }
 
 // A scanning box held in registers for the length of its walk.

@@ -290,7 +290,7 @@ __device__ __forceinline__ void min_if_smaller(unsigned long long* p, unsigned l
 
 __global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsigned long long P) {
   const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  bool keep = false;
+  bool keep = false, other = false;
   int s = -1, l = 3;
   double b[6] = {0, 0, 0, 0, 0, 0};
   __shared__ int block_scene;
@@ -323,7 +323,9 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsign
       keep = near_other;
     }
     B.active[g] = keep ? 1 : 0;
+    other = keep && o != 0 && o != 1 && d.exclude_self && d.n_obj == 2;
   }
+  if (__any_sync(kFull, other) && other) atomicOr(&B.sc[s].obj_other, 1ull);  // only malformed two-object scenes
   // per (scene, list) extents; most warps hold one scene and one list
   unsigned todo = __ballot_sync(kFull, keep);
   while (todo) {
@@ -379,7 +381,11 @@ __global__ void grid_kernel(BatchBroad B) {
   g.axis = axis;
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
-  g.qmax = kBatchQMax;
+  g.qbits = kBatchQBits;
+  const p2c_batch_scene& d = B.scenes[s];
+  const bool split = d.exclude_self && d.n_obj == 2 && sc.obj_other == 0ull;
+  g.split_shift = split ? kBatchQBits - 1 : -1;
+  g.qmax = split ? (kBatchQMax >> 1) : kBatchQMax;
   const int ax[3] = {g.a1, g.a2, axis};
   double base[3], inv[3];
   int cols[2] = {1, 1};
@@ -403,7 +409,7 @@ __global__ void grid_kernel(BatchBroad B) {
       cols[k] = c < 1 ? 1 : c;
       inv[k] = 1.0 / width;
     } else {
-      inv[k] = (range > 0.0 && isfinite(range)) ? (double)kBatchQMax / range : 0.0;
+      inv[k] = (range > 0.0 && isfinite(range)) ? (double)g.qmax / range : 0.0;
     }
   }
   g.base1 = base[0];
@@ -438,9 +444,13 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned l
     const double* b = B.box + 6 * g;
     const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
                                   column(b[G.a2], G.base2, G.inv2, G.g2));
+    int32_t o = 0;
+    if (G.split_shift >= 0) {
+      const long long j = l == 0 ? loc : (l == 1 ? loc - d.nv : loc - d.nv - d.nf);
+      o = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[j];
+    }
     key = ((unsigned long long)s << kBatchSceneShift) | ((unsigned long long)l << kBatchListShift) |
-          ((unsigned long long)c << kBatchQBits) |
-          quantise(b[G.axis], G);
+          ((unsigned long long)c << kBatchQBits) | split_field(G, o, quantise(b[G.axis], G));
   }
   B.keys[0][g] = key;
   B.vals[0][g] = (unsigned)g;
@@ -567,7 +577,7 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const 
     pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi,
                         from_vertex ? g.reach1[1] : g.reach1[0], from_vertex ? g.reach2[1] : g.reach2[0], lane,
-                        kBatchSweepLanes);
+                        kBatchSweepLanes, split_prefix(g, pobj));
     live = w.next_cell(Q, g);
   }
   for (;;) {
@@ -642,7 +652,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const 
     pb = box_at(B.S, (long long)i);
     pf = fbox_of(pb);
     strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
-                        kBatchSweepLanes);
+                        kBatchSweepLanes, split_prefix(g, eobj));
     live = w.next_cell(E, g);
   }
   for (;;) {

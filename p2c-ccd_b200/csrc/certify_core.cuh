@@ -442,6 +442,7 @@ struct WarpSlots {
   unsigned long long coll_key[32];  // this warp's view of the leftmost collision (pruning)
   long long qidx[32];
   int family[32];
+  double nrm[4][32];                // motion norms of the slot's primitive (MotionRadius factors)
 };
 
 struct WarpStats {

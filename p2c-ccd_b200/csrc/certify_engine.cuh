@@ -75,6 +75,32 @@ struct EnginePools {
 
 constexpr int kMaxTreeDepth = 63;  // leaf keys need one bit below the deepest level
 
+// Work-sharing parameters of the loop below (compile-time):
+//   P2C_EXPORT_LANES   subtrees one warp may publish to the pool per iteration;
+//   P2C_EXPORT_FULL    1: only a warp whose lanes are all busy publishes;
+//   P2C_EXPORT_SLACK   a lane publishes when its shallowest pending level is
+//                      within this many levels of the warp's shallowest;
+//   P2C_POOL_POLL      a warp that still has busy lanes looks at the pool
+//                      every this many iterations (a fully idle warp every one);
+//   P2C_HUNGRY_PERIOD  iterations between reads of the idle-warp count (a
+//                      power of two).
+#ifndef P2C_EXPORT_LANES
+#define P2C_EXPORT_LANES 1
+#endif
+#ifndef P2C_EXPORT_FULL
+#define P2C_EXPORT_FULL 1
+#endif
+#ifndef P2C_EXPORT_SLACK
+#define P2C_EXPORT_SLACK 0
+#endif
+#ifndef P2C_POOL_POLL
+#define P2C_POOL_POLL 8
+#endif
+#ifndef P2C_HUNGRY_PERIOD
+#define P2C_HUNGRY_PERIOD 8
+#endif
+static_assert((P2C_HUNGRY_PERIOD & (P2C_HUNGRY_PERIOD - 1)) == 0, "P2C_HUNGRY_PERIOD must be a power of two");
+
 // Phase clock of one warp iteration, compiled only with -DP2C_ENGINE_PROFILE
 // (a measurement build; the library is built without it): lane 0 of every
 // warp adds the SM clock cycles spent in each phase of the loop below to
@@ -264,6 +290,8 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
               T0 = RT0;
               T1 = RT1;
               motion_norms(SlotGeo<WarpSlots>{ws, s}, nrm, ops);
+#pragma unroll
+              for (int i = 0; i < 4; ++i) ws.nrm[i][s] = nrm[i];
               phase = 0;
               path = 0ull;
               donated = 0ull;
@@ -314,8 +342,8 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
             fam = ws.family[slot];
             T0 = ws.T0[slot];
             T1 = ws.T1[slot];
-            NoCount nc;
-            motion_norms(SlotGeo<WarpSlots>{ws, slot}, nrm, nc);  // same rounded values as the owner's
+#pragma unroll
+            for (int i = 0; i < 4; ++i) nrm[i] = ws.nrm[i][slot];  // the owner's rounded values
             path = rpath;
             depth = rdepth;
             sub_depth = rdepth;
@@ -334,7 +362,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
     // ---- (C) subtrees from the global pool ------------------------------------
     if (kExport) {
       idle = __ballot_sync(FULL, slot < 0);
-      if (idle != 0u && queues_done()) {
+      if (idle != 0u && queues_done() && (idle == FULL || iter % P2C_POOL_POLL == 0u)) {
         unsigned long long h = 0;
         int take = 0;
         if (lane == 0) {
@@ -392,6 +420,8 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
             T1 = RT1;
             NoCount nc;
             motion_norms(SlotGeo<WarpSlots>{ws, s}, nrm, nc);
+#pragma unroll
+            for (int i = 0; i < 4; ++i) ws.nrm[i][s] = nrm[i];
             path = pth;
             depth = d;
             sub_depth = d;
@@ -539,7 +569,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
     P2C_PROF_MARK(7)
     // ---- (I) export pending subtrees to hungry warps ---------------------------
     if (kExport) {
-      if ((iter & 7u) == 0u) {
+      if ((iter & (P2C_HUNGRY_PERIOD - 1u)) == 0u) {
         if (lane == 0) {
           pool_hungry = (unsigned long long)volatile_load(&es->hungry.v);
           const unsigned long long rsv = volatile_load(&es->task_reserve.v), hd = volatile_load(&es->task_head.v);
@@ -549,15 +579,16 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         pool_hungry = __shfl_sync(FULL, pool_hungry, 0);
         pool_size = __shfl_sync(FULL, pool_size, 0);
       }
-      // only a warp whose lanes are all busy (nothing left to donate inside
-      // it) gives work away: one subtree per iteration, the shallowest one
-      if (busy == FULL && pool_hungry > 0ull && pool_size < pool_hungry * 4ull) {
+      // a warp whose lanes are all busy (nothing left to donate inside it)
+      // gives work away: up to P2C_EXPORT_LANES subtrees per iteration, the
+      // shallowest ones
+      if ((!P2C_EXPORT_FULL || busy == FULL) && pool_hungry > 0ull && pool_size < pool_hungry * 4ull) {
         const unsigned long long pend =
             (slot >= 0 && !done_lane && phase == 2) ? pending_levels(path, donated, depth, sub_depth) : 0ull;
         const int lvl = pend != 0ull ? __clzll((long long)pend) : 64;  // 64 - shallowest level's bit
         const int best = __reduce_min_sync(FULL, (unsigned)lvl);
-        const unsigned exporters = __ballot_sync(FULL, pend != 0ull && lvl == best);
-        const bool me = exporters != 0u && lane == __ffs((int)exporters) - 1;
+        const unsigned exporters = __ballot_sync(FULL, pend != 0ull && lvl <= best + P2C_EXPORT_SLACK);
+        const bool me = ((exporters >> lane) & 1u) != 0u && __popc(exporters & lt_mask) < P2C_EXPORT_LANES;
         if (me) {
           int gi = sa.gidx[slot];
           // a tree's first export moves its reduction from the slot to a pooled

@@ -27,7 +27,13 @@ struct CertifyScratch {
 // subtree tasks.  Task tags must read zero before each launch.
 constexpr unsigned long long kTreeAggCap = 8192;
 constexpr unsigned long long kTaskCap = 16384;
-constexpr unsigned long long kHelperWarps = 296;  // idle warps that stay for subtrees (2 per SM)
+#ifndef P2C_HELPERS_PER_SM
+#define P2C_HELPERS_PER_SM 2
+#endif
+#ifndef P2C_FETCH_PCT
+#define P2C_FETCH_PCT 100
+#endif
+constexpr unsigned long long kHelperWarps = 148ull * P2C_HELPERS_PER_SM;  // idle warps that stay for subtrees
 constexpr size_t kScratchHeaderBytes = (sizeof(CertifyScratch) + 255) & ~size_t(255);
 constexpr size_t kPoolBytes = kTreeAggCap * sizeof(TreeAgg) + kTaskCap * sizeof(SubtreeTask);
 
@@ -79,6 +85,7 @@ inline CertParams make_params(const p2c_cert_config& cfg, const LaunchShape& sha
   p.max_depth = cfg.max_subdivision_depth;
   const long long warps = (long long)shape.grid * kCertifyWarps;
   long long per_warp = warps > 0 ? (n + warps - 1) / warps : 32;
+  per_warp = (per_warp * P2C_FETCH_PCT + 99) / 100;  // queries a warp takes at first, in percent of its share
   if (per_warp < 1) per_warp = 1;
   if (per_warp > 32) per_warp = 32;
   p.fetch_limit = (int)per_warp;
