@@ -16,18 +16,21 @@
 // filed under the column of its min corner, and a box scans only the columns
 // its partners' min corners can lie in (at most 3 x 3).  Steps, all on the
 // caller's stream without host synchronisation:
-//   1. swept boxes of every vertex, face and edge (t0 and t1 positions,
-//      +thickness) in one launch, with per-axis statistics and object
-//      envelopes (reduced per warp before the atomics);
-//   2. culling: with self pairs excluded, a primitive outside every other
-//      object's envelope cannot have a candidate (the scene tool's object-pair
-//      permission, PrepareScene :521-545, used as a filter);
+//   1. vertex swept boxes (t0 and t1 positions, +thickness): object
+//      envelopes (reduced per warp before the atomics) and per-axis
+//      statistics;
+//   2. swept boxes of every vertex, face and edge and culling: with self
+//      pairs excluded, a primitive outside every other object's envelope
+//      cannot have a candidate (the scene tool's object-pair permission,
+//      PrepareScene :521-545, used as a filter); kept boxes are appended to a
+//      compact list, often a few per cent of the scene;
 //   3. device-side choice of the sweep axis (smallest mean extent relative to
 //      the spread of centres), the column grid and an 8- or 16-bit quantiser
 //      of the sweep-axis minimum (by scene size);
-//   4. ONE CUB radix sort of all three lists on a 24- or 32-bit key
-//      (list | column | quantised minimum; 3 or 4 onesweep passes) and
-//      a gather into per-list struct-of-arrays;
+//   4. ONE radix sort of the kept boxes, with their count read on the device,
+//      on a 24- or 32-bit key (list | column | low field: the quantised
+//      minimum, with the object bit of a two-body split; 3 or 4 passes) and a
+//      gather into per-list struct-of-arrays;
 //   5. sweeps over monotone quantised windows with exact double tests and an
 //      ownership rule so that every pair is emitted once; pairs are compacted
 //      per warp with a ballot and appended with one atomic per warp.
@@ -41,6 +44,7 @@
 #include <cmath>
 
 #include "broadphase.cuh"
+#include "count_sort.cuh"
 
 namespace p2c {
 namespace {
@@ -57,7 +61,6 @@ struct Lists {
   long long off[4];  // global index g: list l holds [off[l], off[l + 1])
   const int32_t* prim[3];
   const int32_t* obj[3];
-  double* box[3];
   __device__ __forceinline__ int list_of(long long g) const { return g < off[1] ? 0 : (g < off[2] ? 1 : 2); }
 };
 
@@ -73,35 +76,30 @@ __global__ void init_scratch_kernel(BroadScratch* sc) {
   }
 }
 
-// Swept boxes of all primitives (Extend/Expand/Swept*Box,
-// scene_object_envelope_native_ti_walltime.cpp:256-301) in one launch.
-__global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restrict__ v_t0,
-                                                         const double* __restrict__ v_t1, Lists L,
-                                                         double thickness, int cull_objects, BroadScratch* sc) {
+// Vertex swept boxes (Extend/Expand/SweptPointBox,
+// scene_object_envelope_native_ti_walltime.cpp:256-301): each joins its
+// object's envelope (the union of the object's vertex boxes; one atomic per
+// object per warp) and the per-axis statistics that choose the sweep axis.
+// Faces and edges are boxes of these vertices, so this pass also finds
+// every non-finite coordinate.
+__global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __restrict__ v_t0,
+                                                            const double* __restrict__ v_t1,
+                                                            const int32_t* __restrict__ v_obj, long long nv,
+                                                            double thickness, int cull_objects, BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
   __shared__ double red[9][kThreads / 32];
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   double b[6] = {0, 0, 0, 0, 0, 0};
-  bool live = g < L.off[3];
-  int l = 0, o = -1;
+  const bool live = g < nv;
+  int o = -1;
   if (live) {
-    l = L.list_of(g);
-    const long long i = g - L.off[l];
-    const bool finite = l == 0 ? swept_box<1>(v_t0, v_t1, nullptr, i, thickness, b)
-                        : l == 1 ? swept_box<3>(v_t0, v_t1, L.prim[1], i, thickness, b)
-                                 : swept_box<2>(v_t0, v_t1, L.prim[2], i, thickness, b);
-    double* dst = L.box[l] + 6 * i;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) dst[k] = b[k];
-    if (!finite) atomicOr(&sc->error_word, 1ull);
-    if (l == 0) o = L.obj[0][i];
+    if (!swept_box<1>(v_t0, v_t1, nullptr, g, thickness, b)) atomicOr(&sc->error_word, 1ull);
+    o = v_obj[g];
   }
-  // object envelopes = union of each object's vertex boxes; one atomic per
-  // object per warp
   if (cull_objects > 0) {
-    const bool mine0 = live && l == 0 && o >= 0 && o < cull_objects;
+    const bool mine0 = live && o >= 0 && o < cull_objects;
     unsigned remaining = __ballot_sync(kFull, mine0);
     while (remaining) {
       const int leader = __ffs((int)remaining) - 1;
@@ -155,11 +153,15 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(const double* __restric
   if (lane == 0 && cnt) atomicAdd(&sc->count, (unsigned long long)cnt);
 }
 
-// Keep a box unless it is a vertex in no face or (self pairs excluded) it
-// lies outside every other object's envelope.  The kept boxes' extents per
-// list size the column grid.
-__global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_objects,
-                                                            unsigned char* __restrict__ active, BroadScratch* sc) {
+// Every primitive's swept box (Swept*Box, :256-301), kept unless it is a
+// vertex in no face or (self pairs excluded) it lies outside every other
+// object's envelope.  Kept boxes are appended (one atomic per warp) to a
+// compact list of (box, primitive) entries that everything after works on;
+// their extents per list size the column grid.
+__global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict__ v_t0,
+                                                        const double* __restrict__ v_t1, Lists L, double thickness,
+                                                        int cull_objects, double* __restrict__ cbox,
+                                                        unsigned* __restrict__ cprim, BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -171,8 +173,9 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
     const long long i = g - L.off[l];
     const int o = L.obj[l][i];
     keep = !(l == 0 && o < 0);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) b[k] = L.box[l][6 * i + k];
+    if (l == 0) swept_box<1>(v_t0, v_t1, nullptr, i, thickness, b);
+    else if (l == 1) swept_box<3>(v_t0, v_t1, L.prim[1], i, thickness, b);
+    else swept_box<2>(v_t0, v_t1, L.prim[2], i, thickness, b);
     if (keep && cull_objects > 0) {
       bool near_other = false;
       for (int q = 0; q < cull_objects && !near_other; ++q) {
@@ -187,10 +190,26 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(Lists L, int cull_ob
       }
       keep = near_other;
     }
-    active[g] = keep ? 1 : 0;
     other = keep && o != 0 && o != 1;
   }
   if (__any_sync(kFull, other) && (threadIdx.x & 31) == 0) atomicOr(&sc->obj_other, 1ull);
+  {
+    const unsigned m = __ballot_sync(kFull, keep);
+    if (m != 0u) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs((int)m) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(&sc->keyed, (unsigned long long)__popc(m));
+      base = __shfl_sync(kFull, base, leader);
+      if (keep) {
+        const unsigned long long c = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
+        double* dst = cbox + 6 * c;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) dst[k] = b[k];
+        cprim[c] = (unsigned)g;
+      }
+    }
+  }
   // per-list reductions; most warps hold one list only
   const int l0 = __shfl_sync(kFull, l, 0);
   const bool uniform = __all_sync(kFull, l == l0);
@@ -288,57 +307,64 @@ __global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
   sc->grid = g;
 }
 
-__global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const unsigned char* __restrict__ active,
+// Sort key of every kept box (compact entry c, value c).  The order of the
+// compact entries does not matter: they are sorted on their full keys and
+// the pairs are sorted at the end.
+__global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const double* __restrict__ cbox,
+                                                        const unsigned* __restrict__ cprim,
                                                         unsigned* __restrict__ keys, unsigned* __restrict__ vals,
                                                         const BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
-  const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (g >= L.off[3]) return;
   const Grid& G = sc->grid;
-  unsigned key = ~0u;
-  if (active[g]) {
+  const unsigned long long n = sc->keyed;
+  for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (unsigned long long)gridDim.x * blockDim.x) {
+    const long long g = cprim[c];
     const int l = L.list_of(g);
-    const long long i = g - L.off[l];
-    const double* b = L.box[l] + 6 * i;
-    const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
-                                  column(b[G.a2], G.base2, G.inv2, G.g2));
-    const int32_t o = G.split_shift >= 0 ? L.obj[l][i] : 0;
-    key = ((unsigned)l << (kCellBits + G.qbits)) | (c << G.qbits) | split_field(G, o, quantise(b[G.axis], G));
+    const double* b = cbox + 6 * c;
+    const unsigned cell = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
+                                     column(b[G.a2], G.base2, G.inv2, G.g2));
+    const int32_t o = G.split_shift >= 0 ? L.obj[l][g - L.off[l]] : 0;
+    keys[c] = ((unsigned)l << (kCellBits + G.qbits)) | (cell << G.qbits) | split_field(G, o, quantise(b[G.axis], G));
+    vals[c] = (unsigned)c;
   }
-  keys[g] = key;
-  vals[g] = (unsigned)g;
 }
 
 // Sorted entries into per-list struct-of-arrays plus the column ranges.
-__global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const unsigned* __restrict__ keys,
+__global__ void __launch_bounds__(kThreads) gather_kernel(Lists L, const double* __restrict__ cbox,
+                                                          const unsigned* __restrict__ cprim,
+                                                          const unsigned* __restrict__ keys,
                                                           const unsigned* __restrict__ order, SortedBoxes s0,
                                                           SortedBoxes s1, SortedBoxes s2, const BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
   const Grid& G = sc->grid;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (long long)G.seg[3]) return;
-  const unsigned key = keys[i];
-  const int l = (int)(key >> (kCellBits + G.qbits));
-  const SortedBoxes s = l == 0 ? s0 : (l == 1 ? s1 : s2);
-  const long long k = i - (long long)G.seg[l];
-  const long long j = (long long)order[i] - L.off[l];
-  const double* b = L.box[l] + 6 * j;
-  s.lo[k] = b[G.axis];
-  s.hi[k] = b[3 + G.axis];
-  s.alo[k] = b[G.a1];
-  s.ahi[k] = b[3 + G.a1];
-  s.blo[k] = b[G.a2];
-  s.bhi[k] = b[3 + G.a2];
-  s.q[k] = key & ((1u << G.qbits) - 1u);  // quantised min, with the object bit when split
-  s.fb[k] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
-  s.id[k] = (int32_t)j;
-  s.obj[k] = L.obj[l][j];
-  const unsigned head = key >> G.qbits;  // list and column
-  const unsigned cell = head & ((1u << kCellBits) - 1u);
-  if (i == (long long)G.seg[l] || (keys[i - 1] >> G.qbits) != head) s.cell_begin[cell] = (unsigned)k;
-  if (i + 1 == (long long)G.seg[l + 1] || (keys[i + 1] >> G.qbits) != head) s.cell_end[cell] = (unsigned)(k + 1);
+  const long long n = (long long)G.seg[3];
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const unsigned key = keys[i];
+    const int l = (int)(key >> (kCellBits + G.qbits));
+    const SortedBoxes s = l == 0 ? s0 : (l == 1 ? s1 : s2);
+    const long long k = i - (long long)G.seg[l];
+    const unsigned c = order[i];
+    const long long j = (long long)cprim[c] - L.off[l];
+    const double* b = cbox + 6 * (long long)c;
+    s.lo[k] = b[G.axis];
+    s.hi[k] = b[3 + G.axis];
+    s.alo[k] = b[G.a1];
+    s.ahi[k] = b[3 + G.a1];
+    s.blo[k] = b[G.a2];
+    s.bhi[k] = b[3 + G.a2];
+    s.q[k] = key & ((1u << G.qbits) - 1u);  // quantised min, with the object bit when split
+    s.fb[k] = fbox_entry(b[G.a1], b[3 + G.a1], b[G.a2], b[3 + G.a2]);
+    s.id[k] = (int32_t)j;
+    s.obj[k] = L.obj[l][j];
+    const unsigned head = key >> G.qbits;  // list and column
+    const unsigned cell = head & ((1u << kCellBits) - 1u);
+    if (i == (long long)G.seg[l] || (keys[i - 1] >> G.qbits) != head) s.cell_begin[cell] = (unsigned)k;
+    if (i + 1 == (long long)G.seg[l + 1] || (keys[i + 1] >> G.qbits) != head) s.cell_end[cell] = (unsigned)(k + 1);
+  }
 }
 
 // Warp-aggregated append of the pairs found by this iteration.
@@ -365,18 +391,14 @@ constexpr int kSceneSweepLanes = 8;
 // Vertex-face pairs: boxes [0, nv) scan faces from a vertex and own the
 // pairs whose face minimum is >= the vertex minimum; boxes [nv, nv + nf)
 // scan vertices from a face and own the others.  Keys (vertex, face).
-__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
-                                                            const int32_t* __restrict__ faces, int exclude_self,
-                                                            int pack_shift, unsigned long long* out,
-                                                            unsigned long long cap, BroadScratch* sc) {
-  pdl_wait();
-  pdl_trigger();
+__device__ __forceinline__ void sweep_vf_slot(const SortedBoxes& V, const SortedBoxes& F,
+                                              const int32_t* __restrict__ faces, int exclude_self, int pack_shift,
+                                              unsigned long long* out, unsigned long long cap, BroadScratch* sc,
+                                              long long tt) {
   const Grid& g = sc->grid;
   const long long nv = (long long)(g.seg[1] - g.seg[0]), nf = (long long)(g.seg[2] - g.seg[1]);
-  const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long t = tt / kSceneSweepLanes;
   const int lane = (int)(tt % kSceneSweepLanes);
-  if ((long long)blockIdx.x * blockDim.x >= (nv + nf) * kSceneSweepLanes) return;  // whole block beyond the work
   const bool from_vertex = t < nv;
   const long long i = from_vertex ? t : t - nv;
   bool live = from_vertex || i < nf;
@@ -430,19 +452,28 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
   }
 }
 
-// Edge-edge pairs: each edge scans its own list and owns the pairs whose
-// partner minimum is larger (ties: larger edge index).  Keys (lower, higher).
-__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
-                                                            int exclude_self, int pack_shift, unsigned long long* out,
+// Every (kept box, lane) slot in a grid sized for the device (the kept
+// boxes are counted on the device).
+__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
+                                                            const int32_t* __restrict__ faces, int exclude_self,
+                                                            int pack_shift, unsigned long long* out,
                                                             unsigned long long cap, BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
+  const long long work = (long long)(sc->grid.seg[2] - sc->grid.seg[0]) * kSceneSweepLanes;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < work; base += (long long)gridDim.x * blockDim.x)
+    sweep_vf_slot(V, F, faces, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
+}
+
+// Edge-edge pairs: each edge scans its own list and owns the pairs whose
+// partner minimum is larger (ties: larger edge index).  Keys (lower, higher).
+__device__ __forceinline__ void sweep_ee_slot(const SortedBoxes& E, const int32_t* __restrict__ edges,
+                                              int exclude_self, int pack_shift, unsigned long long* out,
+                                              unsigned long long cap, BroadScratch* sc, long long tt) {
   const Grid& g = sc->grid;
   const long long ne = (long long)(g.seg[3] - g.seg[2]);
-  const long long tt = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const long long i = tt / kSceneSweepLanes;
   const int lane = (int)(tt % kSceneSweepLanes);
-  if ((long long)blockIdx.x * blockDim.x >= ne * kSceneSweepLanes) return;
   bool live = i < ne;
   StridedWalker w;
   Box6 pb{};
@@ -490,6 +521,16 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
     }
     append_pair(found, key, out, cap, &sc->ee_count);
   }
+}
+
+__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
+                                                            int exclude_self, int pack_shift, unsigned long long* out,
+                                                            unsigned long long cap, BroadScratch* sc) {
+  pdl_wait();
+  pdl_trigger();
+  const long long work = (long long)(sc->grid.seg[3] - sc->grid.seg[2]) * kSceneSweepLanes;
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < work; base += (long long)gridDim.x * blockDim.x)
+    sweep_ee_slot(E, edges, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
 }
 
 __global__ void fill_u64_kernel(unsigned long long* p, long long n, unsigned long long v) {
@@ -591,14 +632,6 @@ struct Carver {
   }
 };
 
-size_t sort_entries_temp_bytes(long long n) {
-  size_t bytes = 0;
-  cub::DoubleBuffer<unsigned> k(nullptr, nullptr);
-  cub::DoubleBuffer<unsigned> v(nullptr, nullptr);
-  cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)(n > 0 ? n : 1));
-  return bytes;
-}
-
 size_t sort_keys_temp_bytes(long long n) {
   size_t bytes = 0;
   cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
@@ -611,7 +644,10 @@ constexpr long long kCells = (long long)kMaxColumns * kMaxColumns;
 struct Layout {
   BroadScratch* sc;
   BoxList B[3];  // vertices, faces, edges
-  unsigned char* active;
+  double* cbox;     // kept boxes, compaction order
+  unsigned* cprim;  // their primitive indices
+  void* cs_scratch;
+  size_t cs_bytes;
   unsigned* keys[2];
   unsigned* vals[2];
   unsigned* cells;  // 3 lists x (begin, end) x kCells
@@ -623,7 +659,6 @@ struct Layout {
 
 void carve_list(Carver& c, BoxList& L, long long n) {
   L.n = n;
-  L.box = c.take<double>(6 * n);
   L.s.lo = c.take<double>(n);
   L.s.hi = c.take<double>(n);
   L.s.alo = c.take<double>(n);
@@ -644,7 +679,10 @@ Layout carve(void* base, long long nv, long long nf, long long ne, long long pai
   carve_list(c, L.B[0], nv);
   carve_list(c, L.B[1], nf);
   carve_list(c, L.B[2], ne);
-  L.active = c.take<unsigned char>(n);
+  L.cbox = c.take<double>(6 * n);
+  L.cprim = c.take<unsigned>(n);
+  L.cs_bytes = count_sort_scratch_bytes(n);
+  L.cs_scratch = c.take<char>((long long)L.cs_bytes);
   L.keys[0] = c.take<unsigned>(n);
   L.keys[1] = c.take<unsigned>(n);
   L.vals[0] = c.take<unsigned>(n);
@@ -654,7 +692,7 @@ Layout carve(void* base, long long nv, long long nf, long long ne, long long pai
     L.B[l].s.cell_begin = dry ? nullptr : L.cells + (2 * l) * kCells;
     L.B[l].s.cell_end = dry ? nullptr : L.cells + (2 * l + 1) * kCells;
   }
-  L.sort_tmp_bytes = std::max(sort_entries_temp_bytes(n), sort_keys_temp_bytes(pair_cap));
+  L.sort_tmp_bytes = sort_keys_temp_bytes(pair_cap);
   L.sort_tmp = c.take<char>((long long)L.sort_tmp_bytes);
   L.pair_alt = c.take<unsigned long long>(pair_cap);
   L.total = c.off + 256;
@@ -753,29 +791,34 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   lists.obj[0] = scene.v_obj;
   lists.obj[1] = scene.f_obj;
   lists.obj[2] = scene.e_obj;
-  for (int l = 0; l < 3; ++l) lists.box[l] = L.B[l].box;
+  DeviceInfo info;
+  int rc = current_device_info(&info);
+  if (rc != P2C_OK) return rc;
+  const unsigned resident = (unsigned)std::max(1, info.sm_count) * 8u;  // blocks of the device-sized loops
   P2C_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(BroadScratch), s));
   P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
   init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
-  if (n > 0) {
-    P2C_CUDA(launch_pdl(boxes_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
-                        lists, scene.thickness, cull, L.sc));
-    P2C_CUDA(launch_pdl(classify_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists, cull, L.active,
-                        L.sc));
-  }
+  if (scene.nv > 0)
+    P2C_CUDA(launch_pdl(envelope_kernel, dim3(grid_for(scene.nv, kThreads)), dim3(kThreads), 0, s, scene.v_t0,
+                        scene.v_t1, scene.v_obj, (long long)scene.nv, scene.thickness, cull, L.sc));
+  if (n > 0)
+    P2C_CUDA(launch_pdl(cull_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
+                        lists, scene.thickness, cull, L.cbox, L.cprim, L.sc));
   const int qbits = n <= kSmallSceneQPrims ? kQBitsSmall : kQBitsLarge;
   const int two_body = scene.exclude_self && scene.n_obj == 2 ? 1 : 0;
   P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
   if (n > 0) {
-    P2C_CUDA(launch_pdl(keys_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
-                        (const unsigned char*)L.active, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));
-    cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
-    cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
-    size_t tb = L.sort_tmp_bytes;
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, kCellBits + qbits + 2, s));
-    P2C_CUDA(launch_pdl(gather_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, lists,
-                        (const unsigned*)k.Current(), (const unsigned*)v.Current(), L.B[0].s, L.B[1].s, L.B[2].s,
-                        (const BroadScratch*)L.sc));
+    const unsigned loop_grid = std::min(grid_for(n, kThreads), resident);
+    P2C_CUDA(launch_pdl(keys_kernel, dim3(loop_grid), dim3(kThreads), 0, s, lists, (const double*)L.cbox,
+                        (const unsigned*)L.cprim, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));
+    bool second = false;
+    rc = count_sort_pairs(L.keys[0], L.vals[0], L.keys[1], L.vals[1], &L.sc->keyed, n, kCellBits + qbits + 2,
+                          L.cs_scratch, L.cs_bytes, s, &second);
+    if (rc != P2C_OK) return rc;
+    const int b = second ? 1 : 0;
+    P2C_CUDA(launch_pdl(gather_kernel, dim3(loop_grid), dim3(kThreads), 0, s, lists, (const double*)L.cbox,
+                        (const unsigned*)L.cprim, (const unsigned*)L.keys[b], (const unsigned*)L.vals[b], L.B[0].s,
+                        L.B[1].s, L.B[2].s, (const BroadScratch*)L.sc));
   }
   // with sorting, pairs are emitted packed so that the sort touches fewer bits
   const int vf_shift = sort_out ? std::max(1, bit_length(scene.nf)) : 0;
@@ -795,12 +838,14 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     ee_stream = fk->stream;
   }
   if (do_ee)
-    P2C_CUDA(launch_pdl(sweep_ee_kernel, dim3(grid_for(scene.ne * kSceneSweepLanes, kThreads)), dim3(kThreads), 0,
+    P2C_CUDA(launch_pdl(sweep_ee_kernel, dim3(std::min(grid_for(scene.ne * kSceneSweepLanes, kThreads), resident)),
+                        dim3(kThreads), 0,
                         ee_stream, L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out,
                         (unsigned long long)ee_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaEventRecord(fk->join, fk->stream));
   if (do_vf)
-    P2C_CUDA(launch_pdl(sweep_vf_kernel, dim3(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads)),
+    P2C_CUDA(launch_pdl(sweep_vf_kernel,
+                        dim3(std::min(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads), resident)),
                         dim3(kThreads), 0, s, L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out,
                         (unsigned long long)vf_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaStreamWaitEvent(s, fk->join, 0));

@@ -55,7 +55,6 @@ struct SortedBoxes {
 
 struct BoxList {
   long long n = 0;
-  double* box = nullptr;  // n x 6 (primitive order)
   SortedBoxes s{};
 };
 
@@ -93,6 +92,7 @@ struct BroadScratch {
   unsigned long long ee_count;
   unsigned long long error_word;  // bit 0: non-finite coordinate
   unsigned long long obj_other;   // non-zero: a kept primitive's object id is neither 0 nor 1
+  unsigned long long keyed;       // single scene: boxes kept after culling (compact entries)
 };
 
 // Prefix of the partner object's run in a split low field (0 unsplit): a

@@ -7,18 +7,23 @@
 // ~30 launches that each run for a few microseconds).  Primitives are
 // indexed scene-major (scene s holds [P[s], P[s+1]): its vertices, faces,
 // edges); every kernel finds a primitive's scene by binary search over P.
-//   1. prep (one block): prefix offsets of primitives, pair capacities and
-//      column tables per scene; per-scene scratch initialised;
-//   2. swept boxes with per-scene axis statistics and object envelopes
+//   1. prep (one block): prefix offsets of primitives, vertices, pair
+//      capacities and column tables per scene (scratch minima set by a
+//      block per scene);
+//   2. vertex swept boxes: object envelopes and per-scene axis statistics
 //      (block-level sums when a block holds one scene, warp-level otherwise);
-//   3. culling and per-scene, per-list extents;
+//   3. every primitive's swept box, culled against the other objects'
+//      envelopes; kept boxes appended to a compact list (often a few per cent
+//      of the primitives), with per-scene, per-list extents;
 //   4. one thread per scene: sweep axis, column grid (at most
 //      max(64, n/4) cells for a scene of n primitives, 128 x 128 at most),
 //      quantiser;
-//   5. ONE radix sort of 64-bit keys (scene, list, column, 8-bit quantised
-//      min: 24 + scene bits, 4 passes for up to 256 scenes) over all
-//      primitives, a gather into one struct-of-arrays in sorted
-//      order and per-scene column tables holding sorted positions;
+//   5. ONE radix sort, with the count read on the device, of the kept boxes'
+//      keys (scene, list, column, 8-bit low field: the quantised min, with
+//      the object bit of a two-body split; 24 + scene bits: 32-bit keys and 4
+//      passes for up to 256 scenes, 64-bit keys beyond), a gather into one
+//      struct-of-arrays in sorted order and per-scene column tables holding
+//      sorted positions;
 //   6. sweeps that walk only their own scene's columns, appending pairs as
 //      (scene << w | packed pair), w the widest scene's packed pair, into a buffer of the scenes' summed
 //      capacities (scene s owns its capacity's slice, pre-filled with its
@@ -34,6 +39,7 @@
 #include <vector>
 
 #include "broadphase.cuh"
+#include "count_sort.cuh"
 
 namespace p2c {
 
@@ -83,6 +89,7 @@ struct Offsets {
   unsigned long long* vf_cap;  // n + 1
   unsigned long long* ee_cap;  // n + 1
   unsigned long long* cell;    // n + 1 (cells per list; a scene's tables are 3 x its budget)
+  unsigned long long* vert;    // n + 1 (vertices)
 };
 
 struct BatchBroad {
@@ -90,23 +97,35 @@ struct BatchBroad {
   int n;
   Offsets off;
   BroadScratch* sc;          // n
-  double* box;               // 6 x P (global primitive order)
-  unsigned char* active;     // P
+  double* cbox;              // 6 x kept boxes, in compaction order
+  unsigned* cprim;           // global primitive index of each kept box
   unsigned long long* keys[2];
+  unsigned* keys32[2];       // the same buffers as 32-bit keys, used when key32 is set
+  int key32;                 // the scene, list, column and quantiser fields fit 32 bits
+  int sorted_buf;            // which of keys / vals [0] or [1] holds the sorted entries
+  unsigned long long* n_keyed;  // boxes kept after culling (the compact and sorted entries)
   unsigned* vals[2];
   SortedBoxes S;             // P entries in sorted order (cell tables unused here)
   unsigned* cell_begin;      // 3 x total cells
   unsigned* cell_end;
   unsigned long long* pack[2][2];  // vf / ee pair buffers and their sort alternates
+  uint4* chunks[2];                // queued pieces of long windows (box, first, end), per family
+  unsigned long long* chunk_count; // 2 counters
   int pair_bits[2];                // packed pair bits of the widest scene, per family
 };
 
 __device__ __forceinline__ unsigned long long pair_mask(int bits) { return (1ull << bits) - 1ull; }
 
-// Scene of global primitive g, starting from the block's first scene.
-__device__ __forceinline__ int scene_from(const BatchBroad& B, int s_lo, unsigned long long g) {
+// Sorted key i < *n_keyed from the 32- or 64-bit buffer.
+__device__ __forceinline__ unsigned long long sorted_key(const BatchBroad& B, unsigned long long i) {
+  return B.key32 ? (unsigned long long)B.keys32[B.sorted_buf][i] : B.keys[B.sorted_buf][i];
+}
+
+// Segment of g in offsets off (n segments), starting from the block's first
+// segment.
+__device__ __forceinline__ int scene_from(const unsigned long long* off, int n, int s_lo, unsigned long long g) {
   int s = s_lo;
-  while (s + 1 < B.n && __ldg(B.off.prim + s + 1) <= g) ++s;
+  while (s + 1 < n && __ldg(off + s + 1) <= g) ++s;
   return s;
 }
 
@@ -125,16 +144,24 @@ __device__ __forceinline__ int cull_count(const p2c_batch_scene& d) {
 }
 
 // ---- 1. prep -----------------------------------------------------------------
+// Minima start at ~0 and maxima at 0 (the scratch is zeroed before): one
+// block per scene.
+__global__ void init_scenes_kernel(BatchBroad B) {
+  BroadScratch& sc = B.sc[blockIdx.x];
+  for (int k = threadIdx.x; k < kMaxCullObjects * 3; k += blockDim.x) (&sc.obj_lo[0][0])[k] = ~0ull;
+  if (threadIdx.x < 9) sc.list[threadIdx.x / 3].lo_min[threadIdx.x % 3] = ~0ull;
+}
+
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(BatchBroad B) {
   using Scan = cub::BlockScan<unsigned long long, kPrepThreads>;
   __shared__ typename Scan::TempStorage tmp;
-  __shared__ unsigned long long carry[4];
-  if (threadIdx.x < 4) carry[threadIdx.x] = 0ull;
+  __shared__ unsigned long long carry[5];
+  if (threadIdx.x < 5) carry[threadIdx.x] = 0ull;
   __syncthreads();
-  unsigned long long* outs[4] = {B.off.prim, B.off.vf_cap, B.off.ee_cap, B.off.cell};
+  unsigned long long* outs[5] = {B.off.prim, B.off.vf_cap, B.off.ee_cap, B.off.cell, B.off.vert};
   for (int base = 0; base < B.n; base += kPrepThreads) {
     const int s = base + (int)threadIdx.x;
-    unsigned long long v[4] = {0ull, 0ull, 0ull, 0ull};
+    unsigned long long v[5] = {0ull, 0ull, 0ull, 0ull, 0ull};
     if (s < B.n) {
       const p2c_batch_scene& d = B.scenes[s];
       const long long np = d.nv + d.nf + d.ne;
@@ -142,19 +169,9 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(BatchBroad B) {
       v[1] = (unsigned long long)d.vf_cap;
       v[2] = (unsigned long long)d.ee_cap;
       v[3] = (unsigned long long)cell_budget(np);
-      BroadScratch& sc = B.sc[s];
-      for (int q = 0; q < kMaxCullObjects; ++q)
-        for (int a = 0; a < 3; ++a) {
-          sc.obj_lo[q][a] = ~0ull;
-          sc.obj_hi[q][a] = 0ull;
-        }
-      for (int l = 0; l < 3; ++l)
-        for (int a = 0; a < 3; ++a) {
-          sc.list[l].lo_min[a] = ~0ull;
-          sc.list[l].hi_max[a] = 0ull;
-        }
+      v[4] = (unsigned long long)d.nv;
     }
-    for (int k = 0; k < 4; ++k) {
+    for (int k = 0; k < 5; ++k) {
       unsigned long long excl = 0ull, total = 0ull;
       Scan(tmp).ExclusiveSum(v[k], excl, total);
       if (s < B.n) outs[k][s] = carry[k] + excl;
@@ -163,35 +180,35 @@ __global__ void __launch_bounds__(kPrepThreads) prep_kernel(BatchBroad B) {
       __syncthreads();
     }
   }
-  if (threadIdx.x < 4) outs[threadIdx.x][B.n] = carry[threadIdx.x];
+  if (threadIdx.x < 5) outs[threadIdx.x][B.n] = carry[threadIdx.x];
 }
 
-// ---- 2. swept boxes, statistics, envelopes -----------------------------------
-__global__ void __launch_bounds__(kThreads) boxes_kernel(BatchBroad B, unsigned long long P) {
+// ---- 2. vertex envelopes and axis statistics ----------------------------------
+// One thread per vertex of the batch (scene s holds vertices [vert[s],
+// vert[s + 1])): its swept box joins its object's envelope (order keys, one
+// atomic per object and warp) and the scene's sums of extents, centres and
+// squared centres that choose the sweep axis.  Faces and edges are boxes of
+// these vertices, so the vertex pass also finds every non-finite coordinate.
+__global__ void __launch_bounds__(kThreads) envelope_kernel(BatchBroad B, unsigned long long V) {
   __shared__ double red[9][kThreads / 32];
-  __shared__ int scene_lo, scene_hi;
+  __shared__ int scene_lo, scene_hi, block_scene;
   const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
-  const bool live = g < P;
-  int s = -1, l = 0, o = -1;
+  const bool live = g < V;
+  int s = -1, o = -1;
   double b[6] = {0, 0, 0, 0, 0, 0};
-  __shared__ int block_scene;
-  if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
+  if (threadIdx.x == 0) {
+    const unsigned long long first = (unsigned long long)blockIdx.x * blockDim.x;
+    block_scene = scene_lo = find_segment(B.off.vert, B.n, first);
+    scene_hi = find_segment(B.off.vert, B.n, min(first + blockDim.x, V) - 1ull);
+  }
   __syncthreads();
   if (live) {
-    s = scene_from(B, block_scene, g);
+    s = scene_from(B.off.vert, B.n, block_scene, g);
     const p2c_batch_scene& d = B.scenes[s];
-    const long long loc = (long long)(g - B.off.prim[s]);
-    l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
-    const long long i = l == 0 ? loc : (l == 1 ? loc - d.nv : loc - d.nv - d.nf);
-    const bool finite = l == 0 ? swept_box<1>(d.v_t0, d.v_t1, nullptr, i, d.thickness, b)
-                        : l == 1 ? swept_box<3>(d.v_t0, d.v_t1, d.faces, i, d.thickness, b)
-                                 : swept_box<2>(d.v_t0, d.v_t1, d.edges, i, d.thickness, b);
-    double* dst = B.box + 6 * g;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) dst[k] = b[k];
-    if (!finite) atomicOr(&B.sc[s].error_word, 1ull);
-    if (l == 0 && cull_count(d) > 0) o = d.v_obj[i];
+    const long long i = (long long)(g - B.off.vert[s]);
+    if (!swept_box<1>(d.v_t0, d.v_t1, nullptr, i, d.thickness, b)) atomicOr(&B.sc[s].error_word, 1ull);
+    if (cull_count(d) > 0) o = d.v_obj[i];
   }
   // object envelopes: per (scene, object) one atomic per warp
   {
@@ -229,13 +246,6 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(BatchBroad B, unsigned 
       vals[6 + a] = c * c;
     }
   }
-  if (threadIdx.x == 0) {
-    const unsigned long long first = (unsigned long long)blockIdx.x * blockDim.x;
-    const unsigned long long last = min(first + blockDim.x, P) - 1ull;
-    scene_lo = find_segment(B.off.prim, B.n, first);
-    scene_hi = find_segment(B.off.prim, B.n, last);
-  }
-  __syncthreads();
   if (scene_lo == scene_hi) {  // one scene in the block: block sums, 10 atomics
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
@@ -280,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) boxes_kernel(BatchBroad B, unsigned 
   }
 }
 
-// ---- 3. culling and per-list extents -----------------------------------------
+// ---- 3. swept boxes, culling, compaction and per-list extents ------------------
 __device__ __forceinline__ void max_if_larger(unsigned long long* p, unsigned long long v) {
   if (v > *reinterpret_cast<volatile unsigned long long*>(p)) atomicMax(p, v);
 }
@@ -288,7 +298,12 @@ __device__ __forceinline__ void min_if_smaller(unsigned long long* p, unsigned l
   if (v < *reinterpret_cast<volatile unsigned long long*>(p)) atomicMin(p, v);
 }
 
-__global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsigned long long P) {
+// One thread per primitive: its swept box; kept unless it is a vertex in no
+// face or (self pairs excluded) it lies outside every other object's
+// envelope.  Kept boxes are appended (one atomic per warp) to a compact list
+// of (box, primitive) entries that everything after works on, and their
+// extents per (scene, list) size the column grids.
+__global__ void __launch_bounds__(kThreads) cull_kernel(BatchBroad B, unsigned long long P) {
   const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
   bool keep = false, other = false;
   int s = -1, l = 3;
@@ -297,15 +312,16 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsign
   if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
   __syncthreads();
   if (g < P) {
-    s = scene_from(B, block_scene, g);
+    s = scene_from(B.off.prim, B.n, block_scene, g);
     const p2c_batch_scene& d = B.scenes[s];
     const long long loc = (long long)(g - B.off.prim[s]);
     l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
     const long long i = l == 0 ? loc : (l == 1 ? loc - d.nv : loc - d.nv - d.nf);
     const int o = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[i];
     keep = !(l == 0 && o < 0);
-#pragma unroll
-    for (int k = 0; k < 6; ++k) b[k] = B.box[6 * g + k];
+    if (l == 0) swept_box<1>(d.v_t0, d.v_t1, nullptr, i, d.thickness, b);
+    else if (l == 1) swept_box<3>(d.v_t0, d.v_t1, d.faces, i, d.thickness, b);
+    else swept_box<2>(d.v_t0, d.v_t1, d.edges, i, d.thickness, b);
     const int cull = cull_count(d);
     if (keep && cull > 0) {
       const BroadScratch& sc = B.sc[s];
@@ -322,10 +338,27 @@ __global__ void __launch_bounds__(kThreads) classify_kernel(BatchBroad B, unsign
       }
       keep = near_other;
     }
-    B.active[g] = keep ? 1 : 0;
     other = keep && o != 0 && o != 1 && d.exclude_self && d.n_obj == 2;
   }
   if (__any_sync(kFull, other) && other) atomicOr(&B.sc[s].obj_other, 1ull);  // only malformed two-object scenes
+  // compaction of the kept boxes
+  {
+    const unsigned m = __ballot_sync(kFull, keep);
+    if (m != 0u) {
+      const int lane = threadIdx.x & 31;
+      const int leader = __ffs((int)m) - 1;
+      unsigned long long base = 0;
+      if (lane == leader) base = atomicAdd(B.n_keyed, (unsigned long long)__popc(m));
+      base = __shfl_sync(kFull, base, leader);
+      if (keep) {
+        const unsigned long long c = base + (unsigned long long)__popc(m & ((1u << lane) - 1u));
+        double* dst = B.cbox + 6 * c;
+#pragma unroll
+        for (int k = 0; k < 6; ++k) dst[k] = b[k];
+        B.cprim[c] = (unsigned)g;
+      }
+    }
+  }
   // per (scene, list) extents; most warps hold one scene and one list
   unsigned todo = __ballot_sync(kFull, keep);
   while (todo) {
@@ -428,32 +461,35 @@ __global__ void grid_kernel(BatchBroad B) {
 }
 
 // ---- 5. keys, sort, gather ---------------------------------------------------------
-__global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned long long P) {
-  const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  __shared__ int block_scene;
-  if (threadIdx.x == 0) block_scene = find_segment(B.off.prim, B.n, (unsigned long long)blockIdx.x * blockDim.x);
-  __syncthreads();
-  if (g >= P) return;
-  unsigned long long key = ~0ull;
-  if (B.active[g]) {
-    const int s = scene_from(B, block_scene, g);
+// Sort key of every kept box (compact entry c, value c): the order of the
+// compact entries does not matter, they are sorted on their full keys and
+// the pairs are sorted at the end.
+__global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B) {
+  const unsigned long long n = *B.n_keyed;
+  for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
+       c += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long g = B.cprim[c];
+    const int s = find_segment(B.off.prim, B.n, g);
     const p2c_batch_scene& d = B.scenes[s];
     const long long loc = (long long)(g - B.off.prim[s]);
     const int l = loc < d.nv ? 0 : (loc < d.nv + d.nf ? 1 : 2);
     const Grid& G = B.sc[s].grid;
-    const double* b = B.box + 6 * g;
-    const unsigned c = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
-                                  column(b[G.a2], G.base2, G.inv2, G.g2));
+    const double* b = B.cbox + 6 * c;
+    const unsigned cell = (unsigned)(column(b[G.a1], G.base1, G.inv1, G.g1) * G.g2 +
+                                     column(b[G.a2], G.base2, G.inv2, G.g2));
     int32_t o = 0;
     if (G.split_shift >= 0) {
       const long long j = l == 0 ? loc : (l == 1 ? loc - d.nv : loc - d.nv - d.nf);
       o = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[j];
     }
-    key = ((unsigned long long)s << kBatchSceneShift) | ((unsigned long long)l << kBatchListShift) |
-          ((unsigned long long)c << kBatchQBits) | split_field(G, o, quantise(b[G.axis], G));
+    const unsigned long long key = ((unsigned long long)s << kBatchSceneShift) |
+                                   ((unsigned long long)l << kBatchListShift) |
+                                   ((unsigned long long)cell << kBatchQBits) |
+                                   split_field(G, o, quantise(b[G.axis], G));
+    if (B.key32) B.keys32[0][c] = (unsigned)key;
+    else B.keys[0][c] = key;
+    B.vals[0][c] = (unsigned)c;
   }
-  B.keys[0][g] = key;
-  B.vals[0][g] = (unsigned)g;
 }
 
 __device__ __forceinline__ unsigned* cell_table(const BatchBroad& B, unsigned* base, int s, int l) {
@@ -461,20 +497,18 @@ __device__ __forceinline__ unsigned* cell_table(const BatchBroad& B, unsigned* b
   return base + 3ull * c0 + (unsigned long long)l * budget;
 }
 
-__global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const unsigned long long* __restrict__ keys,
-                                                          const unsigned* __restrict__ order, unsigned long long P) {
-  const unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= P) return;
-  const unsigned long long key = keys[i];
-  if (key == ~0ull) return;  // culled entries sort last
+__device__ __forceinline__ void gather_one(const BatchBroad& B, const unsigned* __restrict__ order,
+                                           unsigned long long i, unsigned long long n) {
+  const unsigned long long key = sorted_key(B, i);
   const int s = (int)(key >> kBatchSceneShift);
   const int l = (int)((key >> kBatchListShift) & 3ull);
   const p2c_batch_scene& d = B.scenes[s];
   const Grid& G = B.sc[s].grid;
-  const unsigned long long g = order[i];
+  const unsigned c = order[i];
+  const unsigned long long g = B.cprim[c];
   const long long loc = (long long)(g - B.off.prim[s]);
   const long long j = l == 0 ? loc : (l == 1 ? loc - d.nv : loc - d.nv - d.nf);
-  const double* b = B.box + 6 * g;
+  const double* b = B.cbox + 6 * (unsigned long long)c;
   B.S.lo[i] = b[G.axis];
   B.S.hi[i] = b[3 + G.axis];
   B.S.alo[i] = b[G.a1];
@@ -487,8 +521,17 @@ __global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B, const un
   B.S.obj[i] = (l == 0 ? d.v_obj : (l == 1 ? d.f_obj : d.e_obj))[j];
   const unsigned long long head = key >> kBatchQBits;  // scene, list and column
   const unsigned cell = (unsigned)(head & ((1ull << kCellBits) - 1ull));
-  if (i == 0 || (keys[i - 1] >> kBatchQBits) != head) cell_table(B, B.cell_begin, s, l)[cell] = (unsigned)i;
-  if (i + 1 == P || (keys[i + 1] >> kBatchQBits) != head) cell_table(B, B.cell_end, s, l)[cell] = (unsigned)(i + 1);
+  if (i == 0 || (sorted_key(B, i - 1) >> kBatchQBits) != head) cell_table(B, B.cell_begin, s, l)[cell] = (unsigned)i;
+  if (i + 1 == n || (sorted_key(B, i + 1) >> kBatchQBits) != head)
+    cell_table(B, B.cell_end, s, l)[cell] = (unsigned)(i + 1);
+}
+
+__global__ void __launch_bounds__(kThreads) gather_kernel(BatchBroad B) {
+  const unsigned long long n = *B.n_keyed;
+  const unsigned* __restrict__ order = B.vals[B.sorted_buf];
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (unsigned long long)gridDim.x * blockDim.x)
+    gather_one(B, order, i, n);
 }
 
 // ---- 6. sweeps -------------------------------------------------------------------
@@ -536,153 +579,261 @@ __device__ __forceinline__ SortedBoxes scene_view(const BatchBroad& B, int s, in
 // work; 256 uneven scenes: 11.4 ms with 1 lane, 11.1 with 2, 12.2 with 4).
 constexpr int kBatchSweepLanes = 2;
 
+// Long windows: a lane that has tested kChunk entries of one column's window
+// and is not through it hands the rest to the chunk queue in pieces of
+// kChunk entries, which a second launch spreads over the whole GPU.  A few
+// boxes long along the sweep axis (swept far during the step) have windows
+// of hundreds of partners; walked by one lane they set the length of the
+// whole launch.  When the queue is full the lane walks on by itself.
+constexpr unsigned kChunk = 32;
+constexpr unsigned long long kChunkCap = 1ull << 20;  // chunks per family
+
+// A scanning box of the vertex-face sweep and the partner list it walks.
+struct VfScan {
+  Box6 pb;
+  FBox pf;
+  double lo;
+  int32_t pid, pobj;
+  bool from_vertex;
+  int exclude_self, shift;
+  const int32_t* faces;
+  SortedBoxes Q;
+};
+
+__device__ __forceinline__ void vf_scan_at(const BatchBroad& B, unsigned long long i, int s, bool from_vertex,
+                                           VfScan& c) {
+  const p2c_batch_scene& d = B.scenes[s];
+  c.Q = scene_view(B, s, from_vertex ? 1 : 0);
+  c.from_vertex = from_vertex;
+  c.faces = d.faces;
+  c.exclude_self = d.exclude_self;
+  c.shift = max(1, bit_length_dev(d.nf));
+  c.lo = B.S.lo[i];
+  c.pid = B.S.id[i];
+  c.pobj = B.S.obj[i];
+  c.pb = box_at(B.S, (long long)i);
+  c.pf = fbox_of(c.pb);
+}
+
+// Partner entry j: a pair this box owns, overlapping on all axes and allowed
+// by the object rules (the reference's BuildVFCandidates conditions).
+__device__ __forceinline__ bool vf_test(const VfScan& c, unsigned j, unsigned long long& key) {
+  const float4 qf = c.Q.fb[j];
+  const double qlo = c.Q.lo[j];
+  const bool own = c.from_vertex ? (qlo >= c.lo) : (qlo > c.lo);
+  if (!(own && fmay_overlap(c.pf, qf) && overlap3(c.pb, qlo, c.Q, j))) return false;
+  const int32_t qobj = c.Q.obj[j];
+  const int32_t vtx = c.from_vertex ? c.pid : c.Q.id[j];
+  const int32_t fc = c.from_vertex ? c.Q.id[j] : c.pid;
+  if (c.pobj == qobj) {
+    if (c.exclude_self) return false;
+    const int32_t* fv = c.faces + 3 * (long long)fc;
+    if (__ldg(fv) == vtx || __ldg(fv + 1) == vtx || __ldg(fv + 2) == vtx) return false;
+  }
+  key = pair_key((unsigned)vtx, (unsigned)fc, c.shift);
+  return true;
+}
+
+// A scanning edge of the edge-edge sweep.
+struct EeScan {
+  Box6 pb;
+  FBox pf;
+  double lo;
+  int32_t eid, eobj, a0, a1;
+  int exclude_self, shift;
+  const int32_t* edges;
+  SortedBoxes E;
+};
+
+__device__ __forceinline__ void ee_scan_at(const BatchBroad& B, unsigned long long i, int s, EeScan& c) {
+  const p2c_batch_scene& d = B.scenes[s];
+  c.E = scene_view(B, s, 2);
+  c.edges = d.edges;
+  c.exclude_self = d.exclude_self;
+  c.shift = max(1, bit_length_dev(d.ne));
+  c.lo = B.S.lo[i];
+  c.eid = B.S.id[i];
+  c.eobj = B.S.obj[i];
+  c.a0 = __ldg(c.edges + 2 * (long long)c.eid);
+  c.a1 = __ldg(c.edges + 2 * (long long)c.eid + 1);
+  c.pb = box_at(B.S, (long long)i);
+  c.pf = fbox_of(c.pb);
+}
+
+__device__ __forceinline__ bool ee_test(const EeScan& c, unsigned j, unsigned long long& key) {
+  const float4 qf = c.E.fb[j];
+  const double qlo = c.E.lo[j];
+  const int32_t oid = c.E.id[j];
+  const bool own = qlo > c.lo || (qlo == c.lo && oid > c.eid);
+  if (!(own && fmay_overlap(c.pf, qf) && overlap3(c.pb, qlo, c.E, j))) return false;
+  if (c.E.obj[j] == c.eobj) {
+    if (c.exclude_self) return false;
+    const int32_t b0 = __ldg(c.edges + 2 * (long long)oid), b1 = __ldg(c.edges + 2 * (long long)oid + 1);
+    if (c.a0 == b0 || c.a0 == b1 || c.a1 == b0 || c.a1 == b1) return false;
+  }
+  key = pair_key((unsigned)min(c.eid, oid), (unsigned)max(c.eid, oid), c.shift);
+  return true;
+}
+
+// Hand the rest of the current window, from w.j on, to the chunk queue.
+// Returns false (the lane walks on by itself) when the queue is full.
+__device__ __forceinline__ bool offload_window(StridedWalker& w, const SortedBoxes& Q, unsigned long long box,
+                                               uint4* queue, unsigned long long* queue_count) {
+  unsigned b = w.j, e = w.j_end;
+  while (b < e) {  // first entry past the window
+    const unsigned m = (b + e) >> 1;
+    if (Q.q[m] <= w.q_hi) b = m + 1;
+    else e = m;
+  }
+  const unsigned je = b;
+  const unsigned long long pieces = (je - w.j + kChunk - 1) / kChunk;
+  const unsigned long long base = atomicAdd(queue_count, pieces);
+  if (base + pieces > kChunkCap) {
+    for (unsigned long long k = base; k < kChunkCap; ++k) queue[k] = make_uint4(0u, 0u, 0u, 0u);  // empty
+    return false;
+  }
+  for (unsigned long long k = 0; k < pieces; ++k) {
+    const unsigned jb = w.j + (unsigned)k * kChunk;
+    queue[base + k] = make_uint4((unsigned)box, jb, min(jb + kChunk, je), 0u);
+  }
+  return true;
+}
+
 // Vertex-face pairs, ownership as in the single-scene sweep: a vertex owns
 // the pairs whose face minimum is >= its minimum, a face the others.
-__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B, const unsigned long long* __restrict__ keys,
-                                                            unsigned long long P) {
-  const unsigned long long tt = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sweep_vf_slot(const BatchBroad& B, unsigned long long tt, unsigned long long P) {
   const unsigned long long i = tt / kBatchSweepLanes;
   const int lane = (int)(tt % kBatchSweepLanes);
   bool live = false;
   int s = 0;
   bool from_vertex = false;
   if (i < P) {
-    const unsigned long long key = keys[i];
-    const int l = key == ~0ull ? 3 : (int)((key >> kBatchListShift) & 3ull);
+    const unsigned long long key = sorted_key(B, i);
+    const int l = (int)((key >> kBatchListShift) & 3ull);
     live = l <= 1;
     s = (int)(key >> kBatchSceneShift);
     from_vertex = l == 0;
   }
   if (!__any_sync(kFull, live)) return;
   StridedWalker w;
-  Box6 pb{};
-  FBox pf{};
-  SortedBoxes Q{};
-  Grid g{};
-  double lo = 0.0;
-  int32_t pid = 0, pobj = 0;
-  int shift = 1, exclude_self = 1;
-  const int32_t* faces = nullptr;
+  VfScan c;
+  unsigned run = 0;  // entries of the current window tested here
   if (live) {
-    const p2c_batch_scene& d = B.scenes[s];
-    g = B.sc[s].grid;
-    Q = scene_view(B, s, from_vertex ? 1 : 0);
-    faces = d.faces;
-    exclude_self = d.exclude_self;
-    shift = max(1, bit_length_dev(d.nf));
-    lo = B.S.lo[i];
-    pid = B.S.id[i];
-    pobj = B.S.obj[i];
-    pb = box_at(B.S, (long long)i);
-    pf = fbox_of(pb);
-    strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi,
+    vf_scan_at(B, i, s, from_vertex, c);
+    const Grid& g = B.sc[s].grid;
+    strided_walker_init(w, g, c.lo, c.pb.hi, c.pb.alo, c.pb.ahi, c.pb.blo, c.pb.bhi,
                         from_vertex ? g.reach1[1] : g.reach1[0], from_vertex ? g.reach2[1] : g.reach2[0], lane,
-                        kBatchSweepLanes, split_prefix(g, pobj));
-    live = w.next_cell(Q, g);
+                        kBatchSweepLanes, split_prefix(g, c.pobj));
+    live = w.next_cell(c.Q, g);
   }
   for (;;) {
     if (!__any_sync(kFull, live)) break;
     bool found = false;
     unsigned long long key = 0;
     if (live) {
-      const unsigned j = w.j;
-      const float4 qf = Q.fb[j];
-      const double qlo = Q.lo[j];
-      const bool own = from_vertex ? (qlo >= lo) : (qlo > lo);
-      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, Q, j)) {
-        const int32_t qobj = Q.obj[j];
-        const int32_t vtx = from_vertex ? pid : Q.id[j];
-        const int32_t fc = from_vertex ? Q.id[j] : pid;
-        bool ok = true;
-        if (pobj == qobj) {
-          if (exclude_self) ok = false;
-          else {
-            const int32_t* fv = faces + 3 * (long long)fc;
-            ok = !(__ldg(fv) == vtx || __ldg(fv + 1) == vtx || __ldg(fv + 2) == vtx);
-          }
-        }
-        if (ok) {
-          found = true;
-          key = pair_key((unsigned)vtx, (unsigned)fc, shift);
+      found = vf_test(c, w.j, key);
+      ++w.j;
+      if (w.j >= w.j_end || c.Q.q[w.j] > w.q_hi) {
+        live = w.next_cell(c.Q, B.sc[s].grid);
+        run = 0;
+      } else if (++run == kChunk) {
+        if (offload_window(w, c.Q, i, B.chunks[0], B.chunk_count + 0)) {
+          live = w.next_cell(c.Q, B.sc[s].grid);
+          run = 0;
         }
       }
-      ++w.j;
-      if (w.j >= w.j_end || Q.q[w.j] > w.q_hi) live = w.next_cell(Q, g);
     }
     append_scene_pair(found, s, key, B.pack[0][0], B.off.vf_cap, B.sc, true, B.pair_bits[0]);
   }
 }
 
+// Every (kept box, lane) slot, in a grid sized for the device: the number of
+// kept boxes is known only here.
+__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B) {
+  const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < work;
+       base += (unsigned long long)gridDim.x * blockDim.x)
+    sweep_vf_slot(B, base + threadIdx.x, n);
+}
+
 // Edge-edge pairs: an edge owns the pairs whose partner minimum is larger
 // (ties: larger edge index).
-__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B, const unsigned long long* __restrict__ keys,
-                                                            unsigned long long P) {
-  const unsigned long long tt = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void sweep_ee_slot(const BatchBroad& B, unsigned long long tt, unsigned long long P) {
   const unsigned long long i = tt / kBatchSweepLanes;
   const int lane = (int)(tt % kBatchSweepLanes);
   bool live = false;
   int s = 0;
   if (i < P) {
-    const unsigned long long key = keys[i];
-    live = key != ~0ull && ((key >> kBatchListShift) & 3ull) == 2ull;
+    const unsigned long long key = sorted_key(B, i);
+    live = ((key >> kBatchListShift) & 3ull) == 2ull;
     s = (int)(key >> kBatchSceneShift);
   }
   if (!__any_sync(kFull, live)) return;
   StridedWalker w;
-  Box6 pb{};
-  FBox pf{};
-  SortedBoxes E{};
-  Grid g{};
-  double lo = 0.0;
-  int32_t eid = 0, eobj = 0, a0 = 0, a1 = 0;
-  int shift = 1, exclude_self = 1;
-  const int32_t* edges = nullptr;
+  EeScan c;
+  unsigned run = 0;
   if (live) {
-    const p2c_batch_scene& d = B.scenes[s];
-    g = B.sc[s].grid;
-    E = scene_view(B, s, 2);
-    edges = d.edges;
-    exclude_self = d.exclude_self;
-    shift = max(1, bit_length_dev(d.ne));
-    lo = B.S.lo[i];
-    eid = B.S.id[i];
-    eobj = B.S.obj[i];
-    a0 = __ldg(edges + 2 * (long long)eid);
-    a1 = __ldg(edges + 2 * (long long)eid + 1);
-    pb = box_at(B.S, (long long)i);
-    pf = fbox_of(pb);
-    strided_walker_init(w, g, lo, pb.hi, pb.alo, pb.ahi, pb.blo, pb.bhi, g.reach1[2], g.reach2[2], lane,
-                        kBatchSweepLanes, split_prefix(g, eobj));
-    live = w.next_cell(E, g);
+    ee_scan_at(B, i, s, c);
+    const Grid& g = B.sc[s].grid;
+    strided_walker_init(w, g, c.lo, c.pb.hi, c.pb.alo, c.pb.ahi, c.pb.blo, c.pb.bhi, g.reach1[2], g.reach2[2], lane,
+                        kBatchSweepLanes, split_prefix(g, c.eobj));
+    live = w.next_cell(c.E, g);
   }
   for (;;) {
     if (!__any_sync(kFull, live)) break;
     bool found = false;
     unsigned long long key = 0;
     if (live) {
-      const unsigned j = w.j;
-      const float4 qf = E.fb[j];
-      const double qlo = E.lo[j];
-      const int32_t oid = E.id[j];
-      const bool own = qlo > lo || (qlo == lo && oid > eid);
-      if (own && fmay_overlap(pf, qf) && overlap3(pb, qlo, E, j)) {
-        bool ok = true;
-        if (E.obj[j] == eobj) {
-          if (exclude_self) ok = false;
-          else {
-            const int32_t b0 = __ldg(edges + 2 * (long long)oid), b1 = __ldg(edges + 2 * (long long)oid + 1);
-            ok = !(a0 == b0 || a0 == b1 || a1 == b0 || a1 == b1);
-          }
-        }
-        if (ok) {
-          found = true;
-          key = pair_key((unsigned)min(eid, oid), (unsigned)max(eid, oid), shift);
+      found = ee_test(c, w.j, key);
+      ++w.j;
+      if (w.j >= w.j_end || c.E.q[w.j] > w.q_hi) {
+        live = w.next_cell(c.E, B.sc[s].grid);
+        run = 0;
+      } else if (++run == kChunk) {
+        if (offload_window(w, c.E, i, B.chunks[1], B.chunk_count + 1)) {
+          live = w.next_cell(c.E, B.sc[s].grid);
+          run = 0;
         }
       }
-      ++w.j;
-      if (w.j >= w.j_end || E.q[w.j] > w.q_hi) live = w.next_cell(E, g);
     }
     append_scene_pair(found, s, key, B.pack[1][0], B.off.ee_cap, B.sc, false, B.pair_bits[1]);
+  }
+}
+
+__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B) {
+  const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < work;
+       base += (unsigned long long)gridDim.x * blockDim.x)
+    sweep_ee_slot(B, base + threadIdx.x, n);
+}
+
+// The queued pieces of long windows, one lane each (at most kChunk entries).
+template <int kFamily>
+__global__ void __launch_bounds__(kThreads) chunk_kernel(BatchBroad B) {
+  const unsigned long long n = min(B.chunk_count[kFamily - 1], kChunkCap);
+  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n;
+       base += (unsigned long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = base + threadIdx.x;
+    uint4 item = make_uint4(0u, 0u, 0u, 0u);
+    if (k < n) item = B.chunks[kFamily - 1][k];
+    const bool live = item.z > item.y;
+    int s = 0;
+    VfScan cv;
+    EeScan ce;
+    if (live) {
+      const unsigned long long key = sorted_key(B, item.x);
+      s = (int)(key >> kBatchSceneShift);
+      if (kFamily == 1) vf_scan_at(B, item.x, s, ((key >> kBatchListShift) & 3ull) == 0ull, cv);
+      else ee_scan_at(B, item.x, s, ce);
+    }
+    for (unsigned t = 0; t < kChunk; ++t) {
+      const unsigned j = item.y + t;
+      bool found = false;
+      unsigned long long key = 0;
+      if (live && j < item.z) found = kFamily == 1 ? vf_test(cv, j, key) : ee_test(ce, j, key);
+      if (kFamily == 1) append_scene_pair(found, s, key, B.pack[0][0], B.off.vf_cap, B.sc, true, B.pair_bits[0]);
+      else append_scene_pair(found, s, key, B.pack[1][0], B.off.ee_cap, B.sc, false, B.pair_bits[1]);
+    }
   }
 }
 
@@ -721,7 +872,7 @@ __global__ void export_counts_kernel(BatchBroad B) {
 
 // ---- workspace ---------------------------------------------------------------------
 struct Totals {
-  unsigned long long P = 0, vf = 0, ee = 0, cells = 0;
+  unsigned long long P = 0, V = 0, vf = 0, ee = 0, cells = 0;
   int pair_bits[2] = {2, 2};  // widest packed pair of any scene: vf, ee
 };
 
@@ -730,6 +881,7 @@ Totals totals_of(const p2c_batch_scene* h, int n) {
   for (int s = 0; s < n; ++s) {
     const long long np = h[s].nv + h[s].nf + h[s].ne;
     t.P += (unsigned long long)np;
+    t.V += (unsigned long long)h[s].nv;
     t.vf += (unsigned long long)h[s].vf_cap;
     t.ee += (unsigned long long)h[s].ee_cap;
     t.cells += (unsigned long long)cell_budget(np);
@@ -740,10 +892,8 @@ Totals totals_of(const p2c_batch_scene* h, int n) {
 }
 
 size_t sort_temp_bytes(const Totals& t) {
-  size_t a = 0, b = 0, c = 0;
-  const int np = (int)std::max<unsigned long long>(t.P, 1ull);
-  cub::DeviceRadixSort::SortPairs(nullptr, a, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
-                                  (const unsigned*)nullptr, (unsigned*)nullptr, np);
+  size_t b = 0, c = 0;
+  const size_t a = count_sort_scratch_bytes((long long)std::max<unsigned long long>(t.P, 1ull));
   cub::DeviceRadixSort::SortKeys(nullptr, b, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                  (int)std::max<unsigned long long>(t.vf, 1ull));
   cub::DeviceRadixSort::SortKeys(nullptr, c, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
@@ -776,10 +926,19 @@ Carve carve(void* base, const p2c_batch_scene* scenes_dev, int n, const Totals& 
   B.off.ee_cap = static_cast<unsigned long long*>(take(8 * (size_t)(n + 1)));
   B.off.cell = static_cast<unsigned long long*>(take(8 * (size_t)(n + 1)));
   B.sc = static_cast<BroadScratch*>(take(sizeof(BroadScratch) * (size_t)n));
-  B.box = static_cast<double*>(take(48 * P));
-  B.active = static_cast<unsigned char*>(take(P));
+  B.off.vert = static_cast<unsigned long long*>(take(8 * (size_t)(n + 1)));
+  B.cbox = static_cast<double*>(take(48 * P));
+  B.cprim = static_cast<unsigned*>(take(4 * P));
   B.keys[0] = static_cast<unsigned long long*>(take(8 * P));
   B.keys[1] = static_cast<unsigned long long*>(take(8 * P));
+  B.keys32[0] = reinterpret_cast<unsigned*>(B.keys[0]);
+  B.keys32[1] = reinterpret_cast<unsigned*>(B.keys[1]);
+  B.key32 = 0;
+  B.sorted_buf = 0;
+  B.n_keyed = static_cast<unsigned long long*>(take(8));
+  B.chunk_count = static_cast<unsigned long long*>(take(16));
+  B.chunks[0] = static_cast<uint4*>(take(16 * kChunkCap));
+  B.chunks[1] = static_cast<uint4*>(take(16 * kChunkCap));
   B.vals[0] = static_cast<unsigned*>(take(4 * P));
   B.vals[1] = static_cast<unsigned*>(take(4 * P));
   B.S.lo = static_cast<double*>(take(8 * P));
@@ -835,27 +994,38 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   Carve C = carve(ws, dev, n, t);
   BatchBroad& B = C.B;
   const int scene_bits = std::max(1, bit_length(n - 1));
+  const int key_bits = kBatchSceneShift + scene_bits;
+  B.key32 = key_bits <= 32 ? 1 : 0;  // up to 256 scenes: 32-bit keys halve the key traffic of the sort
   B.pair_bits[0] = t.pair_bits[0];
   B.pair_bits[1] = t.pair_bits[1];
   P2C_CUDA(cudaMemsetAsync(B.sc, 0, sizeof(BroadScratch) * (size_t)n, s));
   P2C_CUDA(cudaMemsetAsync(B.cell_begin, 0, 4 * 3 * (size_t)t.cells, s));
   P2C_CUDA(cudaMemsetAsync(B.cell_end, 0, 4 * 3 * (size_t)t.cells, s));
+  P2C_CUDA(cudaMemsetAsync(B.n_keyed, 0, sizeof(unsigned long long), s));
+  P2C_CUDA(cudaMemsetAsync(B.chunk_count, 0, 2 * sizeof(unsigned long long), s));
+  init_scenes_kernel<<<n, 128, 0, s>>>(B);
   prep_kernel<<<1, kPrepThreads, 0, s>>>(B);
   P2C_CUDA(cudaGetLastError());
   const unsigned long long P = t.P;
-  if (P > 0) {
-    boxes_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, P);
-    classify_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, P);
-  }
+  if (t.V > 0) envelope_kernel<<<grid_for((long long)t.V, kThreads), kThreads, 0, s>>>(B, t.V);
+  if (P > 0) cull_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, P);
   grid_kernel<<<grid_for(n, 128), 128, 0, s>>>(B);
   P2C_CUDA(cudaGetLastError());
+  DeviceInfo info;
+  int rc = current_device_info(&info);
+  if (rc != P2C_OK) return rc;
+  const unsigned resident = (unsigned)std::max(1, info.sm_count) * 8u;  // blocks of the device-sized loops
   if (P > 0) {
-    keys_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, P);
+    keys_kernel<<<std::min(grid_for((long long)P, kThreads), resident), kThreads, 0, s>>>(B);
     P2C_CUDA(cudaGetLastError());
-    size_t tb = C.tmp_bytes;
-    P2C_CUDA(cub::DeviceRadixSort::SortPairs(C.tmp, tb, B.keys[0], B.keys[1], B.vals[0], B.vals[1], (int)P, 0,
-                                             kBatchSceneShift + scene_bits, s));
-    gather_kernel<<<grid_for((long long)P, kThreads), kThreads, 0, s>>>(B, B.keys[1], B.vals[1], P);
+    bool second = false;
+    rc = B.key32 ? count_sort_pairs(B.keys32[0], B.vals[0], B.keys32[1], B.vals[1], B.n_keyed, (long long)P, key_bits,
+                                    C.tmp, C.tmp_bytes, s, &second)
+                 : count_sort_pairs(B.keys[0], B.vals[0], B.keys[1], B.vals[1], B.n_keyed, (long long)P, key_bits,
+                                    C.tmp, C.tmp_bytes, s, &second);
+    if (rc != P2C_OK) return rc;
+    B.sorted_buf = second ? 1 : 0;
+    gather_kernel<<<std::min(grid_for((long long)P, kThreads), resident), kThreads, 0, s>>>(B);
     P2C_CUDA(cudaGetLastError());
   }
   for (int f = 0; f < 2; ++f) {
@@ -866,9 +1036,11 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   }
   P2C_CUDA(cudaGetLastError());
   if (P > 0) {
-    const long long PL = (long long)P * kBatchSweepLanes;
-    if (t.vf > 0) sweep_vf_kernel<<<grid_for(PL, kThreads), kThreads, 0, s>>>(B, B.keys[1], P);
-    if (t.ee > 0) sweep_ee_kernel<<<grid_for(PL, kThreads), kThreads, 0, s>>>(B, B.keys[1], P);
+    const unsigned sweep_grid = std::min(grid_for((long long)P * kBatchSweepLanes, kThreads), resident);
+    if (t.vf > 0) sweep_vf_kernel<<<sweep_grid, kThreads, 0, s>>>(B);
+    if (t.ee > 0) sweep_ee_kernel<<<sweep_grid, kThreads, 0, s>>>(B);
+    if (t.vf > 0) chunk_kernel<1><<<resident, kThreads, 0, s>>>(B);
+    if (t.ee > 0) chunk_kernel<2><<<resident, kThreads, 0, s>>>(B);
     P2C_CUDA(cudaGetLastError());
   }
   for (int f = 0; f < 2; ++f) {
