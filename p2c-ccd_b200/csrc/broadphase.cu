@@ -41,6 +41,7 @@
 #include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 
 #include "broadphase.cuh"
@@ -51,6 +52,18 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr unsigned kFull = 0xffffffffu;
+constexpr long long kCountSortMinPrims = 1ll << 20;  // scenes ranked by the count sort when culled
+
+// The size from which a culled scene's kept boxes are ranked by the count
+// sort: kCountSortMinPrims, or P2C_COUNT_SORT_MIN_PRIMS (tests set 0 to run
+// that path on small scenes).
+long long count_sort_min_prims() {
+  const char* e = std::getenv("P2C_COUNT_SORT_MIN_PRIMS");
+  if (e == nullptr || *e == 0) return kCountSortMinPrims;
+  char* end = nullptr;
+  const long long v = std::strtoll(e, &end, 10);
+  return (end != e && v >= 0) ? v : kCountSortMinPrims;
+}
 
 inline unsigned grid_for(long long n, int threads) {
   const long long g = (n + threads - 1) / threads;
@@ -310,14 +323,23 @@ __global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
 // Sort key of every kept box (compact entry c, value c).  The order of the
 // compact entries does not matter: they are sorted on their full keys and
 // the pairs are sorted at the end.
+// With pad_to > 0 the entries [kept, pad_to) get the key ~0, which sorts
+// after every box (its list field, 3, names no list): a sort sized on the
+// host then ranks them last.
 __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const double* __restrict__ cbox,
                                                         const unsigned* __restrict__ cprim,
                                                         unsigned* __restrict__ keys, unsigned* __restrict__ vals,
-                                                        const BroadScratch* sc) {
+                                                        const BroadScratch* sc, unsigned long long pad_to) {
   pdl_wait();
   pdl_trigger();
   const Grid& G = sc->grid;
   const unsigned long long n = sc->keyed;
+  for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < pad_to;
+       c += (unsigned long long)gridDim.x * blockDim.x)
+    if (c >= n) {
+      keys[c] = ~0u;
+      vals[c] = (unsigned)c;
+    }
   for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (unsigned long long)gridDim.x * blockDim.x) {
     const long long g = cprim[c];
@@ -632,6 +654,14 @@ struct Carver {
   }
 };
 
+size_t sort_entries_temp_bytes(long long n) {
+  size_t bytes = 0;
+  cub::DoubleBuffer<unsigned> k(nullptr, nullptr);
+  cub::DoubleBuffer<unsigned> v(nullptr, nullptr);
+  cub::DeviceRadixSort::SortPairs(nullptr, bytes, k, v, (int)(n > 0 ? n : 1));
+  return bytes;
+}
+
 size_t sort_keys_temp_bytes(long long n) {
   size_t bytes = 0;
   cub::DoubleBuffer<unsigned long long> k(nullptr, nullptr);
@@ -692,7 +722,7 @@ Layout carve(void* base, long long nv, long long nf, long long ne, long long pai
     L.B[l].s.cell_begin = dry ? nullptr : L.cells + (2 * l) * kCells;
     L.B[l].s.cell_end = dry ? nullptr : L.cells + (2 * l + 1) * kCells;
   }
-  L.sort_tmp_bytes = sort_keys_temp_bytes(pair_cap);
+  L.sort_tmp_bytes = std::max(sort_entries_temp_bytes(n), sort_keys_temp_bytes(pair_cap));
   L.sort_tmp = c.take<char>((long long)L.sort_tmp_bytes);
   L.pair_alt = c.take<unsigned long long>(pair_cap);
   L.total = c.off + 256;
@@ -770,6 +800,19 @@ SweepFork* sweep_fork(cudaStream_t s) {
 
 // Candidate generation; counts_dev receives {vf_count, ee_count, error_word,
 // axis | g1 << 8 | g2 << 24 | kept boxes << 40}.
+// Blocks of a loop over device-counted work: exactly what the device holds at
+// once (SMs x resident blocks of this kernel).  All blocks then run side by
+// side and each pass of the loop covers one contiguous stretch of the sorted
+// entries, so the partners they read stay in the L2 (a larger grid runs its
+// blocks in waves that each walk their own far-apart stretches).
+template <class K>
+unsigned resident_grid(K kernel, const DeviceInfo& info) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return (unsigned)std::max(1, info.sm_count) * (unsigned)per_sm;
+}
+
 int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long long vf_cap,
                       unsigned long long* ee_out, long long ee_cap, unsigned long long* counts_dev, bool sort_out,
                       void* ws, size_t ws_bytes, cudaStream_t s) {
@@ -794,7 +837,6 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   DeviceInfo info;
   int rc = current_device_info(&info);
   if (rc != P2C_OK) return rc;
-  const unsigned resident = (unsigned)std::max(1, info.sm_count) * 8u;  // blocks of the device-sized loops
   P2C_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(BroadScratch), s));
   P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
   init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
@@ -808,14 +850,31 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   const int two_body = scene.exclude_self && scene.n_obj == 2 ? 1 : 0;
   P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
   if (n > 0) {
-    const unsigned loop_grid = std::min(grid_for(n, kThreads), resident);
+    const unsigned loop_grid = std::min(grid_for(n, kThreads), resident_grid(gather_kernel, info));
+    // The library's onesweep sort over all n entries (the culled ones padded
+    // to sort last) unless culling applies to a scene of more than
+    // kCountSortMinPrims primitives: then the kept boxes, often a few per
+    // cent, are ranked alone by the count sort.  Below that size the count
+    // sort's twelve launches cost more than ranking every entry (two 40,960-
+    // triangle spheres: 92 us against 56 us cold for 4,464 kept of 245,764).
+    const bool all_entries = cull == 0 || n < count_sort_min_prims();
     P2C_CUDA(launch_pdl(keys_kernel, dim3(loop_grid), dim3(kThreads), 0, s, lists, (const double*)L.cbox,
-                        (const unsigned*)L.cprim, L.keys[0], L.vals[0], (const BroadScratch*)L.sc));
-    bool second = false;
-    rc = count_sort_pairs(L.keys[0], L.vals[0], L.keys[1], L.vals[1], &L.sc->keyed, n, kCellBits + qbits + 2,
-                          L.cs_scratch, L.cs_bytes, s, &second);
-    if (rc != P2C_OK) return rc;
-    const int b = second ? 1 : 0;
+                        (const unsigned*)L.cprim, L.keys[0], L.vals[0], (const BroadScratch*)L.sc,
+                        (unsigned long long)(all_entries ? n : 0)));
+    int b = 0;
+    if (all_entries) {
+      cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
+      cub::DoubleBuffer<unsigned> v(L.vals[0], L.vals[1]);
+      size_t tb = L.sort_tmp_bytes;
+      P2C_CUDA(cub::DeviceRadixSort::SortPairs(L.sort_tmp, tb, k, v, (int)n, 0, kCellBits + qbits + 2, s));
+      b = k.selector;
+    } else {
+      bool second = false;
+      rc = count_sort_pairs(L.keys[0], L.vals[0], L.keys[1], L.vals[1], &L.sc->keyed, n, kCellBits + qbits + 2,
+                            L.cs_scratch, L.cs_bytes, s, &second);
+      if (rc != P2C_OK) return rc;
+      b = second ? 1 : 0;
+    }
     P2C_CUDA(launch_pdl(gather_kernel, dim3(loop_grid), dim3(kThreads), 0, s, lists, (const double*)L.cbox,
                         (const unsigned*)L.cprim, (const unsigned*)L.keys[b], (const unsigned*)L.vals[b], L.B[0].s,
                         L.B[1].s, L.B[2].s, (const BroadScratch*)L.sc));
@@ -838,14 +897,17 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     ee_stream = fk->stream;
   }
   if (do_ee)
-    P2C_CUDA(launch_pdl(sweep_ee_kernel, dim3(std::min(grid_for(scene.ne * kSceneSweepLanes, kThreads), resident)),
+    P2C_CUDA(launch_pdl(sweep_ee_kernel,
+                        dim3(std::min(grid_for(scene.ne * kSceneSweepLanes, kThreads),
+                                      resident_grid(sweep_ee_kernel, info))),
                         dim3(kThreads), 0,
                         ee_stream, L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out,
                         (unsigned long long)ee_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaEventRecord(fk->join, fk->stream));
   if (do_vf)
     P2C_CUDA(launch_pdl(sweep_vf_kernel,
-                        dim3(std::min(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads), resident)),
+                        dim3(std::min(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads),
+                                      resident_grid(sweep_vf_kernel, info))),
                         dim3(kThreads), 0, s, L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out,
                         (unsigned long long)vf_cap, L.sc));
   if (fk != nullptr) P2C_CUDA(cudaStreamWaitEvent(s, fk->join, 0));

@@ -111,6 +111,7 @@ struct BatchBroad {
   unsigned long long* pack[2][2];  // vf / ee pair buffers and their sort alternates
   uint4* chunks[2];                // queued pieces of long windows (box, first, end), per family
   unsigned long long* chunk_count; // 2 counters
+  unsigned long long chunk_cap;    // chunks each queue holds
   int pair_bits[2];                // packed pair bits of the widest scene, per family
 };
 
@@ -464,8 +465,17 @@ __global__ void grid_kernel(BatchBroad B) {
 // Sort key of every kept box (compact entry c, value c): the order of the
 // compact entries does not matter, they are sorted on their full keys and
 // the pairs are sorted at the end.
-__global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B) {
+// With pad_to > 0 the entries [kept, pad_to) get the key ~0, after every box
+// (its list field, 3, names no list), for a sort sized on the host.
+__global__ void __launch_bounds__(kThreads) keys_kernel(BatchBroad B, unsigned long long pad_to) {
   const unsigned long long n = *B.n_keyed;
+  for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < pad_to;
+       c += (unsigned long long)gridDim.x * blockDim.x)
+    if (c >= n) {
+      if (B.key32) B.keys32[0][c] = ~0u;
+      else B.keys[0][c] = ~0ull;
+      B.vals[0][c] = (unsigned)c;
+    }
   for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long g = B.cprim[c];
@@ -586,7 +596,12 @@ constexpr int kBatchSweepLanes = 2;
 // of hundreds of partners; walked by one lane they set the length of the
 // whole launch.  When the queue is full the lane walks on by itself.
 constexpr unsigned kChunk = 32;
-constexpr unsigned long long kChunkCap = 1ull << 20;  // chunks per family
+// Queue capacity per family: one chunk per 8 primitives of the batch, within
+// [4096, 2^20] (a small batch keeps a small workspace).
+__host__ __device__ inline unsigned long long chunk_cap_for(unsigned long long prims) {
+  const unsigned long long c = prims / 8;
+  return c < 4096ull ? 4096ull : (c > (1ull << 20) ? (1ull << 20) : c);
+}
 
 // A scanning box of the vertex-face sweep and the partner list it walks.
 struct VfScan {
@@ -678,7 +693,8 @@ __device__ __forceinline__ bool ee_test(const EeScan& c, unsigned j, unsigned lo
 // Hand the rest of the current window, from w.j on, to the chunk queue.
 // Returns false (the lane walks on by itself) when the queue is full.
 __device__ __forceinline__ bool offload_window(StridedWalker& w, const SortedBoxes& Q, unsigned long long box,
-                                               uint4* queue, unsigned long long* queue_count) {
+                                               uint4* queue, unsigned long long* queue_count,
+                                               unsigned long long cap) {
   unsigned b = w.j, e = w.j_end;
   while (b < e) {  // first entry past the window
     const unsigned m = (b + e) >> 1;
@@ -688,8 +704,8 @@ __device__ __forceinline__ bool offload_window(StridedWalker& w, const SortedBox
   const unsigned je = b;
   const unsigned long long pieces = (je - w.j + kChunk - 1) / kChunk;
   const unsigned long long base = atomicAdd(queue_count, pieces);
-  if (base + pieces > kChunkCap) {
-    for (unsigned long long k = base; k < kChunkCap; ++k) queue[k] = make_uint4(0u, 0u, 0u, 0u);  // empty
+  if (base + pieces > cap) {
+    for (unsigned long long k = base; k < cap; ++k) queue[k] = make_uint4(0u, 0u, 0u, 0u);  // empty
     return false;
   }
   for (unsigned long long k = 0; k < pieces; ++k) {
@@ -737,7 +753,7 @@ __device__ __forceinline__ void sweep_vf_slot(const BatchBroad& B, unsigned long
         live = w.next_cell(c.Q, B.sc[s].grid);
         run = 0;
       } else if (++run == kChunk) {
-        if (offload_window(w, c.Q, i, B.chunks[0], B.chunk_count + 0)) {
+        if (offload_window(w, c.Q, i, B.chunks[0], B.chunk_count + 0, B.chunk_cap)) {
           live = w.next_cell(c.Q, B.sc[s].grid);
           run = 0;
         }
@@ -790,7 +806,7 @@ __device__ __forceinline__ void sweep_ee_slot(const BatchBroad& B, unsigned long
         live = w.next_cell(c.E, B.sc[s].grid);
         run = 0;
       } else if (++run == kChunk) {
-        if (offload_window(w, c.E, i, B.chunks[1], B.chunk_count + 1)) {
+        if (offload_window(w, c.E, i, B.chunks[1], B.chunk_count + 1, B.chunk_cap)) {
           live = w.next_cell(c.E, B.sc[s].grid);
           run = 0;
         }
@@ -810,7 +826,7 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B) {
 // The queued pieces of long windows, one lane each (at most kChunk entries).
 template <int kFamily>
 __global__ void __launch_bounds__(kThreads) chunk_kernel(BatchBroad B) {
-  const unsigned long long n = min(B.chunk_count[kFamily - 1], kChunkCap);
+  const unsigned long long n = min(B.chunk_count[kFamily - 1], B.chunk_cap);
   for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < n;
        base += (unsigned long long)gridDim.x * blockDim.x) {
     const unsigned long long k = base + threadIdx.x;
@@ -893,7 +909,13 @@ Totals totals_of(const p2c_batch_scene* h, int n) {
 
 size_t sort_temp_bytes(const Totals& t) {
   size_t b = 0, c = 0;
-  const size_t a = count_sort_scratch_bytes((long long)std::max<unsigned long long>(t.P, 1ull));
+  size_t a32 = 0, a64 = 0;
+  const int np = (int)std::max<unsigned long long>(t.P, 1ull);
+  cub::DeviceRadixSort::SortPairs(nullptr, a32, (const unsigned*)nullptr, (unsigned*)nullptr, (const unsigned*)nullptr,
+                                  (unsigned*)nullptr, np);
+  cub::DeviceRadixSort::SortPairs(nullptr, a64, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
+                                  (const unsigned*)nullptr, (unsigned*)nullptr, np);
+  const size_t a = std::max(count_sort_scratch_bytes((long long)np), std::max(a32, a64));
   cub::DeviceRadixSort::SortKeys(nullptr, b, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
                                  (int)std::max<unsigned long long>(t.vf, 1ull));
   cub::DeviceRadixSort::SortKeys(nullptr, c, (const unsigned long long*)nullptr, (unsigned long long*)nullptr,
@@ -937,8 +959,9 @@ Carve carve(void* base, const p2c_batch_scene* scenes_dev, int n, const Totals& 
   B.sorted_buf = 0;
   B.n_keyed = static_cast<unsigned long long*>(take(8));
   B.chunk_count = static_cast<unsigned long long*>(take(16));
-  B.chunks[0] = static_cast<uint4*>(take(16 * kChunkCap));
-  B.chunks[1] = static_cast<uint4*>(take(16 * kChunkCap));
+  B.chunk_cap = chunk_cap_for(t.P);
+  B.chunks[0] = static_cast<uint4*>(take(16 * B.chunk_cap));
+  B.chunks[1] = static_cast<uint4*>(take(16 * B.chunk_cap));
   B.vals[0] = static_cast<unsigned*>(take(4 * P));
   B.vals[1] = static_cast<unsigned*>(take(4 * P));
   B.S.lo = static_cast<double*>(take(8 * P));
@@ -983,6 +1006,19 @@ int validate_table(const p2c_batch_scene* h, int n) {
 
 }  // namespace
 
+// Blocks of a loop over device-counted work: exactly what the device holds at
+// once (SMs x resident blocks of this kernel).  All blocks then run side by
+// side and each pass of the loop covers one contiguous stretch of the sorted
+// entries, so the partners they read stay in the L2 (a larger grid runs its
+// blocks in waves that each walk their own far-apart stretches).
+template <class K>
+unsigned resident_grid(K kernel, const DeviceInfo& info) {
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, kThreads, 0) != cudaSuccess || per_sm < 1)
+    per_sm = 1;
+  return (unsigned)std::max(1, info.sm_count) * (unsigned)per_sm;
+}
+
 int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev, int n, void* ws, size_t ws_bytes,
                             cudaStream_t s) {
   const Totals t = totals_of(h, n);
@@ -1014,18 +1050,39 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   DeviceInfo info;
   int rc = current_device_info(&info);
   if (rc != P2C_OK) return rc;
-  const unsigned resident = (unsigned)std::max(1, info.sm_count) * 8u;  // blocks of the device-sized loops
   if (P > 0) {
-    keys_kernel<<<std::min(grid_for((long long)P, kThreads), resident), kThreads, 0, s>>>(B);
+    // No scene culls: nearly every box is kept, and the library's onesweep
+    // sort over all P entries (the others padded to sort last) beats ranking
+    // them with the count sort; otherwise only the kept boxes are ranked.
+    bool any_cull = false;
+    for (int k = 0; k < n && !any_cull; ++k)
+      any_cull = h[k].exclude_self && h[k].n_obj >= 1 && h[k].n_obj <= kMaxCullObjects;
+    keys_kernel<<<std::min(grid_for((long long)P, kThreads), resident_grid(keys_kernel, info)), kThreads, 0, s>>>(B, any_cull ? 0ull : P);
     P2C_CUDA(cudaGetLastError());
     bool second = false;
-    rc = B.key32 ? count_sort_pairs(B.keys32[0], B.vals[0], B.keys32[1], B.vals[1], B.n_keyed, (long long)P, key_bits,
-                                    C.tmp, C.tmp_bytes, s, &second)
-                 : count_sort_pairs(B.keys[0], B.vals[0], B.keys[1], B.vals[1], B.n_keyed, (long long)P, key_bits,
-                                    C.tmp, C.tmp_bytes, s, &second);
-    if (rc != P2C_OK) return rc;
+    if (!any_cull) {
+      size_t tb = C.tmp_bytes;
+      if (B.key32) {
+        cub::DoubleBuffer<unsigned> k(B.keys32[0], B.keys32[1]);
+        cub::DoubleBuffer<unsigned> v(B.vals[0], B.vals[1]);
+        P2C_CUDA(cub::DeviceRadixSort::SortPairs(C.tmp, tb, k, v, (int)P, 0, key_bits, s));
+        second = k.selector == 1;
+      } else {
+        cub::DoubleBuffer<unsigned long long> k(B.keys[0], B.keys[1]);
+        cub::DoubleBuffer<unsigned> v(B.vals[0], B.vals[1]);
+        P2C_CUDA(cub::DeviceRadixSort::SortPairs(C.tmp, tb, k, v, (int)P, 0, key_bits, s));
+        second = k.selector == 1;
+      }
+    } else {
+      rc = B.key32 ? count_sort_pairs(B.keys32[0], B.vals[0], B.keys32[1], B.vals[1], B.n_keyed, (long long)P,
+                                      key_bits, C.tmp, C.tmp_bytes, s, &second)
+                   : count_sort_pairs(B.keys[0], B.vals[0], B.keys[1], B.vals[1], B.n_keyed, (long long)P, key_bits,
+                                      C.tmp, C.tmp_bytes, s, &second);
+      if (rc != P2C_OK) return rc;
+    }
     B.sorted_buf = second ? 1 : 0;
-    gather_kernel<<<std::min(grid_for((long long)P, kThreads), resident), kThreads, 0, s>>>(B);
+    gather_kernel<<<std::min(grid_for((long long)P, kThreads), resident_grid(gather_kernel, info)), kThreads, 0,
+                    s>>>(B);
     P2C_CUDA(cudaGetLastError());
   }
   for (int f = 0; f < 2; ++f) {
@@ -1036,11 +1093,11 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   }
   P2C_CUDA(cudaGetLastError());
   if (P > 0) {
-    const unsigned sweep_grid = std::min(grid_for((long long)P * kBatchSweepLanes, kThreads), resident);
-    if (t.vf > 0) sweep_vf_kernel<<<sweep_grid, kThreads, 0, s>>>(B);
-    if (t.ee > 0) sweep_ee_kernel<<<sweep_grid, kThreads, 0, s>>>(B);
-    if (t.vf > 0) chunk_kernel<1><<<resident, kThreads, 0, s>>>(B);
-    if (t.ee > 0) chunk_kernel<2><<<resident, kThreads, 0, s>>>(B);
+    const unsigned slots = grid_for((long long)P * kBatchSweepLanes, kThreads);
+    if (t.vf > 0) sweep_vf_kernel<<<std::min(slots, resident_grid(sweep_vf_kernel, info)), kThreads, 0, s>>>(B);
+    if (t.ee > 0) sweep_ee_kernel<<<std::min(slots, resident_grid(sweep_ee_kernel, info)), kThreads, 0, s>>>(B);
+    if (t.vf > 0) chunk_kernel<1><<<resident_grid(chunk_kernel<1>, info), kThreads, 0, s>>>(B);
+    if (t.ee > 0) chunk_kernel<2><<<resident_grid(chunk_kernel<2>, info), kThreads, 0, s>>>(B);
     P2C_CUDA(cudaGetLastError());
   }
   for (int f = 0; f < 2; ++f) {

@@ -161,6 +161,28 @@ def test_config2_scene_full_size(cuda_device, oracle_mod):
     _check_results(oracle_mod, pipe, cfg)
 
 
+@pytest.mark.parametrize("n_lon,n_rings", [(40, 30), (160, 128)])
+def test_two_body_scene_with_the_counted_sort(cuda_device, oracle_mod, monkeypatch, n_lon, n_rings):
+    """P2C_COUNT_SORT_MIN_PRIMS=0 ranks the kept boxes of any culled scene with
+    the sort whose count is read on the device (by default only scenes above
+    2^20 primitives): pair sets and certificates still equal the oracle's."""
+    from p2cccd_b200 import scenes
+    from p2cccd_b200.certify import CertConfig
+    from p2cccd_b200.scene import ScenePipeline
+
+    monkeypatch.setenv("P2C_COUNT_SORT_MIN_PRIMS", "0")
+    s = scenes.two_spheres(n_lon=n_lon, n_rings=n_rings, seed=5)
+    cfg = CertConfig(1e-6, 1e-6, 32)
+    pipe = ScenePipeline(s, cuda_device, exclude_self=True, config=cfg)
+    pipe.step_checked()
+    vf, ee = pipe.pairs()
+    o_vf, o_ee = _oracle_pairs(oracle_mod, s, 0.0, True, "sweep")
+    np.testing.assert_array_equal(vf, o_vf)
+    np.testing.assert_array_equal(ee, o_ee)
+    assert len(vf) > 0 and len(ee) > 0
+    _check_results(oracle_mod, pipe, cfg)
+
+
 def test_undecided_queue_and_invalid_geometry(cuda_device, oracle_mod):
     from p2cccd_b200 import scenes
     from p2cccd_b200.certify import CertConfig
