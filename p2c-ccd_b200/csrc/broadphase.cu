@@ -474,8 +474,9 @@ __device__ __forceinline__ void sweep_vf_slot(const SortedBoxes& V, const Sorted
   }
 }
 
-// Every (kept box, lane) slot in a grid sized for the device (the kept
-// boxes are counted on the device).
+// Every (kept box, lane) slot, taken 32 at a time by whichever warp is free
+// (the kept boxes are counted on the device): the warps walk the sorted
+// entries in order and none waits on a share fixed in advance.
 __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
                                                             const int32_t* __restrict__ faces, int exclude_self,
                                                             int pack_shift, unsigned long long* out,
@@ -483,8 +484,11 @@ __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, Sorte
   pdl_wait();
   pdl_trigger();
   const long long work = (long long)(sc->grid.seg[2] - sc->grid.seg[0]) * kSceneSweepLanes;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < work; base += (long long)gridDim.x * blockDim.x)
-    sweep_vf_slot(V, F, faces, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
+  for (;;) {
+    const long long base = next_warp_slots(&sc->sweep_next[0]);
+    if (base >= work) break;
+    sweep_vf_slot(V, F, faces, exclude_self, pack_shift, out, cap, sc, base + (threadIdx.x & 31));
+  }
 }
 
 // Edge-edge pairs: each edge scans its own list and owns the pairs whose
@@ -551,8 +555,11 @@ __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const
   pdl_wait();
   pdl_trigger();
   const long long work = (long long)(sc->grid.seg[3] - sc->grid.seg[2]) * kSceneSweepLanes;
-  for (long long base = (long long)blockIdx.x * blockDim.x; base < work; base += (long long)gridDim.x * blockDim.x)
-    sweep_ee_slot(E, edges, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
+  for (;;) {
+    const long long base = next_warp_slots(&sc->sweep_next[1]);
+    if (base >= work) break;
+    sweep_ee_slot(E, edges, exclude_self, pack_shift, out, cap, sc, base + (threadIdx.x & 31));
+  }
 }
 
 __global__ void fill_u64_kernel(unsigned long long* p, long long n, unsigned long long v) {

@@ -93,7 +93,15 @@ struct BroadScratch {
   unsigned long long error_word;  // bit 0: non-finite coordinate
   unsigned long long obj_other;   // non-zero: a kept primitive's object id is neither 0 nor 1
   unsigned long long keyed;       // single scene: boxes kept after culling (compact entries)
+  unsigned long long sweep_next[2];  // single scene: next slot of the vertex-face / edge-edge sweep
 };
+
+// The next 32 sweep slots for the calling warp (one atomic per warp).
+__device__ __forceinline__ long long next_warp_slots(unsigned long long* next) {
+  unsigned long long base = 0;
+  if ((threadIdx.x & 31) == 0) base = atomicAdd(next, 32ull);
+  return (long long)__shfl_sync(0xffffffffu, base, 0);
+}
 
 // Prefix of the partner object's run in a split low field (0 unsplit): a
 // box of object o (0 or 1) walks the entries of object 1 - o.

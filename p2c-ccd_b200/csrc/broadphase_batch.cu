@@ -112,6 +112,7 @@ struct BatchBroad {
   uint4* chunks[2];                // queued pieces of long windows (box, first, end), per family
   unsigned long long* chunk_count; // 2 counters
   unsigned long long chunk_cap;    // chunks each queue holds
+  unsigned long long* sweep_next;  // 2 counters: next slot of the vertex-face / edge-edge sweep
   int pair_bits[2];                // packed pair bits of the widest scene, per family
 };
 
@@ -763,13 +764,15 @@ __device__ __forceinline__ void sweep_vf_slot(const BatchBroad& B, unsigned long
   }
 }
 
-// Every (kept box, lane) slot, in a grid sized for the device: the number of
-// kept boxes is known only here.
+// Every (kept box, lane) slot, taken 32 at a time by whichever warp is free
+// (the number of kept boxes is known only on the device).
 __global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
-  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < work;
-       base += (unsigned long long)gridDim.x * blockDim.x)
-    sweep_vf_slot(B, base + threadIdx.x, n);
+  for (;;) {
+    const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 0);
+    if (base >= work) break;
+    sweep_vf_slot(B, base + (threadIdx.x & 31), n);
+  }
 }
 
 // Edge-edge pairs: an edge owns the pairs whose partner minimum is larger
@@ -818,9 +821,11 @@ __device__ __forceinline__ void sweep_ee_slot(const BatchBroad& B, unsigned long
 
 __global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
-  for (unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x; base < work;
-       base += (unsigned long long)gridDim.x * blockDim.x)
-    sweep_ee_slot(B, base + threadIdx.x, n);
+  for (;;) {
+    const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 1);
+    if (base >= work) break;
+    sweep_ee_slot(B, base + (threadIdx.x & 31), n);
+  }
 }
 
 // The queued pieces of long windows, one lane each (at most kChunk entries).
@@ -959,6 +964,7 @@ Carve carve(void* base, const p2c_batch_scene* scenes_dev, int n, const Totals& 
   B.sorted_buf = 0;
   B.n_keyed = static_cast<unsigned long long*>(take(8));
   B.chunk_count = static_cast<unsigned long long*>(take(16));
+  B.sweep_next = static_cast<unsigned long long*>(take(16));
   B.chunk_cap = chunk_cap_for(t.P);
   B.chunks[0] = static_cast<uint4*>(take(16 * B.chunk_cap));
   B.chunks[1] = static_cast<uint4*>(take(16 * B.chunk_cap));
@@ -1039,6 +1045,7 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   P2C_CUDA(cudaMemsetAsync(B.cell_end, 0, 4 * 3 * (size_t)t.cells, s));
   P2C_CUDA(cudaMemsetAsync(B.n_keyed, 0, sizeof(unsigned long long), s));
   P2C_CUDA(cudaMemsetAsync(B.chunk_count, 0, 2 * sizeof(unsigned long long), s));
+  P2C_CUDA(cudaMemsetAsync(B.sweep_next, 0, 2 * sizeof(unsigned long long), s));
   init_scenes_kernel<<<n, 128, 0, s>>>(B);
   prep_kernel<<<1, kPrepThreads, 0, s>>>(B);
   P2C_CUDA(cudaGetLastError());
