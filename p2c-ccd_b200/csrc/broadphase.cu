@@ -89,6 +89,41 @@ __global__ void init_scratch_kernel(BroadScratch* sc) {
   }
 }
 
+// Block sums of the per-axis statistics that choose the sweep axis (extents,
+// centres and squared centres of the boxes), ten atomics per block.
+__device__ __forceinline__ void axis_stats(const double b[6], bool live, BroadScratch* sc) {
+  __shared__ double red[9][kThreads / 32];
+  const int lane = threadIdx.x & 31;
+  double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (live) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+      const double c = 0.5 * (b[3 + a] + b[a]);
+      vals[a] = b[3 + a] - b[a];
+      vals[3 + a] = c;
+      vals[6 + a] = c * c;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    double v = vals[k];
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) v += __shfl_down_sync(kFull, v, s);
+    if (lane == 0) red[k][threadIdx.x >> 5] = v;
+  }
+  const unsigned cnt = __popc(__ballot_sync(kFull, live));
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    double s = 0.0;
+    for (int w = 0; w < kThreads / 32; ++w) s += red[threadIdx.x][w];
+    double* dst = threadIdx.x < 3 ? &sc->extent_sum[threadIdx.x]
+                  : threadIdx.x < 6 ? &sc->center_sum[threadIdx.x - 3]
+                                    : &sc->center_sq_sum[threadIdx.x - 6];
+    atomicAdd(dst, s);
+  }
+  if (lane == 0 && cnt) atomicAdd(&sc->count, (unsigned long long)cnt);
+}
+
 // Vertex swept boxes (Extend/Expand/SweptPointBox,
 // scene_object_envelope_native_ti_walltime.cpp:256-301): each joins its
 // object's envelope (the union of the object's vertex boxes; one atomic per
@@ -101,7 +136,6 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
                                                             double thickness, int cull_objects, BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
-  __shared__ double red[9][kThreads / 32];
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const int lane = threadIdx.x & 31;
   double b[6] = {0, 0, 0, 0, 0, 0};
@@ -135,35 +169,9 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
       }
     }
   }
-  // axis statistics (sums of extents, centres, squared centres)
-  double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  if (live) {
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-      const double c = 0.5 * (b[3 + a] + b[a]);
-      vals[a] = b[3 + a] - b[a];
-      vals[3 + a] = c;
-      vals[6 + a] = c * c;
-    }
-  }
-#pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    double v = vals[k];
-#pragma unroll
-    for (int s = 16; s > 0; s >>= 1) v += __shfl_down_sync(kFull, v, s);
-    if (lane == 0) red[k][threadIdx.x >> 5] = v;
-  }
-  const unsigned cnt = __popc(__ballot_sync(kFull, live));
-  __syncthreads();
-  if (threadIdx.x < 9) {
-    double s = 0.0;
-    for (int w = 0; w < kThreads / 32; ++w) s += red[threadIdx.x][w];
-    double* dst = threadIdx.x < 3 ? &sc->extent_sum[threadIdx.x]
-                  : threadIdx.x < 6 ? &sc->center_sum[threadIdx.x - 3]
-                                    : &sc->center_sq_sum[threadIdx.x - 6];
-    atomicAdd(dst, s);
-  }
-  if (lane == 0 && cnt) atomicAdd(&sc->count, (unsigned long long)cnt);
+#ifndef P2C_STATS_ALL
+  axis_stats(b, live, sc);
+#endif
 }
 
 // Every primitive's swept box (Swept*Box, :256-301), kept unless it is a
@@ -173,7 +181,7 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
 // their extents per list size the column grid.
 __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict__ v_t0,
                                                         const double* __restrict__ v_t1, Lists L, double thickness,
-                                                        int cull_objects, double* __restrict__ cbox,
+                                                        int cull_objects, int ordered, double* __restrict__ cbox,
                                                         unsigned* __restrict__ cprim, BroadScratch* sc) {
   pdl_wait();
   pdl_trigger();
@@ -206,7 +214,17 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict
     other = keep && o != 0 && o != 1;
   }
   if (__any_sync(kFull, other) && (threadIdx.x & 31) == 0) atomicOr(&sc->obj_other, 1ull);
-  {
+  if (ordered) {
+    // nothing is culled: every entry in place, in primitive order (a vertex
+    // in no face marked), so the sort ranks equal keys by primitive and the
+    // order of the sorted lists does not depend on the order warps ran in
+    if (g < L.off[3]) {
+      double* dst = cbox + 6 * g;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) dst[k] = b[k];
+      cprim[g] = keep ? (unsigned)g : ~0u;
+    }
+  } else {
     const unsigned m = __ballot_sync(kFull, keep);
     if (m != 0u) {
       const int lane = threadIdx.x & 31;
@@ -251,6 +269,9 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict
       }
     }
   }
+#ifdef P2C_STATS_ALL
+  axis_stats(b, g < L.off[3], sc);
+#endif
 }
 
 // Sweep axis, column grid, sweep-axis quantiser and list segments (one
@@ -272,6 +293,9 @@ __global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
     }
   }
   Grid g;
+#ifdef P2C_FORCE_AXIS
+  axis = P2C_FORCE_AXIS;
+#endif
   g.axis = axis;
   g.a1 = axis == 0 ? 1 : 0;
   g.a2 = axis == 2 ? 1 : 2;
@@ -329,11 +353,15 @@ __global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
 __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const double* __restrict__ cbox,
                                                         const unsigned* __restrict__ cprim,
                                                         unsigned* __restrict__ keys, unsigned* __restrict__ vals,
-                                                        const BroadScratch* sc, unsigned long long pad_to) {
+                                                        const BroadScratch* sc, unsigned long long pad_to,
+                                                        int ordered) {
   pdl_wait();
   pdl_trigger();
   const Grid& G = sc->grid;
-  const unsigned long long n = sc->keyed;
+  // ordered: entries [0, pad_to) in primitive order, culled ones marked ~0;
+  // else the first sc->keyed entries are kept boxes and the rest, up to
+  // pad_to, padding
+  const unsigned long long n = ordered ? pad_to : sc->keyed;
   for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < pad_to;
        c += (unsigned long long)gridDim.x * blockDim.x)
     if (c >= n) {
@@ -342,6 +370,11 @@ __global__ void __launch_bounds__(kThreads) keys_kernel(Lists L, const double* _
     }
   for (unsigned long long c = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; c < n;
        c += (unsigned long long)gridDim.x * blockDim.x) {
+    if (cprim[c] == ~0u) {
+      keys[c] = ~0u;
+      vals[c] = (unsigned)c;
+      continue;
+    }
     const long long g = cprim[c];
     const int l = L.list_of(g);
     const double* b = cbox + 6 * c;
@@ -410,6 +443,18 @@ __device__ __forceinline__ void append_pair(bool found, unsigned long long key, 
 // it shortens the chain and puts more warps on the SMs.
 constexpr int kSceneSweepLanes = 8;
 
+// Resident blocks the sweeps are compiled for (registers per thread capped
+// to fit): the walks are chains of dependent loads, so warps per SM set
+// their speed (the cloth's edge-edge sweep at 54 registers, 4 blocks per SM,
+// took twice as long as at 48, 5 blocks).
+#ifndef P2C_SWEEP_VF_BLOCKS
+#define P2C_SWEEP_VF_BLOCKS 4
+#endif
+#ifndef P2C_SWEEP_EE_BLOCKS
+#define P2C_SWEEP_EE_BLOCKS 5
+#endif
+constexpr int kSweepVfBlocks = P2C_SWEEP_VF_BLOCKS, kSweepEeBlocks = P2C_SWEEP_EE_BLOCKS;
+
 // Vertex-face pairs: boxes [0, nv) scan faces from a vertex and own the
 // pairs whose face minimum is >= the vertex minimum; boxes [nv, nv + nf)
 // scan vertices from a face and own the others.  Keys (vertex, face).
@@ -477,13 +522,18 @@ __device__ __forceinline__ void sweep_vf_slot(const SortedBoxes& V, const Sorted
 // Every (kept box, lane) slot, taken 32 at a time by whichever warp is free
 // (the kept boxes are counted on the device): the warps walk the sorted
 // entries in order and none waits on a share fixed in advance.
-__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
+__global__ void __launch_bounds__(kThreads, kSweepVfBlocks) sweep_vf_kernel(SortedBoxes V, SortedBoxes F,
                                                             const int32_t* __restrict__ faces, int exclude_self,
                                                             int pack_shift, unsigned long long* out,
-                                                            unsigned long long cap, BroadScratch* sc) {
+                                                            unsigned long long cap, BroadScratch* sc, int dynamic) {
   pdl_wait();
   pdl_trigger();
   const long long work = (long long)(sc->grid.seg[2] - sc->grid.seg[0]) * kSceneSweepLanes;
+  if (!dynamic) {  // one slot per thread, the grid sized for every entry
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    if (base < work) sweep_vf_slot(V, F, faces, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
+    return;
+  }
   for (;;) {
     const long long base = next_warp_slots(&sc->sweep_next[0]);
     if (base >= work) break;
@@ -549,12 +599,17 @@ __device__ __forceinline__ void sweep_ee_slot(const SortedBoxes& E, const int32_
   }
 }
 
-__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
+__global__ void __launch_bounds__(kThreads, kSweepEeBlocks) sweep_ee_kernel(SortedBoxes E, const int32_t* __restrict__ edges,
                                                             int exclude_self, int pack_shift, unsigned long long* out,
-                                                            unsigned long long cap, BroadScratch* sc) {
+                                                            unsigned long long cap, BroadScratch* sc, int dynamic) {
   pdl_wait();
   pdl_trigger();
   const long long work = (long long)(sc->grid.seg[3] - sc->grid.seg[2]) * kSceneSweepLanes;
+  if (!dynamic) {  // one slot per thread, the grid sized for every entry
+    const long long base = (long long)blockIdx.x * blockDim.x;
+    if (base < work) sweep_ee_slot(E, edges, exclude_self, pack_shift, out, cap, sc, base + threadIdx.x);
+    return;
+  }
   for (;;) {
     const long long base = next_warp_slots(&sc->sweep_next[1]);
     if (base >= work) break;
@@ -830,6 +885,7 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   Layout L = carve(ws, scene.nv, scene.nf, scene.ne, pair_cap, false);
   const long long n = scene.nv + scene.nf + scene.ne;
   const int cull = (scene.exclude_self && scene.n_obj >= 1 && scene.n_obj <= kMaxCullObjects) ? scene.n_obj : 0;
+  const bool ordered = cull == 0;  // nothing culled: entries stay in primitive order, no compaction
   Lists lists;
   lists.off[0] = 0;
   lists.off[1] = scene.nv;
@@ -852,7 +908,7 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
                         scene.v_t1, scene.v_obj, (long long)scene.nv, scene.thickness, cull, L.sc));
   if (n > 0)
     P2C_CUDA(launch_pdl(cull_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
-                        lists, scene.thickness, cull, L.cbox, L.cprim, L.sc));
+                        lists, scene.thickness, cull, ordered ? 1 : 0, L.cbox, L.cprim, L.sc));
   const int qbits = n <= kSmallSceneQPrims ? kQBitsSmall : kQBitsLarge;
   const int two_body = scene.exclude_self && scene.n_obj == 2 ? 1 : 0;
   P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
@@ -864,10 +920,10 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     // cent, are ranked alone by the count sort.  Below that size the count
     // sort's twelve launches cost more than ranking every entry (two 40,960-
     // triangle spheres: 92 us against 56 us cold for 4,464 kept of 245,764).
-    const bool all_entries = cull == 0 || n < count_sort_min_prims();
+    const bool all_entries = ordered || n < count_sort_min_prims();
     P2C_CUDA(launch_pdl(keys_kernel, dim3(loop_grid), dim3(kThreads), 0, s, lists, (const double*)L.cbox,
                         (const unsigned*)L.cprim, L.keys[0], L.vals[0], (const BroadScratch*)L.sc,
-                        (unsigned long long)(all_entries ? n : 0)));
+                        (unsigned long long)(all_entries ? n : 0), ordered ? 1 : 0));
     int b = 0;
     if (all_entries) {
       cub::DoubleBuffer<unsigned> k(L.keys[0], L.keys[1]);
@@ -896,6 +952,18 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     fill_u64_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ~0ull);
   const bool do_vf = scene.nv + scene.nf > 0 && vf_out != nullptr;
   const bool do_ee = scene.ne > 0 && ee_out != nullptr;
+  // Sweep slots: with culling (often a few per cent of the boxes kept) warps
+  // take them 32 at a time from a counter over a resident grid; without, one
+  // slot per thread over a grid for every entry.
+#ifdef P2C_SWEEP_DYNAMIC
+  const int dynamic = P2C_SWEEP_DYNAMIC;
+#else
+  const int dynamic = ordered ? 0 : 1;
+#endif
+  auto sweep_blocks = [&](auto kernel, long long slots) -> unsigned {
+    const unsigned full = grid_for(slots, kThreads);
+    return dynamic ? std::min(full, resident_grid(kernel, info)) : full;
+  };
   SweepFork* fk = do_vf && do_ee ? sweep_fork(s) : nullptr;
   cudaStream_t ee_stream = s;
   if (fk != nullptr) {
@@ -904,19 +972,14 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     ee_stream = fk->stream;
   }
   if (do_ee)
-    P2C_CUDA(launch_pdl(sweep_ee_kernel,
-                        dim3(std::min(grid_for(scene.ne * kSceneSweepLanes, kThreads),
-                                      resident_grid(sweep_ee_kernel, info))),
-                        dim3(kThreads), 0,
-                        ee_stream, L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out,
-                        (unsigned long long)ee_cap, L.sc));
+    P2C_CUDA(launch_pdl(sweep_ee_kernel, dim3(sweep_blocks(sweep_ee_kernel, scene.ne * kSceneSweepLanes)),
+                        dim3(kThreads), 0, ee_stream, L.B[2].s, scene.edges, scene.exclude_self, ee_shift, ee_out,
+                        (unsigned long long)ee_cap, L.sc, dynamic));
   if (fk != nullptr) P2C_CUDA(cudaEventRecord(fk->join, fk->stream));
   if (do_vf)
-    P2C_CUDA(launch_pdl(sweep_vf_kernel,
-                        dim3(std::min(grid_for((scene.nv + scene.nf) * kSceneSweepLanes, kThreads),
-                                      resident_grid(sweep_vf_kernel, info))),
+    P2C_CUDA(launch_pdl(sweep_vf_kernel, dim3(sweep_blocks(sweep_vf_kernel, (scene.nv + scene.nf) * kSceneSweepLanes)),
                         dim3(kThreads), 0, s, L.B[0].s, L.B[1].s, scene.faces, scene.exclude_self, vf_shift, vf_out,
-                        (unsigned long long)vf_cap, L.sc));
+                        (unsigned long long)vf_cap, L.sc, dynamic));
   if (fk != nullptr) P2C_CUDA(cudaStreamWaitEvent(s, fk->join, 0));
   P2C_CUDA(cudaGetLastError());
   if (small_sort) {

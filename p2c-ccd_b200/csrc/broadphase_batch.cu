@@ -589,6 +589,10 @@ __device__ __forceinline__ SortedBoxes scene_view(const BatchBroad& B, int s, in
 // (the batch fills the GPU many times over, so splitting further only adds
 // work; 256 uneven scenes: 11.4 ms with 1 lane, 11.1 with 2, 12.2 with 4).
 constexpr int kBatchSweepLanes = 2;
+#ifndef P2C_BATCH_SWEEP_BLOCKS
+#define P2C_BATCH_SWEEP_BLOCKS 4
+#endif
+constexpr int kBatchSweepBlocks = P2C_BATCH_SWEEP_BLOCKS;  // resident blocks the sweeps are compiled for
 
 // Long windows: a lane that has tested kChunk entries of one column's window
 // and is not through it hands the rest to the chunk queue in pieces of
@@ -766,7 +770,7 @@ __device__ __forceinline__ void sweep_vf_slot(const BatchBroad& B, unsigned long
 
 // Every (kept box, lane) slot, taken 32 at a time by whichever warp is free
 // (the number of kept boxes is known only on the device).
-__global__ void __launch_bounds__(kThreads) sweep_vf_kernel(BatchBroad B) {
+__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_vf_kernel(BatchBroad B) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
   for (;;) {
     const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 0);
@@ -819,7 +823,7 @@ __device__ __forceinline__ void sweep_ee_slot(const BatchBroad& B, unsigned long
   }
 }
 
-__global__ void __launch_bounds__(kThreads) sweep_ee_kernel(BatchBroad B) {
+__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_ee_kernel(BatchBroad B) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
   for (;;) {
     const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 1);
