@@ -1308,7 +1308,7 @@ def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
     t_end = time.time()
     clocks = sampler.stop((t_begin, t_end))
     # the plain path: each step alone, one at a time, every candidate certified
-    plain_ms = {}
+    plain_ms, ref_ms = {}, {}
     for key, s, excl in pool:
         if key not in picks:
             continue
@@ -1325,6 +1325,8 @@ def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
             p.step_checked()
             ts.append((time.perf_counter() - t0) * 1e3)
         plain_ms[key] = (statistics.median(ts), p.read_counts()[0] + p.read_counts()[1])
+        if cpu_budget is not None:
+            ref_ms[key] = _reference_gpu_step_ms(p, cfg)
         del p
     plain_s = sum(plain_ms[k][0] for k in picks) * 1e-3
     plain = {"steps_per_s": n_req / plain_s, "candidates_per_s": sum(plain_ms[k][1] for k in picks) / plain_s,
@@ -1350,7 +1352,43 @@ def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
     }
     if cpu_budget is not None:
         block["cpu_baseline"] = _tool_serve_sample(pool, cfg, cpu_budget)
+        if ref_ms and all(ref_ms.get(k) is not None for k in picks):
+            ref_s = sum(ref_ms[k] for k in picks) * 1e-3
+            ref = {"steps_per_s": n_req / ref_s, "queries_per_s": sum(plain_ms[k][1] for k in picks) / ref_s,
+                   "ms_per_step_by_mesh": dict(ref_ms),
+                   "what": "the reference's CUDA batch certifier (certificate_cuda.cu compiled unchanged for "
+                           "sm_100a; host records in, malloc, copy, one thread per primitive, sync, copy back, "
+                           "free per call) on every certificate query of each request (its candidates, generated "
+                           "here: the reference has no GPU candidate generation), summed over the stream's "
+                           "requests; certification only"}
+            block["cpu_baseline"]["reference_gpu"] = ref
+            block["served_over_reference_gpu"] = out["anyhit"]["capacity"]["steps_per_s"] / ref["steps_per_s"]
+            block["served_certify_all_over_reference_gpu"] = (out["certify"]["capacity"]["steps_per_s"]
+                                                              / ref["steps_per_s"])
     return block
+
+
+def _reference_gpu_step_ms(pipe, cfg) -> float | None:
+    """Milliseconds the reference's CUDA batch path takes to certify every
+    candidate of the pipeline's last step (median of 3), or None when that
+    build is absent."""
+    import oracle
+
+    if not oracle.ref_cuda_available():
+        return None
+    vf, ee = pipe.materialize()
+    run = lambda rec: oracle.ref_cuda_eval_batch(rec, 0.0, 1.0, cfg.eps_time, cfg.eps_space,
+                                                 cfg.max_subdivision_depth) if len(rec) else None
+    t0 = time.perf_counter()
+    run(vf), run(ee)
+    warm = time.perf_counter() - t0
+    ts = []
+    for _ in range(1 if warm > 0.5 else 3):  # seconds-long steps (the cloth meshes) once
+        t0 = time.perf_counter()
+        run(vf)
+        run(ee)
+        ts.append(time.perf_counter() - t0)
+    return statistics.median(ts) * 1e3
 
 
 def run_serve(args) -> dict:
