@@ -1379,11 +1379,9 @@ def _reference_gpu_step_ms(pipe, cfg) -> float | None:
     vf, ee = pipe.materialize()
     run = lambda rec: oracle.ref_cuda_eval_batch(rec, 0.0, 1.0, cfg.eps_time, cfg.eps_space,
                                                  cfg.max_subdivision_depth) if len(rec) else None
-    t0 = time.perf_counter()
     run(vf), run(ee)
-    warm = time.perf_counter() - t0
     ts = []
-    for _ in range(1 if warm > 0.5 else 3):  # seconds-long steps (the cloth meshes) once
+    for _ in range(3):
         t0 = time.perf_counter()
         run(vf)
         run(ee)

@@ -137,6 +137,27 @@ __device__ __forceinline__ unsigned long long leaf_key(unsigned long long path, 
   return path | (1ull << (63 - depth));
 }
 
+// Publication of pooled subtrees and the last decrement of a shared tree
+// (P2C_ACQ_REL): a release store of the task tag and an acquire load by its
+// taker, and an acquire-release decrement of the tree's outstanding units,
+// instead of full fences around relaxed accesses.
+#ifndef P2C_ACQ_REL
+#define P2C_ACQ_REL 1
+#endif
+__device__ __forceinline__ void store_release(unsigned long long* p, unsigned long long v) {
+  asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long load_acquire(const unsigned long long* p) {
+  unsigned long long v;
+  asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ unsigned decrement_acq_rel(unsigned* p) {  // returns the value before
+  unsigned old;
+  asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(0xffffffffu) : "memory");
+  return old;
+}
+
 __device__ __forceinline__ unsigned long long volatile_load(const unsigned long long* p) {
   return *reinterpret_cast<const volatile unsigned long long*>(p);
 }
@@ -380,14 +401,14 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
           // the slot was reserved by a producer that publishes it right after;
           // wait for its tag, bounded by the time budget
           const SubtreeTask* tk = pools.tasks + h + (unsigned long long)r;
-          unsigned long long tag = volatile_load(&tk->tag);
+          unsigned long long tag = P2C_ACQ_REL ? load_acquire(&tk->tag) : volatile_load(&tk->tag);
           for (unsigned spin = 0; tag == 0ull; ++spin) {
             __nanosleep(64);
-            tag = volatile_load(&tk->tag);
+            tag = P2C_ACQ_REL ? load_acquire(&tk->tag) : volatile_load(&tk->tag);
             if ((spin & 255u) == 255u && prm.budget_ns != 0ull && (global_ns() - t_start) > prm.budget_ns) break;
           }
           if (tag != 0ull) {
-            __threadfence();
+            if (!P2C_ACQ_REL) __threadfence();
             tag -= 1ull;
             const int f = (int)(tag & 1ull) + 1;
             const int d = (int)((tag >> 1) & 127ull);
@@ -617,10 +638,15 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
               atomicAdd(&pools.aggs[gi].outstanding, 1u);
               SubtreeTask* tk = pools.tasks + task;
               tk->path = (path & top_bits(l - 1)) | (1ull << b);
-              __threadfence();
               const unsigned long long q = (unsigned long long)ws.qidx[slot];
-              atomicExch(&tk->tag, ((q << 24) | ((unsigned long long)gi << 8) | ((unsigned long long)l << 1) |
-                                    (unsigned long long)(fam - 1)) + 1ull);
+              const unsigned long long tag = ((q << 24) | ((unsigned long long)gi << 8) |
+                                              ((unsigned long long)l << 1) | (unsigned long long)(fam - 1)) + 1ull;
+              if (P2C_ACQ_REL) {
+                store_release(&tk->tag, tag);
+              } else {
+                __threadfence();
+                atomicExch(&tk->tag, tag);
+              }
               st.donations += 1;
             }
           }
@@ -643,9 +669,15 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
       const int gi = sa.gidx[s];
       const bool last_here = atomicSub(&sa.outstanding[s], 1) == 1;
       if (gi >= 0) {
-        __threadfence();
-        if (atomicSub(&pools.aggs[gi].outstanding, 1u) == 1u) {
+        bool last = false;
+        if (P2C_ACQ_REL) {
+          last = decrement_acq_rel(&pools.aggs[gi].outstanding) == 1u;
+        } else {
           __threadfence();
+          last = atomicSub(&pools.aggs[gi].outstanding, 1u) == 1u;
+          if (last) __threadfence();
+        }
+        if (last) {
           const TreeAgg& A = pools.aggs[gi];
           const Outcome o = outcome_from(volatile_load(&A.coll_key), volatile_load(&A.margin_bits),
                                          volatile_load(&A.undecided) != 0u, T0, T1);
