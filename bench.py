@@ -1302,6 +1302,7 @@ def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
                             **latency_stats(done_r),
                             "p50_ms_per_100k_tris": float(np.percentile(per, 50)),
                             "p99_ms_per_100k_tris": float(np.percentile(per, 99)),
+                            "by_mesh": _latency_by_mesh(done_r, keys, host),
                             "admission_lag_p99_ms": float(np.percentile([r.admit_lag_ms for r in done_r], 99))}
         eng.close()
         out[narrow] = res
@@ -1366,6 +1367,19 @@ def serve_bench(args, dev, rank: int, cpu_budget: float | None) -> dict:
             block["served_certify_all_over_reference_gpu"] = (out["certify"]["capacity"]["steps_per_s"]
                                                               / ref["steps_per_s"])
     return block
+
+
+def _latency_by_mesh(done, keys, host) -> dict:
+    """p50 / p99 latency of each mesh's requests (its triangle count beside)."""
+    import numpy as np
+
+    out = {}
+    for k in keys:
+        lat = [r.latency_ms for r in done if r.mesh == k]
+        if lat:
+            out[k] = {"triangles": int(host[k][2]), "requests": len(lat), "p50_ms": float(np.percentile(lat, 50)),
+                      "p99_ms": float(np.percentile(lat, 99))}
+    return out
 
 
 def _reference_gpu_step_ms(pipe, cfg) -> float | None:
