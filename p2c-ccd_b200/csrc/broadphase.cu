@@ -77,18 +77,6 @@ struct Lists {
   __device__ __forceinline__ int list_of(long long g) const { return g < off[1] ? 0 : (g < off[2] ? 1 : 2); }
 };
 
-__global__ void init_scratch_kernel(BroadScratch* sc) {
-  const int t = threadIdx.x;
-  for (int i = t; i < kMaxCullObjects * 3; i += blockDim.x) {
-    (&sc->obj_lo[0][0])[i] = ~0ull;
-    (&sc->obj_hi[0][0])[i] = 0ull;
-  }
-  if (t < 9) {
-    sc->list[t / 3].lo_min[t % 3] = ~0ull;
-    sc->list[t / 3].hi_max[t % 3] = 0ull;
-  }
-}
-
 // Block sums of the per-axis statistics that choose the sweep axis (extents,
 // centres and squared centres of the boxes), ten atomics per block.
 __device__ __forceinline__ void axis_stats(const double b[6], bool live, BroadScratch* sc) {
@@ -163,7 +151,7 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
           kmax = max(kmax, __shfl_xor_sync(kFull, kmax, s));
         }
         if (lane == leader) {
-          atomicMin(&sc->obj_lo[lo_obj][a], kmin);
+          atomicMax(&sc->obj_nlo[lo_obj][a], ~kmin);
           atomicMax(&sc->obj_hi[lo_obj][a], kmax);
         }
       }
@@ -174,6 +162,91 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
 #endif
 }
 
+// Sweep axis, column grid, sweep-axis quantiser and list segments, by one
+// thread of the last block of the cull launch.  two_body: self pairs are
+// excluded and the scene has two objects, so the keys split by object unless
+// an id other than 0 and 1 was kept.
+__device__ void compute_grid(BroadScratch* sc, int qbits, int two_body) {
+  const double n = sc->count > 0 ? (double)sc->count : 1.0;
+  int axis = 0;
+  double best = INFINITY;
+  for (int a = 0; a < 3; ++a) {
+    const double mean = sc->center_sum[a] / n;
+    const double var = fmax(sc->center_sq_sum[a] / n - mean * mean, 0.0);
+    const double score = (sc->extent_sum[a] / n) / (sqrt(var) + 1e-300);
+    if (score < best) {
+      best = score;
+      axis = a;
+    }
+  }
+  Grid g;
+#ifdef P2C_FORCE_AXIS
+  axis = P2C_FORCE_AXIS;
+#endif
+  g.axis = axis;
+  g.a1 = axis == 0 ? 1 : 0;
+  g.a2 = axis == 2 ? 1 : 2;
+  g.qbits = qbits;
+  const bool split = two_body != 0 && __ldcg(&sc->obj_other) == 0ull;
+  g.split_shift = split ? qbits - 1 : -1;
+  g.qmax = (1u << (split ? qbits - 1 : qbits)) - 1u;
+  const int ax[3] = {g.a1, g.a2, axis};
+  // the kept boxes' counts and extents, summed by every block of the cull
+  // launch (read past L1)
+  unsigned long long active[3], ext_max[3][3], lo_min[3][3], hi_max[3][3];
+  for (int l = 0; l < 3; ++l) {
+    active[l] = __ldcg(&sc->list[l].active);
+    for (int a = 0; a < 3; ++a) {
+      ext_max[l][a] = __ldcg(&sc->list[l].ext_max[a]);
+      lo_min[l][a] = ~__ldcg(&sc->list[l].nlo_min[a]);
+      hi_max[l][a] = __ldcg(&sc->list[l].hi_max[a]);
+    }
+  }
+  double base[3], inv[3];
+  int cols[2] = {1, 1};
+  for (int k = 0; k < 3; ++k) {
+    double lo = INFINITY, hi = -INFINITY, reach = 0.0;
+    for (int l = 0; l < 3; ++l) {
+      const double r = active[l] ? __longlong_as_double((long long)ext_max[l][ax[k]]) : 0.0;
+      if (k < 2) (k == 0 ? g.reach1 : g.reach2)[l] = r;
+      if (active[l] == 0) continue;
+      lo = fmin(lo, unorder_key(lo_min[l][ax[k]]));
+      hi = fmax(hi, unorder_key(hi_max[l][ax[k]]));
+      reach = fmax(reach, r);
+    }
+    const double range = (hi > lo) ? hi - lo : 0.0;
+    base[k] = isfinite(lo) ? lo : 0.0;
+    if (k < 2) {
+      double width = fmax(reach, range / kMaxColumns);
+      if (!(width > 0.0) || !isfinite(width)) width = 1.0;
+      int c = (int)fmin((double)kMaxColumns, floor(range / width) + 1.0);
+      cols[k] = c < 1 ? 1 : c;
+      inv[k] = 1.0 / width;
+    } else {
+      inv[k] = (range > 0.0 && isfinite(range)) ? (double)g.qmax / range : 0.0;
+    }
+  }
+  g.base1 = base[0];
+  g.base2 = base[1];
+  g.inv1 = inv[0];
+  g.inv2 = inv[1];
+  g.g1 = cols[0];
+  g.g2 = cols[1];
+  g.base0 = base[2];
+  g.scale0 = inv[2];
+  g.seg[0] = 0;
+  g.seg[1] = active[0];
+  g.seg[2] = g.seg[1] + active[1];
+  g.seg[3] = g.seg[2] + active[2];
+  sc->grid = g;
+}
+
+__global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
+  pdl_wait();
+  pdl_trigger();
+  compute_grid(sc, qbits, two_body);
+}
+
 // Every primitive's swept box (Swept*Box, :256-301), kept unless it is a
 // vertex in no face or (self pairs excluded) it lies outside every other
 // object's envelope.  Kept boxes are appended (one atomic per warp) to a
@@ -182,7 +255,8 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(const double* __rest
 __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict__ v_t0,
                                                         const double* __restrict__ v_t1, Lists L, double thickness,
                                                         int cull_objects, int ordered, double* __restrict__ cbox,
-                                                        unsigned* __restrict__ cprim, BroadScratch* sc) {
+                                                        unsigned* __restrict__ cprim, BroadScratch* sc, int qbits,
+                                                        int two_body) {
   pdl_wait();
   pdl_trigger();
   const long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -204,7 +278,7 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict
         bool ov = true;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double olo = unorder_key(sc->obj_lo[q][a]), ohi = unorder_key(sc->obj_hi[q][a]);
+          const double olo = unorder_key(~sc->obj_nlo[q][a]), ohi = unorder_key(sc->obj_hi[q][a]);
           ov = ov && b[a] <= ohi && olo <= b[3 + a];
         }
         near_other = ov;
@@ -264,7 +338,7 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict
       }
       if ((threadIdx.x & 31) == 0) {
         atomicMax(&S.ext_max[a], ext);
-        atomicMin(&S.lo_min[a], lo);
+        atomicMax(&S.nlo_min[a], ~lo);
         atomicMax(&S.hi_max[a], hi);
       }
     }
@@ -272,77 +346,20 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(const double* __restrict
 #ifdef P2C_STATS_ALL
   axis_stats(b, g < L.off[3], sc);
 #endif
+  // the last block to finish sizes the grid from everyone's sums
+  __shared__ bool last_block;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    last_block = atomicAdd(&sc->blocks_done, 1u) == gridDim.x - 1u;
+  }
+  __syncthreads();
+  if (last_block && threadIdx.x == 0) {
+    __threadfence();
+    compute_grid(sc, qbits, two_body);
+  }
 }
 
-// Sweep axis, column grid, sweep-axis quantiser and list segments (one
-// thread).  two_body: self pairs are excluded and the scene has two objects,
-// so the keys split by object unless an id other than 0 and 1 was kept.
-__global__ void grid_kernel(BroadScratch* sc, int qbits, int two_body) {
-  pdl_wait();
-  pdl_trigger();
-  const double n = sc->count > 0 ? (double)sc->count : 1.0;
-  int axis = 0;
-  double best = INFINITY;
-  for (int a = 0; a < 3; ++a) {
-    const double mean = sc->center_sum[a] / n;
-    const double var = fmax(sc->center_sq_sum[a] / n - mean * mean, 0.0);
-    const double score = (sc->extent_sum[a] / n) / (sqrt(var) + 1e-300);
-    if (score < best) {
-      best = score;
-      axis = a;
-    }
-  }
-  Grid g;
-#ifdef P2C_FORCE_AXIS
-  axis = P2C_FORCE_AXIS;
-#endif
-  g.axis = axis;
-  g.a1 = axis == 0 ? 1 : 0;
-  g.a2 = axis == 2 ? 1 : 2;
-  g.qbits = qbits;
-  const bool split = two_body != 0 && sc->obj_other == 0ull;
-  g.split_shift = split ? qbits - 1 : -1;
-  g.qmax = (1u << (split ? qbits - 1 : qbits)) - 1u;
-  const int ax[3] = {g.a1, g.a2, axis};
-  double base[3], inv[3];
-  int cols[2] = {1, 1};
-  for (int k = 0; k < 3; ++k) {
-    double lo = INFINITY, hi = -INFINITY, reach = 0.0;
-    for (int l = 0; l < 3; ++l) {
-      const ListStats& L = sc->list[l];
-      const double r = L.active ? __longlong_as_double((long long)L.ext_max[ax[k]]) : 0.0;
-      if (k < 2) (k == 0 ? g.reach1 : g.reach2)[l] = r;
-      if (L.active == 0) continue;
-      lo = fmin(lo, unorder_key(L.lo_min[ax[k]]));
-      hi = fmax(hi, unorder_key(L.hi_max[ax[k]]));
-      reach = fmax(reach, r);
-    }
-    const double range = (hi > lo) ? hi - lo : 0.0;
-    base[k] = isfinite(lo) ? lo : 0.0;
-    if (k < 2) {
-      double width = fmax(reach, range / kMaxColumns);
-      if (!(width > 0.0) || !isfinite(width)) width = 1.0;
-      int c = (int)fmin((double)kMaxColumns, floor(range / width) + 1.0);
-      cols[k] = c < 1 ? 1 : c;
-      inv[k] = 1.0 / width;
-    } else {
-      inv[k] = (range > 0.0 && isfinite(range)) ? (double)g.qmax / range : 0.0;
-    }
-  }
-  g.base1 = base[0];
-  g.base2 = base[1];
-  g.inv1 = inv[0];
-  g.inv2 = inv[1];
-  g.g1 = cols[0];
-  g.g2 = cols[1];
-  g.base0 = base[2];
-  g.scale0 = inv[2];
-  g.seg[0] = 0;
-  g.seg[1] = sc->list[0].active;
-  g.seg[2] = g.seg[1] + sc->list[1].active;
-  g.seg[3] = g.seg[2] + sc->list[2].active;
-  sc->grid = g;
-}
 
 // Sort key of every kept box (compact entry c, value c).  The order of the
 // compact entries does not matter: they are sorted on their full keys and
@@ -673,11 +690,20 @@ __device__ __forceinline__ void small_sort_tile(unsigned long long* p, long long
     p[i] = ~0ull;  // padding beyond the tile
 }
 
+__device__ __forceinline__ void export_counts(const BroadScratch* sc, unsigned long long* counts) {
+  counts[0] = sc->vf_count;
+  counts[1] = sc->ee_count;
+  counts[2] = sc->error_word;
+  counts[3] = (unsigned long long)sc->grid.axis | ((unsigned long long)sc->grid.g1 << 8) |
+              ((unsigned long long)sc->grid.g2 << 24) | (sc->grid.seg[3] << 40);
+}
+
 __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
     unsigned long long* vf, long long vf_cap, int vf_bits, int vf_shift, unsigned long long* ee, long long ee_cap,
-    int ee_bits, int ee_shift, const BroadScratch* sc) {
+    int ee_bits, int ee_shift, const BroadScratch* sc, unsigned long long* counts) {
   pdl_wait();
   pdl_trigger();
+  if (blockIdx.x == 0 && threadIdx.x == 0) export_counts(sc, counts);  // final once the sweeps are done
   extern __shared__ __align__(16) unsigned char smem_sort[];
   const bool is_vf = blockIdx.x == 0;
   unsigned long long* p = is_vf ? vf : ee;
@@ -695,11 +721,7 @@ __global__ void __launch_bounds__(kSmallSortThreads) small_sort_pairs_kernel(
 __global__ void export_counts_kernel(const BroadScratch* sc, unsigned long long* counts) {
   pdl_wait();
   pdl_trigger();
-  counts[0] = sc->vf_count;
-  counts[1] = sc->ee_count;
-  counts[2] = sc->error_word;
-  counts[3] = (unsigned long long)sc->grid.axis | ((unsigned long long)sc->grid.g1 << 8) |
-              ((unsigned long long)sc->grid.g2 << 24) | (sc->grid.seg[3] << 40);
+  export_counts(sc, counts);
 }
 
 // ---- workspace carving -----------------------------------------------------
@@ -902,16 +924,16 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
   if (rc != P2C_OK) return rc;
   P2C_CUDA(cudaMemsetAsync(L.sc, 0, sizeof(BroadScratch), s));
   P2C_CUDA(cudaMemsetAsync(L.cells, 0, sizeof(unsigned) * 6 * kCells, s));
-  init_scratch_kernel<<<1, 256, 0, s>>>(L.sc);
   if (scene.nv > 0)
     P2C_CUDA(launch_pdl(envelope_kernel, dim3(grid_for(scene.nv, kThreads)), dim3(kThreads), 0, s, scene.v_t0,
                         scene.v_t1, scene.v_obj, (long long)scene.nv, scene.thickness, cull, L.sc));
-  if (n > 0)
-    P2C_CUDA(launch_pdl(cull_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
-                        lists, scene.thickness, cull, ordered ? 1 : 0, L.cbox, L.cprim, L.sc));
   const int qbits = n <= kSmallSceneQPrims ? kQBitsSmall : kQBitsLarge;
   const int two_body = scene.exclude_self && scene.n_obj == 2 ? 1 : 0;
-  P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
+  if (n > 0)
+    P2C_CUDA(launch_pdl(cull_kernel, dim3(grid_for(n, kThreads)), dim3(kThreads), 0, s, scene.v_t0, scene.v_t1,
+                        lists, scene.thickness, cull, ordered ? 1 : 0, L.cbox, L.cprim, L.sc, qbits, two_body));
+  else  // no primitive, no cull launch: the (empty) grid on its own
+    P2C_CUDA(launch_pdl(grid_kernel, dim3(1), dim3(1), 0, s, L.sc, qbits, two_body));
   if (n > 0) {
     const unsigned loop_grid = std::min(grid_for(n, kThreads), resident_grid(gather_kernel, info));
     // The library's onesweep sort over all n entries (the culled ones padded
@@ -991,7 +1013,7 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     }
     P2C_CUDA(launch_pdl(small_sort_pairs_kernel, dim3(2), dim3(kSmallSortThreads), kSmallSortSmem, s,
                         vf_out, vf_cap, bit_length(scene.nv) + vf_shift, vf_shift, ee_out, ee_cap,
-                        bit_length(scene.ne) + ee_shift, ee_shift, (const BroadScratch*)L.sc));
+                        bit_length(scene.ne) + ee_shift, ee_shift, (const BroadScratch*)L.sc, counts_dev));
   } else if (sort_out) {
     int rc = sort_pairs(vf_out, vf_cap, bit_length(scene.nv) + vf_shift, L, s);
     if (rc != P2C_OK) return rc;
@@ -1000,7 +1022,8 @@ int launch_broadphase(const p2c_scene& scene, unsigned long long* vf_out, long l
     if (vf_cap > 0) unpack_pairs_kernel<<<grid_for(vf_cap, 256), 256, 0, s>>>(vf_out, vf_cap, vf_shift);
     if (ee_cap > 0) unpack_pairs_kernel<<<grid_for(ee_cap, 256), 256, 0, s>>>(ee_out, ee_cap, ee_shift);
   }
-  P2C_CUDA(launch_pdl(export_counts_kernel, dim3(1), dim3(1), 0, s, (const BroadScratch*)L.sc, counts_dev));
+  if (!small_sort)  // the block sort writes the counts itself
+    P2C_CUDA(launch_pdl(export_counts_kernel, dim3(1), dim3(1), 0, s, (const BroadScratch*)L.sc, counts_dev));
   P2C_CUDA(cudaGetLastError());
   return P2C_OK;
 }

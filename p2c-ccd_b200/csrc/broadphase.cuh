@@ -61,7 +61,7 @@ struct BoxList {
 struct ListStats {
   unsigned long long active;     // boxes kept
   unsigned long long ext_max[3]; // bit pattern of the largest extent per axis (non-negative)
-  unsigned long long lo_min[3];  // order_key of the smallest min per axis
+  unsigned long long nlo_min[3]; // ~order_key of the smallest min per axis (raised by atomicMax: zero = empty)
   unsigned long long hi_max[3];  // order_key of the largest max per axis
 };
 
@@ -84,7 +84,7 @@ struct Grid {
 struct BroadScratch {
   double extent_sum[3], center_sum[3], center_sq_sum[3];
   unsigned long long count;
-  unsigned long long obj_lo[kMaxCullObjects][3];  // order keys of object swept boxes
+  unsigned long long obj_nlo[kMaxCullObjects][3];  // ~order keys of the objects' swept-box minima (zero = empty)
   unsigned long long obj_hi[kMaxCullObjects][3];
   ListStats list[3];  // 0 vertices, 1 faces, 2 edges
   Grid grid;
@@ -94,6 +94,7 @@ struct BroadScratch {
   unsigned long long obj_other;   // non-zero: a kept primitive's object id is neither 0 nor 1
   unsigned long long keyed;       // single scene: boxes kept after culling (compact entries)
   unsigned long long sweep_next[2];  // single scene: next slot of the vertex-face / edge-edge sweep
+  unsigned blocks_done;              // single scene: cull blocks finished (the last sizes the grid)
 };
 
 // The next 32 sweep slots for the calling warp (one atomic per warp).

@@ -8,8 +8,8 @@
 // indexed scene-major (scene s holds [P[s], P[s+1]): its vertices, faces,
 // edges); every kernel finds a primitive's scene by binary search over P.
 //   1. prep (one block): prefix offsets of primitives, vertices, pair
-//      capacities and column tables per scene (scratch minima set by a
-//      block per scene);
+//      capacities and column tables per scene (minima are kept as
+//      complemented keys, so the zeroed scratch starts empty);
 //   2. vertex swept boxes: object envelopes and per-scene axis statistics
 //      (block-level sums when a block holds one scene, warp-level otherwise);
 //   3. every primitive's swept box, culled against the other objects'
@@ -146,14 +146,6 @@ __device__ __forceinline__ int cull_count(const p2c_batch_scene& d) {
 }
 
 // ---- 1. prep -----------------------------------------------------------------
-// Minima start at ~0 and maxima at 0 (the scratch is zeroed before): one
-// block per scene.
-__global__ void init_scenes_kernel(BatchBroad B) {
-  BroadScratch& sc = B.sc[blockIdx.x];
-  for (int k = threadIdx.x; k < kMaxCullObjects * 3; k += blockDim.x) (&sc.obj_lo[0][0])[k] = ~0ull;
-  if (threadIdx.x < 9) sc.list[threadIdx.x / 3].lo_min[threadIdx.x % 3] = ~0ull;
-}
-
 __global__ void __launch_bounds__(kPrepThreads) prep_kernel(BatchBroad B) {
   using Scan = cub::BlockScan<unsigned long long, kPrepThreads>;
   __shared__ typename Scan::TempStorage tmp;
@@ -231,7 +223,7 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(BatchBroad B, unsign
           kmax = max(kmax, __shfl_xor_sync(kFull, kmax, sh));
         }
         if (lane == leader) {
-          atomicMin(&B.sc[ls].obj_lo[lo_obj][a], kmin);
+          atomicMax(&B.sc[ls].obj_nlo[lo_obj][a], ~kmin);
           atomicMax(&B.sc[ls].obj_hi[lo_obj][a], kmax);
         }
       }
@@ -296,9 +288,6 @@ __global__ void __launch_bounds__(kThreads) envelope_kernel(BatchBroad B, unsign
 __device__ __forceinline__ void max_if_larger(unsigned long long* p, unsigned long long v) {
   if (v > *reinterpret_cast<volatile unsigned long long*>(p)) atomicMax(p, v);
 }
-__device__ __forceinline__ void min_if_smaller(unsigned long long* p, unsigned long long v) {
-  if (v < *reinterpret_cast<volatile unsigned long long*>(p)) atomicMin(p, v);
-}
 
 // One thread per primitive: its swept box; kept unless it is a vertex in no
 // face or (self pairs excluded) it lies outside every other object's
@@ -333,7 +322,7 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(BatchBroad B, unsigned l
         bool ov = true;
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-          const double olo = unorder_key(sc.obj_lo[q][a]), ohi = unorder_key(sc.obj_hi[q][a]);
+          const double olo = unorder_key(~sc.obj_nlo[q][a]), ohi = unorder_key(sc.obj_hi[q][a]);
           ov = ov && b[a] <= ohi && olo <= b[3 + a];
         }
         near_other = ov;
@@ -384,7 +373,7 @@ __global__ void __launch_bounds__(kThreads) cull_kernel(BatchBroad B, unsigned l
       }
       if ((threadIdx.x & 31) == leader) {
         max_if_larger(&S.ext_max[a], ext);
-        min_if_smaller(&S.lo_min[a], lo);
+        max_if_larger(&S.nlo_min[a], ~lo);
         max_if_larger(&S.hi_max[a], hi);
       }
     }
@@ -431,7 +420,7 @@ __global__ void grid_kernel(BatchBroad B) {
       const double r = L.active ? __longlong_as_double((long long)L.ext_max[ax[k]]) : 0.0;
       if (k < 2) (k == 0 ? g.reach1 : g.reach2)[l] = r;
       if (L.active == 0) continue;
-      lo = fmin(lo, unorder_key(L.lo_min[ax[k]]));
+      lo = fmin(lo, unorder_key(~L.nlo_min[ax[k]]));
       hi = fmax(hi, unorder_key(L.hi_max[ax[k]]));
       reach = fmax(reach, r);
     }
@@ -1050,7 +1039,6 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   P2C_CUDA(cudaMemsetAsync(B.n_keyed, 0, sizeof(unsigned long long), s));
   P2C_CUDA(cudaMemsetAsync(B.chunk_count, 0, 2 * sizeof(unsigned long long), s));
   P2C_CUDA(cudaMemsetAsync(B.sweep_next, 0, 2 * sizeof(unsigned long long), s));
-  init_scenes_kernel<<<n, 128, 0, s>>>(B);
   prep_kernel<<<1, kPrepThreads, 0, s>>>(B);
   P2C_CUDA(cudaGetLastError());
   const unsigned long long P = t.P;
