@@ -419,12 +419,25 @@ int complete_group(ServeState& S, Slot& sl) {
   return P2C_OK;
 }
 
-// Admit waiting requests into a free slot: as many as max_group allows while
-// the group's memory fits a free range of the arena.
+// Triangles a group takes before it closes (a larger request still forms a
+// group alone): a long step holds its whole group, so small requests are not
+// batched behind it and the slots stay busy with work of similar length.
+#ifndef P2C_SERVE_GROUP_TRIANGLES
+#define P2C_SERVE_GROUP_TRIANGLES 600000
+#endif
+constexpr long long kGroupTriangles = P2C_SERVE_GROUP_TRIANGLES;
+
+// Admit waiting requests into a free slot, in arrival order: as many as
+// max_group allows while the group stays within kGroupTriangles and its
+// memory fits a free range of the arena.
 int admit_into(ServeState& S, Slot& sl, bool others_in_flight) {
   std::vector<Req> group;
   GroupPlan plan;
+  long long tris = 0;
   while (!S.pending.empty() && (int)group.size() < S.cfg.max_group) {
+    const long long nf = S.meshes[S.pending.front().r.mesh_id].nf;
+    if (!group.empty() && tris + nf > kGroupTriangles) break;
+    tris += nf;
     group.push_back(S.pending.front());
     GroupPlan p = plan_group(S, group);
     const size_t o = S.arena.alloc(p.total);  // does the larger group still fit a free range?
