@@ -759,8 +759,13 @@ __device__ __forceinline__ void sweep_vf_slot(const BatchBroad& B, unsigned long
 
 // Every (kept box, lane) slot, taken 32 at a time by whichever warp is free
 // (the number of kept boxes is known only on the device).
-__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_vf_kernel(BatchBroad B) {
+__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_vf_kernel(BatchBroad B, int dynamic) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
+  if (!dynamic) {  // one slot per thread, the grid sized for every primitive
+    const unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x;
+    if (base < work) sweep_vf_slot(B, base + threadIdx.x, n);
+    return;
+  }
   for (;;) {
     const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 0);
     if (base >= work) break;
@@ -812,8 +817,13 @@ __device__ __forceinline__ void sweep_ee_slot(const BatchBroad& B, unsigned long
   }
 }
 
-__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_ee_kernel(BatchBroad B) {
+__global__ void __launch_bounds__(kThreads, kBatchSweepBlocks) sweep_ee_kernel(BatchBroad B, int dynamic) {
   const unsigned long long n = *B.n_keyed, work = n * kBatchSweepLanes;
+  if (!dynamic) {  // one slot per thread, the grid sized for every primitive
+    const unsigned long long base = (unsigned long long)blockIdx.x * blockDim.x;
+    if (base < work) sweep_ee_slot(B, base + threadIdx.x, n);
+    return;
+  }
   for (;;) {
     const unsigned long long base = (unsigned long long)next_warp_slots(B.sweep_next + 1);
     if (base >= work) break;
@@ -1049,13 +1059,13 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   DeviceInfo info;
   int rc = current_device_info(&info);
   if (rc != P2C_OK) return rc;
+  bool any_cull = false;
+  for (int k = 0; k < n && !any_cull; ++k)
+    any_cull = h[k].exclude_self && h[k].n_obj >= 1 && h[k].n_obj <= kMaxCullObjects;
   if (P > 0) {
     // No scene culls: nearly every box is kept, and the library's onesweep
     // sort over all P entries (the others padded to sort last) beats ranking
     // them with the count sort; otherwise only the kept boxes are ranked.
-    bool any_cull = false;
-    for (int k = 0; k < n && !any_cull; ++k)
-      any_cull = h[k].exclude_self && h[k].n_obj >= 1 && h[k].n_obj <= kMaxCullObjects;
     keys_kernel<<<std::min(grid_for((long long)P, kThreads), resident_grid(keys_kernel, info)), kThreads, 0, s>>>(B, any_cull ? 0ull : P);
     P2C_CUDA(cudaGetLastError());
     bool second = false;
@@ -1092,9 +1102,19 @@ int launch_batch_candidates(const p2c_batch_scene* h, const p2c_batch_scene* dev
   }
   P2C_CUDA(cudaGetLastError());
   if (P > 0) {
+    // with culling (often a few per cent kept) warps take sweep slots from a
+    // counter over a resident grid; without, one slot per thread over a grid
+    // for every primitive (faster on dense sheets: no slot fetches)
+#ifdef P2C_BATCH_SWEEP_DYNAMIC
+    const int dynamic = P2C_BATCH_SWEEP_DYNAMIC;
+#else
+    const int dynamic = any_cull ? 1 : 0;
+#endif
     const unsigned slots = grid_for((long long)P * kBatchSweepLanes, kThreads);
-    if (t.vf > 0) sweep_vf_kernel<<<std::min(slots, resident_grid(sweep_vf_kernel, info)), kThreads, 0, s>>>(B);
-    if (t.ee > 0) sweep_ee_kernel<<<std::min(slots, resident_grid(sweep_ee_kernel, info)), kThreads, 0, s>>>(B);
+    const unsigned vf_grid = dynamic ? std::min(slots, resident_grid(sweep_vf_kernel, info)) : slots;
+    const unsigned ee_grid = dynamic ? std::min(slots, resident_grid(sweep_ee_kernel, info)) : slots;
+    if (t.vf > 0) sweep_vf_kernel<<<vf_grid, kThreads, 0, s>>>(B, dynamic);
+    if (t.ee > 0) sweep_ee_kernel<<<ee_grid, kThreads, 0, s>>>(B, dynamic);
     if (t.vf > 0) chunk_kernel<1><<<resident_grid(chunk_kernel<1>, info), kThreads, 0, s>>>(B);
     if (t.ee > 0) chunk_kernel<2><<<resident_grid(chunk_kernel<2>, info), kThreads, 0, s>>>(B);
     P2C_CUDA(cudaGetLastError());
