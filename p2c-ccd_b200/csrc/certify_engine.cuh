@@ -613,7 +613,7 @@ __device__ bool run_engine(const P& prob, const CertParams& prm, int fetch1, int
         if (me) {
           int gi = sa.gidx[slot];
           // a tree's first export moves its reduction from the slot to a pooled
-          // record; one lane of the warp claims the move (others skip this round)
+          // record; one lane of the warp claims the move (others skip this iteration)
           if (gi == -1 && atomicCAS(&sa.gidx[slot], -1, -2) == -1) {
             const unsigned long long idx = atomicAdd(&es->agg_next.v, 1ull);
             if (idx < pools.agg_cap) {
