@@ -499,7 +499,9 @@ int p2c_batch_anyhit(const p2c_batch_scene* scenes_host, const p2c_batch_scene* 
  * creation.  Requests are CCD steps of a registered mesh (the vertex
  * trajectories of one step, host memory).  p2c_serve_poll retires finished
  * groups and admits waiting requests, in admission order, into free slots:
- * the requests admitted together form a group on the slot's own stream
+ * the requests admitted together (up to max_group, and up to 600,000
+ * triangles unless one request alone is larger) form a group on the slot's
+ * own stream
  * (trajectories in; candidates of every request in one p2c_batch_candidates
  * sequence; then either the certificates of every candidate, one
  * p2c_batch_certify launch, or the scheduled any-hit with fallback replay of
