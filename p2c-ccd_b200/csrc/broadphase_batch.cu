@@ -577,7 +577,10 @@ __device__ __forceinline__ SortedBoxes scene_view(const BatchBroad& B, int s, in
 // Lanes that share one scanning box's columns in the batched sweeps: 2
 // (the batch fills the GPU many times over, so splitting further only adds
 // work; 256 uneven scenes: 11.4 ms with 1 lane, 11.1 with 2, 12.2 with 4).
-constexpr int kBatchSweepLanes = 2;
+#ifndef P2C_BATCH_SWEEP_LANES
+#define P2C_BATCH_SWEEP_LANES 2
+#endif
+constexpr int kBatchSweepLanes = P2C_BATCH_SWEEP_LANES;
 #ifndef P2C_BATCH_SWEEP_BLOCKS
 #define P2C_BATCH_SWEEP_BLOCKS 4
 #endif
